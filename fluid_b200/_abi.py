@@ -1,0 +1,98 @@
+"""ctypes binding of ``include/fluid_pp.h`` (``fluid_b200/_lib/libfluid_pp.so``).
+
+There is no fallback: if the CUDA library is missing the import fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libfluid_pp.so")
+
+OK, INVALID_ARG, OOM, NONFINITE, NONCONVERGENCE, TIMEOUT, CUDA, UNSUPPORTED = range(8)
+STATUS_NAMES = {OK: "OK", INVALID_ARG: "INVALID_ARG", OOM: "OOM", NONFINITE: "NONFINITE",
+                NONCONVERGENCE: "NONCONVERGENCE", TIMEOUT: "TIMEOUT", CUDA: "CUDA", UNSUPPORTED: "UNSUPPORTED"}
+PRECISIONS = {"fp32": 0, "fp16": 1, "bf16": 2}
+MAX_LEVELS = 24
+
+# Every symbol include/fluid_pp.h declares (checked by the CPU test suite).
+EXPORTS = (
+    "fluid_pp_plan_hierarchy", "fluid_pp_create", "fluid_pp_destroy", "fluid_pp_set_stream",
+    "fluid_pp_upload_state", "fluid_pp_upload_state_device", "fluid_pp_project", "fluid_pp_project_async",
+    "fluid_pp_receipt_read", "fluid_pp_download", "fluid_pp_device_arrays", "fluid_pp_last_error",
+    "fluid_pp_prepare", "fluid_pp_level_dims", "fluid_pp_get_level", "fluid_pp_get_rhs",
+    "fluid_pp_apply_operator", "fluid_pp_apply_vcycle", "fluid_pp_get_pressure_cells",
+    "fluid_pp_batch_create", "fluid_pp_batch_destroy", "fluid_pp_batch_project",
+)
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("h", ctypes.c_float),
+                ("rho", ctypes.c_float), ("open_top", ctypes.c_int), ("precision", ctypes.c_int),
+                ("device", ctypes.c_int)]
+
+
+class SolveOpts(ctypes.Structure):
+    _fields_ = [("rel_tol", ctypes.c_double), ("abs_tol", ctypes.c_double), ("max_iters", ctypes.c_int),
+                ("pre_sweeps", ctypes.c_int), ("post_sweeps", ctypes.c_int),
+                ("true_residual_every", ctypes.c_int), ("warm_start", ctypes.c_int)]
+
+
+class Receipt(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("iterations", ctypes.c_int), ("liquid_cells", ctypes.c_int),
+                ("levels", ctypes.c_int), ("b_norm", ctypes.c_double), ("rel_residual", ctypes.c_double),
+                ("true_rel_residual", ctypes.c_double), ("max_div_before", ctypes.c_double),
+                ("max_div_after", ctypes.c_double), ("l2_div_before", ctypes.c_double),
+                ("l2_div_after", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["status_name"] = STATUS_NAMES.get(self.status, str(self.status))
+        return d
+
+
+_lib = None
+
+
+def load():
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"fluid_b200 CUDA library missing: {LIB_PATH} (run python -m fluid_b200.build)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, ci, cf = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    pi = ctypes.POINTER(ctypes.c_int)
+    L.fluid_pp_plan_hierarchy.argtypes = [ci, ci, ci, pi, vp, pi, pi, pi]
+    L.fluid_pp_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(vp)]
+    L.fluid_pp_destroy.argtypes = [vp]
+    L.fluid_pp_destroy.restype = None
+    L.fluid_pp_set_stream.argtypes = [vp, vp]
+    L.fluid_pp_upload_state.argtypes = [vp, vp, vp, vp, vp]
+    L.fluid_pp_upload_state_device.argtypes = [vp, vp, vp, vp, vp]
+    L.fluid_pp_project.argtypes = [vp, cf, ctypes.POINTER(SolveOpts), ctypes.POINTER(Receipt)]
+    L.fluid_pp_project_async.argtypes = [vp, cf, ctypes.POINTER(SolveOpts)]
+    L.fluid_pp_receipt_read.argtypes = [vp, ctypes.POINTER(Receipt)]
+    L.fluid_pp_download.argtypes = [vp, vp, vp, vp, vp]
+    L.fluid_pp_device_arrays.argtypes = [vp] + [ctypes.POINTER(vp)] * 5
+    L.fluid_pp_last_error.argtypes = [vp]
+    L.fluid_pp_last_error.restype = ctypes.c_char_p
+    L.fluid_pp_prepare.argtypes = [vp, cf]
+    L.fluid_pp_level_dims.argtypes = [vp, ci, vp]
+    L.fluid_pp_get_level.argtypes = [vp, ci, vp, vp, vp]
+    L.fluid_pp_get_rhs.argtypes = [vp, vp]
+    L.fluid_pp_apply_operator.argtypes = [vp, vp, vp]
+    L.fluid_pp_apply_vcycle.argtypes = [vp, vp, vp, ci, ci]
+    L.fluid_pp_get_pressure_cells.argtypes = [vp, vp]
+    L.fluid_pp_batch_create.argtypes = [ctypes.POINTER(vp), ci, ctypes.POINTER(vp)]
+    L.fluid_pp_batch_destroy.argtypes = [vp]
+    L.fluid_pp_batch_destroy.restype = None
+    L.fluid_pp_batch_project.argtypes = [vp, vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(Receipt)]
+    _lib = L
+    return L
+
+
+def ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)

@@ -1,0 +1,189 @@
+"""Seeded synthetic inputs for the pressure-projection workloads.
+
+The reference ships no dataset for this path; these generators stand in for
+its scenes.  Every array is float32 with x fastest:
+
+* ``vof``  [nz][ny][nx]    liquid volume fraction per cell
+* ``u``    [nz][ny][nx+1]  x-face normal velocity (m/s), face x between cells x-1, x
+* ``v``    [nz][ny+1][nx]  y-face normal velocity
+* ``w``    [nz+1][ny][nx]  z-face normal velocity
+
+A "fluid face" is an interior face with a liquid cell (vof > 0.5) on either
+side; closed-wall faces are zero.  Gravity enters as ``v += dt * g`` on fluid
+y-faces, the body-force update that precedes the projection in the reference
+step (``lib/methods/uniform/webgpu-uniform-reference.ts:1180-1282``).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+GRAVITY = -9.81
+
+
+@dataclass
+class GridState:
+    nx: int
+    ny: int
+    nz: int
+    h: float
+    dt: float
+    vof: np.ndarray
+    u: np.ndarray
+    v: np.ndarray
+    w: np.ndarray
+    rho: float = 1000.0
+    open_top: bool = False
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def cells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+
+def box_fraction(n: int, lo: float, hi: float) -> np.ndarray:
+    """Per-cell coverage of [lo, hi) (in cell units) along one axis."""
+    i = np.arange(n, dtype=np.float64)
+    return np.clip(np.minimum(i + 1, hi) - np.maximum(i, lo), 0.0, 1.0)
+
+
+def box_vof(nx, ny, nz, lo, hi) -> np.ndarray:
+    fx = box_fraction(nx, lo[0], hi[0])
+    fy = box_fraction(ny, lo[1], hi[1])
+    fz = box_fraction(nz, lo[2], hi[2])
+    return fz[:, None, None] * fy[None, :, None] * fx[None, None, :]
+
+
+def sphere_vof(nx, ny, nz, centre, radius) -> np.ndarray:
+    """Linear ramp of the signed distance over one cell (cell units)."""
+    z, y, x = np.meshgrid(np.arange(nz) + 0.5, np.arange(ny) + 0.5, np.arange(nx) + 0.5, indexing="ij")
+    d = np.sqrt((x - centre[0]) ** 2 + (y - centre[1]) ** 2 + (z - centre[2]) ** 2) - radius
+    return np.clip(0.5 - d, 0.0, 1.0)
+
+
+def fluid_face_masks(vof: np.ndarray):
+    nz, ny, nx = vof.shape
+    liq = vof > np.float32(0.5)
+    fu = np.zeros((nz, ny, nx + 1), bool)
+    fu[:, :, 1:nx] = liq[:, :, :-1] | liq[:, :, 1:]
+    fv = np.zeros((nz, ny + 1, nx), bool)
+    fv[:, 1:ny, :] = liq[:, :-1, :] | liq[:, 1:, :]
+    fw = np.zeros((nz + 1, ny, nx), bool)
+    fw[1:nz, :, :] = liq[:-1, :, :] | liq[1:, :, :]
+    return fu, fv, fw
+
+
+def velocities(vof: np.ndarray, rng: np.random.Generator, dt: float, kind: str, scale: float,
+               gravity: float = GRAVITY):
+    """MAC velocities on fluid faces: ``uniform`` in [-scale, scale] or ``gauss`` N(0, scale)."""
+    fu, fv, fw = fluid_face_masks(vof)
+    out = []
+    for m in (fu, fv, fw):
+        if kind == "uniform":
+            a = rng.uniform(-scale, scale, size=m.shape)
+        else:
+            a = rng.normal(0.0, scale, size=m.shape)
+        out.append(np.where(m, a, 0.0))
+    out[1] = np.where(fv, out[1] + dt * gravity, 0.0)
+    return tuple(np.ascontiguousarray(a, np.float32) for a in out)
+
+
+def dam_break_32(seed: int = 1) -> GridState:
+    """32^3, dx = 1/32 m, closed box, corner block x<0.4, y<0.6, z<0.4, U[-0.05,0.05], dt = 1/120."""
+    n = 32
+    rng = np.random.default_rng(seed)
+    vof = box_vof(n, n, n, (0, 0, 0), (0.4 * n, 0.6 * n, 0.4 * n)).astype(np.float32)
+    dt = 1.0 / 120.0
+    u, v, w = velocities(vof, rng, dt, "uniform", 0.05)
+    return GridState(n, n, n, 1.0 / n, dt, vof, u, v, w, meta={"workload": "dam-break 32^3", "seed": seed})
+
+
+def dam_spheres(nx=128, ny=96, nz=128, seed: int = 2, step: int = 0, spheres: int = 16) -> GridState:
+    """Dam block holding 40% of the volume plus falling spheres (r in [4,10] cells) in the air.
+
+    ``step`` advances the sphere centres downward by a quarter cell per step and
+    re-draws the Gaussian (sigma 0.2 m/s) face velocities; dt = 1/60 s.
+    """
+    rng = np.random.default_rng(seed)
+    ax, az = rng.uniform(0.65, 0.85, size=2)
+    ay = 0.4 / (ax * az)
+    hi = (ax * nx, ay * ny, az * nz)
+    vof = box_vof(nx, ny, nz, (0, 0, 0), hi)
+    placed = []
+    tries = 0
+    while len(placed) < spheres and tries < 10000:
+        tries += 1
+        r = rng.uniform(4.0, 10.0)
+        c = np.array([rng.uniform(r + 1, nx - r - 1), rng.uniform(r + 1, ny - r - 1), rng.uniform(r + 1, nz - r - 1)])
+        # keep it in the air region, clear of the block and of other spheres
+        if c[0] - r < hi[0] + 1 and c[1] - r < hi[1] + 1 + 0.25 * 60 and c[2] - r < hi[2] + 1:
+            continue
+        if any(np.linalg.norm(c - p[0]) < r + p[1] + 2 for p in placed):
+            continue
+        placed.append((c, r))
+    for c, r in placed:
+        cc = c.copy()
+        cc[1] = max(r + 0.5, cc[1] - 0.25 * step)
+        vof = np.maximum(vof, sphere_vof(nx, ny, nz, cc, r))
+    vof = vof.astype(np.float32)
+    srng = np.random.default_rng([seed, step])
+    dt = 1.0 / 60.0
+    u, v, w = velocities(vof, srng, dt, "gauss", 0.2)
+    return GridState(nx, ny, nz, 1.0 / nx, dt, vof, u, v, w,
+                     meta={"workload": f"dam+{len(placed)} spheres {nx}x{ny}x{nz}", "seed": seed, "step": step})
+
+
+def log_uniform_edge(rng, lo=24, hi=128) -> int:
+    return int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+
+
+def random_liquid(nx, ny, nz, rng, fill_lo=0.2, fill_hi=0.7, max_tries=200) -> np.ndarray:
+    """Union of 1-6 seeded boxes and spheres whose liquid fraction lies in [fill_lo, fill_hi]."""
+    best = None
+    for _ in range(max_tries):
+        k = int(rng.integers(1, 7))
+        vof = np.zeros((nz, ny, nx))
+        for _s in range(k):
+            if rng.random() < 0.5:
+                lo = [rng.uniform(0, 0.6) * n for n in (nx, ny, nz)]
+                hi = [lo[a] + rng.uniform(0.25, 0.9) * n for a, n in enumerate((nx, ny, nz))]
+                lo[1] = 0.0 if rng.random() < 0.5 else lo[1]   # pools rest on the floor half the time
+                vof = np.maximum(vof, box_vof(nx, ny, nz, lo, hi))
+            else:
+                r = rng.uniform(0.15, 0.45) * min(nx, ny, nz)
+                c = [rng.uniform(r, n - r) for n in (nx, ny, nz)]
+                vof = np.maximum(vof, sphere_vof(nx, ny, nz, c, r))
+        frac = float((vof > 0.5).mean())
+        if fill_lo <= frac <= fill_hi:
+            return vof.astype(np.float32)
+        if best is None or abs(frac - 0.45) < abs(best[0] - 0.45):
+            best = (frac, vof)
+    return best[1].astype(np.float32)
+
+
+def batch_instances(count: int = 64, seed: int = 4, lo: int = 24, hi: int = 128) -> list[GridState]:
+    """Uneven batch: edges log-uniform in [lo, hi] per axis, 1-6 shapes filling 20-70%."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        nx, ny, nz = (log_uniform_edge(rng, lo, hi) for _ in range(3))
+        vof = random_liquid(nx, ny, nz, rng)
+        dt = 1.0 / 60.0
+        u, v, w = velocities(vof, rng, dt, "gauss", 0.2)
+        out.append(GridState(nx, ny, nz, 1.0 / 64.0, dt, vof, u, v, w,
+                             meta={"workload": "batched uneven", "seed": seed, "index": k}))
+    return out
+
+
+def random_small(nx, ny, nz, seed: int, open_top: bool = False, fill=(0.2, 0.7)) -> GridState:
+    rng = np.random.default_rng(seed)
+    vof = random_liquid(nx, ny, nz, rng, *fill)
+    dt = 1.0 / 60.0
+    u, v, w = velocities(vof, rng, dt, "gauss", 0.2)
+    if open_top:
+        liq_top = vof[:, -1, :] > 0.5
+        v[:, -1, :] = np.where(liq_top, rng.normal(0, 0.2, size=liq_top.shape), 0.0).astype(np.float32)
+    return GridState(nx, ny, nz, 1.0 / max(nx, ny, nz), dt, vof, u, v, w, open_top=open_top,
+                     meta={"workload": f"random {nx}x{ny}x{nz}", "seed": seed})

@@ -1,0 +1,871 @@
+// Host orchestration and C ABI of the uniform-grid pressure projection.
+//
+// A handle owns one grid's device arena.  Every solve, single or batched, runs
+// through a fluid_pp_batch: a device table of instance descriptors plus tile
+// lists per stage, so one launch per stage covers every instance.  The CG
+// scalars live on the device (Ctrl); the host only polls the done flags every
+// few iterations.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/fluid_pp.h"
+#include "kernels.cuh"
+#include "plan.h"
+#include "types.h"
+
+using namespace fpp;
+
+namespace {
+
+constexpr int kMaxGrid = 148 * 8;   // 148 SMs x 8 resident 256-thread CTAs
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+size_t storage_bytes(int precision) { return precision == FLUID_PP_FP32 ? 4 : 2; }
+
+struct Arena {
+  char* base = nullptr;
+  size_t used = 0, cap = 0;
+  void* take(size_t bytes) {
+    void* p = base + used;
+    used = align_up(used + bytes, 256);
+    return p;
+  }
+};
+
+}  // namespace
+
+struct fluid_pp_batch;
+
+struct fluid_pp {
+  fluid_pp_config cfg{};
+  HierarchyPlan plan{};
+  cudaStream_t stream = nullptr;
+  std::string err;
+  char* arena = nullptr;
+  size_t arena_bytes = 0;
+  InstDev inst{};        // host copy of the descriptor (device pointers)
+  Ctrl* h_ctrl = nullptr;  // pinned
+  bool has_state = false;
+  bool has_pressure = false;
+  float last_dt = 0.f;
+  fluid_pp_batch* self = nullptr;   // batch of one
+  int set_error(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+};
+
+struct List {
+  int off = 0, n = 0;
+};
+
+struct fluid_pp_batch {
+  std::vector<fluid_pp*> h;
+  int device = 0;
+  int precision = 0;
+  cudaStream_t stream = nullptr;
+  InstDev* d_insts = nullptr;
+  Ctrl* d_ctrl = nullptr;
+  Ctrl* h_ctrl = nullptr;   // pinned mirror
+  Tile* d_tiles = nullptr;
+  int* d_ilist = nullptr;
+  List l0;
+  List lvl[kMaxLevels];      // level-l tiles of instances for which l is not the coarsest
+  List rst[kMaxLevels];      // level-(l+1) tiles of instances for which l is not the coarsest
+  List crs[kMaxLevels];      // level-l tiles (l >= 1) of every instance having level l
+  List bake;
+  List multi, single;        // instance lists (offsets into d_ilist) by coarsest level
+  int maxL = 0;
+  size_t smem_factor = 0;
+  std::string err;
+};
+
+// ------------------------------------------------------------------ helpers
+#define CK(call)                                                                    \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) return fail_cuda(e_, #call);                             \
+  } while (0)
+
+namespace {
+
+thread_local std::string g_err;
+
+int launch_grid(int tiles) { return std::max(1, std::min(tiles, kMaxGrid)); }
+
+int ntiles_of(long long n) { return int((n + kTile - 1) / kTile); }
+
+const Tile* tl(const fluid_pp_batch* B, const List& L) { return B->d_tiles + L.off; }
+const int* il(const fluid_pp_batch* B, const List& L) { return B->d_ilist + L.off; }
+
+}  // namespace
+
+namespace fpp {
+// Thin wrappers: blockIdx.x indexes an instance list instead of the table.
+template <class TD>
+__global__ void k_coarse_factor_list(const InstDev* insts, const int* list) {
+  extern __shared__ double A[];
+  const InstDev& I = insts[list[blockIdx.x]];
+  const LevelDev& L = I.lv[I.nlev - 1];
+  const int m = int(L.n);
+  __shared__ int anchored;
+  __shared__ double diag_mean;
+  __shared__ double pivot_row[kMaxCoarse];
+  __shared__ double pivot_col[kMaxCoarse];
+  if (threadIdx.x == 0) {
+    anchored = 0;
+    diag_mean = 0.0;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < m * m; e += blockDim.x) A[e] = 0.0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    int x, y, z;
+    decode(i, L.nx, L.ny, x, y, z);
+    if (!L.label[i]) {
+      A[i * m + i] = 1.0;
+      atomicOr(&anchored, 1);
+      continue;
+    }
+    if (I.open_top && y == L.ny - 1) atomicOr(&anchored, 1);
+    A[i * m + i] = St<TD>::ld(L.diagT, i);
+    const int sy = L.nx, sz = L.nx * L.ny;
+    if (x > 0 && L.label[i - 1]) A[i * m + i - 1] = -L.wx;
+    if (x + 1 < L.nx && L.label[i + 1]) A[i * m + i + 1] = -L.wx;
+    if (y > 0 && L.label[i - sy]) A[i * m + i - sy] = -L.wy;
+    if (y + 1 < L.ny && L.label[i + sy]) A[i * m + i + sy] = -L.wy;
+    if (z > 0 && L.label[i - sz]) A[i * m + i - sz] = -L.wz;
+    if (z + 1 < L.nz && L.label[i + sz]) A[i * m + i + sz] = -L.wz;
+  }
+  __syncthreads();
+  if (!anchored) {
+    if (threadIdx.x == 0) {
+      double s = 0;
+      for (int i = 0; i < m; ++i) s += A[i * m + i];
+      diag_mean = s / double(m);
+    }
+    __syncthreads();
+    const double add = diag_mean / double(m);
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) A[e] += add;
+    __syncthreads();
+  }
+  for (int k = 0; k < m; ++k) {
+    const double piv = A[k * m + k];
+    for (int j = threadIdx.x; j < m; j += blockDim.x) {
+      pivot_row[j] = (j == k ? 1.0 : A[k * m + j]) / piv;
+      pivot_col[j] = A[j * m + k];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      const int i = e / m, j = e - i * m;
+      if (i == k) A[e] = pivot_row[j];
+      else A[e] = ((j == k) ? 0.0 : A[e]) - pivot_col[i] * pivot_row[j];
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < m * m; e += blockDim.x) I.coarse_inv[e] = A[e];
+}
+
+template <class TZ, class TR>
+__global__ void k_coarse_apply_list(const InstDev* insts, const int* list) {
+  const InstDev& I = insts[list[blockIdx.x]];
+  if (I.ctrl->done) return;
+  const LevelDev& L = I.lv[I.nlev - 1];
+  const int m = int(L.n);
+  __shared__ double rhs[kMaxCoarse];
+  for (int i = threadIdx.x; i < m; i += blockDim.x) rhs[i] = L.label[i] ? double(St<TR>::ld(L.rhs, i)) : 0.0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    double s = 0;
+    const double* row = I.coarse_inv + (long long)i * m;
+    for (int j = 0; j < m; ++j) s += row[j] * rhs[j];
+    St<TZ>::st(L.z, i, L.label[i] ? float(s) : 0.0f);
+  }
+}
+
+// Clears the control words a solve accumulates into (counts and done flag).
+__global__ void k_reset_ctrl(const InstDev* insts, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  Ctrl* c = insts[k].ctrl;
+  c->liquid = 0;
+  c->air = 0;
+  c->top_liquid = 0;
+  c->nonfinite = 0;
+  c->done = 0;
+  c->candidate = 0;
+  c->status = 0;
+  c->converged = 0;
+  c->iter = 0;
+}
+
+// Test hook: make the solve-loop kernels run with the given scale.
+__global__ void k_hook_ctrl(const InstDev* insts, double sigma) {
+  Ctrl* c = insts[0].ctrl;
+  c->done = 0;
+  c->sigma = sigma;
+  c->gamma = 1.0;
+  c->status = 0;
+}
+}  // namespace fpp
+
+namespace {
+
+template <class T>
+void setup_launch(fluid_pp_batch* B, int warm, double rel, double abs_tol, int max_iter, int true_every) {
+  cudaStream_t s = B->stream;
+  const int n = int(B->h.size());
+  k_reset_ctrl<<<(n + 127) / 128, 128, 0, s>>>(B->d_insts, n);
+  k_label_rhs<<<launch_grid(B->l0.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n, warm);
+  for (int l = 1; l < B->maxL; ++l)
+    if (B->crs[l].n) k_coarsen_phi<<<launch_grid(B->crs[l].n), kThreads, 0, s>>>(B->d_insts, tl(B, B->crs[l]), B->crs[l].n);
+  k_bake_diag<T><<<launch_grid(B->bake.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->bake), B->bake.n);
+  if (B->multi.n)
+    k_coarse_factor_list<T><<<B->multi.n, kThreads, B->smem_factor, s>>>(B->d_insts, il(B, B->multi));
+  if (B->single.n)
+    k_coarse_factor_list<T><<<B->single.n, kThreads, B->smem_factor, s>>>(B->d_insts, il(B, B->single));
+  k_cg_init<<<launch_grid(B->l0.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n, rel, abs_tol, max_iter,
+                                                       true_every, warm);
+  k_project_init<<<launch_grid(B->l0.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
+}
+
+template <class T>
+void vcycle_launch(fluid_pp_batch* B, int pre, int post) {
+  cudaStream_t s = B->stream;
+  for (int l = 0; l + 1 < B->maxL; ++l) {
+    const List& Ls = B->lvl[l];
+    if (!Ls.n) continue;
+    const int g = launch_grid(Ls.n);
+    for (int sw = 0; sw < pre; ++sw) {
+      if (l == 0) {
+        k_smooth<float, float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 0, sw == 0);
+        k_smooth<float, float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 1, 0);
+      } else {
+        k_smooth<T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 0, sw == 0);
+        k_smooth<T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 1, 0);
+      }
+    }
+    if (pre == 0) {   // z must start at zero
+      if (l == 0) k_smooth<float, float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 2, 1);
+      else k_smooth<T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 2, 1);
+    }
+    if (l == 0) k_residual<float, float, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l);
+    else k_residual<T, T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l);
+    const List& Lr = B->rst[l];
+    k_restrict<T><<<launch_grid(Lr.n), kThreads, 0, s>>>(B->d_insts, tl(B, Lr), Lr.n, l);
+  }
+  if (B->multi.n) k_coarse_apply_list<T, T><<<B->multi.n, kThreads, 0, s>>>(B->d_insts, il(B, B->multi));
+  if (B->single.n)
+    k_coarse_apply_list<float, float><<<B->single.n, kThreads, 0, s>>>(B->d_insts, il(B, B->single));
+  for (int l = B->maxL - 2; l >= 0; --l) {
+    const List& Ls = B->lvl[l];
+    if (!Ls.n) continue;
+    const int g = launch_grid(Ls.n);
+    if (l == 0) k_prolong<float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l);
+    else k_prolong<T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l);
+    for (int sw = 0; sw < post; ++sw) {
+      if (l == 0) {
+        k_smooth<float, float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 1, 0);
+        k_smooth<float, float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 0, 0);
+      } else {
+        k_smooth<T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 1, 0);
+        k_smooth<T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 0, 0);
+      }
+    }
+  }
+}
+
+template <class T>
+void iter_launch(fluid_pp_batch* B, int pre, int post) {
+  cudaStream_t s = B->stream;
+  const int g = launch_grid(B->l0.n);
+  vcycle_launch<T>(B, pre, post);
+  k_dot_rz<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
+  k_dir<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
+  k_spmv<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
+  k_update<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
+  k_true_residual<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
+}
+
+void finish_launch_any(fluid_pp_batch* B) {
+  cudaStream_t s = B->stream;
+  const int g = launch_grid(B->l0.n);
+  k_grad<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
+  k_receipt<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
+}
+
+}  // namespace
+
+// ==================================================================== batch
+static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out, std::string& err) {
+  if (!handles || count <= 0 || !out) {
+    err = "batch needs at least one handle";
+    return FLUID_PP_INVALID_ARG;
+  }
+  auto B = std::make_unique<fluid_pp_batch>();
+  B->device = handles[0]->cfg.device;
+  B->precision = handles[0]->cfg.precision;
+  B->stream = handles[0]->stream;
+  for (int k = 0; k < count; ++k) {
+    fluid_pp* h = handles[k];
+    if (!h) {
+      err = "null handle in batch";
+      return FLUID_PP_INVALID_ARG;
+    }
+    if (h->cfg.device != B->device || h->cfg.precision != B->precision) {
+      err = "batched handles must share device and precision";
+      return FLUID_PP_INVALID_ARG;
+    }
+    B->h.push_back(h);
+    B->maxL = std::max(B->maxL, h->plan.levels);
+  }
+  cudaSetDevice(B->device);
+  // tile lists
+  std::vector<Tile> tiles;
+  std::vector<int> ilist;
+  auto add_level = [&](List& L, auto pred, int level_of_tiles) {
+    L.off = int(tiles.size());
+    for (int k = 0; k < count; ++k) {
+      const InstDev& I = B->h[k]->inst;
+      if (!pred(I)) continue;
+      const int nt = I.lv[level_of_tiles].ntiles;
+      for (int t = 0; t < nt; ++t) tiles.push_back(Tile{k, level_of_tiles, t, 0});
+    }
+    L.n = int(tiles.size()) - L.off;
+  };
+  add_level(B->l0, [](const InstDev&) { return true; }, 0);
+  for (int l = 0; l < B->maxL; ++l) {
+    add_level(B->lvl[l], [l](const InstDev& I) { return l < I.nlev - 1; }, l);
+    if (l + 1 < B->maxL) add_level(B->rst[l], [l](const InstDev& I) { return l < I.nlev - 1; }, l + 1);
+    if (l >= 1) add_level(B->crs[l], [l](const InstDev& I) { return l < I.nlev; }, l);
+  }
+  B->bake.off = int(tiles.size());
+  for (int k = 0; k < count; ++k) {
+    const InstDev& I = B->h[k]->inst;
+    for (int l = 0; l < I.nlev; ++l)
+      for (int t = 0; t < I.lv[l].ntiles; ++t) tiles.push_back(Tile{k, l, t, 0});
+  }
+  B->bake.n = int(tiles.size()) - B->bake.off;
+  B->multi.off = int(ilist.size());
+  for (int k = 0; k < count; ++k)
+    if (B->h[k]->inst.nlev > 1) ilist.push_back(k);
+  B->multi.n = int(ilist.size()) - B->multi.off;
+  B->single.off = int(ilist.size());
+  for (int k = 0; k < count; ++k)
+    if (B->h[k]->inst.nlev == 1) ilist.push_back(k);
+  B->single.n = int(ilist.size()) - B->single.off;
+  int mmax = 0;
+  for (int k = 0; k < count; ++k) mmax = std::max(mmax, B->h[k]->inst.coarse_m);
+  B->smem_factor = size_t(mmax) * mmax * sizeof(double);
+
+  std::vector<InstDev> insts(count);
+  cudaError_t e = cudaMalloc(&B->d_ctrl, sizeof(Ctrl) * count);
+  if (e == cudaSuccess) e = cudaMemset(B->d_ctrl, 0, sizeof(Ctrl) * count);
+  for (int k = 0; k < count; ++k) {
+    insts[k] = B->h[k]->inst;
+    insts[k].ctrl = B->d_ctrl + k;
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&B->d_insts, sizeof(InstDev) * count);
+  if (e == cudaSuccess) e = cudaMemcpy(B->d_insts, insts.data(), sizeof(InstDev) * count, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&B->d_tiles, sizeof(Tile) * std::max<size_t>(1, tiles.size()));
+  if (e == cudaSuccess && !tiles.empty())
+    e = cudaMemcpy(B->d_tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&B->d_ilist, sizeof(int) * std::max<size_t>(1, ilist.size()));
+  if (e == cudaSuccess && !ilist.empty())
+    e = cudaMemcpy(B->d_ilist, ilist.data(), sizeof(int) * ilist.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMallocHost(&B->h_ctrl, sizeof(Ctrl) * count);
+  if (e == cudaSuccess && B->smem_factor > 48 * 1024) {
+    auto set = [&](const void* f) {
+      return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(B->smem_factor));
+    };
+    e = set((const void*)k_coarse_factor_list<float>);
+    if (e == cudaSuccess) e = set((const void*)k_coarse_factor_list<__half>);
+    if (e == cudaSuccess) e = set((const void*)k_coarse_factor_list<__nv_bfloat16>);
+  }
+  if (e != cudaSuccess) {
+    err = std::string("batch setup: ") + cudaGetErrorString(e);
+    fluid_pp_batch_destroy(B.release());
+    return e == cudaErrorMemoryAllocation ? FLUID_PP_OOM : FLUID_PP_CUDA;
+  }
+  *out = B.release();
+  return FLUID_PP_OK;
+}
+
+static void fill_receipt(const fluid_pp* h, const Ctrl& c, fluid_pp_receipt* r) {
+  std::memset(r, 0, sizeof(*r));
+  r->status = c.status;
+  r->iterations = c.iter;
+  r->liquid_cells = c.liquid;
+  r->levels = h->plan.levels;
+  const double hh = h->cfg.h;
+  r->b_norm = std::sqrt(std::max(0.0, c.bb));
+  r->rel_residual = c.bb > 0 ? std::sqrt(std::max(0.0, c.rr) / c.bb) : 0.0;
+  r->true_rel_residual = c.bb > 0 ? std::sqrt(std::max(0.0, c.rr_true) / c.bb) : 0.0;
+  r->max_div_after = c.red[0] / hh;
+  r->l2_div_after = std::sqrt(std::max(0.0, c.red[1]) * hh);
+  r->max_div_before = c.red[2] / hh;
+  r->l2_div_before = std::sqrt(std::max(0.0, c.red[3]) * hh);
+}
+
+static fluid_pp_solve_opts default_opts() {
+  fluid_pp_solve_opts o{};
+  o.rel_tol = 1e-6;
+  o.abs_tol = 0.0;
+  o.max_iters = 200;
+  o.pre_sweeps = 1;
+  o.post_sweeps = 1;
+  o.true_residual_every = 0;
+  o.warm_start = 0;
+  return o;
+}
+
+template <class T>
+static int batch_project_t(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts& o, bool sync_receipts,
+                           fluid_pp_receipt* receipts) {
+  const int n = int(B->h.size());
+  // per-instance dt into the descriptor table
+  for (int k = 0; k < n; ++k) {
+    fluid_pp* h = B->h[k];
+    const float dt = dts ? dts[k] : h->last_dt;
+    h->last_dt = dt;
+    h->inst.dt = dt;
+    h->inst.pscale = h->cfg.rho * h->cfg.h / dt;
+    cudaMemcpyAsync(reinterpret_cast<char*>(B->d_insts + k) + offsetof(InstDev, dt), &h->inst.dt, sizeof(float),
+                    cudaMemcpyHostToDevice, B->stream);
+    cudaMemcpyAsync(reinterpret_cast<char*>(B->d_insts + k) + offsetof(InstDev, pscale), &h->inst.pscale,
+                    sizeof(float), cudaMemcpyHostToDevice, B->stream);
+  }
+  setup_launch<T>(B, o.warm_start, o.rel_tol, o.abs_tol, o.max_iters, o.true_residual_every);
+  const int check = 4;
+  int it = 0;
+  const int cap = o.max_iters + 2;
+  while (it < cap) {
+    const int burst = std::min(check, cap - it);
+    for (int b = 0; b < burst; ++b) iter_launch<T>(B, o.pre_sweeps, o.post_sweeps);
+    it += burst;
+    cudaMemcpyAsync(B->h_ctrl, B->d_ctrl, sizeof(Ctrl) * n, cudaMemcpyDeviceToHost, B->stream);
+    cudaError_t e = cudaStreamSynchronize(B->stream);
+    if (e != cudaSuccess) {
+      B->err = std::string("solve: ") + cudaGetErrorString(e);
+      return FLUID_PP_CUDA;
+    }
+    bool all = true;
+    for (int k = 0; k < n; ++k) all &= B->h_ctrl[k].done != 0;
+    if (all) break;
+  }
+  finish_launch_any(B);
+  cudaMemcpyAsync(B->h_ctrl, B->d_ctrl, sizeof(Ctrl) * n, cudaMemcpyDeviceToHost, B->stream);
+  if (sync_receipts) {
+    cudaError_t e = cudaStreamSynchronize(B->stream);
+    if (e != cudaSuccess) {
+      B->err = std::string("project: ") + cudaGetErrorString(e);
+      return FLUID_PP_CUDA;
+    }
+    int worst = FLUID_PP_OK;
+    for (int k = 0; k < n; ++k) {
+      if (receipts) fill_receipt(B->h[k], B->h_ctrl[k], receipts + k);
+      B->h[k]->has_pressure = true;
+      if (B->h_ctrl[k].status != FLUID_PP_OK && worst == FLUID_PP_OK) worst = B->h_ctrl[k].status;
+    }
+    return worst;
+  }
+  return FLUID_PP_OK;
+}
+
+static int batch_project(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts* opts, bool sync,
+                         fluid_pp_receipt* receipts) {
+  const fluid_pp_solve_opts o = opts ? *opts : default_opts();
+  if (!(o.rel_tol >= 0) || !(o.abs_tol >= 0) || o.max_iters < 1 || o.pre_sweeps < 0 || o.post_sweeps < 0) {
+    B->err = "invalid solve options";
+    return FLUID_PP_INVALID_ARG;
+  }
+  for (fluid_pp* h : B->h)
+    if (!h->has_state) {
+      B->err = "state not uploaded";
+      return FLUID_PP_INVALID_ARG;
+    }
+  cudaSetDevice(B->device);
+  switch (B->precision) {
+    case FLUID_PP_FP16: return batch_project_t<__half>(B, dts, o, sync, receipts);
+    case FLUID_PP_BF16: return batch_project_t<__nv_bfloat16>(B, dts, o, sync, receipts);
+    default: return batch_project_t<float>(B, dts, o, sync, receipts);
+  }
+}
+
+// ==================================================================== C ABI
+extern "C" {
+
+int fluid_pp_plan_hierarchy(int nx, int ny, int nz, int* level_count, int* level_dims, int* coarsest_cells,
+                            int* semi_coarsened, int* extended) {
+  HierarchyPlan p = plan_hierarchy(nx, ny, nz);
+  if (level_count) *level_count = p.levels;
+  if (coarsest_cells) *coarsest_cells = p.coarsest_haloed;
+  if (semi_coarsened) *semi_coarsened = p.semi ? 1 : 0;
+  if (extended) *extended = p.extended ? 1 : 0;
+  if (!p.ok) return FLUID_PP_INVALID_ARG;
+  if (level_dims)
+    for (int l = 0; l < p.levels; ++l)
+      for (int a = 0; a < 3; ++a) level_dims[3 * l + a] = p.dims[l][a];
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
+  g_err.clear();
+  if (!cfg || !out) return FLUID_PP_INVALID_ARG;
+  *out = nullptr;
+  HierarchyPlan plan = plan_hierarchy(cfg->nx, cfg->ny, cfg->nz);
+  if (!plan.ok) {
+    g_err = plan.rejection ? plan.rejection : "no hierarchy";
+    return FLUID_PP_INVALID_ARG;
+  }
+  if (!(cfg->h > 0) || !std::isfinite(cfg->h) || !(cfg->rho > 0) || !std::isfinite(cfg->rho)) {
+    g_err = "CM11a grid spacing must be positive and finite";
+    return FLUID_PP_INVALID_ARG;
+  }
+  if (cfg->precision < 0 || cfg->precision > 2) {
+    g_err = "unknown precision";
+    return FLUID_PP_INVALID_ARG;
+  }
+  const long long ncoarse =
+      (long long)plan.dims[plan.levels - 1][0] * plan.dims[plan.levels - 1][1] * plan.dims[plan.levels - 1][2];
+  if (ncoarse > kMaxCoarse) {
+    g_err = "coarsest level exceeds the dense solve limit";
+    return FLUID_PP_INVALID_ARG;
+  }
+  if (cudaSetDevice(cfg->device) != cudaSuccess) {
+    g_err = "cannot select CUDA device";
+    return FLUID_PP_CUDA;
+  }
+  auto h = std::make_unique<fluid_pp>();
+  h->cfg = *cfg;
+  h->plan = plan;
+  const size_t sT = storage_bytes(cfg->precision);
+  const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+  const long long N = (long long)nx * ny * nz;
+  // size the arena
+  size_t bytes = 0;
+  auto acc = [&](size_t b) { bytes = align_up(bytes + b, 256); };
+  for (int l = 0; l < plan.levels; ++l) {
+    const long long n = (long long)plan.dims[l][0] * plan.dims[l][1] * plan.dims[l][2];
+    acc(n);             // label
+    acc(4 * n);         // phi
+    acc(4 * n);         // diag
+    acc(sT * n);        // diagT
+    acc((l == 0 ? 4 : sT) * n);   // z
+    acc((l == 0 ? 4 : sT) * n);   // rhs / r
+    acc(sT * n);        // res
+  }
+  const long long nu = (long long)(nx + 1) * ny * nz, nv = (long long)nx * (ny + 1) * nz,
+                  nw = (long long)nx * ny * (nz + 1);
+  acc(4 * N);           // vof
+  acc(4 * nu);
+  acc(4 * nv);
+  acc(4 * nw);
+  for (int k = 0; k < 5; ++k) acc(4 * N);   // b x d q p_si
+  const int nt0 = ntiles_of(N);
+  acc(sizeof(double) * kSlots * nt0);
+  acc(sizeof(double) * ncoarse * ncoarse);
+  acc(sizeof(Ctrl));
+  cudaError_t e = cudaMalloc(&h->arena, bytes);
+  if (e != cudaSuccess) {
+    g_err = std::string("arena allocation: ") + cudaGetErrorString(e);
+    return FLUID_PP_OOM;
+  }
+  h->arena_bytes = bytes;
+  cudaMemset(h->arena, 0, bytes);
+  Arena a{h->arena, 0, bytes};
+  InstDev& I = h->inst;
+  std::memset(&I, 0, sizeof(I));
+  I.nlev = plan.levels;
+  I.nx = nx;
+  I.ny = ny;
+  I.nz = nz;
+  I.open_top = cfg->open_top ? 1 : 0;
+  I.h = cfg->h;
+  I.rho = cfg->rho;
+  I.dt = 1.0f;
+  I.ntiles0 = nt0;
+  I.coarse_m = int(ncoarse);
+  float wmax_prev = 1.0f;
+  for (int l = 0; l < plan.levels; ++l) {
+    LevelDev& L = I.lv[l];
+    L.nx = plan.dims[l][0];
+    L.ny = plan.dims[l][1];
+    L.nz = plan.dims[l][2];
+    L.sx = plan.stride[l][0];
+    L.sy = plan.stride[l][1];
+    L.sz = plan.stride[l][2];
+    L.n = (long long)L.nx * L.ny * L.nz;
+    L.ntiles = ntiles_of(L.n);
+    // spacing ratio h_l / h_0 per axis (webgpu-uniform-pressure-multigrid.ts:588-589)
+    const double rx = double(nx) / L.nx, ry = double(ny) / L.ny, rz = double(nz) / L.nz;
+    const double wx = 1.0 / (rx * rx), wy = 1.0 / (ry * ry), wz = 1.0 / (rz * rz);
+    const double wmax = std::max(wx, std::max(wy, wz));
+    L.wmax = float(wmax);
+    L.wx = float(wx / wmax);
+    L.wy = float(wy / wmax);
+    L.wz = float(wz / wmax);
+    L.ext_phi = float(0.5 * ry);
+    if (l > 0) I.lv[l - 1].to_coarse = wmax_prev / float(wmax);
+    wmax_prev = float(wmax);
+    const long long n = L.n;
+    L.label = static_cast<uint8_t*>(a.take(n));
+    L.phi = static_cast<float*>(a.take(4 * n));
+    L.diag = static_cast<float*>(a.take(4 * n));
+    L.diagT = a.take(sT * n);
+    L.z = a.take((l == 0 ? 4 : sT) * n);
+    L.rhs = a.take((l == 0 ? 4 : sT) * n);
+    L.res = a.take(sT * n);
+  }
+  I.lv[plan.levels - 1].to_coarse = 1.0f;
+  I.vof = static_cast<float*>(a.take(4 * N));
+  I.u = static_cast<float*>(a.take(4 * nu));
+  I.v = static_cast<float*>(a.take(4 * nv));
+  I.w = static_cast<float*>(a.take(4 * nw));
+  I.b = static_cast<float*>(a.take(4 * N));
+  I.x = static_cast<float*>(a.take(4 * N));
+  I.d = static_cast<float*>(a.take(4 * N));
+  I.q = static_cast<float*>(a.take(4 * N));
+  I.p_si = static_cast<float*>(a.take(4 * N));
+  I.partial = static_cast<double*>(a.take(sizeof(double) * kSlots * nt0));
+  I.coarse_inv = static_cast<double*>(a.take(sizeof(double) * ncoarse * ncoarse));
+  I.ctrl = static_cast<Ctrl*>(a.take(sizeof(Ctrl)));
+  fluid_pp* raw = h.get();
+  std::string err;
+  int rc = batch_build(&raw, 1, &h->self, err);
+  if (rc != FLUID_PP_OK) {
+    g_err = err;
+    cudaFree(h->arena);
+    return rc;
+  }
+  *out = h.release();
+  return FLUID_PP_OK;
+}
+
+void fluid_pp_destroy(fluid_pp* pp) {
+  if (!pp) return;
+  cudaSetDevice(pp->cfg.device);
+  if (pp->self) fluid_pp_batch_destroy(pp->self);
+  if (pp->arena) cudaFree(pp->arena);
+  delete pp;
+}
+
+int fluid_pp_set_stream(fluid_pp* pp, void* stream) {
+  if (!pp) return FLUID_PP_INVALID_ARG;
+  pp->stream = static_cast<cudaStream_t>(stream);
+  if (pp->self) pp->self->stream = pp->stream;
+  return FLUID_PP_OK;
+}
+
+static int upload(fluid_pp* pp, const float* vof, const float* u, const float* v, const float* w,
+                  cudaMemcpyKind kind) {
+  if (!pp || !vof || !u || !v || !w) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(pp->cfg.device);
+  const long long nx = pp->cfg.nx, ny = pp->cfg.ny, nz = pp->cfg.nz;
+  const InstDev& I = pp->inst;
+  cudaError_t e = cudaMemcpyAsync((void*)I.vof, vof, 4 * nx * ny * nz, kind, pp->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(I.u, u, 4 * (nx + 1) * ny * nz, kind, pp->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(I.v, v, 4 * nx * (ny + 1) * nz, kind, pp->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(I.w, w, 4 * nx * ny * (nz + 1), kind, pp->stream);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("upload: ") + cudaGetErrorString(e));
+  pp->has_state = true;
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_upload_state(fluid_pp* pp, const float* vof, const float* u, const float* v, const float* w) {
+  return upload(pp, vof, u, v, w, cudaMemcpyHostToDevice);
+}
+
+int fluid_pp_upload_state_device(fluid_pp* pp, const float* vof, const float* u, const float* v, const float* w) {
+  return upload(pp, vof, u, v, w, cudaMemcpyDeviceToDevice);
+}
+
+int fluid_pp_project(fluid_pp* pp, float dt, const fluid_pp_solve_opts* opts, fluid_pp_receipt* receipt) {
+  if (!pp) return FLUID_PP_INVALID_ARG;
+  if (!(dt > 0) || !std::isfinite(dt)) return pp->set_error(FLUID_PP_INVALID_ARG, "dt must be positive and finite");
+  const int rc = batch_project(pp->self, &dt, opts, true, receipt);
+  if (rc != FLUID_PP_OK) pp->err = pp->self->err;
+  return rc;
+}
+
+int fluid_pp_project_async(fluid_pp* pp, float dt, const fluid_pp_solve_opts* opts) {
+  if (!pp) return FLUID_PP_INVALID_ARG;
+  if (!(dt > 0) || !std::isfinite(dt)) return pp->set_error(FLUID_PP_INVALID_ARG, "dt must be positive and finite");
+  const int rc = batch_project(pp->self, &dt, opts, false, nullptr);
+  if (rc != FLUID_PP_OK) pp->err = pp->self->err;
+  return rc;
+}
+
+int fluid_pp_receipt_read(fluid_pp* pp, fluid_pp_receipt* receipt) {
+  if (!pp || !receipt) return FLUID_PP_INVALID_ARG;
+  cudaError_t e = cudaStreamSynchronize(pp->self->stream);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  fill_receipt(pp, pp->self->h_ctrl[0], receipt);
+  pp->has_pressure = true;
+  return receipt->status;
+}
+
+int fluid_pp_download(fluid_pp* pp, float* p, float* u, float* v, float* w) {
+  if (!pp) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(pp->cfg.device);
+  const long long nx = pp->cfg.nx, ny = pp->cfg.ny, nz = pp->cfg.nz;
+  const InstDev& I = pp->inst;
+  cudaError_t e = cudaSuccess;
+  if (p) e = cudaMemcpyAsync(p, I.p_si, 4 * nx * ny * nz, cudaMemcpyDeviceToHost, pp->stream);
+  if (u && e == cudaSuccess) e = cudaMemcpyAsync(u, I.u, 4 * (nx + 1) * ny * nz, cudaMemcpyDeviceToHost, pp->stream);
+  if (v && e == cudaSuccess) e = cudaMemcpyAsync(v, I.v, 4 * nx * (ny + 1) * nz, cudaMemcpyDeviceToHost, pp->stream);
+  if (w && e == cudaSuccess) e = cudaMemcpyAsync(w, I.w, 4 * nx * ny * (nz + 1), cudaMemcpyDeviceToHost, pp->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(pp->stream);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("download: ") + cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_device_arrays(fluid_pp* pp, float** p, float** u, float** v, float** w, float** vof) {
+  if (!pp) return FLUID_PP_INVALID_ARG;
+  if (p) *p = pp->inst.p_si;
+  if (u) *u = pp->inst.u;
+  if (v) *v = pp->inst.v;
+  if (w) *w = pp->inst.w;
+  if (vof) *vof = const_cast<float*>(pp->inst.vof);
+  return FLUID_PP_OK;
+}
+
+const char* fluid_pp_last_error(const fluid_pp* pp) { return pp ? pp->err.c_str() : g_err.c_str(); }
+
+// ------------------------------------------------------------ parity hooks
+int fluid_pp_prepare(fluid_pp* pp, float dt) {
+  if (!pp || !pp->has_state) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(pp->cfg.device);
+  fluid_pp_batch* B = pp->self;
+  pp->inst.dt = dt;
+  pp->inst.pscale = pp->cfg.rho * pp->cfg.h / dt;
+  pp->last_dt = dt;
+  cudaMemcpyAsync(reinterpret_cast<char*>(B->d_insts) + offsetof(InstDev, dt), &pp->inst.dt, sizeof(float),
+                  cudaMemcpyHostToDevice, B->stream);
+  const fluid_pp_solve_opts o = default_opts();
+  switch (B->precision) {
+    case FLUID_PP_FP16: setup_launch<__half>(B, 0, o.rel_tol, o.abs_tol, o.max_iters, 0); break;
+    case FLUID_PP_BF16: setup_launch<__nv_bfloat16>(B, 0, o.rel_tol, o.abs_tol, o.max_iters, 0); break;
+    default: setup_launch<float>(B, 0, o.rel_tol, o.abs_tol, o.max_iters, 0);
+  }
+  cudaError_t e = cudaStreamSynchronize(B->stream);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("prepare: ") + cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_level_dims(fluid_pp* pp, int level, int* dims3) {
+  if (!pp || level < 0 || level >= pp->plan.levels || !dims3) return FLUID_PP_INVALID_ARG;
+  for (int a = 0; a < 3; ++a) dims3[a] = pp->plan.dims[level][a];
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_get_level(fluid_pp* pp, int level, unsigned char* label, float* phi, float* diag) {
+  if (!pp || level < 0 || level >= pp->plan.levels) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(pp->cfg.device);
+  const LevelDev& L = pp->inst.lv[level];
+  cudaError_t e = cudaSuccess;
+  if (label) e = cudaMemcpy(label, L.label, L.n, cudaMemcpyDeviceToHost);
+  if (phi && e == cudaSuccess) e = cudaMemcpy(phi, L.phi, 4 * L.n, cudaMemcpyDeviceToHost);
+  if (diag && e == cudaSuccess) e = cudaMemcpy(diag, L.diag, 4 * L.n, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_get_rhs(fluid_pp* pp, float* b) {
+  if (!pp || !b) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(pp->cfg.device);
+  cudaError_t e = cudaMemcpy(b, pp->inst.b, 4 * pp->inst.lv[0].n, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_get_pressure_cells(fluid_pp* pp, float* x) {
+  if (!pp || !x) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(pp->cfg.device);
+  cudaError_t e = cudaMemcpy(x, pp->inst.x, 4 * pp->inst.lv[0].n, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_apply_operator(fluid_pp* pp, const float* p, float* out) {
+  if (!pp || !p || !out) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(pp->cfg.device);
+  fluid_pp_batch* B = pp->self;
+  const long long N = pp->inst.lv[0].n;
+  cudaMemcpyAsync(pp->inst.d, p, 4 * N, cudaMemcpyHostToDevice, B->stream);
+  k_hook_ctrl<<<1, 1, 0, B->stream>>>(B->d_insts, 1.0);
+  k_spmv<<<launch_grid(B->l0.n), kThreads, 0, B->stream>>>(B->d_insts, tl(B, B->l0), B->l0.n);
+  cudaMemcpyAsync(out, pp->inst.q, 4 * N, cudaMemcpyDeviceToHost, B->stream);
+  cudaError_t e = cudaStreamSynchronize(B->stream);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_apply_vcycle(fluid_pp* pp, const float* r, float* z, int pre, int post) {
+  if (!pp || !r || !z || pre < 0 || post < 0) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(pp->cfg.device);
+  fluid_pp_batch* B = pp->self;
+  const long long N = pp->inst.lv[0].n;
+  double ss = 0;
+  long long cnt = 0;
+  for (long long i = 0; i < N; ++i) {
+    ss += double(r[i]) * r[i];
+    cnt += r[i] != 0.0f;
+  }
+  const double per = cnt ? ss / double(cnt) : 0.0;
+  const double sigma = per > 1e-300 ? 1.0 / std::sqrt(per) : 1.0;
+  cudaMemcpyAsync(pp->inst.lv[0].rhs, r, 4 * N, cudaMemcpyHostToDevice, B->stream);
+  k_hook_ctrl<<<1, 1, 0, B->stream>>>(B->d_insts, sigma);
+  switch (B->precision) {
+    case FLUID_PP_FP16: vcycle_launch<__half>(B, pre, post); break;
+    case FLUID_PP_BF16: vcycle_launch<__nv_bfloat16>(B, pre, post); break;
+    default: vcycle_launch<float>(B, pre, post);
+  }
+  cudaMemcpyAsync(z, pp->inst.lv[0].z, 4 * N, cudaMemcpyDeviceToHost, B->stream);
+  cudaError_t e = cudaStreamSynchronize(B->stream);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+// ------------------------------------------------------------------ batch API
+int fluid_pp_batch_create(fluid_pp* const* handles, int count, fluid_pp_batch** out) {
+  std::string err;
+  const int rc = batch_build(handles, count, out, err);
+  g_err = err;
+  return rc;
+}
+
+void fluid_pp_batch_destroy(fluid_pp_batch* B) {
+  if (!B) return;
+  cudaSetDevice(B->device);
+  if (B->d_insts) cudaFree(B->d_insts);
+  if (B->d_ctrl) cudaFree(B->d_ctrl);
+  if (B->d_tiles) cudaFree(B->d_tiles);
+  if (B->d_ilist) cudaFree(B->d_ilist);
+  if (B->h_ctrl) cudaFreeHost(B->h_ctrl);
+  delete B;
+}
+
+int fluid_pp_batch_project(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts* opts,
+                           fluid_pp_receipt* receipts) {
+  if (!B) return FLUID_PP_INVALID_ARG;
+  if (dts)
+    for (size_t k = 0; k < B->h.size(); ++k)
+      if (!(dts[k] > 0) || !std::isfinite(dts[k])) {
+        B->err = "dt must be positive and finite";
+        return FLUID_PP_INVALID_ARG;
+      }
+  const int rc = batch_project(B, dts, opts, true, receipts);
+  if (rc != FLUID_PP_OK && rc != FLUID_PP_NONCONVERGENCE && rc != FLUID_PP_NONFINITE) g_err = B->err;
+  return rc;
+}
+
+}  // extern "C"

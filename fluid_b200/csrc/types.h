@@ -1,0 +1,88 @@
+// Device-visible descriptors shared by the host orchestration and the kernels.
+#pragma once
+#include <cstdint>
+
+#include "plan.h"
+
+namespace fpp {
+
+constexpr int kThreads = 256;      // threads per CTA for the grid kernels
+constexpr int kTile = 1024;        // cells per work tile (4 per thread)
+constexpr int kMaxCoarse = 128;    // largest coarsest level solved densely
+constexpr int kSlots = 4;          // reduction quantities per stage
+
+// Per-solve control word block, one per instance, resident on the device.
+// All scalar CG state lives here so no host round trip is needed inside a solve.
+struct Ctrl {
+  double bb;          // ||b||^2
+  double thr2;        // stopping threshold squared
+  double gamma;       // r.z of the current direction
+  double beta;
+  double delta;       // d.Ad
+  double alpha;
+  double rr;          // recursive ||r||^2
+  double rr_true;     // float64 ||b - A x||^2
+  double zmean;       // mean of z over liquid cells (unanchored systems only)
+  double bmean;
+  double sigma;       // preconditioner input scale (keeps half-precision levels in range)
+  double red[kSlots]; // last finalised reduction values
+  int iter;
+  int max_iter;
+  int true_every;
+  int first;          // 1 until the first direction is formed
+  int candidate;      // recursive residual below threshold; awaiting float64 check
+  int done;           // solve finished (converged or failed)
+  int status;         // FLUID_PP_* status of the solve
+  int liquid;         // liquid cells on the finest level
+  int air;            // air cells on the finest level
+  int top_liquid;     // liquid cells in the top row (open-top anchoring)
+  int nonfinite;      // non-finite input seen
+  int anchored;       // finest system has a Dirichlet contact
+  int converged;
+  unsigned arrive[8]; // per-stage completion counters (self-resetting)
+  int pad[2];
+};
+
+struct LevelDev {
+  int nx, ny, nz;
+  int sx, sy, sz;     // coarsening factor from the next finer level (1 or 2)
+  long long n;
+  int ntiles;
+  int coarse_block;   // unused marker
+  float wx, wy, wz;   // normalised off-diagonal weights w_a / wmax
+  float wmax;         // (h0 / h_a)^2 maximum over axes; level operators are stored divided by it
+  float ext_phi;      // open-top exterior phi (finest-cell units)
+  float to_coarse;    // wmax(l) / wmax(l+1): restriction rescale into the next level's units
+  uint8_t* label;     // 1 liquid, 0 air
+  float* phi;         // level set, finest-cell units
+  float* diag;        // exact float32 diagonal in finest-cell units (A_l), used by SpMV on level 0
+  void* diagT;        // normalised diagonal in the storage type (smoother)
+  void* z;            // level solution (level 0: float CG vector)
+  void* rhs;          // level right-hand side (level 0: the CG residual r, float)
+  void* res;          // level residual in the storage type
+};
+
+struct InstDev {
+  LevelDev lv[kMaxLevels];
+  int nlev;
+  int nx, ny, nz;
+  int open_top;
+  float h, rho, dt;
+  float pscale;       // rho * h / dt : finest-cell pressure -> Pa
+  int ntiles0;
+  int coarse_m;       // cells of the coarsest level
+  const float* vof;
+  float* u;
+  float* v;
+  float* w;
+  float* b;           // right-hand side, finest-cell units
+  float* x;           // pressure, finest-cell units
+  float* d;           // search direction
+  float* q;           // A d
+  float* p_si;        // pressure output in Pa
+  double* partial;    // kSlots * ntiles0 per-tile reduction partials
+  double* coarse_inv; // coarse_m^2 dense inverse of the coarsest operator
+  Ctrl* ctrl;
+};
+
+}  // namespace fpp

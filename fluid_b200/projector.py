@@ -1,0 +1,220 @@
+"""Host-side mirror of the reference's uniform pressure-projection interface.
+
+``PressureProjector`` stands where the reference's
+``WebGPUUniformPressureMultigrid`` (lib/methods/uniform/
+webgpu-uniform-pressure-multigrid.ts:228-607) plus the ``project`` dispatch
+(lib/methods/uniform/webgpu-uniform-reference.ts:1280-1282) stand: the
+constructor throws ``ValueError`` (the reference's ``RangeError``) for a lattice
+without a hierarchy or a bad spacing; numerical failures on the device are
+reported in the receipt's status, never raised.  All compute runs in the CUDA
+library through the C ABI; nothing here computes the projection.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from ._abi import Config, Receipt, SolveOpts, load, ptr
+
+
+class FluidError(RuntimeError):
+    pass
+
+
+def _check(rc: int, handle=None, what: str = ""):
+    if rc == _abi.OK:
+        return
+    L = load()
+    msg = L.fluid_pp_last_error(handle).decode() if handle is not None else L.fluid_pp_last_error(None).decode()
+    if rc == _abi.INVALID_ARG:
+        raise ValueError(msg or what)
+    if rc == _abi.OOM:
+        raise MemoryError(msg or what)
+    raise FluidError(f"{_abi.STATUS_NAMES.get(rc, rc)}: {msg or what}")
+
+
+def plan_uniform_cm11a_hierarchy(dimensions) -> dict:
+    """Mirror of planUniformCM11aHierarchy (webgpu-uniform-pressure-multigrid.ts:149-169).
+
+    Returns the reference's fields (levelCount, levelDimensions, coarsestCells,
+    semiCoarsened, rejection) plus ``extended`` for ceil-halved lattices the
+    reference rejects.
+    """
+    nx, ny, nz = (int(v) for v in dimensions)
+    L = load()
+    count, coarsest, semi, ext = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    dims = np.zeros((_abi.MAX_LEVELS, 3), np.int32)
+    rc = L.fluid_pp_plan_hierarchy(nx, ny, nz, ctypes.byref(count), ptr(dims), ctypes.byref(coarsest),
+                                   ctypes.byref(semi), ctypes.byref(ext))
+    if rc != _abi.OK:
+        return {"levelCount": 0, "levelDimensions": [], "coarsestCells": 0, "semiCoarsened": False,
+                "extended": False, "rejection": L.fluid_pp_last_error(None).decode() or "rejected"}
+    return {"levelCount": count.value, "levelDimensions": [tuple(int(v) for v in dims[l]) for l in range(count.value)],
+            "coarsestCells": coarsest.value, "semiCoarsened": bool(semi.value), "extended": bool(ext.value),
+            "rejection": None}
+
+
+def solve_opts(rel_tol=1e-6, abs_tol=0.0, max_iters=200, pre_sweeps=1, post_sweeps=1, true_residual_every=0,
+               warm_start=False) -> SolveOpts:
+    return SolveOpts(rel_tol, abs_tol, max_iters, pre_sweeps, post_sweeps, true_residual_every, int(warm_start))
+
+
+class PressureProjector:
+    """One uniform MAC grid resident on a B200: label -> divergence -> MGPCG -> gradient subtract."""
+
+    def __init__(self, dimensions, spacing: float, rho: float = 1000.0, open_top: bool = False,
+                 precision: str = "fp32", device: int = 0):
+        nx, ny, nz = (int(v) for v in dimensions)
+        if precision not in _abi.PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(_abi.PRECISIONS)}")
+        L = load()
+        self.dims = (nx, ny, nz)
+        self.h = float(spacing)
+        self.rho = float(rho)
+        self.precision = precision
+        cfg = Config(nx, ny, nz, self.h, self.rho, int(bool(open_top)), _abi.PRECISIONS[precision], int(device))
+        handle = ctypes.c_void_p()
+        _check(L.fluid_pp_create(ctypes.byref(cfg), ctypes.byref(handle)), None, "create")
+        self._h = handle
+        self._keep = []
+
+    # -- lifecycle -----------------------------------------------------------
+    def destroy(self):
+        if getattr(self, "_h", None):
+            load().fluid_pp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream: int):
+        _check(load().fluid_pp_set_stream(self._h, ctypes.c_void_p(int(stream))), self._h)
+
+    # -- state -----------------------------------------------------------------
+    def upload_state(self, vof, u, v, w):
+        nx, ny, nz = self.dims
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (vof, u, v, w)]
+        sizes = (nx * ny * nz, (nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1))
+        for a, s, name in zip(arrs, sizes, ("vof", "u", "v", "w")):
+            if a.size != s:
+                raise ValueError(f"{name} has {a.size} entries; expected {s}")
+        _check(load().fluid_pp_upload_state(self._h, *(ptr(a) for a in arrs)), self._h, "upload")
+
+    def upload_state_device(self, vof_ptr: int, u_ptr: int, v_ptr: int, w_ptr: int):
+        _check(load().fluid_pp_upload_state_device(self._h, *(ctypes.c_void_p(int(p)) for p in
+                                                             (vof_ptr, u_ptr, v_ptr, w_ptr))), self._h)
+
+    def project(self, dt: float, **opts) -> dict:
+        o = solve_opts(**opts)
+        r = Receipt()
+        rc = load().fluid_pp_project(self._h, float(dt), ctypes.byref(o), ctypes.byref(r))
+        if rc not in (_abi.OK, _abi.NONCONVERGENCE, _abi.NONFINITE):
+            _check(rc, self._h, "project")
+        return r.as_dict()
+
+    def project_async(self, dt: float, **opts):
+        o = solve_opts(**opts)
+        _check(load().fluid_pp_project_async(self._h, float(dt), ctypes.byref(o)), self._h, "project_async")
+
+    def receipt(self) -> dict:
+        r = Receipt()
+        rc = load().fluid_pp_receipt_read(self._h, ctypes.byref(r))
+        if rc not in (_abi.OK, _abi.NONCONVERGENCE, _abi.NONFINITE):
+            _check(rc, self._h, "receipt")
+        return r.as_dict()
+
+    def download(self):
+        nx, ny, nz = self.dims
+        p = np.empty((nz, ny, nx), np.float32)
+        u = np.empty((nz, ny, nx + 1), np.float32)
+        v = np.empty((nz, ny + 1, nx), np.float32)
+        w = np.empty((nz + 1, ny, nx), np.float32)
+        _check(load().fluid_pp_download(self._h, ptr(p), ptr(u), ptr(v), ptr(w)), self._h, "download")
+        return p, u, v, w
+
+    def device_arrays(self) -> dict:
+        ps = [ctypes.c_void_p() for _ in range(5)]
+        _check(load().fluid_pp_device_arrays(self._h, *(ctypes.byref(p) for p in ps)), self._h)
+        return dict(zip(("p", "u", "v", "w", "vof"), (p.value for p in ps)))
+
+    # -- parity hooks ----------------------------------------------------------
+    def prepare(self, dt: float):
+        _check(load().fluid_pp_prepare(self._h, float(dt)), self._h, "prepare")
+
+    def level_dims(self, level: int):
+        d = np.zeros(3, np.int32)
+        _check(load().fluid_pp_level_dims(self._h, level, ptr(d)), self._h)
+        return tuple(int(v) for v in d)
+
+    def level(self, level: int):
+        nx, ny, nz = self.level_dims(level)
+        lab = np.empty((nz, ny, nx), np.uint8)
+        phi = np.empty((nz, ny, nx), np.float32)
+        diag = np.empty((nz, ny, nx), np.float32)
+        _check(load().fluid_pp_get_level(self._h, level, ptr(lab), ptr(phi), ptr(diag)), self._h)
+        return lab, phi, diag
+
+    def rhs(self):
+        nx, ny, nz = self.dims
+        b = np.empty((nz, ny, nx), np.float32)
+        _check(load().fluid_pp_get_rhs(self._h, ptr(b)), self._h)
+        return b
+
+    def pressure_cells(self):
+        nx, ny, nz = self.dims
+        x = np.empty((nz, ny, nx), np.float32)
+        _check(load().fluid_pp_get_pressure_cells(self._h, ptr(x)), self._h)
+        return x
+
+    def apply_operator(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        out = np.empty_like(p)
+        _check(load().fluid_pp_apply_operator(self._h, ptr(p), ptr(out)), self._h)
+        return out
+
+    def apply_vcycle(self, r, pre: int = 1, post: int = 1):
+        r = np.ascontiguousarray(r, np.float32)
+        z = np.empty_like(r)
+        _check(load().fluid_pp_apply_vcycle(self._h, ptr(r), ptr(z), int(pre), int(post)), self._h)
+        return z
+
+
+class BatchProjector:
+    """Projects several handles with one launch per stage (uneven grid sizes allowed)."""
+
+    def __init__(self, projectors):
+        self.projectors = list(projectors)
+        arr = (ctypes.c_void_p * len(self.projectors))(*(p.handle for p in self.projectors))
+        b = ctypes.c_void_p()
+        _check(load().fluid_pp_batch_create(arr, len(self.projectors), ctypes.byref(b)), None, "batch_create")
+        self._b = b
+
+    def destroy(self):
+        if getattr(self, "_b", None):
+            load().fluid_pp_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def project(self, dts, **opts):
+        o = solve_opts(**opts)
+        n = len(self.projectors)
+        dt = np.ascontiguousarray(np.broadcast_to(np.asarray(dts, np.float32), (n,)))
+        rec = (Receipt * n)()
+        rc = load().fluid_pp_batch_project(self._b, ptr(dt), ctypes.byref(o), rec)
+        if rc not in (_abi.OK, _abi.NONCONVERGENCE, _abi.NONFINITE):
+            _check(rc, None, "batch_project")
+        return [r.as_dict() for r in rec]

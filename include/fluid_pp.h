@@ -1,0 +1,156 @@
+/*
+ * fluid_pp.h -- C ABI of the B200 free-surface pressure projection.
+ *
+ * One handle owns one dense uniform MAC grid resident in device memory: the
+ * VOF field, the face velocities, the multigrid hierarchy and the pressure.
+ * A projection runs: cell labelling -> divergence -> ghost-fluid theta
+ * assembly -> multigrid-preconditioned CG -> gradient subtract, entirely on
+ * the device, and returns a receipt.  Every entry point returns an int status
+ * (FLUID_PP_OK on success); no exception crosses the boundary.  Host pointers
+ * are borrowed for the duration of the call only.  One handle per host thread;
+ * the batch entry points are the only calls that touch several handles.
+ *
+ * Array layouts (float32, x fastest, cubic cells of size h):
+ *   vof [nz][ny][nx]      liquid volume fraction
+ *   u   [nz][ny][nx+1]    x-face velocity, face x sits between cells x-1 and x
+ *   v   [nz][ny+1][nx]    y-face velocity
+ *   w   [nz+1][ny][nx]    z-face velocity
+ *   p   [nz][ny][nx]      pressure in Pa (zero outside the liquid)
+ *
+ * Each declaration names the reference interface it replaces (paths inside
+ * the peter-suggate/fluid tree).
+ */
+#ifndef FLUID_PP_H
+#define FLUID_PP_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FLUID_PP_OK 0
+#define FLUID_PP_INVALID_ARG 1   /* host precondition failed (RangeError in the reference) */
+#define FLUID_PP_OOM 2
+#define FLUID_PP_NONFINITE 3     /* non-finite input; the previous pressure is kept */
+#define FLUID_PP_NONCONVERGENCE 4/* iteration cap or lost curvature; iterate published, status set */
+#define FLUID_PP_TIMEOUT 5
+#define FLUID_PP_CUDA 6          /* CUDA runtime error; see fluid_pp_last_error */
+#define FLUID_PP_UNSUPPORTED 7
+
+#define FLUID_PP_MAX_LEVELS 24
+
+enum fluid_pp_precision {
+  FLUID_PP_FP32 = 0, /* multigrid levels stored in float32 */
+  FLUID_PP_FP16 = 1, /* multigrid levels stored in float16, float32 arithmetic */
+  FLUID_PP_BF16 = 2  /* multigrid levels stored in bfloat16, float32 arithmetic */
+};
+
+typedef struct fluid_pp fluid_pp;
+typedef struct fluid_pp_batch fluid_pp_batch;
+
+typedef struct fluid_pp_config {
+  int nx, ny, nz;   /* physical lattice, cells */
+  float h;          /* cell size, m */
+  float rho;        /* liquid density, kg/m^3 */
+  int open_top;     /* 1: the +y domain face is atmospheric air, else a closed wall */
+  int precision;    /* enum fluid_pp_precision: storage of the V-cycle levels */
+  int device;       /* CUDA device ordinal */
+} fluid_pp_config;
+
+typedef struct fluid_pp_solve_opts {
+  double rel_tol;          /* stop when ||b - A p||_2 <= max(abs_tol, rel_tol * ||b||_2) */
+  double abs_tol;
+  int max_iters;           /* CG iteration cap */
+  int pre_sweeps;          /* red-black Gauss-Seidel sweeps before restriction */
+  int post_sweeps;         /* ... after prolongation (equal to pre_sweeps keeps M symmetric) */
+  int true_residual_every; /* recompute r = b - A p in float64 every k iterations (0: only at the end) */
+  int warm_start;          /* 1: start from the previous pressure of this handle */
+} fluid_pp_solve_opts;
+
+typedef struct fluid_pp_receipt {
+  int status;               /* FLUID_PP_* of this solve */
+  int iterations;           /* CG iterations */
+  int liquid_cells;
+  int levels;               /* multigrid levels */
+  double b_norm;            /* ||b||_2, finest-cell units */
+  double rel_residual;      /* recursive ||r||/||b|| at exit */
+  double true_rel_residual; /* ||b - A p||/||b|| recomputed in float64 */
+  double max_div_before;    /* max |div u - div_target| over liquid cells, 1/s */
+  double max_div_after;
+  double l2_div_before;     /* sqrt(sum (div)^2 h^3) over liquid cells */
+  double l2_div_after;
+} fluid_pp_receipt;
+
+/* Hierarchy planner, host only (no GPU needed).
+ * Replaces planUniformCM11aHierarchy
+ * (lib/methods/uniform/webgpu-uniform-pressure-multigrid.ts:149-169).  Lattices
+ * the reference rejects are planned by ceil-halving (extended = 1).
+ * level_dims receives level_count * 3 ints, finest first. */
+int fluid_pp_plan_hierarchy(int nx, int ny, int nz, int* level_count, int* level_dims, int* coarsest_cells,
+                            int* semi_coarsened, int* extended);
+
+/* Replaces `new WebGPUUniformPressureMultigrid(device, dims, spacing, schedule)`
+ * (webgpu-uniform-pressure-multigrid.ts:246-301) plus its initialize()
+ * (:311-324): allocates every level and the resident state. */
+int fluid_pp_create(const fluid_pp_config* config, fluid_pp** out);
+
+/* Replaces WebGPUUniformPressureMultigrid.destroy() (webgpu-uniform-pressure-multigrid.ts:595-604). */
+void fluid_pp_destroy(fluid_pp* pp);
+
+/* Launch every kernel of this handle on `stream` (a cudaStream_t; NULL = legacy default). */
+int fluid_pp_set_stream(fluid_pp* pp, void* stream);
+
+/* Copies the step's VOF and face velocities from host memory into the handle.
+ * Replaces the texture uploads of WebGPUUniformReferenceSolver
+ * (lib/methods/uniform/webgpu-uniform-reference.ts:836-894 initial state,
+ * velocity/volume textures bound at :405-413). */
+int fluid_pp_upload_state(fluid_pp* pp, const float* vof, const float* u, const float* v, const float* w);
+
+/* Device-pointer variant of upload: copies from device buffers (same layouts). */
+int fluid_pp_upload_state_device(fluid_pp* pp, const float* vof, const float* u, const float* v, const float* w);
+
+/* Label -> divergence -> assemble -> MGPCG -> gradient subtract, on the device.
+ * Replaces WebGPUUniformPressureMultigrid.encode (webgpu-uniform-pressure-multigrid.ts:327-364)
+ * followed by the `project` dispatch (webgpu-uniform-reference.ts:1280-1282);
+ * the receipt replaces the diagnostics words read by readStats
+ * (webgpu-uniform-reference.ts:1358-1420).  dt in seconds; opts may be NULL
+ * (rel 1e-6, 200 iterations, 1+1 sweeps).  The receipt is written after the
+ * stream synchronises. */
+int fluid_pp_project(fluid_pp* pp, float dt, const fluid_pp_solve_opts* opts, fluid_pp_receipt* receipt);
+
+/* Asynchronous form: enqueues the projection on the handle's stream and returns
+ * without synchronising; fluid_pp_receipt_read() synchronises and fills it. */
+int fluid_pp_project_async(fluid_pp* pp, float dt, const fluid_pp_solve_opts* opts);
+int fluid_pp_receipt_read(fluid_pp* pp, fluid_pp_receipt* receipt);
+
+/* Copies pressure (Pa) and projected velocities to host memory; any pointer may be NULL.
+ * Replaces the pressureTexture / velocity readback (webgpu-uniform-pressure-multigrid.ts:303). */
+int fluid_pp_download(fluid_pp* pp, float* p, float* u, float* v, float* w);
+
+/* Device pointers of the resident arrays (for zero-copy consumers); any may be NULL. */
+int fluid_pp_device_arrays(fluid_pp* pp, float** p, float** u, float** v, float** w, float** vof);
+
+/* Last error message of this handle (empty string when none). */
+const char* fluid_pp_last_error(const fluid_pp* pp);
+
+/* Parity hooks (host arrays).  Level data after the last project/prepare:
+ * label (1 liquid, 0 air), phi (finest-cell units), diag (float32, finest-cell units). */
+int fluid_pp_prepare(fluid_pp* pp, float dt);   /* label + divergence + hierarchy only */
+int fluid_pp_level_dims(fluid_pp* pp, int level, int* dims3);
+int fluid_pp_get_level(fluid_pp* pp, int level, unsigned char* label, float* phi, float* diag);
+int fluid_pp_get_rhs(fluid_pp* pp, float* b);
+int fluid_pp_apply_operator(fluid_pp* pp, const float* p, float* out);  /* finest A, host in/out */
+int fluid_pp_apply_vcycle(fluid_pp* pp, const float* r, float* z, int pre, int post);
+int fluid_pp_get_pressure_cells(fluid_pp* pp, float* x);             /* solution, finest-cell units */
+
+/* Batched projection of several handles in one set of launches per stage.
+ * Replaces nothing in the reference (which runs one solver per device); the
+ * per-solve semantics are those of fluid_pp_project. */
+int fluid_pp_batch_create(fluid_pp* const* handles, int count, fluid_pp_batch** out);
+void fluid_pp_batch_destroy(fluid_pp_batch* batch);
+int fluid_pp_batch_project(fluid_pp_batch* batch, const float* dts, const fluid_pp_solve_opts* opts,
+                           fluid_pp_receipt* receipts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLUID_PP_H */

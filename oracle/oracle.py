@@ -1,0 +1,181 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU baseline leg
+and reference arm may import this module.  It wraps ``oracle/_build/liboracle.so``
+(built from ``oracle/oracle.cpp`` by ``oracle/Makefile``), a float64 restatement
+of the reference's dense MAC ghost-fluid pressure projection; see the header of
+``oracle.cpp`` for the reference files and lines it follows.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        c_int, c_long, c_double, vp = ctypes.c_int, ctypes.c_long, ctypes.c_double, ctypes.c_void_p
+        L.orc_plan_hierarchy.argtypes = [c_int, c_int, c_int, ctypes.POINTER(c_int), vp, vp,
+                                         ctypes.POINTER(c_long), ctypes.POINTER(c_int), ctypes.POINTER(c_int)]
+        L.orc_plan_hierarchy.restype = c_int
+        L.orc_create.argtypes = [c_int, c_int, c_int, c_int, c_double, c_double]
+        L.orc_create.restype = vp
+        L.orc_destroy.argtypes = [vp]
+        L.orc_set_threads.argtypes = [vp, c_int]
+        L.orc_set_state.argtypes = [vp, vp, vp, vp, vp, c_double]
+        L.orc_set_state.restype = c_int
+        L.orc_num_levels.argtypes = [vp]
+        L.orc_num_levels.restype = c_int
+        L.orc_level_dims.argtypes = [vp, c_int, vp, vp, vp]
+        L.orc_get_level.argtypes = [vp, c_int, vp, vp, vp]
+        L.orc_get_rhs.argtypes = [vp, vp, vp]
+        L.orc_apply_level.argtypes = [vp, c_int, vp, vp]
+        L.orc_vcycle.argtypes = [vp, vp, vp, c_int, c_int]
+        L.orc_solve_jacobi.argtypes = [vp, c_double, c_double, c_int, vp, vp]
+        L.orc_solve_jacobi.restype = c_int
+        L.orc_solve_mgpcg.argtypes = [vp, c_double, c_double, c_int, c_int, c_int, vp, vp]
+        L.orc_solve_mgpcg.restype = c_int
+        L.orc_grad_subtract.argtypes = [vp, vp, vp, vp, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def plan_hierarchy(nx: int, ny: int, nz: int) -> dict:
+    """Planner restatement: reference lockstep/semi-coarsening, else ceil-halving."""
+    L = lib()
+    count = ctypes.c_int()
+    dims = np.zeros((24, 3), np.int32)
+    strides = np.zeros((24, 3), np.int32)
+    coarsest = ctypes.c_long()
+    semi = ctypes.c_int()
+    ext = ctypes.c_int()
+    rc = L.orc_plan_hierarchy(nx, ny, nz, ctypes.byref(count), _p(dims), _p(strides),
+                              ctypes.byref(coarsest), ctypes.byref(semi), ctypes.byref(ext))
+    return {"ok": rc == 0, "levels": [tuple(int(v) for v in dims[i]) for i in range(count.value)],
+            "strides": [tuple(int(v) for v in strides[i]) for i in range(count.value)],
+            "coarsest_cells": int(coarsest.value), "semi": bool(semi.value), "extended": bool(ext.value)}
+
+
+INFO_KEYS = ("iterations", "converged", "recursive_rel_residual", "true_rel_residual", "b_norm",
+             "reductions", "failure", "liquid_cells")
+
+
+class Oracle:
+    """One dense uniform grid; mirrors the device handle's lifecycle."""
+
+    def __init__(self, nx: int, ny: int, nz: int, h: float, rho: float = 1000.0, open_top: bool = False):
+        self.n = (nx, ny, nz)
+        self.h, self.rho = h, rho
+        self.open_top = bool(open_top)
+        self._h = lib().orc_create(nx, ny, nz, int(open_top), h, rho)
+        if not self._h:
+            raise ValueError("CM11a coarsest grid must be integral and fit its 256-lane high-precision solve")
+        self.dt = 1.0
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_destroy(self._h)
+            self._h = None
+
+    def set_threads(self, threads: int):
+        lib().orc_set_threads(self._h, int(threads))
+
+    def set_state(self, vof, u, v, w, dt: float):
+        nx, ny, nz = self.n
+        self._vof = np.ascontiguousarray(vof, np.float32).reshape(nz, ny, nx)
+        self._u = np.ascontiguousarray(u, np.float32).reshape(nz, ny, nx + 1)
+        self._v = np.ascontiguousarray(v, np.float32).reshape(nz, ny + 1, nx)
+        self._w = np.ascontiguousarray(w, np.float32).reshape(nz + 1, ny, nx)
+        self.dt = dt
+        lib().orc_set_state(self._h, _p(self._vof), _p(self._u), _p(self._v), _p(self._w), dt)
+
+    @property
+    def num_levels(self) -> int:
+        return lib().orc_num_levels(self._h)
+
+    def level_dims(self, l: int):
+        d = np.zeros(3, np.int32)
+        wgt = np.zeros(3, np.float64)
+        anch = np.zeros(1, np.int32)
+        lib().orc_level_dims(self._h, l, _p(d), _p(wgt), _p(anch))
+        return tuple(int(x) for x in d), tuple(float(x) for x in wgt), bool(anch[0])
+
+    def level(self, l: int):
+        (nx, ny, nz), _, _ = self.level_dims(l)
+        lab = np.zeros((nz, ny, nx), np.uint8)
+        phi = np.zeros((nz, ny, nx), np.float32)
+        diag = np.zeros((nz, ny, nx), np.float64)
+        lib().orc_get_level(self._h, l, _p(lab), _p(phi), _p(diag))
+        return lab, phi, diag
+
+    def rhs(self):
+        nx, ny, nz = self.n
+        b = np.zeros((nz, ny, nx), np.float64)
+        q = np.zeros((nz, ny, nx), np.float64)
+        lib().orc_get_rhs(self._h, _p(b), _p(q))
+        return b, q
+
+    def apply(self, p, l: int = 0):
+        (nx, ny, nz), _, _ = self.level_dims(l)
+        p = np.ascontiguousarray(p, np.float64).reshape(nz, ny, nx)
+        out = np.zeros_like(p)
+        lib().orc_apply_level(self._h, l, _p(p), _p(out))
+        return out
+
+    def vcycle(self, r, pre: int = 1, post: int = 1):
+        nx, ny, nz = self.n
+        r = np.ascontiguousarray(r, np.float64).reshape(nz, ny, nx)
+        z = np.zeros_like(r)
+        lib().orc_vcycle(self._h, _p(r), _p(z), pre, post)
+        return z
+
+    def solve_jacobi(self, rel_tol=1e-10, abs_tol=1e-12, max_iter=None):
+        nx, ny, nz = self.n
+        p = np.zeros((nz, ny, nx), np.float64)
+        info = np.zeros(8, np.float64)
+        if max_iter is None:
+            max_iter = max(64, 4 * nx * ny * nz)
+        lib().orc_solve_jacobi(self._h, rel_tol, abs_tol, int(max_iter), _p(p), _p(info))
+        return p, dict(zip(INFO_KEYS, info.tolist()))
+
+    def solve_mgpcg(self, rel_tol=1e-10, abs_tol=0.0, max_iter=200, pre=1, post=1):
+        nx, ny, nz = self.n
+        p = np.zeros((nz, ny, nx), np.float64)
+        info = np.zeros(8, np.float64)
+        lib().orc_solve_mgpcg(self._h, rel_tol, abs_tol, int(max_iter), pre, post, _p(p), _p(info))
+        return p, dict(zip(INFO_KEYS, info.tolist()))
+
+    def grad_subtract(self, p):
+        nx, ny, nz = self.n
+        p = np.ascontiguousarray(p, np.float64).reshape(nz, ny, nx)
+        uo = np.zeros((nz, ny, nx + 1), np.float32)
+        vo = np.zeros((nz, ny + 1, nx), np.float32)
+        wo = np.zeros((nz + 1, ny, nx), np.float32)
+        out = np.zeros(4, np.float64)
+        lib().orc_grad_subtract(self._h, _p(p), _p(uo), _p(vo), _p(wo), _p(out))
+        return (uo, vo, wo), {"max_div_before": out[0], "max_div_after": out[1],
+                              "l2_div_before": out[2], "l2_div_after": out[3]}
+
+    def pressure_si(self, p_cells):
+        """Dimensional pressure (Pa) from finest-cell-unit pressure."""
+        return p_cells * self.rho * self.h / self.dt

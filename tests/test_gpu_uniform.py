@@ -1,0 +1,179 @@
+"""Parity of the CUDA uniform-grid projection against the float64 oracle (GPU)."""
+import numpy as np
+import pytest
+
+from fluid_b200 import BatchProjector, PressureProjector, configs
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+REL_L2_PRESSURE = 1e-5      # pressure vs the float64 oracle
+DIV_RATIO = 1e-6            # max post-projection divergence / max pre-projection divergence
+REL_RES = 1e-6
+
+
+def _pair(s, precision="fp32"):
+    pp = PressureProjector((s.nx, s.ny, s.nz), s.h, s.rho, s.open_top, precision)
+    pp.upload_state(s.vof, s.u, s.v, s.w)
+    o = Oracle(s.nx, s.ny, s.nz, s.h, s.rho, s.open_top)
+    o.set_state(s.vof, s.u, s.v, s.w, s.dt)
+    return pp, o
+
+
+CASES = {
+    "dam32": lambda: configs.dam_break_32(),
+    "odd37x50x29": lambda: configs.random_small(37, 50, 29, seed=11),
+    "semi2x64x48": lambda: configs.random_small(2, 64, 48, seed=12),
+    "open_top24": lambda: configs.random_small(24, 24, 24, seed=13, open_top=True),
+    "thin40x8x24": lambda: configs.random_small(40, 8, 24, seed=14),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_labels_and_level_maps_bit_exact(name):
+    s = CASES[name]()
+    pp, o = _pair(s)
+    pp.prepare(s.dt)
+    assert o.num_levels == len([1 for _ in range(o.num_levels)])
+    for l in range(o.num_levels):
+        (dims, _, _) = o.level_dims(l)
+        assert pp.level_dims(l) == dims
+        lab_d, phi_d, diag_d = pp.level(l)
+        lab_o, phi_o, diag_o = o.level(l)
+        np.testing.assert_array_equal(lab_d, lab_o, err_msg=f"labels level {l}")
+        np.testing.assert_array_equal(phi_d.view(np.uint32), phi_o.view(np.uint32), err_msg=f"phi level {l}")
+        np.testing.assert_allclose(diag_d, diag_o, rtol=2e-6, atol=1e-12, err_msg=f"diag level {l}")
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_rhs_and_operator(name):
+    s = CASES[name]()
+    pp, o = _pair(s)
+    pp.prepare(s.dt)
+    b_o, _ = o.rhs()
+    b_d = pp.rhs()
+    scale = np.abs(b_o).max()
+    assert np.abs(b_d - b_o).max() <= 1e-6 * scale
+    lab, _, _ = o.level(0)
+    rng = np.random.default_rng(5)
+    p = (rng.normal(size=lab.shape) * lab).astype(np.float32)
+    ap_d = pp.apply_operator(p)
+    ap_o = o.apply(p.astype(np.float64))
+    assert np.linalg.norm(ap_d - ap_o) <= 1e-6 * np.linalg.norm(ap_o)
+
+
+@pytest.mark.parametrize("name", ["dam32", "odd37x50x29", "semi2x64x48", "open_top24"])
+def test_vcycle_matches_oracle_and_is_symmetric(name):
+    s = CASES[name]()
+    pp, o = _pair(s)
+    pp.prepare(s.dt)
+    lab, _, _ = o.level(0)
+    rng = np.random.default_rng(7)
+    x = (rng.normal(size=lab.shape) * lab).astype(np.float32)
+    y = (rng.normal(size=lab.shape) * lab).astype(np.float32)
+    for pre in (1, 2):
+        zx = pp.apply_vcycle(x, pre, pre)
+        zo = o.vcycle(x.astype(np.float64), pre, pre)
+        assert np.linalg.norm(zx - zo) <= 2e-5 * np.linalg.norm(zo), pre
+        zy = pp.apply_vcycle(y, pre, pre)
+        a, b = float(np.dot(x.ravel().astype(np.float64), zy.ravel())), float(np.dot(zx.ravel().astype(np.float64), y.ravel()))
+        assert abs(a - b) <= 1e-5 * np.sqrt(abs(np.dot(x.ravel(), zx.ravel()) * np.dot(y.ravel(), zy.ravel())))
+
+
+def _check_projection(s, precision, rec, pp, o):
+    assert rec["status_name"] == "OK", rec
+    assert rec["true_rel_residual"] <= REL_RES
+    p_ref, info = o.solve_mgpcg(1e-12, 0.0, 300, 2, 2)
+    assert info["converged"] == 1.0
+    x = pp.pressure_cells().astype(np.float64)
+    err = np.linalg.norm(x - p_ref) / np.linalg.norm(p_ref)
+    assert err <= REL_L2_PRESSURE, (precision, err)
+    assert rec["max_div_after"] <= DIV_RATIO * rec["max_div_before"], rec
+    (uo, vo, wo), orec = o.grad_subtract(p_ref)
+    p_si, u, v, w = pp.download()
+    scale = max(np.abs(uo).max(), np.abs(vo).max(), np.abs(wo).max())
+    for dev, ref in ((u, uo), (v, vo), (w, wo)):
+        assert np.abs(dev - ref).max() <= 1e-4 * scale
+    np.testing.assert_allclose(p_si, o.pressure_si(p_ref).astype(np.float32) * (x != 0),
+                               rtol=0, atol=1e-4 * np.abs(o.pressure_si(p_ref)).max())
+    return err
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16"])
+@pytest.mark.parametrize("name", ["dam32", "odd37x50x29", "open_top24"])
+def test_project_matches_oracle(name, precision):
+    s = CASES[name]()
+    pp, o = _pair(s, precision)
+    rec = pp.project(s.dt, rel_tol=REL_RES)
+    _check_projection(s, precision, rec, pp, o)
+
+
+def test_all_liquid_box_nullspace():
+    n = 16
+    rng = np.random.default_rng(3)
+    vof = np.ones((n, n, n), np.float32)
+    s = configs.GridState(n, n, n, 1.0 / n, 1 / 60, vof, *configs.velocities(vof, rng, 1 / 60, "gauss", 0.2))
+    pp, o = _pair(s)
+    rec = pp.project(s.dt, rel_tol=REL_RES)
+    assert rec["status_name"] == "OK", rec
+    p_ref, info = o.solve_mgpcg(1e-12, 0.0, 300, 2, 2)
+    x = pp.pressure_cells().astype(np.float64)
+    x -= x.mean()
+    assert np.linalg.norm(x - p_ref) <= REL_L2_PRESSURE * np.linalg.norm(p_ref)
+    assert rec["max_div_after"] <= DIV_RATIO * rec["max_div_before"]
+
+
+def test_nonfinite_input_keeps_previous_pressure():
+    s = configs.dam_break_32()
+    pp, _ = _pair(s)
+    rec = pp.project(s.dt)
+    assert rec["status_name"] == "OK"
+    p0, u0, v0, w0 = pp.download()
+    bad = s.vof.copy()
+    bad[3, 3, 3] = np.nan
+    pp.upload_state(bad, u0, v0, w0)
+    rec2 = pp.project(s.dt)
+    assert rec2["status_name"] == "NONFINITE"
+    p1, _, _, _ = pp.download()
+    np.testing.assert_array_equal(p0, p1)
+
+
+def test_iteration_cap_reports_nonconvergence():
+    s = configs.dam_break_32()
+    pp, _ = _pair(s)
+    rec = pp.project(s.dt, rel_tol=1e-12, max_iters=2)
+    assert rec["status_name"] == "NONCONVERGENCE"
+    assert rec["iterations"] == 2
+
+
+def test_batch_is_identical_to_single():
+    states = [configs.random_small(n[0], n[1], n[2], seed=20 + k)
+              for k, n in enumerate([(24, 30, 28), (37, 25, 41), (16, 16, 16), (48, 20, 33)])]
+    singles = []
+    for s in states:
+        pp = PressureProjector((s.nx, s.ny, s.nz), s.h)
+        pp.upload_state(s.vof, s.u, s.v, s.w)
+        singles.append((pp.project(s.dt), pp.pressure_cells()))
+    pps = []
+    for s in states:
+        pp = PressureProjector((s.nx, s.ny, s.nz), s.h)
+        pp.upload_state(s.vof, s.u, s.v, s.w)
+        pps.append(pp)
+    batch = BatchProjector(pps)
+    recs = batch.project([s.dt for s in states])
+    for (r1, x1), r2, pp in zip(singles, recs, pps):
+        assert r2["status_name"] == "OK"
+        assert r1["iterations"] == r2["iterations"]
+        np.testing.assert_array_equal(x1, pp.pressure_cells())
+
+
+def test_full_size_dam_spheres_properties():
+    s = configs.dam_spheres()
+    for precision in ("fp32", "fp16"):
+        pp = PressureProjector((s.nx, s.ny, s.nz), s.h, precision=precision)
+        pp.upload_state(s.vof, s.u, s.v, s.w)
+        rec = pp.project(s.dt, rel_tol=REL_RES)
+        assert rec["status_name"] == "OK", rec
+        assert rec["true_rel_residual"] <= REL_RES
+        assert rec["max_div_after"] <= DIV_RATIO * rec["max_div_before"], rec
+        assert rec["levels"] == 7
