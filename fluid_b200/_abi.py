@@ -24,7 +24,12 @@ EXPORTS = (
     "fluid_pp_prepare", "fluid_pp_level_dims", "fluid_pp_get_level", "fluid_pp_get_rhs",
     "fluid_pp_apply_operator", "fluid_pp_apply_vcycle", "fluid_pp_get_pressure_cells",
     "fluid_pp_batch_create", "fluid_pp_batch_destroy", "fluid_pp_batch_project",
+    "fluid_pp_kernel_launches", "fluid_pp_set_profiling", "fluid_pp_profile_read",
+    "fluid_pp_batch_set_profiling", "fluid_pp_batch_profile_read",
 )
+STAGES = ("reset", "label", "coarsen", "bake", "factor", "init", "smooth0", "smoothc", "residual0", "residualc",
+          "restrict0", "restrictc", "coarse", "prolong0", "prolongc", "dot", "dir", "spmv", "update", "true",
+          "grad", "receipt")
 
 
 class Config(ctypes.Structure):
@@ -36,7 +41,8 @@ class Config(ctypes.Structure):
 class SolveOpts(ctypes.Structure):
     _fields_ = [("rel_tol", ctypes.c_double), ("abs_tol", ctypes.c_double), ("max_iters", ctypes.c_int),
                 ("pre_sweeps", ctypes.c_int), ("post_sweeps", ctypes.c_int),
-                ("true_residual_every", ctypes.c_int), ("warm_start", ctypes.c_int)]
+                ("true_residual_every", ctypes.c_int), ("warm_start", ctypes.c_int),
+                ("rel_tol_inf", ctypes.c_double)]
 
 
 class Receipt(ctypes.Structure):
@@ -90,6 +96,12 @@ def load():
     L.fluid_pp_batch_destroy.argtypes = [vp]
     L.fluid_pp_batch_destroy.restype = None
     L.fluid_pp_batch_project.argtypes = [vp, vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(Receipt)]
+    L.fluid_pp_kernel_launches.argtypes = []
+    L.fluid_pp_kernel_launches.restype = ctypes.c_ulonglong
+    L.fluid_pp_set_profiling.argtypes = [vp, ci]
+    L.fluid_pp_profile_read.argtypes = [vp, vp, vp, ci]
+    L.fluid_pp_batch_set_profiling.argtypes = [vp, ci]
+    L.fluid_pp_batch_profile_read.argtypes = [vp, vp, vp, ci]
     _lib = L
     return L
 

@@ -58,9 +58,16 @@ def box_vof(nx, ny, nz, lo, hi) -> np.ndarray:
 
 def sphere_vof(nx, ny, nz, centre, radius) -> np.ndarray:
     """Linear ramp of the signed distance over one cell (cell units)."""
-    z, y, x = np.meshgrid(np.arange(nz) + 0.5, np.arange(ny) + 0.5, np.arange(nx) + 0.5, indexing="ij")
+    out = np.zeros((nz, ny, nx))
+    lo = [max(0, int(math.floor(c - radius - 2))) for c in centre]
+    hi = [min(n, int(math.ceil(c + radius + 2))) for c, n in zip(centre, (nx, ny, nz))]
+    if any(h <= l for l, h in zip(lo, hi)):
+        return out
+    z, y, x = np.meshgrid(np.arange(lo[2], hi[2]) + 0.5, np.arange(lo[1], hi[1]) + 0.5,
+                          np.arange(lo[0], hi[0]) + 0.5, indexing="ij")
     d = np.sqrt((x - centre[0]) ** 2 + (y - centre[1]) ** 2 + (z - centre[2]) ** 2) - radius
-    return np.clip(0.5 - d, 0.0, 1.0)
+    out[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]] = np.clip(0.5 - d, 0.0, 1.0)
+    return out
 
 
 def fluid_face_masks(vof: np.ndarray):

