@@ -26,6 +26,7 @@ EXPORTS = (
     "fluid_pp_batch_create", "fluid_pp_batch_destroy", "fluid_pp_batch_project",
     "fluid_pp_kernel_launches", "fluid_pp_set_profiling", "fluid_pp_profile_read",
     "fluid_pp_batch_set_profiling", "fluid_pp_batch_profile_read",
+    "fluid_pp_apply_operator_noalloc",
 )
 STAGES = ("reset", "label", "coarsen", "bake", "factor", "init", "smooth0", "smoothc", "residual0", "residualc",
           "restrict0", "restrictc", "coarse", "prolong0", "prolongc", "dot", "dir", "spmv", "update", "true",
@@ -102,6 +103,7 @@ def load():
     L.fluid_pp_profile_read.argtypes = [vp, vp, vp, ci]
     L.fluid_pp_batch_set_profiling.argtypes = [vp, ci]
     L.fluid_pp_batch_profile_read.argtypes = [vp, vp, vp, ci]
+    L.fluid_pp_apply_operator_noalloc.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp, vp]
     _lib = L
     return L
 

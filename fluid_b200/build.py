@@ -15,8 +15,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libfluid_pp.so")
-SOURCES = ["solver.cu", "plan.cpp"]
-HEADERS = ["kernels.cuh", "types.h", "plan.h"]
+SOURCES = ["solver.cu", "noalloc.cu", "plan.cpp"]
+HEADERS = ["kernels.cuh", "device_util.cuh", "types.h", "plan.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -1,0 +1,177 @@
+// Inline device helpers shared by every kernel translation unit: work-tile
+// geometry, storage-type access, the canonical stencil fold, deterministic
+// block reductions and the last-tile-arrives pattern, trilinear transfer weights.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "../../include/fluid_pp.h"
+#include "types.h"
+
+namespace fpp {
+
+struct Tile {
+  int inst;
+  int level;
+  int tile;
+  int pad;
+};
+
+constexpr int kTX = 32, kTY = 8, kTZ = 4;   // tile extent; kTX * kTY == kThreads
+constexpr int kBlockThreads = 1024;        // coarse-block CTA
+
+__host__ __device__ inline int tiles_of(int nx, int ny, int nz) {
+  return ((nx + kTX - 1) / kTX) * ((ny + kTY - 1) / kTY) * ((nz + kTZ - 1) / kTZ);
+}
+
+// The cells of tile t owned by this thread.
+struct TileIt {
+  int x, y, z0, k, nx, ny, nz;
+  bool ok;
+  __device__ __forceinline__ TileIt(int t, int nx_, int ny_, int nz_) : k(0), nx(nx_), ny(ny_), nz(nz_) {
+    const int ntx = (nx + kTX - 1) / kTX, nty = (ny + kTY - 1) / kTY;
+    const int tx = t % ntx, r = t / ntx, ty = r % nty, tz = r / nty;
+    x = tx * kTX + int(threadIdx.x & (kTX - 1));
+    y = ty * kTY + int(threadIdx.x / kTX);
+    z0 = tz * kTZ;
+    ok = x < nx && y < ny;
+  }
+  __device__ __forceinline__ bool next(int& cx, int& cy, int& cz, int& i) {
+    if (!ok || k >= kTZ) return false;
+    const int z = z0 + k++;
+    if (z >= nz) return false;
+    cx = x;
+    cy = y;
+    cz = z;
+    i = x + nx * (y + ny * z);
+    return true;
+  }
+};
+
+// ------------------------------------------------------------ storage types
+template <class T>
+struct St;
+template <>
+struct St<float> {
+  static __device__ __forceinline__ float ld(const void* p, long long i) { return static_cast<const float*>(p)[i]; }
+  static __device__ __forceinline__ void st(void* p, long long i, float v) { static_cast<float*>(p)[i] = v; }
+};
+template <>
+struct St<__half> {
+  static __device__ __forceinline__ float ld(const void* p, long long i) {
+    return __half2float(static_cast<const __half*>(p)[i]);
+  }
+  static __device__ __forceinline__ void st(void* p, long long i, float v) {
+    static_cast<__half*>(p)[i] = __float2half_rn(v);
+  }
+};
+template <>
+struct St<__nv_bfloat16> {
+  static __device__ __forceinline__ float ld(const void* p, long long i) {
+    return __bfloat162float(static_cast<const __nv_bfloat16*>(p)[i]);
+  }
+  static __device__ __forceinline__ void st(void* p, long long i, float v) {
+    static_cast<__nv_bfloat16*>(p)[i] = __float2bfloat16_rn(v);
+  }
+};
+
+__device__ __forceinline__ void decode(int i, int nx, int ny, int& x, int& y, int& z) {
+  const int yz = i / nx;
+  x = i - yz * nx;
+  z = yz / ny;
+  y = yz - z * ny;
+}
+
+// cm12GhostFluidTheta (lib/core/cm12-numerics.ts:37-45), epsilon 1e-12.
+__device__ __forceinline__ float ghost_theta(float liquid_phi, float air_phi) {
+  const float a = fabsf(liquid_phi);
+  return fminf(1.0f, fmaxf(0.05f, a / fmaxf(a + fabsf(air_phi), 1e-12f)));
+}
+
+// Canonical fold of the six face terms (mgD4Sum6, mg.wgsl.ts:49).
+__device__ __forceinline__ float d4sum6(float xm, float xp, float ym, float yp, float zm, float zp) {
+  return ((xm + xp) + (zm + zp)) + (ym + yp);
+}
+
+// Deterministic block reductions (fixed shuffle tree).  Result valid in warp 0.
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0;
+  if (w == 0) {
+    r = l < int(blockDim.x >> 5) ? sh[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+  }
+  __syncthreads();
+  return r;
+}
+__device__ __forceinline__ double block_max(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0;
+  if (w == 0) {
+    r = l < int(blockDim.x >> 5) ? sh[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+  }
+  __syncthreads();
+  return r;
+}
+
+// Publish this tile's partials and report whether it is the instance's last.
+__device__ __forceinline__ bool arrive_last(unsigned* counter, int total, int* flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned prev = atomicAdd(counter, 1u);
+    *flag = prev == unsigned(total - 1);
+    if (*flag) {
+      __threadfence();
+      *counter = 0u;   // every tile of this instance has arrived: reset for the next launch
+    }
+  }
+  __syncthreads();
+  return *flag != 0;
+}
+
+// Sum (op 0) or max (op 1) of one slot over all tiles, in tile order.
+__device__ __forceinline__ double gather_slot(const double* partial, int slot, int ntiles, int op, double* sh) {
+  const volatile double* p = partial + (long long)slot * ntiles;
+  double acc = 0;
+  for (int t = threadIdx.x; t < ntiles; t += blockDim.x) acc = op ? fmax(acc, p[t]) : acc + p[t];
+  return op ? block_max(acc, sh) : block_sum(acc, sh);
+}
+
+// Cell-centred trilinear prolongation taps along one axis (mgTrilinearPressure,
+// mg.wgsl.ts:217-241): taps outside the grid dropped, weights renormalised.
+__device__ __forceinline__ int taps1d(int f, int stride, int nc, int* c, float* w) {
+  if (stride == 1) {
+    c[0] = f;
+    w[0] = 1.0f;
+    return 1;
+  }
+  const int k = f >> 1;
+  int a, b;
+  float wa, wb;
+  if ((f & 1) == 0) { a = k - 1; wa = 0.25f; b = k; wb = 0.75f; }
+  else { a = k; wa = 0.75f; b = k + 1; wb = 0.25f; }
+  int n = 0;
+  if (a >= 0 && a < nc) { c[n] = a; w[n] = wa; ++n; }
+  if (b >= 0 && b < nc) { c[n] = b; w[n] = wb; ++n; }
+  if (n == 1) w[0] = 1.0f;
+  return n;
+}
+
+// Weight of coarse cell c in the stencil of fine cell f along an axis that
+// coarsened by two (the transpose entries of taps1d).
+__device__ __forceinline__ float p1d(int f, int c, int nc) {
+  const int d = f - 2 * c;
+  if (d == 0) return c == 0 ? 1.0f : 0.75f;
+  if (d == 1) return c + 1 == nc ? 1.0f : 0.75f;
+  return 0.25f;   // d == -1 or d == 2
+}
+
+}  // namespace fpp

@@ -1,0 +1,125 @@
+// Allocation-free form of the finest-level operator apply (A p and p . A p).
+//
+// Some host applications cannot let a plug-in allocate device memory: a game
+// engine or renderer that has reserved the GPU's memory for its own pool, or a
+// framework whose caching allocator holds the free memory, so that a cudaMalloc
+// from this library would fail or break the host's memory budget.  For them this
+// entry point does all of its work in caller-provided buffers plus one fixed
+// scratch array that lives in this library's device image.
+//
+// The scratch array below is file-scope device memory: every GPU that loads
+// the library holds it (about 128 KB) until the process exits.  Its name is a
+// host-side stand-in, not a device address, so the host looks the address up
+// with cudaGetSymbolAddress once per device (with that device current) and
+// passes it to the kernel.  Every call on a device shares the one array and it
+// keeps the last call's contents, so calls whose GPU work overlaps (different
+// streams, or the same stream from several threads without ordering) race on it.
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+
+#include "../../include/fluid_pp.h"
+#include "device_util.cuh"
+
+namespace {
+
+// Partials of at most kNoAllocMaxTiles work tiles (32x8x4 cells each), then
+// the arrival counter of the last-tile reduction.
+constexpr int kNoAllocMaxTiles = 16384;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxTiles + 32];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mutex;
+double* g_scratch_ptr[kMaxDevices] = {};
+
+}  // namespace
+
+namespace fpp {
+void set_global_error(const std::string& message);   // read back by fluid_pp_last_error(NULL)
+
+// out = A p on the finest level and *p_dot_ap = p . A p (float64, tile order).
+// A is the ghost-fluid operator of k_spmv: diag on liquid cells, -1 to liquid
+// neighbours; air entries of p are treated as zero.
+__global__ void k_spmv_noalloc(int nx, int ny, int nz, const uint8_t* __restrict__ label,
+                               const float* __restrict__ diag, const float* __restrict__ p, float* __restrict__ out,
+                               double* __restrict__ p_dot_ap, double* scratch, int ntiles) {
+  __shared__ double sh[32];
+  __shared__ int flag;
+  unsigned* counter = reinterpret_cast<unsigned*>(scratch + kNoAllocMaxTiles);
+  const int sy = nx, sz = nx * ny;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    double dq = 0;
+    int x, y, z, i;
+    for (TileIt it(t, nx, ny, nz); it.next(x, y, z, i);) {
+      float q = 0.0f;
+      if (label[i]) {
+        auto nb = [&](bool in, int j) { return (in && label[j]) ? p[j] : 0.0f; };
+        const float s = d4sum6(nb(x > 0, i - 1), nb(x + 1 < nx, i + 1), nb(y > 0, i - sy), nb(y + 1 < ny, i + sy),
+                               nb(z > 0, i - sz), nb(z + 1 < nz, i + sz));
+        q = diag[i] * p[i] - s;
+        dq += double(p[i]) * q;
+      }
+      out[i] = q;
+    }
+    const double a = block_sum(dq, sh);
+    if (threadIdx.x == 0) scratch[t] = a;
+    if (arrive_last(counter, ntiles, &flag)) {
+      const double total = gather_slot(scratch, 0, ntiles, 0, sh);
+      if (threadIdx.x == 0) *p_dot_ap = total;
+    }
+  }
+}
+
+}  // namespace fpp
+
+extern "C" int fluid_pp_apply_operator_noalloc(int nx, int ny, int nz, const unsigned char* label,
+                                               const float* diag, const float* p, float* out, double* p_dot_ap,
+                                               void* stream) {
+  if (nx < 1 || ny < 1 || nz < 1 || !label || !diag || !p || !out || !p_dot_ap) {
+    fpp::set_global_error("fluid_pp_apply_operator_noalloc: null pointer or empty lattice");
+    return FLUID_PP_INVALID_ARG;
+  }
+  const long long tiles = (long long)((nx + fpp::kTX - 1) / fpp::kTX) * ((ny + fpp::kTY - 1) / fpp::kTY) *
+                          ((nz + fpp::kTZ - 1) / fpp::kTZ);
+  if (tiles > kNoAllocMaxTiles || (long long)nx * ny * nz > (1LL << 30)) {
+    fpp::set_global_error("fluid_pp_apply_operator_noalloc: lattice needs " + std::to_string(tiles) +
+                    " work tiles of 32x8x4 cells; the fixed scratch holds " + std::to_string(kNoAllocMaxTiles));
+    return FLUID_PP_INVALID_ARG;
+  }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    fpp::set_global_error("fluid_pp_apply_operator_noalloc: no usable current device");
+    return FLUID_PP_CUDA;
+  }
+  double* scratch = nullptr;
+  {
+    // First call on this device: look up the scratch address with the device current.
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_scratch_ptr[dev]) {
+      void* ptr = nullptr;
+      e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+      if (e != cudaSuccess) {
+        fpp::set_global_error(std::string("fluid_pp_apply_operator_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        return FLUID_PP_CUDA;
+      }
+      g_scratch_ptr[dev] = static_cast<double*>(ptr);
+    }
+    scratch = g_scratch_ptr[dev];
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // The arrival counter must start at zero; the partials are all overwritten.
+  e = cudaMemsetAsync(scratch + kNoAllocMaxTiles, 0, sizeof(double), s);
+  if (e == cudaSuccess) {
+    const int grid = int(tiles < 148 * 8 ? tiles : 148 * 8);
+    fpp::k_spmv_noalloc<<<grid, fpp::kThreads, 0, s>>>(nx, ny, nz, label, diag, p, out, p_dot_ap, scratch, int(tiles));
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    fpp::set_global_error(std::string("fluid_pp_apply_operator_noalloc: ") + cudaGetErrorString(e));
+    return FLUID_PP_CUDA;
+  }
+  return FLUID_PP_OK;
+}
+

@@ -377,6 +377,10 @@ int ensure_graphs(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
 
 }  // namespace
 
+namespace fpp {
+void set_global_error(const std::string& message) { g_err = message; }
+}  // namespace fpp
+
 // ==================================================================== batch
 static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out, std::string& err) {
   if (!handles || count <= 0 || !out) {

@@ -174,6 +174,27 @@ int fluid_pp_profile_read(fluid_pp* pp, double* ms, long long* launches, int res
 int fluid_pp_batch_set_profiling(fluid_pp_batch* batch, int on);
 int fluid_pp_batch_profile_read(fluid_pp_batch* batch, double* ms, long long* launches, int reset);
 
+/* Allocation-free finest-level operator apply.  This entry point has no
+ * counterpart in the reference.  It is for host applications that cannot let a
+ * plug-in allocate device memory (an engine or renderer that has reserved the
+ * GPU's memory for its own pool, or a framework whose caching allocator holds
+ * the free memory): it allocates nothing and calls no allocating routine.
+ * All buffers are caller-owned device memory, x fastest, nx*ny*nz cells:
+ * label (1 liquid / 0 air) and diag as returned by fluid_pp_get_level(level 0)
+ * for the same state, p the vector to apply.  Writes out = A p (the operator of
+ * fluid_pp_apply_operator, with air entries of p treated as zero) and
+ * *p_dot_ap = p . A p, accumulated in float64 in a fixed order, asynchronously
+ * on `stream` (a cudaStream_t, NULL = legacy default stream).
+ * Reduction scratch is one fixed device array inside the library (about 128 KB
+ * per GPU, held until the process exits), enough for lattices of up to 16384
+ * work tiles of 32x8x4 cells (e.g. 256^3); larger lattices return
+ * FLUID_PP_INVALID_ARG with the reason in fluid_pp_last_error(NULL).
+ * The first call on each device looks the scratch address up with that device
+ * current; make that first call before any stream capture.  Calls on one device
+ * share the scratch, so calls whose GPU work overlaps race. */
+int fluid_pp_apply_operator_noalloc(int nx, int ny, int nz, const unsigned char* label, const float* diag,
+                                    const float* p, float* out, double* p_dot_ap, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
