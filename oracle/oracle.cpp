@@ -697,8 +697,83 @@ int orc_solve_jacobi(void* h, double relTol, double absTol, int maxIter, double*
   return fail;
 }
 
-// octree-pipelined-pcg.ts:305-594 (direct-curvature PCG, Neumaier dots, true
-// residual acceptance) with the symmetric V-cycle as the fixed SPD preconditioner.
+}  // extern "C"
+
+namespace {
+// The direct-curvature PCG of octree-pipelined-pcg.ts:305-594: Neumaier dots,
+// delta = d.Ad reduced directly every step, stop on the recursive residual and
+// accept only after an independent b - Ax check.  Failure codes: 1 lost
+// positivity/curvature, 2 maximum iterations, 3 true-residual validation.
+template <class ApplyA, class ApplyM>
+int directCurvaturePCG(long N, ApplyA applyA, ApplyM applyM, const double* b, double* x, bool hasGuess,
+                       double relTol, double absTol, int maxIter, double* info, long liquid) {
+  std::vector<double> r(b, b + N), z(N), Az(N), d(N), Ad(N), tr(N);
+  if (hasGuess) {
+    applyA(x, tr.data());
+    for (long i = 0; i < N; ++i) r[i] = b[i] - tr[i];
+  } else {
+    std::fill(x, x + N, 0.0);
+  }
+  const double bnorm = std::sqrt(std::max(0.0, neumaierDot(b, b, N)));
+  const double thr = std::max(absTol, relTol * std::max(bnorm, 1e-300));
+  const double bn = bnorm > 0 ? bnorm : 1.0;
+  applyM(r.data(), z.data());
+  applyA(z.data(), Az.data());
+  double gamma = neumaierDot(r.data(), z.data(), N);
+  double delta = neumaierDot(z.data(), Az.data(), N);
+  double rr = neumaierDot(r.data(), r.data(), N);
+  int reductions = 1, it = 0, fail = 0;
+  double rec = std::sqrt(std::max(0.0, rr));
+  auto trueNorm = [&]() {
+    applyA(x, tr.data());
+    for (long i = 0; i < N; ++i) tr[i] = b[i] - tr[i];
+    return std::sqrt(std::max(0.0, neumaierDot(tr.data(), tr.data(), N)));
+  };
+  if (rec <= thr) {
+    fillInfo(info, 0, 1, rec / bn, rec / bn, bnorm, reductions, 0, liquid);
+    return 0;
+  }
+  if (!(gamma > 0) || !(delta > 0)) {
+    fillInfo(info, 0, 0, rec / bn, rec / bn, bnorm, reductions, 1, liquid);
+    return 1;
+  }
+  double alpha = gamma / delta;
+  d = z;
+  Ad = Az;
+  for (;;) {
+    for (long i = 0; i < N; ++i) { x[i] += alpha * d[i]; r[i] -= alpha * Ad[i]; }
+    ++it;
+    applyM(r.data(), z.data());
+    const double gammaN = neumaierDot(r.data(), z.data(), N);
+    rr = neumaierDot(r.data(), r.data(), N);
+    ++reductions;
+    rec = std::sqrt(std::max(0.0, rr));
+    if (rec <= thr) {
+      const double tn = trueNorm();
+      fail = tn <= thr ? 0 : 3;
+      fillInfo(info, it, fail == 0, rec / bn, tn / bn, bnorm, reductions, fail, liquid);
+      return fail;
+    }
+    if (!(gammaN > 0)) { fail = 1; break; }
+    if (it >= maxIter) { fail = 2; break; }
+    const double beta = gammaN / gamma;
+    for (long i = 0; i < N; ++i) d[i] = z[i] + beta * d[i];
+    applyA(d.data(), Ad.data());
+    delta = neumaierDot(d.data(), Ad.data(), N);
+    ++reductions;
+    if (!(delta > 0)) { fail = 1; break; }
+    alpha = gammaN / delta;
+    gamma = gammaN;
+  }
+  const double tn = trueNorm();
+  fillInfo(info, it, 0, rec / bn, tn / bn, bnorm, reductions, fail, liquid);
+  return fail;
+}
+}  // namespace
+
+extern "C" {
+
+// The symmetric V-cycle as the fixed SPD preconditioner of directCurvaturePCG.
 int orc_solve_mgpcg(void* h, double relTol, double absTol, int maxIter, int pre, int post, double* x,
                     double* info) {
   Ctx& c = *static_cast<Ctx*>(h);
@@ -712,64 +787,30 @@ int orc_solve_mgpcg(void* h, double relTol, double absTol, int maxIter, int pre,
   }
   std::vector<double> b(c.b);
   if (!L.anchored) meanZero(L, b.data());
-  std::vector<double> r(b), z(N), Az(N), d(N), Ad(N);
-  std::fill(x, x + N, 0.0);
-  double bnorm = std::sqrt(std::max(0.0, neumaierDot(b.data(), b.data(), N)));
-  double thr = std::max(absTol, relTol * std::max(bnorm, 1e-300));
-  precondition(c, wk, r.data(), z.data(), pre, post);
-  applyLevel(L, z.data(), Az.data(), 1);
-  double gamma = neumaierDot(r.data(), z.data(), N);
-  double delta = neumaierDot(z.data(), Az.data(), N);
-  double rr = neumaierDot(r.data(), r.data(), N);
-  int reductions = 1, it = 0, fail = 0;
   long liquid = 0;
   for (long i = 0; i < N; ++i) liquid += L.label[i];
-  double rec = std::sqrt(std::max(0.0, rr));
-  if (rec <= thr) {
-    fillInfo(info, 0, 1, bnorm > 0 ? rec / bnorm : 0, bnorm > 0 ? rec / bnorm : 0, bnorm, reductions, 0, liquid);
-    return 0;
-  }
-  if (!(gamma > 0) || !(delta > 0)) {
-    fillInfo(info, 0, 0, 1, 1, bnorm, reductions, 1, liquid);
-    return 1;
-  }
-  double alpha = gamma / delta;
-  d = z;
-  Ad = Az;
-  for (;;) {
-    for (long i = 0; i < N; ++i) { x[i] += alpha * d[i]; r[i] -= alpha * Ad[i]; }
-    ++it;
-    precondition(c, wk, r.data(), z.data(), pre, post);
-    double gammaN = neumaierDot(r.data(), z.data(), N);
-    rr = neumaierDot(r.data(), r.data(), N);
-    ++reductions;
-    rec = std::sqrt(std::max(0.0, rr));
-    if (rec <= thr) {
-      std::vector<double> tr(N);
-      applyLevel(L, x, tr.data(), 1);
-      for (long i = 0; i < N; ++i) tr[i] = b[i] - tr[i];
-      double tn = std::sqrt(std::max(0.0, neumaierDot(tr.data(), tr.data(), N)));
-      fail = tn <= thr ? 0 : 3;
-      fillInfo(info, it, fail == 0, rec / bnorm, tn / bnorm, bnorm, reductions, fail, liquid);
-      return fail;
+  auto A = [&](const double* in, double* out) { applyLevel(L, in, out, 1); };
+  auto M = [&](const double* in, double* out) { precondition(c, wk, in, out, pre, post); };
+  return directCurvaturePCG(N, A, M, b.data(), x, false, relTol, absTol, maxIter, info, liquid);
+}
+
+// Dense-matrix form of the same recurrence for the reference's known-answer
+// systems: A is n x n row major, minv the Jacobi inverse diagonal or NULL
+// (identity preconditioner), x0 an initial guess or NULL.
+int orc_pcg_dense(int n, const double* A, const double* b, const double* minv, const double* x0, int maxIter,
+                  double relTol, double absTol, double* x, double* info) {
+  auto Am = [&](const double* in, double* out) {
+    for (int i = 0; i < n; ++i) {
+      double s = 0;
+      for (int j = 0; j < n; ++j) s += A[long(i) * n + j] * in[j];
+      out[i] = s;
     }
-    if (it >= maxIter || !(gammaN > 0)) break;
-    double beta = gammaN / gamma;
-    for (long i = 0; i < N; ++i) d[i] = z[i] + beta * d[i];
-    applyLevel(L, d.data(), Ad.data(), 1);
-    delta = neumaierDot(d.data(), Ad.data(), N);
-    ++reductions;
-    if (!(delta > 0)) { fail = 1; break; }
-    alpha = gammaN / delta;
-    gamma = gammaN;
-  }
-  std::vector<double> tr(N);
-  applyLevel(L, x, tr.data(), 1);
-  for (long i = 0; i < N; ++i) tr[i] = b[i] - tr[i];
-  double tn = std::sqrt(std::max(0.0, neumaierDot(tr.data(), tr.data(), N)));
-  if (!fail) fail = 2;
-  fillInfo(info, it, 0, rec / bnorm, tn / bnorm, bnorm, reductions, fail, liquid);
-  return fail;
+  };
+  auto M = [&](const double* in, double* out) {
+    for (int i = 0; i < n; ++i) out[i] = minv ? minv[i] * in[i] : in[i];
+  };
+  if (x0) std::copy(x0, x0 + n, x);
+  return directCurvaturePCG(n, Am, M, b, x, x0 != nullptr, relTol, absTol, maxIter, info, n);
 }
 
 // Gradient subtract (atlas pressureCorrection + projectedFaceVelocity, and the

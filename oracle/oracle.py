@@ -52,6 +52,8 @@ def lib():
         L.orc_solve_mgpcg.argtypes = [vp, c_double, c_double, c_int, c_int, c_int, vp, vp]
         L.orc_solve_mgpcg.restype = c_int
         L.orc_grad_subtract.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.orc_pcg_dense.argtypes = [c_int, vp, vp, vp, vp, c_int, c_double, c_double, vp, vp]
+        L.orc_pcg_dense.restype = c_int
         _lib = L
     return _lib
 
@@ -78,6 +80,23 @@ def plan_hierarchy(nx: int, ny: int, nz: int) -> dict:
 
 INFO_KEYS = ("iterations", "converged", "recursive_rel_residual", "true_rel_residual", "b_norm",
              "reductions", "failure", "liquid_cells")
+FAILURES = {0: None, 1: "non-positive-direction-curvature", 2: "maximum-iterations", 3: "true-residual-validation"}
+
+
+def pcg_dense(A, b, minv=None, x0=None, max_iter=None, rel_tol=1e-10, abs_tol=0.0):
+    """The C++ oracle's direct-curvature PCG on a dense system (known-answer checks)."""
+    A = np.ascontiguousarray(A, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    n = b.size
+    mv = None if minv is None else np.ascontiguousarray(minv, np.float64)
+    g = None if x0 is None else np.ascontiguousarray(x0, np.float64)
+    x = np.zeros(n, np.float64)
+    info = np.zeros(8, np.float64)
+    rc = lib().orc_pcg_dense(n, _p(A), _p(b), _p(mv), _p(g), int(n if max_iter is None else max_iter),
+                             rel_tol, abs_tol, _p(x), _p(info))
+    d = dict(zip(INFO_KEYS, info.tolist()))
+    d["failure_name"] = FAILURES.get(rc, str(rc))
+    return x, d
 
 
 class Oracle:
