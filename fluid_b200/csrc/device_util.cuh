@@ -17,27 +17,29 @@ struct Tile {
   int pad;
 };
 
-constexpr int kTX = 32, kTY = 8, kTZ = 4;   // tile extent; kTX * kTY == kThreads
+constexpr int kTX = 32, kTY = 8;   // tile extent in x and y; kTX * kTY == kThreads
+constexpr int kMaxDepth = 4;       // cells per thread along z: 1, 2 or 4 per level
 constexpr int kBlockThreads = 1024;        // coarse-block CTA
 
-__host__ __device__ inline int tiles_of(int nx, int ny, int nz) {
-  return ((nx + kTX - 1) / kTX) * ((ny + kTY - 1) / kTY) * ((nz + kTZ - 1) / kTZ);
+__host__ __device__ inline int tiles_of(int nx, int ny, int nz, int depth) {
+  return ((nx + kTX - 1) / kTX) * ((ny + kTY - 1) / kTY) * ((nz + depth - 1) / depth);
 }
 
-// The cells of tile t owned by this thread.
+// The cells of tile t owned by this thread: column (x, y), cells z0 .. z0+depth-1.
 struct TileIt {
-  int x, y, z0, k, nx, ny, nz;
+  int x, y, z0, k, nx, ny, nz, depth;
   bool ok;
-  __device__ __forceinline__ TileIt(int t, int nx_, int ny_, int nz_) : k(0), nx(nx_), ny(ny_), nz(nz_) {
+  __device__ __forceinline__ TileIt(int t, int nx_, int ny_, int nz_, int depth_)
+      : k(0), nx(nx_), ny(ny_), nz(nz_), depth(depth_) {
     const int ntx = (nx + kTX - 1) / kTX, nty = (ny + kTY - 1) / kTY;
     const int tx = t % ntx, r = t / ntx, ty = r % nty, tz = r / nty;
     x = tx * kTX + int(threadIdx.x & (kTX - 1));
     y = ty * kTY + int(threadIdx.x / kTX);
-    z0 = tz * kTZ;
+    z0 = tz * depth;
     ok = x < nx && y < ny;
   }
   __device__ __forceinline__ bool next(int& cx, int& cy, int& cz, int& i) {
-    if (!ok || k >= kTZ) return false;
+    if (!ok || k >= depth) return false;
     const int z = z0 + k++;
     if (z >= nz) return false;
     cx = x;
@@ -74,6 +76,18 @@ struct St<__nv_bfloat16> {
     static_cast<__nv_bfloat16*>(p)[i] = __float2bfloat16_rn(v);
   }
 };
+
+__device__ __forceinline__ float tof(float v) { return v; }
+__device__ __forceinline__ float tof(__half v) { return __half2float(v); }
+__device__ __forceinline__ float tof(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <class T>
+__device__ __forceinline__ T fromf(float v);
+template <>
+__device__ __forceinline__ float fromf<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ __half fromf<__half>(float v) { return __float2half_rn(v); }
+template <>
+__device__ __forceinline__ __nv_bfloat16 fromf<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
 
 __device__ __forceinline__ void decode(int i, int nx, int ny, int& x, int& y, int& z) {
   const int yz = i / nx;
@@ -137,11 +151,28 @@ __device__ __forceinline__ bool arrive_last(unsigned* counter, int total, int* f
   return *flag != 0;
 }
 
-// Sum (op 0) or max (op 1) of one slot over all tiles, in tile order.
+// Sum (op 0) or max (op 1) of one slot over all tiles.  Thread j owns tiles
+// j, j + blockDim, ... and folds them in four interleaved accumulators (a fixed
+// order), then the block folds the threads: deterministic for a given tile
+// count.  Loads bypass L1 (__ldcg): the partials were written by other CTAs
+// before the arrival counter released them.
 __device__ __forceinline__ double gather_slot(const double* partial, int slot, int ntiles, int op, double* sh) {
-  const volatile double* p = partial + (long long)slot * ntiles;
-  double acc = 0;
-  for (int t = threadIdx.x; t < ntiles; t += blockDim.x) acc = op ? fmax(acc, p[t]) : acc + p[t];
+  const double* p = partial + (long long)slot * ntiles;
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
+  const int stride = blockDim.x;
+  int t = threadIdx.x;
+  for (; t + 3 * stride < ntiles; t += 4 * stride) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double v = __ldcg(p + t + u * stride);
+      a[u] = op ? fmax(a[u], v) : a[u] + v;
+    }
+  }
+  for (int u = 0; t < ntiles; t += stride, ++u) {
+    const double v = __ldcg(p + t);
+    a[u & 3] = op ? fmax(a[u & 3], v) : a[u & 3] + v;
+  }
+  const double acc = op ? fmax(fmax(a[0], a[1]), fmax(a[2], a[3])) : (a[0] + a[1]) + (a[2] + a[3]);
   return op ? block_max(acc, sh) : block_sum(acc, sh);
 }
 

@@ -24,7 +24,7 @@ __global__ void k_label_rhs(const InstDev* insts, const Tile* tiles, int ntiles,
     int liquid = 0, air = 0, top = 0, bad = 0;
     const long long uS = I.nx + 1, vS = I.ny + 1;
     int x, y, z, i;
-    for (TileIt it(tl.tile, I.nx, I.ny, I.nz); it.next(x, y, z, i);) {
+    for (TileIt it(tl.tile, I.nx, I.ny, I.nz, L.depth); it.next(x, y, z, i);) {
       const float rho = I.vof[i];
       const bool liq = rho > 0.5f;
       L.label[i] = liq ? 1 : 0;
@@ -83,7 +83,7 @@ __global__ void k_coarsen_phi(const InstDev* insts, const Tile* tiles, int ntile
     const LevelDev& C = I.lv[tl.level];
     const LevelDev& F = I.lv[tl.level - 1];
     int x, y, z, i;
-    for (TileIt it(tl.tile, C.nx, C.ny, C.nz); it.next(x, y, z, i);) {
+    for (TileIt it(tl.tile, C.nx, C.ny, C.nz, C.depth); it.next(x, y, z, i);) {
       float ph[8], ps[8], pf[8], nf[8];
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
@@ -124,7 +124,7 @@ __global__ void k_bake_diag(const InstDev* insts, const Tile* tiles, int ntiles)
     const float wx = L.wx * L.wmax, wy = L.wy * L.wmax, wz = L.wz * L.wmax;
     const int sy = L.nx, sz = L.nx * L.ny;
     int x, y, z, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz); it.next(x, y, z, i);) {
+    for (TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth); it.next(x, y, z, i);) {
       float d = 0.0f;
       if (L.label[i]) {
         const float ph = L.phi[i];
@@ -235,7 +235,7 @@ __global__ void k_cg_init(const InstDev* insts, const Tile* tiles, int ntiles, d
     double sbb = 0, sb = 0, srr = 0, mb = 0, mr = 0;
     const int sy = L.nx, sz = L.nx * L.ny;
     int x, y, z, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz); it.next(x, y, z, i);) {
+    for (TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth); it.next(x, y, z, i);) {
       const float b = I.b[i];
       float rv = b;
       if (warm && L.label[i]) {
@@ -314,7 +314,7 @@ __global__ void k_project_init(const InstDev* insts, const Tile* tiles, int ntil
     float* r = static_cast<float*>(L.rhs);
     const float m = float(c->bmean);
     int x, y, z, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz); it.next(x, y, z, i);) {
+    for (TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth); it.next(x, y, z, i);) {
       if (!L.label[i]) continue;
       I.b[i] -= m;
       r[i] -= m;
@@ -323,59 +323,98 @@ __global__ void k_project_init(const InstDev* insts, const Tile* tiles, int ntil
 }
 
 // ================================================================= V-cycle
+// The grid kernels below are written in two phases: every load of a thread's
+// column of kTZ cells is issued first (descriptor fields are copied to
+// registers up front), stores follow, so a launch costs about one memory round
+// trip per dependency level instead of one per cell.
+
 // One colour pass of red-black Gauss-Seidel on the normalised level operator
 // (mgSmoothColour, mg.wgsl.ts:325-344, without the p_min projection).  With
 // zero_init the pass starts from z = 0 and also clears the other colour.
 template <class TZ, class TR, class TD>
-__global__ void k_smooth(const InstDev* insts, const Tile* tiles, int ntiles, int level, int colour, int zero_init) {
+__global__ void __launch_bounds__(kThreads) k_smooth(const InstDev* insts, const Tile* tiles, int ntiles, int level,
+                                                     int colour, int zero_init) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
-    if (I.ctrl->done) continue;
-    const LevelDev& L = I.lv[level];
+    const int done = I.ctrl->done;
+    const LevelDev L = I.lv[level];
+    const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
+    if (done || !it.ok) continue;
+    const TZ* z = static_cast<const TZ*>(L.z);
+    TZ* zo = static_cast<TZ*>(L.z);
+    const TR* __restrict__ rhs = static_cast<const TR*>(L.rhs);
+    const TD* __restrict__ dg = static_cast<const TD*>(L.diagT);
+    const uint8_t* __restrict__ lab = L.label;
     const int sy = L.nx, sz = L.nx * L.ny;
-    int x, y, z, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz); it.next(x, y, z, i);) {
-      if (((x + y + z) & 1) != colour) {
-        if (zero_init) St<TZ>::st(L.z, i, 0.0f);
-        continue;
+    const int x = it.x, y = it.y;
+    const int i0 = x + L.nx * (y + L.ny * it.z0);
+    float val[kMaxDepth];
+    bool wr[kMaxDepth];
+#pragma unroll
+    for (int k = 0; k < kMaxDepth; ++k) {
+      if (k >= it.depth) break;
+      const int zz = it.z0 + k, i = i0 + k * sz;
+      wr[k] = false;
+      val[k] = 0.0f;
+      if (zz < L.nz) {
+        if (((x + y + zz) & 1) == colour) {
+          float s = 0.0f;
+          if (!zero_init) {
+            const float xm = x > 0 ? L.wx * tof(z[i - 1]) : 0.0f, xp = x + 1 < L.nx ? L.wx * tof(z[i + 1]) : 0.0f;
+            const float ym = y > 0 ? L.wy * tof(z[i - sy]) : 0.0f, yp = y + 1 < L.ny ? L.wy * tof(z[i + sy]) : 0.0f;
+            const float zm = zz > 0 ? L.wz * tof(z[i - sz]) : 0.0f, zp = zz + 1 < L.nz ? L.wz * tof(z[i + sz]) : 0.0f;
+            s = d4sum6(xm, xp, ym, yp, zm, zp);
+          }
+          val[k] = lab[i] ? (tof(rhs[i]) + s) / tof(dg[i]) : 0.0f;
+          wr[k] = true;
+        } else if (zero_init) {
+          wr[k] = true;
+        }
       }
-      if (!L.label[i]) {
-        St<TZ>::st(L.z, i, 0.0f);
-        continue;
-      }
-      float s = 0.0f;
-      if (!zero_init) {
-        auto nb = [&](bool in, int j, float w) { return in ? w * St<TZ>::ld(L.z, j) : 0.0f; };
-        s = d4sum6(nb(x > 0, i - 1, L.wx), nb(x + 1 < L.nx, i + 1, L.wx), nb(y > 0, i - sy, L.wy),
-                   nb(y + 1 < L.ny, i + sy, L.wy), nb(z > 0, i - sz, L.wz), nb(z + 1 < L.nz, i + sz, L.wz));
-      }
-      St<TZ>::st(L.z, i, (St<TR>::ld(L.rhs, i) + s) / St<TD>::ld(L.diagT, i));
     }
+#pragma unroll
+    for (int k = 0; k < kMaxDepth; ++k)
+      if (k < it.depth && wr[k]) zo[i0 + k * sz] = fromf<TZ>(val[k]);
   }
 }
 
 // res = scale * (rhs - A z) on liquid cells (mgResidual, mg.wgsl.ts:197-205).
 // On level 0 the residual is scaled by sigma so half-precision levels stay in range.
 template <class TZ, class TR, class TD, class TS>
-__global__ void k_residual(const InstDev* insts, const Tile* tiles, int ntiles, int level) {
+__global__ void __launch_bounds__(kThreads) k_residual(const InstDev* insts, const Tile* tiles, int ntiles,
+                                                       int level) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
-    if (I.ctrl->done) continue;
-    const LevelDev& L = I.lv[level];
-    const float scale = level == 0 ? float(I.ctrl->sigma) : 1.0f;
+    const int done = I.ctrl->done;
+    const double sigma = I.ctrl->sigma;
+    const LevelDev L = I.lv[level];
+    const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
+    if (done || !it.ok) continue;
+    const float scale = level == 0 ? float(sigma) : 1.0f;
+    const TZ* __restrict__ z = static_cast<const TZ*>(L.z);
+    const TR* __restrict__ rhs = static_cast<const TR*>(L.rhs);
+    const TD* __restrict__ dg = static_cast<const TD*>(L.diagT);
+    const uint8_t* __restrict__ lab = L.label;
+    TS* __restrict__ res = static_cast<TS*>(L.res);
     const int sy = L.nx, sz = L.nx * L.ny;
-    int x, y, z, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz); it.next(x, y, z, i);) {
+    const int x = it.x, y = it.y;
+    const int i0 = x + L.nx * (y + L.ny * it.z0);
+#pragma unroll
+    for (int k = 0; k < kMaxDepth; ++k) {
+      if (k >= it.depth) break;
+      const int zz = it.z0 + k, i = i0 + k * sz;
+      if (zz >= L.nz) continue;
       float r = 0.0f;
-      if (L.label[i]) {
-        auto nb = [&](bool in, int j, float w) { return in ? w * St<TZ>::ld(L.z, j) : 0.0f; };
-        const float s = d4sum6(nb(x > 0, i - 1, L.wx), nb(x + 1 < L.nx, i + 1, L.wx), nb(y > 0, i - sy, L.wy),
-                               nb(y + 1 < L.ny, i + sy, L.wy), nb(z > 0, i - sz, L.wz), nb(z + 1 < L.nz, i + sz, L.wz));
-        r = scale * (St<TR>::ld(L.rhs, i) - (St<TD>::ld(L.diagT, i) * St<TZ>::ld(L.z, i) - s));
+      if (lab[i]) {
+        const float xm = x > 0 ? L.wx * tof(z[i - 1]) : 0.0f, xp = x + 1 < L.nx ? L.wx * tof(z[i + 1]) : 0.0f;
+        const float ym = y > 0 ? L.wy * tof(z[i - sy]) : 0.0f, yp = y + 1 < L.ny ? L.wy * tof(z[i + sy]) : 0.0f;
+        const float zm = zz > 0 ? L.wz * tof(z[i - sz]) : 0.0f, zp = zz + 1 < L.nz ? L.wz * tof(z[i + sz]) : 0.0f;
+        const float s = d4sum6(xm, xp, ym, yp, zm, zp);
+        r = scale * (tof(rhs[i]) - (tof(dg[i]) * tof(z[i]) - s));
       }
-      St<TS>::st(L.res, i, r);
+      res[i] = fromf<TS>(r);
     }
   }
 }
@@ -383,80 +422,211 @@ __global__ void k_residual(const InstDev* insts, const Tile* tiles, int ntiles, 
 // rhs_{l+1} = to_coarse * P^T res_l / 2^k (the transpose of the prolongation, so
 // the V-cycle is a symmetric preconditioner); coarse air cells get zero.
 template <class TS>
-__global__ void k_restrict(const InstDev* insts, const Tile* tiles, int ntiles, int level) {
+__global__ void __launch_bounds__(kThreads) k_restrict(const InstDev* insts, const Tile* tiles, int ntiles,
+                                                       int level) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
-    if (I.ctrl->done) continue;
-    const LevelDev& F = I.lv[level];
-    const LevelDev& C = I.lv[level + 1];
+    const int done = I.ctrl->done;
+    const LevelDev F = I.lv[level];
+    const LevelDev C = I.lv[level + 1];
+    const TileIt it(tl.tile, C.nx, C.ny, C.nz, C.depth);
+    if (done || !it.ok) continue;
+    const TS* __restrict__ res = static_cast<const TS*>(F.res);
+    TS* __restrict__ out = static_cast<TS*>(C.rhs);
     const float scale = F.to_coarse / float((C.sx == 2 ? 2 : 1) * (C.sy == 2 ? 2 : 1) * (C.sz == 2 ? 2 : 1));
-    int X, Y, Z, i;
-    for (TileIt it(tl.tile, C.nx, C.ny, C.nz); it.next(X, Y, Z, i);) {
+    // x and y stencils are the same for the whole column
+    const int X = it.x, Y = it.y;
+    int fx[4], fy[4];
+    float wx[4], wy[4];
+    int nxx = 0, nyy = 0;
+    if (C.sx == 2) {
+      for (int q = 2 * X - 1; q <= 2 * X + 2; ++q)
+        if (q >= 0 && q < F.nx) { fx[nxx] = q; wx[nxx] = p1d(q, X, C.nx); ++nxx; }
+    } else { fx[0] = X; wx[0] = 1.0f; nxx = 1; }
+    if (C.sy == 2) {
+      for (int q = 2 * Y - 1; q <= 2 * Y + 2; ++q)
+        if (q >= 0 && q < F.ny) { fy[nyy] = q; wy[nyy] = p1d(q, Y, C.ny); ++nyy; }
+    } else { fy[0] = Y; wy[0] = 1.0f; nyy = 1; }
+    const int csz = C.nx * C.ny;
+    const int ci0 = X + C.nx * (Y + C.ny * it.z0);
+    for (int k = 0; k < it.depth; ++k) {
+      const int Z = it.z0 + k;
+      if (Z >= C.nz) break;
+      const int i = ci0 + k * csz;
       float acc = 0.0f;
       if (C.label[i]) {
-        int fx[4], fy[4], fz[4];
-        float wx[4], wy[4], wz[4];
-        int nxx = 0, nyy = 0, nzz = 0;
-        auto axis = [](int stride, int c, int nc, int nf, int* f, float* w) {
-          if (stride == 1) {
-            f[0] = c;
-            w[0] = 1.0f;
-            return 1;
-          }
-          int n = 0;
-          for (int q = 2 * c - 1; q <= 2 * c + 2; ++q)
-            if (q >= 0 && q < nf) {
-              f[n] = q;
-              w[n] = p1d(q, c, nc);
-              ++n;
-            }
-          return n;
-        };
-        nxx = axis(C.sx, X, C.nx, F.nx, fx, wx);
-        nyy = axis(C.sy, Y, C.ny, F.ny, fy, wy);
-        nzz = axis(C.sz, Z, C.nz, F.nz, fz, wz);
+        int fz[4];
+        float wz[4];
+        int nzz = 0;
+        if (C.sz == 2) {
+          for (int q = 2 * Z - 1; q <= 2 * Z + 2; ++q)
+            if (q >= 0 && q < F.nz) { fz[nzz] = q; wz[nzz] = p1d(q, Z, C.nz); ++nzz; }
+        } else { fz[0] = Z; wz[0] = 1.0f; nzz = 1; }
         for (int c2 = 0; c2 < nzz; ++c2) {
           for (int c1 = 0; c1 < nyy; ++c1) {
-            const float wyz = wz[c2] * wy[c1];
             const int row = F.nx * (fy[c1] + F.ny * fz[c2]);
             float s = 0.0f;
-            for (int c0 = 0; c0 < nxx; ++c0) s += wx[c0] * St<TS>::ld(F.res, row + fx[c0]);
-            acc += wyz * s;
+#pragma unroll 4
+            for (int c0 = 0; c0 < nxx; ++c0) s += wx[c0] * tof(res[row + fx[c0]]);
+            acc += wz[c2] * wy[c1] * s;
           }
         }
         acc *= scale;
       }
-      St<TS>::st(C.rhs, i, acc);
+      out[i] = fromf<TS>(acc);
     }
+  }
+}
+
+// Residual and restriction fused, one CTA per coarse tile of kRX x kRY x kRZ
+// cells.  The CTA computes the fine residual scale * (rhs - A z) of its fine
+// footprint (the tile's children plus a one-cell halo on coarsened axes) into
+// shared memory, then applies R = P^T / 2^k separably: a 4-tap x pass, a y pass
+// and a z pass.  Same operator as k_residual + k_restrict (summation order of
+// the taps differs), without the residual's round trip through memory.
+constexpr int kRX = 16, kRY = 4, kRZ = 4;
+constexpr int kRFX = 2 * kRX + 2, kRFY = 2 * kRY + 2, kRFZ = 2 * kRZ + 2;
+
+__host__ __device__ inline int rtiles_of(int nx, int ny, int nz) {
+  return ((nx + kRX - 1) / kRX) * ((ny + kRY - 1) / kRY) * ((nz + kRZ - 1) / kRZ);
+}
+
+// Fine index range [f0, f0 + fn) feeding coarse cells [c0, c0 + cn) along one axis.
+__device__ __forceinline__ void fine_span(int stride, int c0, int cn, int nf, int& f0, int& fn) {
+  if (stride == 1) {
+    f0 = c0;
+    fn = cn;
+    return;
+  }
+  const int lo = max(2 * c0 - 1, 0), hi = min(2 * (c0 + cn) + 1, nf);
+  f0 = lo;
+  fn = hi - lo;
+}
+
+// 4-tap restriction along one axis from a shared-memory line: coarse index c,
+// fine values v[(f - f0) * step].
+__device__ __forceinline__ float rline(int stride, int c, int nc, int nf, int f0, const float* v, int step) {
+  if (stride == 1) return v[(c - f0) * step];
+  float s = 0.0f;
+#pragma unroll
+  for (int d = -1; d <= 2; ++d) {
+    const int f = 2 * c + d;
+    if (f >= 0 && f < nf) s += p1d(f, c, nc) * v[(f - f0) * step];
+  }
+  return s;
+}
+
+template <class TZ, class TR, class TD, class TS>
+__global__ void __launch_bounds__(kThreads) k_residual_restrict(const InstDev* insts, const Tile* tiles, int ntiles,
+                                                                int level) {
+  __shared__ float res_s[kRFZ * kRFY * kRFX];
+  __shared__ float xs[kRFZ * kRFY * kRX];
+  __shared__ float ys[kRFZ * kRY * kRX];
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    const InstDev& I = insts[tl.inst];
+    const int done = I.ctrl->done;
+    const double sigma = I.ctrl->sigma;
+    const LevelDev F = I.lv[level];
+    const LevelDev C = I.lv[level + 1];
+    if (done) continue;   // uniform per CTA
+    const float scale = level == 0 ? float(sigma) : 1.0f;
+    const int ntx = (C.nx + kRX - 1) / kRX, nty = (C.ny + kRY - 1) / kRY;
+    const int tx = tl.tile % ntx, tr = tl.tile / ntx, ty = tr % nty, tz = tr / nty;
+    const int cx0 = tx * kRX, cy0 = ty * kRY, cz0 = tz * kRZ;
+    const int cnx = min(kRX, C.nx - cx0), cny = min(kRY, C.ny - cy0), cnz = min(kRZ, C.nz - cz0);
+    int fx0, fnx, fy0, fny, fz0, fnz;
+    fine_span(C.sx, cx0, cnx, F.nx, fx0, fnx);
+    fine_span(C.sy, cy0, cny, F.ny, fy0, fny);
+    fine_span(C.sz, cz0, cnz, F.nz, fz0, fnz);
+    const TZ* __restrict__ z = static_cast<const TZ*>(F.z);
+    const TR* __restrict__ rhs = static_cast<const TR*>(F.rhs);
+    const TD* __restrict__ dg = static_cast<const TD*>(F.diagT);
+    const uint8_t* __restrict__ lab = F.label;
+    const int sy = F.nx, sz = F.nx * F.ny;
+    // fine residual of the footprint
+    const int fcount = fnx * fny * fnz;
+    for (int e = threadIdx.x; e < fcount; e += blockDim.x) {
+      const int lx = e % fnx, lr = e / fnx, ly = lr % fny, lz = lr / fny;
+      const int x = fx0 + lx, y = fy0 + ly, zz = fz0 + lz;
+      const int i = x + F.nx * (y + F.ny * zz);
+      float r = 0.0f;
+      if (lab[i]) {
+        const float xm = x > 0 ? F.wx * tof(z[i - 1]) : 0.0f, xp = x + 1 < F.nx ? F.wx * tof(z[i + 1]) : 0.0f;
+        const float ym = y > 0 ? F.wy * tof(z[i - sy]) : 0.0f, yp = y + 1 < F.ny ? F.wy * tof(z[i + sy]) : 0.0f;
+        const float zm = zz > 0 ? F.wz * tof(z[i - sz]) : 0.0f, zp = zz + 1 < F.nz ? F.wz * tof(z[i + sz]) : 0.0f;
+        r = scale * (tof(rhs[i]) - (tof(dg[i]) * tof(z[i]) - d4sum6(xm, xp, ym, yp, zm, zp)));
+      }
+      res_s[(lz * kRFY + ly) * kRFX + lx] = r;
+    }
+    __syncthreads();
+    // x pass: (fine z, fine y, coarse x)
+    for (int e = threadIdx.x; e < fnz * fny * cnx; e += blockDim.x) {
+      const int cx = e % cnx, lr = e / cnx, ly = lr % fny, lz = lr / fny;
+      xs[(lz * kRFY + ly) * kRX + cx] = rline(C.sx, cx0 + cx, C.nx, F.nx, fx0, &res_s[(lz * kRFY + ly) * kRFX], 1);
+    }
+    __syncthreads();
+    // y pass: (fine z, coarse y, coarse x)
+    for (int e = threadIdx.x; e < fnz * cny * cnx; e += blockDim.x) {
+      const int cx = e % cnx, lr = e / cnx, cy = lr % cny, lz = lr / cny;
+      ys[(lz * kRY + cy) * kRX + cx] = rline(C.sy, cy0 + cy, C.ny, F.ny, fy0, &xs[lz * kRFY * kRX + cx], kRX);
+    }
+    __syncthreads();
+    // z pass and store
+    const float out_scale = F.to_coarse / float((C.sx == 2 ? 2 : 1) * (C.sy == 2 ? 2 : 1) * (C.sz == 2 ? 2 : 1));
+    TS* __restrict__ out = static_cast<TS*>(C.rhs);
+    for (int e = threadIdx.x; e < cnz * cny * cnx; e += blockDim.x) {
+      const int cx = e % cnx, lr = e / cnx, cy = lr % cny, cz = lr / cny;
+      const int X = cx0 + cx, Y = cy0 + cy, Z = cz0 + cz;
+      const int ci = X + C.nx * (Y + C.ny * Z);
+      float acc = 0.0f;
+      if (C.label[ci]) acc = out_scale * rline(C.sz, Z, C.nz, F.nz, fz0, &ys[cy * kRX + cx], kRY * kRX);
+      out[ci] = fromf<TS>(acc);
+    }
+    __syncthreads();   // shared buffers are reused by the next tile of this CTA
   }
 }
 
 // z_l += P z_{l+1} on liquid cells (mgProlongateAdd, mg.wgsl.ts:243-246);
 // from level 1 into level 0 the sigma scaling is undone.
 template <class TZF, class TZC>
-__global__ void k_prolong(const InstDev* insts, const Tile* tiles, int ntiles, int level) {
+__global__ void __launch_bounds__(kThreads) k_prolong(const InstDev* insts, const Tile* tiles, int ntiles,
+                                                      int level) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
-    if (I.ctrl->done) continue;
-    const LevelDev& F = I.lv[level];
-    const LevelDev& C = I.lv[level + 1];
-    const float unscale = level == 0 ? float(1.0 / I.ctrl->sigma) : 1.0f;
-    int x, y, z, i;
-    for (TileIt it(tl.tile, F.nx, F.ny, F.nz); it.next(x, y, z, i);) {
-      if (!F.label[i]) continue;
-      int cx[2], cy[2], cz[2];
-      float wx[2], wy[2], wz[2];
-      const int nxx = taps1d(x, C.sx, C.nx, cx, wx);
-      const int nyy = taps1d(y, C.sy, C.ny, cy, wy);
-      const int nzz = taps1d(z, C.sz, C.nz, cz, wz);
+    const int done = I.ctrl->done;
+    const double sigma = I.ctrl->sigma;
+    const LevelDev F = I.lv[level];
+    const LevelDev C = I.lv[level + 1];
+    const TileIt it(tl.tile, F.nx, F.ny, F.nz, F.depth);
+    if (done || !it.ok) continue;
+    const float unscale = level == 0 ? float(1.0 / sigma) : 1.0f;
+    const TZC* __restrict__ zc = static_cast<const TZC*>(C.z);
+    TZF* __restrict__ zf = static_cast<TZF*>(F.z);
+    const uint8_t* __restrict__ lab = F.label;
+    int cx[2], cy[2];
+    float wx[2], wy[2];
+    const int nxx = taps1d(it.x, C.sx, C.nx, cx, wx);
+    const int nyy = taps1d(it.y, C.sy, C.ny, cy, wy);
+    const int sz = F.nx * F.ny;
+    const int i0 = it.x + F.nx * (it.y + F.ny * it.z0);
+#pragma unroll
+    for (int k = 0; k < kMaxDepth; ++k) {
+      if (k >= it.depth) break;
+      const int zz = it.z0 + k, i = i0 + k * sz;
+      if (zz >= F.nz || !lab[i]) continue;
+      int cz[2];
+      float wz[2];
+      const int nzz = taps1d(zz, C.sz, C.nz, cz, wz);
       float s = 0.0f;
       for (int c2 = 0; c2 < nzz; ++c2)
-        for (int c1 = 0; c1 < nyy; ++c1)
-          for (int c0 = 0; c0 < nxx; ++c0)
-            s += wx[c0] * wy[c1] * wz[c2] * St<TZC>::ld(C.z, cx[c0] + C.nx * (cy[c1] + C.ny * cz[c2]));
-      St<TZF>::st(F.z, i, St<TZF>::ld(F.z, i) + s * unscale);
+        for (int c1 = 0; c1 < nyy; ++c1) {
+          const int row = C.nx * (cy[c1] + C.ny * cz[c2]);
+          for (int c0 = 0; c0 < nxx; ++c0) s += wx[c0] * wy[c1] * wz[c2] * tof(zc[row + cx[c0]]);
+        }
+      zf[i] = fromf<TZF>(tof(zf[i]) + s * unscale);
     }
   }
 }
@@ -464,143 +634,186 @@ __global__ void k_prolong(const InstDev* insts, const Tile* tiles, int ntiles, i
 // The small levels of the V-cycle in one CTA per instance, in shared memory:
 // levels first..nlev-1 (each at most kCoarseBlockCells) are loaded, smoothed,
 // restricted, solved densely at the coarsest, prolongated and smoothed again
-// with the same arithmetic as the grid kernels, then z of level `first` is
-// written back for the prolongation into the finer grid level.
+// with the same operators as the grid kernels, then z of level `first` is
+// written back for the prolongation into the finer grid level.  Each level
+// keeps packed cell coordinates, a red-then-black cell order (a colour pass
+// touches only its own cells) and the reciprocal diagonal, so a pass is a few
+// shared-memory loads and FMAs per cell.
+struct BlockLevel {
+  int nx, ny, nz, n, nred, sx, sy, sz;
+  float wx, wy, wz, to_coarse;
+  float* z;
+  float* rhs;
+  float* res;
+  float* diag;
+  float* inv;
+  unsigned* xyz;       // x | y << 10 | z << 20
+  unsigned short* ord; // red cells first, then black
+  uint8_t* lab;
+};
+
+__host__ __device__ inline long long block_level_bytes(long long n) {
+  return 20 * n + 4 * n + 2 * ((n + 1) & ~1LL) + ((n + 3) & ~3LL);
+}
+
+// Red cells ((x + y + z) even) among the row-major predecessors of (x, y, z)
+// in an nx * ny * nz box: a run of len cells starting on parity p holds
+// (len + 1 - p) / 2 red cells, and consecutive rows and planes alternate their
+// starting parity.
+__device__ __forceinline__ int red_runs(int k, int len, int p0) {
+  const int even = p0 ? k / 2 : (k + 1) / 2;   // runs that start red
+  return even * ((len + 1) / 2) + (k - even) * (len / 2);
+}
+__device__ __forceinline__ int red_before(int x, int y, int z, int nx, int ny) {
+  return red_runs(z, nx * ny, 0) + red_runs(y, nx, z & 1) + red_runs(1, x, (y + z) & 1);
+}
+
 template <class T>
-__global__ void k_coarse_block(const InstDev* insts, const int* list, int pre, int post) {
+__global__ void __launch_bounds__(kBlockThreads) k_coarse_block(const InstDev* insts, const int* list, int pre,
+                                                                int post) {
   extern __shared__ float smem[];
+  __shared__ BlockLevel B[kMaxLevels];
+  __shared__ int s_first, s_last, s_done;
   const InstDev& I = insts[list[blockIdx.x]];
-  if (I.ctrl->done) return;
-  const int first = I.first_block, last = I.nlev - 1;
-  float* zs[kMaxLevels];
-  float* rs[kMaxLevels];
-  float* es[kMaxLevels];
-  float* ds[kMaxLevels];
-  uint8_t* ls[kMaxLevels];
-  {
-    float* p = smem;
-    for (int l = first; l <= last; ++l) {
-      const int n = int(I.lv[l].n);
-      zs[l] = p; p += n;
-      rs[l] = p; p += n;
-      es[l] = p; p += n;
-      ds[l] = p; p += n;
-    }
-    uint8_t* q = reinterpret_cast<uint8_t*>(p);
-    for (int l = first; l <= last; ++l) {
-      ls[l] = q;
-      q += (I.lv[l].n + 3) & ~3LL;
-    }
-  }
-  for (int l = first; l <= last; ++l) {
-    const LevelDev& L = I.lv[l];
-    for (int i = threadIdx.x; i < int(L.n); i += blockDim.x) {
-      ds[l][i] = St<T>::ld(L.diagT, i);
-      ls[l][i] = L.label[i];
-      if (l == first) rs[l][i] = St<T>::ld(L.rhs, i);
+  if (threadIdx.x == 0) {
+    s_done = I.ctrl->done;
+    s_first = I.first_block;
+    s_last = I.nlev - 1;
+    char* p = reinterpret_cast<char*>(smem);
+    for (int l = s_first; l <= s_last; ++l) {
+      const LevelDev& L = I.lv[l];
+      BlockLevel& b = B[l];
+      b.nx = L.nx; b.ny = L.ny; b.nz = L.nz; b.n = int(L.n);
+      b.sx = L.sx; b.sy = L.sy; b.sz = L.sz;
+      b.wx = L.wx; b.wy = L.wy; b.wz = L.wz; b.to_coarse = L.to_coarse;
+      b.z = reinterpret_cast<float*>(p); p += 4 * b.n;
+      b.rhs = reinterpret_cast<float*>(p); p += 4 * b.n;
+      b.res = reinterpret_cast<float*>(p); p += 4 * b.n;
+      b.diag = reinterpret_cast<float*>(p); p += 4 * b.n;
+      b.inv = reinterpret_cast<float*>(p); p += 4 * b.n;
+      b.xyz = reinterpret_cast<unsigned*>(p); p += 4 * b.n;
+      b.ord = reinterpret_cast<unsigned short*>(p); p += 2 * ((b.n + 1) & ~1);
+      b.lab = reinterpret_cast<uint8_t*>(p); p += (b.n + 3) & ~3;
+      // red cells of a box: ceil(n / 2) when the corner cell is red
+      b.nred = (b.n + 1) / 2;
     }
   }
   __syncthreads();
-  auto nbsum = [&](const LevelDev& L, const float* z, int i, int x, int y, int zz) {
-    const int sy = L.nx, sz = L.nx * L.ny;
-    auto nb = [&](bool in, int j, float w) { return in ? w * z[j] : 0.0f; };
-    return d4sum6(nb(x > 0, i - 1, L.wx), nb(x + 1 < L.nx, i + 1, L.wx), nb(y > 0, i - sy, L.wy),
-                  nb(y + 1 < L.ny, i + sy, L.wy), nb(zz > 0, i - sz, L.wz), nb(zz + 1 < L.nz, i + sz, L.wz));
-  };
-  auto pass = [&](int l, int colour, int zero_init) {
+  if (s_done) return;
+  const int first = s_first, last = s_last;
+  for (int l = first; l <= last; ++l) {
     const LevelDev& L = I.lv[l];
-    float* z = zs[l];
-    for (int i = threadIdx.x; i < int(L.n); i += blockDim.x) {
+    const BlockLevel& b = B[l];
+    const T* dg = static_cast<const T*>(L.diagT);
+    const T* rh = static_cast<const T*>(L.rhs);
+    for (int i = threadIdx.x; i < b.n; i += blockDim.x) {
       int x, y, zz;
-      decode(i, L.nx, L.ny, x, y, zz);
-      if (((x + y + zz) & 1) != colour) {
-        if (zero_init) z[i] = 0.0f;
-        continue;
+      decode(i, b.nx, b.ny, x, y, zz);
+      const float d = tof(dg[i]);
+      const uint8_t lb = L.label[i];
+      b.diag[i] = d;
+      b.inv[i] = lb ? 1.0f / d : 0.0f;
+      b.lab[i] = lb;
+      b.xyz[i] = unsigned(x) | (unsigned(y) << 10) | (unsigned(zz) << 20);
+      const int red = red_before(x, y, zz, b.nx, b.ny);
+      b.ord[((x + y + zz) & 1) ? b.nred + (i - red) : red] = (unsigned short)i;
+      if (l == first) b.rhs[i] = tof(rh[i]);
+    }
+  }
+  __syncthreads();
+  auto nbsum = [](const BlockLevel& b, const float* z, int i, unsigned c) {
+    const int x = int(c & 1023u), y = int((c >> 10) & 1023u), zz = int(c >> 20);
+    const int sy = b.nx, sz = b.nx * b.ny;
+    const float xm = x > 0 ? b.wx * z[i - 1] : 0.0f, xp = x + 1 < b.nx ? b.wx * z[i + 1] : 0.0f;
+    const float ym = y > 0 ? b.wy * z[i - sy] : 0.0f, yp = y + 1 < b.ny ? b.wy * z[i + sy] : 0.0f;
+    const float zm = zz > 0 ? b.wz * z[i - sz] : 0.0f, zp = zz + 1 < b.nz ? b.wz * z[i + sz] : 0.0f;
+    return d4sum6(xm, xp, ym, yp, zm, zp);
+  };
+  // one colour pass; colour 2 clears z
+  auto pass = [&](int l, int colour, int zero_init) {
+    const BlockLevel& b = B[l];
+    if (colour == 2) {
+      for (int i = threadIdx.x; i < b.n; i += blockDim.x) b.z[i] = 0.0f;
+    } else {
+      const int j0 = colour == 0 ? 0 : b.nred, j1 = colour == 0 ? b.nred : b.n;
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        const int i = b.ord[j];
+        const float s = zero_init ? 0.0f : nbsum(b, b.z, i, b.xyz[i]);
+        b.z[i] = (b.rhs[i] + s) * b.inv[i];
       }
-      if (!ls[l][i]) {
-        z[i] = 0.0f;
-        continue;
-      }
-      const float s = zero_init ? 0.0f : nbsum(L, z, i, x, y, zz);
-      z[i] = (rs[l][i] + s) / ds[l][i];
+      if (zero_init)   // the other colour starts at zero
+        for (int j = (colour == 0 ? b.nred : 0) + threadIdx.x; j < (colour == 0 ? b.n : b.nred); j += blockDim.x)
+          b.z[b.ord[j]] = 0.0f;
     }
     __syncthreads();
   };
   // down
   for (int l = first; l < last; ++l) {
-    const LevelDev& L = I.lv[l];
+    const BlockLevel& F = B[l];
     for (int sw = 0; sw < pre; ++sw) {
       pass(l, 0, sw == 0);
       pass(l, 1, 0);
     }
     if (pre == 0) pass(l, 2, 1);
-    for (int i = threadIdx.x; i < int(L.n); i += blockDim.x) {
-      float r = 0.0f;
-      if (ls[l][i]) {
-        int x, y, zz;
-        decode(i, L.nx, L.ny, x, y, zz);
-        r = rs[l][i] - (ds[l][i] * zs[l][i] - nbsum(L, zs[l], i, x, y, zz));
-      }
-      es[l][i] = r;
-    }
+    for (int i = threadIdx.x; i < F.n; i += blockDim.x)
+      F.res[i] = F.lab[i] ? F.rhs[i] - (F.diag[i] * F.z[i] - nbsum(F, F.z, i, F.xyz[i])) : 0.0f;
     __syncthreads();
-    const LevelDev& C = I.lv[l + 1];
-    const float scale = L.to_coarse / float((C.sx == 2 ? 2 : 1) * (C.sy == 2 ? 2 : 1) * (C.sz == 2 ? 2 : 1));
-    for (int i = threadIdx.x; i < int(C.n); i += blockDim.x) {
+    const BlockLevel& C = B[l + 1];
+    const float scale = F.to_coarse / float((C.sx == 2 ? 2 : 1) * (C.sy == 2 ? 2 : 1) * (C.sz == 2 ? 2 : 1));
+    for (int i = threadIdx.x; i < C.n; i += blockDim.x) {
       float acc = 0.0f;
-      if (ls[l + 1][i]) {
-        int X, Y, Z;
-        decode(i, C.nx, C.ny, X, Y, Z);
-        const int x0 = C.sx == 2 ? max(2 * X - 1, 0) : X, x1 = C.sx == 2 ? min(2 * X + 2, L.nx - 1) : X;
-        const int y0 = C.sy == 2 ? max(2 * Y - 1, 0) : Y, y1 = C.sy == 2 ? min(2 * Y + 2, L.ny - 1) : Y;
-        const int z0 = C.sz == 2 ? max(2 * Z - 1, 0) : Z, z1 = C.sz == 2 ? min(2 * Z + 2, L.nz - 1) : Z;
+      if (C.lab[i]) {
+        const unsigned cc = C.xyz[i];
+        const int X = int(cc & 1023u), Y = int((cc >> 10) & 1023u), Z = int(cc >> 20);
+        const int x0 = C.sx == 2 ? max(2 * X - 1, 0) : X, x1 = C.sx == 2 ? min(2 * X + 2, F.nx - 1) : X;
+        const int y0 = C.sy == 2 ? max(2 * Y - 1, 0) : Y, y1 = C.sy == 2 ? min(2 * Y + 2, F.ny - 1) : Y;
+        const int z0 = C.sz == 2 ? max(2 * Z - 1, 0) : Z, z1 = C.sz == 2 ? min(2 * Z + 2, F.nz - 1) : Z;
         for (int fz = z0; fz <= z1; ++fz) {
           const float wz = C.sz == 2 ? p1d(fz, Z, C.nz) : 1.0f;
           for (int fy = y0; fy <= y1; ++fy) {
             const float wyz = wz * (C.sy == 2 ? p1d(fy, Y, C.ny) : 1.0f);
-            const int row = L.nx * (fy + L.ny * fz);
+            const int row = F.nx * (fy + F.ny * fz);
             float s = 0.0f;
-            for (int fx = x0; fx <= x1; ++fx) s += (C.sx == 2 ? p1d(fx, X, C.nx) : 1.0f) * es[l][row + fx];
+            for (int fx = x0; fx <= x1; ++fx) s += (C.sx == 2 ? p1d(fx, X, C.nx) : 1.0f) * F.res[row + fx];
             acc += wyz * s;
           }
         }
         acc *= scale;
       }
-      rs[l + 1][i] = acc;
+      C.rhs[i] = acc;
     }
     __syncthreads();
   }
   // coarsest: dense float64 inverse
   {
-    const LevelDev& L = I.lv[last];
-    const int m = int(L.n);
+    const BlockLevel& b = B[last];
+    const int m = b.n;
+    const double* inv = I.coarse_inv;
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
       double s = 0;
-      const double* row = I.coarse_inv + (long long)i * m;
-      for (int j = 0; j < m; ++j) s += row[j] * (ls[last][j] ? double(rs[last][j]) : 0.0);
-      zs[last][i] = ls[last][i] ? float(s) : 0.0f;
+      const double* row = inv + (long long)i * m;
+      for (int j = 0; j < m; ++j) s += row[j] * (b.lab[j] ? double(b.rhs[j]) : 0.0);
+      b.z[i] = b.lab[i] ? float(s) : 0.0f;
     }
     __syncthreads();
   }
   // up
   for (int l = last - 1; l >= first; --l) {
-    const LevelDev& F = I.lv[l];
-    const LevelDev& C = I.lv[l + 1];
-    for (int i = threadIdx.x; i < int(F.n); i += blockDim.x) {
-      if (!ls[l][i]) continue;
-      int x, y, zz;
-      decode(i, F.nx, F.ny, x, y, zz);
+    const BlockLevel& F = B[l];
+    const BlockLevel& C = B[l + 1];
+    for (int i = threadIdx.x; i < F.n; i += blockDim.x) {
+      if (!F.lab[i]) continue;
+      const unsigned c = F.xyz[i];
       int cx[2], cy[2], cz[2];
       float wx[2], wy[2], wz[2];
-      const int nxx = taps1d(x, C.sx, C.nx, cx, wx);
-      const int nyy = taps1d(y, C.sy, C.ny, cy, wy);
-      const int nzz = taps1d(zz, C.sz, C.nz, cz, wz);
+      const int nxx = taps1d(int(c & 1023u), C.sx, C.nx, cx, wx);
+      const int nyy = taps1d(int((c >> 10) & 1023u), C.sy, C.ny, cy, wy);
+      const int nzz = taps1d(int(c >> 20), C.sz, C.nz, cz, wz);
       float s = 0.0f;
       for (int c2 = 0; c2 < nzz; ++c2)
         for (int c1 = 0; c1 < nyy; ++c1)
-          for (int c0 = 0; c0 < nxx; ++c0)
-            s += wx[c0] * wy[c1] * wz[c2] * zs[l + 1][cx[c0] + C.nx * (cy[c1] + C.ny * cz[c2])];
-      zs[l][i] += s;
+          for (int c0 = 0; c0 < nxx; ++c0) s += wx[c0] * wy[c1] * wz[c2] * C.z[cx[c0] + C.nx * (cy[c1] + C.ny * cz[c2])];
+      F.z[i] += s;
     }
     __syncthreads();
     for (int sw = 0; sw < post; ++sw) {
@@ -608,8 +821,9 @@ __global__ void k_coarse_block(const InstDev* insts, const int* list, int pre, i
       pass(l, 0, 0);
     }
   }
-  const LevelDev& Lf = I.lv[first];
-  for (int i = threadIdx.x; i < int(Lf.n); i += blockDim.x) St<T>::st(Lf.z, i, zs[first][i]);
+  const BlockLevel& Bf = B[first];
+  T* zo = static_cast<T*>(I.lv[first].z);
+  for (int i = threadIdx.x; i < Bf.n; i += blockDim.x) zo[i] = fromf<T>(Bf.z[i]);
 }
 
 // Coarsest solve z = A_c^{-1} rhs in float64 for single-level hierarchies.
@@ -631,37 +845,53 @@ __global__ void k_coarse_apply(const InstDev* insts, const int* list) {
 }
 
 // ================================================================= CG kernels
+// Level-0 column helper: calls f(k, z, i) for the thread's valid cells, fully
+// unrolled so the loads of all kTZ cells are in flight together.
+template <class F>
+__device__ __forceinline__ void for_column(const TileIt& it, int nx, int ny, int nz, F f) {
+  if (!it.ok) return;
+  const int sz = nx * ny;
+  const int i0 = it.x + nx * (it.y + ny * it.z0);
+#pragma unroll
+  for (int k = 0; k < kMaxDepth; ++k)
+    if (k < it.depth && it.z0 + k < nz) f(k, it.z0 + k, i0 + k * sz);
+}
+
 // gamma = r . (z - zmean) with float64 accumulation; beta from the previous gamma.
-__global__ void k_dot_rz(const InstDev* insts, const Tile* tiles, int ntiles) {
+__global__ void __launch_bounds__(kThreads) k_dot_rz(const InstDev* insts, const Tile* tiles, int ntiles) {
   __shared__ double sh[32];
   __shared__ int flag;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
     Ctrl* c = I.ctrl;
-    if (c->done) continue;
-    const LevelDev& L = I.lv[0];
-    const float* r = static_cast<const float*>(L.rhs);
-    const float* z = static_cast<const float*>(L.z);
+    const int done = c->done;
+    const LevelDev L = I.lv[0];
+    const int nt0 = I.ntiles0;
+    double* partial = I.partial;
+    if (done) continue;
+    const float* __restrict__ r = static_cast<const float*>(L.rhs);
+    const float* __restrict__ z = static_cast<const float*>(L.z);
+    const uint8_t* __restrict__ lab = L.label;
     double rz = 0, zs = 0, rs = 0;
-    int x, y, zz, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz); it.next(x, y, zz, i);) {
-      if (!L.label[i]) continue;
+    const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
+    for_column(it, L.nx, L.ny, L.nz, [&](int, int, int i) {
+      if (!lab[i]) return;
       const double zv = z[i], rv = r[i];
       rz += rv * zv;
       zs += zv;
       rs += rv;
-    }
+    });
     const double a0 = block_sum(rz, sh), a1 = block_sum(zs, sh), a2 = block_sum(rs, sh);
     if (threadIdx.x == 0) {
-      I.partial[0 * I.ntiles0 + tl.tile] = a0;
-      I.partial[1 * I.ntiles0 + tl.tile] = a1;
-      I.partial[2 * I.ntiles0 + tl.tile] = a2;
+      partial[0 * nt0 + tl.tile] = a0;
+      partial[1 * nt0 + tl.tile] = a1;
+      partial[2 * nt0 + tl.tile] = a2;
     }
-    if (arrive_last(&c->arrive[kStGamma], I.ntiles0, &flag)) {
-      const double g = gather_slot(I.partial, 0, I.ntiles0, 0, sh);
-      const double zsum = gather_slot(I.partial, 1, I.ntiles0, 0, sh);
-      const double rsum = gather_slot(I.partial, 2, I.ntiles0, 0, sh);
+    if (arrive_last(&c->arrive[kStGamma], nt0, &flag)) {
+      const double g = gather_slot(partial, 0, nt0, 0, sh);
+      const double zsum = gather_slot(partial, 1, nt0, 0, sh);
+      const double rsum = gather_slot(partial, 2, nt0, 0, sh);
       if (threadIdx.x == 0) {
         double gamma = g;
         c->zmean = 0.0;
@@ -683,50 +913,59 @@ __global__ void k_dot_rz(const InstDev* insts, const Tile* tiles, int ntiles) {
 }
 
 // d = (z - zmean) + beta d on liquid cells.
-__global__ void k_dir(const InstDev* insts, const Tile* tiles, int ntiles) {
+__global__ void __launch_bounds__(kThreads) k_dir(const InstDev* insts, const Tile* tiles, int ntiles) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
     const Ctrl* c = I.ctrl;
-    if (c->done) continue;
-    const LevelDev& L = I.lv[0];
-    const float* z = static_cast<const float*>(L.z);
+    const int done = c->done;
     const float beta = float(c->beta), zm = float(c->zmean);
-    int x, y, zz, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz); it.next(x, y, zz, i);)
-      I.d[i] = L.label[i] ? (z[i] - zm) + beta * I.d[i] : 0.0f;
+    const LevelDev L = I.lv[0];
+    float* __restrict__ d = I.d;
+    if (done) continue;
+    const float* __restrict__ z = static_cast<const float*>(L.z);
+    const uint8_t* __restrict__ lab = L.label;
+    const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
+    for_column(it, L.nx, L.ny, L.nz, [&](int, int, int i) { d[i] = lab[i] ? (z[i] - zm) + beta * d[i] : 0.0f; });
   }
 }
 
 // q = A d and delta = d . q (applyLiquidOperator, atlas :1171-1192), alpha = gamma / delta.
-__global__ void k_spmv(const InstDev* insts, const Tile* tiles, int ntiles) {
+__global__ void __launch_bounds__(kThreads) k_spmv(const InstDev* insts, const Tile* tiles, int ntiles) {
   __shared__ double sh[32];
   __shared__ int flag;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
     Ctrl* c = I.ctrl;
-    if (c->done) continue;
-    const LevelDev& L = I.lv[0];
-    const float* D = I.d;
+    const int done = c->done;
+    const LevelDev L = I.lv[0];
+    const int nt0 = I.ntiles0;
+    double* partial = I.partial;
+    const float* __restrict__ D = I.d;
+    float* __restrict__ Q = I.q;
+    if (done) continue;
+    const float* __restrict__ dg = L.diag;
+    const uint8_t* __restrict__ lab = L.label;
     double dq = 0;
     const int sy = L.nx, sz = L.nx * L.ny;
-    int x, y, z, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz); it.next(x, y, z, i);) {
+    const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
+    const int x = it.x, y = it.y;
+    for_column(it, L.nx, L.ny, L.nz, [&](int, int zz, int i) {
       float q = 0.0f;
-      if (L.label[i]) {
+      if (lab[i]) {
         const float s = d4sum6(x > 0 ? D[i - 1] : 0.0f, x + 1 < L.nx ? D[i + 1] : 0.0f, y > 0 ? D[i - sy] : 0.0f,
-                               y + 1 < L.ny ? D[i + sy] : 0.0f, z > 0 ? D[i - sz] : 0.0f,
-                               z + 1 < L.nz ? D[i + sz] : 0.0f);
-        q = L.diag[i] * D[i] - s;
+                               y + 1 < L.ny ? D[i + sy] : 0.0f, zz > 0 ? D[i - sz] : 0.0f,
+                               zz + 1 < L.nz ? D[i + sz] : 0.0f);
+        q = dg[i] * D[i] - s;
         dq += double(D[i]) * q;
       }
-      I.q[i] = q;
-    }
+      Q[i] = q;
+    });
     const double a0 = block_sum(dq, sh);
-    if (threadIdx.x == 0) I.partial[tl.tile] = a0;
-    if (arrive_last(&c->arrive[kStSpmv], I.ntiles0, &flag)) {
-      const double delta = gather_slot(I.partial, 0, I.ntiles0, 0, sh);
+    if (threadIdx.x == 0) partial[tl.tile] = a0;
+    if (arrive_last(&c->arrive[kStSpmv], nt0, &flag)) {
+      const double delta = gather_slot(partial, 0, nt0, 0, sh);
       if (threadIdx.x == 0) {
         c->delta = delta;
         if (!(delta > 0.0) || !isfinite(delta)) {
@@ -741,40 +980,48 @@ __global__ void k_spmv(const InstDev* insts, const Tile* tiles, int ntiles) {
 }
 
 // x += alpha d (double-single), r -= alpha q, rr = r . r, max |r|.
-__global__ void k_update(const InstDev* insts, const Tile* tiles, int ntiles) {
+__global__ void __launch_bounds__(kThreads) k_update(const InstDev* insts, const Tile* tiles, int ntiles) {
   __shared__ double sh[32];
   __shared__ int flag;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
     Ctrl* c = I.ctrl;
-    if (c->done) continue;
-    const LevelDev& L = I.lv[0];
-    float* r = static_cast<float*>(L.rhs);
+    const int done = c->done;
     const double alpha = c->alpha;
+    const LevelDev L = I.lv[0];
+    const int nt0 = I.ntiles0;
+    double* partial = I.partial;
+    float* __restrict__ X = I.x;
+    float* __restrict__ Xlo = I.xlo;
+    const float* __restrict__ D = I.d;
+    const float* __restrict__ Q = I.q;
+    if (done) continue;
+    float* __restrict__ r = static_cast<float*>(L.rhs);
+    const uint8_t* __restrict__ lab = L.label;
     const float alpha_f = float(alpha);
     double rr = 0, mr = 0;
-    int x, y, z, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz); it.next(x, y, z, i);) {
-      if (!L.label[i]) continue;
+    const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
+    for_column(it, L.nx, L.ny, L.nz, [&](int, int, int i) {
+      if (!lab[i]) return;
       // double-single accumulation: x_hi + x_lo carries the pressure to ~1e-14
-      const double xv = double(I.x[i]) + double(I.xlo[i]) + alpha * double(I.d[i]);
+      const double xv = double(X[i]) + double(Xlo[i]) + alpha * double(D[i]);
       const float hi = float(xv);
-      I.x[i] = hi;
-      I.xlo[i] = float(xv - double(hi));
-      const float rv = r[i] - alpha_f * I.q[i];
+      X[i] = hi;
+      Xlo[i] = float(xv - double(hi));
+      const float rv = r[i] - alpha_f * Q[i];
       r[i] = rv;
       rr += double(rv) * rv;
       mr = fmax(mr, fabs(double(rv)));
-    }
+    });
     const double a0 = block_sum(rr, sh), a1 = block_max(mr, sh);
     if (threadIdx.x == 0) {
-      I.partial[tl.tile] = a0;
-      I.partial[I.ntiles0 + tl.tile] = a1;
+      partial[tl.tile] = a0;
+      partial[nt0 + tl.tile] = a1;
     }
-    if (arrive_last(&c->arrive[kStUpdate], I.ntiles0, &flag)) {
-      const double s = gather_slot(I.partial, 0, I.ntiles0, 0, sh);
-      const double m = gather_slot(I.partial, 1, I.ntiles0, 1, sh);
+    if (arrive_last(&c->arrive[kStUpdate], nt0, &flag)) {
+      const double s = gather_slot(partial, 0, nt0, 0, sh);
+      const double m = gather_slot(partial, 1, nt0, 1, sh);
       if (threadIdx.x == 0) {
         c->rr = s;
         c->rmax = m;
@@ -793,43 +1040,51 @@ __global__ void k_update(const InstDev* insts, const Tile* tiles, int ntiles) {
 
 // Float64 true residual r = b - A x, replacing the recursive residual; decides
 // convergence for candidates (octree-pipelined-pcg.ts:501-541 acceptance rule).
-__global__ void k_true_residual(const InstDev* insts, const Tile* tiles, int ntiles) {
+__global__ void __launch_bounds__(kThreads) k_true_residual(const InstDev* insts, const Tile* tiles, int ntiles) {
   __shared__ double sh[32];
   __shared__ int flag;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
     Ctrl* c = I.ctrl;
-    if (c->done) continue;
-    if (!c->candidate && !(c->true_every > 0 && c->iter % c->true_every == 0)) continue;
-    const LevelDev& L = I.lv[0];
-    float* r = static_cast<float*>(L.rhs);
-    auto X = [&](int j) { return double(I.x[j]) + double(I.xlo[j]); };
+    const int done = c->done, cand = c->candidate, every = c->true_every, iter = c->iter;
+    if (done || (!cand && !(every > 0 && iter % every == 0))) continue;
+    const LevelDev L = I.lv[0];
+    const int nt0 = I.ntiles0;
+    double* partial = I.partial;
+    float* __restrict__ r = static_cast<float*>(L.rhs);
+    const float* __restrict__ Xh = I.x;
+    const float* __restrict__ Xl = I.xlo;
+    const float* __restrict__ B = I.b;
+    const float* __restrict__ dg = L.diag;
+    const uint8_t* __restrict__ lab = L.label;
+    auto X = [&](int j) { return double(Xh[j]) + double(Xl[j]); };
     double rr = 0, mr = 0;
     const int sy = L.nx, sz = L.nx * L.ny;
-    int x, y, z, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz); it.next(x, y, z, i);) {
-      if (!L.label[i]) continue;
+    const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
+    const int x = it.x, y = it.y;
+    for_column(it, L.nx, L.ny, L.nz, [&](int, int zz, int i) {
+      if (!lab[i]) return;
       double s = 0;
       if (x > 0) s += X(i - 1);
       if (x + 1 < L.nx) s += X(i + 1);
       if (y > 0) s += X(i - sy);
       if (y + 1 < L.ny) s += X(i + sy);
-      if (z > 0) s += X(i - sz);
-      if (z + 1 < L.nz) s += X(i + sz);
-      const double rv = double(I.b[i]) - (double(L.diag[i]) * X(i) - s);
+      if (zz > 0) s += X(i - sz);
+      if (zz + 1 < L.nz) s += X(i + sz);
+      const double rv = double(B[i]) - (double(dg[i]) * X(i) - s);
       r[i] = float(rv);
       rr += rv * rv;
       mr = fmax(mr, fabs(rv));
-    }
+    });
     const double a0 = block_sum(rr, sh), a1 = block_max(mr, sh);
     if (threadIdx.x == 0) {
-      I.partial[tl.tile] = a0;
-      I.partial[I.ntiles0 + tl.tile] = a1;
+      partial[tl.tile] = a0;
+      partial[nt0 + tl.tile] = a1;
     }
-    if (arrive_last(&c->arrive[kStTrue], I.ntiles0, &flag)) {
-      const double s = gather_slot(I.partial, 0, I.ntiles0, 0, sh);
-      const double m = gather_slot(I.partial, 1, I.ntiles0, 1, sh);
+    if (arrive_last(&c->arrive[kStTrue], nt0, &flag)) {
+      const double s = gather_slot(partial, 0, nt0, 0, sh);
+      const double m = gather_slot(partial, 1, nt0, 1, sh);
       if (threadIdx.x == 0) {
         c->rr_true = s;
         c->rr = s;
@@ -878,7 +1133,7 @@ __global__ void k_grad(const InstDev* insts, const Tile* tiles, int ntiles) {
     const LevelDev& L = I.lv[0];
     const long long uS = I.nx + 1, vS = I.ny + 1;
     int x, y, z, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz); it.next(x, y, z, i);) {
+    for (TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth); it.next(x, y, z, i);) {
       const long long urow = uS * (y + (long long)I.ny * z);
       const long long vcol = x + (long long)I.nx * vS * z;
       const int sz = I.nx * I.ny;
@@ -919,7 +1174,7 @@ __global__ void k_receipt(const InstDev* insts, const Tile* tiles, int ntiles) {
     double mb = 0, sb = 0, ma = 0, sa = 0;
     const long long uS = I.nx + 1, vS = I.ny + 1;
     int x, y, z, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz); it.next(x, y, z, i);) {
+    for (TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth); it.next(x, y, z, i);) {
       if (!L.label[i]) continue;
       const long long urow = uS * (y + (long long)I.ny * z);
       const long long vcol = x + (long long)I.nx * vS * z;

@@ -51,7 +51,7 @@ __global__ void k_spmv_noalloc(int nx, int ny, int nz, const uint8_t* __restrict
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     double dq = 0;
     int x, y, z, i;
-    for (TileIt it(t, nx, ny, nz); it.next(x, y, z, i);) {
+    for (TileIt it(t, nx, ny, nz, kMaxDepth); it.next(x, y, z, i);) {
       float q = 0.0f;
       if (label[i]) {
         auto nb = [&](bool in, int j) { return (in && label[j]) ? p[j] : 0.0f; };
@@ -81,7 +81,7 @@ extern "C" int fluid_pp_apply_operator_noalloc(int nx, int ny, int nz, const uns
     return FLUID_PP_INVALID_ARG;
   }
   const long long tiles = (long long)((nx + fpp::kTX - 1) / fpp::kTX) * ((ny + fpp::kTY - 1) / fpp::kTY) *
-                          ((nz + fpp::kTZ - 1) / fpp::kTZ);
+                          ((nz + fpp::kMaxDepth - 1) / fpp::kMaxDepth);
   if (tiles > kNoAllocMaxTiles || (long long)nx * ny * nz > (1LL << 30)) {
     fpp::set_global_error("fluid_pp_apply_operator_noalloc: lattice needs " + std::to_string(tiles) +
                     " work tiles of 32x8x4 cells; the fixed scratch holds " + std::to_string(kNoAllocMaxTiles));

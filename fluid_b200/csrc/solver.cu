@@ -227,13 +227,14 @@ void vcycle_launch(fluid_pp_batch* B, int pre, int post) {
       smooth_pass<T>(B, l, 1, 0);
     }
     if (pre == 0) smooth_pass<T>(B, l, 2, 1);   // z must start at zero
-    if (l == 0)
-      FPP_LAUNCH(B, kPrResidual0, k_residual<float, float, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l));
-    else
-      FPP_LAUNCH(B, kPrResidualC, k_residual<T, T, T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l));
+    (void)g;
     const List& Lr = B->rst[l];
-    FPP_LAUNCH(B, l == 0 ? kPrRestrict0 : kPrRestrictC,
-               k_restrict<T><<<launch_grid(Lr.n), kThreads, 0, s>>>(B->d_insts, tl(B, Lr), Lr.n, l));
+    if (l == 0)
+      FPP_LAUNCH(B, kPrRestrict0, k_residual_restrict<float, float, T, T><<<launch_grid(Lr.n), kThreads, 0, s>>>(
+                                      B->d_insts, tl(B, Lr), Lr.n, l));
+    else
+      FPP_LAUNCH(B, kPrRestrictC, k_residual_restrict<T, T, T, T><<<launch_grid(Lr.n), kThreads, 0, s>>>(
+                                      B->d_insts, tl(B, Lr), Lr.n, l));
   }
   if (B->multi.n)
     FPP_LAUNCH(B, kPrCoarse, k_coarse_block<T><<<B->multi.n, kBlockThreads, B->smem_block, s>>>(
@@ -408,12 +409,14 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
   // tile lists
   std::vector<Tile> tiles;
   std::vector<int> ilist;
-  auto add_level = [&](List& L, auto pred, int level_of_tiles) {
+  // restriction tiles (coarse tiles of kRX x kRY x kRZ) when `restrict_tiles`
+  auto add_level = [&](List& L, auto pred, int level_of_tiles, bool restrict_tiles = false) {
     L.off = int(tiles.size());
     for (int k = 0; k < count; ++k) {
       const InstDev& I = B->h[k]->inst;
       if (!pred(I)) continue;
-      const int nt = I.lv[level_of_tiles].ntiles;
+      const LevelDev& Lv = I.lv[level_of_tiles];
+      const int nt = restrict_tiles ? rtiles_of(Lv.nx, Lv.ny, Lv.nz) : Lv.ntiles;
       for (int t = 0; t < nt; ++t) tiles.push_back(Tile{k, level_of_tiles, t, 0});
     }
     L.n = int(tiles.size()) - L.off;
@@ -423,7 +426,7 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
   for (int l = 0; l < B->maxL; ++l) {
     add_level(B->lvl[l], [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; }, l);
     if (l + 1 < B->maxL)
-      add_level(B->rst[l], [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; }, l + 1);
+      add_level(B->rst[l], [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; }, l + 1, true);
     if (l >= 1) add_level(B->crs[l], [l](const InstDev& I) { return l < I.nlev; }, l);
   }
   B->bake.off = int(tiles.size());
@@ -686,7 +689,10 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
     g_err = "lattice exceeds 2^30 cells";
     return FLUID_PP_INVALID_ARG;
   }
-  const int nt0 = tiles_of(nx, ny, nz);
+  // Cells per thread along z: keep at least ~2 waves of fully occupied SMs
+  // (148 x 2048 threads) in flight; small levels get one cell per thread.
+  auto depth_of = [](long long n) { return n >= 4LL * 600000 ? 4 : n >= 2LL * 600000 ? 2 : 1; };
+  const int nt0 = tiles_of(nx, ny, nz, depth_of(N));
   acc(sizeof(double) * kSlots * nt0);
   acc(sizeof(double) * ncoarse * ncoarse);
   acc(sizeof(Ctrl));
@@ -720,7 +726,8 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
     L.sy = plan.stride[l][1];
     L.sz = plan.stride[l][2];
     L.n = (long long)L.nx * L.ny * L.nz;
-    L.ntiles = tiles_of(L.nx, L.ny, L.nz);
+    L.depth = depth_of(L.n);
+    L.ntiles = tiles_of(L.nx, L.ny, L.nz, L.depth);
     // spacing ratio h_l / h_0 per axis (webgpu-uniform-pressure-multigrid.ts:588-589)
     const double rx = double(nx) / L.nx, ry = double(ny) / L.ny, rz = double(nz) / L.nz;
     const double wx = 1.0 / (rx * rx), wy = 1.0 / (ry * ry), wz = 1.0 / (rz * rz);
@@ -749,7 +756,7 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
   if (plan.levels > 1) {
     for (int l = 1; l < plan.levels; ++l) {
       long long bytes = 0;
-      for (int j = l; j < plan.levels; ++j) bytes += 16 * I.lv[j].n + ((I.lv[j].n + 3) & ~3LL);
+      for (int j = l; j < plan.levels; ++j) bytes += block_level_bytes(I.lv[j].n);
       if (I.lv[l].n <= kCoarseBlockCells && bytes <= kCoarseBlockSmem) {
         I.first_block = l;
         I.block_smem = int(bytes);

@@ -53,7 +53,7 @@ struct LevelDev {
   int sx, sy, sz;     // coarsening factor from the next finer level (1 or 2)
   long long n;
   int ntiles;
-  int coarse_block;   // unused marker
+  int depth;          // cells per thread along z in this level's work tiles
   float wx, wy, wz;   // normalised off-diagonal weights w_a / wmax
   float wmax;         // (h0 / h_a)^2 maximum over axes; level operators are stored divided by it
   float ext_phi;      // open-top exterior phi (finest-cell units)
