@@ -30,7 +30,7 @@ EXPORTS = (
 )
 STAGES = ("reset", "label", "coarsen", "bake", "factor", "init", "smooth0", "smoothc", "residual0", "residualc",
           "restrict0", "restrictc", "coarse", "prolong0", "prolongc", "dot", "dir", "spmv", "update", "true",
-          "grad", "receipt")
+          "grad", "receipt", "down0", "downc", "up0", "upc", "dirspmv")
 
 
 class Config(ctypes.Structure):

@@ -16,7 +16,6 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libfluid_pp.so")
 SOURCES = ["solver.cu", "noalloc.cu", "plan.cpp"]
-HEADERS = ["kernels.cuh", "device_util.cuh", "types.h", "plan.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -31,8 +30,8 @@ def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "fluid_pp.h")]
-    return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "fluid_pp.h")]
+    return any(os.path.getmtime(p) > t for p in deps if os.path.isfile(p))
 
 
 def build(force: bool = False, verbose: bool = False) -> str:

@@ -18,7 +18,7 @@ struct Tile {
 };
 
 constexpr int kTX = 32, kTY = 8;   // tile extent in x and y; kTX * kTY == kThreads
-constexpr int kMaxDepth = 4;       // cells per thread along z: 1, 2 or 4 per level
+constexpr int kMaxDepth = 8;       // cells per thread along z: 8 on level 0, 1, 2 or 4 on coarser levels
 constexpr int kBlockThreads = 1024;        // coarse-block CTA
 
 __host__ __device__ inline int tiles_of(int nx, int ny, int nz, int depth) {
@@ -168,9 +168,9 @@ __device__ __forceinline__ double gather_slot(const double* partial, int slot, i
       a[u] = op ? fmax(a[u], v) : a[u] + v;
     }
   }
-  for (int u = 0; t < ntiles; t += stride, ++u) {
+  for (; t < ntiles; t += stride) {
     const double v = __ldcg(p + t);
-    a[u & 3] = op ? fmax(a[u & 3], v) : a[u & 3] + v;
+    a[0] = op ? fmax(a[0], v) : a[0] + v;
   }
   const double acc = op ? fmax(fmax(a[0], a[1]), fmax(a[2], a[3])) : (a[0] + a[1]) + (a[2] + a[3]);
   return op ? block_max(acc, sh) : block_sum(acc, sh);
@@ -194,6 +194,27 @@ __device__ __forceinline__ int taps1d(int f, int stride, int nc, int* c, float* 
   if (b >= 0 && b < nc) { c[n] = b; w[n] = wb; ++n; }
   if (n == 1) w[0] = 1.0f;
   return n;
+}
+
+// The same taps as taps1d in a fixed pair: a dropped tap repeats a valid index
+// with weight zero, so callers can unroll the 2 x 2 x 2 stencil.
+__device__ __forceinline__ void taps2(int f, int stride, int nc, int* c, float* w) {
+  if (stride == 1) {
+    c[0] = c[1] = f;
+    w[0] = 1.0f;
+    w[1] = 0.0f;
+    return;
+  }
+  const int k = f >> 1;
+  int a, b;
+  float wa, wb;
+  if ((f & 1) == 0) { a = k - 1; wa = 0.25f; b = k; wb = 0.75f; }
+  else { a = k; wa = 0.75f; b = k + 1; wb = 0.25f; }
+  const bool ia = a >= 0 && a < nc, ib = b >= 0 && b < nc;
+  c[0] = ia ? a : b;
+  c[1] = ib ? b : a;
+  w[0] = ia ? (ib ? wa : 1.0f) : 0.0f;
+  w[1] = ib ? (ia ? wb : 1.0f) : 0.0f;
 }
 
 // Weight of coarse cell c in the stencil of fine cell f along an axis that

@@ -379,112 +379,11 @@ __global__ void __launch_bounds__(kThreads) k_smooth(const InstDev* insts, const
   }
 }
 
-// res = scale * (rhs - A z) on liquid cells (mgResidual, mg.wgsl.ts:197-205).
-// On level 0 the residual is scaled by sigma so half-precision levels stay in range.
-template <class TZ, class TR, class TD, class TS>
-__global__ void __launch_bounds__(kThreads) k_residual(const InstDev* insts, const Tile* tiles, int ntiles,
-                                                       int level) {
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const Tile tl = tiles[t];
-    const InstDev& I = insts[tl.inst];
-    const int done = I.ctrl->done;
-    const double sigma = I.ctrl->sigma;
-    const LevelDev L = I.lv[level];
-    const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
-    if (done || !it.ok) continue;
-    const float scale = level == 0 ? float(sigma) : 1.0f;
-    const TZ* __restrict__ z = static_cast<const TZ*>(L.z);
-    const TR* __restrict__ rhs = static_cast<const TR*>(L.rhs);
-    const TD* __restrict__ dg = static_cast<const TD*>(L.diagT);
-    const uint8_t* __restrict__ lab = L.label;
-    TS* __restrict__ res = static_cast<TS*>(L.res);
-    const int sy = L.nx, sz = L.nx * L.ny;
-    const int x = it.x, y = it.y;
-    const int i0 = x + L.nx * (y + L.ny * it.z0);
-#pragma unroll
-    for (int k = 0; k < kMaxDepth; ++k) {
-      if (k >= it.depth) break;
-      const int zz = it.z0 + k, i = i0 + k * sz;
-      if (zz >= L.nz) continue;
-      float r = 0.0f;
-      if (lab[i]) {
-        const float xm = x > 0 ? L.wx * tof(z[i - 1]) : 0.0f, xp = x + 1 < L.nx ? L.wx * tof(z[i + 1]) : 0.0f;
-        const float ym = y > 0 ? L.wy * tof(z[i - sy]) : 0.0f, yp = y + 1 < L.ny ? L.wy * tof(z[i + sy]) : 0.0f;
-        const float zm = zz > 0 ? L.wz * tof(z[i - sz]) : 0.0f, zp = zz + 1 < L.nz ? L.wz * tof(z[i + sz]) : 0.0f;
-        const float s = d4sum6(xm, xp, ym, yp, zm, zp);
-        r = scale * (tof(rhs[i]) - (tof(dg[i]) * tof(z[i]) - s));
-      }
-      res[i] = fromf<TS>(r);
-    }
-  }
-}
-
-// rhs_{l+1} = to_coarse * P^T res_l / 2^k (the transpose of the prolongation, so
-// the V-cycle is a symmetric preconditioner); coarse air cells get zero.
-template <class TS>
-__global__ void __launch_bounds__(kThreads) k_restrict(const InstDev* insts, const Tile* tiles, int ntiles,
-                                                       int level) {
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const Tile tl = tiles[t];
-    const InstDev& I = insts[tl.inst];
-    const int done = I.ctrl->done;
-    const LevelDev F = I.lv[level];
-    const LevelDev C = I.lv[level + 1];
-    const TileIt it(tl.tile, C.nx, C.ny, C.nz, C.depth);
-    if (done || !it.ok) continue;
-    const TS* __restrict__ res = static_cast<const TS*>(F.res);
-    TS* __restrict__ out = static_cast<TS*>(C.rhs);
-    const float scale = F.to_coarse / float((C.sx == 2 ? 2 : 1) * (C.sy == 2 ? 2 : 1) * (C.sz == 2 ? 2 : 1));
-    // x and y stencils are the same for the whole column
-    const int X = it.x, Y = it.y;
-    int fx[4], fy[4];
-    float wx[4], wy[4];
-    int nxx = 0, nyy = 0;
-    if (C.sx == 2) {
-      for (int q = 2 * X - 1; q <= 2 * X + 2; ++q)
-        if (q >= 0 && q < F.nx) { fx[nxx] = q; wx[nxx] = p1d(q, X, C.nx); ++nxx; }
-    } else { fx[0] = X; wx[0] = 1.0f; nxx = 1; }
-    if (C.sy == 2) {
-      for (int q = 2 * Y - 1; q <= 2 * Y + 2; ++q)
-        if (q >= 0 && q < F.ny) { fy[nyy] = q; wy[nyy] = p1d(q, Y, C.ny); ++nyy; }
-    } else { fy[0] = Y; wy[0] = 1.0f; nyy = 1; }
-    const int csz = C.nx * C.ny;
-    const int ci0 = X + C.nx * (Y + C.ny * it.z0);
-    for (int k = 0; k < it.depth; ++k) {
-      const int Z = it.z0 + k;
-      if (Z >= C.nz) break;
-      const int i = ci0 + k * csz;
-      float acc = 0.0f;
-      if (C.label[i]) {
-        int fz[4];
-        float wz[4];
-        int nzz = 0;
-        if (C.sz == 2) {
-          for (int q = 2 * Z - 1; q <= 2 * Z + 2; ++q)
-            if (q >= 0 && q < F.nz) { fz[nzz] = q; wz[nzz] = p1d(q, Z, C.nz); ++nzz; }
-        } else { fz[0] = Z; wz[0] = 1.0f; nzz = 1; }
-        for (int c2 = 0; c2 < nzz; ++c2) {
-          for (int c1 = 0; c1 < nyy; ++c1) {
-            const int row = F.nx * (fy[c1] + F.ny * fz[c2]);
-            float s = 0.0f;
-#pragma unroll 4
-            for (int c0 = 0; c0 < nxx; ++c0) s += wx[c0] * tof(res[row + fx[c0]]);
-            acc += wz[c2] * wy[c1] * s;
-          }
-        }
-        acc *= scale;
-      }
-      out[i] = fromf<TS>(acc);
-    }
-  }
-}
-
 // Residual and restriction fused, one CTA per coarse tile of kRX x kRY x kRZ
 // cells.  The CTA computes the fine residual scale * (rhs - A z) of its fine
 // footprint (the tile's children plus a one-cell halo on coarsened axes) into
 // shared memory, then applies R = P^T / 2^k separably: a 4-tap x pass, a y pass
-// and a z pass.  Same operator as k_residual + k_restrict (summation order of
-// the taps differs), without the residual's round trip through memory.
+// and a z pass, without the residual's round trip through memory.
 constexpr int kRX = 16, kRY = 4, kRZ = 4;
 constexpr int kRFX = 2 * kRX + 2, kRFY = 2 * kRY + 2, kRFZ = 2 * kRZ + 2;
 
@@ -845,6 +744,39 @@ __global__ void k_coarse_apply(const InstDev* insts, const int* list) {
 }
 
 // ================================================================= CG kernels
+// gamma = r . (z - zmean) from its three sums; beta from the previous gamma.
+// A non-positive or non-finite gamma ends the solve (the preconditioned system
+// lost definiteness).
+__device__ __forceinline__ void finish_gamma(Ctrl* c, double rz, double zsum, double rsum) {
+  double gamma = rz;
+  c->zmean = 0.0;
+  if (!c->anchored) {
+    c->zmean = zsum / double(c->liquid);
+    gamma = rz - c->zmean * rsum;
+  }
+  if (!(gamma > 0.0) || !isfinite(gamma)) {
+    c->done = 1;
+    c->status = FLUID_PP_NONCONVERGENCE;
+  } else {
+    c->beta = c->first ? 0.0 : gamma / c->gamma;
+    c->gamma = gamma;
+    c->first = 0;
+  }
+}
+
+// delta = d . A d and alpha = gamma / delta (direct curvature).
+__device__ __forceinline__ void finish_delta(Ctrl* c, double delta) {
+  c->delta = delta;
+  if (!(delta > 0.0) || !isfinite(delta)) {
+    c->done = 1;
+    c->status = FLUID_PP_NONCONVERGENCE;
+  } else {
+    c->alpha = c->gamma / delta;
+  }
+}
+
+// The current search direction (the fused path alternates two buffers).
+__device__ __forceinline__ float* dir_cur(const InstDev& I) { return I.ctrl->dsel ? I.d2 : I.d; }
 // Level-0 column helper: calls f(k, z, i) for the thread's valid cells, fully
 // unrolled so the loads of all kTZ cells are in flight together.
 template <class F>
@@ -892,22 +824,7 @@ __global__ void __launch_bounds__(kThreads) k_dot_rz(const InstDev* insts, const
       const double g = gather_slot(partial, 0, nt0, 0, sh);
       const double zsum = gather_slot(partial, 1, nt0, 0, sh);
       const double rsum = gather_slot(partial, 2, nt0, 0, sh);
-      if (threadIdx.x == 0) {
-        double gamma = g;
-        c->zmean = 0.0;
-        if (!c->anchored) {
-          c->zmean = zsum / double(c->liquid);
-          gamma = g - c->zmean * rsum;
-        }
-        if (!(gamma > 0.0) || !isfinite(gamma)) {
-          c->done = 1;
-          c->status = FLUID_PP_NONCONVERGENCE;
-        } else {
-          c->beta = c->first ? 0.0 : gamma / c->gamma;
-          c->gamma = gamma;
-          c->first = 0;
-        }
-      }
+      if (threadIdx.x == 0) finish_gamma(c, g, zsum, rsum);
     }
   }
 }
@@ -921,7 +838,7 @@ __global__ void __launch_bounds__(kThreads) k_dir(const InstDev* insts, const Ti
     const int done = c->done;
     const float beta = float(c->beta), zm = float(c->zmean);
     const LevelDev L = I.lv[0];
-    float* __restrict__ d = I.d;
+    float* __restrict__ d = dir_cur(I);
     if (done) continue;
     const float* __restrict__ z = static_cast<const float*>(L.z);
     const uint8_t* __restrict__ lab = L.label;
@@ -942,7 +859,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv(const InstDev* insts, const T
     const LevelDev L = I.lv[0];
     const int nt0 = I.ntiles0;
     double* partial = I.partial;
-    const float* __restrict__ D = I.d;
+    const float* __restrict__ D = dir_cur(I);
     float* __restrict__ Q = I.q;
     if (done) continue;
     const float* __restrict__ dg = L.diag;
@@ -966,15 +883,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv(const InstDev* insts, const T
     if (threadIdx.x == 0) partial[tl.tile] = a0;
     if (arrive_last(&c->arrive[kStSpmv], nt0, &flag)) {
       const double delta = gather_slot(partial, 0, nt0, 0, sh);
-      if (threadIdx.x == 0) {
-        c->delta = delta;
-        if (!(delta > 0.0) || !isfinite(delta)) {
-          c->done = 1;
-          c->status = FLUID_PP_NONCONVERGENCE;
-        } else {
-          c->alpha = c->gamma / delta;
-        }
-      }
+      if (threadIdx.x == 0) finish_delta(c, delta);
     }
   }
 }
@@ -994,7 +903,7 @@ __global__ void __launch_bounds__(kThreads) k_update(const InstDev* insts, const
     double* partial = I.partial;
     float* __restrict__ X = I.x;
     float* __restrict__ Xlo = I.xlo;
-    const float* __restrict__ D = I.d;
+    const float* __restrict__ D = dir_cur(I);
     const float* __restrict__ Q = I.q;
     if (done) continue;
     float* __restrict__ r = static_cast<float*>(L.rhs);
@@ -1002,14 +911,25 @@ __global__ void __launch_bounds__(kThreads) k_update(const InstDev* insts, const
     const float alpha_f = float(alpha);
     double rr = 0, mr = 0;
     const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
-    for_column(it, L.nx, L.ny, L.nz, [&](int, int, int i) {
-      if (!lab[i]) return;
+    // every load of the column first (the label does not gate them), then the updates
+    float xh[kMaxDepth], xl[kMaxDepth], dv[kMaxDepth], qv[kMaxDepth], rv0[kMaxDepth];
+    uint8_t lb[kMaxDepth];
+    for_column(it, L.nx, L.ny, L.nz, [&](int k, int, int i) {
+      lb[k] = lab[i];
+      xh[k] = X[i];
+      xl[k] = Xlo[i];
+      dv[k] = D[i];
+      qv[k] = Q[i];
+      rv0[k] = r[i];
+    });
+    for_column(it, L.nx, L.ny, L.nz, [&](int k, int, int i) {
+      if (!lb[k]) return;
       // double-single accumulation: x_hi + x_lo carries the pressure to ~1e-14
-      const double xv = double(X[i]) + double(Xlo[i]) + alpha * double(D[i]);
+      const double xv = double(xh[k]) + double(xl[k]) + alpha * double(dv[k]);
       const float hi = float(xv);
       X[i] = hi;
       Xlo[i] = float(xv - double(hi));
-      const float rv = r[i] - alpha_f * Q[i];
+      const float rv = rv0[k] - alpha_f * qv[k];
       r[i] = rv;
       rr += double(rv) * rv;
       mr = fmax(mr, fabs(double(rv)));
@@ -1063,16 +983,26 @@ __global__ void __launch_bounds__(kThreads) k_true_residual(const InstDev* insts
     const int sy = L.nx, sz = L.nx * L.ny;
     const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
     const int x = it.x, y = it.y;
-    for_column(it, L.nx, L.ny, L.nz, [&](int, int zz, int i) {
-      if (!lab[i]) return;
+    // neighbour sums need no label: x is zero on air cells
+    double sv[kMaxDepth], av[kMaxDepth];
+    float bv[kMaxDepth];
+    uint8_t lb[kMaxDepth];
+    for_column(it, L.nx, L.ny, L.nz, [&](int k, int zz, int i) {
       double s = 0;
-      if (x > 0) s += X(i - 1);
-      if (x + 1 < L.nx) s += X(i + 1);
-      if (y > 0) s += X(i - sy);
-      if (y + 1 < L.ny) s += X(i + sy);
-      if (zz > 0) s += X(i - sz);
-      if (zz + 1 < L.nz) s += X(i + sz);
-      const double rv = double(B[i]) - (double(dg[i]) * X(i) - s);
+      s += x > 0 ? X(i - 1) : 0.0;
+      s += x + 1 < L.nx ? X(i + 1) : 0.0;
+      s += y > 0 ? X(i - sy) : 0.0;
+      s += y + 1 < L.ny ? X(i + sy) : 0.0;
+      s += zz > 0 ? X(i - sz) : 0.0;
+      s += zz + 1 < L.nz ? X(i + sz) : 0.0;
+      lb[k] = lab[i];
+      sv[k] = s;
+      av[k] = double(dg[i]) * X(i);
+      bv[k] = B[i];
+    });
+    for_column(it, L.nx, L.ny, L.nz, [&](int k, int, int i) {
+      if (!lb[k]) return;
+      const double rv = double(bv[k]) - (av[k] - sv[k]);
       r[i] = float(rv);
       rr += rv * rv;
       mr = fmax(mr, fabs(rv));
@@ -1256,6 +1186,7 @@ __global__ void k_hook_ctrl(const InstDev* insts, double sigma) {
   c->sigma = sigma;
   c->gamma = 1.0;
   c->status = 0;
+  c->dsel = 0;
 }
 
 }  // namespace fpp

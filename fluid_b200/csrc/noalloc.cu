@@ -38,6 +38,8 @@ double* g_scratch_ptr[kMaxDevices] = {};
 namespace fpp {
 void set_global_error(const std::string& message);   // read back by fluid_pp_last_error(NULL)
 
+constexpr int kNoAllocDepth = 4;   // cells per thread along z in the 32x8x4 work tiles
+
 // out = A p on the finest level and *p_dot_ap = p . A p (float64, tile order).
 // A is the ghost-fluid operator of k_spmv: diag on liquid cells, -1 to liquid
 // neighbours; air entries of p are treated as zero.
@@ -51,7 +53,7 @@ __global__ void k_spmv_noalloc(int nx, int ny, int nz, const uint8_t* __restrict
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     double dq = 0;
     int x, y, z, i;
-    for (TileIt it(t, nx, ny, nz, kMaxDepth); it.next(x, y, z, i);) {
+    for (TileIt it(t, nx, ny, nz, kNoAllocDepth); it.next(x, y, z, i);) {
       float q = 0.0f;
       if (label[i]) {
         auto nb = [&](bool in, int j) { return (in && label[j]) ? p[j] : 0.0f; };
@@ -81,7 +83,7 @@ extern "C" int fluid_pp_apply_operator_noalloc(int nx, int ny, int nz, const uns
     return FLUID_PP_INVALID_ARG;
   }
   const long long tiles = (long long)((nx + fpp::kTX - 1) / fpp::kTX) * ((ny + fpp::kTY - 1) / fpp::kTY) *
-                          ((nz + fpp::kMaxDepth - 1) / fpp::kMaxDepth);
+                          ((nz + fpp::kNoAllocDepth - 1) / fpp::kNoAllocDepth);
   if (tiles > kNoAllocMaxTiles || (long long)nx * ny * nz > (1LL << 30)) {
     fpp::set_global_error("fluid_pp_apply_operator_noalloc: lattice needs " + std::to_string(tiles) +
                     " work tiles of 32x8x4 cells; the fixed scratch holds " + std::to_string(kNoAllocMaxTiles));

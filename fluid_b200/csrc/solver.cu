@@ -17,7 +17,7 @@
 #include <vector>
 
 #include "../../include/fluid_pp.h"
-#include "kernels.cuh"
+#include "fused.cuh"
 #include "plan.h"
 #include "types.h"
 
@@ -82,11 +82,15 @@ struct fluid_pp_batch {
   List lvl[kMaxLevels];      // level-l tiles of instances for which l is not the coarsest
   List rst[kMaxLevels];      // level-(l+1) tiles of instances for which l is not the coarsest
   List crs[kMaxLevels];      // level-l tiles (l >= 1) of every instance having level l
+  List dn[kMaxLevels];       // fused down-step tiles (coarse tiles of level l+1) of grid level l
+  List up[kMaxLevels];       // fused up-step tiles (fine tiles of level l) of grid level l
+  List l0single;             // level-0 tiles of single-level instances
   List bake;
   List multi, single;        // instance lists (offsets into d_ilist) by coarsest level
   int maxL = 0;
   size_t smem_factor = 0;
   size_t smem_block = 0;
+  size_t smem_down = 0, smem_up = 0;
   std::string err;
   // CUDA graphs: setup, the device-side CG loop (conditional WHILE node), finish
   bool graphs_valid = false;
@@ -125,7 +129,9 @@ enum ProfStage {
   kPrRestrictC = FLUID_PP_STAGE_RESTRICTC, kPrCoarse = FLUID_PP_STAGE_COARSE, kPrProlong0 = FLUID_PP_STAGE_PROLONG0,
   kPrProlongC = FLUID_PP_STAGE_PROLONGC, kPrDot = FLUID_PP_STAGE_DOT, kPrDir = FLUID_PP_STAGE_DIR,
   kPrSpmv = FLUID_PP_STAGE_SPMV, kPrUpdate = FLUID_PP_STAGE_UPDATE, kPrTrue = FLUID_PP_STAGE_TRUE,
-  kPrGrad = FLUID_PP_STAGE_GRAD, kPrReceipt = FLUID_PP_STAGE_RECEIPT
+  kPrGrad = FLUID_PP_STAGE_GRAD, kPrReceipt = FLUID_PP_STAGE_RECEIPT, kPrDown0 = FLUID_PP_STAGE_DOWN0,
+  kPrDownC = FLUID_PP_STAGE_DOWNC, kPrUp0 = FLUID_PP_STAGE_UP0, kPrUpC = FLUID_PP_STAGE_UPC,
+  kPrDirSpmv = FLUID_PP_STAGE_DIRSPMV
 };
 
 std::atomic<unsigned long long> g_launches{0};
@@ -257,11 +263,51 @@ void vcycle_launch(fluid_pp_batch* B, int pre, int post) {
   }
 }
 
+// The default schedule (one sweep down, one up): per grid level one fused down
+// launch and one fused up launch; the level-0 up launch also forms gamma.
+template <class T>
+void vcycle_fused(fluid_pp_batch* B, int with_dot) {
+  cudaStream_t s = B->stream;
+  for (int l = 0; l + 1 < B->maxL; ++l) {
+    const List& Ld = B->dn[l];
+    if (!Ld.n) continue;
+    if (l == 0)
+      FPP_LAUNCH(B, kPrDown0, k_down<float, float, T, T><<<Ld.n, kFThreads, B->smem_down, s>>>(B->d_insts, tl(B, Ld), 0));
+    else
+      FPP_LAUNCH(B, kPrDownC, k_down<T, T, T, T><<<Ld.n, kFThreads, B->smem_down, s>>>(B->d_insts, tl(B, Ld), l));
+  }
+  if (B->multi.n)
+    FPP_LAUNCH(B, kPrCoarse, k_coarse_block<T><<<B->multi.n, kBlockThreads, B->smem_block, s>>>(
+                                 B->d_insts, il(B, B->multi), 1, 1));
+  if (B->single.n)
+    FPP_LAUNCH(B, kPrCoarse,
+               k_coarse_apply<float, float><<<B->single.n, kThreads, 0, s>>>(B->d_insts, il(B, B->single)));
+  for (int l = B->maxL - 2; l >= 0; --l) {
+    const List& Lu = B->up[l];
+    if (!Lu.n) continue;
+    if (l == 0)
+      FPP_LAUNCH(B, kPrUp0, k_up<float, float, T, T><<<Lu.n, kFThreads, B->smem_up, s>>>(B->d_insts, tl(B, Lu), 0,
+                                                                                          with_dot));
+    else
+      FPP_LAUNCH(B, kPrUpC, k_up<T, T, T, T><<<Lu.n, kFThreads, B->smem_up, s>>>(B->d_insts, tl(B, Lu), l, 0));
+  }
+  if (with_dot && B->l0single.n)
+    FPP_LAUNCH(B, kPrDot, k_dot_rz<<<launch_grid(B->l0single.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->l0single),
+                                                                                 B->l0single.n));
+}
+
 template <class T>
 void iter_launch(fluid_pp_batch* B, int pre, int post) {
   cudaStream_t s = B->stream;
   const Tile* t0 = tl(B, B->l0);
   const int n0 = B->l0.n, g = launch_grid(n0);
+  if (pre == 1 && post == 1) {
+    vcycle_fused<T>(B, 1);
+    FPP_LAUNCH(B, kPrDirSpmv, k_dirspmv<<<n0, kFThreads, 0, s>>>(B->d_insts, t0));
+    FPP_LAUNCH(B, kPrUpdate, k_update<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+    FPP_LAUNCH(B, kPrTrue, k_true_residual<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+    return;
+  }
   vcycle_launch<T>(B, pre, post);
   FPP_LAUNCH(B, kPrDot, k_dot_rz<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
   FPP_LAUNCH(B, kPrDir, k_dir<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
@@ -383,6 +429,19 @@ void set_global_error(const std::string& message) { g_err = message; }
 }  // namespace fpp
 
 // ==================================================================== batch
+template <class T>
+static cudaError_t set_fused_smem(size_t down, size_t up) {
+  auto set = [](const void* f, size_t bytes) {
+    return bytes > 48 * 1024 ? cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes))
+                             : cudaSuccess;
+  };
+  cudaError_t e = set((const void*)k_down<float, float, T, T>, down);
+  if (e == cudaSuccess) e = set((const void*)k_down<T, T, T, T>, down);
+  if (e == cudaSuccess) e = set((const void*)k_up<float, float, T, T>, up);
+  if (e == cudaSuccess) e = set((const void*)k_up<T, T, T, T>, up);
+  return e;
+}
+
 static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out, std::string& err) {
   if (!handles || count <= 0 || !out) {
     err = "batch needs at least one handle";
@@ -428,7 +487,19 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
     if (l + 1 < B->maxL)
       add_level(B->rst[l], [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; }, l + 1, true);
     if (l >= 1) add_level(B->crs[l], [l](const InstDev& I) { return l < I.nlev; }, l);
+    auto grid_level = [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; };
+    B->dn[l].off = int(tiles.size());
+    for (int k = 0; k < count; ++k)
+      if (grid_level(B->h[k]->inst))
+        for (int t = 0; t < B->h[k]->inst.lv[l].dtiles; ++t) tiles.push_back(Tile{k, l, t, 0});
+    B->dn[l].n = int(tiles.size()) - B->dn[l].off;
+    B->up[l].off = int(tiles.size());
+    for (int k = 0; k < count; ++k)
+      if (grid_level(B->h[k]->inst))
+        for (int t = 0; t < B->h[k]->inst.lv[l].utiles; ++t) tiles.push_back(Tile{k, l, t, 0});
+    B->up[l].n = int(tiles.size()) - B->up[l].off;
   }
+  add_level(B->l0single, [](const InstDev& I) { return I.nlev == 1; }, 0);
   B->bake.off = int(tiles.size());
   for (int k = 0; k < count; ++k) {
     const InstDev& I = B->h[k]->inst;
@@ -447,7 +518,13 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
   int mmax = 0;
   for (int k = 0; k < count; ++k) {
     mmax = std::max(mmax, B->h[k]->inst.coarse_m);
-    if (B->h[k]->inst.nlev > 1) B->smem_block = std::max(B->smem_block, size_t(B->h[k]->inst.block_smem));
+    const InstDev& I = B->h[k]->inst;
+    if (I.nlev > 1) B->smem_block = std::max(B->smem_block, size_t(I.block_smem));
+    for (int l = 0; l < I.first_block && l + 1 < I.nlev; ++l) {
+      const LevelDev &L = I.lv[l], &C = I.lv[l + 1];
+      B->smem_down = std::max(B->smem_down, size_t(down_smem_bytes(L.dcx, L.dcy, L.dcz, C.sx, C.sy, C.sz)));
+      B->smem_up = std::max(B->smem_up, size_t(up_smem_bytes(L.utx, L.uty, L.utz, C.sx, C.sy, C.sz)));
+    }
   }
   B->smem_factor = size_t(mmax) * mmax * sizeof(double);
 
@@ -480,6 +557,9 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
   if (e == cudaSuccess) e = set_smem((const void*)k_coarse_block<float>, B->smem_block);
   if (e == cudaSuccess) e = set_smem((const void*)k_coarse_block<__half>, B->smem_block);
   if (e == cudaSuccess) e = set_smem((const void*)k_coarse_block<__nv_bfloat16>, B->smem_block);
+  if (e == cudaSuccess) e = set_fused_smem<float>(B->smem_down, B->smem_up);
+  if (e == cudaSuccess) e = set_fused_smem<__half>(B->smem_down, B->smem_up);
+  if (e == cudaSuccess) e = set_fused_smem<__nv_bfloat16>(B->smem_down, B->smem_up);
   if (e != cudaSuccess) {
     err = std::string("batch setup: ") + cudaGetErrorString(e);
     fluid_pp_batch_destroy(B.release());
@@ -676,7 +756,7 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
     acc(sT * n);        // diagT
     acc((l == 0 ? 4 : sT) * n);   // z
     acc((l == 0 ? 4 : sT) * n);   // rhs / r
-    acc(sT * n);        // res
+    acc((l == 0 ? 4 : sT) * n);   // res (z type)
   }
   const long long nu = (long long)(nx + 1) * ny * nz, nv = (long long)nx * (ny + 1) * nz,
                   nw = (long long)nx * ny * (nz + 1);
@@ -684,7 +764,7 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
   acc(4 * nu);
   acc(4 * nv);
   acc(4 * nw);
-  for (int k = 0; k < 6; ++k) acc(4 * N);   // b x xlo d q p_si
+  for (int k = 0; k < 7; ++k) acc(4 * N);   // b x xlo d d2 q p_si
   if (N > (1LL << 30)) {
     g_err = "lattice exceeds 2^30 cells";
     return FLUID_PP_INVALID_ARG;
@@ -692,7 +772,7 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
   // Cells per thread along z: keep at least ~2 waves of fully occupied SMs
   // (148 x 2048 threads) in flight; small levels get one cell per thread.
   auto depth_of = [](long long n) { return n >= 4LL * 600000 ? 4 : n >= 2LL * 600000 ? 2 : 1; };
-  const int nt0 = tiles_of(nx, ny, nz, depth_of(N));
+  const int nt0 = tiles_of(nx, ny, nz, kMaxDepth);   // level 0: 32 x 8 x 8 tiles
   acc(sizeof(double) * kSlots * nt0);
   acc(sizeof(double) * ncoarse * ncoarse);
   acc(sizeof(Ctrl));
@@ -726,7 +806,7 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
     L.sy = plan.stride[l][1];
     L.sz = plan.stride[l][2];
     L.n = (long long)L.nx * L.ny * L.nz;
-    L.depth = depth_of(L.n);
+    L.depth = l == 0 ? kMaxDepth : depth_of(L.n);
     L.ntiles = tiles_of(L.nx, L.ny, L.nz, L.depth);
     // spacing ratio h_l / h_0 per axis (webgpu-uniform-pressure-multigrid.ts:588-589)
     const double rx = double(nx) / L.nx, ry = double(ny) / L.ny, rz = double(nz) / L.nz;
@@ -746,9 +826,35 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
     L.diagT = a.take(sT * n);
     L.z = a.take((l == 0 ? 4 : sT) * n);
     L.rhs = a.take((l == 0 ? 4 : sT) * n);
-    L.res = a.take(sT * n);
+    L.res = a.take((l == 0 ? 4 : sT) * n);
   }
   I.lv[plan.levels - 1].to_coarse = 1.0f;
+  // Fused-kernel tile shapes per grid level: the largest shape that still gives
+  // every SM two tiles (level 0's up step keeps the 32 x 8 x 8 tiles of the CG
+  // kernels, whose reduction partials it shares).
+  for (int l = 0; l + 1 < plan.levels; ++l) {
+    LevelDev& L = I.lv[l];
+    const LevelDev& Cl = I.lv[l + 1];
+    auto count = [](int n0, int n1, int n2, const int* t) {
+      return ((n0 + t[0] - 1) / t[0]) * ((n1 + t[1] - 1) / t[1]) * ((n2 + t[2] - 1) / t[2]);
+    };
+    static const int dshape[5][3] = {{16, 4, 4}, {8, 4, 4}, {8, 4, 2}, {8, 2, 2}, {4, 2, 2}};
+    for (const auto& t : dshape) {
+      L.dcx = t[0];
+      L.dcy = t[1];
+      L.dcz = t[2];
+      L.dtiles = count(Cl.nx, Cl.ny, Cl.nz, t);
+      if (L.dtiles >= 2 * 148) break;
+    }
+    static const int ushape[5][3] = {{kTX, kTY, kMaxDepth}, {32, 8, 4}, {16, 8, 4}, {16, 4, 4}, {8, 4, 4}};
+    for (const auto& t : ushape) {
+      L.utx = t[0];
+      L.uty = t[1];
+      L.utz = t[2];
+      L.utiles = count(L.nx, L.ny, L.nz, t);
+      if (l == 0 || L.utiles >= 2 * 148) break;
+    }
+  }
   // The single-CTA coarse block takes every level from the first one (>= 1) that
   // fits kCoarseBlockCells and whose tail of levels fits the shared-memory budget.
   I.first_block = plan.levels;
@@ -772,6 +878,7 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
   I.x = static_cast<float*>(a.take(4 * N));
   I.xlo = static_cast<float*>(a.take(4 * N));
   I.d = static_cast<float*>(a.take(4 * N));
+  I.d2 = static_cast<float*>(a.take(4 * N));
   I.q = static_cast<float*>(a.take(4 * N));
   I.p_si = static_cast<float*>(a.take(4 * N));
   I.partial = static_cast<double*>(a.take(sizeof(double) * kSlots * nt0));
@@ -972,10 +1079,11 @@ int fluid_pp_apply_vcycle(fluid_pp* pp, const float* r, float* z, int pre, int p
   const double sigma = per > 1e-300 ? 1.0 / std::sqrt(per) : 1.0;
   cudaMemcpyAsync(pp->inst.lv[0].rhs, r, 4 * N, cudaMemcpyHostToDevice, B->stream);
   k_hook_ctrl<<<1, 1, 0, B->stream>>>(B->d_insts, sigma);
+  const bool fused = pre == 1 && post == 1;
   switch (B->precision) {
-    case FLUID_PP_FP16: vcycle_launch<__half>(B, pre, post); break;
-    case FLUID_PP_BF16: vcycle_launch<__nv_bfloat16>(B, pre, post); break;
-    default: vcycle_launch<float>(B, pre, post);
+    case FLUID_PP_FP16: fused ? vcycle_fused<__half>(B, 0) : vcycle_launch<__half>(B, pre, post); break;
+    case FLUID_PP_BF16: fused ? vcycle_fused<__nv_bfloat16>(B, 0) : vcycle_launch<__nv_bfloat16>(B, pre, post); break;
+    default: fused ? vcycle_fused<float>(B, 0) : vcycle_launch<float>(B, pre, post);
   }
   cudaMemcpyAsync(z, pp->inst.lv[0].z, 4 * N, cudaMemcpyDeviceToHost, B->stream);
   cudaError_t e = cudaStreamSynchronize(B->stream);

@@ -7,7 +7,7 @@
 namespace fpp {
 
 constexpr int kThreads = 256;      // threads per CTA for the grid kernels
-constexpr int kTile = 1024;        // cells per work tile (4 per thread)
+constexpr int kFThreads = 512;     // threads per CTA for the fused shared-memory kernels
 constexpr int kMaxCoarse = 128;    // largest coarsest level solved densely
 constexpr int kSlots = 6;          // reduction quantities per stage
 constexpr int kCoarseBlockCells = 4096;          // levels this small run inside one CTA
@@ -45,7 +45,8 @@ struct Ctrl {
   int anchored;       // finest system has a Dirichlet contact
   int converged;
   unsigned arrive[8]; // per-stage completion counters (self-resetting)
-  int pad[2];
+  int dsel;           // which of d / d2 holds the current search direction
+  int pad;
 };
 
 struct LevelDev {
@@ -54,6 +55,10 @@ struct LevelDev {
   long long n;
   int ntiles;
   int depth;          // cells per thread along z in this level's work tiles
+  int dcx, dcy, dcz;  // fused down step l -> l+1: coarse cells per tile (level l+1 units)
+  int dtiles;         // tiles of that step
+  int utx, uty, utz;  // fused up step l+1 -> l: fine cells per tile
+  int utiles;
   float wx, wy, wz;   // normalised off-diagonal weights w_a / wmax
   float wmax;         // (h0 / h_a)^2 maximum over axes; level operators are stored divided by it
   float ext_phi;      // open-top exterior phi (finest-cell units)
@@ -64,7 +69,7 @@ struct LevelDev {
   void* diagT;        // normalised diagonal in the storage type (smoother)
   void* z;            // level solution (level 0: float CG vector)
   void* rhs;          // level right-hand side (level 0: the CG residual r, float)
-  void* res;          // level residual in the storage type
+  void* res;          // scratch in the z type: the pre-smoothed z between the fused down and up steps
 };
 
 struct InstDev {
@@ -85,7 +90,8 @@ struct InstDev {
   float* b;           // right-hand side, finest-cell units
   float* x;           // pressure, finest-cell units: x + xlo is a double-single value
   float* xlo;         // low part of the double-single pressure
-  float* d;           // search direction
+  float* d;           // search direction (double-buffered with d2, see Ctrl::dsel)
+  float* d2;
   float* q;           // A d
   float* p_si;        // pressure output in Pa
   double* partial;    // kSlots * ntiles0 per-tile reduction partials

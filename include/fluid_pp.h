@@ -51,9 +51,10 @@ enum fluid_pp_stage {
   FLUID_PP_STAGE_RESIDUAL0, FLUID_PP_STAGE_RESIDUALC, FLUID_PP_STAGE_RESTRICT0, FLUID_PP_STAGE_RESTRICTC,
   FLUID_PP_STAGE_COARSE, FLUID_PP_STAGE_PROLONG0, FLUID_PP_STAGE_PROLONGC, FLUID_PP_STAGE_DOT,
   FLUID_PP_STAGE_DIR, FLUID_PP_STAGE_SPMV, FLUID_PP_STAGE_UPDATE, FLUID_PP_STAGE_TRUE, FLUID_PP_STAGE_GRAD,
-  FLUID_PP_STAGE_RECEIPT
+  FLUID_PP_STAGE_RECEIPT, FLUID_PP_STAGE_DOWN0, FLUID_PP_STAGE_DOWNC, FLUID_PP_STAGE_UP0, FLUID_PP_STAGE_UPC,
+  FLUID_PP_STAGE_DIRSPMV
 };
-#define FLUID_PP_PROFILE_STAGES 22
+#define FLUID_PP_PROFILE_STAGES 27
 
 typedef struct fluid_pp fluid_pp;
 typedef struct fluid_pp_batch fluid_pp_batch;

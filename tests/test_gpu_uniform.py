@@ -110,6 +110,16 @@ def test_project_matches_oracle(name, precision):
     _check_projection(s, precision, rec, pp, o)
 
 
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+@pytest.mark.parametrize("name", ["dam32", "semi2x64x48"])
+def test_project_two_sweep_schedule(name, precision):
+    """Two sweeps down and up run the per-pass grid kernels instead of the fused ones."""
+    s = CASES[name]()
+    pp, o = _pair(s, precision)
+    rec = pp.project(s.dt, rel_tol=REL_RES, rel_tol_inf=0.5 * DIV_RATIO, pre_sweeps=2, post_sweeps=2)
+    _check_projection(s, precision, rec, pp, o)
+
+
 @pytest.mark.parametrize("name", ["dam32", "odd37x50x29", "open_top24"])
 def test_project_at_l2_tolerance(name):
     """At the benchmark's operating point (L2 criterion only) the max-norm ratio stays near 1e-6."""
