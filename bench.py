@@ -1,23 +1,31 @@
-"""Benchmark: MGPCG pressure-projection solves/s on one B200 (and N replicas).
+"""Benchmark: MGPCG solves/s on one B200 (and N replicas): mixed/batched vs plain FP32.
 
-Workload (one "step" = one projection): the 128x96x128 dam break with 16
-falling spheres, consecutive steps at dt = 1/60 s, each with its own seeded
-velocity field, solved to relative residual 1e-6 with the mixed-precision
-solver (float16 V-cycle levels, float32 CG vectors, float64 dots/scalars).
-Inputs are resident in HBM before timing; L2 is flushed (a 256 MB write)
-between timed steps; every step is timed with CUDA events on the launching
-stream.  The same steps are also timed with the plain float32 solver, through
-the public API with host buffers (e2e), and with per-stage kernel events for
-the roofline.
+Headline workload (one "step" = one batched projection): 64 independent
+uniform MAC grids of uneven size (edges log-uniform in 24-128 per axis, liquid
+= seeded unions of 1-6 boxes and spheres filling 20-70%, Gaussian velocities
+sigma 0.2 m/s), all projected to relative residual 1e-6 by one batched solve
+(one launch per stage for every instance, CUDA graphs with a device-side
+loop) with float16 V-cycle levels, float32 CG vectors and float64 dots.  The
+comparator is plain float32 single-solve MGPCG over the same 64 instances, one
+handle after the other.  Secondary: the 128x96x128 dam break with 16 spheres
+(consecutive steps), mixed vs plain, single solve.
+
+Inputs are resident in HBM before timing (the timed step re-uploads each
+instance's state device-to-device, as a simulation step hands over its
+advected state); L2 is flushed (256 MB write) before every timed step; every
+step is timed with CUDA events on the launching stream.  `e2e` repeats the
+headline through the public API from pinned host buffers with the results read
+back to the host.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Under torchrun (N > 1) every rank runs its own replica (the path does not
-shard within a solve): value = all solves / max-over-ranks time.
+Under torchrun (N > 1) every rank runs its own replica (a solve does not
+shard): value = all solves / max-over-ranks time.
 """
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import os
 import statistics
@@ -31,8 +39,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "MGPCG solves/s @rel-res 1e-6: mixed/batched vs plain FP32 on 1 B200; p50/p99 ms"
-WORKLOAD = "dam break + 16 falling spheres, 128x96x128 uniform MAC grid, dt=1/60, rel-res 1e-6"
+WORKLOAD = ("64 independent uniform MAC grids in one batched projection per step: edges log-uniform 24-128 "
+            "per axis, liquid = 1-6 seeded boxes/spheres filling 20-70%, Gaussian velocities sigma 0.2 m/s, "
+            "rel-res 1e-6 per instance")
+WORKLOAD2 = "dam break + 16 falling spheres, 128x96x128 uniform MAC grid, dt=1/60, rel-res 1e-6"
 L2_FLUSH_BYTES = 256 << 20
+BATCH = 64
+
 
 # Algorithmic bytes per finest cell of one launch, by kernel stage (s = bytes of
 # the V-cycle storage type): every array a launch touches counts once at its
@@ -40,7 +53,6 @@ L2_FLUSH_BYTES = 256 << 20
 def stage_bytes_per_cell(stage: str, s: int) -> float:
     return {
         "smooth0": 4 + 4 + s + 1 + 2,          # z, r, diag(s), label in; half of z out
-        "residual0": 4 + 4 + s + 1 + s,        # z, r, diag, label in; residual out
         "restrict0": 4 + 4 + s + 1 + (s + 1) / 8.0,   # z, r, diag, label in; coarse label in, coarse rhs out
         "prolong0": 4 + 4 + 1 + s / 8.0,       # z in/out, label, coarse z
         "spmv": 4 + 4 + 1 + 4,                 # d, diag, label in; q out
@@ -54,8 +66,8 @@ def stage_bytes_per_cell(stage: str, s: int) -> float:
     }.get(stage, 0.0)
 
 
-# DRAM bytes per launch of the dominant kernel from the committed ncu capture
-# (profiles/); None until a capture of the current kernel exists.
+# DRAM bytes per launch of a stage's kernel on the 128x96x128 workload, from the
+# committed ncu captures (profiles/); absent until a capture of the current kernel exists.
 NCU_TRAFFIC_BYTES = {}
 
 
@@ -121,66 +133,77 @@ def dist_setup():
 
 
 def reference_arm(args):
-    """The reference's CPU path (float64 Jacobi-PCG of the atlas oracle), all host threads."""
+    """The reference's CPU path (float64 Jacobi-PCG of the atlas oracle) on the headline
+    workload, all host threads.  Each step solves a bounded sample of the 64 instances
+    (step k solves instances 4k .. 4k+3 mod 64) and the metric counts solves."""
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
     from fluid_b200 import configs
     from oracle.oracle import Oracle
     threads = os.cpu_count() or 1
-    times = []
-    iters = []
-    total = args.warmup + args.steps
-    o = None
-    for k in range(total):
-        s = configs.dam_spheres(step=k % 50)
-        if o is None:
+    insts = configs.batch_instances(BATCH)
+    per_step = 4
+    times, iters = [], []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        for j in range(per_step):
+            s = insts[(k * per_step + j) % BATCH]
             o = Oracle(s.nx, s.ny, s.nz, s.h, s.rho)
             o.set_threads(threads)
-        o.set_state(s.vof, s.u, s.v, s.w, s.dt)
-        t0 = time.perf_counter()
-        _, info = o.solve_jacobi(1e-6, 0.0)
+            o.set_state(s.vof, s.u, s.v, s.w, s.dt)
+            _, info = o.solve_jacobi(1e-6, 0.0)
+            iters.append(info["iterations"])
         dt = time.perf_counter() - t0
         if k >= args.warmup:
             times.append(dt)
-            iters.append(info["iterations"])
     tot = sum(times)
-    value = len(times) / tot
+    value = per_step * len(times) / tot
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "cells": 128 * 96 * 128, "solver": "Jacobi-PCG float64 (atlas oracle)"},
+        "config": {"workload": WORKLOAD, "instances": BATCH, "cells": int(sum(s.cells for s in insts)),
+                   "solver": "Jacobi-PCG float64 (atlas oracle), one instance after another"},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
-                         "sample": f"{len(times)} full solves of consecutive steps, rel-res 1e-6, "
-                                   f"mean {statistics.mean(iters):.0f} PCG iterations"},
+                         "sample": f"{per_step} of the 64 instances per step (rotating), full solves to rel-res "
+                                   f"1e-6, mean {statistics.mean(iters):.0f} PCG iterations, OpenMP"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "p50_ms": 1000 * statistics.median(times), "p99_ms": 1000 * float(np.percentile(times, 99)),
+        "p50_ms": 1000 * statistics.median(times) / per_step,
+        "p99_ms": 1000 * float(np.percentile(times, 99)) / per_step,
     }
     print(json.dumps(line))
     return 0
 
 
-def cpu_baseline_sample():
-    from fluid_b200 import configs
+def cpu_baseline_sample(insts):
+    """The oracle's float64 Jacobi-PCG on 4 of the 64 headline instances, all host threads."""
     from oracle.oracle import Oracle
     threads = os.cpu_count() or 1
-    s = configs.dam_spheres(step=0)
-    o = Oracle(s.nx, s.ny, s.nz, s.h, s.rho)
-    o.set_threads(threads)
-    o.set_state(s.vof, s.u, s.v, s.w, s.dt)
     t0 = time.perf_counter()
-    _, info = o.solve_jacobi(1e-6, 0.0)
+    its = []
+    for s in insts[:4]:
+        o = Oracle(s.nx, s.ny, s.nz, s.h, s.rho)
+        o.set_threads(threads)
+        o.set_state(s.vof, s.u, s.v, s.w, s.dt)
+        _, info = o.solve_jacobi(1e-6, 0.0)
+        its.append(int(info["iterations"]))
     dt = time.perf_counter() - t0
-    return {"value": 1.0 / dt, "unit": "solves/s", "cores": threads, "kind": "port",
-            "sample": f"1 full solve of step 0 (float64 Jacobi-PCG, {int(info['iterations'])} iterations, "
-                      f"rel-res 1e-6) on the host, OpenMP"}
+    return {"value": 4 / dt, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"instances 0-3 of the 64 ({sum(s.cells for s in insts[:4])} cells), float64 Jacobi-PCG "
+                      f"to rel-res 1e-6 ({its} iterations), OpenMP on the host"}
+
+
+def note(msg: str):
+    """Progress on stderr (stdout carries only the JSON line)."""
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
 
 
 def main():
+    faulthandler.enable()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16", "bf16"])
@@ -194,7 +217,7 @@ def main():
 
     import torch
 
-    from fluid_b200 import PressureProjector, configs
+    from fluid_b200 import BatchProjector, PressureProjector, _abi, configs
     from fluid_b200.projector import kernel_launches
 
     world, rank, local = dist_setup()
@@ -205,126 +228,212 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     stream = torch.cuda.current_stream()
-    total = args.warmup + args.steps
-    # 50 consecutive simulation steps; timed steps cycle through them
-    states = [configs.dam_spheres(step=k) for k in range(min(total, 50))]
-    nst = len(states)
-    s0 = states[0]
-    dev = [tuple(torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (s.vof, s.u, s.v, s.w)) for s in states]
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     opts = dict(rel_tol=1e-6, pre_sweeps=args.sweeps, post_sweeps=args.sweeps)
+    total = args.warmup + args.steps
 
-    def run(precision, profile=False):
-        pp = PressureProjector((s0.nx, s0.ny, s0.nz), s0.h, s0.rho, precision=precision, device=local)
-        pp.set_stream(stream.cuda_stream)
-        pp.set_profiling(profile)
-        times, recs = [], []
-        for k in range(total):
-            flush.zero_()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            pp.upload_state_device(*(t.data_ptr() for t in dev[k % nst]))
-            rec = pp.project(states[k % nst].dt, **opts)
-            b.record(stream)
-            b.synchronize()
+    def max_over_ranks(ms):
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            return float(t.item())
+        return ms
+
+    def timed(fn):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        out = fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b), out
+
+    # ------------------------------------------------------------ headline: batched
+    note("generating the 64 instances")
+    insts = configs.batch_instances(BATCH)
+    cells = int(sum(s.cells for s in insts))
+    dev = [tuple(torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (s.vof, s.u, s.v, s.w)) for s in insts]
+    dts = [s.dt for s in insts]
+
+    def make(precision):
+        pps = [PressureProjector((s.nx, s.ny, s.nz), s.h, s.rho, precision=precision, device=local) for s in insts]
+        for p in pps:
+            p.set_stream(stream.cuda_stream)
+        return pps
+
+    def upload_dev(pps):
+        for p, d in zip(pps, dev):
+            p.upload_state_device(*(t.data_ptr() for t in d))
+
+    def run_batched(precision, steps, profile=False):
+        pps = make(precision)
+        B = BatchProjector(pps)
+        B.set_profiling(profile)
+        times, recs = [], None
+
+        def step():
+            upload_dev(pps)
+            return B.project(dts, **opts)
+        for k in range(args.warmup + steps):
+            ms, recs = timed(step)
             if k >= args.warmup:
-                times.append(a.elapsed_time(b))
-                recs.append(rec)
-            if k == args.warmup - 1 and profile:
-                pp.profile(reset=True)
-        prof = pp.profile(reset=True) if profile else None
-        pp.destroy()
+                times.append(ms)
+            if profile and k == args.warmup - 1:
+                B.profile(reset=True)
+        prof = B.profile(reset=True) if profile else None
+        B.destroy()
+        for p in pps:
+            p.destroy()
         return times, recs, prof
 
-    # timed region: mixed precision (headline)
+    def run_single_sequence(precision, steps):
+        pps = make(precision)
+        times, recs = [], None
+
+        def step():
+            out = []
+            for p, d, s in zip(pps, dev, insts):
+                p.upload_state_device(*(t.data_ptr() for t in d))
+                out.append(p.project(s.dt, **opts))
+            return out
+        for k in range(args.warmup + steps):
+            ms, recs = timed(step)
+            if k >= args.warmup:
+                times.append(ms)
+        for p in pps:
+            p.destroy()
+        return times, recs
+
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     l0 = kernel_launches()
+    note("headline: batched mixed")
     with ClockSampler(local) as clk:
-        times, recs, _ = run(args.precision)
+        times, recs, _ = run_batched(args.precision, args.steps)
     torch.cuda.synchronize()
     launches = kernel_launches() - l0
-    tot_ms = sum(times)
-    if world > 1:
-        t = torch.tensor([tot_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        tot_ms = float(t.item())
-    value = world * args.steps / (tot_ms / 1000.0)
+    tot_ms = max_over_ranks(sum(times))
+    value = world * BATCH * args.steps / (tot_ms / 1000.0)
     bad = [r for r in recs if r["status_name"] != "OK" or r["true_rel_residual"] > 1e-6]
 
-    # plain float32 on the same steps
-    times32, recs32, _ = run("fp32")
-    plain = args.steps / (sum(times32) / 1000.0)
+    plain_steps = max(3, args.steps // 5)
+    note("plain fp32 single-solve sequence")
+    times_plain, _ = run_single_sequence("fp32", plain_steps)
+    note("batched fp32")
+    plain = BATCH * len(times_plain) / (sum(times_plain) / 1000.0)
+    times_b32, _, _ = run_batched("fp32", plain_steps)
+    batched32 = BATCH * len(times_b32) / (sum(times_b32) / 1000.0)
 
-    # per-stage kernel events on the same steps (roofline)
-    _, _, prof = run(args.precision, profile=True)
+    # ------------------------------------------------ secondary: 128x96x128 single
+    steps2 = min(args.steps, 50)
+    note("128x96x128 single solves")
+    states = [configs.dam_spheres(step=k) for k in range(min(args.warmup + steps2, 50))]
+    nst = len(states)
+    s0 = states[0]
+    dev2 = [tuple(torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (s.vof, s.u, s.v, s.w)) for s in states]
+
+    def run_single(precision, profile=False):
+        pp = PressureProjector((s0.nx, s0.ny, s0.nz), s0.h, s0.rho, precision=precision, device=local)
+        pp.set_stream(stream.cuda_stream)
+        pp.set_profiling(profile)
+        tt, rr = [], []
+        for k in range(args.warmup + steps2):
+            st, d2 = states[k % nst], dev2[k % nst]
+
+            def step():
+                pp.upload_state_device(*(t.data_ptr() for t in d2))
+                return pp.project(st.dt, **opts)
+            ms, rec = timed(step)
+            if k >= args.warmup:
+                tt.append(ms)
+                rr.append(rec)
+            if profile and k == args.warmup - 1:
+                pp.profile(reset=True)
+        prof = pp.profile(reset=True) if profile else None
+        pp.destroy()
+        return tt, rr, prof
+
+    t2_mixed, r2_mixed, _ = run_single(args.precision)
+    t2_plain, _, _ = run_single("fp32")
+    # per-stage kernel events for the roofline (direct launches of the same solves)
+    _, _, prof = run_single(args.precision, profile=True)
     sbytes = 4 if args.precision == "fp32" else 2
-    ncell = s0.cells
+    ncell2 = s0.cells
     stages = {k: v for k, v in prof.items() if stage_bytes_per_cell(k, sbytes) > 0}
     dom = max(stages, key=lambda k: stages[k]["ms"])
     per_launch_ms = prof[dom]["ms"] / prof[dom]["launches"]
-    alg = stage_bytes_per_cell(dom, sbytes) * ncell
+    alg = stage_bytes_per_cell(dom, sbytes) * ncell2
     hbm, peak_kind = peaks()
     achieved = alg / (per_launch_ms / 1000.0) / 1e9
     tot_prof = sum(v["ms"] for v in prof.values())
     traffic = NCU_TRAFFIC_BYTES.get(dom)
 
-    # end to end through the public API with pinned host buffers
-    pp = PressureProjector((s0.nx, s0.ny, s0.nz), s0.h, s0.rho, precision=args.precision, device=local)
-    pp.set_stream(stream.cuda_stream)
+    # ------------------------------------------- e2e: public API from host buffers
+    note("e2e from host buffers")
+    pps = make(args.precision)
+    B = BatchProjector(pps)
     host_in = [tuple(torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (s.vof, s.u, s.v, s.w))
-               for s in states]
-    host_out = tuple(torch.empty(sh, dtype=torch.float32).pin_memory()
-                     for sh in ((s0.nz, s0.ny, s0.nx), (s0.nz, s0.ny, s0.nx + 1), (s0.nz, s0.ny + 1, s0.nx),
-                                (s0.nz + 1, s0.ny, s0.nx)))
-    h2d = sum(t.numel() * 4 for t in host_in[0])
-    d2h = sum(t.numel() * 4 for t in host_out)
-    from fluid_b200 import _abi
+               for s in insts]
+    host_out = [tuple(torch.empty(sh, dtype=torch.float32).pin_memory()
+                      for sh in ((s.nz, s.ny, s.nx), (s.nz, s.ny, s.nx + 1), (s.nz, s.ny + 1, s.nx),
+                                 (s.nz + 1, s.ny, s.nx))) for s in insts]
+    h2d = sum(t.numel() * 4 for tup in host_in for t in tup)
+    d2h = sum(t.numel() * 4 for tup in host_out for t in tup)
     L = _abi.load()
+
+    def e2e_step():
+        for p, hi in zip(pps, host_in):
+            p.upload_state(*(t.numpy() for t in hi))
+        out = B.project(dts, **opts)
+        for p, ho in zip(pps, host_out):
+            L.fluid_pp_download(p.handle, *(_abi.ptr(t.numpy()) for t in ho))
+        return out
     e2e_ms = []
     for k in range(total):
-        flush.zero_()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        pp.upload_state(*(t.numpy() for t in host_in[k % nst]))
-        pp.project(states[k % nst].dt, **opts)
-        L.fluid_pp_download(pp.handle, *(_abi.ptr(t.numpy()) for t in host_out))
-        b.record(stream)
-        b.synchronize()
+        ms, _ = timed(e2e_step)
         if k >= args.warmup:
-            e2e_ms.append(a.elapsed_time(b))
-    pp.destroy()
-    e2e_tot = sum(e2e_ms)
-    if world > 1:
-        t = torch.tensor([e2e_tot], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_tot = float(t.item())
-    e2e_value = world * args.steps / (e2e_tot / 1000.0)
+            e2e_ms.append(ms)
+    B.destroy()
+    for p in pps:
+        p.destroy()
+    e2e_value = world * BATCH * len(e2e_ms) / (max_over_ranks(sum(e2e_ms)) / 1000.0)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample()
+        note("cpu baseline sample")
+        cpu = cpu_baseline_sample(insts)
 
     its = [r["iterations"] for r in recs]
+    cell_its = sum(s.cells * r["iterations"] for s, r in zip(insts, recs))
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "cells": ncell, "precision": f"{args.precision} V-cycle levels, f32 CG "
-                   "vectors, f64 dots/scalars/coarsest", "sweeps": args.sweeps, "l2": "flushed between steps (256 MB write)",
+        "config": {"workload": WORKLOAD, "instances": BATCH, "cells": cells, "seed": 4,
+                   "precision": f"{args.precision} V-cycle levels, f32 CG vectors, f64 dots/scalars/coarsest",
+                   "sweeps": args.sweeps, "l2": "flushed before every timed step (256 MB write)",
                    "parallelism": f"{world} replicas" if world > 1 else "single GPU"},
         "p50_ms": statistics.median(times), "p99_ms": float(np.percentile(times, 99)),
-        "iterations_mean": statistics.mean(its),
-        "cell_iterations_per_s": ncell * statistics.mean(its) * value,
-        "plain_fp32_solves_per_s": plain, "plain_fp32_p50_ms": statistics.median(times32),
-        "mixed_vs_plain": value / (world * plain),
+        "iterations_min_max": [min(its), max(its)],
+        "cell_iterations_per_s": world * cell_its * args.steps / (tot_ms / 1000.0),
+        "plain_fp32_single_solves_per_s": plain,
+        "plain_fp32_single_p50_ms_per_64": statistics.median(times_plain),
+        "batched_fp32_solves_per_s": batched32,
+        "mixed_batched_vs_plain_single": value / (world * plain),
         "failed_solves": len(bad),
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
-                     "alg_bytes_per_launch": alg, "launch_ms": per_launch_ms,
-                     "share_of_step": prof[dom]["ms"] / tot_prof},
-        "stage_ms_per_step": {k: round(v["ms"] / args.steps, 4) for k, v in sorted(prof.items())},
+        "dam_spheres_128x96x128": {
+            "workload": WORKLOAD2, "steps": steps2,
+            "mixed_solves_per_s": len(t2_mixed) / (sum(t2_mixed) / 1000.0),
+            "plain_fp32_solves_per_s": len(t2_plain) / (sum(t2_plain) / 1000.0),
+            "mixed_p50_ms": statistics.median(t2_mixed), "mixed_p99_ms": float(np.percentile(t2_mixed, 99)),
+            "iterations_mean": statistics.mean(r["iterations"] for r in r2_mixed),
+            "stage_ms_per_solve": {k: round(v["ms"] / steps2, 4) for k, v in sorted(prof.items())},
+        },
+        "roofline": {"bound": "hbm", "kernel": dom, "workload": "dam_spheres_128x96x128 (one instance per launch)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": peak_kind, "traffic": traffic, "alg_bytes_per_launch": alg,
+                     "launch_ms": per_launch_ms, "share_of_step": prof[dom]["ms"] / tot_prof},
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),

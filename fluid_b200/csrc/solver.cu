@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -88,6 +89,7 @@ struct fluid_pp_batch {
   List bake;
   List multi, single;        // instance lists (offsets into d_ilist) by coarsest level
   int maxL = 0;
+  cudaError_t launch_err = cudaSuccess;   // first failed launch since the last check
   size_t smem_factor = 0;
   size_t smem_block = 0;
   size_t smem_down = 0, smem_up = 0;
@@ -178,12 +180,22 @@ namespace {
 
 // Every launch goes through FPP_LAUNCH: it counts the launch and, when the
 // batch is profiling, brackets it with CUDA events on the launching stream.
-#define FPP_LAUNCH(B, stage, ...)   \
-  do {                              \
-    prof_begin(B, stage);           \
-    __VA_ARGS__;                    \
-    prof_end(B, stage);             \
+#define FPP_LAUNCH(B, stage, ...)                                  \
+  do {                                                             \
+    prof_begin(B, stage);                                          \
+    __VA_ARGS__;                                                   \
+    const cudaError_t launch_e_ = cudaGetLastError();              \
+    if (launch_e_ != cudaSuccess && (B)->launch_err == cudaSuccess) \
+      (B)->launch_err = launch_e_;                                 \
+    prof_end(B, stage);                                            \
   } while (0)
+
+// Returns and clears the first launch error recorded on the batch.
+cudaError_t take_launch_error(fluid_pp_batch* B) {
+  const cudaError_t e = B->launch_err;
+  B->launch_err = cudaSuccess;
+  return e;
+}
 
 template <class T>
 void setup_launch(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
@@ -372,6 +384,7 @@ int ensure_graphs(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
     setup_launch<T>(B, o);
     B->n_setup = g_launches.load() - c0;
     e = cudaStreamEndCapture(cs, &B->g_setup);
+    if (e == cudaSuccess) e = take_launch_error(B);
   }
   // loop
   cudaGraphConditionalHandle handle{};
@@ -393,8 +406,11 @@ int ensure_graphs(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
     iter_launch<T>(B, o.pre_sweeps, o.post_sweeps);
     const unsigned cap = unsigned(o.max_iters + 2);
     k_loop_cond<<<1, 256, 0, cs>>>(B->d_insts, n, B->d_loop, cap, handle);
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess && B->launch_err == cudaSuccess) B->launch_err = le;
     B->n_body = g_launches.load() - c0 + 1;
     e = cudaStreamEndCapture(cs, &body);
+    if (e == cudaSuccess) e = take_launch_error(B);
   }
   // finish
   if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
@@ -403,12 +419,14 @@ int ensure_graphs(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
     finish_launch_any(B);
     B->n_finish = g_launches.load() - c0;
     e = cudaStreamEndCapture(cs, &B->g_finish);
+    if (e == cudaSuccess) e = take_launch_error(B);
   }
   if (e == cudaSuccess) e = cudaGraphInstantiate(&B->x_setup, B->g_setup, 0);
   if (e == cudaSuccess) e = cudaGraphInstantiate(&B->x_loop, B->g_loop, 0);
   if (e == cudaSuccess) e = cudaGraphInstantiate(&B->x_finish, B->g_finish, 0);
   // captured launches did not execute
   g_launches.store(before);
+  take_launch_error(B);
   B->stream = saved;
   B->profiling = prof;
   cudaStreamDestroy(cs);
@@ -429,16 +447,46 @@ void set_global_error(const std::string& message) { g_err = message; }
 }  // namespace fpp
 
 // ==================================================================== batch
+// Dynamic shared memory limits are a property of the kernel function, shared by
+// every handle in the process: they are set once per device to the most any
+// instance can ask for (the largest tile shapes over every stride pattern, the
+// largest dense coarsest level, the coarse-block budget), never lowered.
 template <class T>
-static cudaError_t set_fused_smem(size_t down, size_t up) {
+static cudaError_t configure_kernels_t(size_t factor, size_t block, size_t down, size_t up) {
   auto set = [](const void* f, size_t bytes) {
     return bytes > 48 * 1024 ? cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes))
                              : cudaSuccess;
   };
-  cudaError_t e = set((const void*)k_down<float, float, T, T>, down);
+  cudaError_t e = set((const void*)k_coarse_factor<T>, factor);
+  if (e == cudaSuccess) e = set((const void*)k_coarse_block<T>, block);
+  if (e == cudaSuccess) e = set((const void*)k_down<float, float, T, T>, down);
   if (e == cudaSuccess) e = set((const void*)k_down<T, T, T, T>, down);
   if (e == cudaSuccess) e = set((const void*)k_up<float, float, T, T>, up);
   if (e == cudaSuccess) e = set((const void*)k_up<T, T, T, T>, up);
+  return e;
+}
+
+static std::mutex g_cfg_mutex;
+static bool g_cfg_done[64] = {};
+
+static cudaError_t configure_kernels() {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(g_cfg_mutex);
+  if (dev >= 0 && dev < 64 && g_cfg_done[dev]) return cudaSuccess;
+  size_t down = 0, up = 0;
+  for (int m = 0; m < 8; ++m) {
+    const int sx = (m & 1) ? 2 : 1, sy = (m & 2) ? 2 : 1, sz = (m & 4) ? 2 : 1;
+    down = std::max(down, size_t(down_smem_bytes(16, 4, 4, sx, sy, sz)));
+    up = std::max(up, size_t(up_smem_bytes(kTX, kTY, kMaxDepth, sx, sy, sz)));
+  }
+  const size_t factor = size_t(kMaxCoarse) * kMaxCoarse * sizeof(double);
+  const size_t block = kCoarseBlockSmem;
+  e = configure_kernels_t<float>(factor, block, down, up);
+  if (e == cudaSuccess) e = configure_kernels_t<__half>(factor, block, down, up);
+  if (e == cudaSuccess) e = configure_kernels_t<__nv_bfloat16>(factor, block, down, up);
+  if (e == cudaSuccess && dev >= 0 && dev < 64) g_cfg_done[dev] = true;
   return e;
 }
 
@@ -547,19 +595,7 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
   if (e == cudaSuccess) e = cudaMalloc(&B->d_loop, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMemset(B->d_loop, 0, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMallocHost(&B->h_loop, sizeof(unsigned));
-  auto set_smem = [](const void* f, size_t bytes) {
-    return bytes > 48 * 1024 ? cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes))
-                             : cudaSuccess;
-  };
-  if (e == cudaSuccess) e = set_smem((const void*)k_coarse_factor<float>, B->smem_factor);
-  if (e == cudaSuccess) e = set_smem((const void*)k_coarse_factor<__half>, B->smem_factor);
-  if (e == cudaSuccess) e = set_smem((const void*)k_coarse_factor<__nv_bfloat16>, B->smem_factor);
-  if (e == cudaSuccess) e = set_smem((const void*)k_coarse_block<float>, B->smem_block);
-  if (e == cudaSuccess) e = set_smem((const void*)k_coarse_block<__half>, B->smem_block);
-  if (e == cudaSuccess) e = set_smem((const void*)k_coarse_block<__nv_bfloat16>, B->smem_block);
-  if (e == cudaSuccess) e = set_fused_smem<float>(B->smem_down, B->smem_up);
-  if (e == cudaSuccess) e = set_fused_smem<__half>(B->smem_down, B->smem_up);
-  if (e == cudaSuccess) e = set_fused_smem<__nv_bfloat16>(B->smem_down, B->smem_up);
+  if (e == cudaSuccess) e = configure_kernels();
   if (e != cudaSuccess) {
     err = std::string("batch setup: ") + cudaGetErrorString(e);
     fluid_pp_batch_destroy(B.release());
@@ -638,7 +674,8 @@ static int batch_project_t(fluid_pp_batch* B, const float* dts, const fluid_pp_s
       for (int b = 0; b < burst; ++b) iter_launch<T>(B, o.pre_sweeps, o.post_sweeps);
       it += burst;
       cudaMemcpyAsync(B->h_ctrl, B->d_ctrl, sizeof(Ctrl) * n, cudaMemcpyDeviceToHost, B->stream);
-      cudaError_t e = cudaStreamSynchronize(B->stream);
+      cudaError_t e = take_launch_error(B);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
       if (e != cudaSuccess) {
         B->err = std::string("solve: ") + cudaGetErrorString(e);
         return FLUID_PP_CUDA;
@@ -648,6 +685,11 @@ static int batch_project_t(fluid_pp_batch* B, const float* dts, const fluid_pp_s
       if (all) break;
     }
     finish_launch_any(B);
+    const cudaError_t e = take_launch_error(B);
+    if (e != cudaSuccess) {
+      B->err = std::string("launch: ") + cudaGetErrorString(e);
+      return FLUID_PP_CUDA;
+    }
   }
   cudaMemcpyAsync(B->h_ctrl, B->d_ctrl, sizeof(Ctrl) * n, cudaMemcpyDeviceToHost, B->stream);
   if (graphed) cudaMemcpyAsync(B->h_loop, B->d_loop, sizeof(unsigned), cudaMemcpyDeviceToHost, B->stream);

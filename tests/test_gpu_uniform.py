@@ -191,6 +191,24 @@ def test_batch_is_identical_to_single():
         np.testing.assert_array_equal(x1, pp.pressure_cells())
 
 
+def test_handles_created_large_first_solve_alone():
+    """Kernel limits are process-wide: creating a small handle after a large one must not
+    break the large one's own solve (shared-memory limits are never lowered)."""
+    big = configs.random_small(120, 72, 100, seed=31)
+    small = configs.random_small(24, 20, 26, seed=32)
+    handles = []
+    for prec in ("fp32", "fp16"):
+        pb = PressureProjector((big.nx, big.ny, big.nz), big.h, precision=prec)
+        ps = PressureProjector((small.nx, small.ny, small.nz), small.h, precision=prec)
+        pb.upload_state(big.vof, big.u, big.v, big.w)
+        ps.upload_state(small.vof, small.u, small.v, small.w)
+        rb = pb.project(big.dt)
+        rs = ps.project(small.dt)
+        assert rb["status_name"] == "OK" and rs["status_name"] == "OK", (rb, rs)
+        assert rb["true_rel_residual"] <= REL_RES and rs["true_rel_residual"] <= REL_RES
+        handles += [pb, ps]
+
+
 def test_full_size_dam_spheres_properties():
     s = configs.dam_spheres()
     for precision in ("fp32", "fp16"):
