@@ -27,6 +27,11 @@ EXPORTS = (
     "fluid_pp_kernel_launches", "fluid_pp_set_profiling", "fluid_pp_profile_read",
     "fluid_pp_batch_set_profiling", "fluid_pp_batch_profile_read",
     "fluid_pp_apply_operator_noalloc",
+    "fluid_pp_tall_choose_base", "fluid_pp_tall_limit_bases", "fluid_pp_tall_plan", "fluid_pp_tall_create",
+    "fluid_pp_tall_destroy", "fluid_pp_tall_set_stream", "fluid_pp_tall_upload_state",
+    "fluid_pp_tall_upload_state_device", "fluid_pp_tall_project", "fluid_pp_tall_download",
+    "fluid_pp_tall_prepare", "fluid_pp_tall_get_rhs", "fluid_pp_tall_get_labels", "fluid_pp_tall_apply_operator",
+    "fluid_pp_tall_get_pressure", "fluid_pp_tall_last_error",
 )
 STAGES = ("reset", "label", "coarsen", "bake", "factor", "init", "smooth0", "smoothc", "residual0", "residualc",
           "restrict0", "restrictc", "coarse", "prolong0", "prolongc", "dot", "dir", "spmv", "update", "true",
@@ -36,6 +41,12 @@ STAGES = ("reset", "label", "coarsen", "bake", "factor", "init", "smooth0", "smo
 class Config(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("h", ctypes.c_float),
                 ("rho", ctypes.c_float), ("open_top", ctypes.c_int), ("precision", ctypes.c_int),
+                ("device", ctypes.c_int)]
+
+
+class TallConfig(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("nz", ctypes.c_int), ("fine_ny", ctypes.c_int), ("band", ctypes.c_int),
+                ("h", ctypes.c_float), ("rho", ctypes.c_float), ("precision", ctypes.c_int),
                 ("device", ctypes.c_int)]
 
 
@@ -104,6 +115,24 @@ def load():
     L.fluid_pp_batch_set_profiling.argtypes = [vp, ci]
     L.fluid_pp_batch_profile_read.argtypes = [vp, vp, vp, ci]
     L.fluid_pp_apply_operator_noalloc.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp, vp]
+    L.fluid_pp_tall_choose_base.argtypes = [ci, ci, ci, ci, ci, ci]
+    L.fluid_pp_tall_limit_bases.argtypes = [vp, ci, ci, ci, ci]
+    L.fluid_pp_tall_plan.argtypes = [ci, ci, ci, ci, vp, pi, vp]
+    L.fluid_pp_tall_create.argtypes = [ctypes.POINTER(TallConfig), vp, ctypes.POINTER(vp)]
+    L.fluid_pp_tall_destroy.argtypes = [vp]
+    L.fluid_pp_tall_destroy.restype = None
+    L.fluid_pp_tall_set_stream.argtypes = [vp, vp]
+    L.fluid_pp_tall_upload_state.argtypes = [vp, vp, vp, vp, vp]
+    L.fluid_pp_tall_upload_state_device.argtypes = [vp, vp, vp, vp, vp]
+    L.fluid_pp_tall_project.argtypes = [vp, cf, ctypes.POINTER(SolveOpts), ctypes.POINTER(Receipt)]
+    L.fluid_pp_tall_download.argtypes = [vp, vp, vp, vp, vp]
+    L.fluid_pp_tall_prepare.argtypes = [vp, cf]
+    L.fluid_pp_tall_get_rhs.argtypes = [vp, vp]
+    L.fluid_pp_tall_get_labels.argtypes = [vp, ci, vp]
+    L.fluid_pp_tall_apply_operator.argtypes = [vp, vp, vp]
+    L.fluid_pp_tall_get_pressure.argtypes = [vp, vp]
+    L.fluid_pp_tall_last_error.argtypes = [vp]
+    L.fluid_pp_tall_last_error.restype = ctypes.c_char_p
     _lib = L
     return L
 

@@ -194,3 +194,111 @@ def random_small(nx, ny, nz, seed: int, open_top: bool = False, fill=(0.2, 0.7))
         v[:, -1, :] = np.where(liq_top, rng.normal(0, 0.2, size=liq_top.shape), 0.0).astype(np.float32)
     return GridState(nx, ny, nz, 1.0 / max(nx, ny, nz), dt, vof, u, v, w, open_top=open_top,
                      meta={"workload": f"random {nx}x{ny}x{nz}", "seed": seed})
+
+
+# ------------------------------------------------------------------ tall cells
+@dataclass
+class TallState:
+    """Packed tall-cell state: arrays float32 [nz][P][nx], P = band + 2 (see fluid_b200.tall)."""
+    nx: int
+    nz: int
+    fine_ny: int
+    band: int
+    bases: np.ndarray   # int32 [nz][nx]
+    h: float
+    dt: float
+    vof: np.ndarray
+    u: np.ndarray
+    v: np.ndarray
+    w: np.ndarray
+    rho: float = 1000.0
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def P(self) -> int:
+        return self.band + 2
+
+    @property
+    def samples(self) -> int:
+        return self.nx * self.P * self.nz
+
+    @property
+    def dense_cells(self) -> int:
+        return self.nx * self.fine_ny * self.nz
+
+
+def tall_sample_rows(bases: np.ndarray, band: int) -> np.ndarray:
+    """World row of every packed sample, int64 [nz][P][nx]."""
+    nz, nx = bases.shape
+    j = np.arange(band + 2)[None, :, None]
+    b = bases[:, None, :].astype(np.int64)
+    return np.where(j == 0, 0, np.where(j == 1, b - 1, b + j - 2))
+
+
+def tall_waves(nx: int = 256, nz: int = 256, fine_ny: int = 1024, band: int = 32, seed: int = 3,
+               mean: float = 600.0, waves: int = 8, amp_max: float = 12.0, lam=(16.0, 256.0), sigma: float = 0.1,
+               quality: str = "high") -> TallState:
+    """Deep wave tank on a tall-cell grid: surface height (cells) = mean + sum of `waves`
+    seeded sinusoids (amplitude <= amp_max, wavelength log-uniform in lam, random
+    direction and phase).  Bases per column come from chooseTallCellBase with the
+    band pinned to `band` and the quality preset's halos, then
+    limitNeighboringTallCellBases with nx + nz passes (the reference's call);
+    VOF is the covered fraction of each row (a tall sample holds its rows' mean);
+    Gaussian velocities (sigma m/s) on faces with a liquid side, zero at walls."""
+    from .tall import SETTINGS, choose_tall_base, limit_neighboring_bases
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(0.0, amp_max, waves)
+    wl = np.exp(rng.uniform(math.log(lam[0]), math.log(lam[1]), waves))
+    ang = rng.uniform(0.0, 2 * math.pi, waves)
+    ph = rng.uniform(0.0, 2 * math.pi, waves)
+    xs = np.arange(nx) + 0.5
+    zs = np.arange(nz) + 0.5
+    X, Z = np.meshgrid(xs, zs)   # [nz][nx]
+    H = np.full((nz, nx), float(mean))
+    for a, l, t, p in zip(amp, wl, ang, ph):
+        H += a * np.sin(2 * math.pi / l * (math.cos(t) * X + math.sin(t) * Z) + p)
+    H = np.clip(H, 1.0, fine_ny - 1.0)
+    st = SETTINGS[quality]
+    wet_rows = np.ceil(H - 0.5).astype(np.int64)   # rows y with y + 0.5 < H
+    raw = np.empty(nx * nz, np.float32)
+    for z in range(nz):
+        for x in range(nx):
+            top = int(wet_rows[z, x]) - 1
+            raw[x + nx * z] = choose_tall_base(top, min(top + 1, fine_ny - 1), fine_ny, band, st["liquid_halo"],
+                                               st["air_halo"])
+    bases = limit_neighboring_bases(raw, nx, nz, st["max_delta"], nx + nz).astype(np.int32).reshape(nz, nx)
+    P = band + 2
+    rows = tall_sample_rows(bases, band)   # [nz][P][nx]
+    frac_row = lambda y: np.clip(H[:, None, :] - y, 0.0, 1.0)
+    vof = frac_row(rows).astype(np.float32)
+    # a tall sample holds the mean covered fraction of its rows [0, base)
+    bb = bases.astype(np.float64)
+    covered = np.clip(H, 0.0, bb) / bb
+    vof[:, 0, :] = covered
+    vof[:, 1, :] = covered
+    active = rows < fine_ny
+    vof[~active] = 0.0
+    liquid = vof > 0.5
+    liquid[:, 1, :] = liquid[:, 0, :]
+
+    def dense_liquid(xq, yq, zq):
+        """Liquid flag of dense cells (arrays of equal shape); outside -> False."""
+        inside = (xq >= 0) & (xq < nx) & (zq >= 0) & (zq < nz) & (yq >= 0) & (yq < fine_ny)
+        xc, zc = np.clip(xq, 0, nx - 1), np.clip(zq, 0, nz - 1)
+        b = bases[zc, xc].astype(np.int64)
+        j = np.where(yq < b, 0, yq - b + 2)
+        ok = inside & (j < P)
+        jc = np.clip(j, 0, P - 1)
+        return ok & liquid[zc, jc, xc]
+
+    zi, ji, xi = np.meshgrid(np.arange(nz), np.arange(P), np.arange(nx), indexing="ij")
+    own = liquid & active
+    u = np.zeros((nz, P, nx), np.float32)
+    v = np.zeros((nz, P, nx), np.float32)
+    w = np.zeros((nz, P, nx), np.float32)
+    for arr, (dx, dy, dz), wall in ((u, (1, 0, 0), xi + 1 >= nx), (v, (0, 1, 0), rows + 1 >= fine_ny),
+                                    (w, (0, 0, 1), zi + 1 >= nz)):
+        fluid = (own | dense_liquid(xi + dx, rows + dy, zi + dz)) & active & ~wall
+        arr[fluid] = rng.normal(0.0, sigma, size=int(fluid.sum())).astype(np.float32)
+    return TallState(nx, nz, fine_ny, band, bases, 1.0 / nx, 1.0 / 60.0, vof, u, v, w,
+                     meta={"workload": f"tall waves {nx}x{nz} columns, {fine_ny} rows, band {band}", "seed": seed})

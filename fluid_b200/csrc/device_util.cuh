@@ -226,4 +226,99 @@ __device__ __forceinline__ float p1d(int f, int c, int nc) {
   return 0.25f;   // d == -1 or d == 2
 }
 
+// ------------------------------------------------------------ CG scalars
+// The per-solve scalar logic shared by every CG kernel family; each runs in the
+// thread that finished a reduction.
+
+// Preconditioner input scale: 1 / rms of the residual over liquid cells.
+__device__ __forceinline__ void set_sigma(Ctrl* c, double rr) {
+  const double per = rr / double(c->liquid > 0 ? c->liquid : 1);
+  c->sigma = per > 1e-300 ? 1.0 / sqrt(per) : 1.0;
+}
+
+// gamma = r . (z - zmean) from its three sums; beta from the previous gamma.
+// A non-positive or non-finite gamma ends the solve (the preconditioned system
+// lost definiteness).
+__device__ __forceinline__ void finish_gamma(Ctrl* c, double rz, double zsum, double rsum) {
+  double gamma = rz;
+  c->zmean = 0.0;
+  if (!c->anchored) {
+    c->zmean = zsum / double(c->liquid);
+    gamma = rz - c->zmean * rsum;
+  }
+  if (!(gamma > 0.0) || !isfinite(gamma)) {
+    c->done = 1;
+    c->status = FLUID_PP_NONCONVERGENCE;
+  } else {
+    c->beta = c->first ? 0.0 : gamma / c->gamma;
+    c->gamma = gamma;
+    c->first = 0;
+  }
+}
+
+// delta = d . A d and alpha = gamma / delta (direct curvature).
+__device__ __forceinline__ void finish_delta(Ctrl* c, double delta) {
+  c->delta = delta;
+  if (!(delta > 0.0) || !isfinite(delta)) {
+    c->done = 1;
+    c->status = FLUID_PP_NONCONVERGENCE;
+  } else {
+    c->alpha = c->gamma / delta;
+  }
+}
+
+// x += alpha d, r -= alpha q finished: ||r||^2 = s, max |r| = m.  Below the
+// tolerance (or at the iteration cap) the solve becomes a candidate for the
+// float64 acceptance check.
+__device__ __forceinline__ void finish_update(Ctrl* c, double s, double m) {
+  c->rr = s;
+  c->rmax = m;
+  c->iter += 1;
+  set_sigma(c, s);
+  if (!isfinite(s)) {
+    c->done = 1;
+    c->status = FLUID_PP_NONCONVERGENCE;
+  } else if ((s <= c->thr2 && (c->thr_inf <= 0 || m <= c->thr_inf)) || c->iter >= c->max_iter) {
+    c->candidate = 1;
+  }
+}
+
+// Float64 true residual finished (octree-pipelined-pcg.ts:501-541 acceptance rule).
+__device__ __forceinline__ void finish_true(Ctrl* c, double s, double m) {
+  c->rr_true = s;
+  c->rr = s;
+  c->rmax = m;
+  set_sigma(c, s);
+  if (c->candidate) {
+    if (s <= c->thr2 && (c->thr_inf <= 0 || m <= c->thr_inf)) {
+      c->done = 1;
+      c->converged = 1;
+      c->status = FLUID_PP_OK;
+    } else if (c->iter >= c->max_iter) {
+      c->done = 1;
+      c->status = FLUID_PP_NONCONVERGENCE;
+    }
+    c->candidate = 0;
+  }
+}
+
+// In-place Gauss-Jordan inverse of an SPD m x m matrix in shared memory (no
+// pivoting needed), all threads of the CTA; prow/pcol hold m doubles each.
+__device__ __forceinline__ void gauss_jordan_inplace(double* A, int m, double* prow, double* pcol) {
+  for (int k = 0; k < m; ++k) {
+    const double piv = A[k * m + k];
+    for (int j = threadIdx.x; j < m; j += blockDim.x) {
+      prow[j] = (j == k ? 1.0 : A[k * m + j]) / piv;
+      pcol[j] = A[j * m + k];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      const int i = e / m, j = e - i * m;
+      if (i == k) A[e] = prow[j];
+      else A[e] = ((j == k) ? 0.0 : A[e]) - pcol[i] * prow[j];
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace fpp

@@ -195,31 +195,13 @@ __global__ void k_coarse_factor(const InstDev* insts, const int* list) {
     for (int e = threadIdx.x; e < m * m; e += blockDim.x) A[e] += add;
     __syncthreads();
   }
-  // In-place Gauss-Jordan inversion (SPD: no pivoting needed).
-  for (int k = 0; k < m; ++k) {
-    const double piv = A[k * m + k];
-    for (int j = threadIdx.x; j < m; j += blockDim.x) {
-      pivot_row[j] = (j == k ? 1.0 : A[k * m + j]) / piv;
-      pivot_col[j] = A[j * m + k];
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-      const int i = e / m, j = e - i * m;
-      if (i == k) A[e] = pivot_row[j];
-      else A[e] = ((j == k) ? 0.0 : A[e]) - pivot_col[i] * pivot_row[j];
-    }
-    __syncthreads();
-  }
+  gauss_jordan_inplace(A, m, pivot_row, pivot_col);
   for (int e = threadIdx.x; e < m * m; e += blockDim.x) I.coarse_inv[e] = A[e];
 }
 
 // ================================================================= CG scalars
 enum Stage { kStInit = 0, kStGamma = 1, kStSpmv = 2, kStUpdate = 3, kStTrue = 4, kStReceipt = 5 };
 
-__device__ __forceinline__ void set_sigma(Ctrl* c, double rr) {
-  const double per = rr / double(c->liquid > 0 ? c->liquid : 1);
-  c->sigma = per > 1e-300 ? 1.0 / sqrt(per) : 1.0;
-}
 
 // r = b - A x (x already masked to liquid), bb, sums for the nullspace.
 __global__ void k_cg_init(const InstDev* insts, const Tile* tiles, int ntiles, double rel_tol, double abs_tol,
@@ -744,37 +726,6 @@ __global__ void k_coarse_apply(const InstDev* insts, const int* list) {
 }
 
 // ================================================================= CG kernels
-// gamma = r . (z - zmean) from its three sums; beta from the previous gamma.
-// A non-positive or non-finite gamma ends the solve (the preconditioned system
-// lost definiteness).
-__device__ __forceinline__ void finish_gamma(Ctrl* c, double rz, double zsum, double rsum) {
-  double gamma = rz;
-  c->zmean = 0.0;
-  if (!c->anchored) {
-    c->zmean = zsum / double(c->liquid);
-    gamma = rz - c->zmean * rsum;
-  }
-  if (!(gamma > 0.0) || !isfinite(gamma)) {
-    c->done = 1;
-    c->status = FLUID_PP_NONCONVERGENCE;
-  } else {
-    c->beta = c->first ? 0.0 : gamma / c->gamma;
-    c->gamma = gamma;
-    c->first = 0;
-  }
-}
-
-// delta = d . A d and alpha = gamma / delta (direct curvature).
-__device__ __forceinline__ void finish_delta(Ctrl* c, double delta) {
-  c->delta = delta;
-  if (!(delta > 0.0) || !isfinite(delta)) {
-    c->done = 1;
-    c->status = FLUID_PP_NONCONVERGENCE;
-  } else {
-    c->alpha = c->gamma / delta;
-  }
-}
-
 // The current search direction (the fused path alternates two buffers).
 __device__ __forceinline__ float* dir_cur(const InstDev& I) { return I.ctrl->dsel ? I.d2 : I.d; }
 // Level-0 column helper: calls f(k, z, i) for the thread's valid cells, fully
@@ -942,18 +893,7 @@ __global__ void __launch_bounds__(kThreads) k_update(const InstDev* insts, const
     if (arrive_last(&c->arrive[kStUpdate], nt0, &flag)) {
       const double s = gather_slot(partial, 0, nt0, 0, sh);
       const double m = gather_slot(partial, 1, nt0, 1, sh);
-      if (threadIdx.x == 0) {
-        c->rr = s;
-        c->rmax = m;
-        c->iter += 1;
-        set_sigma(c, s);
-        if (!isfinite(s)) {
-          c->done = 1;
-          c->status = FLUID_PP_NONCONVERGENCE;
-        } else if ((s <= c->thr2 && (c->thr_inf <= 0 || m <= c->thr_inf)) || c->iter >= c->max_iter) {
-          c->candidate = 1;
-        }
-      }
+      if (threadIdx.x == 0) finish_update(c, s, m);
     }
   }
 }
@@ -1015,23 +955,7 @@ __global__ void __launch_bounds__(kThreads) k_true_residual(const InstDev* insts
     if (arrive_last(&c->arrive[kStTrue], nt0, &flag)) {
       const double s = gather_slot(partial, 0, nt0, 0, sh);
       const double m = gather_slot(partial, 1, nt0, 1, sh);
-      if (threadIdx.x == 0) {
-        c->rr_true = s;
-        c->rr = s;
-        c->rmax = m;
-        set_sigma(c, s);
-        if (c->candidate) {
-          if (s <= c->thr2 && (c->thr_inf <= 0 || m <= c->thr_inf)) {
-            c->done = 1;
-            c->converged = 1;
-            c->status = FLUID_PP_OK;
-          } else if (c->iter >= c->max_iter) {
-            c->done = 1;
-            c->status = FLUID_PP_NONCONVERGENCE;
-          }
-          c->candidate = 0;
-        }
-      }
+      if (threadIdx.x == 0) finish_true(c, s, m);
     }
   }
 }

@@ -1,0 +1,1261 @@
+// Restricted tall-cell pressure projection: MGPCG on the packed tall-cell grid.
+//
+// Layout (lib/core/tall-cell-grid.ts:171-190, 398-409): an nx x nz grid of
+// columns; column (x, z) has a tall cell over world rows [0, base) and a cubic
+// band of `band` rows above it.  Every quantity is packed per column in
+// P = band + 2 samples, index x + nx * (j + P * z): j = 0 is the tall cell's
+// bottom subcell (row 0), j = 1 its top subcell (row base - 1), j >= 2 the band
+// row base + j - 2.
+//
+// Operator.  The paper's two-sample tall cell gives a non-symmetric system
+// (docs/papers/tallCells.txt:356-361); this solver keeps CG by building the
+// operator from the faces of the equivalent dense MAC grid, the repo's own
+// face-row idiom (sparse-atlas-composite-projection.ts:381-620):
+// A = sum over faces (1/theta) g g^T with g = T_i - T_j, where T maps the
+// samples to a dense cell (a tall subcell interpolates its column's two
+// samples linearly, Eq. 5 of the paper; a band cell is its sample; rows above
+// the band are air).  A = T^T A_dense T is SPD by construction.  Band rows are
+// stored as ELL rows of at most kBandW entries, the two tall rows of a column
+// as a 2 x 2 diagonal block plus ELL rows of at most kTallW entries.
+//
+// Hierarchy: each coarser tall grid halves columns, rows and band, and its
+// bases cover the finer tall cells (tall_plan.cpp).  Coarse phi is the mean of
+// the 8 fine dense children; operators are rediscretised with the same rule
+// (normalised levels: unit face weights).  Prolongation interpolates the
+// coarse dense field trilinearly (taps dropped and renormalised at walls, the
+// rule of mgTrilinearPressure, mg.wgsl.ts:217-241) at every fine sample's own
+// position; restriction is its transpose times 1/2 (to_coarse 4 / 8 children),
+// accumulated in 32.32 fixed point so the sum is order-independent.  Smoother:
+// symmetric 4-colour block Gauss-Seidel (band red, band black, tall columns
+// with x + z even, odd; reversed after the coarse correction).  The coarsest
+// level (at most kMaxCoarse samples) is inverted densely in float64.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/fluid_pp.h"
+#include "device_util.cuh"
+#include "tall_plan.h"
+#include "types.h"
+
+namespace fpp {
+void set_global_error(const std::string& message);
+
+namespace tall {
+
+constexpr int kBandW = 10;        // off-diagonal slots of a band row
+constexpr int kTallW = 48;        // off-block slots of a tall row
+constexpr int kTB = 256;          // threads per CTA
+constexpr int kTGrid = 148 * 8;   // grid cap (grid-stride beyond)
+constexpr double kFix = 4294967296.0;   // 2^32: restriction fixed point
+
+struct TLevel {
+  int nx, nz, fine_ny, band, P;
+  int n;        // samples
+  int ncol;     // columns
+  int* bases;
+  float* phi;
+  uint8_t* label;
+  float* diag;  // A[k][k]; air and inactive samples 1
+  float* a01;   // per column A[j0][j1]
+  int* bidx;    // kBandW x n
+  float* bval;
+  int* tidx;    // kTallW x 2 ncol, row 2 * column + (j == 1)
+  float* tval;
+  float* z;
+  float* rhs;
+  float* res;
+  unsigned long long* acc;   // restriction accumulators (levels >= 1)
+};
+
+struct TInst {
+  TLevel lv[kMaxLevels];
+  int nlev;
+  float h, rho, dt, pscale;
+  float* vof;       // packed, level 0
+  float* u;
+  float* v;
+  float* w;
+  float* b;
+  float* x;
+  float* xlo;
+  float* d;
+  float* q;
+  float* p_si;
+  double* partial;  // kSlots x kTGrid
+  double* coarse_inv;
+  int coarse_m;
+  Ctrl* ctrl;
+  int* err;         // 1: an ELL row overflowed
+};
+
+// ------------------------------------------------------------------ helpers
+__device__ __forceinline__ int sidx(const TLevel& L, int x, int j, int z) { return x + L.nx * (j + L.P * z); }
+
+__device__ __forceinline__ int sample_row(int j, int b) { return j == 0 ? 0 : (j == 1 ? b - 1 : b + j - 2); }
+
+// Dense cell (x, y, z) as samples: tall rows interpolate (1 - t, t), a band
+// row is its sample, rows above the band are air (phi 0.5).
+struct Rep {
+  int n;
+  int s0, s1;
+  double w0, w1;
+  bool liq;
+  float phi;
+};
+
+__device__ __forceinline__ Rep rep_of(const TLevel& L, int x, int y, int z) {
+  Rep r;
+  const int b = L.bases[x + L.nx * z];
+  if (y < b) {
+    const double t = double(y) / double(b - 1);
+    r.n = 2;
+    r.s0 = sidx(L, x, 0, z);
+    r.s1 = sidx(L, x, 1, z);
+    r.w0 = 1.0 - t;
+    r.w1 = t;
+  } else if (y < b + L.band) {
+    r.n = 1;
+    r.s0 = r.s1 = sidx(L, x, y - b + 2, z);
+    r.w0 = 1.0;
+    r.w1 = 0.0;
+  } else {
+    r.n = 0;
+    r.s0 = r.s1 = -1;
+    r.w0 = r.w1 = 0.0;
+    r.liq = false;
+    r.phi = 0.5f;
+    return r;
+  }
+  r.liq = L.label[r.s0] != 0;
+  r.phi = L.phi[r.s0];
+  return r;
+}
+
+__device__ __forceinline__ double ghost_theta_d(float liquid_phi, float air_phi) {
+  const double a = fabs(double(liquid_phi));
+  return fmin(1.0, fmax(0.05, a / fmax(a + fabs(double(air_phi)), 1e-12)));
+}
+
+// Value of a packed array at dense cell (x, y, z) (zero above the band).
+__device__ __forceinline__ double dense_val(const TLevel& L, const float* a, int x, int y, int z) {
+  const int b = L.bases[x + L.nx * z];
+  if (y < b) {
+    const double t = double(y) / double(b - 1);
+    return (1.0 - t) * double(a[sidx(L, x, 0, z)]) + t * double(a[sidx(L, x, 1, z)]);
+  }
+  if (y < b + L.band) return double(a[sidx(L, x, y - b + 2, z)]);
+  return 0.0;
+}
+
+__device__ __forceinline__ bool sample_active(const TLevel& L, int k, int& x, int& j, int& z, int& b) {
+  x = k % L.nx;
+  const int r = k / L.nx;
+  j = r % L.P;
+  z = r / L.P;
+  b = L.bases[x + L.nx * z];
+  return j < 2 || b + j - 2 < L.fine_ny;
+}
+
+// ------------------------------------------------------------------ setup
+// Level-0 labels and phi from the packed VOF (liquid iff vof > 0.5, phi = 0.5 - vof).
+__global__ void k_tall_label(TInst* I) {
+  const TLevel& L = I->lv[0];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+    int x, j, z, b;
+    const bool act = sample_active(L, k, x, j, z, b);
+    const float f = I->vof[k];
+    if (!isfinite(f)) atomicExch(&I->ctrl->nonfinite, 1);
+    L.phi[k] = act ? 0.5f - f : 0.5f;
+    bool liq;
+    if (j < 2) liq = I->vof[sidx(L, x, 0, z)] > 0.5f;   // the tall segment follows its bottom sample
+    else liq = act && f > 0.5f;
+    L.label[k] = liq ? 1 : 0;
+    if (liq && j != 1) atomicAdd(&I->ctrl->liquid, j == 0 ? 2 : 1);
+    if (!liq && act && j != 1) atomicAdd(&I->ctrl->air, 1);
+  }
+}
+
+// Coarse phi: mean of the fine dense children's phi (fine rows above the band
+// are air, 0.5); liquid iff phi < 0, a tall segment following its bottom sample.
+__global__ void k_tall_coarsen(TInst* I, int l) {
+  const TLevel& F = I->lv[l];
+  const TLevel& C = I->lv[l + 1];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C.n; k += gridDim.x * blockDim.x) {
+    int X, j, Z, b;
+    if (!sample_active(C, k, X, j, Z, b)) {
+      C.phi[k] = 0.5f;
+      continue;
+    }
+    const int Y = sample_row(j, b);
+    float s = 0.0f;
+    int cnt = 0;
+    for (int dz = 0; dz < 2; ++dz)
+      for (int dy = 0; dy < 2; ++dy)
+        for (int dx = 0; dx < 2; ++dx) {
+          const int x = 2 * X + dx, y = 2 * Y + dy, z = 2 * Z + dz;
+          if (x >= F.nx || y >= F.fine_ny || z >= F.nz) continue;
+          s += rep_of(F, x, y, z).phi;
+          ++cnt;
+        }
+    C.phi[k] = s / float(cnt > 0 ? cnt : 1);
+  }
+}
+
+__global__ void k_tall_coarse_labels(TInst* I, int l) {
+  const TLevel& C = I->lv[l];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C.n; k += gridDim.x * blockDim.x) {
+    int x, j, z, b;
+    const bool act = sample_active(C, k, x, j, z, b);
+    bool liq = act && C.phi[k] < 0.0f;
+    if (j < 2) liq = C.phi[sidx(C, x, 0, z)] < 0.0f;
+    C.label[k] = liq ? 1 : 0;
+  }
+}
+
+// Band rows: diagonal and up to kBandW neighbour entries from the six faces.
+__global__ void k_tall_assemble_band(TInst* I, int l) {
+  const TLevel& L = I->lv[l];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+    int x, j, z, b;
+    const bool act = sample_active(L, k, x, j, z, b);
+    if (j < 2) continue;
+    int cnt = 0;
+    double dg = 0.0;
+    if (act && L.label[k]) {
+      const int y = b + j - 2;
+      const float ph = L.phi[k];
+      const int nb[6][3] = {{x - 1, y, z}, {x + 1, y, z}, {x, y - 1, z}, {x, y + 1, z}, {x, y, z - 1}, {x, y, z + 1}};
+      for (int f = 0; f < 6; ++f) {
+        const int xn = nb[f][0], yn = nb[f][1], zn = nb[f][2];
+        if (xn < 0 || yn < 0 || zn < 0 || xn >= L.nx || yn >= L.fine_ny || zn >= L.nz) continue;
+        const Rep rn = rep_of(L, xn, yn, zn);
+        if (rn.liq) {
+          dg += 1.0;
+          if (rn.w0 != 0.0 && cnt < kBandW) {
+            L.bidx[cnt * L.n + k] = rn.s0;
+            L.bval[cnt * L.n + k] = float(-rn.w0);
+            ++cnt;
+          }
+          if (rn.n == 2 && rn.w1 != 0.0 && cnt < kBandW) {
+            L.bidx[cnt * L.n + k] = rn.s1;
+            L.bval[cnt * L.n + k] = float(-rn.w1);
+            ++cnt;
+          }
+        } else {
+          dg += 1.0 / ghost_theta_d(ph, rn.phi);
+        }
+      }
+      L.diag[k] = float(dg);
+    } else {
+      L.diag[k] = 1.0f;
+    }
+    for (int s = cnt; s < kBandW; ++s) {
+      L.bidx[s * L.n + k] = k;
+      L.bval[s * L.n + k] = 0.0f;
+    }
+  }
+}
+
+// The two tall rows of a column: 2 x 2 block (internal faces, the face to the
+// first band row, lateral faces summed over the tall rows) and the couplings
+// to the neighbour columns' samples.
+__global__ void k_tall_assemble_tall(TInst* I, int l) {
+  const TLevel& L = I->lv[l];
+  const int nrow = 2 * L.ncol;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < L.ncol; c += gridDim.x * blockDim.x) {
+    const int x = c % L.nx, z = c / L.nx;
+    const int b = L.bases[c];
+    const int s0 = sidx(L, x, 0, z), s1 = sidx(L, x, 1, z);
+    int n0 = 0, n1 = 0;
+    auto add = [&](int row, int& cnt, int s, double v) {
+      if (v == 0.0) return;
+      if (cnt >= kTallW) {
+        atomicExch(I->err, 1);
+        return;
+      }
+      L.tidx[cnt * nrow + row] = s;
+      L.tval[cnt * nrow + row] = float(v);
+      ++cnt;
+    };
+    if (L.label[s0]) {
+      const float ph = L.phi[s0];
+      double a00 = 0.0, a01 = 0.0, a11 = 0.0;
+      const double kin = 1.0 / double(b - 1);   // b - 1 internal faces of slope 1 / (b - 1)
+      a00 += kin;
+      a11 += kin;
+      a01 -= kin;
+      {
+        const int s2 = sidx(L, x, 2, z);
+        if (L.label[s2]) {
+          a11 += 1.0;
+          add(2 * c + 1, n1, s2, -1.0);
+        } else {
+          a11 += 1.0 / ghost_theta_d(ph, L.phi[s2]);
+        }
+      }
+      const int dirs[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+      for (int d = 0; d < 4; ++d) {
+        const int xn = x + dirs[d][0], zn = z + dirs[d][1];
+        if (xn < 0 || zn < 0 || xn >= L.nx || zn >= L.nz) continue;
+        double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
+        for (int y = 0; y < b; ++y) {
+          const double t = double(y) / double(b - 1);
+          const Rep rn = rep_of(L, xn, y, zn);
+          if (rn.liq) {
+            a00 += (1.0 - t) * (1.0 - t);
+            a01 += (1.0 - t) * t;
+            a11 += t * t;
+            if (rn.n == 2) {
+              c00 += (1.0 - t) * rn.w0;
+              c01 += (1.0 - t) * rn.w1;
+              c10 += t * rn.w0;
+              c11 += t * rn.w1;
+            } else {
+              add(2 * c, n0, rn.s0, -(1.0 - t));
+              add(2 * c + 1, n1, rn.s0, -t);
+            }
+          } else {
+            const double inv = 1.0 / ghost_theta_d(ph, rn.phi);
+            a00 += (1.0 - t) * (1.0 - t) * inv;
+            a01 += (1.0 - t) * t * inv;
+            a11 += t * t * inv;
+          }
+        }
+        const int m0 = sidx(L, xn, 0, zn), m1 = sidx(L, xn, 1, zn);
+        add(2 * c, n0, m0, -c00);
+        add(2 * c, n0, m1, -c01);
+        add(2 * c + 1, n1, m0, -c10);
+        add(2 * c + 1, n1, m1, -c11);
+      }
+      L.diag[s0] = float(a00);
+      L.diag[s1] = float(a11);
+      L.a01[c] = float(a01);
+    } else {
+      L.diag[s0] = 1.0f;
+      L.diag[s1] = 1.0f;
+      L.a01[c] = 0.0f;
+    }
+    for (int s = n0; s < kTallW; ++s) {
+      L.tidx[s * nrow + 2 * c] = s0;
+      L.tval[s * nrow + 2 * c] = 0.0f;
+    }
+    for (int s = n1; s < kTallW; ++s) {
+      L.tidx[s * nrow + 2 * c + 1] = s1;
+      L.tval[s * nrow + 2 * c + 1] = 0.0f;
+    }
+  }
+}
+
+// Off-diagonal part of row k of A applied to v (the 2 x 2 block excluded for
+// tall rows); returns it in float64.
+__device__ __forceinline__ double offdiag(const TLevel& L, int k, int j, int col, const float* v) {
+  double s = 0.0;
+  if (j >= 2) {
+#pragma unroll
+    for (int e = 0; e < kBandW; ++e) s += double(L.bval[e * L.n + k]) * double(v[L.bidx[e * L.n + k]]);
+  } else {
+    const int nrow = 2 * L.ncol, row = 2 * col + j;
+    for (int e = 0; e < kTallW; ++e) {
+      const float a = L.tval[e * nrow + row];
+      if (a == 0.0f) break;   // entries are packed from slot 0
+      s += double(a) * double(v[L.tidx[e * nrow + row]]);
+    }
+  }
+  return s;
+}
+
+// (A v)_k in float64 for a liquid sample.
+__device__ __forceinline__ double apply_row(const TLevel& L, int k, int x, int j, int z, const float* v) {
+  const int col = x + L.nx * z;
+  double s = double(L.diag[k]) * double(v[k]) + offdiag(L, k, j, col, v);
+  if (j < 2) s += double(L.a01[col]) * double(v[sidx(L, x, 1 - j, z)]);
+  return s;
+}
+
+// Dense inverse of the coarsest level (air and inactive samples identity rows).
+__global__ void k_tall_factor(TInst* I) {
+  extern __shared__ double A[];
+  __shared__ double prow[kMaxCoarse], pcol[kMaxCoarse];
+  const TLevel& L = I->lv[I->nlev - 1];
+  const int m = L.n;
+  for (int e = threadIdx.x; e < m * m; e += blockDim.x) A[e] = 0.0;
+  __syncthreads();
+  for (int k = threadIdx.x; k < m; k += blockDim.x) {
+    int x, j, z, b;
+    const bool act = sample_active(L, k, x, j, z, b);
+    if (!act || !L.label[k]) {
+      A[k * m + k] = 1.0;
+      continue;
+    }
+    const int col = x + L.nx * z;
+    A[k * m + k] = L.diag[k];
+    if (j >= 2) {
+      for (int e = 0; e < kBandW; ++e) A[k * m + L.bidx[e * L.n + k]] += L.bval[e * L.n + k];
+    } else {
+      const int nrow = 2 * L.ncol, row = 2 * col + j;
+      A[k * m + sidx(L, x, 1 - j, z)] += L.a01[col];
+      for (int e = 0; e < kTallW; ++e) A[k * m + L.tidx[e * nrow + row]] += L.tval[e * nrow + row];
+    }
+  }
+  __syncthreads();
+  gauss_jordan_inplace(A, m, prow, pcol);
+  for (int e = threadIdx.x; e < m * m; e += blockDim.x) I->coarse_inv[e] = A[e];
+}
+
+// b = T^T (-div u) over liquid dense cells; tall samples sum their rows.
+__device__ __forceinline__ double dense_div(const TInst& I, const TLevel& L, int x, int y, int z) {
+  const double du = dense_val(L, I.u, x, y, z) - (x > 0 ? dense_val(L, I.u, x - 1, y, z) : 0.0);
+  const double dv = dense_val(L, I.v, x, y, z) - (y > 0 ? dense_val(L, I.v, x, y - 1, z) : 0.0);
+  const double dw = dense_val(L, I.w, x, y, z) - (z > 0 ? dense_val(L, I.w, x, y, z - 1) : 0.0);
+  return (du + dw) + dv;
+}
+
+__global__ void k_tall_rhs(TInst* I) {
+  const TLevel& L = I->lv[0];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+    int x, j, z, b;
+    const bool act = sample_active(L, k, x, j, z, b);
+    if (j == 1) continue;   // written with j = 0
+    if (j >= 2) {
+      I->b[k] = (act && L.label[k]) ? float(-dense_div(*I, L, x, b + j - 2, z)) : 0.0f;
+      continue;
+    }
+    double b0 = 0.0, b1 = 0.0;
+    if (L.label[k]) {
+      for (int y = 0; y < b; ++y) {
+        const double t = double(y) / double(b - 1);
+        const double dv = -dense_div(*I, L, x, y, z);
+        b0 += (1.0 - t) * dv;
+        b1 += t * dv;
+      }
+    }
+    I->b[k] = float(b0);
+    I->b[sidx(L, x, 1, z)] = float(b1);
+  }
+}
+
+// ---------------------------------------------------------- reductions
+// Grid-stride partial sums in a fixed order, published per block; the last
+// block to arrive folds them (deterministic for a fixed grid).
+template <int N>
+__device__ __forceinline__ bool reduce_grid(TInst* I, int stage, const double (&v)[N], const bool (&is_max)[N],
+                                            double (&out)[N]) {
+  __shared__ double sh[32];
+  __shared__ int flag;
+  double r[N];
+#pragma unroll
+  for (int s = 0; s < N; ++s) r[s] = is_max[s] ? block_max(v[s], sh) : block_sum(v[s], sh);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int s = 0; s < N; ++s) I->partial[s * kTGrid + blockIdx.x] = r[s];
+  if (!arrive_last(&I->ctrl->arrive[stage], gridDim.x, &flag)) return false;
+#pragma unroll
+  for (int s = 0; s < N; ++s) out[s] = gather_slot(I->partial + s * kTGrid, 0, gridDim.x, is_max[s] ? 1 : 0, sh);
+  return true;
+}
+
+// ------------------------------------------------------------------ CG
+__global__ void k_tall_reset(TInst* I) {
+  Ctrl* c = I->ctrl;
+  c->liquid = 0;
+  c->air = 0;
+  c->nonfinite = 0;
+  c->done = 0;
+  c->candidate = 0;
+  c->status = 0;
+  c->converged = 0;
+  c->iter = 0;
+  *I->err = 0;
+}
+
+// r = b (cold start: x = 0), ||b||^2, ||b||_inf, thresholds.
+__global__ void k_tall_cg_init(TInst* I, double rel_tol, double abs_tol, int max_iter, int true_every,
+                               double rel_tol_inf) {
+  const TLevel& L = I->lv[0];
+  double bb = 0.0, bmax = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+    const float bv = L.label[k] ? I->b[k] : 0.0f;
+    L.rhs[k] = bv;
+    I->x[k] = 0.0f;
+    I->xlo[k] = 0.0f;
+    I->d[k] = 0.0f;
+    bb += double(bv) * bv;
+    bmax = fmax(bmax, fabs(double(bv)));
+  }
+  const double v[2] = {bb, bmax};
+  const bool mx[2] = {false, true};
+  double o[2];
+  if (reduce_grid<2>(I, 0, v, mx, o) && threadIdx.x == 0) {
+    Ctrl* c = I->ctrl;
+    c->anchored = 1;
+    c->bmean = 0.0;
+    c->bb = o[0];
+    c->rr = o[0];
+    c->rr_true = o[0];
+    const double thr = fmax(abs_tol, rel_tol * sqrt(o[0]));
+    c->thr2 = thr * thr;
+    c->bmax = o[1];
+    c->rmax = o[1];
+    c->thr_inf = rel_tol_inf > 0 ? rel_tol_inf * o[1] : 0.0;
+    c->iter = 0;
+    c->max_iter = max_iter;
+    c->true_every = true_every;
+    c->first = 1;
+    c->candidate = 0;
+    c->converged = 0;
+    c->done = 0;
+    c->status = FLUID_PP_OK;
+    c->dsel = 0;
+    set_sigma(c, o[0]);
+    if (c->nonfinite) {
+      c->done = 1;
+      c->status = FLUID_PP_NONFINITE;
+    } else if (*I->err) {
+      c->done = 1;
+      c->status = FLUID_PP_UNSUPPORTED;
+    } else if (c->liquid == 0 || o[0] <= c->thr2) {
+      c->done = 1;
+      c->converged = 1;
+    }
+  }
+}
+
+// gamma = r . z
+__global__ void k_tall_dot(TInst* I) {
+  const Ctrl* c = I->ctrl;
+  if (c->done) return;
+  const TLevel& L = I->lv[0];
+  double rz = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x)
+    if (L.label[k]) rz += double(L.rhs[k]) * double(L.z[k]);
+  const double v[1] = {rz};
+  const bool mx[1] = {false};
+  double o[1];
+  if (reduce_grid<1>(I, 1, v, mx, o) && threadIdx.x == 0) finish_gamma(I->ctrl, o[0], 0.0, 0.0);
+}
+
+// d = z + beta d
+__global__ void k_tall_dir(TInst* I) {
+  const Ctrl* c = I->ctrl;
+  if (c->done) return;
+  const float beta = float(c->beta);
+  const TLevel& L = I->lv[0];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x)
+    I->d[k] = L.label[k] ? (beta == 0.0f ? L.z[k] : L.z[k] + beta * I->d[k]) : 0.0f;
+}
+
+// q = A d, delta = d . q
+__global__ void k_tall_spmv(TInst* I) {
+  const Ctrl* c = I->ctrl;
+  if (c->done) return;
+  const TLevel& L = I->lv[0];
+  double dq = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+    int x, j, z, b;
+    sample_active(L, k, x, j, z, b);
+    float q = 0.0f;
+    if (L.label[k]) {
+      q = float(apply_row(L, k, x, j, z, I->d));
+      dq += double(I->d[k]) * double(q);
+    }
+    I->q[k] = q;
+  }
+  const double v[1] = {dq};
+  const bool mx[1] = {false};
+  double o[1];
+  if (reduce_grid<1>(I, 2, v, mx, o) && threadIdx.x == 0) finish_delta(I->ctrl, o[0]);
+}
+
+// x += alpha d (double-single), r -= alpha q
+__global__ void k_tall_update(TInst* I) {
+  const Ctrl* c = I->ctrl;
+  if (c->done) return;
+  const double alpha = c->alpha;
+  const float af = float(alpha);
+  const TLevel& L = I->lv[0];
+  double rr = 0.0, mr = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+    if (!L.label[k]) continue;
+    const double xv = double(I->x[k]) + double(I->xlo[k]) + alpha * double(I->d[k]);
+    const float hi = float(xv);
+    I->x[k] = hi;
+    I->xlo[k] = float(xv - double(hi));
+    const float rv = L.rhs[k] - af * I->q[k];
+    L.rhs[k] = rv;
+    rr += double(rv) * rv;
+    mr = fmax(mr, fabs(double(rv)));
+  }
+  const double v[2] = {rr, mr};
+  const bool mx[2] = {false, true};
+  double o[2];
+  if (reduce_grid<2>(I, 3, v, mx, o) && threadIdx.x == 0) finish_update(I->ctrl, o[0], o[1]);
+}
+
+// float64 r = b - A x with the double-single x
+__global__ void k_tall_true(TInst* I) {
+  const Ctrl* c = I->ctrl;
+  if (c->done || (!c->candidate && !(c->true_every > 0 && c->iter % c->true_every == 0))) return;
+  const TLevel& L = I->lv[0];
+  double rr = 0.0, mr = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+    if (!L.label[k]) continue;
+    int x, j, z, b;
+    sample_active(L, k, x, j, z, b);
+    const int col = x + L.nx * z;
+    auto X = [&](int s) { return double(I->x[s]) + double(I->xlo[s]); };
+    double s = double(L.diag[k]) * X(k);
+    if (j >= 2) {
+      for (int e = 0; e < kBandW; ++e) s += double(L.bval[e * L.n + k]) * X(L.bidx[e * L.n + k]);
+    } else {
+      const int nrow = 2 * L.ncol, row = 2 * col + j;
+      s += double(L.a01[col]) * X(sidx(L, x, 1 - j, z));
+      for (int e = 0; e < kTallW; ++e) s += double(L.tval[e * nrow + row]) * X(L.tidx[e * nrow + row]);
+    }
+    const double rv = double(I->b[k]) - s;
+    L.rhs[k] = float(rv);
+    rr += rv * rv;
+    mr = fmax(mr, fabs(rv));
+  }
+  const double v[2] = {rr, mr};
+  const bool mx[2] = {false, true};
+  double o[2];
+  if (reduce_grid<2>(I, 4, v, mx, o) && threadIdx.x == 0) finish_true(I->ctrl, o[0], o[1]);
+}
+
+// ------------------------------------------------------------------ V-cycle
+__global__ void k_tall_zero(TInst* I, int l) {
+  if (I->ctrl->done) return;
+  const TLevel& L = I->lv[l];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) L.z[k] = 0.0f;
+}
+
+// One colour of the block Gauss-Seidel sweep: 0/1 band cells with (x + y + z)
+// even/odd, 2/3 tall blocks of columns with (x + z) even/odd.
+__global__ void k_tall_smooth(TInst* I, int l, int colour) {
+  if (I->ctrl->done) return;
+  const TLevel& L = I->lv[l];
+  if (colour < 2) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+      int x, j, z, b;
+      const bool act = sample_active(L, k, x, j, z, b);
+      if (j < 2 || !act || ((x + b + j - 2 + z) & 1) != colour) continue;
+      if (!L.label[k]) {
+        L.z[k] = 0.0f;
+        continue;
+      }
+      L.z[k] = float((double(L.rhs[k]) - offdiag(L, k, j, x + L.nx * z, L.z)) / double(L.diag[k]));
+    }
+  } else {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < L.ncol; c += gridDim.x * blockDim.x) {
+      const int x = c % L.nx, z = c / L.nx;
+      if (((x + z) & 1) != colour - 2) continue;
+      const int s0 = sidx(L, x, 0, z), s1 = sidx(L, x, 1, z);
+      if (!L.label[s0]) {
+        L.z[s0] = L.z[s1] = 0.0f;
+        continue;
+      }
+      const double r0 = double(L.rhs[s0]) - offdiag(L, s0, 0, c, L.z);
+      const double r1 = double(L.rhs[s1]) - offdiag(L, s1, 1, c, L.z);
+      const double a00 = L.diag[s0], a11 = L.diag[s1], a01 = L.a01[c];
+      const double det = a00 * a11 - a01 * a01;
+      L.z[s0] = float((a11 * r0 - a01 * r1) / det);
+      L.z[s1] = float((a00 * r1 - a01 * r0) / det);
+    }
+  }
+}
+
+// res = scale (rhs - A z); level 0 scales by sigma.
+__global__ void k_tall_residual(TInst* I, int l) {
+  if (I->ctrl->done) return;
+  const TLevel& L = I->lv[l];
+  const double scale = l == 0 ? I->ctrl->sigma : 1.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+    int x, j, z, b;
+    sample_active(L, k, x, j, z, b);
+    L.res[k] = L.label[k] ? float(scale * (double(L.rhs[k]) - apply_row(L, k, x, j, z, L.z))) : 0.0f;
+  }
+}
+
+// Coarse dense cells feeding fine sample (x, row y, z) with their weights.
+struct Taps {
+  int n;
+  int x[8], y[8], z[8];
+  double w[8];
+};
+
+__device__ __forceinline__ void fine_taps(const TLevel& C, int x, int y, int z, Taps& T) {
+  int cx[2], cy[2], cz[2];
+  float wx[2], wy[2], wz[2];
+  const int nxx = taps1d(x, 2, C.nx, cx, wx);
+  const int nyy = taps1d(y, 2, C.fine_ny, cy, wy);
+  const int nzz = taps1d(z, 2, C.nz, cz, wz);
+  T.n = 0;
+  for (int c2 = 0; c2 < nzz; ++c2)
+    for (int c1 = 0; c1 < nyy; ++c1)
+      for (int c0 = 0; c0 < nxx; ++c0) {
+        T.x[T.n] = cx[c0];
+        T.y[T.n] = cy[c1];
+        T.z[T.n] = cz[c2];
+        T.w[T.n] = double(wx[c0]) * double(wy[c1]) * double(wz[c2]);
+        ++T.n;
+      }
+}
+
+// acc_c += 1/2 P^T res_f in 32.32 fixed point (order-independent sums).
+__global__ void k_tall_restrict(TInst* I, int l) {
+  if (I->ctrl->done) return;
+  const TLevel& F = I->lv[l];
+  const TLevel& C = I->lv[l + 1];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < F.n; k += gridDim.x * blockDim.x) {
+    if (!F.label[k]) continue;
+    const float r = F.res[k];
+    if (r == 0.0f) continue;
+    int x, j, z, b;
+    sample_active(F, k, x, j, z, b);
+    Taps T;
+    fine_taps(C, x, sample_row(j, b), z, T);
+    for (int t = 0; t < T.n; ++t) {
+      const Rep rc = rep_of(C, T.x[t], T.y[t], T.z[t]);
+      if (!rc.liq) continue;
+      const double v = 0.5 * T.w[t] * double(r);
+      atomicAdd(&C.acc[rc.s0], (unsigned long long)llrint(v * rc.w0 * kFix));
+      if (rc.n == 2) atomicAdd(&C.acc[rc.s1], (unsigned long long)llrint(v * rc.w1 * kFix));
+    }
+  }
+}
+
+__global__ void k_tall_restrict_finish(TInst* I, int l) {
+  if (I->ctrl->done) return;
+  const TLevel& C = I->lv[l];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C.n; k += gridDim.x * blockDim.x) {
+    const long long a = (long long)C.acc[k];
+    C.rhs[k] = C.label[k] ? float(double(a) / kFix) : 0.0f;
+    C.acc[k] = 0ull;
+  }
+}
+
+// z_f += P z_c on liquid fine samples; into level 0 the sigma scale is undone.
+__global__ void k_tall_prolong(TInst* I, int l) {
+  if (I->ctrl->done) return;
+  const TLevel& F = I->lv[l];
+  const TLevel& C = I->lv[l + 1];
+  const double unscale = l == 0 ? 1.0 / I->ctrl->sigma : 1.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < F.n; k += gridDim.x * blockDim.x) {
+    if (!F.label[k]) continue;
+    int x, j, z, b;
+    sample_active(F, k, x, j, z, b);
+    Taps T;
+    fine_taps(C, x, sample_row(j, b), z, T);
+    double s = 0.0;
+    for (int t = 0; t < T.n; ++t) s += T.w[t] * dense_val(C, C.z, T.x[t], T.y[t], T.z[t]);
+    F.z[k] = float(double(F.z[k]) + s * unscale);
+  }
+}
+
+// z = A^{-1} rhs on the coarsest level (one CTA, a warp per row).
+__global__ void k_tall_coarse_apply(TInst* I) {
+  if (I->ctrl->done) return;
+  const TLevel& L = I->lv[I->nlev - 1];
+  const int m = L.n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int i = warp; i < m; i += nw) {
+    double s = 0.0;
+    for (int j = lane; j < m; j += 32) s += I->coarse_inv[(long long)i * m + j] * (L.label[j] ? double(L.rhs[j]) : 0.0);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) L.z[i] = L.label[i] ? float(s) : 0.0f;
+  }
+}
+
+// ------------------------------------------------------------------ finish
+__device__ __forceinline__ double pressure_at(const TInst& I, const TLevel& L, int x, int y, int z) {
+  const Rep r = rep_of(L, x, y, z);
+  if (!r.liq) return 0.0;
+  auto X = [&](int s) { return double(I.x[s]) + double(I.xlo[s]); };
+  return r.n == 2 ? r.w0 * X(r.s0) + r.w1 * X(r.s1) : X(r.s0);
+}
+
+// Each sample's own +x/+y/+z faces: u -= (p_j - p_i) / theta at the sample's
+// row; faces with no liquid side and wall faces are zero.  Pressure in Pa.
+__global__ void k_tall_grad(TInst* I) {
+  if (I->ctrl->status == FLUID_PP_NONFINITE) return;
+  const TLevel& L = I->lv[0];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+    int x, j, z, b;
+    const bool act = sample_active(L, k, x, j, z, b);
+    if (!act) {
+      I->u[k] = I->v[k] = I->w[k] = 0.0f;
+      I->p_si[k] = 0.0f;
+      continue;
+    }
+    const int y = sample_row(j, b);
+    const Rep ri = rep_of(L, x, y, z);
+    const double pi = pressure_at(*I, L, x, y, z);
+    auto face = [&](float u, int xn, int yn, int zn, bool in) -> float {
+      if (!in) return 0.0f;
+      const Rep rn = rep_of(L, xn, yn, zn);
+      if (!ri.liq && !rn.liq) return 0.0f;
+      const double th = (ri.liq && rn.liq) ? 1.0 : (ri.liq ? ghost_theta_d(ri.phi, rn.phi) : ghost_theta_d(rn.phi, ri.phi));
+      return float(double(u) - (pressure_at(*I, L, xn, yn, zn) - pi) / th);
+    };
+    const float un = face(I->u[k], x + 1, y, z, x + 1 < L.nx);
+    const float vn = face(I->v[k], x, y + 1, z, y + 1 < L.fine_ny);
+    const float wn = face(I->w[k], x, y, z + 1, z + 1 < L.nz);
+    I->p_si[k] = L.label[k] ? float((double(I->x[k]) + double(I->xlo[k])) * double(I->pscale)) : 0.0f;
+    I->u[k] = un;
+    I->v[k] = vn;
+    I->w[k] = wn;
+  }
+}
+
+// Divergence receipts over the liquid band cells the packed faces represent
+// exactly: rows inside the bands of the column and of its four neighbours
+// (every face of such a cell is a sample's own face or a tall cell's top
+// face).  max |div| and sum div^2 of the current packed velocities.
+__global__ void k_tall_receipt(TInst* I, int slot) {
+  const TLevel& L = I->lv[0];
+  double mx = 0.0, ss = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+    int x, j, z, b;
+    const bool act = sample_active(L, k, x, j, z, b);
+    if (j < 2 || !act || !L.label[k]) continue;
+    int lo = b, hi = b;   // rows [lo, hi + band) are inside every band
+    auto nb = [&](int c) {
+      lo = max(lo, L.bases[c]);
+      hi = min(hi, L.bases[c]);
+    };
+    if (x > 0) nb(x - 1 + L.nx * z);
+    if (x + 1 < L.nx) nb(x + 1 + L.nx * z);
+    if (z > 0) nb(x + L.nx * (z - 1));
+    if (z + 1 < L.nz) nb(x + L.nx * (z + 1));
+    const int y = b + j - 2;
+    if (y < lo || y >= hi + L.band) continue;
+    const double dv = dense_div(*I, L, x, b + j - 2, z);
+    mx = fmax(mx, fabs(dv));
+    ss += dv * dv;
+  }
+  const double v[2] = {mx, ss};
+  const bool m2[2] = {true, false};
+  double o[2];
+  if (reduce_grid<2>(I, 5, v, m2, o) && threadIdx.x == 0) {
+    I->ctrl->red[2 * slot] = o[0];
+    I->ctrl->red[2 * slot + 1] = o[1];
+  }
+}
+
+}  // namespace tall
+}  // namespace fpp
+
+// ==================================================================== host
+using namespace fpp;
+using namespace fpp::tall;
+
+struct fluid_pp_tall {
+  fluid_pp_tall_config cfg{};
+  TallPlan plan;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  char* arena = nullptr;
+  TInst inst{};
+  TInst* d_inst = nullptr;
+  Ctrl* h_ctrl = nullptr;
+  bool has_state = false;
+  int set_error(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+};
+
+namespace {
+
+int grid_for(long long n) { return int(std::max(1LL, std::min<long long>((n + kTB - 1) / kTB, kTGrid))); }
+
+size_t up256(size_t v) { return (v + 255) / 256 * 256; }
+
+void launch_vcycle(fluid_pp_tall* T) {
+  TInst& I = T->inst;
+  cudaStream_t s = T->stream;
+  const int L = I.nlev;
+  for (int l = 0; l + 1 < L; ++l) {
+    const int g = grid_for(I.lv[l].n), gc = grid_for(I.lv[l].ncol);
+    k_tall_zero<<<g, kTB, 0, s>>>(T->d_inst, l);
+    k_tall_smooth<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
+    k_tall_smooth<<<g, kTB, 0, s>>>(T->d_inst, l, 1);
+    k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 2);
+    k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 3);
+    k_tall_residual<<<g, kTB, 0, s>>>(T->d_inst, l);
+    k_tall_restrict<<<g, kTB, 0, s>>>(T->d_inst, l);
+    k_tall_restrict_finish<<<grid_for(I.lv[l + 1].n), kTB, 0, s>>>(T->d_inst, l + 1);
+  }
+  k_tall_coarse_apply<<<1, 1024, 0, s>>>(T->d_inst);
+  for (int l = L - 2; l >= 0; --l) {
+    const int g = grid_for(I.lv[l].n), gc = grid_for(I.lv[l].ncol);
+    k_tall_prolong<<<g, kTB, 0, s>>>(T->d_inst, l);
+    k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 3);
+    k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 2);
+    k_tall_smooth<<<g, kTB, 0, s>>>(T->d_inst, l, 1);
+    k_tall_smooth<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
+  }
+}
+
+void launch_setup(fluid_pp_tall* T) {
+  TInst& I = T->inst;
+  cudaStream_t s = T->stream;
+  k_tall_reset<<<1, 1, 0, s>>>(T->d_inst);
+  k_tall_label<<<grid_for(I.lv[0].n), kTB, 0, s>>>(T->d_inst);
+  for (int l = 0; l + 1 < I.nlev; ++l) {
+    k_tall_coarsen<<<grid_for(I.lv[l + 1].n), kTB, 0, s>>>(T->d_inst, l);
+    k_tall_coarse_labels<<<grid_for(I.lv[l + 1].n), kTB, 0, s>>>(T->d_inst, l + 1);
+  }
+  for (int l = 0; l < I.nlev; ++l) {
+    k_tall_assemble_band<<<grid_for(I.lv[l].n), kTB, 0, s>>>(T->d_inst, l);
+    k_tall_assemble_tall<<<grid_for(I.lv[l].ncol), kTB, 0, s>>>(T->d_inst, l);
+  }
+  const size_t m = size_t(I.coarse_m);
+  k_tall_factor<<<1, 1024, m * m * sizeof(double), s>>>(T->d_inst);
+  k_tall_rhs<<<grid_for(I.lv[0].n), kTB, 0, s>>>(T->d_inst);
+}
+
+int tall_create(const fluid_pp_tall_config* cfg, const int* bases, fluid_pp_tall** out) {
+  if (!cfg || !bases || !out) return FLUID_PP_INVALID_ARG;
+  if (cfg->precision != FLUID_PP_FP32) {
+    fpp::set_global_error("the tall-cell solver stores its levels in float32 only");
+    return FLUID_PP_UNSUPPORTED;
+  }
+  TallPlan plan = plan_tall(cfg->nx, cfg->nz, cfg->fine_ny, cfg->band, bases);
+  if (!plan.ok) {
+    fpp::set_global_error(plan.rejection ? plan.rejection : "tall layout rejected");
+    return FLUID_PP_INVALID_ARG;
+  }
+  if (cudaSetDevice(cfg->device) != cudaSuccess) {
+    fpp::set_global_error("cudaSetDevice failed");
+    return FLUID_PP_CUDA;
+  }
+  auto T = std::make_unique<fluid_pp_tall>();
+  T->cfg = *cfg;
+  T->plan = plan;
+  const int L = int(plan.levels.size());
+  // arena size
+  size_t bytes = 0;
+  auto acc = [&](size_t b) { bytes = up256(bytes + b); };
+  for (int l = 0; l < L; ++l) {
+    const TallLevel& P = plan.levels[l];
+    const size_t n = size_t(P.samples()), nc = size_t(P.nx) * P.nz;
+    acc(4 * nc);                                   // bases
+    acc(4 * n); acc(n); acc(4 * n); acc(4 * nc);   // phi label diag a01
+    acc(4 * kBandW * n); acc(4 * kBandW * n);      // bidx bval
+    acc(4 * kTallW * 2 * nc); acc(4 * kTallW * 2 * nc);
+    acc(4 * n); acc(4 * n); acc(4 * n);            // z rhs res
+    if (l > 0) acc(8 * n);                         // acc
+  }
+  const size_t n0 = size_t(plan.levels[0].samples());
+  for (int k = 0; k < 10; ++k) acc(4 * n0);        // vof u v w b x xlo d q p_si
+  acc(sizeof(double) * kSlots * kTGrid);
+  const size_t m = size_t(plan.levels[L - 1].samples());
+  acc(sizeof(double) * m * m);
+  acc(sizeof(Ctrl));
+  acc(sizeof(int));
+  if (cudaMalloc(&T->arena, bytes) != cudaSuccess) {
+    fpp::set_global_error("tall arena allocation failed");
+    return FLUID_PP_OOM;
+  }
+  cudaMemset(T->arena, 0, bytes);
+  size_t used = 0;
+  auto take = [&](size_t b) {
+    void* p = T->arena + used;
+    used = up256(used + b);
+    return p;
+  };
+  TInst& I = T->inst;
+  std::memset(&I, 0, sizeof(I));
+  I.nlev = L;
+  I.h = cfg->h;
+  I.rho = cfg->rho;
+  for (int l = 0; l < L; ++l) {
+    const TallLevel& P = plan.levels[l];
+    TLevel& V = I.lv[l];
+    V.nx = P.nx;
+    V.nz = P.nz;
+    V.fine_ny = P.fine_ny;
+    V.band = P.band;
+    V.P = P.P();
+    V.n = int(P.samples());
+    V.ncol = P.nx * P.nz;
+    const size_t n = size_t(V.n), nc = size_t(V.ncol);
+    V.bases = static_cast<int*>(take(4 * nc));
+    cudaMemcpy(V.bases, P.bases.data(), 4 * nc, cudaMemcpyHostToDevice);
+    V.phi = static_cast<float*>(take(4 * n));
+    V.label = static_cast<uint8_t*>(take(n));
+    V.diag = static_cast<float*>(take(4 * n));
+    V.a01 = static_cast<float*>(take(4 * nc));
+    V.bidx = static_cast<int*>(take(4 * kBandW * n));
+    V.bval = static_cast<float*>(take(4 * kBandW * n));
+    V.tidx = static_cast<int*>(take(4 * kTallW * 2 * nc));
+    V.tval = static_cast<float*>(take(4 * kTallW * 2 * nc));
+    V.z = static_cast<float*>(take(4 * n));
+    V.rhs = static_cast<float*>(take(4 * n));
+    V.res = static_cast<float*>(take(4 * n));
+    V.acc = l > 0 ? static_cast<unsigned long long*>(take(8 * n)) : nullptr;
+  }
+  I.vof = static_cast<float*>(take(4 * n0));
+  I.u = static_cast<float*>(take(4 * n0));
+  I.v = static_cast<float*>(take(4 * n0));
+  I.w = static_cast<float*>(take(4 * n0));
+  I.b = static_cast<float*>(take(4 * n0));
+  I.x = static_cast<float*>(take(4 * n0));
+  I.xlo = static_cast<float*>(take(4 * n0));
+  I.d = static_cast<float*>(take(4 * n0));
+  I.q = static_cast<float*>(take(4 * n0));
+  I.p_si = static_cast<float*>(take(4 * n0));
+  I.partial = static_cast<double*>(take(sizeof(double) * kSlots * kTGrid));
+  I.coarse_inv = static_cast<double*>(take(sizeof(double) * m * m));
+  I.coarse_m = int(m);
+  I.ctrl = static_cast<Ctrl*>(take(sizeof(Ctrl)));
+  I.err = static_cast<int*>(take(sizeof(int)));
+  cudaError_t e = cudaMalloc(&T->d_inst, sizeof(TInst));
+  if (e == cudaSuccess) e = cudaMallocHost(&T->h_ctrl, sizeof(Ctrl));
+  // the largest coarsest level any tall grid can have (the limit is process-wide and never lowered)
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_tall_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(kMaxCoarse * kMaxCoarse * sizeof(double)));
+  if (e != cudaSuccess) {
+    fpp::set_global_error(std::string("tall setup: ") + cudaGetErrorString(e));
+    if (T->d_inst) cudaFree(T->d_inst);
+    if (T->h_ctrl) cudaFreeHost(T->h_ctrl);
+    cudaFree(T->arena);
+    return FLUID_PP_OOM;
+  }
+  cudaMemcpy(T->d_inst, &I, sizeof(TInst), cudaMemcpyHostToDevice);
+  *out = T.release();
+  return FLUID_PP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fluid_pp_tall_choose_base(int lowest_surface, int highest_surface, int fine_ny, int regular_layers,
+                              int liquid_halo, int air_halo) {
+  return tall_choose_base(lowest_surface, highest_surface, fine_ny, regular_layers, liquid_halo, air_halo);
+}
+
+int fluid_pp_tall_limit_bases(float* bases, int nx, int nz, int max_delta, int passes) {
+  if (!bases || nx < 1 || nz < 1 || passes < 0) return FLUID_PP_INVALID_ARG;
+  tall_limit_bases(bases, nx, nz, max_delta, passes);
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_tall_plan(int nx, int nz, int fine_ny, int band, const int* bases, int* level_count, int* level_shapes) {
+  if (!bases || !level_count) return FLUID_PP_INVALID_ARG;
+  TallPlan p = plan_tall(nx, nz, fine_ny, band, bases);
+  if (!p.ok) {
+    fpp::set_global_error(p.rejection ? p.rejection : "tall layout rejected");
+    return FLUID_PP_INVALID_ARG;
+  }
+  *level_count = int(p.levels.size());
+  if (level_shapes)
+    for (size_t l = 0; l < p.levels.size(); ++l) {
+      level_shapes[4 * l + 0] = p.levels[l].nx;
+      level_shapes[4 * l + 1] = p.levels[l].fine_ny;
+      level_shapes[4 * l + 2] = p.levels[l].nz;
+      level_shapes[4 * l + 3] = p.levels[l].band;
+    }
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_tall_create(const fluid_pp_tall_config* config, const int* bases, fluid_pp_tall** out) {
+  return tall_create(config, bases, out);
+}
+
+void fluid_pp_tall_destroy(fluid_pp_tall* T) {
+  if (!T) return;
+  cudaSetDevice(T->cfg.device);
+  if (T->d_inst) cudaFree(T->d_inst);
+  if (T->h_ctrl) cudaFreeHost(T->h_ctrl);
+  if (T->arena) cudaFree(T->arena);
+  delete T;
+}
+
+int fluid_pp_tall_set_stream(fluid_pp_tall* T, void* stream) {
+  if (!T) return FLUID_PP_INVALID_ARG;
+  T->stream = static_cast<cudaStream_t>(stream);
+  return FLUID_PP_OK;
+}
+
+static int tall_upload(fluid_pp_tall* T, const float* vof, const float* u, const float* v, const float* w,
+                       cudaMemcpyKind kind) {
+  if (!T || !vof || !u || !v || !w) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(T->cfg.device);
+  const size_t n = size_t(T->inst.lv[0].n) * 4;
+  cudaError_t e = cudaMemcpyAsync(T->inst.vof, vof, n, kind, T->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(T->inst.u, u, n, kind, T->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(T->inst.v, v, n, kind, T->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(T->inst.w, w, n, kind, T->stream);
+  if (e != cudaSuccess) return T->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  T->has_state = true;
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_tall_upload_state(fluid_pp_tall* T, const float* vof, const float* u, const float* v, const float* w) {
+  return tall_upload(T, vof, u, v, w, cudaMemcpyHostToDevice);
+}
+
+int fluid_pp_tall_upload_state_device(fluid_pp_tall* T, const float* vof, const float* u, const float* v,
+                                      const float* w) {
+  return tall_upload(T, vof, u, v, w, cudaMemcpyDeviceToDevice);
+}
+
+static void tall_set_dt(fluid_pp_tall* T, float dt) {
+  T->inst.dt = dt;
+  T->inst.pscale = T->cfg.rho * T->cfg.h / dt;
+  cudaMemcpyAsync(reinterpret_cast<char*>(T->d_inst) + offsetof(TInst, dt), &T->inst.dt, sizeof(float),
+                  cudaMemcpyHostToDevice, T->stream);
+  cudaMemcpyAsync(reinterpret_cast<char*>(T->d_inst) + offsetof(TInst, pscale), &T->inst.pscale, sizeof(float),
+                  cudaMemcpyHostToDevice, T->stream);
+}
+
+int fluid_pp_tall_project(fluid_pp_tall* T, float dt, const fluid_pp_solve_opts* opts, fluid_pp_receipt* receipt) {
+  if (!T) return FLUID_PP_INVALID_ARG;
+  if (!(dt > 0) || !std::isfinite(dt)) return T->set_error(FLUID_PP_INVALID_ARG, "dt must be positive and finite");
+  if (!T->has_state) return T->set_error(FLUID_PP_INVALID_ARG, "state not uploaded");
+  fluid_pp_solve_opts o{1e-6, 0.0, 200, 1, 1, 0, 0, 0.0};
+  if (opts) o = *opts;
+  if (!(o.rel_tol >= 0) || !(o.abs_tol >= 0) || o.max_iters < 1)
+    return T->set_error(FLUID_PP_INVALID_ARG, "invalid solve options");
+  cudaSetDevice(T->cfg.device);
+  cudaStream_t s = T->stream;
+  TInst& I = T->inst;
+  tall_set_dt(T, dt);
+  launch_setup(T);
+  const int g0 = grid_for(I.lv[0].n);
+  k_tall_receipt<<<g0, kTB, 0, s>>>(T->d_inst, 0);
+  k_tall_cg_init<<<g0, kTB, 0, s>>>(T->d_inst, o.rel_tol, o.abs_tol, o.max_iters, o.true_residual_every,
+                                    o.rel_tol_inf);
+  const int cap = o.max_iters + 2;
+  for (int it = 0; it < cap;) {
+    const int burst = std::min(4, cap - it);
+    for (int k = 0; k < burst; ++k) {
+      if (I.nlev > 1) {
+        launch_vcycle(T);
+      } else {
+        k_tall_coarse_apply<<<1, 1024, 0, s>>>(T->d_inst);
+      }
+      k_tall_dot<<<g0, kTB, 0, s>>>(T->d_inst);
+      k_tall_dir<<<g0, kTB, 0, s>>>(T->d_inst);
+      k_tall_spmv<<<g0, kTB, 0, s>>>(T->d_inst);
+      k_tall_update<<<g0, kTB, 0, s>>>(T->d_inst);
+      k_tall_true<<<g0, kTB, 0, s>>>(T->d_inst);
+    }
+    it += burst;
+    cudaMemcpyAsync(T->h_ctrl, I.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return T->set_error(FLUID_PP_CUDA, std::string("tall solve: ") + cudaGetErrorString(e));
+    if (T->h_ctrl->done) break;
+  }
+  k_tall_grad<<<g0, kTB, 0, s>>>(T->d_inst);
+  k_tall_receipt<<<g0, kTB, 0, s>>>(T->d_inst, 1);
+  cudaMemcpyAsync(T->h_ctrl, I.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return T->set_error(FLUID_PP_CUDA, std::string("tall finish: ") + cudaGetErrorString(e));
+  const Ctrl& c = *T->h_ctrl;
+  int status = c.status;
+  if (!c.done && status == FLUID_PP_OK) status = FLUID_PP_NONCONVERGENCE;
+  if (receipt) {
+    std::memset(receipt, 0, sizeof(*receipt));
+    receipt->status = status;
+    receipt->iterations = c.iter;
+    receipt->liquid_cells = c.liquid;
+    receipt->levels = I.nlev;
+    receipt->b_norm = std::sqrt(std::max(0.0, c.bb));
+    receipt->rel_residual = c.bb > 0 ? std::sqrt(std::max(0.0, c.rr) / c.bb) : 0.0;
+    receipt->true_rel_residual = c.bb > 0 ? std::sqrt(std::max(0.0, c.rr_true) / c.bb) : 0.0;
+    const double hh = T->cfg.h;
+    receipt->max_div_before = c.red[0] / hh;
+    receipt->l2_div_before = std::sqrt(std::max(0.0, c.red[1]) * hh);
+    receipt->max_div_after = c.red[2] / hh;
+    receipt->l2_div_after = std::sqrt(std::max(0.0, c.red[3]) * hh);
+  }
+  if (status == FLUID_PP_UNSUPPORTED)
+    T->err = "a tall row has more neighbour entries than its ELL width (column bases differ too much)";
+  return status;
+}
+
+int fluid_pp_tall_download(fluid_pp_tall* T, float* p, float* u, float* v, float* w) {
+  if (!T) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(T->cfg.device);
+  const size_t n = size_t(T->inst.lv[0].n) * 4;
+  cudaError_t e = cudaSuccess;
+  if (p) e = cudaMemcpyAsync(p, T->inst.p_si, n, cudaMemcpyDeviceToHost, T->stream);
+  if (e == cudaSuccess && u) e = cudaMemcpyAsync(u, T->inst.u, n, cudaMemcpyDeviceToHost, T->stream);
+  if (e == cudaSuccess && v) e = cudaMemcpyAsync(v, T->inst.v, n, cudaMemcpyDeviceToHost, T->stream);
+  if (e == cudaSuccess && w) e = cudaMemcpyAsync(w, T->inst.w, n, cudaMemcpyDeviceToHost, T->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(T->stream);
+  if (e != cudaSuccess) return T->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_tall_get_pressure(fluid_pp_tall* T, float* p) {
+  if (!T || !p) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(T->cfg.device);
+  const size_t n = size_t(T->inst.lv[0].n);
+  std::vector<float> lo(n);
+  cudaError_t e = cudaMemcpy(p, T->inst.x, 4 * n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(lo.data(), T->inst.xlo, 4 * n, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return T->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  for (size_t i = 0; i < n; ++i) p[i] = float(double(p[i]) + double(lo[i]));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_tall_prepare(fluid_pp_tall* T, float dt) {
+  if (!T || !T->has_state || !(dt > 0)) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(T->cfg.device);
+  tall_set_dt(T, dt);
+  launch_setup(T);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(T->stream);
+  if (e != cudaSuccess) return T->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  int err = 0;
+  cudaMemcpy(&err, T->inst.err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (err) return T->set_error(FLUID_PP_UNSUPPORTED, "a tall row overflowed its ELL width");
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_tall_get_rhs(fluid_pp_tall* T, float* b) {
+  if (!T || !b) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(T->cfg.device);
+  cudaError_t e = cudaMemcpy(b, T->inst.b, size_t(T->inst.lv[0].n) * 4, cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? FLUID_PP_OK : T->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+}
+
+int fluid_pp_tall_get_labels(fluid_pp_tall* T, int level, unsigned char* label) {
+  if (!T || !label || level < 0 || level >= T->inst.nlev) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(T->cfg.device);
+  cudaError_t e = cudaMemcpy(label, T->inst.lv[level].label, size_t(T->inst.lv[level].n), cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? FLUID_PP_OK : T->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+}
+
+// out = A p on level 0 (after fluid_pp_tall_prepare); air entries of p ignored.
+int fluid_pp_tall_apply_operator(fluid_pp_tall* T, const float* p, float* out) {
+  if (!T || !p || !out) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(T->cfg.device);
+  const size_t n = size_t(T->inst.lv[0].n);
+  TInst& I = T->inst;
+  cudaMemcpyAsync(I.d, p, 4 * n, cudaMemcpyHostToDevice, T->stream);
+  k_tall_reset<<<1, 1, 0, T->stream>>>(T->d_inst);
+  k_tall_spmv<<<grid_for(n), kTB, 0, T->stream>>>(T->d_inst);
+  cudaMemcpyAsync(out, I.q, 4 * n, cudaMemcpyDeviceToHost, T->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(T->stream);
+  return e == cudaSuccess ? FLUID_PP_OK : T->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+}
+
+const char* fluid_pp_tall_last_error(fluid_pp_tall* T) { return T ? T->err.c_str() : ""; }
+
+}  // extern "C"

@@ -196,6 +196,66 @@ int fluid_pp_batch_profile_read(fluid_pp_batch* batch, double* ms, long long* la
 int fluid_pp_apply_operator_noalloc(int nx, int ny, int nz, const unsigned char* label, const float* diag,
                                     const float* p, float* out, double* p_dot_ap, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Restricted tall-cell grid (lib/core/tall-cell-grid.ts).  An nx x nz grid of
+ * columns over fine_ny world rows: each column has one tall cell over rows
+ * [0, base) and a cubic band of `band` rows above it.  Every per-cell array is
+ * packed per column in P = band + 2 samples, float32 [nz][P][nx]: sample 0 is
+ * the tall cell's bottom subcell (row 0), sample 1 its top subcell
+ * (row base - 1), sample j >= 2 the band row base + j - 2 (tall-cell-grid.ts:
+ * 171-190, 398-409).  Face velocities are packed the same way: each sample
+ * owns the +x, +y and +z faces of its cell.
+ * ---------------------------------------------------------------------- */
+typedef struct fluid_pp_tall fluid_pp_tall;
+
+typedef struct fluid_pp_tall_config {
+  int nx, nz;      /* columns */
+  int fine_ny;     /* world rows */
+  int band;        /* cubic rows per column (B_y) */
+  float h;         /* cell size, m */
+  float rho;       /* liquid density, kg/m^3 */
+  int precision;   /* FLUID_PP_FP32 */
+  int device;
+} fluid_pp_tall_config;
+
+/* chooseTallCellBase (lib/core/tall-cell-grid.ts:61-82), host only. */
+int fluid_pp_tall_choose_base(int lowest_surface, int highest_surface, int fine_ny, int regular_layers,
+                              int liquid_halo, int air_halo);
+
+/* limitNeighboringTallCellBases (tall-cell-grid.ts:84-106), host only; bases
+ * (x + nx * z) are limited in place. */
+int fluid_pp_tall_limit_bases(float* bases, int nx, int nz, int max_delta, int passes);
+
+/* Tall multigrid hierarchy, host only: level_shapes receives level_count * 4
+ * ints (nx, fine_ny, nz, band), finest first. */
+int fluid_pp_tall_plan(int nx, int nz, int fine_ny, int band, const int* bases, int* level_count, int* level_shapes);
+
+/* Replaces the restricted backend's pressure setup (createTallCellLayout,
+ * tall-cell-grid.ts:309-436, plus the tall-cell multigrid of
+ * docs/papers/tallCells.txt Alg. 2): allocates the hierarchy for the given
+ * bases (every base >= 2, band inside the domain).  Errors: fluid_pp_last_error(NULL). */
+int fluid_pp_tall_create(const fluid_pp_tall_config* config, const int* bases, fluid_pp_tall** out);
+void fluid_pp_tall_destroy(fluid_pp_tall* tall);
+int fluid_pp_tall_set_stream(fluid_pp_tall* tall, void* stream);
+/* Packed VOF and owned face velocities from host (or device) memory. */
+int fluid_pp_tall_upload_state(fluid_pp_tall* tall, const float* vof, const float* u, const float* v, const float* w);
+int fluid_pp_tall_upload_state_device(fluid_pp_tall* tall, const float* vof, const float* u, const float* v,
+                                      const float* w);
+/* Labels, assembly, MGPCG to the tolerance, gradient subtract on the packed
+ * faces, receipt (divergence receipts over liquid band cells). */
+int fluid_pp_tall_project(fluid_pp_tall* tall, float dt, const fluid_pp_solve_opts* opts, fluid_pp_receipt* receipt);
+/* Pressure in Pa and the projected faces, packed. */
+int fluid_pp_tall_download(fluid_pp_tall* tall, float* p, float* u, float* v, float* w);
+/* Diagnostics for parity tests: prepare runs labels, hierarchy and assembly
+ * for dt; then the finest-level rhs, labels per level, A p, the solved pressure
+ * (finest-cell units, double-single rounded once). */
+int fluid_pp_tall_prepare(fluid_pp_tall* tall, float dt);
+int fluid_pp_tall_get_rhs(fluid_pp_tall* tall, float* b);
+int fluid_pp_tall_get_labels(fluid_pp_tall* tall, int level, unsigned char* label);
+int fluid_pp_tall_apply_operator(fluid_pp_tall* tall, const float* p, float* out);
+int fluid_pp_tall_get_pressure(fluid_pp_tall* tall, float* p);
+const char* fluid_pp_tall_last_error(fluid_pp_tall* tall);
+
 #ifdef __cplusplus
 }
 #endif
