@@ -369,6 +369,34 @@ def main():
     tot_prof = sum(v["ms"] for v in prof.values())
     traffic = NCU_TRAFFIC_BYTES.get(dom)
 
+    # ------------------------------------ secondary: tall-cell 256^2 columns x 1024 rows
+    note("tall-cell waves")
+    from fluid_b200.tall import TallProjector
+    ts = configs.tall_waves()
+    tp = TallProjector(ts.nx, ts.nz, ts.fine_ny, ts.band, ts.bases, ts.h, ts.rho, device=local)
+    tp.set_stream(stream.cuda_stream)
+    dev3 = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (ts.vof, ts.u, ts.v, ts.w)]
+    t3, r3 = [], None
+    steps3 = max(3, min(args.steps, 20))
+
+    def tall_step():
+        tp.upload_state_device(*(t.data_ptr() for t in dev3))
+        return tp.project(ts.dt, rel_tol=1e-6)
+    for k in range(args.warmup + steps3):
+        ms, r3 = timed(tall_step)
+        if k >= args.warmup:
+            t3.append(ms)
+    tp.destroy()
+    tall_line = {
+        "workload": ts.meta["workload"] + ", surface 600 + 8 seeded sinusoids (amplitude <= 12, wavelength 16-256)",
+        "samples": ts.samples, "dense_equivalent_cells": ts.dense_cells, "steps": steps3,
+        "solves_per_s": len(t3) / (sum(t3) / 1000.0), "p50_ms": statistics.median(t3),
+        "p99_ms": float(np.percentile(t3, 99)), "iterations": r3["iterations"], "levels": r3["levels"],
+        "status": r3["status_name"], "true_rel_residual": r3["true_rel_residual"],
+        "sample_iterations_per_s": ts.samples * r3["iterations"] * len(t3) / (sum(t3) / 1000.0),
+        "precision": "f32 levels, f32 CG vectors, f64 dots/scalars/coarsest",
+    }
+
     # ------------------------------------------- e2e: public API from host buffers
     note("e2e from host buffers")
     pps = make(args.precision)
@@ -430,6 +458,7 @@ def main():
             "iterations_mean": statistics.mean(r["iterations"] for r in r2_mixed),
             "stage_ms_per_solve": {k: round(v["ms"] / steps2, 4) for k, v in sorted(prof.items())},
         },
+        "tall_cell_256x256x1024": tall_line,
         "roofline": {"bound": "hbm", "kernel": dom, "workload": "dam_spheres_128x96x128 (one instance per launch)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": peak_kind, "traffic": traffic, "alg_bytes_per_launch": alg,

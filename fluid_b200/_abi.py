@@ -31,7 +31,8 @@ EXPORTS = (
     "fluid_pp_tall_destroy", "fluid_pp_tall_set_stream", "fluid_pp_tall_upload_state",
     "fluid_pp_tall_upload_state_device", "fluid_pp_tall_project", "fluid_pp_tall_download",
     "fluid_pp_tall_prepare", "fluid_pp_tall_get_rhs", "fluid_pp_tall_get_labels", "fluid_pp_tall_apply_operator",
-    "fluid_pp_tall_get_pressure", "fluid_pp_tall_last_error",
+    "fluid_pp_tall_get_pressure", "fluid_pp_tall_last_error", "fluid_pp_required_bytes",
+    "fluid_pp_tall_required_bytes", "fluid_pp_batch_set_graphs",
 )
 STAGES = ("reset", "label", "coarsen", "bake", "factor", "init", "smooth0", "smoothc", "residual0", "residualc",
           "restrict0", "restrictc", "coarse", "prolong0", "prolongc", "dot", "dir", "spmv", "update", "true",
@@ -113,6 +114,7 @@ def load():
     L.fluid_pp_set_profiling.argtypes = [vp, ci]
     L.fluid_pp_profile_read.argtypes = [vp, vp, vp, ci]
     L.fluid_pp_batch_set_profiling.argtypes = [vp, ci]
+    L.fluid_pp_batch_set_graphs.argtypes = [vp, ci]
     L.fluid_pp_batch_profile_read.argtypes = [vp, vp, vp, ci]
     L.fluid_pp_apply_operator_noalloc.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp, vp]
     L.fluid_pp_tall_choose_base.argtypes = [ci, ci, ci, ci, ci, ci]
@@ -133,6 +135,8 @@ def load():
     L.fluid_pp_tall_get_pressure.argtypes = [vp, vp]
     L.fluid_pp_tall_last_error.argtypes = [vp]
     L.fluid_pp_tall_last_error.restype = ctypes.c_char_p
+    L.fluid_pp_required_bytes.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_ulonglong)]
+    L.fluid_pp_tall_required_bytes.argtypes = [ctypes.POINTER(TallConfig), vp, ctypes.POINTER(ctypes.c_ulonglong)]
     _lib = L
     return L
 

@@ -105,6 +105,9 @@ struct fluid_pp_batch {
   bool pending_graph_count = false;
   // per-stage kernel timing (events on the launching stream), off by default
   bool profiling = false;
+  // CUDA graphs for the solve (on by default); a batch whose composition changes
+  // every few solves runs direct launches instead of paying for a new capture
+  bool use_graphs = true;
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
   std::vector<int> ev_stage;
@@ -650,7 +653,7 @@ static int batch_project_t(fluid_pp_batch* B, const float* dts, const fluid_pp_s
                     sizeof(float), cudaMemcpyHostToDevice, B->stream);
   }
   bool graphed = false;
-  if (!B->profiling) {
+  if (!B->profiling && B->use_graphs) {
     const int rc = ensure_graphs<T>(B, o);
     if (rc != FLUID_PP_OK) return rc;
     cudaError_t e = cudaGraphLaunch(B->x_setup, B->stream);
@@ -754,6 +757,39 @@ int fluid_pp_plan_hierarchy(int nx, int ny, int nz, int* level_count, int* level
   return FLUID_PP_OK;
 }
 
+// Device bytes of one handle's arena (every level, the resident state, the CG
+// vectors, reduction partials, the dense coarsest inverse, the control block).
+static size_t arena_size(const fluid_pp_config& cfg, const HierarchyPlan& plan) {
+  const size_t sT = storage_bytes(cfg.precision);
+  const int nx = cfg.nx, ny = cfg.ny, nz = cfg.nz;
+  const long long N = (long long)nx * ny * nz;
+  size_t bytes = 0;
+  auto acc = [&](size_t b) { bytes = align_up(bytes + b, 256); };
+  for (int l = 0; l < plan.levels; ++l) {
+    const long long n = (long long)plan.dims[l][0] * plan.dims[l][1] * plan.dims[l][2];
+    acc(n);                        // label
+    acc(4 * n);                    // phi
+    acc(4 * n);                    // diag
+    acc(sT * n);                   // diagT
+    acc((l == 0 ? 4 : sT) * n);    // z
+    acc((l == 0 ? 4 : sT) * n);    // rhs / r
+    acc((l == 0 ? 4 : sT) * n);    // res (z type)
+  }
+  const long long nu = (long long)(nx + 1) * ny * nz, nv = (long long)nx * (ny + 1) * nz,
+                  nw = (long long)nx * ny * (nz + 1);
+  acc(4 * N);                      // vof
+  acc(4 * nu);
+  acc(4 * nv);
+  acc(4 * nw);
+  for (int k = 0; k < 7; ++k) acc(4 * N);   // b x xlo d d2 q p_si
+  const long long ncoarse =
+      (long long)plan.dims[plan.levels - 1][0] * plan.dims[plan.levels - 1][1] * plan.dims[plan.levels - 1][2];
+  acc(sizeof(double) * kSlots * tiles_of(nx, ny, nz, kMaxDepth));
+  acc(sizeof(double) * ncoarse * ncoarse);
+  acc(sizeof(Ctrl));
+  return bytes;
+}
+
 int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
   g_err.clear();
   if (!cfg || !out) return FLUID_PP_INVALID_ARG;
@@ -787,26 +823,6 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
   const size_t sT = storage_bytes(cfg->precision);
   const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
   const long long N = (long long)nx * ny * nz;
-  // size the arena
-  size_t bytes = 0;
-  auto acc = [&](size_t b) { bytes = align_up(bytes + b, 256); };
-  for (int l = 0; l < plan.levels; ++l) {
-    const long long n = (long long)plan.dims[l][0] * plan.dims[l][1] * plan.dims[l][2];
-    acc(n);             // label
-    acc(4 * n);         // phi
-    acc(4 * n);         // diag
-    acc(sT * n);        // diagT
-    acc((l == 0 ? 4 : sT) * n);   // z
-    acc((l == 0 ? 4 : sT) * n);   // rhs / r
-    acc((l == 0 ? 4 : sT) * n);   // res (z type)
-  }
-  const long long nu = (long long)(nx + 1) * ny * nz, nv = (long long)nx * (ny + 1) * nz,
-                  nw = (long long)nx * ny * (nz + 1);
-  acc(4 * N);           // vof
-  acc(4 * nu);
-  acc(4 * nv);
-  acc(4 * nw);
-  for (int k = 0; k < 7; ++k) acc(4 * N);   // b x xlo d d2 q p_si
   if (N > (1LL << 30)) {
     g_err = "lattice exceeds 2^30 cells";
     return FLUID_PP_INVALID_ARG;
@@ -815,9 +831,9 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
   // (148 x 2048 threads) in flight; small levels get one cell per thread.
   auto depth_of = [](long long n) { return n >= 4LL * 600000 ? 4 : n >= 2LL * 600000 ? 2 : 1; };
   const int nt0 = tiles_of(nx, ny, nz, kMaxDepth);   // level 0: 32 x 8 x 8 tiles
-  acc(sizeof(double) * kSlots * nt0);
-  acc(sizeof(double) * ncoarse * ncoarse);
-  acc(sizeof(Ctrl));
+  const size_t bytes = arena_size(*cfg, plan);
+  const long long nu = (long long)(nx + 1) * ny * nz, nv = (long long)nx * (ny + 1) * nz,
+                  nw = (long long)nx * ny * (nz + 1);
   cudaError_t e = cudaMalloc(&h->arena, bytes);
   if (e != cudaSuccess) {
     g_err = std::string("arena allocation: ") + cudaGetErrorString(e);
@@ -935,6 +951,19 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
     return rc;
   }
   *out = h.release();
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_required_bytes(const fluid_pp_config* cfg, unsigned long long* bytes) {
+  if (!cfg || !bytes) return FLUID_PP_INVALID_ARG;
+  HierarchyPlan plan = plan_hierarchy(cfg->nx, cfg->ny, cfg->nz);
+  if (!plan.ok) {
+    g_err = plan.rejection ? plan.rejection : "no hierarchy";
+    return FLUID_PP_INVALID_ARG;
+  }
+  // the arena plus the handle's own batch tables (tile lists, descriptors)
+  const long long N = (long long)cfg->nx * cfg->ny * cfg->nz;
+  *bytes = arena_size(*cfg, plan) + sizeof(InstDev) + sizeof(Ctrl) + size_t(N / 64 + 4096) * sizeof(Tile);
   return FLUID_PP_OK;
 }
 
@@ -1157,6 +1186,12 @@ void fluid_pp_batch_destroy(fluid_pp_batch* B) {
 }
 
 unsigned long long fluid_pp_kernel_launches(void) { return g_launches.load(); }
+
+int fluid_pp_batch_set_graphs(fluid_pp_batch* B, int on) {
+  if (!B) return FLUID_PP_INVALID_ARG;
+  B->use_graphs = on != 0;
+  return FLUID_PP_OK;
+}
 
 int fluid_pp_batch_set_profiling(fluid_pp_batch* B, int on) {
   if (!B) return FLUID_PP_INVALID_ARG;

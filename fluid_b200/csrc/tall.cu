@@ -921,26 +921,10 @@ void launch_setup(fluid_pp_tall* T) {
   k_tall_rhs<<<grid_for(I.lv[0].n), kTB, 0, s>>>(T->d_inst);
 }
 
-int tall_create(const fluid_pp_tall_config* cfg, const int* bases, fluid_pp_tall** out) {
-  if (!cfg || !bases || !out) return FLUID_PP_INVALID_ARG;
-  if (cfg->precision != FLUID_PP_FP32) {
-    fpp::set_global_error("the tall-cell solver stores its levels in float32 only");
-    return FLUID_PP_UNSUPPORTED;
-  }
-  TallPlan plan = plan_tall(cfg->nx, cfg->nz, cfg->fine_ny, cfg->band, bases);
-  if (!plan.ok) {
-    fpp::set_global_error(plan.rejection ? plan.rejection : "tall layout rejected");
-    return FLUID_PP_INVALID_ARG;
-  }
-  if (cudaSetDevice(cfg->device) != cudaSuccess) {
-    fpp::set_global_error("cudaSetDevice failed");
-    return FLUID_PP_CUDA;
-  }
-  auto T = std::make_unique<fluid_pp_tall>();
-  T->cfg = *cfg;
-  T->plan = plan;
+// Device bytes of one tall handle's arena (every level's arrays and ELL rows,
+// the packed state, the CG vectors, partials, coarsest inverse, control).
+size_t tall_arena_size(const TallPlan& plan) {
   const int L = int(plan.levels.size());
-  // arena size
   size_t bytes = 0;
   auto acc = [&](size_t b) { bytes = up256(bytes + b); };
   for (int l = 0; l < L; ++l) {
@@ -960,6 +944,31 @@ int tall_create(const fluid_pp_tall_config* cfg, const int* bases, fluid_pp_tall
   acc(sizeof(double) * m * m);
   acc(sizeof(Ctrl));
   acc(sizeof(int));
+  return bytes;
+}
+
+int tall_create(const fluid_pp_tall_config* cfg, const int* bases, fluid_pp_tall** out) {
+  if (!cfg || !bases || !out) return FLUID_PP_INVALID_ARG;
+  if (cfg->precision != FLUID_PP_FP32) {
+    fpp::set_global_error("the tall-cell solver stores its levels in float32 only");
+    return FLUID_PP_UNSUPPORTED;
+  }
+  TallPlan plan = plan_tall(cfg->nx, cfg->nz, cfg->fine_ny, cfg->band, bases);
+  if (!plan.ok) {
+    fpp::set_global_error(plan.rejection ? plan.rejection : "tall layout rejected");
+    return FLUID_PP_INVALID_ARG;
+  }
+  if (cudaSetDevice(cfg->device) != cudaSuccess) {
+    fpp::set_global_error("cudaSetDevice failed");
+    return FLUID_PP_CUDA;
+  }
+  auto T = std::make_unique<fluid_pp_tall>();
+  T->cfg = *cfg;
+  T->plan = plan;
+  const int L = int(plan.levels.size());
+  const size_t bytes = tall_arena_size(plan);
+  const size_t n0 = size_t(plan.levels[0].samples());
+  const size_t m = size_t(plan.levels[L - 1].samples());
   if (cudaMalloc(&T->arena, bytes) != cudaSuccess) {
     fpp::set_global_error("tall arena allocation failed");
     return FLUID_PP_OOM;
@@ -1257,5 +1266,16 @@ int fluid_pp_tall_apply_operator(fluid_pp_tall* T, const float* p, float* out) {
 }
 
 const char* fluid_pp_tall_last_error(fluid_pp_tall* T) { return T ? T->err.c_str() : ""; }
+
+int fluid_pp_tall_required_bytes(const fluid_pp_tall_config* cfg, const int* bases, unsigned long long* bytes) {
+  if (!cfg || !bases || !bytes) return FLUID_PP_INVALID_ARG;
+  TallPlan plan = plan_tall(cfg->nx, cfg->nz, cfg->fine_ny, cfg->band, bases);
+  if (!plan.ok) {
+    fpp::set_global_error(plan.rejection ? plan.rejection : "tall layout rejected");
+    return FLUID_PP_INVALID_ARG;
+  }
+  *bytes = tall_arena_size(plan) + sizeof(TInst);
+  return FLUID_PP_OK;
+}
 
 }  // extern "C"

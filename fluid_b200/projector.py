@@ -233,6 +233,10 @@ class BatchProjector:
     def set_profiling(self, on: bool):
         _check(load().fluid_pp_batch_set_profiling(self._b, int(bool(on))), None)
 
+    def set_graphs(self, on: bool):
+        """CUDA-graph replay (default) or direct launches; results are identical."""
+        _check(load().fluid_pp_batch_set_graphs(self._b, int(bool(on))), None)
+
     def profile(self, reset: bool = True) -> dict:
         return _read_profile(load().fluid_pp_batch_profile_read, self._b, reset)
 

@@ -1,0 +1,307 @@
+"""Continuous-batching projection server: many resident simulations on one GPU.
+
+Stands where the reference's per-simulation advance loop stands
+(``GPUSolverInstance.advanceTo``, lib/core/method-contract.ts:355, driven per
+simulation from the render worker): every admitted simulation keeps its
+state, hierarchy and CG workspace resident on the device, and each server tick
+runs one projection step of every resident simulation.  The uniform ones run
+as one batched solve (one launch per kernel stage across all of them,
+``fluid_pp_batch_project``); the tall-cell ones run in a second host thread on
+their own stream, so both kinds of work overlap on the device.
+
+Admission is FIFO by an HBM budget (``fluid_pp_required_bytes`` /
+``fluid_pp_tall_required_bytes`` plus the resident state) and a slot limit: a
+request that arrives while others are on the GPU joins at the next tick once
+memory and a slot are free, and leaves the batch when its steps are done.
+
+Step latency is wall time from the moment a step is ready (the simulation's
+previous step finished, or its admission) to the moment its projection has
+finished, as a client of the server would see it.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import statistics
+import time
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi, configs
+from ._abi import Config, TallConfig, load
+from .projector import BatchProjector, PressureProjector
+from .tall import TallProjector
+
+
+@dataclass
+class Request:
+    rid: int
+    kind: str                  # "uniform" | "tall"
+    states: list               # states the steps cycle through (configs.GridState / TallState)
+    steps: int
+    arrival: float             # seconds after the start of the run
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def cells(self) -> int:
+        s = self.states[0]
+        return s.cells if self.kind == "uniform" else s.samples
+
+
+def required_bytes(req: Request, precision: str) -> int:
+    """Device bytes the request holds while resident (handle + its state copies)."""
+    s = req.states[0]
+    out = ctypes.c_ulonglong()
+    L = load()
+    if req.kind == "uniform":
+        cfg = Config(s.nx, s.ny, s.nz, float(s.h), float(s.rho), int(s.open_top), _abi.PRECISIONS[precision], 0)
+        rc = L.fluid_pp_required_bytes(ctypes.byref(cfg), ctypes.byref(out))
+        state = 4 * (s.cells + (s.nx + 1) * s.ny * s.nz + s.nx * (s.ny + 1) * s.nz + s.nx * s.ny * (s.nz + 1))
+    else:
+        cfg = TallConfig(s.nx, s.nz, s.fine_ny, s.band, float(s.h), float(s.rho), _abi.PRECISIONS["fp32"], 0)
+        b = np.ascontiguousarray(s.bases.ravel(), np.int32)
+        rc = L.fluid_pp_tall_required_bytes(ctypes.byref(cfg), _abi.ptr(b), ctypes.byref(out))
+        state = 4 * 4 * s.samples
+    if rc != _abi.OK:
+        raise ValueError(L.fluid_pp_last_error(None).decode())
+    return int(out.value) + state * len(req.states)
+
+
+class _Sim:
+    def __init__(self, req: Request, precision: str, device: int, stream, torch):
+        self.req = req
+        self.kind = req.kind
+        s = req.states[0]
+        if req.kind == "uniform":
+            self.h = PressureProjector((s.nx, s.ny, s.nz), s.h, s.rho, s.open_top, precision, device)
+        else:
+            self.h = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho, "fp32", device)
+        self.h.set_stream(stream.cuda_stream)
+        with torch.cuda.stream(stream):
+            self.dev = [tuple(torch.from_numpy(np.ascontiguousarray(a)).to(f"cuda:{device}", non_blocking=False)
+                              for a in (st.vof, st.u, st.v, st.w)) for st in req.states]
+        self.step = 0
+        self.ready = 0.0
+        self.latencies: list[float] = []
+        self.receipts: list[dict] = []
+        self.pressures: list[np.ndarray] = []
+
+    def upload(self):
+        d = self.dev[self.step % len(self.dev)]
+        self.h.upload_state_device(*(t.data_ptr() for t in d))
+
+    @property
+    def dt(self) -> float:
+        return self.req.states[self.step % len(self.req.states)].dt
+
+    def destroy(self):
+        self.h.destroy()
+        self.dev = None
+
+
+class Server:
+    """Admits requests by HBM budget and runs one projection step of every resident
+    simulation per tick (continuous batching)."""
+
+    def __init__(self, budget_bytes: float = 150e9, max_slots: int = 48, precision: str = "fp16", device: int = 0,
+                 rel_tol: float = 1e-6, record: bool = False):
+        import torch
+        self.torch = torch
+        self.budget = float(budget_bytes)
+        self.max_slots = int(max_slots)
+        self.precision = precision
+        self.device = int(device)
+        self.rel_tol = float(rel_tol)
+        self.record = record
+        torch.cuda.set_device(self.device)
+        self.s_uniform = torch.cuda.Stream(device=self.device)
+        self.pool = ThreadPoolExecutor(max_workers=self.max_slots)
+        self.pending: list[tuple[Request, int]] = []
+        self.active: list[_Sim] = []
+        self.done: list[_Sim] = []
+        self.used = 0.0
+        self.peak_used = 0.0
+        self._batch = None
+        self._batch_key = None
+        self.batch_sizes: list[int] = []
+        self.ticks = 0
+
+    # -- admission ----------------------------------------------------------------
+    def submit(self, req: Request):
+        self.pending.append((req, required_bytes(req, self.precision)))
+
+    def _admit(self, now: float):
+        while self.pending and len(self.active) < self.max_slots:
+            req, need = self.pending[0]
+            if self.used + need > self.budget:
+                if not self.active and need > self.budget:
+                    raise MemoryError(f"request {req.rid} needs {need} bytes, over the whole budget")
+                break
+            self.pending.pop(0)
+            # uniform simulations share the batch's stream; each tall one gets its own
+            stream = self.s_uniform if req.kind == "uniform" else self.torch.cuda.Stream(device=self.device)
+            sim = _Sim(req, self.precision, self.device, stream, self.torch)
+            sim.bytes = need
+            sim.ready = now
+            self.used += need
+            self.peak_used = max(self.peak_used, self.used)
+            self.active.append(sim)
+
+    # -- one tick -------------------------------------------------------------------
+    def _uniform_batch(self, sims):
+        key = tuple(id(s.h) for s in sims)
+        if key != self._batch_key:
+            if self._batch is not None:
+                self._batch.destroy()
+            self._batch = BatchProjector([s.h for s in sims]) if sims else None
+            if self._batch is not None:
+                self._batch.set_graphs(False)   # lives for a few ticks: direct launches beat a new capture
+            self._batch_key = key
+        return self._batch
+
+    def tick(self, clock):
+        uni = [s for s in self.active if s.kind == "uniform"]
+        tall = [s for s in self.active if s.kind == "tall"]
+        finished: dict[int, float] = {}
+        errors: list[BaseException] = []
+
+        def run_uniform():
+            try:
+                if not uni:
+                    return
+                for s in uni:
+                    s.upload()
+                recs = self._uniform_batch(uni).project([s.dt for s in uni], rel_tol=self.rel_tol)
+                t = clock()
+                for s, r in zip(uni, recs):
+                    s.receipts.append(r)
+                    finished[id(s)] = t
+                self.batch_sizes.append(len(uni))
+            except BaseException as e:   # surfaced after join
+                errors.append(e)
+
+        def run_tall(s):
+            s.upload()
+            r = s.h.project(s.dt, rel_tol=self.rel_tol)
+            s.receipts.append(r)
+            finished[id(s)] = clock()
+
+        futures = [self.pool.submit(run_tall, s) for s in tall]
+        run_uniform()
+        for f in futures:
+            try:
+                f.result()
+            except BaseException as e:
+                errors.append(e)
+        if errors:
+            raise errors[0]
+        self.ticks += 1
+        for s in list(self.active):
+            t = finished[id(s)]
+            s.latencies.append(t - s.ready)
+            if self.record:
+                s.pressures.append(s.h.pressure_cells() if s.kind == "uniform" else s.h.pressure())
+            s.ready = t
+            s.step += 1
+            if s.step >= s.req.steps:
+                self.active.remove(s)
+                self.used -= s.bytes
+                s.destroy()
+                self.done.append(s)
+        if not any(s.kind == "uniform" for s in self.active) and self._batch is not None:
+            self._batch.destroy()
+            self._batch, self._batch_key = None, None
+
+    # -- the loop -------------------------------------------------------------------
+    def run(self, requests: list[Request], duration_s: float | None = None) -> dict:
+        """Feeds requests at their arrival times (wall clock) and ticks until every
+        request finished, or until duration_s (then the run stops after the tick)."""
+        queue = sorted(requests, key=lambda r: r.arrival)
+        t0 = time.perf_counter()
+        clock = lambda: time.perf_counter() - t0
+        i = 0
+        while True:
+            now = clock()
+            while i < len(queue) and queue[i].arrival <= now:
+                self.submit(queue[i])
+                i += 1
+            self._admit(now)
+            if self.active:
+                self.tick(clock)
+            elif i < len(queue):
+                time.sleep(max(0.0, min(0.005, queue[i].arrival - clock())))
+            elif not self.pending:
+                break
+            if duration_s is not None and clock() >= duration_s:
+                break
+        elapsed = clock()
+        sims = self.done + self.active
+        lat = [x for s in sims for x in s.latencies]
+        big = [x for s in sims if s.req.cells >= 1_200_000 for x in s.latencies]
+        out = {
+            "elapsed_s": elapsed, "requests_submitted": i, "requests_finished": len(self.done),
+            "requests_resident_at_end": len(self.active), "requests_waiting_at_end": len(self.pending),
+            "step_solves": len(lat), "solves_per_s": len(lat) / elapsed if elapsed > 0 else 0.0,
+            "p50_step_ms": 1000 * statistics.median(lat) if lat else None,
+            "p99_step_ms": 1000 * float(np.percentile(lat, 99)) if lat else None,
+            "p99_step_ms_ge_1p2M_cells": 1000 * float(np.percentile(big, 99)) if big else None,
+            "steps_ge_1p2M_cells": len(big), "ticks": self.ticks,
+            "mean_uniform_batch": statistics.mean(self.batch_sizes) if self.batch_sizes else 0.0,
+            "peak_resident_bytes": self.peak_used,
+            "failed_steps": sum(1 for s in sims for r in s.receipts if r["status_name"] != "OK"),
+        }
+        return out
+
+    def shutdown(self):
+        self.pool.shutdown(wait=True)
+        for s in self.active:
+            s.destroy()
+        self.active = []
+        if self._batch is not None:
+            self._batch.destroy()
+            self._batch = None
+
+
+def serving_requests(rate: float = 40.0, duration_s: float = 120.0, seed: int = 5, templates: int = 6,
+                     steps=(30, 300), uniform_edge=(32, 160), tall_side=(64, 256), tall_band=(24, 40),
+                     tall_rows: int = 256, pin_1p2m: bool = True) -> list[Request]:
+    """Poisson arrivals (rate per second) over duration_s: 50/50 a uniform grid
+    (edges log-uniform in uniform_edge per axis) or a tall-cell grid (columns
+    log-uniform side in tall_side, band uniform in tall_band), each for a seeded
+    number of steps.  The states come from `templates` seeded shapes of each kind
+    (two consecutive states per shape, the steps alternate between them), so the
+    stream needs no per-request generation on the host; with pin_1p2m the first
+    uniform shape is a 1.2M-cell grid, so the stream always holds that size."""
+    rng = np.random.default_rng(seed)
+    uni_t, tall_t = [], []
+    for k in range(templates):
+        nx, ny, nz = (configs.log_uniform_edge(rng, *uniform_edge) for _ in range(3))
+        if k == 0 and pin_1p2m:
+            nx, ny, nz = 112, 96, 112   # 1,204,224 cells: the size the latency target names
+        pair = []
+        for step in range(2):
+            vof = configs.random_liquid(nx, ny, nz, np.random.default_rng(seed * 1000 + k))
+            u, v, w = configs.velocities(vof, np.random.default_rng(seed * 1000 + k + 17 * step), 1 / 60, "gauss", 0.2)
+            pair.append(configs.GridState(nx, ny, nz, 1.0 / max(nx, ny, nz), 1 / 60, vof, u, v, w))
+        uni_t.append(pair)
+        side = int(round(math.exp(rng.uniform(math.log(tall_side[0]), math.log(tall_side[1])))))
+        band = int(rng.integers(tall_band[0], tall_band[1] + 1))
+        s0 = configs.tall_waves(side, side, tall_rows, band, seed=seed * 1000 + k, mean=0.6 * tall_rows, amp_max=8)
+        # the second state keeps the layout (bases are fixed per handle) and redraws the velocities
+        vrng = np.random.default_rng(seed * 1000 + k + 17)
+        redraw = lambda a: np.where(a != 0, vrng.normal(0.0, 0.1, a.shape), 0.0).astype(np.float32)
+        s1 = configs.TallState(s0.nx, s0.nz, s0.fine_ny, s0.band, s0.bases, s0.h, s0.dt, s0.vof, redraw(s0.u),
+                               redraw(s0.v), redraw(s0.w), meta=dict(s0.meta))
+        tall_t.append([s0, s1])
+    out, t, rid = [], 0.0, 0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration_s:
+            break
+        kind = "uniform" if rng.random() < 0.5 else "tall"
+        tpl = (uni_t if kind == "uniform" else tall_t)[int(rng.integers(0, templates))]
+        out.append(Request(rid, kind, tpl, int(rng.integers(steps[0], steps[1] + 1)), t))
+        rid += 1
+    return out

@@ -106,6 +106,10 @@ int fluid_pp_plan_hierarchy(int nx, int ny, int nz, int* level_count, int* level
  * (:311-324): allocates every level and the resident state. */
 int fluid_pp_create(const fluid_pp_config* config, fluid_pp** out);
 
+/* Device bytes a handle for this configuration allocates (its arena and tables);
+ * host only.  The serving loop's admission by HBM budget reads it. */
+int fluid_pp_required_bytes(const fluid_pp_config* config, unsigned long long* bytes);
+
 /* Replaces WebGPUUniformPressureMultigrid.destroy() (webgpu-uniform-pressure-multigrid.ts:595-604). */
 void fluid_pp_destroy(fluid_pp* pp);
 
@@ -162,6 +166,12 @@ int fluid_pp_batch_create(fluid_pp* const* handles, int count, fluid_pp_batch** 
 void fluid_pp_batch_destroy(fluid_pp_batch* batch);
 int fluid_pp_batch_project(fluid_pp_batch* batch, const float* dts, const fluid_pp_solve_opts* opts,
                            fluid_pp_receipt* receipts);
+
+/* Solve a batch through CUDA graphs (on = 1, the default: the solve is captured
+ * once per option set and replayed) or with direct launches (on = 0: for a batch
+ * that lives for a few solves, e.g. a serving tick, capture would cost more
+ * than it saves).  Results are identical either way. */
+int fluid_pp_batch_set_graphs(fluid_pp_batch* batch, int on);
 
 /* Diagnostics (no reference counterpart; the reference times passes with
  * GPUPassTimestampRecorder, lib/core/performance-trace.ts:1183).
@@ -255,6 +265,8 @@ int fluid_pp_tall_get_labels(fluid_pp_tall* tall, int level, unsigned char* labe
 int fluid_pp_tall_apply_operator(fluid_pp_tall* tall, const float* p, float* out);
 int fluid_pp_tall_get_pressure(fluid_pp_tall* tall, float* p);
 const char* fluid_pp_tall_last_error(fluid_pp_tall* tall);
+/* Device bytes a tall handle for this layout allocates; host only. */
+int fluid_pp_tall_required_bytes(const fluid_pp_tall_config* config, const int* bases, unsigned long long* bytes);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,64 @@
+"""Continuous-batching server: results alone and in the mix, admission by budget (GPU)."""
+import numpy as np
+import pytest
+
+from fluid_b200 import configs
+from fluid_b200.serving import Request, Server, required_bytes, serving_requests
+
+pytestmark = pytest.mark.gpu
+
+
+def _uniform(nx, ny, nz, seed):
+    pair = []
+    for step in range(2):
+        vof = configs.random_liquid(nx, ny, nz, np.random.default_rng(seed))
+        u, v, w = configs.velocities(vof, np.random.default_rng(seed + 17 * step), 1 / 60, "gauss", 0.2)
+        pair.append(configs.GridState(nx, ny, nz, 1.0 / max(nx, ny, nz), 1 / 60, vof, u, v, w))
+    return pair
+
+
+def _tall(side, seed):
+    s0 = configs.tall_waves(side, side, 96, 24, seed=seed, mean=50, amp_max=4, lam=(8, 32))
+    s1 = configs.TallState(s0.nx, s0.nz, s0.fine_ny, s0.band, s0.bases, s0.h, s0.dt, s0.vof, -s0.u, -s0.v, -s0.w)
+    return [s0, s1]
+
+
+def _requests():
+    return [Request(0, "uniform", _uniform(40, 28, 36, 1), 4, 0.0),
+            Request(1, "tall", _tall(20, 2), 3, 0.0),
+            Request(2, "uniform", _uniform(24, 50, 30, 3), 5, 0.0),
+            Request(3, "uniform", _uniform(33, 33, 33, 4), 3, 0.0)]
+
+
+def test_each_result_is_the_same_alone_and_in_the_mix():
+    mix = Server(record=True)
+    stats = mix.run(_requests())
+    assert stats["requests_finished"] == 4 and stats["failed_steps"] == 0
+    got = {s.req.rid: s.pressures for s in mix.done}
+    for req in _requests():
+        alone = Server(record=True)
+        alone.run([req])
+        (sim,) = alone.done
+        assert len(sim.pressures) == req.steps == len(got[req.rid])
+        for a, b in zip(sim.pressures, got[req.rid]):
+            np.testing.assert_array_equal(a, b)
+
+
+def test_admission_respects_the_budget():
+    reqs = _requests()
+    need = [required_bytes(r, "fp16") for r in reqs]
+    budget = max(need) + min(need) // 2     # never two of the larger ones at once
+    srv = Server(budget_bytes=budget)
+    stats = srv.run(reqs)
+    assert stats["requests_finished"] == 4
+    assert srv.peak_used <= budget
+
+
+def test_poisson_stream_short():
+    reqs = serving_requests(rate=20.0, duration_s=1.5, seed=7, templates=2, steps=(3, 8), uniform_edge=(24, 64),
+                            tall_side=(16, 32), tall_band=(24, 32), tall_rows=96)
+    srv = Server(max_slots=16)
+    stats = srv.run(reqs)
+    assert stats["requests_finished"] == len(reqs)
+    assert stats["failed_steps"] == 0
+    assert stats["p99_step_ms"] is not None and stats["solves_per_s"] > 0
