@@ -397,6 +397,19 @@ def main():
         "precision": "f32 levels, f32 CG vectors, f64 dots/scalars/coarsest",
     }
 
+    # ------------------------- serving: Poisson stream with continuous batching
+    note("serving stream")
+    from fluid_b200.serving import Server, serving_requests
+    serve_s = 10.0
+    reqs = serving_requests(rate=40.0, duration_s=serve_s, seed=5, templates=6)
+    srv = Server(budget_bytes=150e9, max_slots=16, precision=args.precision, device=local)
+    serving = srv.run(reqs, duration_s=serve_s)
+    srv.shutdown()
+    serving.update({"workload": f"Poisson arrivals at 40/s for {serve_s:.0f} s (first {serve_s:.0f} s of the "
+                                "120 s stream): 50/50 uniform grids (edges log-uniform 32-160, one 1.2M-cell shape) "
+                                "and tall-cell grids (64^2-256^2 columns, 24-40 band), 30-300 steps each",
+                    "budget_bytes": 150e9, "slots": 16})
+
     # ------------------------------------------- e2e: public API from host buffers
     note("e2e from host buffers")
     pps = make(args.precision)
@@ -459,6 +472,7 @@ def main():
             "stage_ms_per_solve": {k: round(v["ms"] / steps2, 4) for k, v in sorted(prof.items())},
         },
         "tall_cell_256x256x1024": tall_line,
+        "serving": serving,
         "roofline": {"bound": "hbm", "kernel": dom, "workload": "dam_spheres_128x96x128 (one instance per launch)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": peak_kind, "traffic": traffic, "alg_bytes_per_launch": alg,
