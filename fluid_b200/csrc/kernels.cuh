@@ -489,8 +489,8 @@ __global__ void __launch_bounds__(kThreads) k_prolong(const InstDev* insts, cons
     const uint8_t* __restrict__ lab = F.label;
     int cx[2], cy[2];
     float wx[2], wy[2];
-    const int nxx = taps1d(it.x, C.sx, C.nx, cx, wx);
-    const int nyy = taps1d(it.y, C.sy, C.ny, cy, wy);
+    taps2(it.x, C.sx, C.nx, cx, wx);
+    taps2(it.y, C.sy, C.ny, cy, wy);
     const int sz = F.nx * F.ny;
     const int i0 = it.x + F.nx * (it.y + F.ny * it.z0);
 #pragma unroll
@@ -500,12 +500,15 @@ __global__ void __launch_bounds__(kThreads) k_prolong(const InstDev* insts, cons
       if (zz >= F.nz || !lab[i]) continue;
       int cz[2];
       float wz[2];
-      const int nzz = taps1d(zz, C.sz, C.nz, cz, wz);
+      taps2(zz, C.sz, C.nz, cz, wz);
       float s = 0.0f;
-      for (int c2 = 0; c2 < nzz; ++c2)
-        for (int c1 = 0; c1 < nyy; ++c1) {
+#pragma unroll
+      for (int c2 = 0; c2 < 2; ++c2)
+#pragma unroll
+        for (int c1 = 0; c1 < 2; ++c1) {
           const int row = C.nx * (cy[c1] + C.ny * cz[c2]);
-          for (int c0 = 0; c0 < nxx; ++c0) s += wx[c0] * wy[c1] * wz[c2] * tof(zc[row + cx[c0]]);
+#pragma unroll
+          for (int c0 = 0; c0 < 2; ++c0) s += wx[c0] * wy[c1] * wz[c2] * tof(zc[row + cx[c0]]);
         }
       zf[i] = fromf<TZF>(tof(zf[i]) + s * unscale);
     }
@@ -554,51 +557,89 @@ __global__ void __launch_bounds__(kBlockThreads) k_coarse_block(const InstDev* i
                                                                 int post) {
   extern __shared__ float smem[];
   __shared__ BlockLevel B[kMaxLevels];
+  __shared__ LevelDev sl[kMaxLevels];
   __shared__ int s_first, s_last, s_done;
-  const InstDev& I = insts[list[blockIdx.x]];
+  const InstDev* __restrict__ Ip = insts + list[blockIdx.x];
   if (threadIdx.x == 0) {
-    s_done = I.ctrl->done;
-    s_first = I.first_block;
-    s_last = I.nlev - 1;
-    char* p = reinterpret_cast<char*>(smem);
-    for (int l = s_first; l <= s_last; ++l) {
-      const LevelDev& L = I.lv[l];
-      BlockLevel& b = B[l];
-      b.nx = L.nx; b.ny = L.ny; b.nz = L.nz; b.n = int(L.n);
-      b.sx = L.sx; b.sy = L.sy; b.sz = L.sz;
-      b.wx = L.wx; b.wy = L.wy; b.wz = L.wz; b.to_coarse = L.to_coarse;
-      b.z = reinterpret_cast<float*>(p); p += 4 * b.n;
-      b.rhs = reinterpret_cast<float*>(p); p += 4 * b.n;
-      b.res = reinterpret_cast<float*>(p); p += 4 * b.n;
-      b.diag = reinterpret_cast<float*>(p); p += 4 * b.n;
-      b.inv = reinterpret_cast<float*>(p); p += 4 * b.n;
-      b.xyz = reinterpret_cast<unsigned*>(p); p += 4 * b.n;
-      b.ord = reinterpret_cast<unsigned short*>(p); p += 2 * ((b.n + 1) & ~1);
-      b.lab = reinterpret_cast<uint8_t*>(p); p += (b.n + 3) & ~3;
-      // red cells of a box: ceil(n / 2) when the corner cell is red
-      b.nred = (b.n + 1) / 2;
-    }
+    s_done = Ip->ctrl->done;
+    s_first = Ip->first_block;
+    s_last = Ip->nlev - 1;
   }
   __syncthreads();
   if (s_done) return;
   const int first = s_first, last = s_last;
-  for (int l = first; l <= last; ++l) {
-    const LevelDev& L = I.lv[l];
-    const BlockLevel& b = B[l];
-    const T* dg = static_cast<const T*>(L.diagT);
-    const T* rh = static_cast<const T*>(L.rhs);
-    for (int i = threadIdx.x; i < b.n; i += blockDim.x) {
-      int x, y, zz;
-      decode(i, b.nx, b.ny, x, y, zz);
-      const float d = tof(dg[i]);
-      const uint8_t lb = L.label[i];
-      b.diag[i] = d;
-      b.inv[i] = lb ? 1.0f / d : 0.0f;
-      b.lab[i] = lb;
-      b.xyz[i] = unsigned(x) | (unsigned(y) << 10) | (unsigned(zz) << 20);
-      const int red = red_before(x, y, zz, b.nx, b.ny);
-      b.ord[((x + y + zz) & 1) ? b.nred + (i - red) : red] = (unsigned short)i;
-      if (l == first) b.rhs[i] = tof(rh[i]);
+  // The block levels' descriptors, copied cooperatively into shared memory
+  // first: one round trip instead of one per field.
+  {
+    static_assert(sizeof(LevelDev) % 4 == 0, "LevelDev is copied as 32-bit words");
+    const int nw = (last - first + 1) * int(sizeof(LevelDev) / 4);
+    const unsigned* src = reinterpret_cast<const unsigned*>(&Ip->lv[first]);
+    unsigned* dst = reinterpret_cast<unsigned*>(&sl[first]);
+    for (int w = threadIdx.x; w < nw; w += blockDim.x) dst[w] = __ldg(src + w);
+  }
+  __syncthreads();
+  if (threadIdx.x <= last - first) {   // one thread per level lays out its arrays
+    const int l = first + int(threadIdx.x);
+    char* p = reinterpret_cast<char*>(smem);
+    for (int k = first; k < l; ++k) p += block_level_bytes(sl[k].n);
+    const LevelDev& L = sl[l];
+    BlockLevel& b = B[l];
+    b.nx = L.nx; b.ny = L.ny; b.nz = L.nz; b.n = int(L.n);
+    b.sx = L.sx; b.sy = L.sy; b.sz = L.sz;
+    b.wx = L.wx; b.wy = L.wy; b.wz = L.wz; b.to_coarse = L.to_coarse;
+    b.z = reinterpret_cast<float*>(p); p += 4 * b.n;
+    b.rhs = reinterpret_cast<float*>(p); p += 4 * b.n;
+    b.res = reinterpret_cast<float*>(p); p += 4 * b.n;
+    b.diag = reinterpret_cast<float*>(p); p += 4 * b.n;
+    b.inv = reinterpret_cast<float*>(p); p += 4 * b.n;
+    b.xyz = reinterpret_cast<unsigned*>(p); p += 4 * b.n;
+    b.ord = reinterpret_cast<unsigned short*>(p); p += 2 * ((b.n + 1) & ~1);
+    b.lab = reinterpret_cast<uint8_t*>(p);
+    // red cells of a box: ceil(n / 2) when the corner cell is red
+    b.nred = (b.n + 1) / 2;
+  }
+  __syncthreads();
+  // All block levels' cells in one flattened loop (cell e of the run
+  // first..last), every global load of a thread's cells issued before its first
+  // store, so the levels' round trips overlap.
+  {
+    int total = 0;
+    for (int l = first; l <= last; ++l) total += B[l].n;
+    constexpr int kU = 4;
+    for (int e0 = threadIdx.x; e0 < total; e0 += kU * blockDim.x) {
+      float d[kU], r[kU];
+      uint8_t lb[kU];
+      int lv[kU], ix[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        int e = e0 + u * int(blockDim.x), l = first;
+        while (l < last && e >= B[l].n) e -= B[l++].n;
+        lv[u] = l;
+        ix[u] = e;
+        d[u] = 1.0f;
+        r[u] = 0.0f;
+        lb[u] = 0;
+        if (e < B[l].n) {
+          d[u] = tof(static_cast<const T*>(sl[l].diagT)[e]);
+          lb[u] = sl[l].label[e];
+          if (l == first) r[u] = tof(static_cast<const T*>(sl[l].rhs)[e]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const BlockLevel& b = B[lv[u]];
+        const int i = ix[u];
+        if (i >= b.n) continue;
+        int x, y, zz;
+        decode(i, b.nx, b.ny, x, y, zz);
+        b.diag[i] = d[u];
+        b.inv[i] = lb[u] ? 1.0f / d[u] : 0.0f;
+        b.lab[i] = lb[u];
+        b.xyz[i] = unsigned(x) | (unsigned(y) << 10) | (unsigned(zz) << 20);
+        const int red = red_before(x, y, zz, b.nx, b.ny);
+        b.ord[((x + y + zz) & 1) ? b.nred + (i - red) : red] = (unsigned short)i;
+        if (lv[u] == first) b.rhs[i] = r[u];
+      }
     }
   }
   __syncthreads();
@@ -640,28 +681,48 @@ __global__ void __launch_bounds__(kBlockThreads) k_coarse_block(const InstDev* i
       F.res[i] = F.lab[i] ? F.rhs[i] - (F.diag[i] * F.z[i] - nbsum(F, F.z, i, F.xyz[i])) : 0.0f;
     __syncthreads();
     const BlockLevel& C = B[l + 1];
-    const float scale = F.to_coarse / float((C.sx == 2 ? 2 : 1) * (C.sy == 2 ? 2 : 1) * (C.sz == 2 ? 2 : 1));
-    for (int i = threadIdx.x; i < C.n; i += blockDim.x) {
-      float acc = 0.0f;
-      if (C.lab[i]) {
-        const unsigned cc = C.xyz[i];
-        const int X = int(cc & 1023u), Y = int((cc >> 10) & 1023u), Z = int(cc >> 20);
-        const int x0 = C.sx == 2 ? max(2 * X - 1, 0) : X, x1 = C.sx == 2 ? min(2 * X + 2, F.nx - 1) : X;
-        const int y0 = C.sy == 2 ? max(2 * Y - 1, 0) : Y, y1 = C.sy == 2 ? min(2 * Y + 2, F.ny - 1) : Y;
-        const int z0 = C.sz == 2 ? max(2 * Z - 1, 0) : Z, z1 = C.sz == 2 ? min(2 * Z + 2, F.nz - 1) : Z;
-        for (int fz = z0; fz <= z1; ++fz) {
-          const float wz = C.sz == 2 ? p1d(fz, Z, C.nz) : 1.0f;
-          for (int fy = y0; fy <= y1; ++fy) {
-            const float wyz = wz * (C.sy == 2 ? p1d(fy, Y, C.ny) : 1.0f);
-            const int row = F.nx * (fy + F.ny * fz);
-            float s = 0.0f;
-            for (int fx = x0; fx <= x1; ++fx) s += (C.sx == 2 ? p1d(fx, X, C.nx) : 1.0f) * F.res[row + fx];
-            acc += wyz * s;
-          }
+    {
+      // R = P^T / 2^k as a fixed 4 x 4 x 4 stencil: taps outside the level (or
+      // beyond a stride-1 axis' single tap) carry weight 0 at a clamped index.
+      const int fnx = F.nx, fny = F.ny, fnz = F.nz, cn = C.n, cnx = C.nx, cny = C.ny, cnz = C.nz;
+      const int csx = C.sx, csy = C.sy, csz = C.sz;
+      const float scale = F.to_coarse / float((csx == 2 ? 2 : 1) * (csy == 2 ? 2 : 1) * (csz == 2 ? 2 : 1));
+      const float* __restrict__ fres = F.res;
+      const unsigned* __restrict__ cxyz = C.xyz;
+      const uint8_t* __restrict__ clab = C.lab;
+      float* __restrict__ crhs = C.rhs;
+      auto taps4 = [](int c, int s2, int nc, int nf, int* f, float* w) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int fi = s2 == 2 ? 2 * c - 1 + k : c;
+          const bool ok = s2 == 2 ? (fi >= 0 && fi < nf) : k == 0;
+          f[k] = min(max(fi, 0), nf - 1);
+          w[k] = ok ? (s2 == 2 ? p1d(fi, c, nc) : 1.0f) : 0.0f;
         }
-        acc *= scale;
+      };
+      for (int i = threadIdx.x; i < cn; i += blockDim.x) {
+        float acc = 0.0f;
+        if (clab[i]) {
+          const unsigned cc = cxyz[i];
+          int fx[4], fy[4], fz[4];
+          float wx[4], wy[4], wz[4];
+          taps4(int(cc & 1023u), csx, cnx, fnx, fx, wx);
+          taps4(int((cc >> 10) & 1023u), csy, cny, fny, fy, wy);
+          taps4(int(cc >> 20), csz, cnz, fnz, fz, wz);
+#pragma unroll
+          for (int k2 = 0; k2 < 4; ++k2) {
+#pragma unroll
+            for (int k1 = 0; k1 < 4; ++k1) {
+              const int row = fnx * (fy[k1] + fny * fz[k2]);
+              const float s = ((wx[0] * fres[row + fx[0]] + wx[1] * fres[row + fx[1]]) +
+                               (wx[2] * fres[row + fx[2]] + wx[3] * fres[row + fx[3]]));
+              acc += (wz[k2] * wy[k1]) * s;
+            }
+          }
+          acc *= scale;
+        }
+        crhs[i] = acc;
       }
-      C.rhs[i] = acc;
     }
     __syncthreads();
   }
@@ -669,7 +730,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_coarse_block(const InstDev* i
   {
     const BlockLevel& b = B[last];
     const int m = b.n;
-    const double* inv = I.coarse_inv;
+    const double* __restrict__ inv = Ip->coarse_inv;
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
       double s = 0;
       const double* row = inv + (long long)i * m;
@@ -687,13 +748,16 @@ __global__ void __launch_bounds__(kBlockThreads) k_coarse_block(const InstDev* i
       const unsigned c = F.xyz[i];
       int cx[2], cy[2], cz[2];
       float wx[2], wy[2], wz[2];
-      const int nxx = taps1d(int(c & 1023u), C.sx, C.nx, cx, wx);
-      const int nyy = taps1d(int((c >> 10) & 1023u), C.sy, C.ny, cy, wy);
-      const int nzz = taps1d(int(c >> 20), C.sz, C.nz, cz, wz);
+      taps2(int(c & 1023u), C.sx, C.nx, cx, wx);
+      taps2(int((c >> 10) & 1023u), C.sy, C.ny, cy, wy);
+      taps2(int(c >> 20), C.sz, C.nz, cz, wz);
       float s = 0.0f;
-      for (int c2 = 0; c2 < nzz; ++c2)
-        for (int c1 = 0; c1 < nyy; ++c1)
-          for (int c0 = 0; c0 < nxx; ++c0) s += wx[c0] * wy[c1] * wz[c2] * C.z[cx[c0] + C.nx * (cy[c1] + C.ny * cz[c2])];
+#pragma unroll
+      for (int c2 = 0; c2 < 2; ++c2)
+#pragma unroll
+        for (int c1 = 0; c1 < 2; ++c1)
+#pragma unroll
+          for (int c0 = 0; c0 < 2; ++c0) s += wx[c0] * wy[c1] * wz[c2] * C.z[cx[c0] + C.nx * (cy[c1] + C.ny * cz[c2])];
       F.z[i] += s;
     }
     __syncthreads();
@@ -703,7 +767,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_coarse_block(const InstDev* i
     }
   }
   const BlockLevel& Bf = B[first];
-  T* zo = static_cast<T*>(I.lv[first].z);
+  T* zo = static_cast<T*>(sl[first].z);
   for (int i = threadIdx.x; i < Bf.n; i += blockDim.x) zo[i] = fromf<T>(Bf.z[i]);
 }
 
