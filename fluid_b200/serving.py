@@ -106,7 +106,7 @@ class Server:
     simulation per tick (continuous batching)."""
 
     def __init__(self, budget_bytes: float = 150e9, max_slots: int = 48, precision: str = "fp16", device: int = 0,
-                 rel_tol: float = 1e-6, record: bool = False):
+                 rel_tol: float = 1e-6, record: bool = False, admit_per_tick: int = 2):
         import torch
         self.torch = torch
         self.budget = float(budget_bytes)
@@ -116,7 +116,11 @@ class Server:
         self.rel_tol = float(rel_tol)
         self.record = record
         torch.cuda.set_device(self.device)
-        self.s_uniform = torch.cuda.Stream(device=self.device)
+        # uniform steps on a high-priority stream, tall-cell steps on low-priority ones
+        lo, hi = torch.cuda.Stream.priority_range()
+        self.prio_low, self.prio_high = lo, hi
+        self.s_uniform = torch.cuda.Stream(device=self.device, priority=hi)
+        self.admit_per_tick = int(admit_per_tick)
         self.pool = ThreadPoolExecutor(max_workers=self.max_slots)
         self.pending: list[tuple[Request, int]] = []
         self.active: list[_Sim] = []
@@ -133,7 +137,10 @@ class Server:
         self.pending.append((req, required_bytes(req, self.precision)))
 
     def _admit(self, now: float):
-        while self.pending and len(self.active) < self.max_slots:
+        """At most admit_per_tick creations per tick: a handle's creation and first
+        upload delay every resident simulation's next step."""
+        admitted = 0
+        while self.pending and len(self.active) < self.max_slots and admitted < self.admit_per_tick:
             req, need = self.pending[0]
             if self.used + need > self.budget:
                 if not self.active and need > self.budget:
@@ -141,13 +148,15 @@ class Server:
                 break
             self.pending.pop(0)
             # uniform simulations share the batch's stream; each tall one gets its own
-            stream = self.s_uniform if req.kind == "uniform" else self.torch.cuda.Stream(device=self.device)
+            stream = (self.s_uniform if req.kind == "uniform"
+                      else self.torch.cuda.Stream(device=self.device, priority=self.prio_low))
             sim = _Sim(req, self.precision, self.device, stream, self.torch)
             sim.bytes = need
             sim.ready = now
             self.used += need
             self.peak_used = max(self.peak_used, self.used)
             self.active.append(sim)
+            admitted += 1
 
     # -- one tick -------------------------------------------------------------------
     def _uniform_batch(self, sims):
