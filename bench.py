@@ -66,9 +66,10 @@ def stage_bytes_per_cell(stage: str, s: int) -> float:
     }.get(stage, 0.0)
 
 
-# DRAM bytes per launch of a stage's kernel on the 128x96x128 workload, from the
-# committed ncu captures (profiles/); absent until a capture of the current kernel exists.
-NCU_TRAFFIC_BYTES = {}
+# DRAM bytes (read + write) per launch of a stage's kernel on the 128x96x128
+# workload, fp16 levels, from the committed ncu capture
+# profiles/fused_kernels_dam_spheres_128x96x128_fp16.md (cold-cache launches).
+NCU_TRAFFIC_BYTES = {"up0": 17.77e6, "down0": 11.25e6, "dirspmv": 17.25e6, "update": 33.55e6}
 
 
 def peaks():

@@ -1,0 +1,58 @@
+"""A few projections of a named workload with direct kernel launches, for profilers.
+
+Kernels inside the solve's CUDA graphs (conditional WHILE nodes) are not visible
+to ncu, so this runs the same solves with one launch per kernel (the profiling
+mode of the library) and prints one line per solve:
+
+  python -m fluid_b200.profile_run --workload dam --solves 3
+  python -m fluid_b200.profile_run --workload tall --solves 1
+  python -m fluid_b200.profile_run --workload batch --solves 2
+
+dam   : 128x96x128 dam break + 16 spheres, fp16 levels (the bench's secondary uniform workload)
+tall  : 256^2 columns x 1024 rows, band 32 (the bench's tall-cell workload)
+batch : the bench's 64 uneven uniform grids in one batched solve
+"""
+from __future__ import annotations
+
+import argparse
+
+from . import BatchProjector, PressureProjector, configs
+from .tall import TallProjector
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", choices=["dam", "tall", "batch"], default="dam")
+    ap.add_argument("--solves", type=int, default=2)
+    ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16", "bf16"])
+    args = ap.parse_args()
+    if args.workload == "dam":
+        s = configs.dam_spheres()
+        pp = PressureProjector((s.nx, s.ny, s.nz), s.h, s.rho, precision=args.precision)
+        pp.set_profiling(True)
+        for _ in range(args.solves):
+            pp.upload_state(s.vof, s.u, s.v, s.w)
+            r = pp.project(s.dt, rel_tol=1e-6)
+            print(r["status_name"], r["iterations"], flush=True)
+    elif args.workload == "tall":
+        s = configs.tall_waves()
+        tp = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho)
+        for _ in range(args.solves):
+            tp.upload_state(s.vof, s.u, s.v, s.w)
+            r = tp.project(s.dt, rel_tol=1e-6)
+            print(r["status_name"], r["iterations"], flush=True)
+    else:
+        insts = configs.batch_instances()
+        pps = [PressureProjector((s.nx, s.ny, s.nz), s.h, s.rho, precision=args.precision) for s in insts]
+        B = BatchProjector(pps)
+        B.set_profiling(True)
+        for _ in range(args.solves):
+            for p, s in zip(pps, insts):
+                p.upload_state(s.vof, s.u, s.v, s.w)
+            recs = B.project([s.dt for s in insts], rel_tol=1e-6)
+            print(sum(r["status_name"] == "OK" for r in recs), max(r["iterations"] for r in recs), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
