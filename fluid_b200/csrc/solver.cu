@@ -27,6 +27,17 @@ using namespace fpp;
 namespace {
 
 constexpr int kMaxGrid = 148 * 8;   // 148 SMs x 8 resident 256-thread CTAs
+constexpr int kFillTiles = 2 * 148;  // fused-kernel tiles that give every SM two
+
+// Fused-kernel tile shapes, largest first: coarse cells per down-step tile and
+// fine cells per up-step tile (level 0's up step always uses the CG kernels'
+// 32 x 8 x 8 tiles, whose reduction partials it shares).
+constexpr int kDownShapes[5][3] = {{16, 4, 4}, {8, 4, 4}, {8, 4, 2}, {8, 2, 2}, {4, 2, 2}};
+constexpr int kUpShapes[5][3] = {{32, 8, 8}, {32, 8, 4}, {16, 8, 4}, {16, 4, 4}, {8, 4, 4}};
+
+int shape_tiles(int n0, int n1, int n2, const int* t) {
+  return ((n0 + t[0] - 1) / t[0]) * ((n1 + t[1] - 1) / t[1]) * ((n2 + t[2] - 1) / t[2]);
+}
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -516,6 +527,49 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
     B->maxL = std::max(B->maxL, h->plan.levels);
   }
   cudaSetDevice(B->device);
+  // The batch's own copies of the instance descriptors.  Fused-kernel tile
+  // shapes are chosen over the whole batch: the largest shape whose tiles,
+  // summed over every instance with that grid level, still give every SM two.
+  // (Results do not depend on the shape: halo cells repeat their owner's
+  // arithmetic.)
+  std::vector<InstDev> insts(count);
+  for (int k = 0; k < count; ++k) insts[k] = B->h[k]->inst;
+  for (int l = 0; l + 1 < B->maxL; ++l) {
+    auto grid = [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; };
+    for (int pick = 0; pick < 5; ++pick) {
+      long long total = 0;
+      for (const InstDev& I : insts)
+        if (grid(I)) total += shape_tiles(I.lv[l + 1].nx, I.lv[l + 1].ny, I.lv[l + 1].nz, kDownShapes[pick]);
+      if (total >= kFillTiles || pick == 4) {
+        for (InstDev& I : insts)
+          if (grid(I)) {
+            LevelDev& L = I.lv[l];
+            L.dcx = kDownShapes[pick][0];
+            L.dcy = kDownShapes[pick][1];
+            L.dcz = kDownShapes[pick][2];
+            L.dtiles = shape_tiles(I.lv[l + 1].nx, I.lv[l + 1].ny, I.lv[l + 1].nz, kDownShapes[pick]);
+          }
+        break;
+      }
+    }
+    if (l == 0) continue;   // level 0 keeps the 32 x 8 x 8 up tiles
+    for (int pick = 0; pick < 5; ++pick) {
+      long long total = 0;
+      for (const InstDev& I : insts)
+        if (grid(I)) total += shape_tiles(I.lv[l].nx, I.lv[l].ny, I.lv[l].nz, kUpShapes[pick]);
+      if (total >= kFillTiles || pick == 4) {
+        for (InstDev& I : insts)
+          if (grid(I)) {
+            LevelDev& L = I.lv[l];
+            L.utx = kUpShapes[pick][0];
+            L.uty = kUpShapes[pick][1];
+            L.utz = kUpShapes[pick][2];
+            L.utiles = shape_tiles(L.nx, L.ny, L.nz, kUpShapes[pick]);
+          }
+        break;
+      }
+    }
+  }
   // tile lists
   std::vector<Tile> tiles;
   std::vector<int> ilist;
@@ -541,13 +595,13 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
     auto grid_level = [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; };
     B->dn[l].off = int(tiles.size());
     for (int k = 0; k < count; ++k)
-      if (grid_level(B->h[k]->inst))
-        for (int t = 0; t < B->h[k]->inst.lv[l].dtiles; ++t) tiles.push_back(Tile{k, l, t, 0});
+      if (grid_level(insts[k]))
+        for (int t = 0; t < insts[k].lv[l].dtiles; ++t) tiles.push_back(Tile{k, l, t, 0});
     B->dn[l].n = int(tiles.size()) - B->dn[l].off;
     B->up[l].off = int(tiles.size());
     for (int k = 0; k < count; ++k)
-      if (grid_level(B->h[k]->inst))
-        for (int t = 0; t < B->h[k]->inst.lv[l].utiles; ++t) tiles.push_back(Tile{k, l, t, 0});
+      if (grid_level(insts[k]))
+        for (int t = 0; t < insts[k].lv[l].utiles; ++t) tiles.push_back(Tile{k, l, t, 0});
     B->up[l].n = int(tiles.size()) - B->up[l].off;
   }
   add_level(B->l0single, [](const InstDev& I) { return I.nlev == 1; }, 0);
@@ -569,7 +623,7 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
   int mmax = 0;
   for (int k = 0; k < count; ++k) {
     mmax = std::max(mmax, B->h[k]->inst.coarse_m);
-    const InstDev& I = B->h[k]->inst;
+    const InstDev& I = insts[k];
     if (I.nlev > 1) B->smem_block = std::max(B->smem_block, size_t(I.block_smem));
     for (int l = 0; l < I.first_block && l + 1 < I.nlev; ++l) {
       const LevelDev &L = I.lv[l], &C = I.lv[l + 1];
@@ -579,13 +633,9 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
   }
   B->smem_factor = size_t(mmax) * mmax * sizeof(double);
 
-  std::vector<InstDev> insts(count);
   cudaError_t e = cudaMalloc(&B->d_ctrl, sizeof(Ctrl) * count);
   if (e == cudaSuccess) e = cudaMemset(B->d_ctrl, 0, sizeof(Ctrl) * count);
-  for (int k = 0; k < count; ++k) {
-    insts[k] = B->h[k]->inst;
-    insts[k].ctrl = B->d_ctrl + k;
-  }
+  for (int k = 0; k < count; ++k) insts[k].ctrl = B->d_ctrl + k;
   if (e == cudaSuccess) e = cudaMalloc(&B->d_insts, sizeof(InstDev) * count);
   if (e == cudaSuccess) e = cudaMemcpy(B->d_insts, insts.data(), sizeof(InstDev) * count, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMalloc(&B->d_tiles, sizeof(Tile) * std::max<size_t>(1, tiles.size()));
@@ -887,30 +937,25 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
     L.res = a.take((l == 0 ? 4 : sT) * n);
   }
   I.lv[plan.levels - 1].to_coarse = 1.0f;
-  // Fused-kernel tile shapes per grid level: the largest shape that still gives
-  // every SM two tiles (level 0's up step keeps the 32 x 8 x 8 tiles of the CG
-  // kernels, whose reduction partials it shares).
+  // Fused-kernel tile shapes per grid level for a solve on its own: the largest
+  // shape that still gives every SM two tiles (a batch re-chooses them over all
+  // its instances, batch_build).
   for (int l = 0; l + 1 < plan.levels; ++l) {
     LevelDev& L = I.lv[l];
     const LevelDev& Cl = I.lv[l + 1];
-    auto count = [](int n0, int n1, int n2, const int* t) {
-      return ((n0 + t[0] - 1) / t[0]) * ((n1 + t[1] - 1) / t[1]) * ((n2 + t[2] - 1) / t[2]);
-    };
-    static const int dshape[5][3] = {{16, 4, 4}, {8, 4, 4}, {8, 4, 2}, {8, 2, 2}, {4, 2, 2}};
-    for (const auto& t : dshape) {
+    for (const auto& t : kDownShapes) {
       L.dcx = t[0];
       L.dcy = t[1];
       L.dcz = t[2];
-      L.dtiles = count(Cl.nx, Cl.ny, Cl.nz, t);
-      if (L.dtiles >= 2 * 148) break;
+      L.dtiles = shape_tiles(Cl.nx, Cl.ny, Cl.nz, t);
+      if (L.dtiles >= kFillTiles) break;
     }
-    static const int ushape[5][3] = {{kTX, kTY, kMaxDepth}, {32, 8, 4}, {16, 8, 4}, {16, 4, 4}, {8, 4, 4}};
-    for (const auto& t : ushape) {
+    for (const auto& t : kUpShapes) {
       L.utx = t[0];
       L.uty = t[1];
       L.utz = t[2];
-      L.utiles = count(L.nx, L.ny, L.nz, t);
-      if (l == 0 || L.utiles >= 2 * 148) break;
+      L.utiles = shape_tiles(L.nx, L.ny, L.nz, t);
+      if (l == 0 || L.utiles >= kFillTiles) break;
     }
   }
   // The single-CTA coarse block takes every level from the first one (>= 1) that
