@@ -629,19 +629,20 @@ __global__ void k_tall_true(TInst* I) {
 }
 
 // ------------------------------------------------------------------ V-cycle
-__global__ void k_tall_zero(TInst* I, int l) {
-  if (I->ctrl->done) return;
+// Each V-cycle stage is a device function over the samples t0, t0 + ts, ...;
+// the grid kernels call it with the grid's threads, the single-CTA block for
+// the small levels (k_tall_vblock) with the CTA's.
+__device__ __forceinline__ void tv_zero(TInst* I, int l, int t0, int ts) {
   const TLevel& L = I->lv[l];
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) L.z[k] = 0.0f;
+  for (int k = t0; k < L.n; k += ts) L.z[k] = 0.0f;
 }
 
 // One colour of the block Gauss-Seidel sweep: 0/1 band cells with (x + y + z)
 // even/odd, 2/3 tall blocks of columns with (x + z) even/odd.
-__global__ void k_tall_smooth(TInst* I, int l, int colour) {
-  if (I->ctrl->done) return;
+__device__ __forceinline__ void tv_smooth(TInst* I, int l, int colour, int t0, int ts) {
   const TLevel& L = I->lv[l];
   if (colour < 2) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+    for (int k = t0; k < L.n; k += ts) {
       int x, j, z, b;
       const bool act = sample_active(L, k, x, j, z, b);
       if (j < 2 || !act || ((x + b + j - 2 + z) & 1) != colour) continue;
@@ -652,7 +653,7 @@ __global__ void k_tall_smooth(TInst* I, int l, int colour) {
       L.z[k] = float((double(L.rhs[k]) - offdiag(L, k, j, x + L.nx * z, L.z)) / double(L.diag[k]));
     }
   } else {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < L.ncol; c += gridDim.x * blockDim.x) {
+    for (int c = t0; c < L.ncol; c += ts) {
       const int x = c % L.nx, z = c / L.nx;
       if (((x + z) & 1) != colour - 2) continue;
       const int s0 = sidx(L, x, 0, z), s1 = sidx(L, x, 1, z);
@@ -671,11 +672,10 @@ __global__ void k_tall_smooth(TInst* I, int l, int colour) {
 }
 
 // res = scale (rhs - A z); level 0 scales by sigma.
-__global__ void k_tall_residual(TInst* I, int l) {
-  if (I->ctrl->done) return;
+__device__ __forceinline__ void tv_residual(TInst* I, int l, int t0, int ts) {
   const TLevel& L = I->lv[l];
   const double scale = l == 0 ? I->ctrl->sigma : 1.0;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+  for (int k = t0; k < L.n; k += ts) {
     int x, j, z, b;
     sample_active(L, k, x, j, z, b);
     L.res[k] = L.label[k] ? float(scale * (double(L.rhs[k]) - apply_row(L, k, x, j, z, L.z))) : 0.0f;
@@ -708,11 +708,10 @@ __device__ __forceinline__ void fine_taps(const TLevel& C, int x, int y, int z, 
 }
 
 // acc_c += 1/2 P^T res_f in 32.32 fixed point (order-independent sums).
-__global__ void k_tall_restrict(TInst* I, int l) {
-  if (I->ctrl->done) return;
+__device__ __forceinline__ void tv_restrict(TInst* I, int l, int t0, int ts) {
   const TLevel& F = I->lv[l];
   const TLevel& C = I->lv[l + 1];
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < F.n; k += gridDim.x * blockDim.x) {
+  for (int k = t0; k < F.n; k += ts) {
     if (!F.label[k]) continue;
     const float r = F.res[k];
     if (r == 0.0f) continue;
@@ -730,10 +729,9 @@ __global__ void k_tall_restrict(TInst* I, int l) {
   }
 }
 
-__global__ void k_tall_restrict_finish(TInst* I, int l) {
-  if (I->ctrl->done) return;
+__device__ __forceinline__ void tv_restrict_finish(TInst* I, int l, int t0, int ts) {
   const TLevel& C = I->lv[l];
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C.n; k += gridDim.x * blockDim.x) {
+  for (int k = t0; k < C.n; k += ts) {
     const long long a = (long long)C.acc[k];
     C.rhs[k] = C.label[k] ? float(double(a) / kFix) : 0.0f;
     C.acc[k] = 0ull;
@@ -741,12 +739,11 @@ __global__ void k_tall_restrict_finish(TInst* I, int l) {
 }
 
 // z_f += P z_c on liquid fine samples; into level 0 the sigma scale is undone.
-__global__ void k_tall_prolong(TInst* I, int l) {
-  if (I->ctrl->done) return;
+__device__ __forceinline__ void tv_prolong(TInst* I, int l, int t0, int ts) {
   const TLevel& F = I->lv[l];
   const TLevel& C = I->lv[l + 1];
   const double unscale = l == 0 ? 1.0 / I->ctrl->sigma : 1.0;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < F.n; k += gridDim.x * blockDim.x) {
+  for (int k = t0; k < F.n; k += ts) {
     if (!F.label[k]) continue;
     int x, j, z, b;
     sample_active(F, k, x, j, z, b);
@@ -758,9 +755,8 @@ __global__ void k_tall_prolong(TInst* I, int l) {
   }
 }
 
-// z = A^{-1} rhs on the coarsest level (one CTA, a warp per row).
-__global__ void k_tall_coarse_apply(TInst* I) {
-  if (I->ctrl->done) return;
+// z = A^{-1} rhs on the coarsest level, a warp per row (threads t0 .. t0 + ts of one CTA).
+__device__ __forceinline__ void tv_coarse_apply(TInst* I) {
   const TLevel& L = I->lv[I->nlev - 1];
   const int m = L.n;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -769,6 +765,58 @@ __global__ void k_tall_coarse_apply(TInst* I) {
     for (int j = lane; j < m; j += 32) s += I->coarse_inv[(long long)i * m + j] * (L.label[j] ? double(L.rhs[j]) : 0.0);
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) L.z[i] = L.label[i] ? float(s) : 0.0f;
+  }
+}
+
+#define TALL_GRID_KERNEL(name, call)                                                        \
+  __global__ void name(TInst* I, int l, int arg) {                                           \
+    if (I->ctrl->done) return;                                                               \
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x, ts = gridDim.x * blockDim.x;      \
+    (void)arg;                                                                               \
+    call;                                                                                    \
+  }
+TALL_GRID_KERNEL(k_tall_zero, tv_zero(I, l, t0, ts))
+TALL_GRID_KERNEL(k_tall_smooth, tv_smooth(I, l, arg, t0, ts))
+TALL_GRID_KERNEL(k_tall_residual, tv_residual(I, l, t0, ts))
+TALL_GRID_KERNEL(k_tall_restrict, tv_restrict(I, l, t0, ts))
+TALL_GRID_KERNEL(k_tall_restrict_finish, tv_restrict_finish(I, l, t0, ts))
+TALL_GRID_KERNEL(k_tall_prolong, tv_prolong(I, l, t0, ts))
+#undef TALL_GRID_KERNEL
+
+__global__ void k_tall_coarse_apply(TInst* I) {
+  if (I->ctrl->done) return;
+  tv_coarse_apply(I);
+}
+
+// The small levels first .. nlev-1 of the V-cycle in one CTA: the same stages
+// as the grid kernels, separated by barriers instead of launches (global
+// memory written before a barrier is visible to the CTA after it).
+__global__ void __launch_bounds__(1024) k_tall_vblock(TInst* I, int first) {
+  if (I->ctrl->done) return;
+  const int t0 = threadIdx.x, ts = blockDim.x, last = I->nlev - 1;
+  for (int l = first; l < last; ++l) {
+    tv_zero(I, l, t0, ts);
+    __syncthreads();
+    for (int c = 0; c < 4; ++c) {
+      tv_smooth(I, l, c, t0, ts);
+      __syncthreads();
+    }
+    tv_residual(I, l, t0, ts);
+    __syncthreads();
+    tv_restrict(I, l, t0, ts);
+    __syncthreads();
+    tv_restrict_finish(I, l + 1, t0, ts);
+    __syncthreads();
+  }
+  tv_coarse_apply(I);
+  __syncthreads();
+  for (int l = last - 1; l >= first; --l) {
+    tv_prolong(I, l, t0, ts);
+    __syncthreads();
+    for (int c = 3; c >= 0; --c) {
+      tv_smooth(I, l, c, t0, ts);
+      __syncthreads();
+    }
   }
 }
 
@@ -877,25 +925,35 @@ int grid_for(long long n) { return int(std::max(1LL, std::min<long long>((n + kT
 
 size_t up256(size_t v) { return (v + 255) / 256 * 256; }
 
-void launch_vcycle(fluid_pp_tall* T) {
+// Levels below kTallBlockSamples run in the single-CTA block; the finer ones
+// launch one grid kernel per stage.
+constexpr long long kTallBlockSamples = 8192;
+
+int tall_first_block(const TallPlan& plan) {
+  const int L = int(plan.levels.size());
+  for (int l = 1; l < L; ++l)
+    if (plan.levels[l].samples() <= kTallBlockSamples) return l;
+  return L - 1;
+}
+
+void launch_vcycle(fluid_pp_tall* T, int first) {
   TInst& I = T->inst;
   cudaStream_t s = T->stream;
-  const int L = I.nlev;
-  for (int l = 0; l + 1 < L; ++l) {
+  for (int l = 0; l < first; ++l) {
     const int g = grid_for(I.lv[l].n), gc = grid_for(I.lv[l].ncol);
-    k_tall_zero<<<g, kTB, 0, s>>>(T->d_inst, l);
+    k_tall_zero<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
     k_tall_smooth<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
     k_tall_smooth<<<g, kTB, 0, s>>>(T->d_inst, l, 1);
     k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 2);
     k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 3);
-    k_tall_residual<<<g, kTB, 0, s>>>(T->d_inst, l);
-    k_tall_restrict<<<g, kTB, 0, s>>>(T->d_inst, l);
-    k_tall_restrict_finish<<<grid_for(I.lv[l + 1].n), kTB, 0, s>>>(T->d_inst, l + 1);
+    k_tall_residual<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
+    k_tall_restrict<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
+    k_tall_restrict_finish<<<grid_for(I.lv[l + 1].n), kTB, 0, s>>>(T->d_inst, l + 1, 0);
   }
-  k_tall_coarse_apply<<<1, 1024, 0, s>>>(T->d_inst);
-  for (int l = L - 2; l >= 0; --l) {
+  k_tall_vblock<<<1, 1024, 0, s>>>(T->d_inst, first);
+  for (int l = first - 1; l >= 0; --l) {
     const int g = grid_for(I.lv[l].n), gc = grid_for(I.lv[l].ncol);
-    k_tall_prolong<<<g, kTB, 0, s>>>(T->d_inst, l);
+    k_tall_prolong<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
     k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 3);
     k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 2);
     k_tall_smooth<<<g, kTB, 0, s>>>(T->d_inst, l, 1);
@@ -1150,7 +1208,7 @@ int fluid_pp_tall_project(fluid_pp_tall* T, float dt, const fluid_pp_solve_opts*
     const int burst = std::min(4, cap - it);
     for (int k = 0; k < burst; ++k) {
       if (I.nlev > 1) {
-        launch_vcycle(T);
+        launch_vcycle(T, tall_first_block(T->plan));
       } else {
         k_tall_coarse_apply<<<1, 1024, 0, s>>>(T->d_inst);
       }
