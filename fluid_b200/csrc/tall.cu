@@ -15,8 +15,10 @@
 // samples to a dense cell (a tall subcell interpolates its column's two
 // samples linearly, Eq. 5 of the paper; a band cell is its sample; rows above
 // the band are air).  A = T^T A_dense T is SPD by construction.  Band rows are
-// stored as ELL rows of at most kBandW entries, the two tall rows of a column
-// as a 2 x 2 diagonal block plus ELL rows of at most kTallW entries.
+// applied matrix-free (band_entries: the six face neighbours found through the
+// column bases, a tall neighbour interpolating its two samples) with a stored
+// diagonal; the two tall rows of a column are a 2 x 2 diagonal block plus ELL
+// rows of at most kTallW entries.
 //
 // Hierarchy: each coarser tall grid halves columns, rows and band, and its
 // bases cover the finer tall cells (tall_plan.cpp).  Coarse phi is the mean of
@@ -48,7 +50,6 @@ void set_global_error(const std::string& message);
 
 namespace tall {
 
-constexpr int kBandW = 10;        // off-diagonal slots of a band row
 constexpr int kTallW = 48;        // off-block slots of a tall row
 constexpr int kTB = 256;          // threads per CTA
 constexpr int kTGrid = 148 * 8;   // grid cap (grid-stride beyond)
@@ -58,13 +59,12 @@ struct TLevel {
   int nx, nz, fine_ny, band, P;
   int n;        // samples
   int ncol;     // columns
+  unsigned long long mnx, mP;   // magic64 of nx and P (sample index decode)
   int* bases;
   float* phi;
   uint8_t* label;
   float* diag;  // A[k][k]; air and inactive samples 1
   float* a01;   // per column A[j0][j1]
-  int* bidx;    // kBandW x n
-  float* bval;
   int* tidx;    // kTallW x 2 ncol, row 2 * column + (j == 1)
   float* tval;
   float* z;
@@ -95,6 +95,13 @@ struct TInst {
 };
 
 // ------------------------------------------------------------------ helpers
+// floor(n / d) for 32-bit n and d with m = magic64(d) = ceil(2^64 / d) (0 for
+// d = 1): m d - 2^64 < d, so n m / 2^64 stays below the next multiple of 2^64 / d.
+inline unsigned long long magic64(unsigned d) { return d <= 1 ? 0ull : ~0ull / d + 1ull; }
+__device__ __forceinline__ unsigned divq(unsigned n, unsigned long long m) {
+  return m == 0 ? n : unsigned(__umul64hi(n, m));
+}
+
 __device__ __forceinline__ int sidx(const TLevel& L, int x, int j, int z) { return x + L.nx * (j + L.P * z); }
 
 __device__ __forceinline__ int sample_row(int j, int b) { return j == 0 ? 0 : (j == 1 ? b - 1 : b + j - 2); }
@@ -154,10 +161,10 @@ __device__ __forceinline__ double dense_val(const TLevel& L, const float* a, int
 }
 
 __device__ __forceinline__ bool sample_active(const TLevel& L, int k, int& x, int& j, int& z, int& b) {
-  x = k % L.nx;
-  const int r = k / L.nx;
-  j = r % L.P;
-  z = r / L.P;
+  const unsigned r = divq(unsigned(k), L.mnx), zz = divq(r, L.mP);
+  x = k - int(r) * L.nx;
+  j = int(r - zz * unsigned(L.P));
+  z = int(zz);
   b = L.bases[x + L.nx * z];
   return j < 2 || b + j - 2 < L.fine_ny;
 }
@@ -218,14 +225,44 @@ __global__ void k_tall_coarse_labels(TInst* I, int l) {
   }
 }
 
-// Band rows: diagonal and up to kBandW neighbour entries from the six faces.
+// Off-diagonal entries of band row (x, j >= 2, z) of a column of base b: for
+// each liquid face neighbour, -w for every sample of its representation (a
+// tall neighbour row interpolates its column's two samples, weights 1 - t and
+// t).  Air and wall neighbours have none (their terms sit on the diagonal).
+template <class Fn>
+__device__ __forceinline__ void band_entries(const TLevel& L, int x, int j, int z, int b, Fn f) {
+  const int y = b + j - 2;
+  auto lateral = [&](int xn, int zn) {
+    if (xn < 0 || zn < 0 || xn >= L.nx || zn >= L.nz) return;
+    const int bn = L.bases[xn + L.nx * zn];
+    if (y < bn) {
+      const int s0 = sidx(L, xn, 0, zn);
+      if (!L.label[s0]) return;
+      const double t = double(y) / double(bn - 1);
+      if (t != 1.0) f(s0, -(1.0 - t));
+      if (t != 0.0) f(s0 + L.nx, -t);   // sample 1 of that column
+    } else if (y < bn + L.band) {
+      const int sn = sidx(L, xn, y - bn + 2, zn);
+      if (L.label[sn]) f(sn, -1.0);
+    }
+  };
+  lateral(x - 1, z);
+  lateral(x + 1, z);
+  lateral(x, z - 1);
+  lateral(x, z + 1);
+  const int k = sidx(L, x, j, z);
+  const int below = j == 2 ? sidx(L, x, 1, z) : k - L.nx;   // the tall cell's top subcell under the band
+  if (L.label[below]) f(below, -1.0);
+  if (j + 1 < L.P && y + 1 < L.fine_ny && L.label[k + L.nx]) f(k + L.nx, -1.0);
+}
+
+// Band rows: the diagonal (face weights, 1/theta on faces to air, none on walls).
 __global__ void k_tall_assemble_band(TInst* I, int l) {
   const TLevel& L = I->lv[l];
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
     int x, j, z, b;
     const bool act = sample_active(L, k, x, j, z, b);
     if (j < 2) continue;
-    int cnt = 0;
     double dg = 0.0;
     if (act && L.label[k]) {
       const int y = b + j - 2;
@@ -235,29 +272,11 @@ __global__ void k_tall_assemble_band(TInst* I, int l) {
         const int xn = nb[f][0], yn = nb[f][1], zn = nb[f][2];
         if (xn < 0 || yn < 0 || zn < 0 || xn >= L.nx || yn >= L.fine_ny || zn >= L.nz) continue;
         const Rep rn = rep_of(L, xn, yn, zn);
-        if (rn.liq) {
-          dg += 1.0;
-          if (rn.w0 != 0.0 && cnt < kBandW) {
-            L.bidx[cnt * L.n + k] = rn.s0;
-            L.bval[cnt * L.n + k] = float(-rn.w0);
-            ++cnt;
-          }
-          if (rn.n == 2 && rn.w1 != 0.0 && cnt < kBandW) {
-            L.bidx[cnt * L.n + k] = rn.s1;
-            L.bval[cnt * L.n + k] = float(-rn.w1);
-            ++cnt;
-          }
-        } else {
-          dg += 1.0 / ghost_theta_d(ph, rn.phi);
-        }
+        dg += rn.liq ? 1.0 : 1.0 / ghost_theta_d(ph, rn.phi);
       }
       L.diag[k] = float(dg);
     } else {
       L.diag[k] = 1.0f;
-    }
-    for (int s = cnt; s < kBandW; ++s) {
-      L.bidx[s * L.n + k] = k;
-      L.bval[s * L.n + k] = 0.0f;
     }
   }
 }
@@ -269,7 +288,7 @@ __global__ void k_tall_assemble_tall(TInst* I, int l) {
   const TLevel& L = I->lv[l];
   const int nrow = 2 * L.ncol;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < L.ncol; c += gridDim.x * blockDim.x) {
-    const int x = c % L.nx, z = c / L.nx;
+    const int z = int(divq(unsigned(c), L.mnx)), x = c - z * L.nx;
     const int b = L.bases[c];
     const int s0 = sidx(L, x, 0, z), s1 = sidx(L, x, 1, z);
     int n0 = 0, n1 = 0;
@@ -352,30 +371,34 @@ __global__ void k_tall_assemble_tall(TInst* I, int l) {
   }
 }
 
-// Off-diagonal part of row k of A applied to v (the 2 x 2 block excluded for
-// tall rows); returns it in float64.
-__device__ __forceinline__ double offdiag(const TLevel& L, int k, int j, int col, const float* v) {
+// Off-diagonal part of band row (x, j >= 2, z) of a column of base b applied
+// to v, in float64.
+__device__ __forceinline__ double band_off(const TLevel& L, int x, int j, int z, int b, const float* v) {
   double s = 0.0;
-  if (j >= 2) {
-#pragma unroll
-    for (int e = 0; e < kBandW; ++e) s += double(L.bval[e * L.n + k]) * double(v[L.bidx[e * L.n + k]]);
-  } else {
-    const int nrow = 2 * L.ncol, row = 2 * col + j;
-    for (int e = 0; e < kTallW; ++e) {
-      const float a = L.tval[e * nrow + row];
-      if (a == 0.0f) break;   // entries are packed from slot 0
-      s += double(a) * double(v[L.tidx[e * nrow + row]]);
-    }
+  band_entries(L, x, j, z, b, [&](int sn, double w) { s += double(float(w)) * double(v[sn]); });
+  return s;
+}
+
+// Off-block part of tall row j of column col applied to v (the 2 x 2 block
+// excluded; entries are packed from slot 0), in float64.
+__device__ __forceinline__ double tall_off(const TLevel& L, int col, int j, const float* v) {
+  const int nrow = 2 * L.ncol, row = 2 * col + j;
+  double s = 0.0;
+  for (int e = 0; e < kTallW; ++e) {
+    const float a = L.tval[e * nrow + row];
+    if (a == 0.0f) break;
+    s += double(a) * double(v[L.tidx[e * nrow + row]]);
   }
   return s;
 }
 
-// (A v)_k in float64 for a liquid sample.
-__device__ __forceinline__ double apply_row(const TLevel& L, int k, int x, int j, int z, const float* v) {
+// (A v)_k in float64 for a liquid sample (x, j, z) of a column of base b.
+__device__ __forceinline__ double apply_row(const TLevel& L, int k, int x, int j, int z, int b, const float* v) {
   const int col = x + L.nx * z;
-  double s = double(L.diag[k]) * double(v[k]) + offdiag(L, k, j, col, v);
-  if (j < 2) s += double(L.a01[col]) * double(v[sidx(L, x, 1 - j, z)]);
-  return s;
+  double s = double(L.diag[k]) * double(v[k]);
+  if (j >= 2) return s + band_off(L, x, j, z, b, v);
+  s += tall_off(L, col, j, v);
+  return s + double(L.a01[col]) * double(v[sidx(L, x, 1 - j, z)]);
 }
 
 // Dense inverse of the coarsest level (air and inactive samples identity rows).
@@ -396,7 +419,7 @@ __global__ void k_tall_factor(TInst* I) {
     const int col = x + L.nx * z;
     A[k * m + k] = L.diag[k];
     if (j >= 2) {
-      for (int e = 0; e < kBandW; ++e) A[k * m + L.bidx[e * L.n + k]] += L.bval[e * L.n + k];
+      band_entries(L, x, j, z, b, [&](int sn, double w) { A[k * m + sn] += float(w); });
     } else {
       const int nrow = 2 * L.ncol, row = 2 * col + j;
       A[k * m + sidx(L, x, 1 - j, z)] += L.a01[col];
@@ -561,7 +584,7 @@ __global__ void k_tall_spmv(TInst* I) {
     sample_active(L, k, x, j, z, b);
     float q = 0.0f;
     if (L.label[k]) {
-      q = float(apply_row(L, k, x, j, z, I->d));
+      q = float(apply_row(L, k, x, j, z, b, I->d));
       dq += double(I->d[k]) * double(q);
     }
     I->q[k] = q;
@@ -611,7 +634,7 @@ __global__ void k_tall_true(TInst* I) {
     auto X = [&](int s) { return double(I->x[s]) + double(I->xlo[s]); };
     double s = double(L.diag[k]) * X(k);
     if (j >= 2) {
-      for (int e = 0; e < kBandW; ++e) s += double(L.bval[e * L.n + k]) * X(L.bidx[e * L.n + k]);
+      band_entries(L, x, j, z, b, [&](int sn, double w) { s += double(float(w)) * X(sn); });
     } else {
       const int nrow = 2 * L.ncol, row = 2 * col + j;
       s += double(L.a01[col]) * X(sidx(L, x, 1 - j, z));
@@ -650,19 +673,19 @@ __device__ __forceinline__ void tv_smooth(TInst* I, int l, int colour, int t0, i
         L.z[k] = 0.0f;
         continue;
       }
-      L.z[k] = float((double(L.rhs[k]) - offdiag(L, k, j, x + L.nx * z, L.z)) / double(L.diag[k]));
+      L.z[k] = float((double(L.rhs[k]) - band_off(L, x, j, z, b, L.z)) / double(L.diag[k]));
     }
   } else {
     for (int c = t0; c < L.ncol; c += ts) {
-      const int x = c % L.nx, z = c / L.nx;
+      const int z = int(divq(unsigned(c), L.mnx)), x = c - z * L.nx;
       if (((x + z) & 1) != colour - 2) continue;
       const int s0 = sidx(L, x, 0, z), s1 = sidx(L, x, 1, z);
       if (!L.label[s0]) {
         L.z[s0] = L.z[s1] = 0.0f;
         continue;
       }
-      const double r0 = double(L.rhs[s0]) - offdiag(L, s0, 0, c, L.z);
-      const double r1 = double(L.rhs[s1]) - offdiag(L, s1, 1, c, L.z);
+      const double r0 = double(L.rhs[s0]) - tall_off(L, c, 0, L.z);
+      const double r1 = double(L.rhs[s1]) - tall_off(L, c, 1, L.z);
       const double a00 = L.diag[s0], a11 = L.diag[s1], a01 = L.a01[c];
       const double det = a00 * a11 - a01 * a01;
       L.z[s0] = float((a11 * r0 - a01 * r1) / det);
@@ -678,36 +701,15 @@ __device__ __forceinline__ void tv_residual(TInst* I, int l, int t0, int ts) {
   for (int k = t0; k < L.n; k += ts) {
     int x, j, z, b;
     sample_active(L, k, x, j, z, b);
-    L.res[k] = L.label[k] ? float(scale * (double(L.rhs[k]) - apply_row(L, k, x, j, z, L.z))) : 0.0f;
+    L.res[k] = L.label[k] ? float(scale * (double(L.rhs[k]) - apply_row(L, k, x, j, z, b, L.z))) : 0.0f;
   }
 }
 
-// Coarse dense cells feeding fine sample (x, row y, z) with their weights.
-struct Taps {
-  int n;
-  int x[8], y[8], z[8];
-  double w[8];
-};
-
-__device__ __forceinline__ void fine_taps(const TLevel& C, int x, int y, int z, Taps& T) {
-  int cx[2], cy[2], cz[2];
-  float wx[2], wy[2], wz[2];
-  const int nxx = taps1d(x, 2, C.nx, cx, wx);
-  const int nyy = taps1d(y, 2, C.fine_ny, cy, wy);
-  const int nzz = taps1d(z, 2, C.nz, cz, wz);
-  T.n = 0;
-  for (int c2 = 0; c2 < nzz; ++c2)
-    for (int c1 = 0; c1 < nyy; ++c1)
-      for (int c0 = 0; c0 < nxx; ++c0) {
-        T.x[T.n] = cx[c0];
-        T.y[T.n] = cy[c1];
-        T.z[T.n] = cz[c2];
-        T.w[T.n] = double(wx[c0]) * double(wy[c1]) * double(wz[c2]);
-        ++T.n;
-      }
-}
-
-// acc_c += 1/2 P^T res_f in 32.32 fixed point (order-independent sums).
+// acc_c += 1/2 P^T res_f in 32.32 fixed point (order-independent sums).  The
+// fine sample at dense (x, row y, z) takes the 2 x 2 x 2 trilinear taps of the
+// coarse dense cells around it (taps2: a dropped tap has weight 0); a coarse
+// tall cell passes its share to the column's two samples (1 - t, t), a coarse
+// band cell to its sample, air cells take nothing.
 __device__ __forceinline__ void tv_restrict(TInst* I, int l, int t0, int ts) {
   const TLevel& F = I->lv[l];
   const TLevel& C = I->lv[l + 1];
@@ -717,15 +719,39 @@ __device__ __forceinline__ void tv_restrict(TInst* I, int l, int t0, int ts) {
     if (r == 0.0f) continue;
     int x, j, z, b;
     sample_active(F, k, x, j, z, b);
-    Taps T;
-    fine_taps(C, x, sample_row(j, b), z, T);
-    for (int t = 0; t < T.n; ++t) {
-      const Rep rc = rep_of(C, T.x[t], T.y[t], T.z[t]);
-      if (!rc.liq) continue;
-      const double v = 0.5 * T.w[t] * double(r);
-      atomicAdd(&C.acc[rc.s0], (unsigned long long)llrint(v * rc.w0 * kFix));
-      if (rc.n == 2) atomicAdd(&C.acc[rc.s1], (unsigned long long)llrint(v * rc.w1 * kFix));
-    }
+    int cx[2], cy[2], cz[2];
+    float wx[2], wy[2], wz[2];
+    taps2(x, 2, C.nx, cx, wx);
+    taps2(sample_row(j, b), 2, C.fine_ny, cy, wy);
+    taps2(z, 2, C.nz, cz, wz);
+    const double hr = 0.5 * double(r);
+#pragma unroll
+    for (int c2 = 0; c2 < 2; ++c2)
+#pragma unroll
+      for (int c0 = 0; c0 < 2; ++c0) {
+        const double wxz = double(wx[c0]) * double(wz[c2]);
+        if (wxz == 0.0) continue;
+        const int bc = C.bases[cx[c0] + C.nx * cz[c2]];
+        const int s0 = sidx(C, cx[c0], 0, cz[c2]);
+        long long t0acc = 0, t1acc = 0;   // the column's tall samples, summed over the y taps
+#pragma unroll
+        for (int c1 = 0; c1 < 2; ++c1) {
+          if (wy[c1] == 0.0f) continue;
+          const int Y = cy[c1];
+          const double v = hr * (wxz * double(wy[c1]));
+          if (Y < bc) {
+            if (!C.label[s0]) continue;
+            const double t = double(Y) / double(bc - 1);
+            t0acc += llrint(v * (1.0 - t) * kFix);
+            t1acc += llrint(v * t * kFix);
+          } else if (Y < bc + C.band) {
+            const int sn = s0 + C.nx * (Y - bc + 2);
+            if (C.label[sn]) atomicAdd(&C.acc[sn], (unsigned long long)llrint(v * kFix));
+          }
+        }
+        if (t0acc != 0) atomicAdd(&C.acc[s0], (unsigned long long)t0acc);
+        if (t1acc != 0) atomicAdd(&C.acc[s0 + C.nx], (unsigned long long)t1acc);
+      }
   }
 }
 
@@ -738,7 +764,9 @@ __device__ __forceinline__ void tv_restrict_finish(TInst* I, int l, int t0, int 
   }
 }
 
-// z_f += P z_c on liquid fine samples; into level 0 the sigma scale is undone.
+// z_f += P z_c on liquid fine samples (the taps of tv_restrict, a coarse tall
+// cell interpolating its column's two samples); into level 0 the sigma scale
+// is undone.
 __device__ __forceinline__ void tv_prolong(TInst* I, int l, int t0, int ts) {
   const TLevel& F = I->lv[l];
   const TLevel& C = I->lv[l + 1];
@@ -747,10 +775,36 @@ __device__ __forceinline__ void tv_prolong(TInst* I, int l, int t0, int ts) {
     if (!F.label[k]) continue;
     int x, j, z, b;
     sample_active(F, k, x, j, z, b);
-    Taps T;
-    fine_taps(C, x, sample_row(j, b), z, T);
+    int cx[2], cy[2], cz[2];
+    float wx[2], wy[2], wz[2];
+    taps2(x, 2, C.nx, cx, wx);
+    taps2(sample_row(j, b), 2, C.fine_ny, cy, wy);
+    taps2(z, 2, C.nz, cz, wz);
+    int bc[2][2];
+#pragma unroll
+    for (int c2 = 0; c2 < 2; ++c2)
+#pragma unroll
+      for (int c0 = 0; c0 < 2; ++c0) bc[c2][c0] = C.bases[cx[c0] + C.nx * cz[c2]];
     double s = 0.0;
-    for (int t = 0; t < T.n; ++t) s += T.w[t] * dense_val(C, C.z, T.x[t], T.y[t], T.z[t]);
+#pragma unroll
+    for (int c2 = 0; c2 < 2; ++c2)
+#pragma unroll
+      for (int c1 = 0; c1 < 2; ++c1)
+#pragma unroll
+        for (int c0 = 0; c0 < 2; ++c0) {
+          const double w = double(wx[c0]) * double(wy[c1]) * double(wz[c2]);
+          if (w == 0.0) continue;
+          const int B = bc[c2][c0], Y = cy[c1];
+          const int s0 = sidx(C, cx[c0], 0, cz[c2]);
+          double val = 0.0;
+          if (Y < B) {
+            const double t = double(Y) / double(B - 1);
+            val = (1.0 - t) * double(C.z[s0]) + t * double(C.z[s0 + C.nx]);
+          } else if (Y < B + C.band) {
+            val = double(C.z[s0 + C.nx * (Y - B + 2)]);
+          }
+          s += w * val;
+        }
     F.z[k] = float(double(F.z[k]) + s * unscale);
   }
 }
@@ -990,7 +1044,6 @@ size_t tall_arena_size(const TallPlan& plan) {
     const size_t n = size_t(P.samples()), nc = size_t(P.nx) * P.nz;
     acc(4 * nc);                                   // bases
     acc(4 * n); acc(n); acc(4 * n); acc(4 * nc);   // phi label diag a01
-    acc(4 * kBandW * n); acc(4 * kBandW * n);      // bidx bval
     acc(4 * kTallW * 2 * nc); acc(4 * kTallW * 2 * nc);
     acc(4 * n); acc(4 * n); acc(4 * n);            // z rhs res
     if (l > 0) acc(8 * n);                         // acc
@@ -1053,6 +1106,8 @@ int tall_create(const fluid_pp_tall_config* cfg, const int* bases, fluid_pp_tall
     V.P = P.P();
     V.n = int(P.samples());
     V.ncol = P.nx * P.nz;
+    V.mnx = magic64(unsigned(V.nx));
+    V.mP = magic64(unsigned(V.P));
     const size_t n = size_t(V.n), nc = size_t(V.ncol);
     V.bases = static_cast<int*>(take(4 * nc));
     cudaMemcpy(V.bases, P.bases.data(), 4 * nc, cudaMemcpyHostToDevice);
@@ -1060,8 +1115,6 @@ int tall_create(const fluid_pp_tall_config* cfg, const int* bases, fluid_pp_tall
     V.label = static_cast<uint8_t*>(take(n));
     V.diag = static_cast<float*>(take(4 * n));
     V.a01 = static_cast<float*>(take(4 * nc));
-    V.bidx = static_cast<int*>(take(4 * kBandW * n));
-    V.bval = static_cast<float*>(take(4 * kBandW * n));
     V.tidx = static_cast<int*>(take(4 * kTallW * 2 * nc));
     V.tval = static_cast<float*>(take(4 * kTallW * 2 * nc));
     V.z = static_cast<float*>(take(4 * n));
