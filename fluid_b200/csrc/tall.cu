@@ -283,88 +283,129 @@ __global__ void k_tall_assemble_band(TInst* I, int l) {
 
 // The two tall rows of a column: 2 x 2 block (internal faces, the face to the
 // first band row, lateral faces summed over the tall rows) and the couplings
-// to the neighbour columns' samples.
+// to the neighbour columns' samples.  One warp per column: the lanes split the
+// column's rows, band couplings take ELL slots in row order by ballot prefix
+// counts, the lateral sums are reduced over the warp.
 __global__ void k_tall_assemble_tall(TInst* I, int l) {
   const TLevel& L = I->lv[l];
   const int nrow = 2 * L.ncol;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < L.ncol; c += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  const unsigned below = (1u << lane) - 1u;
+  auto wsum = [](double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+  };
+  for (int c = blockIdx.x * wpb + (threadIdx.x >> 5); c < L.ncol; c += gridDim.x * wpb) {
     const int z = int(divq(unsigned(c), L.mnx)), x = c - z * L.nx;
     const int b = L.bases[c];
     const int s0 = sidx(L, x, 0, z), s1 = sidx(L, x, 1, z);
-    int n0 = 0, n1 = 0;
-    auto add = [&](int row, int& cnt, int s, double v) {
+    int n0 = 0, n1 = 0;   // warp-uniform slot counts
+    // One entry, called by the whole warp with uniform arguments.
+    auto put = [&](int row, int& cnt, int s, double v) {
       if (v == 0.0) return;
       if (cnt >= kTallW) {
-        atomicExch(I->err, 1);
+        if (lane == 0) atomicExch(I->err, 1);
         return;
       }
-      L.tidx[cnt * nrow + row] = s;
-      L.tval[cnt * nrow + row] = float(v);
+      if (lane == 0) {
+        L.tidx[cnt * nrow + row] = s;
+        L.tval[cnt * nrow + row] = float(v);
+      }
       ++cnt;
+    };
+    // One entry per lane with p set, in lane order.
+    auto put_lanes = [&](int row, int& cnt, bool p, int s, double v) {
+      const unsigned m = __ballot_sync(0xffffffffu, p);
+      const int slot = cnt + __popc(m & below);
+      if (p) {
+        if (slot < kTallW) {
+          L.tidx[slot * nrow + row] = s;
+          L.tval[slot * nrow + row] = float(v);
+        } else {
+          atomicExch(I->err, 1);
+        }
+      }
+      cnt = min(kTallW, cnt + __popc(m));
     };
     if (L.label[s0]) {
       const float ph = L.phi[s0];
-      double a00 = 0.0, a01 = 0.0, a11 = 0.0;
       const double kin = 1.0 / double(b - 1);   // b - 1 internal faces of slope 1 / (b - 1)
-      a00 += kin;
-      a11 += kin;
-      a01 -= kin;
+      double a00 = kin, a01 = -kin, a11 = kin;
       {
         const int s2 = sidx(L, x, 2, z);
         if (L.label[s2]) {
           a11 += 1.0;
-          add(2 * c + 1, n1, s2, -1.0);
+          put(2 * c + 1, n1, s2, -1.0);
         } else {
           a11 += 1.0 / ghost_theta_d(ph, L.phi[s2]);
         }
       }
+      double p00 = 0.0, p01 = 0.0, p11 = 0.0;   // this lane's share of the lateral faces
       const int dirs[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
       for (int d = 0; d < 4; ++d) {
         const int xn = x + dirs[d][0], zn = z + dirs[d][1];
         if (xn < 0 || zn < 0 || xn >= L.nx || zn >= L.nz) continue;
         double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
-        for (int y = 0; y < b; ++y) {
-          const double t = double(y) / double(b - 1);
-          const Rep rn = rep_of(L, xn, y, zn);
-          if (rn.liq) {
-            a00 += (1.0 - t) * (1.0 - t);
-            a01 += (1.0 - t) * t;
-            a11 += t * t;
-            if (rn.n == 2) {
-              c00 += (1.0 - t) * rn.w0;
-              c01 += (1.0 - t) * rn.w1;
-              c10 += t * rn.w0;
-              c11 += t * rn.w1;
+        for (int y0 = 0; y0 < b; y0 += 32) {
+          const int y = y0 + lane;
+          bool p0 = false, p1 = false;
+          int sb = 0;
+          double t = 0.0;
+          if (y < b) {
+            t = double(y) / double(b - 1);
+            const Rep rn = rep_of(L, xn, y, zn);
+            if (rn.liq) {
+              p00 += (1.0 - t) * (1.0 - t);
+              p01 += (1.0 - t) * t;
+              p11 += t * t;
+              if (rn.n == 2) {
+                c00 += (1.0 - t) * rn.w0;
+                c01 += (1.0 - t) * rn.w1;
+                c10 += t * rn.w0;
+                c11 += t * rn.w1;
+              } else {
+                sb = rn.s0;
+                p0 = (1.0 - t) != 0.0;
+                p1 = t != 0.0;
+              }
             } else {
-              add(2 * c, n0, rn.s0, -(1.0 - t));
-              add(2 * c + 1, n1, rn.s0, -t);
+              const double inv = 1.0 / ghost_theta_d(ph, rn.phi);
+              p00 += (1.0 - t) * (1.0 - t) * inv;
+              p01 += (1.0 - t) * t * inv;
+              p11 += t * t * inv;
             }
-          } else {
-            const double inv = 1.0 / ghost_theta_d(ph, rn.phi);
-            a00 += (1.0 - t) * (1.0 - t) * inv;
-            a01 += (1.0 - t) * t * inv;
-            a11 += t * t * inv;
           }
+          put_lanes(2 * c, n0, p0, sb, -(1.0 - t));
+          put_lanes(2 * c + 1, n1, p1, sb, -t);
         }
+        c00 = wsum(c00);
+        c01 = wsum(c01);
+        c10 = wsum(c10);
+        c11 = wsum(c11);
         const int m0 = sidx(L, xn, 0, zn), m1 = sidx(L, xn, 1, zn);
-        add(2 * c, n0, m0, -c00);
-        add(2 * c, n0, m1, -c01);
-        add(2 * c + 1, n1, m0, -c10);
-        add(2 * c + 1, n1, m1, -c11);
+        put(2 * c, n0, m0, -c00);
+        put(2 * c, n0, m1, -c01);
+        put(2 * c + 1, n1, m0, -c10);
+        put(2 * c + 1, n1, m1, -c11);
       }
-      L.diag[s0] = float(a00);
-      L.diag[s1] = float(a11);
-      L.a01[c] = float(a01);
-    } else {
+      a00 += wsum(p00);
+      a01 += wsum(p01);
+      a11 += wsum(p11);
+      if (lane == 0) {
+        L.diag[s0] = float(a00);
+        L.diag[s1] = float(a11);
+        L.a01[c] = float(a01);
+      }
+    } else if (lane == 0) {
       L.diag[s0] = 1.0f;
       L.diag[s1] = 1.0f;
       L.a01[c] = 0.0f;
     }
-    for (int s = n0; s < kTallW; ++s) {
+    for (int s = n0 + lane; s < kTallW; s += 32) {
       L.tidx[s * nrow + 2 * c] = s0;
       L.tval[s * nrow + 2 * c] = 0.0f;
     }
-    for (int s = n1; s < kTallW; ++s) {
+    for (int s = n1 + lane; s < kTallW; s += 32) {
       L.tidx[s * nrow + 2 * c + 1] = s1;
       L.tval[s * nrow + 2 * c + 1] = 0.0f;
     }
@@ -380,16 +421,58 @@ __device__ __forceinline__ double band_off(const TLevel& L, int x, int j, int z,
 }
 
 // Off-block part of tall row j of column col applied to v (the 2 x 2 block
-// excluded; entries are packed from slot 0), in float64.
+// excluded), in float64.  Entries are packed from slot 0 and padded with
+// weight 0 on a valid index, so each chunk of 8 slots is loaded at once and a
+// chunk ending in padding is the last.
 __device__ __forceinline__ double tall_off(const TLevel& L, int col, int j, const float* v) {
   const int nrow = 2 * L.ncol, row = 2 * col + j;
   double s = 0.0;
-  for (int e = 0; e < kTallW; ++e) {
-    const float a = L.tval[e * nrow + row];
-    if (a == 0.0f) break;
-    s += double(a) * double(v[L.tidx[e * nrow + row]]);
+  for (int e0 = 0; e0 < kTallW; e0 += 8) {
+    float a[8], vv[8];
+    int id[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      a[e] = L.tval[(e0 + e) * nrow + row];
+      id[e] = L.tidx[(e0 + e) * nrow + row];
+    }
+#pragma unroll
+    for (int e = 0; e < 8; ++e) vv[e] = v[id[e]];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) s += double(a[e]) * double(vv[e]);
+    if (a[7] == 0.0f) break;
   }
   return s;
+}
+
+// tall_off for both tall rows of column col (rows 2 col and 2 col + 1 are
+// adjacent in every slot: one 8-byte load per slot for the pair).
+__device__ __forceinline__ void tall_off_pair(const TLevel& L, int col, const float* v, double& o0, double& o1) {
+  const float2* tv = reinterpret_cast<const float2*>(L.tval);
+  const int2* ti = reinterpret_cast<const int2*>(L.tidx);
+  double s0 = 0.0, s1 = 0.0;
+  for (int e0 = 0; e0 < kTallW; e0 += 8) {
+    float2 a[8];
+    int2 id[8];
+    float v0[8], v1[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      a[e] = tv[(e0 + e) * L.ncol + col];
+      id[e] = ti[(e0 + e) * L.ncol + col];
+    }
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      v0[e] = v[id[e].x];
+      v1[e] = v[id[e].y];
+    }
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      s0 += double(a[e].x) * double(v0[e]);
+      s1 += double(a[e].y) * double(v1[e]);
+    }
+    if (a[7].x == 0.0f && a[7].y == 0.0f) break;
+  }
+  o0 = s0;
+  o1 = s1;
 }
 
 // (A v)_k in float64 for a liquid sample (x, j, z) of a column of base b.
@@ -684,8 +767,10 @@ __device__ __forceinline__ void tv_smooth(TInst* I, int l, int colour, int t0, i
         L.z[s0] = L.z[s1] = 0.0f;
         continue;
       }
-      const double r0 = double(L.rhs[s0]) - tall_off(L, c, 0, L.z);
-      const double r1 = double(L.rhs[s1]) - tall_off(L, c, 1, L.z);
+      double o0, o1;
+      tall_off_pair(L, c, L.z, o0, o1);
+      const double r0 = double(L.rhs[s0]) - o0;
+      const double r1 = double(L.rhs[s1]) - o1;
       const double a00 = L.diag[s0], a11 = L.diag[s1], a01 = L.a01[c];
       const double det = a00 * a11 - a01 * a01;
       L.z[s0] = float((a11 * r0 - a01 * r1) / det);
@@ -1026,7 +1111,7 @@ void launch_setup(fluid_pp_tall* T) {
   }
   for (int l = 0; l < I.nlev; ++l) {
     k_tall_assemble_band<<<grid_for(I.lv[l].n), kTB, 0, s>>>(T->d_inst, l);
-    k_tall_assemble_tall<<<grid_for(I.lv[l].ncol), kTB, 0, s>>>(T->d_inst, l);
+    k_tall_assemble_tall<<<grid_for(32LL * I.lv[l].ncol), kTB, 0, s>>>(T->d_inst, l);
   }
   const size_t m = size_t(I.coarse_m);
   k_tall_factor<<<1, 1024, m * m * sizeof(double), s>>>(T->d_inst);
