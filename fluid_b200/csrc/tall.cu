@@ -59,7 +59,7 @@ struct TLevel {
   int nx, nz, fine_ny, band, P;
   int n;        // samples
   int ncol;     // columns
-  unsigned long long mnx, mP;   // magic64 of nx and P (sample index decode)
+  unsigned long long mnx, mP, mnc;   // magic64 of nx, P and ncol (index decode)
   int* bases;
   float* phi;
   uint8_t* label;
@@ -743,21 +743,117 @@ __device__ __forceinline__ void tv_zero(TInst* I, int l, int t0, int ts) {
   for (int k = t0; k < L.n; k += ts) L.z[k] = 0.0f;
 }
 
+// Band colour sweeps run over work items of G consecutive band rows of one
+// column (item = column + ncol * group, so a warp's lanes are adjacent
+// columns): an item loads its column's base and the four lateral bases once,
+// then issues every load of its G / 2 rows of the colour before the first
+// update.  Rows of one colour never neighbour each other, so the loads see no
+// update of the same sweep.  Grid launches take kBandGroup rows per item, the
+// single-CTA block (64 registers a thread) kBlockBandGroup.
+constexpr int kBandGroup = 8;
+constexpr int kBlockBandGroup = 2;
+
+// Off-diagonal taps of band row y of a column on lateral neighbour column
+// (xn, zn) of base bn (bn < 0: outside the grid), as in band_entries without
+// the label test: a tall neighbour row interpolates samples (ia, ib), a band
+// one is sample ia, air and walls give index self with no weight.  Callers
+// apply them to vectors that are 0 on every sample that is not liquid.
+__device__ __forceinline__ void lateral_idx(const TLevel& L, int xn, int zn, int bn, int y, int self, int& ia, int& ib) {
+  ia = ib = self;
+  if (bn < 0) return;
+  if (y < bn) {
+    ia = sidx(L, xn, 0, zn);
+    ib = ia + L.nx;
+  } else if (y < bn + L.band) {
+    ia = sidx(L, xn, y - bn + 2, zn);
+  }
+}
+__device__ __forceinline__ void lateral_w(const TLevel& L, int bn, int y, double& wa, double& wb) {
+  wa = wb = 0.0;
+  if (bn < 0) return;
+  if (y < bn) {
+    const double t = double(y) / double(bn - 1);
+    wa = double(float(-(1.0 - t)));
+    wb = double(float(-t));
+  } else if (y < bn + L.band) {
+    wa = -1.0;
+  }
+}
+
+template <int G>
+__device__ __forceinline__ void tv_smooth_band(TInst* I, int l, int colour, int t0, int ts) {
+  static_assert(G % 2 == 0, "a band row group holds both colours");
+  const TLevel& L = I->lv[l];
+  constexpr int R = G / 2;
+  const int items = ((L.band + G - 1) / G) * L.ncol;
+  for (int it = t0; it < items; it += ts) {
+    const int g = int(divq(unsigned(it), L.mnc));
+    const int col = it - g * L.ncol;
+    const int z = int(divq(unsigned(col), L.mnx)), x = col - z * L.nx;
+    const int b = L.bases[col];
+    const int xn[4] = {x - 1, x + 1, x, x}, zn[4] = {z, z, z - 1, z + 1};
+    int bn[4];
+    bn[0] = x > 0 ? L.bases[col - 1] : -1;
+    bn[1] = x + 1 < L.nx ? L.bases[col + 1] : -1;
+    bn[2] = z > 0 ? L.bases[col - L.nx] : -1;
+    bn[3] = z + 1 < L.nz ? L.bases[col + L.nx] : -1;
+    const int jb0 = g * G + ((colour + x + b + z) & 1);   // (x + y + z) & 1 == colour
+    float v[R][10], rh[R], dg[R];
+    int kk[R];
+    bool act[R], liq[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int jb = jb0 + 2 * r, y = b + jb;
+      act[r] = jb < L.band && y < L.fine_ny;
+      kk[r] = sidx(L, x, jb + 2, z);
+      liq[r] = false;
+      if (act[r]) {
+        const int k = kk[r];
+        liq[r] = L.label[k] != 0;
+        rh[r] = L.rhs[k];
+        dg[r] = L.diag[k];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+          int ia, ib;
+          lateral_idx(L, xn[d], zn[d], bn[d], y, k, ia, ib);
+          v[r][2 * d] = L.z[ia];
+          v[r][2 * d + 1] = L.z[ib];
+        }
+        v[r][8] = L.z[jb == 0 ? sidx(L, x, 1, z) : k - L.nx];   // the tall cell's top subcell under the band
+        v[r][9] = jb + 1 < L.band && y + 1 < L.fine_ny ? L.z[k + L.nx] : 0.0f;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (!act[r]) continue;
+      if (!liq[r]) {
+        L.z[kk[r]] = 0.0f;
+        continue;
+      }
+      const int y = b + jb0 + 2 * r;
+      double s = 0.0;
+#pragma unroll
+      for (int d = 0; d < 4; ++d) {
+        double wa, wb;
+        lateral_w(L, bn[d], y, wa, wb);
+        s += wa * double(v[r][2 * d]);
+        s += wb * double(v[r][2 * d + 1]);
+      }
+      s += -1.0 * double(v[r][8]);
+      s += -1.0 * double(v[r][9]);
+      L.z[kk[r]] = float((double(rh[r]) - s) / double(dg[r]));
+    }
+  }
+}
+
 // One colour of the block Gauss-Seidel sweep: 0/1 band cells with (x + y + z)
-// even/odd, 2/3 tall blocks of columns with (x + z) even/odd.
+// even/odd (items of G band rows), 2/3 tall blocks of columns with (x + z)
+// even/odd.
+template <int G>
 __device__ __forceinline__ void tv_smooth(TInst* I, int l, int colour, int t0, int ts) {
   const TLevel& L = I->lv[l];
   if (colour < 2) {
-    for (int k = t0; k < L.n; k += ts) {
-      int x, j, z, b;
-      const bool act = sample_active(L, k, x, j, z, b);
-      if (j < 2 || !act || ((x + b + j - 2 + z) & 1) != colour) continue;
-      if (!L.label[k]) {
-        L.z[k] = 0.0f;
-        continue;
-      }
-      L.z[k] = float((double(L.rhs[k]) - band_off(L, x, j, z, b, L.z)) / double(L.diag[k]));
-    }
+    tv_smooth_band<G>(I, l, colour, t0, ts);
   } else {
     for (int c = t0; c < L.ncol; c += ts) {
       const int z = int(divq(unsigned(c), L.mnx)), x = c - z * L.nx;
@@ -915,7 +1011,7 @@ __device__ __forceinline__ void tv_coarse_apply(TInst* I) {
     call;                                                                                    \
   }
 TALL_GRID_KERNEL(k_tall_zero, tv_zero(I, l, t0, ts))
-TALL_GRID_KERNEL(k_tall_smooth, tv_smooth(I, l, arg, t0, ts))
+TALL_GRID_KERNEL(k_tall_smooth, tv_smooth<kBandGroup>(I, l, arg, t0, ts))
 TALL_GRID_KERNEL(k_tall_residual, tv_residual(I, l, t0, ts))
 TALL_GRID_KERNEL(k_tall_restrict, tv_restrict(I, l, t0, ts))
 TALL_GRID_KERNEL(k_tall_restrict_finish, tv_restrict_finish(I, l, t0, ts))
@@ -937,7 +1033,7 @@ __global__ void __launch_bounds__(1024) k_tall_vblock(TInst* I, int first) {
     tv_zero(I, l, t0, ts);
     __syncthreads();
     for (int c = 0; c < 4; ++c) {
-      tv_smooth(I, l, c, t0, ts);
+      tv_smooth<kBlockBandGroup>(I, l, c, t0, ts);
       __syncthreads();
     }
     tv_residual(I, l, t0, ts);
@@ -953,7 +1049,7 @@ __global__ void __launch_bounds__(1024) k_tall_vblock(TInst* I, int first) {
     tv_prolong(I, l, t0, ts);
     __syncthreads();
     for (int c = 3; c >= 0; --c) {
-      tv_smooth(I, l, c, t0, ts);
+      tv_smooth<kBlockBandGroup>(I, l, c, t0, ts);
       __syncthreads();
     }
   }
@@ -1061,6 +1157,8 @@ struct fluid_pp_tall {
 namespace {
 
 int grid_for(long long n) { return int(std::max(1LL, std::min<long long>((n + kTB - 1) / kTB, kTGrid))); }
+// Grid of a band colour sweep: one thread per (column, kBandGroup rows) item.
+int grid_band(const TLevel& L) { return grid_for(1LL * ((L.band + kBandGroup - 1) / kBandGroup) * L.ncol); }
 
 size_t up256(size_t v) { return (v + 255) / 256 * 256; }
 
@@ -1079,10 +1177,10 @@ void launch_vcycle(fluid_pp_tall* T, int first) {
   TInst& I = T->inst;
   cudaStream_t s = T->stream;
   for (int l = 0; l < first; ++l) {
-    const int g = grid_for(I.lv[l].n), gc = grid_for(I.lv[l].ncol);
+    const int g = grid_for(I.lv[l].n), gc = grid_for(I.lv[l].ncol), gb = grid_band(I.lv[l]);
     k_tall_zero<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
-    k_tall_smooth<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
-    k_tall_smooth<<<g, kTB, 0, s>>>(T->d_inst, l, 1);
+    k_tall_smooth<<<gb, kTB, 0, s>>>(T->d_inst, l, 0);
+    k_tall_smooth<<<gb, kTB, 0, s>>>(T->d_inst, l, 1);
     k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 2);
     k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 3);
     k_tall_residual<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
@@ -1091,12 +1189,12 @@ void launch_vcycle(fluid_pp_tall* T, int first) {
   }
   k_tall_vblock<<<1, 1024, 0, s>>>(T->d_inst, first);
   for (int l = first - 1; l >= 0; --l) {
-    const int g = grid_for(I.lv[l].n), gc = grid_for(I.lv[l].ncol);
+    const int g = grid_for(I.lv[l].n), gc = grid_for(I.lv[l].ncol), gb = grid_band(I.lv[l]);
     k_tall_prolong<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
     k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 3);
     k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 2);
-    k_tall_smooth<<<g, kTB, 0, s>>>(T->d_inst, l, 1);
-    k_tall_smooth<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
+    k_tall_smooth<<<gb, kTB, 0, s>>>(T->d_inst, l, 1);
+    k_tall_smooth<<<gb, kTB, 0, s>>>(T->d_inst, l, 0);
   }
 }
 
@@ -1193,6 +1291,7 @@ int tall_create(const fluid_pp_tall_config* cfg, const int* bases, fluid_pp_tall
     V.ncol = P.nx * P.nz;
     V.mnx = magic64(unsigned(V.nx));
     V.mP = magic64(unsigned(V.P));
+    V.mnc = magic64(unsigned(V.ncol));
     const size_t n = size_t(V.n), nc = size_t(V.ncol);
     V.bases = static_cast<int*>(take(4 * nc));
     cudaMemcpy(V.bases, P.bases.data(), 4 * nc, cudaMemcpyHostToDevice);
