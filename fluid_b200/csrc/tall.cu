@@ -160,6 +160,14 @@ __device__ __forceinline__ double dense_val(const TLevel& L, const float* a, int
   return 0.0;
 }
 
+// Sample k -> column coordinates (x, z) and packed row j.
+__device__ __forceinline__ void decode(const TLevel& L, int k, int& x, int& j, int& z) {
+  const unsigned r = divq(unsigned(k), L.mnx), zz = divq(r, L.mP);
+  x = k - int(r) * L.nx;
+  j = int(r - zz * unsigned(L.P));
+  z = int(zz);
+}
+
 __device__ __forceinline__ bool sample_active(const TLevel& L, int k, int& x, int& j, int& z, int& b) {
   const unsigned r = divq(unsigned(k), L.mnx), zz = divq(r, L.mP);
   x = k - int(r) * L.nx;
@@ -281,131 +289,120 @@ __global__ void k_tall_assemble_band(TInst* I, int l) {
   }
 }
 
+// Integer power sums over rows 0 .. n - 1 (exact in float64 for n < 2^17).
+__device__ __forceinline__ double psum1(int n) { return 0.5 * double(n) * double(n - 1); }
+__device__ __forceinline__ double psum2(int n) { return double(n - 1) * double(n) * double(2 * n - 1) / 6.0; }
+
 // The two tall rows of a column: 2 x 2 block (internal faces, the face to the
 // first band row, lateral faces summed over the tall rows) and the couplings
-// to the neighbour columns' samples.  One warp per column: the lanes split the
-// column's rows, band couplings take ELL slots in row order by ballot prefix
-// counts, the lateral sums are reduced over the warp.
+// to the neighbour columns' samples.  A tall row interpolates (1 - t, t) with
+// t = y / B, B = b - 1; on the rows facing a neighbour's tall cell (t' = y /
+// B') or air the lateral sums have closed forms in the power sums S0, S1, S2
+// of those rows:
+//   sum (1 - t)^2 = (B^2 S0 - 2 B S1 + S2) / B^2,  sum (1 - t) t = (B S1 - S2) / B^2,
+//   sum t^2 = S2 / B^2,  sum (1 - t)(1 - t') = (B B' S0 - (B + B') S1 + S2) / (B B'),
+//   sum (1 - t) t' = (B S1 - S2) / (B B'),  sum t (1 - t') = (B' S1 - S2) / (B B'),
+//   sum t t' = S2 / (B B')
+// (integer numerators, one rounding).  Rows facing the neighbour's band rows
+// are summed one by one and give band entries in row order.
 __global__ void k_tall_assemble_tall(TInst* I, int l) {
   const TLevel& L = I->lv[l];
   const int nrow = 2 * L.ncol;
-  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-  const unsigned below = (1u << lane) - 1u;
-  auto wsum = [](double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-  };
-  for (int c = blockIdx.x * wpb + (threadIdx.x >> 5); c < L.ncol; c += gridDim.x * wpb) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < L.ncol; c += gridDim.x * blockDim.x) {
     const int z = int(divq(unsigned(c), L.mnx)), x = c - z * L.nx;
     const int b = L.bases[c];
     const int s0 = sidx(L, x, 0, z), s1 = sidx(L, x, 1, z);
-    int n0 = 0, n1 = 0;   // warp-uniform slot counts
-    // One entry, called by the whole warp with uniform arguments.
-    auto put = [&](int row, int& cnt, int s, double v) {
+    int n0 = 0, n1 = 0;
+    auto add = [&](int row, int& cnt, int s, double v) {
       if (v == 0.0) return;
       if (cnt >= kTallW) {
-        if (lane == 0) atomicExch(I->err, 1);
+        atomicExch(I->err, 1);
         return;
       }
-      if (lane == 0) {
-        L.tidx[cnt * nrow + row] = s;
-        L.tval[cnt * nrow + row] = float(v);
-      }
+      L.tidx[cnt * nrow + row] = s;
+      L.tval[cnt * nrow + row] = float(v);
       ++cnt;
-    };
-    // One entry per lane with p set, in lane order.
-    auto put_lanes = [&](int row, int& cnt, bool p, int s, double v) {
-      const unsigned m = __ballot_sync(0xffffffffu, p);
-      const int slot = cnt + __popc(m & below);
-      if (p) {
-        if (slot < kTallW) {
-          L.tidx[slot * nrow + row] = s;
-          L.tval[slot * nrow + row] = float(v);
-        } else {
-          atomicExch(I->err, 1);
-        }
-      }
-      cnt = min(kTallW, cnt + __popc(m));
     };
     if (L.label[s0]) {
       const float ph = L.phi[s0];
-      const double kin = 1.0 / double(b - 1);   // b - 1 internal faces of slope 1 / (b - 1)
+      const double B = double(b - 1), BB = B * B;
+      const double kin = 1.0 / B;   // b - 1 internal faces of slope 1 / (b - 1)
       double a00 = kin, a01 = -kin, a11 = kin;
       {
         const int s2 = sidx(L, x, 2, z);
         if (L.label[s2]) {
           a11 += 1.0;
-          put(2 * c + 1, n1, s2, -1.0);
+          add(2 * c + 1, n1, s2, -1.0);
         } else {
           a11 += 1.0 / ghost_theta_d(ph, L.phi[s2]);
         }
       }
-      double p00 = 0.0, p01 = 0.0, p11 = 0.0;   // this lane's share of the lateral faces
+      // Closed-form (1 - t)^2, (1 - t) t, t^2 sums over rows [y0, y1), times w.
+      auto self_sums = [&](int y0, int y1, double w) {
+        if (y1 <= y0) return;
+        const double S0 = double(y1 - y0), S1 = psum1(y1) - psum1(y0), S2 = psum2(y1) - psum2(y0);
+        a00 += w * ((BB * S0 - 2.0 * B * S1 + S2) / BB);
+        a01 += w * ((B * S1 - S2) / BB);
+        a11 += w * (S2 / BB);
+      };
       const int dirs[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
       for (int d = 0; d < 4; ++d) {
         const int xn = x + dirs[d][0], zn = z + dirs[d][1];
         if (xn < 0 || zn < 0 || xn >= L.nx || zn >= L.nz) continue;
-        double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
-        for (int y0 = 0; y0 < b; y0 += 32) {
-          const int y = y0 + lane;
-          bool p0 = false, p1 = false;
-          int sb = 0;
-          double t = 0.0;
-          if (y < b) {
-            t = double(y) / double(b - 1);
-            const Rep rn = rep_of(L, xn, y, zn);
-            if (rn.liq) {
-              p00 += (1.0 - t) * (1.0 - t);
-              p01 += (1.0 - t) * t;
-              p11 += t * t;
-              if (rn.n == 2) {
-                c00 += (1.0 - t) * rn.w0;
-                c01 += (1.0 - t) * rn.w1;
-                c10 += t * rn.w0;
-                c11 += t * rn.w1;
-              } else {
-                sb = rn.s0;
-                p0 = (1.0 - t) != 0.0;
-                p1 = t != 0.0;
-              }
-            } else {
-              const double inv = 1.0 / ghost_theta_d(ph, rn.phi);
-              p00 += (1.0 - t) * (1.0 - t) * inv;
-              p01 += (1.0 - t) * t * inv;
-              p11 += t * t * inv;
-            }
-          }
-          put_lanes(2 * c, n0, p0, sb, -(1.0 - t));
-          put_lanes(2 * c + 1, n1, p1, sb, -t);
-        }
-        c00 = wsum(c00);
-        c01 = wsum(c01);
-        c10 = wsum(c10);
-        c11 = wsum(c11);
+        const int bn = L.bases[xn + L.nx * zn];
         const int m0 = sidx(L, xn, 0, zn), m1 = sidx(L, xn, 1, zn);
-        put(2 * c, n0, m0, -c00);
-        put(2 * c, n0, m1, -c01);
-        put(2 * c + 1, n1, m0, -c10);
-        put(2 * c + 1, n1, m1, -c11);
+        // rows [0, min(b, bn)) face the neighbour's tall cell
+        const int mt = min(b, bn);
+        double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
+        if (L.label[m0]) {
+          self_sums(0, mt, 1.0);
+          const double Bn = double(bn - 1), BBn = B * Bn;
+          const double S0 = double(mt), S1 = psum1(mt), S2 = psum2(mt);
+          c00 = (BBn * S0 - (B + Bn) * S1 + S2) / BBn;
+          c01 = (B * S1 - S2) / BBn;
+          c10 = (Bn * S1 - S2) / BBn;
+          c11 = S2 / BBn;
+        } else {
+          self_sums(0, mt, 1.0 / ghost_theta_d(ph, L.phi[m0]));
+        }
+        // rows [bn, min(b, bn + band)) face the neighbour's band rows
+        const int ye = min(b, bn + L.band);
+        for (int y = bn; y < ye; ++y) {
+          const double t = double(y) / B;
+          const int sn = sidx(L, xn, y - bn + 2, zn);
+          if (L.label[sn]) {
+            a00 += (1.0 - t) * (1.0 - t);
+            a01 += (1.0 - t) * t;
+            a11 += t * t;
+            add(2 * c, n0, sn, -(1.0 - t));
+            add(2 * c + 1, n1, sn, -t);
+          } else {
+            const double inv = 1.0 / ghost_theta_d(ph, L.phi[sn]);
+            a00 += (1.0 - t) * (1.0 - t) * inv;
+            a01 += (1.0 - t) * t * inv;
+            a11 += t * t * inv;
+          }
+        }
+        // rows [bn + band, b) face air above the neighbour's band (phi 0.5)
+        self_sums(max(bn + L.band, 0), b, 1.0 / ghost_theta_d(ph, 0.5f));
+        add(2 * c, n0, m0, -c00);
+        add(2 * c, n0, m1, -c01);
+        add(2 * c + 1, n1, m0, -c10);
+        add(2 * c + 1, n1, m1, -c11);
       }
-      a00 += wsum(p00);
-      a01 += wsum(p01);
-      a11 += wsum(p11);
-      if (lane == 0) {
-        L.diag[s0] = float(a00);
-        L.diag[s1] = float(a11);
-        L.a01[c] = float(a01);
-      }
-    } else if (lane == 0) {
+      L.diag[s0] = float(a00);
+      L.diag[s1] = float(a11);
+      L.a01[c] = float(a01);
+    } else {
       L.diag[s0] = 1.0f;
       L.diag[s1] = 1.0f;
       L.a01[c] = 0.0f;
     }
-    for (int s = n0 + lane; s < kTallW; s += 32) {
+    for (int s = n0; s < kTallW; ++s) {
       L.tidx[s * nrow + 2 * c] = s0;
       L.tval[s * nrow + 2 * c] = 0.0f;
     }
-    for (int s = n1 + lane; s < kTallW; s += 32) {
+    for (int s = n1; s < kTallW; ++s) {
       L.tidx[s * nrow + 2 * c + 1] = s1;
       L.tval[s * nrow + 2 * c + 1] = 0.0f;
     }
@@ -484,6 +481,132 @@ __device__ __forceinline__ double apply_row(const TLevel& L, int k, int x, int j
   return s + double(L.a01[col]) * double(v[sidx(L, x, 1 - j, z)]);
 }
 
+// Off-diagonal taps of band row y of a column on lateral neighbour column
+// (xn, zn) of base bn (bn < 0: outside the grid), as in band_entries without
+// the label test: a tall neighbour row interpolates samples (ia, ib), a band
+// one is sample ia, air and walls give index self with no weight.  Callers
+// apply them to vectors that are 0 on every sample that is not liquid.
+__device__ __forceinline__ void lateral_idx(const TLevel& L, int xn, int zn, int bn, int y, int self, int& ia, int& ib) {
+  ia = ib = self;
+  if (bn < 0) return;
+  if (y < bn) {
+    ia = sidx(L, xn, 0, zn);
+    ib = ia + L.nx;
+  } else if (y < bn + L.band) {
+    ia = sidx(L, xn, y - bn + 2, zn);
+  }
+}
+__device__ __forceinline__ void lateral_w(const TLevel& L, int bn, int y, double& wa, double& wb) {
+  wa = wb = 0.0;
+  if (bn < 0) return;
+  if (y < bn) {
+    const double t = double(y) / double(bn - 1);
+    wa = double(float(-(1.0 - t)));
+    wb = double(float(-t));
+  } else if (y < bn + L.band) {
+    wa = -1.0;
+  }
+}
+
+// Operator applies over every sample run over work items: items 0 .. ncol - 1
+// are the columns' tall row pairs, item ncol + column + ncol * group the G
+// band rows group * G .. group * G + G - 1 of a column (a warp's lanes are
+// adjacent columns).  A band item loads its column's base and lateral bases
+// once and issues the loads of all its rows before the first result.
+constexpr int kApplyGroup = 4;
+
+__host__ __device__ inline long long apply_items(int ncol, int band, int G) {
+  return 1LL * ncol * (1 + (band + G - 1) / G);
+}
+
+// (A v)_k of both tall rows of column col: out(k, liquid, Av, v_k).
+template <class Out>
+__device__ __forceinline__ void tall_pair_apply(const TLevel& L, int col, const float* v, Out out) {
+  const int z = int(divq(unsigned(col), L.mnx)), x = col - z * L.nx;
+  const int s0 = sidx(L, x, 0, z), s1 = s0 + L.nx;
+  const bool l0 = L.label[s0] != 0, l1 = L.label[s1] != 0;
+  const float v0 = v[s0], v1 = v[s1];
+  double a0 = 0.0, a1 = 0.0;
+  if (l0 || l1) {
+    double o0, o1;
+    tall_off_pair(L, col, v, o0, o1);
+    const double a01 = L.a01[col];
+    a0 = double(L.diag[s0]) * double(v0);
+    a0 += o0;
+    a0 = a0 + a01 * double(v1);
+    a1 = double(L.diag[s1]) * double(v1);
+    a1 += o1;
+    a1 = a1 + a01 * double(v0);
+  }
+  out(s0, l0, a0, v0);
+  out(s1, l1, a1, v1);
+}
+
+// (A v)_k of the G band rows of band item it: out(k, liquid, Av, v_k, e) for
+// each row inside the band (inactive rows above the fine grid as not liquid),
+// e = extra(k) loaded with the row's operands.  v must be 0 on every sample
+// that is not liquid (the label tests of band_entries are left out).
+template <int G, class Extra, class Out>
+__device__ __forceinline__ void band_rows_apply(const TLevel& L, int it, const float* v, Extra extra, Out out) {
+  const int g = int(divq(unsigned(it), L.mnc));
+  const int col = it - g * L.ncol;
+  const int z = int(divq(unsigned(col), L.mnx)), x = col - z * L.nx;
+  const int b = L.bases[col];
+  const int xn[4] = {x - 1, x + 1, x, x}, zn[4] = {z, z, z - 1, z + 1};
+  int bn[4];
+  bn[0] = x > 0 ? L.bases[col - 1] : -1;
+  bn[1] = x + 1 < L.nx ? L.bases[col + 1] : -1;
+  bn[2] = z > 0 ? L.bases[col - L.nx] : -1;
+  bn[3] = z + 1 < L.nz ? L.bases[col + L.nx] : -1;
+  float vv[G][11], dg[G], ex[G];
+  bool liq[G];
+#pragma unroll
+  for (int r = 0; r < G; ++r) {
+    const int jb = g * G + r, y = b + jb;
+    const int k = sidx(L, x, jb + 2, z);
+    liq[r] = false;
+    ex[r] = dg[r] = 0.0f;
+    if (jb < L.band && y < L.fine_ny) {
+      liq[r] = L.label[k] != 0;
+      dg[r] = L.diag[k];
+      ex[r] = extra(k);
+      vv[r][10] = v[k];
+#pragma unroll
+      for (int d = 0; d < 4; ++d) {
+        int ia, ib;
+        lateral_idx(L, xn[d], zn[d], bn[d], y, k, ia, ib);
+        vv[r][2 * d] = v[ia];
+        vv[r][2 * d + 1] = v[ib];
+      }
+      vv[r][8] = v[jb == 0 ? sidx(L, x, 1, z) : k - L.nx];
+      vv[r][9] = jb + 1 < L.band && y + 1 < L.fine_ny ? v[k + L.nx] : 0.0f;
+    } else {
+      vv[r][10] = 0.0f;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < G; ++r) {
+    const int jb = g * G + r;
+    if (jb >= L.band) continue;
+    const int y = b + jb;
+    double av = 0.0;
+    if (liq[r]) {
+      double s = 0.0;
+#pragma unroll
+      for (int d = 0; d < 4; ++d) {
+        double wa, wb;
+        lateral_w(L, bn[d], y, wa, wb);
+        s += wa * double(vv[r][2 * d]);
+        s += wb * double(vv[r][2 * d + 1]);
+      }
+      s += -1.0 * double(vv[r][8]);
+      s += -1.0 * double(vv[r][9]);
+      av = double(dg[r]) * double(vv[r][10]) + s;
+    }
+    out(sidx(L, x, jb + 2, z), liq[r], av, vv[r][10], ex[r]);
+  }
+}
+
 // Dense inverse of the coarsest level (air and inactive samples identity rows).
 __global__ void k_tall_factor(TInst* I) {
   extern __shared__ double A[];
@@ -524,25 +647,38 @@ __device__ __forceinline__ double dense_div(const TInst& I, const TLevel& L, int
 
 __global__ void k_tall_rhs(TInst* I) {
   const TLevel& L = I->lv[0];
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
-    int x, j, z, b;
-    const bool act = sample_active(L, k, x, j, z, b);
-    if (j == 1) continue;   // written with j = 0
-    if (j >= 2) {
-      I->b[k] = (act && L.label[k]) ? float(-dense_div(*I, L, x, b + j - 2, z)) : 0.0f;
-      continue;
-    }
+  // Tall segments, a warp per column: b0 = sum (1 - t) (-div), b1 = sum t (-div)
+  // over the column's tall rows, the lanes splitting the rows.
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int c = gw; c < L.ncol; c += nw) {
+    const int z = int(divq(unsigned(c), L.mnx)), x = c - z * L.nx;
+    const int b = L.bases[c];
+    const int s0 = sidx(L, x, 0, z);
     double b0 = 0.0, b1 = 0.0;
-    if (L.label[k]) {
-      for (int y = 0; y < b; ++y) {
+    if (L.label[s0]) {
+      for (int y = lane; y < b; y += 32) {
         const double t = double(y) / double(b - 1);
         const double dv = -dense_div(*I, L, x, y, z);
         b0 += (1.0 - t) * dv;
         b1 += t * dv;
       }
+      for (int o = 16; o > 0; o >>= 1) {
+        b0 += __shfl_xor_sync(0xffffffffu, b0, o);
+        b1 += __shfl_xor_sync(0xffffffffu, b1, o);
+      }
     }
-    I->b[k] = float(b0);
-    I->b[sidx(L, x, 1, z)] = float(b1);
+    if (lane == 0) {
+      I->b[s0] = float(b0);
+      I->b[s0 + L.nx] = float(b1);
+    }
+  }
+  // Band samples, a thread each.
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
+    int x, j, z, b;
+    const bool act = sample_active(L, k, x, j, z, b);
+    if (j < 2) continue;
+    I->b[k] = (act && L.label[k]) ? float(-dense_div(*I, L, x, b + j - 2, z)) : 0.0f;
   }
 }
 
@@ -656,21 +792,33 @@ __global__ void k_tall_dir(TInst* I) {
     I->d[k] = L.label[k] ? (beta == 0.0f ? L.z[k] : L.z[k] + beta * I->d[k]) : 0.0f;
 }
 
+// d = d on liquid samples, 0 elsewhere (the operator apply reads d without
+// label tests).
+__global__ void k_tall_mask_d(TInst* I) {
+  const TLevel& L = I->lv[0];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x)
+    if (!L.label[k]) I->d[k] = 0.0f;
+}
+
 // q = A d, delta = d . q
 __global__ void k_tall_spmv(TInst* I) {
   const Ctrl* c = I->ctrl;
   if (c->done) return;
   const TLevel& L = I->lv[0];
   double dq = 0.0;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n; k += gridDim.x * blockDim.x) {
-    int x, j, z, b;
-    sample_active(L, k, x, j, z, b);
-    float q = 0.0f;
-    if (L.label[k]) {
-      q = float(apply_row(L, k, x, j, z, b, I->d));
-      dq += double(I->d[k]) * double(q);
-    }
+  auto put = [&](int k, bool liq, double av, float dk) {
+    const float q = liq ? float(av) : 0.0f;
+    if (liq) dq += double(dk) * double(q);
     I->q[k] = q;
+  };
+  const long long items = apply_items(L.ncol, L.band, kApplyGroup);
+  for (long long it = blockIdx.x * blockDim.x + threadIdx.x; it < items; it += gridDim.x * blockDim.x) {
+    if (it < L.ncol) {
+      tall_pair_apply(L, int(it), I->d, put);
+    } else {
+      band_rows_apply<kApplyGroup>(L, int(it - L.ncol), I->d, [](int) { return 0.0f; },
+                                   [&](int k, bool liq, double av, float dk, float) { put(k, liq, av, dk); });
+    }
   }
   const double v[1] = {dq};
   const bool mx[1] = {false};
@@ -752,33 +900,6 @@ __device__ __forceinline__ void tv_zero(TInst* I, int l, int t0, int ts) {
 // single-CTA block (64 registers a thread) kBlockBandGroup.
 constexpr int kBandGroup = 8;
 constexpr int kBlockBandGroup = 2;
-
-// Off-diagonal taps of band row y of a column on lateral neighbour column
-// (xn, zn) of base bn (bn < 0: outside the grid), as in band_entries without
-// the label test: a tall neighbour row interpolates samples (ia, ib), a band
-// one is sample ia, air and walls give index self with no weight.  Callers
-// apply them to vectors that are 0 on every sample that is not liquid.
-__device__ __forceinline__ void lateral_idx(const TLevel& L, int xn, int zn, int bn, int y, int self, int& ia, int& ib) {
-  ia = ib = self;
-  if (bn < 0) return;
-  if (y < bn) {
-    ia = sidx(L, xn, 0, zn);
-    ib = ia + L.nx;
-  } else if (y < bn + L.band) {
-    ia = sidx(L, xn, y - bn + 2, zn);
-  }
-}
-__device__ __forceinline__ void lateral_w(const TLevel& L, int bn, int y, double& wa, double& wb) {
-  wa = wb = 0.0;
-  if (bn < 0) return;
-  if (y < bn) {
-    const double t = double(y) / double(bn - 1);
-    wa = double(float(-(1.0 - t)));
-    wb = double(float(-t));
-  } else if (y < bn + L.band) {
-    wa = -1.0;
-  }
-}
 
 template <int G>
 __device__ __forceinline__ void tv_smooth_band(TInst* I, int l, int colour, int t0, int ts) {
@@ -875,18 +996,30 @@ __device__ __forceinline__ void tv_smooth(TInst* I, int l, int colour, int t0, i
   }
 }
 
-// res = scale (rhs - A z); level 0 scales by sigma.
+// res = scale (rhs - A z); level 0 scales by sigma.  Work items as in the
+// operator apply, G band rows each.
+template <int G>
 __device__ __forceinline__ void tv_residual(TInst* I, int l, int t0, int ts) {
   const TLevel& L = I->lv[l];
   const double scale = l == 0 ? I->ctrl->sigma : 1.0;
-  for (int k = t0; k < L.n; k += ts) {
-    int x, j, z, b;
-    sample_active(L, k, x, j, z, b);
-    L.res[k] = L.label[k] ? float(scale * (double(L.rhs[k]) - apply_row(L, k, x, j, z, b, L.z))) : 0.0f;
+  const long long items = apply_items(L.ncol, L.band, G);
+  for (long long it = t0; it < items; it += ts) {
+    if (it < L.ncol) {
+      tall_pair_apply(L, int(it), L.z, [&](int k, bool liq, double av, float) {
+        L.res[k] = liq ? float(scale * (double(L.rhs[k]) - av)) : 0.0f;
+      });
+    } else {
+      band_rows_apply<G>(L, int(it - L.ncol), L.z, [&](int k) { return L.rhs[k]; },
+                         [&](int k, bool liq, double av, float, float rhs) {
+                           L.res[k] = liq ? float(scale * (double(rhs) - av)) : 0.0f;
+                         });
+    }
   }
 }
 
-// acc_c += 1/2 P^T res_f in 32.32 fixed point (order-independent sums).  The
+// acc_c += 1/2 P^T res_f in 32.32 fixed point (order-independent sums; sums
+// that land on samples that are not liquid are dropped by tv_restrict_finish,
+// which reads only liquid accumulators and clears them all).  The
 // fine sample at dense (x, row y, z) takes the 2 x 2 x 2 trilinear taps of the
 // coarse dense cells around it (taps2: a dropped tap has weight 0); a coarse
 // tall cell passes its share to the column's two samples (1 - t, t), a coarse
@@ -895,11 +1028,12 @@ __device__ __forceinline__ void tv_restrict(TInst* I, int l, int t0, int ts) {
   const TLevel& F = I->lv[l];
   const TLevel& C = I->lv[l + 1];
   for (int k = t0; k < F.n; k += ts) {
-    if (!F.label[k]) continue;
+    int x, j, z;
+    decode(F, k, x, j, z);
+    const bool liq = F.label[k] != 0;   // the three loads issue together
     const float r = F.res[k];
-    if (r == 0.0f) continue;
-    int x, j, z, b;
-    sample_active(F, k, x, j, z, b);
+    const int b = F.bases[x + F.nx * z];
+    if (!liq || r == 0.0f) continue;
     int cx[2], cy[2], cz[2];
     float wx[2], wy[2], wz[2];
     taps2(x, 2, C.nx, cx, wx);
@@ -921,13 +1055,11 @@ __device__ __forceinline__ void tv_restrict(TInst* I, int l, int t0, int ts) {
           const int Y = cy[c1];
           const double v = hr * (wxz * double(wy[c1]));
           if (Y < bc) {
-            if (!C.label[s0]) continue;
             const double t = double(Y) / double(bc - 1);
             t0acc += llrint(v * (1.0 - t) * kFix);
             t1acc += llrint(v * t * kFix);
           } else if (Y < bc + C.band) {
-            const int sn = s0 + C.nx * (Y - bc + 2);
-            if (C.label[sn]) atomicAdd(&C.acc[sn], (unsigned long long)llrint(v * kFix));
+            atomicAdd(&C.acc[s0 + C.nx * (Y - bc + 2)], (unsigned long long)llrint(v * kFix));
           }
         }
         if (t0acc != 0) atomicAdd(&C.acc[s0], (unsigned long long)t0acc);
@@ -953,9 +1085,12 @@ __device__ __forceinline__ void tv_prolong(TInst* I, int l, int t0, int ts) {
   const TLevel& C = I->lv[l + 1];
   const double unscale = l == 0 ? 1.0 / I->ctrl->sigma : 1.0;
   for (int k = t0; k < F.n; k += ts) {
-    if (!F.label[k]) continue;
-    int x, j, z, b;
-    sample_active(F, k, x, j, z, b);
+    int x, j, z;
+    decode(F, k, x, j, z);
+    const bool liq = F.label[k] != 0;   // the three loads issue together
+    const float zf = F.z[k];
+    const int b = F.bases[x + F.nx * z];
+    if (!liq) continue;
     int cx[2], cy[2], cz[2];
     float wx[2], wy[2], wz[2];
     taps2(x, 2, C.nx, cx, wx);
@@ -986,7 +1121,7 @@ __device__ __forceinline__ void tv_prolong(TInst* I, int l, int t0, int ts) {
           }
           s += w * val;
         }
-    F.z[k] = float(double(F.z[k]) + s * unscale);
+    F.z[k] = float(double(zf) + s * unscale);
   }
 }
 
@@ -1012,7 +1147,7 @@ __device__ __forceinline__ void tv_coarse_apply(TInst* I) {
   }
 TALL_GRID_KERNEL(k_tall_zero, tv_zero(I, l, t0, ts))
 TALL_GRID_KERNEL(k_tall_smooth, tv_smooth<kBandGroup>(I, l, arg, t0, ts))
-TALL_GRID_KERNEL(k_tall_residual, tv_residual(I, l, t0, ts))
+TALL_GRID_KERNEL(k_tall_residual, tv_residual<kApplyGroup>(I, l, t0, ts))
 TALL_GRID_KERNEL(k_tall_restrict, tv_restrict(I, l, t0, ts))
 TALL_GRID_KERNEL(k_tall_restrict_finish, tv_restrict_finish(I, l, t0, ts))
 TALL_GRID_KERNEL(k_tall_prolong, tv_prolong(I, l, t0, ts))
@@ -1036,7 +1171,7 @@ __global__ void __launch_bounds__(1024) k_tall_vblock(TInst* I, int first) {
       tv_smooth<kBlockBandGroup>(I, l, c, t0, ts);
       __syncthreads();
     }
-    tv_residual(I, l, t0, ts);
+    tv_residual<1>(I, l, t0, ts);
     __syncthreads();
     tv_restrict(I, l, t0, ts);
     __syncthreads();
@@ -1183,7 +1318,7 @@ void launch_vcycle(fluid_pp_tall* T, int first) {
     k_tall_smooth<<<gb, kTB, 0, s>>>(T->d_inst, l, 1);
     k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 2);
     k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 3);
-    k_tall_residual<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
+    k_tall_residual<<<grid_for(apply_items(I.lv[l].ncol, I.lv[l].band, kApplyGroup)), kTB, 0, s>>>(T->d_inst, l, 0);
     k_tall_restrict<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
     k_tall_restrict_finish<<<grid_for(I.lv[l + 1].n), kTB, 0, s>>>(T->d_inst, l + 1, 0);
   }
@@ -1209,7 +1344,7 @@ void launch_setup(fluid_pp_tall* T) {
   }
   for (int l = 0; l < I.nlev; ++l) {
     k_tall_assemble_band<<<grid_for(I.lv[l].n), kTB, 0, s>>>(T->d_inst, l);
-    k_tall_assemble_tall<<<grid_for(32LL * I.lv[l].ncol), kTB, 0, s>>>(T->d_inst, l);
+    k_tall_assemble_tall<<<grid_for(I.lv[l].ncol), kTB, 0, s>>>(T->d_inst, l);
   }
   const size_t m = size_t(I.coarse_m);
   k_tall_factor<<<1, 1024, m * m * sizeof(double), s>>>(T->d_inst);
@@ -1553,6 +1688,7 @@ int fluid_pp_tall_apply_operator(fluid_pp_tall* T, const float* p, float* out) {
   TInst& I = T->inst;
   cudaMemcpyAsync(I.d, p, 4 * n, cudaMemcpyHostToDevice, T->stream);
   k_tall_reset<<<1, 1, 0, T->stream>>>(T->d_inst);
+  k_tall_mask_d<<<grid_for(n), kTB, 0, T->stream>>>(T->d_inst);
   k_tall_spmv<<<grid_for(n), kTB, 0, T->stream>>>(T->d_inst);
   cudaMemcpyAsync(out, I.q, 4 * n, cudaMemcpyDeviceToHost, T->stream);
   cudaError_t e = cudaGetLastError();
