@@ -481,31 +481,69 @@ __device__ __forceinline__ double apply_row(const TLevel& L, int k, int x, int j
   return s + double(L.a01[col]) * double(v[sidx(L, x, 1 - j, z)]);
 }
 
-// Off-diagonal taps of band row y of a column on lateral neighbour column
-// (xn, zn) of base bn (bn < 0: outside the grid), as in band_entries without
-// the label test: a tall neighbour row interpolates samples (ia, ib), a band
-// one is sample ia, air and walls give index self with no weight.  Callers
-// apply them to vectors that are 0 on every sample that is not liquid.
-__device__ __forceinline__ void lateral_idx(const TLevel& L, int xn, int zn, int bn, int y, int self, int& ia, int& ib) {
-  ia = ib = self;
-  if (bn < 0) return;
-  if (y < bn) {
-    ia = sidx(L, xn, 0, zn);
-    ib = ia + L.nx;
-  } else if (y < bn + L.band) {
-    ia = sidx(L, xn, y - bn + 2, zn);
+// A band work item's column: its base b and, per lateral neighbour d in
+// band_entries' order (x - 1, x + 1, z - 1, z + 1), e = bn - b (band row jb
+// faces the neighbour's tall cell for jb < e, its band rows for e <= jb <
+// e + band, air above; outside the grid e = -2^30, always air), the index
+// offset from row jb's own sample to the neighbour's band sample of the same
+// dense row (the same for every row), the neighbour's bottom sample and base.
+struct BandCol {
+  int x, z, b;
+  int e[4], off[4], tn[4];
+  float rbn[4];   // 1 / (bn - 1): a tall neighbour row interpolates with t = y / (bn - 1)
+};
+
+__device__ __forceinline__ void band_col(const TLevel& L, int col, BandCol& c) {
+  c.z = int(divq(unsigned(col), L.mnx));
+  c.x = col - c.z * L.nx;
+  c.b = L.bases[col];
+  const int dx[4] = {-1, 1, 0, 0}, dz[4] = {0, 0, -1, 1};
+  const bool in[4] = {c.x > 0, c.x + 1 < L.nx, c.z > 0, c.z + 1 < L.nz};
+  int bn[4];
+#pragma unroll
+  for (int d = 0; d < 4; ++d) bn[d] = in[d] ? L.bases[col + dx[d] + L.nx * dz[d]] : 2;
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    c.e[d] = in[d] ? bn[d] - c.b : -(1 << 30);
+    c.off[d] = dx[d] + L.nx * (c.b - bn[d]) + L.nx * L.P * dz[d];
+    c.tn[d] = in[d] ? sidx(L, c.x + dx[d], 0, c.z + dz[d]) : 0;
+    c.rbn[d] = __frcp_rn(float(bn[d] - 1));
   }
 }
-__device__ __forceinline__ void lateral_w(const TLevel& L, int bn, int y, double& wa, double& wb) {
-  wa = wb = 0.0;
-  if (bn < 0) return;
-  if (y < bn) {
-    const double t = double(y) / double(bn - 1);
-    wa = double(float(-(1.0 - t)));
-    wb = double(float(-t));
-  } else if (y < bn + L.band) {
-    wa = -1.0;
+
+// The off-diagonal operands of band row jb (own sample k): per lateral
+// neighbour its band sample, or its tall pair, or nothing (0); then the
+// sample below (the tall cell's top sample for jb = 0: also k - nx) and above.
+__device__ __forceinline__ void band_row_loads(const TLevel& L, const BandCol& c, int jb, int k, const float* v,
+                                               float (&vv)[10]) {
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    const bool tall = jb < c.e[d], band = !tall && jb < c.e[d] + L.band;
+    vv[2 * d] = tall ? v[c.tn[d]] : (band ? v[k + c.off[d]] : 0.0f);
+    vv[2 * d + 1] = tall ? v[c.tn[d] + L.nx] : 0.0f;
   }
+  vv[8] = v[k - L.nx];
+  vv[9] = jb + 1 < L.band && c.b + jb + 1 < L.fine_ny ? v[k + L.nx] : 0.0f;
+}
+
+// Off-diagonal part of band row jb applied to the operands of band_row_loads,
+// in float: the weights of band_entries (a tall neighbour row interpolates
+// with t = y / (bn - 1), here y times the float reciprocal), without the label
+// tests (the vectors are 0 on every sample that is not liquid).
+__device__ __forceinline__ float band_row_off(const TLevel& L, const BandCol& c, int jb, const float (&vv)[10]) {
+  float s = 0.0f;
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    const bool tall = jb < c.e[d];
+    const float t = float(c.b + jb) * c.rbn[d];
+    const float wa = tall ? t - 1.0f : (jb < c.e[d] + L.band ? -1.0f : 0.0f);
+    const float wb = tall ? -t : 0.0f;
+    s = fmaf(wa, vv[2 * d], s);
+    s = fmaf(wb, vv[2 * d + 1], s);
+  }
+  s -= vv[8];
+  s -= vv[9];
+  return s;
 }
 
 // Operator applies over every sample run over work items: items 0 .. ncol - 1
@@ -513,7 +551,7 @@ __device__ __forceinline__ void lateral_w(const TLevel& L, int bn, int y, double
 // band rows group * G .. group * G + G - 1 of a column (a warp's lanes are
 // adjacent columns).  A band item loads its column's base and lateral bases
 // once and issues the loads of all its rows before the first result.
-constexpr int kApplyGroup = 4;
+constexpr int kApplyGroup = 2;
 
 __host__ __device__ inline long long apply_items(int ncol, int band, int G) {
   return 1LL * ncol * (1 + (band + G - 1) / G);
@@ -542,68 +580,37 @@ __device__ __forceinline__ void tall_pair_apply(const TLevel& L, int col, const 
   out(s1, l1, a1, v1);
 }
 
-// (A v)_k of the G band rows of band item it: out(k, liquid, Av, v_k, e) for
-// each row inside the band (inactive rows above the fine grid as not liquid),
-// e = extra(k) loaded with the row's operands.  v must be 0 on every sample
-// that is not liquid (the label tests of band_entries are left out).
+// (A v)_k of the G band rows of band item it, in float: out(k,
+// liquid, Av, v_k, e) for each row inside the band (inactive rows above the
+// fine grid as not liquid), e = extra(k) loaded with the row's operands.  v
+// must be 0 on every sample that is not liquid.
 template <int G, class Extra, class Out>
 __device__ __forceinline__ void band_rows_apply(const TLevel& L, int it, const float* v, Extra extra, Out out) {
   const int g = int(divq(unsigned(it), L.mnc));
-  const int col = it - g * L.ncol;
-  const int z = int(divq(unsigned(col), L.mnx)), x = col - z * L.nx;
-  const int b = L.bases[col];
-  const int xn[4] = {x - 1, x + 1, x, x}, zn[4] = {z, z, z - 1, z + 1};
-  int bn[4];
-  bn[0] = x > 0 ? L.bases[col - 1] : -1;
-  bn[1] = x + 1 < L.nx ? L.bases[col + 1] : -1;
-  bn[2] = z > 0 ? L.bases[col - L.nx] : -1;
-  bn[3] = z + 1 < L.nz ? L.bases[col + L.nx] : -1;
-  float vv[G][11], dg[G], ex[G];
+  BandCol c;
+  band_col(L, it - g * L.ncol, c);
+  float vv[G][10], vk[G], dg[G], ex[G];
   bool liq[G];
 #pragma unroll
   for (int r = 0; r < G; ++r) {
-    const int jb = g * G + r, y = b + jb;
-    const int k = sidx(L, x, jb + 2, z);
+    const int jb = g * G + r;
+    const int k = sidx(L, c.x, jb + 2, c.z);
     liq[r] = false;
-    ex[r] = dg[r] = 0.0f;
-    if (jb < L.band && y < L.fine_ny) {
+    vk[r] = dg[r] = ex[r] = 0.0f;
+    if (jb < L.band && c.b + jb < L.fine_ny) {
       liq[r] = L.label[k] != 0;
       dg[r] = L.diag[k];
       ex[r] = extra(k);
-      vv[r][10] = v[k];
-#pragma unroll
-      for (int d = 0; d < 4; ++d) {
-        int ia, ib;
-        lateral_idx(L, xn[d], zn[d], bn[d], y, k, ia, ib);
-        vv[r][2 * d] = v[ia];
-        vv[r][2 * d + 1] = v[ib];
-      }
-      vv[r][8] = v[jb == 0 ? sidx(L, x, 1, z) : k - L.nx];
-      vv[r][9] = jb + 1 < L.band && y + 1 < L.fine_ny ? v[k + L.nx] : 0.0f;
-    } else {
-      vv[r][10] = 0.0f;
+      vk[r] = v[k];
+      band_row_loads(L, c, jb, k, v, vv[r]);
     }
   }
 #pragma unroll
   for (int r = 0; r < G; ++r) {
     const int jb = g * G + r;
     if (jb >= L.band) continue;
-    const int y = b + jb;
-    double av = 0.0;
-    if (liq[r]) {
-      double s = 0.0;
-#pragma unroll
-      for (int d = 0; d < 4; ++d) {
-        double wa, wb;
-        lateral_w(L, bn[d], y, wa, wb);
-        s += wa * double(vv[r][2 * d]);
-        s += wb * double(vv[r][2 * d + 1]);
-      }
-      s += -1.0 * double(vv[r][8]);
-      s += -1.0 * double(vv[r][9]);
-      av = double(dg[r]) * double(vv[r][10]) + s;
-    }
-    out(sidx(L, x, jb + 2, z), liq[r], av, vv[r][10], ex[r]);
+    const float av = liq[r] ? fmaf(dg[r], vk[r], band_row_off(L, c, jb, vv[r])) : 0.0f;
+    out(sidx(L, c.x, jb + 2, c.z), liq[r], av, vk[r], ex[r]);
   }
 }
 
@@ -898,7 +905,7 @@ __device__ __forceinline__ void tv_zero(TInst* I, int l, int t0, int ts) {
 // update.  Rows of one colour never neighbour each other, so the loads see no
 // update of the same sweep.  Grid launches take kBandGroup rows per item, the
 // single-CTA block (64 registers a thread) kBlockBandGroup.
-constexpr int kBandGroup = 8;
+constexpr int kBandGroup = 4;
 constexpr int kBlockBandGroup = 2;
 
 template <int G>
@@ -909,60 +916,31 @@ __device__ __forceinline__ void tv_smooth_band(TInst* I, int l, int colour, int 
   const int items = ((L.band + G - 1) / G) * L.ncol;
   for (int it = t0; it < items; it += ts) {
     const int g = int(divq(unsigned(it), L.mnc));
-    const int col = it - g * L.ncol;
-    const int z = int(divq(unsigned(col), L.mnx)), x = col - z * L.nx;
-    const int b = L.bases[col];
-    const int xn[4] = {x - 1, x + 1, x, x}, zn[4] = {z, z, z - 1, z + 1};
-    int bn[4];
-    bn[0] = x > 0 ? L.bases[col - 1] : -1;
-    bn[1] = x + 1 < L.nx ? L.bases[col + 1] : -1;
-    bn[2] = z > 0 ? L.bases[col - L.nx] : -1;
-    bn[3] = z + 1 < L.nz ? L.bases[col + L.nx] : -1;
-    const int jb0 = g * G + ((colour + x + b + z) & 1);   // (x + y + z) & 1 == colour
-    float v[R][10], rh[R], dg[R];
-    int kk[R];
+    BandCol c;
+    band_col(L, it - g * L.ncol, c);
+    const int jb0 = g * G + ((colour + c.x + c.b + c.z) & 1);   // (x + y + z) & 1 == colour
+    float vv[R][10], rh[R], dg[R];
     bool act[R], liq[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int jb = jb0 + 2 * r, y = b + jb;
-      act[r] = jb < L.band && y < L.fine_ny;
-      kk[r] = sidx(L, x, jb + 2, z);
+      const int jb = jb0 + 2 * r;
+      const int k = sidx(L, c.x, jb + 2, c.z);
+      act[r] = jb < L.band && c.b + jb < L.fine_ny;
       liq[r] = false;
+      rh[r] = dg[r] = 0.0f;
       if (act[r]) {
-        const int k = kk[r];
         liq[r] = L.label[k] != 0;
         rh[r] = L.rhs[k];
         dg[r] = L.diag[k];
-#pragma unroll
-        for (int d = 0; d < 4; ++d) {
-          int ia, ib;
-          lateral_idx(L, xn[d], zn[d], bn[d], y, k, ia, ib);
-          v[r][2 * d] = L.z[ia];
-          v[r][2 * d + 1] = L.z[ib];
-        }
-        v[r][8] = L.z[jb == 0 ? sidx(L, x, 1, z) : k - L.nx];   // the tall cell's top subcell under the band
-        v[r][9] = jb + 1 < L.band && y + 1 < L.fine_ny ? L.z[k + L.nx] : 0.0f;
+        band_row_loads(L, c, jb, k, L.z, vv[r]);
       }
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       if (!act[r]) continue;
-      if (!liq[r]) {
-        L.z[kk[r]] = 0.0f;
-        continue;
-      }
-      const int y = b + jb0 + 2 * r;
-      double s = 0.0;
-#pragma unroll
-      for (int d = 0; d < 4; ++d) {
-        double wa, wb;
-        lateral_w(L, bn[d], y, wa, wb);
-        s += wa * double(v[r][2 * d]);
-        s += wb * double(v[r][2 * d + 1]);
-      }
-      s += -1.0 * double(v[r][8]);
-      s += -1.0 * double(v[r][9]);
-      L.z[kk[r]] = float((double(rh[r]) - s) / double(dg[r]));
+      const int jb = jb0 + 2 * r;
+      const int k = sidx(L, c.x, jb + 2, c.z);
+      L.z[k] = liq[r] ? (rh[r] - band_row_off(L, c, jb, vv[r])) / dg[r] : 0.0f;
     }
   }
 }
@@ -1010,9 +988,9 @@ __device__ __forceinline__ void tv_residual(TInst* I, int l, int t0, int ts) {
       });
     } else {
       band_rows_apply<G>(L, int(it - L.ncol), L.z, [&](int k) { return L.rhs[k]; },
-                         [&](int k, bool liq, double av, float, float rhs) {
-                           L.res[k] = liq ? float(scale * (double(rhs) - av)) : 0.0f;
-                         });
+                                [&](int k, bool liq, float av, float, float rhs) {
+                                  L.res[k] = liq ? float(scale * double(rhs - av)) : 0.0f;
+                                });
     }
   }
 }
