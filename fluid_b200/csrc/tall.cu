@@ -995,7 +995,8 @@ __device__ __forceinline__ void tv_residual(TInst* I, int l, int t0, int ts) {
   }
 }
 
-// acc_c += 1/2 P^T res_f in 32.32 fixed point (order-independent sums; sums
+// acc_c += 1/2 P^T res_f in 32.32 fixed point, each term rounded from float
+// (order-independent integer sums; sums
 // that land on samples that are not liquid are dropped by tv_restrict_finish,
 // which reads only liquid accumulators and clears them all).  The
 // fine sample at dense (x, row y, z) takes the 2 x 2 x 2 trilinear taps of the
@@ -1005,6 +1006,7 @@ __device__ __forceinline__ void tv_residual(TInst* I, int l, int t0, int ts) {
 __device__ __forceinline__ void tv_restrict(TInst* I, int l, int t0, int ts) {
   const TLevel& F = I->lv[l];
   const TLevel& C = I->lv[l + 1];
+  constexpr float kFixF = 4294967296.0f;
   for (int k = t0; k < F.n; k += ts) {
     int x, j, z;
     decode(F, k, x, j, z);
@@ -1017,27 +1019,33 @@ __device__ __forceinline__ void tv_restrict(TInst* I, int l, int t0, int ts) {
     taps2(x, 2, C.nx, cx, wx);
     taps2(sample_row(j, b), 2, C.fine_ny, cy, wy);
     taps2(z, 2, C.nz, cz, wz);
-    const double hr = 0.5 * double(r);
+    const float hr = 0.5f * r;
+    int bc[2][2];
+#pragma unroll
+    for (int c2 = 0; c2 < 2; ++c2)
+#pragma unroll
+      for (int c0 = 0; c0 < 2; ++c0) bc[c2][c0] = C.bases[cx[c0] + C.nx * cz[c2]];
 #pragma unroll
     for (int c2 = 0; c2 < 2; ++c2)
 #pragma unroll
       for (int c0 = 0; c0 < 2; ++c0) {
-        const double wxz = double(wx[c0]) * double(wz[c2]);
-        if (wxz == 0.0) continue;
-        const int bc = C.bases[cx[c0] + C.nx * cz[c2]];
+        const float wxz = wx[c0] * wz[c2];   // products of quarters: exact
+        if (wxz == 0.0f) continue;
+        const int B = bc[c2][c0];
+        const float rB = __frcp_rn(float(B - 1));
         const int s0 = sidx(C, cx[c0], 0, cz[c2]);
         long long t0acc = 0, t1acc = 0;   // the column's tall samples, summed over the y taps
 #pragma unroll
         for (int c1 = 0; c1 < 2; ++c1) {
           if (wy[c1] == 0.0f) continue;
           const int Y = cy[c1];
-          const double v = hr * (wxz * double(wy[c1]));
-          if (Y < bc) {
-            const double t = double(Y) / double(bc - 1);
-            t0acc += llrint(v * (1.0 - t) * kFix);
-            t1acc += llrint(v * t * kFix);
-          } else if (Y < bc + C.band) {
-            atomicAdd(&C.acc[s0 + C.nx * (Y - bc + 2)], (unsigned long long)llrint(v * kFix));
+          const float v = hr * (wxz * wy[c1]) * kFixF;
+          if (Y < B) {
+            const float t = float(Y) * rB;
+            t0acc += __float2ll_rn(v * (1.0f - t));
+            t1acc += __float2ll_rn(v * t);
+          } else if (Y < B + C.band) {
+            atomicAdd(&C.acc[s0 + C.nx * (Y - B + 2)], (unsigned long long)__float2ll_rn(v));
           }
         }
         if (t0acc != 0) atomicAdd(&C.acc[s0], (unsigned long long)t0acc);
@@ -1061,7 +1069,7 @@ __device__ __forceinline__ void tv_restrict_finish(TInst* I, int l, int t0, int 
 __device__ __forceinline__ void tv_prolong(TInst* I, int l, int t0, int ts) {
   const TLevel& F = I->lv[l];
   const TLevel& C = I->lv[l + 1];
-  const double unscale = l == 0 ? 1.0 / I->ctrl->sigma : 1.0;
+  const float unscale = l == 0 ? float(1.0 / I->ctrl->sigma) : 1.0f;
   for (int k = t0; k < F.n; k += ts) {
     int x, j, z;
     decode(F, k, x, j, z);
@@ -1079,27 +1087,27 @@ __device__ __forceinline__ void tv_prolong(TInst* I, int l, int t0, int ts) {
     for (int c2 = 0; c2 < 2; ++c2)
 #pragma unroll
       for (int c0 = 0; c0 < 2; ++c0) bc[c2][c0] = C.bases[cx[c0] + C.nx * cz[c2]];
-    double s = 0.0;
+    float s = 0.0f;
 #pragma unroll
     for (int c2 = 0; c2 < 2; ++c2)
 #pragma unroll
       for (int c1 = 0; c1 < 2; ++c1)
 #pragma unroll
         for (int c0 = 0; c0 < 2; ++c0) {
-          const double w = double(wx[c0]) * double(wy[c1]) * double(wz[c2]);
-          if (w == 0.0) continue;
+          const float w = wx[c0] * wy[c1] * wz[c2];   // exact
+          if (w == 0.0f) continue;
           const int B = bc[c2][c0], Y = cy[c1];
           const int s0 = sidx(C, cx[c0], 0, cz[c2]);
-          double val = 0.0;
+          float val = 0.0f;
           if (Y < B) {
-            const double t = double(Y) / double(B - 1);
-            val = (1.0 - t) * double(C.z[s0]) + t * double(C.z[s0 + C.nx]);
+            const float t = float(Y) * __frcp_rn(float(B - 1));
+            val = (1.0f - t) * C.z[s0] + t * C.z[s0 + C.nx];
           } else if (Y < B + C.band) {
-            val = double(C.z[s0 + C.nx * (Y - B + 2)]);
+            val = C.z[s0 + C.nx * (Y - B + 2)];
           }
-          s += w * val;
+          s = fmaf(w, val, s);
         }
-    F.z[k] = float(double(zf) + s * unscale);
+    F.z[k] = fmaf(s, unscale, zf);
   }
 }
 
@@ -1136,36 +1144,115 @@ __global__ void k_tall_coarse_apply(TInst* I) {
   tv_coarse_apply(I);
 }
 
+// Shared-memory layout of the block levels when they are held on chip: per
+// level first .. nlev - 1 the float z, rhs and diag and the byte label of
+// every sample, the int bases and float a01 of every column, each array
+// 16-byte aligned.  The same walk sizes it on the host and carves it on the
+// device.
+constexpr size_t kVBlockSmemMax = 200 * 1024;
+
+template <class Take>
+__host__ __device__ inline void vblock_carve(TInst& W, int first, Take take) {
+  for (int l = first; l < W.nlev; ++l) {
+    TLevel& V = W.lv[l];
+    V.z = static_cast<float*>(take(4 * size_t(V.n)));
+    V.rhs = static_cast<float*>(take(4 * size_t(V.n)));
+    V.diag = static_cast<float*>(take(4 * size_t(V.n)));
+    V.label = static_cast<uint8_t*>(take(size_t(V.n)));
+    V.bases = static_cast<int*>(take(4 * size_t(V.ncol)));
+    V.a01 = static_cast<float*>(take(4 * size_t(V.ncol)));
+    if (l > first) V.acc = static_cast<unsigned long long*>(take(8 * size_t(V.n)));
+  }
+}
+
+// Copy of `bytes` between 16-byte aligned buffers by the CTA's threads, four
+// 16-byte words in flight per thread.
+__device__ __forceinline__ void cta_copy16(void* dst, const void* src, size_t bytes) {
+  const uint4* s4 = static_cast<const uint4*>(src);
+  uint4* d4 = static_cast<uint4*>(dst);
+  const int n4 = int(bytes / 16), t0 = threadIdx.x, ts = blockDim.x;
+  for (int i = t0; i < n4; i += 4 * ts) {
+    uint4 v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (i + u * ts < n4) v[u] = s4[i + u * ts];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (i + u * ts < n4) d4[i + u * ts] = v[u];
+  }
+  const unsigned char* sb = static_cast<const unsigned char*>(src);
+  unsigned char* db = static_cast<unsigned char*>(dst);
+  for (size_t i = size_t(n4) * 16 + t0; i < bytes; i += ts) db[i] = sb[i];
+}
+
 // The small levels first .. nlev-1 of the V-cycle in one CTA: the same stages
-// as the grid kernels, separated by barriers instead of launches (global
-// memory written before a barrier is visible to the CTA after it).
-__global__ void __launch_bounds__(1024) k_tall_vblock(TInst* I, int first) {
+// as the grid kernels, separated by barriers instead of launches (memory
+// written before a barrier is visible to the CTA after it).  With on_chip
+// the stages run on a shared-memory copy of the instance whose block-level z,
+// rhs, diag, label, bases and a01 and the coarser levels' restriction
+// accumulators live in shared memory (vblock_carve): the operator and the
+// level-first rhs are loaded once, the level-first z is written back at the
+// end; residuals, the tall-row couplings and the coarsest inverse stay in
+// global memory.
+__global__ void __launch_bounds__(1024) k_tall_vblock(TInst* I, int first, int on_chip) {
   if (I->ctrl->done) return;
+  extern __shared__ __align__(16) unsigned char vsm[];
+  __shared__ __align__(16) TInst SI;
   const int t0 = threadIdx.x, ts = blockDim.x, last = I->nlev - 1;
+  TInst* W = I;
+  if (on_chip) {
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(I);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&SI);
+    for (int w = t0; w < int(sizeof(TInst) / 8); w += ts) dst[w] = src[w];
+    __syncthreads();
+    if (t0 == 0) {
+      size_t off = 0;
+      vblock_carve(SI, first, [&](size_t bytes) {
+        void* p = vsm + off;
+        off += (bytes + 15) & ~size_t(15);
+        return p;
+      });
+    }
+    __syncthreads();
+    for (int l = first; l <= last; ++l) {
+      const TLevel& G = I->lv[l];
+      const TLevel& V = SI.lv[l];
+      cta_copy16(V.diag, G.diag, 4 * size_t(V.n));
+      cta_copy16(V.label, G.label, size_t(V.n));
+      cta_copy16(V.bases, G.bases, 4 * size_t(V.ncol));
+      cta_copy16(V.a01, G.a01, 4 * size_t(V.ncol));
+      if (l == first) cta_copy16(V.rhs, G.rhs, 4 * size_t(V.n));
+      else
+        for (int k = t0; k < V.n; k += ts) V.acc[k] = 0ull;   // cleared again by every restrict_finish
+    }
+    __syncthreads();
+    W = &SI;
+  }
   for (int l = first; l < last; ++l) {
-    tv_zero(I, l, t0, ts);
+    tv_zero(W, l, t0, ts);
     __syncthreads();
     for (int c = 0; c < 4; ++c) {
-      tv_smooth<kBlockBandGroup>(I, l, c, t0, ts);
+      tv_smooth<kBlockBandGroup>(W, l, c, t0, ts);
       __syncthreads();
     }
-    tv_residual<1>(I, l, t0, ts);
+    tv_residual<1>(W, l, t0, ts);
     __syncthreads();
-    tv_restrict(I, l, t0, ts);
+    tv_restrict(W, l, t0, ts);
     __syncthreads();
-    tv_restrict_finish(I, l + 1, t0, ts);
+    tv_restrict_finish(W, l + 1, t0, ts);
     __syncthreads();
   }
-  tv_coarse_apply(I);
+  tv_coarse_apply(W);
   __syncthreads();
   for (int l = last - 1; l >= first; --l) {
-    tv_prolong(I, l, t0, ts);
+    tv_prolong(W, l, t0, ts);
     __syncthreads();
     for (int c = 3; c >= 0; --c) {
-      tv_smooth<kBlockBandGroup>(I, l, c, t0, ts);
+      tv_smooth<kBlockBandGroup>(W, l, c, t0, ts);
       __syncthreads();
     }
   }
+  if (on_chip) cta_copy16(I->lv[first].z, SI.lv[first].z, 4 * size_t(SI.lv[first].n));
 }
 
 // ------------------------------------------------------------------ finish
@@ -1279,6 +1366,17 @@ size_t up256(size_t v) { return (v + 255) / 256 * 256; }
 // launch one grid kernel per stage.
 constexpr long long kTallBlockSamples = 8192;
 
+// Dynamic shared memory of the block levels held on chip, 0 if they do not fit.
+size_t vblock_smem_bytes(const TInst& I, int first) {
+  TInst W = I;
+  size_t off = 0;
+  vblock_carve(W, first, [&](size_t bytes) {
+    off += (bytes + 15) & ~size_t(15);
+    return static_cast<void*>(nullptr);
+  });
+  return off <= kVBlockSmemMax ? off : 0;
+}
+
 int tall_first_block(const TallPlan& plan) {
   const int L = int(plan.levels.size());
   for (int l = 1; l < L; ++l)
@@ -1300,7 +1398,8 @@ void launch_vcycle(fluid_pp_tall* T, int first) {
     k_tall_restrict<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
     k_tall_restrict_finish<<<grid_for(I.lv[l + 1].n), kTB, 0, s>>>(T->d_inst, l + 1, 0);
   }
-  k_tall_vblock<<<1, 1024, 0, s>>>(T->d_inst, first);
+  const size_t sm = vblock_smem_bytes(I, first);
+  k_tall_vblock<<<1, 1024, sm, s>>>(T->d_inst, first, sm > 0 ? 1 : 0);
   for (int l = first - 1; l >= 0; --l) {
     const int g = grid_for(I.lv[l].n), gc = grid_for(I.lv[l].ncol), gb = grid_band(I.lv[l]);
     k_tall_prolong<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
@@ -1440,6 +1539,9 @@ int tall_create(const fluid_pp_tall_config* cfg, const int* bases, fluid_pp_tall
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)k_tall_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(kMaxCoarse * kMaxCoarse * sizeof(double)));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_tall_vblock, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(kVBlockSmemMax));
   if (e != cudaSuccess) {
     fpp::set_global_error(std::string("tall setup: ") + cudaGetErrorString(e));
     if (T->d_inst) cudaFree(T->d_inst);
