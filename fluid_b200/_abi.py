@@ -33,6 +33,8 @@ EXPORTS = (
     "fluid_pp_tall_prepare", "fluid_pp_tall_get_rhs", "fluid_pp_tall_get_labels", "fluid_pp_tall_apply_operator",
     "fluid_pp_tall_get_pressure", "fluid_pp_tall_last_error", "fluid_pp_required_bytes",
     "fluid_pp_tall_required_bytes", "fluid_pp_batch_set_graphs",
+    "fluid_pp_set_allocation_cache", "fluid_pp_allocation_cache_bytes",
+    "fluid_pp_tall_project_begin", "fluid_pp_tall_project_continue", "fluid_pp_tall_project_end",
 )
 STAGES = ("reset", "label", "coarsen", "bake", "factor", "init", "smooth0", "smoothc", "residual0", "residualc",
           "restrict0", "restrictc", "coarse", "prolong0", "prolongc", "dot", "dir", "spmv", "update", "true",
@@ -117,6 +119,8 @@ def load():
     L.fluid_pp_batch_set_graphs.argtypes = [vp, ci]
     L.fluid_pp_batch_profile_read.argtypes = [vp, vp, vp, ci]
     L.fluid_pp_apply_operator_noalloc.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp, vp]
+    L.fluid_pp_set_allocation_cache.argtypes = [ci, ctypes.c_ulonglong]
+    L.fluid_pp_allocation_cache_bytes.argtypes = [ci, ctypes.POINTER(ctypes.c_ulonglong)]
     L.fluid_pp_tall_choose_base.argtypes = [ci, ci, ci, ci, ci, ci]
     L.fluid_pp_tall_limit_bases.argtypes = [vp, ci, ci, ci, ci]
     L.fluid_pp_tall_plan.argtypes = [ci, ci, ci, ci, vp, pi, vp]
@@ -127,6 +131,9 @@ def load():
     L.fluid_pp_tall_upload_state.argtypes = [vp, vp, vp, vp, vp]
     L.fluid_pp_tall_upload_state_device.argtypes = [vp, vp, vp, vp, vp]
     L.fluid_pp_tall_project.argtypes = [vp, cf, ctypes.POINTER(SolveOpts), ctypes.POINTER(Receipt)]
+    L.fluid_pp_tall_project_begin.argtypes = [vp, cf, ctypes.POINTER(SolveOpts)]
+    L.fluid_pp_tall_project_continue.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_int)]
+    L.fluid_pp_tall_project_end.argtypes = [vp, ctypes.POINTER(Receipt)]
     L.fluid_pp_tall_download.argtypes = [vp, vp, vp, vp, vp]
     L.fluid_pp_tall_prepare.argtypes = [vp, cf]
     L.fluid_pp_tall_get_rhs.argtypes = [vp, vp]

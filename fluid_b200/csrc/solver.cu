@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "alloc.h"
 #include "../../include/fluid_pp.h"
 #include "fused.cuh"
 #include "plan.h"
@@ -633,21 +634,21 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
   }
   B->smem_factor = size_t(mmax) * mmax * sizeof(double);
 
-  cudaError_t e = cudaMalloc(&B->d_ctrl, sizeof(Ctrl) * count);
+  cudaError_t e = dev_alloc(reinterpret_cast<void**>(&B->d_ctrl), sizeof(Ctrl) * count);
   if (e == cudaSuccess) e = cudaMemset(B->d_ctrl, 0, sizeof(Ctrl) * count);
   for (int k = 0; k < count; ++k) insts[k].ctrl = B->d_ctrl + k;
-  if (e == cudaSuccess) e = cudaMalloc(&B->d_insts, sizeof(InstDev) * count);
+  if (e == cudaSuccess) e = dev_alloc(reinterpret_cast<void**>(&B->d_insts), sizeof(InstDev) * count);
   if (e == cudaSuccess) e = cudaMemcpy(B->d_insts, insts.data(), sizeof(InstDev) * count, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMalloc(&B->d_tiles, sizeof(Tile) * std::max<size_t>(1, tiles.size()));
+  if (e == cudaSuccess) e = dev_alloc(reinterpret_cast<void**>(&B->d_tiles), sizeof(Tile) * std::max<size_t>(1, tiles.size()));
   if (e == cudaSuccess && !tiles.empty())
     e = cudaMemcpy(B->d_tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMalloc(&B->d_ilist, sizeof(int) * std::max<size_t>(1, ilist.size()));
+  if (e == cudaSuccess) e = dev_alloc(reinterpret_cast<void**>(&B->d_ilist), sizeof(int) * std::max<size_t>(1, ilist.size()));
   if (e == cudaSuccess && !ilist.empty())
     e = cudaMemcpy(B->d_ilist, ilist.data(), sizeof(int) * ilist.size(), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMallocHost(&B->h_ctrl, sizeof(Ctrl) * count);
-  if (e == cudaSuccess) e = cudaMalloc(&B->d_loop, sizeof(unsigned));
+  if (e == cudaSuccess) e = host_alloc(reinterpret_cast<void**>(&B->h_ctrl), sizeof(Ctrl) * count);
+  if (e == cudaSuccess) e = dev_alloc(reinterpret_cast<void**>(&B->d_loop), sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMemset(B->d_loop, 0, sizeof(unsigned));
-  if (e == cudaSuccess) e = cudaMallocHost(&B->h_loop, sizeof(unsigned));
+  if (e == cudaSuccess) e = host_alloc(reinterpret_cast<void**>(&B->h_loop), sizeof(unsigned));
   if (e == cudaSuccess) e = configure_kernels();
   if (e != cudaSuccess) {
     err = std::string("batch setup: ") + cudaGetErrorString(e);
@@ -884,7 +885,7 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
   const size_t bytes = arena_size(*cfg, plan);
   const long long nu = (long long)(nx + 1) * ny * nz, nv = (long long)nx * (ny + 1) * nz,
                   nw = (long long)nx * ny * (nz + 1);
-  cudaError_t e = cudaMalloc(&h->arena, bytes);
+  cudaError_t e = dev_alloc(reinterpret_cast<void**>(&h->arena), bytes);
   if (e != cudaSuccess) {
     g_err = std::string("arena allocation: ") + cudaGetErrorString(e);
     return FLUID_PP_OOM;
@@ -992,7 +993,7 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
   int rc = batch_build(&raw, 1, &h->self, err);
   if (rc != FLUID_PP_OK) {
     g_err = err;
-    cudaFree(h->arena);
+    dev_release(h->arena, h->stream);
     return rc;
   }
   *out = h.release();
@@ -1016,7 +1017,7 @@ void fluid_pp_destroy(fluid_pp* pp) {
   if (!pp) return;
   cudaSetDevice(pp->cfg.device);
   if (pp->self) fluid_pp_batch_destroy(pp->self);
-  if (pp->arena) cudaFree(pp->arena);
+  dev_release(pp->arena, pp->stream);
   delete pp;
 }
 
@@ -1218,14 +1219,14 @@ int fluid_pp_batch_create(fluid_pp* const* handles, int count, fluid_pp_batch** 
 void fluid_pp_batch_destroy(fluid_pp_batch* B) {
   if (!B) return;
   cudaSetDevice(B->device);
-  if (B->d_insts) cudaFree(B->d_insts);
-  if (B->d_ctrl) cudaFree(B->d_ctrl);
-  if (B->d_tiles) cudaFree(B->d_tiles);
-  if (B->d_ilist) cudaFree(B->d_ilist);
-  if (B->h_ctrl) cudaFreeHost(B->h_ctrl);
   destroy_graphs(B);
-  if (B->d_loop) cudaFree(B->d_loop);
-  if (B->h_loop) cudaFreeHost(B->h_loop);
+  dev_release(B->d_insts, B->stream);
+  dev_release(B->d_ctrl, B->stream);
+  dev_release(B->d_tiles, B->stream);
+  dev_release(B->d_ilist, B->stream);
+  host_release(B->h_ctrl, B->stream);
+  dev_release(B->d_loop, B->stream);
+  host_release(B->h_loop, B->stream);
   for (cudaEvent_t e : B->ev_pool) cudaEventDestroy(e);
   delete B;
 }

@@ -37,9 +37,11 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
+#include "alloc.h"
 #include "../../include/fluid_pp.h"
 #include "device_util.cuh"
 #include "tall_plan.h"
@@ -1348,6 +1350,9 @@ struct fluid_pp_tall {
   TInst* d_inst = nullptr;
   Ctrl* h_ctrl = nullptr;
   bool has_state = false;
+  bool solving = false;   // between fluid_pp_tall_project_begin and _end
+  bool solved = false;    // the CG loop reported done
+  int it = 0, cap = 0;    // CG iterations launched, iteration cap (+2 slack)
   int set_error(int code, const std::string& m) {
     err = m;
     return code;
@@ -1375,6 +1380,29 @@ size_t vblock_smem_bytes(const TInst& I, int first) {
     return static_cast<void*>(nullptr);
   });
   return off <= kVBlockSmemMax ? off : 0;
+}
+
+// Shared-memory limits of the tall kernels, set once per device: the largest
+// coarsest level any tall grid can have and the block levels held on chip.
+// Setting a kernel's attribute while another thread launches that kernel is a
+// race, so later handle creations (which may run beside other handles'
+// solves) never touch them again.
+std::mutex g_tall_cfg_mutex;
+bool g_tall_cfg_done[64] = {};
+
+cudaError_t configure_tall_kernels() {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(g_tall_cfg_mutex);
+  if (dev >= 0 && dev < 64 && g_tall_cfg_done[dev]) return cudaSuccess;
+  e = cudaFuncSetAttribute((const void*)k_tall_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           int(kMaxCoarse * kMaxCoarse * sizeof(double)));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_tall_vblock, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(kVBlockSmemMax));
+  if (e == cudaSuccess && dev >= 0 && dev < 64) g_tall_cfg_done[dev] = true;
+  return e;
 }
 
 int tall_first_block(const TallPlan& plan) {
@@ -1475,7 +1503,7 @@ int tall_create(const fluid_pp_tall_config* cfg, const int* bases, fluid_pp_tall
   const size_t bytes = tall_arena_size(plan);
   const size_t n0 = size_t(plan.levels[0].samples());
   const size_t m = size_t(plan.levels[L - 1].samples());
-  if (cudaMalloc(&T->arena, bytes) != cudaSuccess) {
+  if (dev_alloc(reinterpret_cast<void**>(&T->arena), bytes) != cudaSuccess) {
     fpp::set_global_error("tall arena allocation failed");
     return FLUID_PP_OOM;
   }
@@ -1533,20 +1561,14 @@ int tall_create(const fluid_pp_tall_config* cfg, const int* bases, fluid_pp_tall
   I.coarse_m = int(m);
   I.ctrl = static_cast<Ctrl*>(take(sizeof(Ctrl)));
   I.err = static_cast<int*>(take(sizeof(int)));
-  cudaError_t e = cudaMalloc(&T->d_inst, sizeof(TInst));
-  if (e == cudaSuccess) e = cudaMallocHost(&T->h_ctrl, sizeof(Ctrl));
-  // the largest coarsest level any tall grid can have (the limit is process-wide and never lowered)
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute((const void*)k_tall_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(kMaxCoarse * kMaxCoarse * sizeof(double)));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute((const void*)k_tall_vblock, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(kVBlockSmemMax));
+  cudaError_t e = dev_alloc(reinterpret_cast<void**>(&T->d_inst), sizeof(TInst));
+  if (e == cudaSuccess) e = host_alloc(reinterpret_cast<void**>(&T->h_ctrl), sizeof(Ctrl));
+  if (e == cudaSuccess) e = configure_tall_kernels();
   if (e != cudaSuccess) {
     fpp::set_global_error(std::string("tall setup: ") + cudaGetErrorString(e));
-    if (T->d_inst) cudaFree(T->d_inst);
-    if (T->h_ctrl) cudaFreeHost(T->h_ctrl);
-    cudaFree(T->arena);
+    dev_release(T->d_inst, T->stream);
+    host_release(T->h_ctrl, T->stream);
+    dev_release(T->arena, T->stream);
     return FLUID_PP_OOM;
   }
   cudaMemcpy(T->d_inst, &I, sizeof(TInst), cudaMemcpyHostToDevice);
@@ -1594,9 +1616,9 @@ int fluid_pp_tall_create(const fluid_pp_tall_config* config, const int* bases, f
 void fluid_pp_tall_destroy(fluid_pp_tall* T) {
   if (!T) return;
   cudaSetDevice(T->cfg.device);
-  if (T->d_inst) cudaFree(T->d_inst);
-  if (T->h_ctrl) cudaFreeHost(T->h_ctrl);
-  if (T->arena) cudaFree(T->arena);
+  dev_release(T->d_inst, T->stream);
+  host_release(T->h_ctrl, T->stream);
+  dev_release(T->arena, T->stream);
   delete T;
 }
 
@@ -1638,7 +1660,7 @@ static void tall_set_dt(fluid_pp_tall* T, float dt) {
                   cudaMemcpyHostToDevice, T->stream);
 }
 
-int fluid_pp_tall_project(fluid_pp_tall* T, float dt, const fluid_pp_solve_opts* opts, fluid_pp_receipt* receipt) {
+int fluid_pp_tall_project_begin(fluid_pp_tall* T, float dt, const fluid_pp_solve_opts* opts) {
   if (!T) return FLUID_PP_INVALID_ARG;
   if (!(dt > 0) || !std::isfinite(dt)) return T->set_error(FLUID_PP_INVALID_ARG, "dt must be positive and finite");
   if (!T->has_state) return T->set_error(FLUID_PP_INVALID_ARG, "state not uploaded");
@@ -1655,9 +1677,23 @@ int fluid_pp_tall_project(fluid_pp_tall* T, float dt, const fluid_pp_solve_opts*
   k_tall_receipt<<<g0, kTB, 0, s>>>(T->d_inst, 0);
   k_tall_cg_init<<<g0, kTB, 0, s>>>(T->d_inst, o.rel_tol, o.abs_tol, o.max_iters, o.true_residual_every,
                                     o.rel_tol_inf);
-  const int cap = o.max_iters + 2;
-  for (int it = 0; it < cap;) {
-    const int burst = std::min(4, cap - it);
+  T->solving = true;
+  T->solved = false;
+  T->it = 0;
+  T->cap = o.max_iters + 2;
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_tall_project_continue(fluid_pp_tall* T, int max_iterations, int* finished) {
+  if (!T || !finished) return FLUID_PP_INVALID_ARG;
+  if (!T->solving) return T->set_error(FLUID_PP_INVALID_ARG, "no projection begun");
+  cudaSetDevice(T->cfg.device);
+  cudaStream_t s = T->stream;
+  TInst& I = T->inst;
+  const int g0 = grid_for(I.lv[0].n);
+  int budget = max_iterations > 0 ? max_iterations : T->cap;
+  while (!T->solved && T->it < T->cap && budget > 0) {
+    const int burst = std::min({4, T->cap - T->it, budget});
     for (int k = 0; k < burst; ++k) {
       if (I.nlev > 1) {
         launch_vcycle(T, tall_first_block(T->plan));
@@ -1670,13 +1706,29 @@ int fluid_pp_tall_project(fluid_pp_tall* T, float dt, const fluid_pp_solve_opts*
       k_tall_update<<<g0, kTB, 0, s>>>(T->d_inst);
       k_tall_true<<<g0, kTB, 0, s>>>(T->d_inst);
     }
-    it += burst;
+    T->it += burst;
+    budget -= burst;
     cudaMemcpyAsync(T->h_ctrl, I.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return T->set_error(FLUID_PP_CUDA, std::string("tall solve: ") + cudaGetErrorString(e));
-    if (T->h_ctrl->done) break;
+    if (e != cudaSuccess) {
+      T->solving = false;
+      return T->set_error(FLUID_PP_CUDA, std::string("tall solve: ") + cudaGetErrorString(e));
+    }
+    if (T->h_ctrl->done) T->solved = true;
   }
+  *finished = (T->solved || T->it >= T->cap) ? 1 : 0;
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_tall_project_end(fluid_pp_tall* T, fluid_pp_receipt* receipt) {
+  if (!T) return FLUID_PP_INVALID_ARG;
+  if (!T->solving) return T->set_error(FLUID_PP_INVALID_ARG, "no projection begun");
+  T->solving = false;
+  cudaSetDevice(T->cfg.device);
+  cudaStream_t s = T->stream;
+  TInst& I = T->inst;
+  const int g0 = grid_for(I.lv[0].n);
   k_tall_grad<<<g0, kTB, 0, s>>>(T->d_inst);
   k_tall_receipt<<<g0, kTB, 0, s>>>(T->d_inst, 1);
   cudaMemcpyAsync(T->h_ctrl, I.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s);
@@ -1704,6 +1756,15 @@ int fluid_pp_tall_project(fluid_pp_tall* T, float dt, const fluid_pp_solve_opts*
   if (status == FLUID_PP_UNSUPPORTED)
     T->err = "a tall row has more neighbour entries than its ELL width (column bases differ too much)";
   return status;
+}
+
+int fluid_pp_tall_project(fluid_pp_tall* T, float dt, const fluid_pp_solve_opts* opts, fluid_pp_receipt* receipt) {
+  int rc = fluid_pp_tall_project_begin(T, dt, opts);
+  if (rc != FLUID_PP_OK) return rc;
+  int finished = 0;
+  rc = fluid_pp_tall_project_continue(T, 0, &finished);
+  if (rc != FLUID_PP_OK) return rc;
+  return fluid_pp_tall_project_end(T, receipt);
 }
 
 int fluid_pp_tall_download(fluid_pp_tall* T, float* p, float* u, float* v, float* w) {

@@ -3,16 +3,24 @@
 Stands where the reference's per-simulation advance loop stands
 (``GPUSolverInstance.advanceTo``, lib/core/method-contract.ts:355, driven per
 simulation from the render worker): every admitted simulation keeps its
-state, hierarchy and CG workspace resident on the device, and each server tick
-runs one projection step of every resident simulation.  The uniform ones run
-as one batched solve (one launch per kernel stage across all of them,
-``fluid_pp_batch_project``); the tall-cell ones run in a second host thread on
-their own stream, so both kinds of work overlap on the device.
+state, hierarchy and CG workspace resident on the device and advances one
+projection step after another.
 
-Admission is FIFO by an HBM budget (``fluid_pp_required_bytes`` /
-``fluid_pp_tall_required_bytes`` plus the resident state) and a slot limit: a
-request that arrives while others are on the GPU joins at the next tick once
-memory and a slot are free, and leaves the batch when its steps are done.
+One host thread drives the device and interleaves two kinds of work: a
+batched step of every resident uniform simulation (one launch per kernel
+stage across all of them, ``fluid_pp_batch_project``), then a slice of at
+most ``tall_slice_iterations`` CG iterations of the current tall-cell solve
+(``fluid_pp_tall_project_begin/continue/end``; the tall-cell simulations take
+their steps in round-robin order), or, in a round that admits a request, the
+admission instead; then the next batched uniform step, and so on.  A uniform
+step therefore waits for at most one slice or one admission, however many
+tall-cell simulations are resident, and every resident simulation keeps
+advancing.  Between steps, finished
+simulations leave (their device blocks go to the library's allocation cache,
+``fluid_pp_set_allocation_cache``, since cudaFree of a large arena can take
+longer than many steps) and queued requests are admitted FIFO by an HBM budget
+(``fluid_pp_required_bytes`` / ``fluid_pp_tall_required_bytes`` plus the
+resident state) and a slot limit, at most ``admit_per_step`` at a time.
 
 Step latency is wall time from the moment a step is ready (the simulation's
 previous step finished, or its admission) to the moment its projection has
@@ -24,7 +32,6 @@ import ctypes
 import math
 import statistics
 import time
-from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -70,7 +77,7 @@ def required_bytes(req: Request, precision: str) -> int:
 
 
 class _Sim:
-    def __init__(self, req: Request, precision: str, device: int, stream, torch):
+    def __init__(self, req: Request, precision: str, device: int, stream, copy_stream, torch):
         self.req = req
         self.kind = req.kind
         s = req.states[0]
@@ -79,11 +86,13 @@ class _Sim:
         else:
             self.h = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho, "fp32", device)
         self.h.set_stream(stream.cuda_stream)
-        with torch.cuda.stream(stream):
+        with torch.cuda.stream(copy_stream):
             self.dev = [tuple(torch.from_numpy(np.ascontiguousarray(a)).to(f"cuda:{device}", non_blocking=False)
                               for a in (st.vof, st.u, st.v, st.w)) for st in req.states]
+        copy_stream.synchronize()   # the states are complete before another stream reads them
         self.step = 0
         self.ready = 0.0
+        self.bytes = 0
         self.latencies: list[float] = []
         self.receipts: list[dict] = []
         self.pressures: list[np.ndarray] = []
@@ -102,11 +111,13 @@ class _Sim:
 
 
 class Server:
-    """Admits requests by HBM budget and runs one projection step of every resident
-    simulation per tick (continuous batching)."""
+    """Admits requests by HBM budget and advances every resident simulation,
+    interleaving batched uniform steps with single tall-cell steps (continuous
+    batching)."""
 
     def __init__(self, budget_bytes: float = 150e9, max_slots: int = 48, precision: str = "fp16", device: int = 0,
-                 rel_tol: float = 1e-6, record: bool = False, admit_per_tick: int = 2):
+                 rel_tol: float = 1e-6, record: bool = False, admit_per_step: int = 1,
+                 cache_bytes: float = 16e9, tall_slice_iterations: int = 8):
         import torch
         self.torch = torch
         self.budget = float(budget_bytes)
@@ -115,118 +126,123 @@ class Server:
         self.device = int(device)
         self.rel_tol = float(rel_tol)
         self.record = record
+        self.admit_per_step = int(admit_per_step)
         torch.cuda.set_device(self.device)
-        # uniform steps on a high-priority stream, tall-cell steps on low-priority ones
-        lo, hi = torch.cuda.Stream.priority_range()
-        self.prio_low, self.prio_high = lo, hi
-        self.s_uniform = torch.cuda.Stream(device=self.device, priority=hi)
-        self.admit_per_tick = int(admit_per_tick)
-        self.pool = ThreadPoolExecutor(max_workers=self.max_slots)
+        self.stream = torch.cuda.Stream(device=self.device)
+        # handles come and go every few steps: keep their blocks for reuse
+        # instead of cudaFree / cudaFreeHost, which take up to ~1 s for large arenas
+        self.L = load()
+        self.cache_bytes = int(cache_bytes)
+        self.L.fluid_pp_set_allocation_cache(self.device, ctypes.c_ulonglong(self.cache_bytes))
+        self.L.fluid_pp_set_allocation_cache(-1, ctypes.c_ulonglong(min(self.cache_bytes, 256 << 20)))
         self.pending: list[tuple[Request, int]] = []
         self.active: list[_Sim] = []
         self.done: list[_Sim] = []
         self.used = 0.0
         self.peak_used = 0.0
-        self._batch = None
-        self._batch_key = None
         self.batch_sizes: list[int] = []
-        self.ticks = 0
+        self.uniform_steps = 0
+        self.tall_steps = 0
+        self._batch = None
+        self._members: list[_Sim] = []
+        self._next_tall = 0
+        self._tall_cur = None            # the tall-cell simulation whose solve is in progress
+        self.tall_slice = int(tall_slice_iterations)
 
-    # -- admission ----------------------------------------------------------------
+    # -- admission and retirement (between steps) ----------------------------------
     def submit(self, req: Request):
         self.pending.append((req, required_bytes(req, self.precision)))
 
-    def _admit(self, now: float):
-        """At most admit_per_tick creations per tick: a handle's creation and first
-        upload delay every resident simulation's next step."""
+    def _admit(self, now: float) -> int:
         admitted = 0
-        while self.pending and len(self.active) < self.max_slots and admitted < self.admit_per_tick:
+        while self.pending and len(self.active) < self.max_slots and admitted < self.admit_per_step:
             req, need = self.pending[0]
             if self.used + need > self.budget:
                 if not self.active and need > self.budget:
                     raise MemoryError(f"request {req.rid} needs {need} bytes, over the whole budget")
                 break
             self.pending.pop(0)
-            # uniform simulations share the batch's stream; each tall one gets its own
-            stream = (self.s_uniform if req.kind == "uniform"
-                      else self.torch.cuda.Stream(device=self.device, priority=self.prio_low))
-            sim = _Sim(req, self.precision, self.device, stream, self.torch)
+            sim = _Sim(req, self.precision, self.device, self.stream, self.stream, self.torch)
             sim.bytes = need
             sim.ready = now
             self.used += need
             self.peak_used = max(self.peak_used, self.used)
             self.active.append(sim)
             admitted += 1
+        return admitted
 
-    # -- one tick -------------------------------------------------------------------
-    def _uniform_batch(self, sims):
-        key = tuple(id(s.h) for s in sims)
-        if key != self._batch_key:
+    def _retire(self):
+        leaving = [s for s in self.active if s.step >= s.req.steps]
+        if not leaving:
+            return
+        if self._batch is not None and any(s in self._members for s in leaving):
+            self._batch.destroy()
+            self._batch, self._members = None, []
+        for s in leaving:
+            self.active.remove(s)
+            self.used -= s.bytes
+            s.destroy()
+            self.done.append(s)
+
+    def _record(self, sim: _Sim, receipt: dict, t: float):
+        sim.receipts.append(receipt)
+        sim.latencies.append(t - sim.ready)
+        if self.record:
+            sim.pressures.append(sim.h.pressure_cells() if sim.kind == "uniform" else sim.h.pressure())
+        sim.ready = t
+        sim.step += 1
+
+    # -- steps ----------------------------------------------------------------------
+    def _uniform_step(self, members: list[_Sim], clock):
+        if [id(s) for s in members] != [id(s) for s in self._members]:
             if self._batch is not None:
                 self._batch.destroy()
-            self._batch = BatchProjector([s.h for s in sims]) if sims else None
-            if self._batch is not None:
-                self._batch.set_graphs(False)   # lives for a few ticks: direct launches beat a new capture
-            self._batch_key = key
-        return self._batch
-
-    def tick(self, clock):
-        uni = [s for s in self.active if s.kind == "uniform"]
-        tall = [s for s in self.active if s.kind == "tall"]
-        finished: dict[int, float] = {}
-        errors: list[BaseException] = []
-
-        def run_uniform():
-            try:
-                if not uni:
-                    return
-                for s in uni:
-                    s.upload()
-                recs = self._uniform_batch(uni).project([s.dt for s in uni], rel_tol=self.rel_tol)
-                t = clock()
-                for s, r in zip(uni, recs):
-                    s.receipts.append(r)
-                    finished[id(s)] = t
-                self.batch_sizes.append(len(uni))
-            except BaseException as e:   # surfaced after join
-                errors.append(e)
-
-        def run_tall(s):
+            self._batch = BatchProjector([s.h for s in members])
+            self._batch.set_graphs(False)   # membership changes every few steps: direct launches
+            self._members = list(members)
+        for s in members:
             s.upload()
-            r = s.h.project(s.dt, rel_tol=self.rel_tol)
-            s.receipts.append(r)
-            finished[id(s)] = clock()
+        recs = self._batch.project([s.dt for s in members], rel_tol=self.rel_tol)
+        t = clock()
+        for s, r in zip(members, recs):
+            self._record(s, r, t)
+        self.batch_sizes.append(len(members))
+        self.uniform_steps += 1
 
-        futures = [self.pool.submit(run_tall, s) for s in tall]
-        run_uniform()
-        for f in futures:
-            try:
-                f.result()
-            except BaseException as e:
-                errors.append(e)
-        if errors:
-            raise errors[0]
-        self.ticks += 1
-        for s in list(self.active):
-            t = finished[id(s)]
-            s.latencies.append(t - s.ready)
-            if self.record:
-                s.pressures.append(s.h.pressure_cells() if s.kind == "uniform" else s.h.pressure())
-            s.ready = t
-            s.step += 1
-            if s.step >= s.req.steps:
-                self.active.remove(s)
-                self.used -= s.bytes
-                s.destroy()
-                self.done.append(s)
-        if not any(s.kind == "uniform" for s in self.active) and self._batch is not None:
-            self._batch.destroy()
-            self._batch, self._batch_key = None, None
+    def _tall_slice(self, clock):
+        """At most tall_slice iterations of the current tall-cell solve; a new
+        solve (upload, assembly, CG start) begins with the next simulation in
+        round-robin order when none is in progress."""
+        sim = self._tall_cur
+        if sim is None:
+            tall = [s for s in self.active if s.kind == "tall"]
+            self._next_tall %= len(tall)
+            sim = tall[self._next_tall]
+            self._next_tall += 1
+            sim.upload()
+            sim.h.project_begin(sim.dt, rel_tol=self.rel_tol)
+            self._tall_cur = sim
+        if sim.h.project_continue(self.tall_slice):
+            r = sim.h.project_end()
+            self._record(sim, r, clock())
+            self.tall_steps += 1
+            self._tall_cur = None
+
+    def _round(self, clock, admitted: bool):
+        """One batched uniform step (if any uniform simulation is resident), then
+        one slice of a tall-cell solve unless this round admitted a request: an
+        admission takes the slice's place between two uniform steps instead of
+        adding to the gap."""
+        uni = [s for s in self.active if s.kind == "uniform"]
+        if uni:
+            self._uniform_step(uni, clock)
+        if any(s.kind == "tall" for s in self.active) and not (admitted and uni):
+            self._tall_slice(clock)
 
     # -- the loop -------------------------------------------------------------------
     def run(self, requests: list[Request], duration_s: float | None = None) -> dict:
-        """Feeds requests at their arrival times (wall clock) and ticks until every
-        request finished, or until duration_s (then the run stops after the tick)."""
+        """Feeds requests at their arrival times (wall clock) and runs rounds until
+        every request finished, or until duration_s (then the run stops after the round)."""
         queue = sorted(requests, key=lambda r: r.arrival)
         t0 = time.perf_counter()
         clock = lambda: time.perf_counter() - t0
@@ -236,27 +252,34 @@ class Server:
             while i < len(queue) and queue[i].arrival <= now:
                 self.submit(queue[i])
                 i += 1
-            self._admit(now)
+            admitted = self._admit(now)
             if self.active:
-                self.tick(clock)
+                self._round(clock, admitted > 0)
+                self._retire()
             elif i < len(queue):
                 time.sleep(max(0.0, min(0.005, queue[i].arrival - clock())))
             elif not self.pending:
                 break
             if duration_s is not None and clock() >= duration_s:
                 break
+        if self._batch is not None:
+            self._batch.destroy()
+            self._batch, self._members = None, []
         elapsed = clock()
         sims = self.done + self.active
         lat = [x for s in sims for x in s.latencies]
         big = [x for s in sims if s.req.cells >= 1_200_000 for x in s.latencies]
+        big_u = [x for s in sims if s.kind == "uniform" and s.req.cells >= 1_200_000 for x in s.latencies]
+        pct = lambda xs, q: 1000 * float(np.percentile(xs, q)) if xs else None
         out = {
             "elapsed_s": elapsed, "requests_submitted": i, "requests_finished": len(self.done),
             "requests_resident_at_end": len(self.active), "requests_waiting_at_end": len(self.pending),
             "step_solves": len(lat), "solves_per_s": len(lat) / elapsed if elapsed > 0 else 0.0,
-            "p50_step_ms": 1000 * statistics.median(lat) if lat else None,
-            "p99_step_ms": 1000 * float(np.percentile(lat, 99)) if lat else None,
-            "p99_step_ms_ge_1p2M_cells": 1000 * float(np.percentile(big, 99)) if big else None,
-            "steps_ge_1p2M_cells": len(big), "ticks": self.ticks,
+            "p50_step_ms": pct(lat, 50), "p99_step_ms": pct(lat, 99),
+            "p50_step_ms_ge_1p2M_cells": pct(big, 50), "p99_step_ms_ge_1p2M_cells": pct(big, 99),
+            "steps_ge_1p2M_cells": len(big),
+            "p99_uniform_step_ms_ge_1p2M_cells": pct(big_u, 99),
+            "uniform_batched_steps": self.uniform_steps, "tall_steps": self.tall_steps,
             "mean_uniform_batch": statistics.mean(self.batch_sizes) if self.batch_sizes else 0.0,
             "peak_resident_bytes": self.peak_used,
             "failed_steps": sum(1 for s in sims for r in s.receipts if r["status_name"] != "OK"),
@@ -264,13 +287,15 @@ class Server:
         return out
 
     def shutdown(self):
-        self.pool.shutdown(wait=True)
+        """Destroys the resident simulations and frees the allocation cache."""
+        if self._batch is not None:
+            self._batch.destroy()
+            self._batch, self._members = None, []
         for s in self.active:
             s.destroy()
         self.active = []
-        if self._batch is not None:
-            self._batch.destroy()
-            self._batch = None
+        self.L.fluid_pp_set_allocation_cache(self.device, ctypes.c_ulonglong(0))
+        self.L.fluid_pp_set_allocation_cache(-1, ctypes.c_ulonglong(0))
 
 
 def serving_requests(rate: float = 40.0, duration_s: float = 120.0, seed: int = 5, templates: int = 6,

@@ -126,6 +126,25 @@ class TallProjector:
             _check(rc, self._h, "project")
         return r.as_dict()
 
+    # -- the same projection in slices (a server interleaves other steps between them)
+    def project_begin(self, dt: float, **opts):
+        o = solve_opts(**opts)
+        _check(load().fluid_pp_tall_project_begin(self._h, float(dt), ctypes.byref(o)), self._h, "project_begin")
+
+    def project_continue(self, max_iterations: int) -> bool:
+        """Runs at most max_iterations more CG iterations; True once the solve is finished."""
+        done = ctypes.c_int()
+        _check(load().fluid_pp_tall_project_continue(self._h, int(max_iterations), ctypes.byref(done)), self._h,
+               "project_continue")
+        return bool(done.value)
+
+    def project_end(self) -> dict:
+        r = Receipt()
+        rc = load().fluid_pp_tall_project_end(self._h, ctypes.byref(r))
+        if rc not in (_abi.OK, _abi.NONCONVERGENCE, _abi.NONFINITE, _abi.UNSUPPORTED):
+            _check(rc, self._h, "project_end")
+        return r.as_dict()
+
     def download(self):
         out = [np.empty(self.shape, np.float32) for _ in range(4)]
         _check(load().fluid_pp_tall_download(self._h, *(ptr(a) for a in out)), self._h, "download")

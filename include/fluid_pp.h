@@ -206,6 +206,20 @@ int fluid_pp_batch_profile_read(fluid_pp_batch* batch, double* ms, long long* la
 int fluid_pp_apply_operator_noalloc(int nx, int ny, int nz, const unsigned char* label, const float* diag,
                                     const float* p, float* out, double* p_dot_ap, void* stream);
 
+/* Allocation cache for servers that create and destroy handles continuously
+ * (no reference counterpart: the reference allocates one GPU solver per
+ * simulation, lib/core/method-contract.ts:355).  cudaFree waits for the whole
+ * device; with the cache on, destroying a handle or batch waits only for its
+ * own stream and keeps its device blocks (and pinned control blocks, device
+ * -1) on a free list of at most max_cached_bytes, from which later handles of
+ * similar sizes are carved without any CUDA allocation call.  0 (the default)
+ * turns caching off and frees the list.  Cached bytes stay allocated on the
+ * device until trimmed this way.  With the cache on, the work of a handle or
+ * batch must have been issued on its own stream (fluid_pp_set_stream, the
+ * batch's first handle's stream) or have finished before it is destroyed. */
+int fluid_pp_set_allocation_cache(int device, unsigned long long max_cached_bytes);
+int fluid_pp_allocation_cache_bytes(int device, unsigned long long* cached_bytes);
+
 /* ------------------------------------------------------------------------
  * Restricted tall-cell grid (lib/core/tall-cell-grid.ts).  An nx x nz grid of
  * columns over fine_ny world rows: each column has one tall cell over rows
@@ -254,6 +268,16 @@ int fluid_pp_tall_upload_state_device(fluid_pp_tall* tall, const float* vof, con
 /* Labels, assembly, MGPCG to the tolerance, gradient subtract on the packed
  * faces, receipt (divergence receipts over liquid band cells). */
 int fluid_pp_tall_project(fluid_pp_tall* tall, float dt, const fluid_pp_solve_opts* opts, fluid_pp_receipt* receipt);
+/* The same projection in slices (no reference counterpart: a serving loop
+ * interleaves other simulations' steps between the slices of a long solve).
+ * begin enqueues labels, assembly, right-hand side and the CG start on the
+ * handle's stream; continue runs at most max_iterations more CG iterations
+ * (<= 0: until done) and sets *finished once the solve converged or hit its
+ * iteration cap; end enqueues the gradient subtract, synchronises and fills
+ * the receipt.  fluid_pp_tall_project is begin + continue(0) + end. */
+int fluid_pp_tall_project_begin(fluid_pp_tall* tall, float dt, const fluid_pp_solve_opts* opts);
+int fluid_pp_tall_project_continue(fluid_pp_tall* tall, int max_iterations, int* finished);
+int fluid_pp_tall_project_end(fluid_pp_tall* tall, fluid_pp_receipt* receipt);
 /* Pressure in Pa and the projected faces, packed. */
 int fluid_pp_tall_download(fluid_pp_tall* tall, float* p, float* u, float* v, float* w);
 /* Diagnostics for parity tests: prepare runs labels, hierarchy and assembly

@@ -73,3 +73,23 @@ def test_tall_full_size_waves_converge():
     assert rec["true_rel_residual"] <= REL_RES
     assert rec["levels"] == 7
     assert rec["max_div_after"] <= 1e-4 * rec["max_div_before"], rec
+
+
+def test_tall_sliced_projection_matches_one_call():
+    """begin + continue in slices of 3 iterations + end gives the one-call result bit for bit."""
+    s = configs.tall_waves(20, 20, 96, 24, seed=2, mean=50, amp_max=4, lam=(8, 32))
+    a = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho)
+    a.upload_state(s.vof, s.u, s.v, s.w)
+    ra = a.project(s.dt, rel_tol=1e-6)
+    b = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho)
+    b.upload_state(s.vof, s.u, s.v, s.w)
+    b.project_begin(s.dt, rel_tol=1e-6)
+    slices = 1
+    while not b.project_continue(3):
+        slices += 1
+    rb = b.project_end()
+    assert slices >= 2
+    assert ra["iterations"] == rb["iterations"] and rb["status_name"] == "OK"
+    np.testing.assert_array_equal(a.pressure(), b.pressure())
+    a.destroy()
+    b.destroy()
