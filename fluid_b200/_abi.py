@@ -33,7 +33,7 @@ EXPORTS = (
     "fluid_pp_tall_prepare", "fluid_pp_tall_get_rhs", "fluid_pp_tall_get_labels", "fluid_pp_tall_apply_operator",
     "fluid_pp_tall_get_pressure", "fluid_pp_tall_last_error", "fluid_pp_required_bytes",
     "fluid_pp_tall_required_bytes", "fluid_pp_batch_set_graphs",
-    "fluid_pp_set_allocation_cache", "fluid_pp_allocation_cache_bytes",
+    "fluid_pp_set_allocation_cache", "fluid_pp_allocation_cache_bytes", "fluid_pp_reserve_allocation",
     "fluid_pp_tall_project_begin", "fluid_pp_tall_project_continue", "fluid_pp_tall_project_end",
 )
 STAGES = ("reset", "label", "coarsen", "bake", "factor", "init", "smooth0", "smoothc", "residual0", "residualc",
@@ -121,6 +121,7 @@ def load():
     L.fluid_pp_apply_operator_noalloc.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp, vp]
     L.fluid_pp_set_allocation_cache.argtypes = [ci, ctypes.c_ulonglong]
     L.fluid_pp_allocation_cache_bytes.argtypes = [ci, ctypes.POINTER(ctypes.c_ulonglong)]
+    L.fluid_pp_reserve_allocation.argtypes = [ci, ctypes.c_ulonglong]
     L.fluid_pp_tall_choose_base.argtypes = [ci, ci, ci, ci, ci, ci]
     L.fluid_pp_tall_limit_bases.argtypes = [vp, ci, ci, ci, ci]
     L.fluid_pp_tall_plan.argtypes = [ci, ci, ci, ci, vp, pi, vp]

@@ -1,6 +1,15 @@
 // Caching allocator for handle arenas, batch tables and pinned control blocks.
+//
+// Two tiers per device, both used only while caching is on for the device:
+//  * slabs reserved up front (fluid_pp_reserve_allocation): device memory
+//    handed out by best fit over free address ranges that coalesce on release,
+//    so an admission never maps new memory;
+//  * a free list of whole blocks from earlier cudaMalloc calls, reused for
+//    requests of a similar size (at most a quarter larger).
+// Anything else is a plain cudaMalloc / cudaFree.
 #include "alloc.h"
 
+#include <iterator>
 #include <map>
 #include <mutex>
 #include <string>
@@ -15,17 +24,23 @@ void set_global_error(const std::string& message);
 
 namespace {
 
-constexpr int kHostKey = -1;   // cache key of pinned host memory
+constexpr int kHostKey = -1;     // cache key of pinned host memory
+constexpr size_t kAlign = 256;   // slab ranges keep cudaMalloc's alignment
 
 struct Cache {
-  size_t limit = 0;     // bytes the free list may hold (0: caching off)
-  size_t cached = 0;    // bytes on the free list
-  std::multimap<size_t, void*> blocks;   // free blocks by size
+  size_t limit = 0;     // bytes the block free list may hold (0: caching off)
+  size_t cached = 0;    // bytes on the block free list
+  std::multimap<size_t, void*> blocks;   // free whole blocks by size
+  // slab tier
+  std::vector<std::pair<char*, size_t>> slabs;
+  std::map<char*, size_t> free_by_addr;        // free ranges by start
+  std::multimap<size_t, char*> free_by_size;   // the same ranges by size
 };
 
 struct Live {
   int key;
   size_t bytes;
+  bool slab;
 };
 
 std::mutex g_mu;
@@ -53,7 +68,48 @@ cudaError_t raw_alloc(int key, void** p, size_t bytes) {
   return key == kHostKey ? cudaMallocHost(p, bytes) : cudaMalloc(p, bytes);
 }
 
-// Frees the free list of `key` down to `keep` bytes (caller holds no lock).
+// Slab ranges (caller holds g_mu).
+void slab_insert(Cache& c, char* p, size_t n) {
+  c.free_by_addr[p] = n;
+  c.free_by_size.emplace(n, p);
+}
+void slab_erase(Cache& c, std::map<char*, size_t>::iterator it) {
+  auto range = c.free_by_size.equal_range(it->second);
+  for (auto s = range.first; s != range.second; ++s)
+    if (s->second == it->first) {
+      c.free_by_size.erase(s);
+      break;
+    }
+  c.free_by_addr.erase(it);
+}
+char* slab_take(Cache& c, size_t n) {
+  auto it = c.free_by_size.lower_bound(n);
+  if (it == c.free_by_size.end()) return nullptr;
+  char* p = it->second;
+  const size_t have = it->first;
+  slab_erase(c, c.free_by_addr.find(p));
+  if (have > n) slab_insert(c, p + n, have - n);
+  return p;
+}
+void slab_give(Cache& c, char* p, size_t n) {
+  auto next = c.free_by_addr.lower_bound(p);
+  if (next != c.free_by_addr.end() && p + n == next->first) {   // merge with the range after
+    n += next->second;
+    slab_erase(c, next);
+  }
+  auto prev = c.free_by_addr.lower_bound(p);
+  if (prev != c.free_by_addr.begin()) {
+    --prev;
+    if (prev->first + prev->second == p) {   // merge with the range before
+      p = prev->first;
+      n += prev->second;
+      slab_erase(c, prev);
+    }
+  }
+  slab_insert(c, p, n);
+}
+
+// Frees the block free list of `key` down to `keep` bytes (caller holds no lock).
 void trim(int key, size_t keep) {
   std::vector<void*> out;
   {
@@ -74,10 +130,18 @@ cudaError_t alloc_key(int key, void** p, size_t bytes) {
   {
     std::lock_guard<std::mutex> g(g_mu);
     Cache& c = g_cache[key];
+    if (c.limit > 0 && !c.free_by_size.empty()) {
+      const size_t n = bytes ? (bytes + kAlign - 1) / kAlign * kAlign : kAlign;
+      if (char* s = slab_take(c, n)) {
+        *p = s;
+        g_live[*p] = Live{key, n, true};
+        return cudaSuccess;
+      }
+    }
     auto it = c.blocks.lower_bound(bs);
     if (it != c.blocks.end() && it->first <= bs + bs / 4) {
       *p = it->second;
-      g_live[*p] = Live{key, it->first};
+      g_live[*p] = Live{key, it->first, false};
       c.cached -= it->first;
       c.blocks.erase(it);
       return cudaSuccess;
@@ -94,7 +158,7 @@ cudaError_t alloc_key(int key, void** p, size_t bytes) {
     return e;
   }
   std::lock_guard<std::mutex> g(g_mu);
-  g_live[*p] = Live{key, bs};
+  g_live[*p] = Live{key, bs, false};
   return cudaSuccess;
 }
 
@@ -109,7 +173,7 @@ void release_key(void* p, cudaStream_t last_use) {
     info = it->second;
     g_live.erase(it);
     const Cache& c = g_cache[info.key];
-    keep = c.cached + info.bytes <= c.limit;
+    keep = info.slab || c.cached + info.bytes <= c.limit;
   }
   if (!keep) {
     raw_free(info.key, p);
@@ -118,8 +182,12 @@ void release_key(void* p, cudaStream_t last_use) {
   cudaStreamSynchronize(last_use);   // the block's last work has finished before anyone reuses it
   std::lock_guard<std::mutex> g(g_mu);
   Cache& c = g_cache[info.key];
-  c.blocks.emplace(info.bytes, p);
-  c.cached += info.bytes;
+  if (info.slab) {
+    slab_give(c, static_cast<char*>(p), info.bytes);
+  } else {
+    c.blocks.emplace(info.bytes, p);
+    c.cached += info.bytes;
+  }
 }
 
 int current_device() {
@@ -153,12 +221,52 @@ int fluid_pp_set_allocation_cache(int device, unsigned long long max_cached_byte
       return FLUID_PP_INVALID_ARG;
     }
   }
+  std::vector<char*> slabs;
   {
     std::lock_guard<std::mutex> g(g_mu);
-    g_cache[device].limit = size_t(max_cached_bytes);
+    Cache& c = g_cache[device];
+    c.limit = size_t(max_cached_bytes);
+    // with caching off, the slabs go once none of their ranges is in use
+    if (max_cached_bytes == 0) {
+      size_t free_bytes = 0, slab_bytes = 0;
+      for (const auto& r : c.free_by_addr) free_bytes += r.second;
+      for (const auto& s : c.slabs) slab_bytes += s.second;
+      if (free_bytes == slab_bytes) {
+        for (const auto& s : c.slabs) slabs.push_back(s.first);
+        c.slabs.clear();
+        c.free_by_addr.clear();
+        c.free_by_size.clear();
+      }
+    }
   }
   trim(device, size_t(max_cached_bytes));
+  for (char* s : slabs) raw_free(device, s);
   if (device >= 0) cudaSetDevice(prev);
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_reserve_allocation(int device, unsigned long long bytes) {
+  if (device < 0 || bytes == 0) return FLUID_PP_INVALID_ARG;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    fpp::set_global_error("reserve allocation: no such device");
+    return FLUID_PP_INVALID_ARG;
+  }
+  void* p = nullptr;
+  const size_t n = (size_t(bytes) + kAlign - 1) / kAlign * kAlign;
+  const cudaError_t e = cudaMalloc(&p, n);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    fpp::set_global_error(std::string("reserve allocation: ") + cudaGetErrorString(e));
+    return FLUID_PP_OOM;
+  }
+  std::lock_guard<std::mutex> g(g_mu);
+  Cache& c = g_cache[device];
+  c.slabs.emplace_back(static_cast<char*>(p), n);
+  slab_give(c, static_cast<char*>(p), n);
   return FLUID_PP_OK;
 }
 
@@ -166,7 +274,12 @@ int fluid_pp_allocation_cache_bytes(int device, unsigned long long* cached_bytes
   if (device < kHostKey || !cached_bytes) return FLUID_PP_INVALID_ARG;
   std::lock_guard<std::mutex> g(g_mu);
   auto it = g_cache.find(device);
-  *cached_bytes = it == g_cache.end() ? 0ull : (unsigned long long)it->second.cached;
+  size_t n = 0;
+  if (it != g_cache.end()) {
+    n = it->second.cached;
+    for (const auto& r : it->second.free_by_addr) n += r.second;
+  }
+  *cached_bytes = (unsigned long long)n;
   return FLUID_PP_OK;
 }
 

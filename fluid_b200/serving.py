@@ -117,7 +117,7 @@ class Server:
 
     def __init__(self, budget_bytes: float = 150e9, max_slots: int = 48, precision: str = "fp16", device: int = 0,
                  rel_tol: float = 1e-6, record: bool = False, admit_per_step: int = 1,
-                 cache_bytes: float = 16e9, tall_slice_iterations: int = 8):
+                 cache_bytes: float = 16e9, reserve_bytes: float = 4e9, tall_slice_iterations: int = 8):
         import torch
         self.torch = torch
         self.budget = float(budget_bytes)
@@ -135,6 +135,14 @@ class Server:
         self.cache_bytes = int(cache_bytes)
         self.L.fluid_pp_set_allocation_cache(self.device, ctypes.c_ulonglong(self.cache_bytes))
         self.L.fluid_pp_set_allocation_cache(-1, ctypes.c_ulonglong(min(self.cache_bytes, 256 << 20)))
+        # memory mapped before the first admission: handles are carved from a
+        # reserved slab, and torch's pool (the state copies) is warmed the same way
+        have = ctypes.c_ulonglong()
+        self.L.fluid_pp_allocation_cache_bytes(self.device, ctypes.byref(have))
+        if reserve_bytes > have.value:   # top up what the cache already holds free
+            self.L.fluid_pp_reserve_allocation(self.device, ctypes.c_ulonglong(int(reserve_bytes) - have.value))
+            warm = torch.empty(int(reserve_bytes) // 4, dtype=torch.uint8, device=f"cuda:{self.device}")
+            del warm
         self.pending: list[tuple[Request, int]] = []
         self.active: list[_Sim] = []
         self.done: list[_Sim] = []

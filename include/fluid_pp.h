@@ -218,6 +218,13 @@ int fluid_pp_apply_operator_noalloc(int nx, int ny, int nz, const unsigned char*
  * batch must have been issued on its own stream (fluid_pp_set_stream, the
  * batch's first handle's stream) or have finished before it is destroyed. */
 int fluid_pp_set_allocation_cache(int device, unsigned long long max_cached_bytes);
+/* Reserves `bytes` of device memory for the cache in one cudaMalloc, so that
+ * later handles are carved from memory already mapped (a first-time cudaMalloc
+ * of a large arena can take tens of ms).  While the cache is on, handles take
+ * slab ranges by best fit and released ranges coalesce.  The slabs are freed
+ * when the cache is turned off with none of their ranges in use. */
+int fluid_pp_reserve_allocation(int device, unsigned long long bytes);
+/* Bytes the cache holds free on `device` (block list plus free slab ranges). */
 int fluid_pp_allocation_cache_bytes(int device, unsigned long long* cached_bytes);
 
 /* ------------------------------------------------------------------------

@@ -33,11 +33,13 @@ def _requests():
 def test_each_result_is_the_same_alone_and_in_the_mix():
     mix = Server(record=True)
     stats = mix.run(_requests())
+    mix.shutdown()
     assert stats["requests_finished"] == 4 and stats["failed_steps"] == 0
     got = {s.req.rid: s.pressures for s in mix.done}
     for req in _requests():
         alone = Server(record=True)
         alone.run([req])
+        alone.shutdown()
         (sim,) = alone.done
         assert len(sim.pressures) == req.steps == len(got[req.rid])
         for a, b in zip(sim.pressures, got[req.rid]):
@@ -50,6 +52,7 @@ def test_admission_respects_the_budget():
     budget = max(need) + min(need) // 2     # never two of the larger ones at once
     srv = Server(budget_bytes=budget)
     stats = srv.run(reqs)
+    srv.shutdown()
     assert stats["requests_finished"] == 4
     assert srv.peak_used <= budget
 
@@ -59,6 +62,38 @@ def test_poisson_stream_short():
                             tall_side=(16, 32), tall_band=(24, 32), tall_rows=96)
     srv = Server(max_slots=16)
     stats = srv.run(reqs)
+    srv.shutdown()
     assert stats["requests_finished"] == len(reqs)
     assert stats["failed_steps"] == 0
     assert stats["p99_step_ms"] is not None and stats["solves_per_s"] > 0
+
+
+def test_allocation_cache_carves_and_returns_reserved_memory():
+    """Handles are carved from a reserved slab, give their ranges back on destroy,
+    and a solve on reused memory is bit-identical to the first."""
+    import ctypes
+    from fluid_b200._abi import load
+    from fluid_b200.projector import PressureProjector
+    L = load()
+    got = ctypes.c_ulonglong()
+    assert L.fluid_pp_set_allocation_cache(0, ctypes.c_ulonglong(1 << 30)) == 0
+    assert L.fluid_pp_reserve_allocation(0, ctypes.c_ulonglong(512 << 20)) == 0
+    L.fluid_pp_allocation_cache_bytes(0, ctypes.byref(got))
+    free0 = got.value
+    assert free0 >= 512 << 20
+    (s, _) = _uniform(40, 28, 36, 1)
+    out = []
+    for _ in range(2):
+        p = PressureProjector((s.nx, s.ny, s.nz), s.h, s.rho, precision="fp16")
+        L.fluid_pp_allocation_cache_bytes(0, ctypes.byref(got))
+        assert got.value < free0          # the arena came from the slab
+        p.upload_state(s.vof, s.u, s.v, s.w)
+        assert p.project(s.dt, rel_tol=1e-6)["status_name"] == "OK"
+        out.append(p.pressure_cells())
+        p.destroy()
+        L.fluid_pp_allocation_cache_bytes(0, ctypes.byref(got))
+        assert got.value == free0         # every range coalesced back
+    np.testing.assert_array_equal(out[0], out[1])
+    assert L.fluid_pp_set_allocation_cache(0, ctypes.c_ulonglong(0)) == 0
+    L.fluid_pp_allocation_cache_bytes(0, ctypes.byref(got))
+    assert got.value == 0
