@@ -256,6 +256,218 @@ __global__ void __launch_bounds__(kFThreads, 2) k_down(const InstDev* insts, con
   }
 }
 
+// ====================================================== marching down step
+// The same down step for a level that coarsens by two on every axis, as a
+// 2.5-D march: a CTA owns a coarse tile of kMX x kMY x kMZ cells and streams
+// the fine planes under it once, bottom to top.  Rings of planes in shared
+// memory hold what the stencils still need: rhs / diag / label of 3 planes,
+// z of 4, and the x-then-y restricted residual of 4.  Step p stages fine plane
+// p (loads prefetched into registers during step p - 1) with its red cells
+// set pointwise, sweeps the black cells of plane p - 1, forms the residual of
+// plane p - 2 (storing its interior z to the level's scratch array) and
+// restricts it in x and y; coarse plane Z is finished by the z pass once fine
+// plane 2Z + 2 is restricted.  Used for level 0, whose lattices fill the tiles;
+// coarser levels keep the box kernel, whose tile shape follows the lattice.  Every cell gets the box kernel's arithmetic in
+// the same order, so both give the same bits; only the halo's shape differs:
+// (2 kMX + 6)(2 kMY + 6) staged cells per 4 kMX kMY interior ones in a plane,
+// and 6 extra planes per 2 kMZ.
+constexpr int kMX = 16, kMY = 8, kMZ = 8;             // coarse cells per tile
+constexpr int kMThreads = 256;
+constexpr int kMHX = 2 * kMX + 6, kMHY = 2 * kMY + 6;   // staged plane (F +- 2)
+constexpr int kMHP = kMHX * kMHY;
+constexpr int kMFX = 2 * kMX + 2, kMFY = 2 * kMY + 2;   // residual plane (interior + restriction taps)
+constexpr int kMPer = (kMHP + kMThreads - 1) / kMThreads;
+
+__host__ __device__ inline int march_down_tiles(int cnx, int cny, int cnz) {
+  return ((cnx + kMX - 1) / kMX) * ((cny + kMY - 1) / kMY) * ((cnz + kMZ - 1) / kMZ);
+}
+
+template <class TZ, class TR, class TD, class TS>
+__global__ void __launch_bounds__(kMThreads, 4) k_down_m(const InstDev* insts, const Tile* tiles, int level) {
+  __shared__ float rhs_r[3][kMHP];
+  __shared__ float dg_r[3][kMHP];
+  __shared__ uint8_t lab_r[3][kMHP];
+  __shared__ float z_r[4][kMHP];
+  __shared__ float res_p[kMFX * kMFY];
+  __shared__ float ys_r[4][kMY * kMX];
+  const Tile tl = tiles[blockIdx.x];
+  const InstDev& I = insts[tl.inst];
+  const Ctrl* c = I.ctrl;
+  if (c->done) return;
+  const LevelDev& F = I.lv[level];
+  const LevelDev& C = I.lv[level + 1];
+  const float scale = level == 0 ? float(c->sigma) : 1.0f;
+  const int nx = F.nx, ny = F.ny, nz = F.nz, nxy = nx * ny;
+  const int ntx = (C.nx + kMX - 1) / kMX, nty = (C.ny + kMY - 1) / kMY;
+  const int tx = tl.tile % ntx, tr = tl.tile / ntx, ty = tr % nty, tz = tr / nty;
+  const int cx0 = tx * kMX, cy0 = ty * kMY, cz0 = tz * kMZ;
+  const int hx0 = 2 * cx0 - 3, hy0 = 2 * cy0 - 3;   // staged plane origin
+  const int fx0 = 2 * cx0 - 1, fy0 = 2 * cy0 - 1;   // residual plane origin
+  const int pz0 = 2 * cz0 - 3, pz1 = 2 * (cz0 + kMZ) + 2;
+  const TR* __restrict__ rhs = static_cast<const TR*>(F.rhs);
+  const TD* __restrict__ dg = static_cast<const TD*>(F.diagT);
+  const uint8_t* __restrict__ lab = F.label;
+  TZ* __restrict__ zo = static_cast<TZ*>(F.res);
+  TS* __restrict__ out = static_cast<TS*>(C.rhs);
+  const float wx = F.wx, wy = F.wy, wz = F.wz;
+  const float out_scale = F.to_coarse / 8.0f;
+  const int t = threadIdx.x;
+  // The thread's cells keep their (x, y) in every plane: their in-plane offsets,
+  // global column offsets, lattice masks and colour parities are set once.
+  int aoff[kMPer];      // staged cells: global column offset, -1 outside the lattice or the plane
+  unsigned apar = 0;    // bit k: (x + y) of staged cell k is odd
+#pragma unroll
+  for (int k = 0; k < kMPer; ++k) {
+    const int e = t + k * kMThreads;
+    const int gx = hx0 + e % kMHX, gy = hy0 + e / kMHX;
+    aoff[k] = (e < kMHP && gx >= 0 && gy >= 0 && gx < nx && gy < ny) ? gx + nx * gy : -1;
+    apar |= unsigned((gx + gy) & 1) << k;
+  }
+  constexpr int kW = (kMHX - 2) / 2;                  // black cells per row of G
+  constexpr int kBPer = (kW * (kMHY - 2) + kMThreads - 1) / kMThreads;
+  int bs[kBPer];        // black cells: in-plane index at even offset; parity term of the row
+  unsigned bpar = 0;
+#pragma unroll
+  for (int k = 0; k < kBPer; ++k) {
+    const int e = t + k * kMThreads;
+    const int ey = 1 + e / kW;
+    bs[k] = e < kW * (kMHY - 2) ? ey * kMHX + 1 + 2 * (e % kW) : -1;
+    bpar |= unsigned((hx0 + 1 + hy0 + ey) & 1) << k;
+  }
+  constexpr int kRPer = (kMFX * kMFY + kMThreads - 1) / kMThreads;
+  int rofs[kRPer];      // residual cells: global column offset of interior cells, -1 else
+#pragma unroll
+  for (int k = 0; k < kRPer; ++k) {
+    const int e = t + k * kMThreads;
+    const int lx = e % kMFX, ly = e / kMFX, gx = fx0 + lx, gy = fy0 + ly;
+    rofs[k] = (e < kMFX * kMFY && lx >= 1 && lx <= 2 * kMX && ly >= 1 && ly <= 2 * kMY && gx < nx && gy < ny)
+                  ? gx + nx * gy
+                  : -1;
+  }
+  // restriction: this thread's coarse (x, y) and its 4 x 4 fine taps (weight 0
+  // on taps outside the lattice, whose residual is 0: the fold keeps rline's
+  // order and bits)
+  const int rcx = t % kMX, rcy = t / kMX, RX = cx0 + rcx, RY = cy0 + rcy;
+  const bool rown = t < kMX * kMY && RX < C.nx && RY < C.ny;
+  float wxr[4], wyr[4];
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    const int fx = 2 * RX + d - 1, fy = 2 * RY + d - 1;
+    wxr[d] = (fx >= 0 && fx < nx) ? p1d(fx, RX, C.nx) : 0.0f;
+    wyr[d] = (fy >= 0 && fy < ny) ? p1d(fy, RY, C.ny) : 0.0f;
+  }
+  const int rbase = (2 * rcy) * kMFX + 2 * rcx;   // res_p index of tap (d = -1, d = -1)
+  float pr[kMPer], pd[kMPer];
+  uint8_t pl[kMPer];
+  auto fetch = [&](int p) {
+    const bool pin = p >= 0 && p < nz;
+#pragma unroll
+    for (int k = 0; k < kMPer; ++k) {
+      pr[k] = 0.0f;
+      pd[k] = 1.0f;
+      pl[k] = 0;
+      if (pin && aoff[k] >= 0) {
+        const int i = aoff[k] + nxy * p;
+        pl[k] = lab[i];
+        pr[k] = tof(rhs[i]);
+        pd[k] = tof(dg[i]);
+      }
+    }
+  };
+  auto slot3 = [&](int p) { return (p - pz0) % 3; };
+  auto slot4 = [&](int p) { return (p - pz0) & 3; };
+  // z pass of coarse plane Z = (r - 2) / 2, whose last fine plane r is restricted
+  auto zpass = [&](int r) {
+    if (!rown || r < 2 * cz0 + 2 || ((r - 2) & 1)) return;
+    const int Z = (r - 2) >> 1;
+    if (Z >= cz0 + kMZ || Z >= C.nz) return;
+    const int ci = RX + C.nx * (RY + C.ny * Z);
+    float acc = 0.0f;
+    if (C.label[ci]) {
+      float sum = 0.0f;
+#pragma unroll
+      for (int d = -1; d <= 2; ++d) {
+        const int f = 2 * Z + d;
+        if (f >= 0 && f < nz) sum += p1d(f, Z, C.nz) * ys_r[slot4(f)][t];
+      }
+      acc = out_scale * sum;
+    }
+    out[ci] = fromf<TS>(acc);
+  };
+  fetch(pz0);
+  for (int p = pz0; p <= pz1; ++p) {
+    const int k = p - pz0;
+    // stage plane p: red cells start the sweep at rhs / diag, black cells at zero
+    {
+      const int sa = slot3(p), za = slot4(p);
+      const unsigned red = (p & 1) ? apar : ~apar;   // bit k: cell k is red in plane p
+#pragma unroll
+      for (int kk = 0; kk < kMPer; ++kk) {
+        const int e = t + kk * kMThreads;
+        if (e >= kMHP) continue;
+        rhs_r[sa][e] = pr[kk];
+        dg_r[sa][e] = pd[kk];
+        lab_r[sa][e] = pl[kk];
+        z_r[za][e] = (pl[kk] && ((red >> kk) & 1u)) ? rnd<TZ>(pr[kk] * __frcp_rn(pd[kk])) : 0.0f;
+      }
+    }
+    if (p < pz1) fetch(p + 1);
+    zpass(p - 3);   // the previous step restricted fine plane p - 3
+    __syncthreads();
+    // black cells of plane q = p - 1 inside G = F +- 1 (their neighbours are red)
+    if (k >= 2) {
+      const int q = p - 1, sq = slot3(q), zq = slot4(q), zm = slot4(q - 1), zp = slot4(p);
+      const float* zc = z_r[zq];
+#pragma unroll
+      for (int kk = 0; kk < kBPer; ++kk) {
+        if (bs[kk] < 0) continue;
+        const int s = bs[kk] + int((((bpar >> kk) ^ unsigned(q)) & 1u) ^ 1u);
+        if (!lab_r[sq][s]) continue;
+        const float nb = d4sum6(wx * zc[s - 1], wx * zc[s + 1], wy * zc[s - kMHX], wy * zc[s + kMHX],
+                                wz * z_r[zm][s], wz * z_r[zp][s]);
+        z_r[zq][s] = rnd<TZ>((rhs_r[sq][s] + nb) * __frcp_rn(dg_r[sq][s]));
+      }
+    }
+    __syncthreads();
+    // residual of plane r = p - 2 on F; its interior z goes to the scratch array
+    const int r = p - 2;
+    if (k >= 4) {
+      const int sr = slot3(r), zr = slot4(r), zm = slot4(r - 1), zp = slot4(r + 1);
+      const bool zin = r >= 2 * cz0 && r < 2 * (cz0 + kMZ) && r < nz;
+      const float* zc = z_r[zr];
+#pragma unroll
+      for (int kk = 0; kk < kRPer; ++kk) {
+        const int e = t + kk * kMThreads;
+        if (e >= kMFX * kMFY) continue;
+        const int s = (e / kMFX + 2) * kMHX + e % kMFX + 2;
+        float rv = 0.0f;
+        if (lab_r[sr][s])
+          rv = scale * (rhs_r[sr][s] - (dg_r[sr][s] * zc[s] -
+                                         d4sum6(wx * zc[s - 1], wx * zc[s + 1], wy * zc[s - kMHX], wy * zc[s + kMHX],
+                                                wz * z_r[zm][s], wz * z_r[zp][s])));
+        res_p[e] = rv;
+        if (zin && rofs[kk] >= 0) zo[rofs[kk] + nxy * r] = fromf<TZ>(zc[s]);
+      }
+    }
+    __syncthreads();
+    // x then y restriction of the plane into the ring, one coarse (x, y) per thread
+    if (k >= 4 && t < kMX * kMY) {
+      float sy = 0.0f;
+#pragma unroll
+      for (int dy = 0; dy < 4; ++dy) {
+        const float* row = &res_p[rbase + dy * kMFX];
+        float sx = 0.0f;
+#pragma unroll
+        for (int dx = 0; dx < 4; ++dx) sx += wxr[dx] * row[dx];
+        sy += wyr[dy] * sx;
+      }
+      ys_r[slot4(r)][t] = sy;
+    }
+    __syncthreads();
+  }
+  zpass(pz1 - 2);
+}
+
 // ================================================================ up step
 // z_l += P z_{l+1} (mgProlongateAdd, mg.wgsl.ts:243-246; from level 1 into
 // level 0 the sigma scaling is undone), then one sweep black then red, one fine
@@ -389,6 +601,250 @@ __global__ void __launch_bounds__(kFThreads, 2) k_up(const InstDev* insts, const
     const double zs = gather_slot(partial, 1, nt0, 0, sh);
     const double rs = gather_slot(partial, 2, nt0, 0, sh);
     if (threadIdx.x == 0) finish_gamma(c, g, zs, rs);
+  }
+}
+
+// ======================================================== marching up step
+// The level-0 up step of a level coarsened by two on every axis as a 2.5-D
+// march (see k_down_m): a CTA owns kUX x kUY x kUZ fine cells and streams the
+// planes under them once.  Step p stages fine plane p of the halo box E = T +- 2
+// with the prolongated coarse correction added (each thread keeps its cells'
+// x / y taps for the whole march; coarse planes arrive in a ring of 3),
+// sweeps the black cells of plane p - 1 on T +- 1, then the red cells of plane
+// p - 2 on T, writing that plane's z and its gamma partials.  Each cell gets
+// k_up's arithmetic in the same order.
+constexpr int kUX = 32, kUY = 16, kUZ = 16;            // fine cells per tile
+constexpr int kUEX = kUX + 4, kUEY = kUY + 4, kUEP = kUEX * kUEY;
+constexpr int kUQX = (kUX + 4) / 2 + 3, kUQY = (kUY + 4) / 2 + 3, kUQP = kUQX * kUQY;   // coarse plane box
+constexpr int kUPer = (kUEP + kMThreads - 1) / kMThreads;
+
+__host__ __device__ inline int march_up_tiles(int nx, int ny, int nz) {
+  return ((nx + kUX - 1) / kUX) * ((ny + kUY - 1) / kUY) * ((nz + kUZ - 1) / kUZ);
+}
+
+template <class TZF, class TR, class TD, class TZC>
+__global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, const Tile* tiles, int with_dot) {
+  __shared__ float rhs_r[3][kUEP];
+  __shared__ float dg_r[3][kUEP];
+  __shared__ uint8_t lab_r[3][kUEP];
+  __shared__ float z_r[4][kUEP];
+  __shared__ float zc_r[3][kUQP];
+  __shared__ double sh[32];
+  __shared__ int flag;
+  const Tile tl = tiles[blockIdx.x];
+  const InstDev& I = insts[tl.inst];
+  Ctrl* c = I.ctrl;
+  if (c->done) return;
+  const LevelDev& F = I.lv[0];
+  const LevelDev& C = I.lv[1];
+  const float unscale = float(1.0 / c->sigma);
+  const int nx = F.nx, ny = F.ny, nz = F.nz, nxy = nx * ny;
+  const int ntx = (nx + kUX - 1) / kUX, nty = (ny + kUY - 1) / kUY;
+  const int tx = tl.tile % ntx, tr = tl.tile / ntx, ty = tr % nty, tz = tr / nty;
+  const int x0 = tx * kUX, y0 = ty * kUY, z0 = tz * kUZ;
+  const int ex0 = x0 - 2, ey0 = y0 - 2;            // staged plane origin
+  const int pz0 = z0 - 2, pz1 = z0 + kUZ + 1;      // fine planes streamed
+  // coarse columns under the in-lattice part of the staged plane (k_up's cspan)
+  auto cspan = [](int e0, int en, int nf, int nc, int& c0, int& cn) {
+    const int lo = max(e0, 0), hi = min(e0 + en - 1, nf - 1);
+    c0 = max(lo / 2 - 1, 0);
+    cn = min(hi / 2 + 1, nc - 1) - c0 + 1;
+  };
+  int qx0, qex, qy0, qey;
+  cspan(ex0, kUEX, nx, C.nx, qx0, qex);
+  cspan(ey0, kUEY, ny, C.ny, qy0, qey);
+  const TZF* __restrict__ zf = static_cast<const TZF*>(F.res);
+  const TR* __restrict__ rhs = static_cast<const TR*>(F.rhs);
+  const TD* __restrict__ dg = static_cast<const TD*>(F.diagT);
+  const uint8_t* __restrict__ lab = F.label;
+  const TZC* __restrict__ zc = static_cast<const TZC*>(C.z);
+  TZF* __restrict__ zo = static_cast<TZF*>(F.z);
+  const float wx = F.wx, wy = F.wy, wz = F.wz;
+  const int t = threadIdx.x;
+  // The thread's staged cells keep their (x, y) in every plane: column offset
+  // (-1 outside the lattice), the coarse-plane offset of tap (c1, c0) = (0, 0)
+  // with the steps to taps 1 along x and y (0 where a wall dropped the tap),
+  // and the x / y tap weights.
+  int aoff[kUPer], qb[kUPer];
+  unsigned qstep = 0;   // bits 2k, 2k + 1: x and y step of cell k
+  float wxx[kUPer][2], wyy[kUPer][2];
+#pragma unroll
+  for (int k = 0; k < kUPer; ++k) {
+    const int e = t + k * kMThreads;
+    const int gx = ex0 + e % kUEX, gy = ey0 + e / kUEX;
+    aoff[k] = (e < kUEP && gx >= 0 && gy >= 0 && gx < nx && gy < ny) ? gx + nx * gy : -1;
+    int cx[2], cy[2];
+    taps2(gx, 2, C.nx, cx, wxx[k]);
+    taps2(gy, 2, C.ny, cy, wyy[k]);
+    qb[k] = (cx[0] - qx0) + qex * (cy[0] - qy0);
+    qstep |= (unsigned(cx[1] - cx[0] == 1) << (2 * k)) | (unsigned(cy[1] - cy[0] == 1) << (2 * k + 1));
+  }
+  constexpr int kW = (kUEX - 2) / 2;                  // black cells per row of T +- 1
+  constexpr int kBPer = (kW * (kUEY - 2) + kMThreads - 1) / kMThreads;
+  int bs[kBPer];
+  unsigned bpar = 0;
+#pragma unroll
+  for (int k = 0; k < kBPer; ++k) {
+    const int e = t + k * kMThreads;
+    const int ey = 1 + e / kW;
+    bs[k] = e < kW * (kUEY - 2) ? ey * kUEX + 1 + 2 * (e % kW) : -1;
+    bpar |= unsigned((ex0 + 1 + ey0 + ey) & 1) << k;
+  }
+  constexpr int kTPer = (kUX * kUY + kMThreads - 1) / kMThreads;
+  int ts_[kTPer], tofs[kTPer];   // interior cells: in-plane index, column offset (-1 outside the lattice)
+  unsigned tpar = 0;
+#pragma unroll
+  for (int k = 0; k < kTPer; ++k) {
+    const int e = t + k * kMThreads;
+    const int lx = e % kUX, ly = e / kUX, gx = x0 + lx, gy = y0 + ly;
+    ts_[k] = (ly + 2) * kUEX + lx + 2;
+    tofs[k] = (e < kUX * kUY && gx < nx && gy < ny) ? gx + nx * gy : -1;
+    tpar |= unsigned((gx + gy) & 1) << k;
+  }
+  // coarse planes: Z goes to slot Z % 3
+  auto load_coarse = [&](int Z) {
+    float* d = zc_r[Z % 3];
+    for (int e = t; e < qex * qey; e += kMThreads) {
+      const int cxl = e % qex, cyl = e / qex;
+      d[cxl + qex * cyl] = tof(zc[(qx0 + cxl) + C.nx * ((qy0 + cyl) + C.ny * Z)]);
+    }
+  };
+  auto coarse_hi = [&](int p) {   // the highest coarse plane fine plane p reads
+    int cz[2];
+    float w[2];
+    taps2(min(max(p, 0), nz - 1), 2, C.nz, cz, w);
+    return max(cz[0], cz[1]);
+  };
+  float pz_[kUPer], pr[kUPer], pd[kUPer];
+  uint8_t pl[kUPer];
+  auto fetch = [&](int p) {
+    const bool pin = p >= 0 && p < nz;
+#pragma unroll
+    for (int k = 0; k < kUPer; ++k) {
+      pz_[k] = 0.0f;
+      pr[k] = 0.0f;
+      pd[k] = 1.0f;
+      pl[k] = 0;
+      if (pin && aoff[k] >= 0) {
+        const int i = aoff[k] + nxy * p;
+        pl[k] = lab[i];
+        pz_[k] = tof(zf[i]);
+        pr[k] = tof(rhs[i]);
+        pd[k] = tof(dg[i]);
+      }
+    }
+  };
+  auto slot3 = [&](int p) { return (p - pz0) % 3; };
+  auto slot4 = [&](int p) { return (p - pz0) & 3; };
+  int zhi_loaded;
+  {
+    int cz[2];
+    float w[2];
+    taps2(min(max(pz0, 0), nz - 1), 2, C.nz, cz, w);
+    zhi_loaded = coarse_hi(pz0);
+    for (int Z = min(cz[0], cz[1]); Z <= zhi_loaded; ++Z) load_coarse(Z);
+  }
+  fetch(pz0);
+  __syncthreads();
+  double rz = 0.0, zsum = 0.0, rsum = 0.0;
+  for (int p = pz0; p <= pz1; ++p) {
+    const int k = p - pz0;
+    // stage plane p with the prolongated correction on liquid cells
+    {
+      const int sa = slot3(p), za = slot4(p);
+      int czs[2];
+      float wzz[2];
+      taps2(p, 2, C.nz, czs, wzz);
+#pragma unroll
+      for (int kk = 0; kk < kUPer; ++kk) {
+        const int e = t + kk * kMThreads;
+        if (e >= kUEP) continue;
+        rhs_r[sa][e] = pr[kk];
+        dg_r[sa][e] = pd[kk];
+        lab_r[sa][e] = pl[kk];
+        float zv = pz_[kk];
+        if (pl[kk]) {
+          const int sx = int((qstep >> (2 * kk)) & 1u), sy = int((qstep >> (2 * kk + 1)) & 1u) * qex;
+          float acc = 0.0f;
+#pragma unroll
+          for (int c2 = 0; c2 < 2; ++c2) {
+            const float* q = zc_r[czs[c2] % 3] + qb[kk];
+#pragma unroll
+            for (int c1 = 0; c1 < 2; ++c1)
+#pragma unroll
+              for (int c0 = 0; c0 < 2; ++c0)
+                acc += wxx[kk][c0] * wyy[kk][c1] * wzz[c2] * q[c1 * sy + c0 * sx];
+          }
+          zv = rnd<TZF>(zv + acc * unscale);
+        }
+        z_r[za][e] = zv;
+      }
+    }
+    if (p < pz1) fetch(p + 1);
+    __syncthreads();
+    // the next plane's coarse planes (their slots are free: plane p no longer reads them)
+    if (p < pz1) {
+      const int need = coarse_hi(p + 1);
+      for (int Z = zhi_loaded + 1; Z <= need; ++Z) load_coarse(Z);
+      zhi_loaded = max(zhi_loaded, need);
+    }
+    // black cells of plane q = p - 1 on T +- 1
+    if (k >= 2) {
+      const int q = p - 1, sq = slot3(q), zq = slot4(q), zm = slot4(q - 1), zp = slot4(p);
+      const float* zq_ = z_r[zq];
+#pragma unroll
+      for (int kk = 0; kk < kBPer; ++kk) {
+        if (bs[kk] < 0) continue;
+        const int s = bs[kk] + int((((bpar >> kk) ^ unsigned(q)) & 1u) ^ 1u);
+        if (!lab_r[sq][s]) continue;
+        const float nb = d4sum6(wx * zq_[s - 1], wx * zq_[s + 1], wy * zq_[s - kUEX], wy * zq_[s + kUEX],
+                                wz * z_r[zm][s], wz * z_r[zp][s]);
+        z_r[zq][s] = rnd<TZF>((rhs_r[sq][s] + nb) * __frcp_rn(dg_r[sq][s]));
+      }
+    }
+    __syncthreads();
+    // red cells of plane r = p - 2 on T, then the plane's output and gamma partials
+    if (k >= 4) {
+      const int r = p - 2, sr = slot3(r), zr = slot4(r), zm = slot4(r - 1), zp = slot4(r + 1);
+      const float* zr_ = z_r[zr];
+      const unsigned red = (r & 1) ? tpar : ~tpar;
+      const bool rin = r < nz;
+#pragma unroll
+      for (int kk = 0; kk < kTPer; ++kk) {
+        const int s = ts_[kk];
+        float zv = zr_[s];
+        const bool liq = lab_r[sr][s] != 0;
+        if (liq && ((red >> kk) & 1u))
+          zv = rnd<TZF>((rhs_r[sr][s] + d4sum6(wx * zr_[s - 1], wx * zr_[s + 1], wy * zr_[s - kUEX],
+                                               wy * zr_[s + kUEX], wz * z_r[zm][s], wz * z_r[zp][s])) *
+                        __frcp_rn(dg_r[sr][s]));
+        if (rin && tofs[kk] >= 0) {
+          zo[tofs[kk] + nxy * r] = fromf<TZF>(zv);
+          if (liq) {
+            const double rv = rhs_r[sr][s];
+            rz += rv * double(zv);
+            zsum += zv;
+            rsum += rv;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!with_dot) return;   // uniform over the launch
+  const int nt = march_up_tiles(nx, ny, nz);
+  double* partial = I.partial;
+  const double a0 = block_sum(rz, sh), a1 = block_sum(zsum, sh), a2 = block_sum(rsum, sh);
+  if (t == 0) {
+    partial[0 * nt + tl.tile] = a0;
+    partial[1 * nt + tl.tile] = a1;
+    partial[2 * nt + tl.tile] = a2;
+  }
+  if (arrive_last(&c->arrive[kStGamma], nt, &flag)) {
+    const double g = gather_slot(partial, 0, nt, 0, sh);
+    const double zs = gather_slot(partial, 1, nt, 0, sh);
+    const double rs = gather_slot(partial, 2, nt, 0, sh);
+    if (t == 0) finish_gamma(c, g, zs, rs);
   }
 }
 
