@@ -266,11 +266,11 @@ __global__ void __launch_bounds__(kFThreads, 2) k_down(const InstDev* insts, con
 // set pointwise, sweeps the black cells of plane p - 1, forms the residual of
 // plane p - 2 (storing its interior z to the level's scratch array) and
 // restricts it in x and y; coarse plane Z is finished by the z pass once fine
-// plane 2Z + 2 is restricted.  Used for level 0, whose lattices fill the tiles;
-// coarser levels keep the box kernel, whose tile shape follows the lattice.  Every cell gets the box kernel's arithmetic in
+// plane 2Z + 2 is restricted.  Every cell gets the box kernel's arithmetic in
 // the same order, so both give the same bits; only the halo's shape differs:
 // (2 kMX + 6)(2 kMY + 6) staged cells per 4 kMX kMY interior ones in a plane,
 // and 6 extra planes per 2 kMZ.
+constexpr int kMarchLevels = 2;                       // grid levels 0 .. kMarchLevels - 1 may march
 constexpr int kMX = 16, kMY = 8, kMZ = 8;             // coarse cells per tile
 constexpr int kMThreads = 256;
 constexpr int kMHX = 2 * kMX + 6, kMHY = 2 * kMY + 6;   // staged plane (F +- 2)
@@ -605,14 +605,14 @@ __global__ void __launch_bounds__(kFThreads, 2) k_up(const InstDev* insts, const
 }
 
 // ======================================================== marching up step
-// The level-0 up step of a level coarsened by two on every axis as a 2.5-D
-// march (see k_down_m): a CTA owns kUX x kUY x kUZ fine cells and streams the
+// The up step of a level coarsened by two on every axis as a 2.5-D march (see
+// k_down_m): a CTA owns kUX x kUY x kUZ fine cells and streams the
 // planes under them once.  Step p stages fine plane p of the halo box E = T +- 2
 // with the prolongated coarse correction added (each thread keeps its cells'
 // x / y taps for the whole march; coarse planes arrive in a ring of 3),
 // sweeps the black cells of plane p - 1 on T +- 1, then the red cells of plane
-// p - 2 on T, writing that plane's z and its gamma partials.  Each cell gets
-// k_up's arithmetic in the same order.
+// p - 2 on T, writing that plane's z (and on level 0 with with_dot its gamma
+// partials).  Each cell gets k_up's arithmetic in the same order.
 constexpr int kUX = 32, kUY = 16, kUZ = 16;            // fine cells per tile
 constexpr int kUEX = kUX + 4, kUEY = kUY + 4, kUEP = kUEX * kUEY;
 constexpr int kUQX = (kUX + 4) / 2 + 3, kUQY = (kUY + 4) / 2 + 3, kUQP = kUQX * kUQY;   // coarse plane box
@@ -623,7 +623,8 @@ __host__ __device__ inline int march_up_tiles(int nx, int ny, int nz) {
 }
 
 template <class TZF, class TR, class TD, class TZC>
-__global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, const Tile* tiles, int with_dot) {
+__global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, const Tile* tiles, int level,
+                                                        int with_dot) {
   __shared__ float rhs_r[3][kUEP];
   __shared__ float dg_r[3][kUEP];
   __shared__ uint8_t lab_r[3][kUEP];
@@ -635,9 +636,9 @@ __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, con
   const InstDev& I = insts[tl.inst];
   Ctrl* c = I.ctrl;
   if (c->done) return;
-  const LevelDev& F = I.lv[0];
-  const LevelDev& C = I.lv[1];
-  const float unscale = float(1.0 / c->sigma);
+  const LevelDev& F = I.lv[level];
+  const LevelDev& C = I.lv[level + 1];
+  const float unscale = level == 0 ? float(1.0 / c->sigma) : 1.0f;
   const int nx = F.nx, ny = F.ny, nz = F.nz, nxy = nx * ny;
   const int ntx = (nx + kUX - 1) / kUX, nty = (ny + kUY - 1) / kUY;
   const int tx = tl.tile % ntx, tr = tl.tile / ntx, ty = tr % nty, tz = tr / nty;

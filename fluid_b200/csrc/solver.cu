@@ -96,8 +96,8 @@ struct fluid_pp_batch {
   List rst[kMaxLevels];      // level-(l+1) tiles of instances for which l is not the coarsest
   List crs[kMaxLevels];      // level-l tiles (l >= 1) of every instance having level l
   List dn[kMaxLevels];       // fused down-step tiles (coarse tiles of level l+1) of grid level l
-  List dnm[kMaxLevels];      // marching down-step tiles of grid level l (level 0 coarsened by two on every axis)
-  List upm;                  // marching up-step tiles of level 0 (same condition)
+  List dnm[kMaxLevels];      // marching down-step tiles of grid level l (levels < kMarchLevels coarsened by two on every axis)
+  List upm[kMaxLevels];      // marching up-step tiles (same condition)
   List up[kMaxLevels];       // fused up-step tiles (fine tiles of level l) of grid level l
   List l0single;             // level-0 tiles of single-level instances
   List bake;
@@ -319,9 +319,13 @@ void vcycle_fused(fluid_pp_batch* B, int with_dot) {
     FPP_LAUNCH(B, kPrCoarse,
                k_coarse_apply<float, float><<<B->single.n, kThreads, 0, s>>>(B->d_insts, il(B, B->single)));
   for (int l = B->maxL - 2; l >= 0; --l) {
-    if (l == 0 && B->upm.n)
-      FPP_LAUNCH(B, kPrUp0, k_up_m<float, float, T, T><<<B->upm.n, kMThreads, 0, s>>>(B->d_insts, tl(B, B->upm),
-                                                                                      with_dot));
+    if (B->upm[l].n) {
+      if (l == 0)
+        FPP_LAUNCH(B, kPrUp0, k_up_m<float, float, T, T><<<B->upm[l].n, kMThreads, 0, s>>>(
+                                  B->d_insts, tl(B, B->upm[l]), 0, with_dot));
+      else
+        FPP_LAUNCH(B, kPrUpC, k_up_m<T, T, T, T><<<B->upm[l].n, kMThreads, 0, s>>>(B->d_insts, tl(B, B->upm[l]), l, 0));
+    }
     const List& Lu = B->up[l];
     if (!Lu.n) continue;
     if (l == 0)
@@ -606,10 +610,10 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
       add_level(B->rst[l], [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; }, l + 1, true);
     if (l >= 1) add_level(B->crs[l], [l](const InstDev& I) { return l < I.nlev; }, l);
     auto grid_level = [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; };
-    // level 0 coarsened by two on every axis takes the marching down step
+    // levels 0 and 1 coarsened by two on every axis take the marching steps
     auto marching = [l](const InstDev& I) {
       const LevelDev& C = I.lv[l + 1];
-      return l == 0 && C.sx == 2 && C.sy == 2 && C.sz == 2;
+      return l <= kMarchLevels - 1 && C.sx == 2 && C.sy == 2 && C.sz == 2;
     };
     B->dn[l].off = int(tiles.size());
     for (int k = 0; k < count; ++k)
@@ -629,15 +633,14 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
       if (grid_level(insts[k]) && !marching(insts[k]))
         for (int t = 0; t < insts[k].lv[l].utiles; ++t) tiles.push_back(Tile{k, l, t, 0});
     B->up[l].n = int(tiles.size()) - B->up[l].off;
-    if (l == 0) {
-      B->upm.off = int(tiles.size());
-      for (int k = 0; k < count; ++k)
-        if (grid_level(insts[k]) && marching(insts[k])) {
-          const int nt = march_up_tiles(insts[k].lv[0].nx, insts[k].lv[0].ny, insts[k].lv[0].nz);
-          for (int t = 0; t < nt; ++t) tiles.push_back(Tile{k, 0, t, 0});
-        }
-      B->upm.n = int(tiles.size()) - B->upm.off;
-    }
+    B->upm[l].off = int(tiles.size());
+    for (int k = 0; k < count; ++k)
+      if (grid_level(insts[k]) && marching(insts[k])) {
+        const LevelDev& Lv = insts[k].lv[l];
+        const int nt = march_up_tiles(Lv.nx, Lv.ny, Lv.nz);
+        for (int t = 0; t < nt; ++t) tiles.push_back(Tile{k, l, t, 0});
+      }
+    B->upm[l].n = int(tiles.size()) - B->upm[l].off;
   }
   add_level(B->l0single, [](const InstDev& I) { return I.nlev == 1; }, 0);
   B->bake.off = int(tiles.size());
