@@ -66,10 +66,11 @@ def stage_bytes_per_cell(stage: str, s: int) -> float:
     }.get(stage, 0.0)
 
 
-# DRAM bytes (read + write) per launch of a stage's kernel on the 128x96x128
-# workload, fp16 levels, from the committed ncu capture
-# profiles/fused_kernels_dam_spheres_128x96x128_fp16.md (cold-cache launches).
-NCU_TRAFFIC_BYTES = {"up0": 17.77e6, "down0": 11.25e6, "dirspmv": 17.25e6, "update": 33.55e6}
+# DRAM bytes (read + write) per launch of a stage's kernel on the batched
+# workload (64 instances, fp16 levels, a first-iteration launch with every
+# instance iterating), from the committed ncu capture
+# profiles/marching_vcycle_batch64_fp16.md (cold-cache launches).
+NCU_TRAFFIC_BYTES = {"up0": 197.87e6, "down0": 134.09e6}
 
 
 def peaks():
@@ -357,18 +358,28 @@ def main():
 
     t2_mixed, r2_mixed, _ = run_single(args.precision)
     t2_plain, _, _ = run_single("fp32")
-    # per-stage kernel events for the roofline (direct launches of the same solves)
+    # per-stage kernel events of the 128x96x128 solves (direct launches), reported per solve
     _, _, prof = run_single(args.precision, profile=True)
+
+    # roofline of the headline: per-stage kernel events of the batched solve
+    # (direct launches of the same 64 solves).  A launch of a level-0 stage
+    # touches every cell of every instance still iterating, so the stage's
+    # algorithmic bytes over the solve are bytes/cell x sum(cells_i x iterations_i).
+    note("headline per-stage events")
+    prof_steps = 2
+    _, brecs, bprof = run_batched(args.precision, prof_steps, profile=True)
     sbytes = 4 if args.precision == "fp32" else 2
-    ncell2 = s0.cells
-    stages = {k: v for k, v in prof.items() if stage_bytes_per_cell(k, sbytes) > 0}
+    cell_iters = prof_steps * sum(s_.cells * r["iterations"] for s_, r in zip(insts, brecs))
+    stages = {k: v for k, v in bprof.items() if stage_bytes_per_cell(k, sbytes) > 0 and v["launches"] > 0}
     dom = max(stages, key=lambda k: stages[k]["ms"])
-    per_launch_ms = prof[dom]["ms"] / prof[dom]["launches"]
-    alg = stage_bytes_per_cell(dom, sbytes) * ncell2
+    per_launch_ms = bprof[dom]["ms"] / bprof[dom]["launches"]
+    alg = stage_bytes_per_cell(dom, sbytes) * cell_iters / bprof[dom]["launches"]
     hbm, peak_kind = peaks()
     achieved = alg / (per_launch_ms / 1000.0) / 1e9
-    tot_prof = sum(v["ms"] for v in prof.values())
+    tot_prof = sum(v["ms"] for v in bprof.values())
     traffic = NCU_TRAFFIC_BYTES.get(dom)
+    stage_gbs = {k: round(stage_bytes_per_cell(k, sbytes) * cell_iters / (v["ms"] / 1000.0) / 1e9, 1)
+                 for k, v in stages.items()}
 
     # ------------------------------------ secondary: tall-cell 256^2 columns x 1024 rows
     note("tall-cell waves")
@@ -474,10 +485,11 @@ def main():
         },
         "tall_cell_256x256x1024": tall_line,
         "serving": serving,
-        "roofline": {"bound": "hbm", "kernel": dom, "workload": "dam_spheres_128x96x128 (one instance per launch)",
+        "roofline": {"bound": "hbm", "kernel": dom, "workload": "the headline batch (64 instances per launch)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": peak_kind, "traffic": traffic, "alg_bytes_per_launch": alg,
-                     "launch_ms": per_launch_ms, "share_of_step": prof[dom]["ms"] / tot_prof},
+                     "launch_ms": per_launch_ms, "share_of_step": bprof[dom]["ms"] / tot_prof,
+                     "stage_gbs": stage_gbs},
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),

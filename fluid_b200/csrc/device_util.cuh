@@ -108,6 +108,35 @@ __device__ __forceinline__ float d4sum6(float xm, float xp, float ym, float yp, 
 }
 
 // Deterministic block reductions (fixed shuffle tree).  Result valid in warp 0.
+// Three block_sum folds in one pass (each value takes block_sum's tree, so the
+// bits are block_sum's); sh holds 3 x 32 doubles.  Results valid in warp 0.
+__device__ __forceinline__ void block_sum3(double& a, double& b, double& c, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    sh[w] = a;
+    sh[32 + w] = b;
+    sh[64 + w] = c;
+  }
+  __syncthreads();
+  if (w == 0) {
+    const bool in = l < int(blockDim.x >> 5);
+    a = in ? sh[l] : 0.0;
+    b = in ? sh[32 + l] : 0.0;
+    c = in ? sh[64 + l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+  }
+  __syncthreads();
+}
+
 __device__ __forceinline__ double block_sum(double v, double* sh) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;

@@ -611,8 +611,8 @@ __global__ void __launch_bounds__(kFThreads, 2) k_up(const InstDev* insts, const
 // with the prolongated coarse correction added (each thread keeps its cells'
 // x / y taps for the whole march; coarse planes arrive in a ring of 3),
 // sweeps the black cells of plane p - 1 on T +- 1, then the red cells of plane
-// p - 2 on T, writing that plane's z (and on level 0 with with_dot its gamma
-// partials).  Each cell gets k_up's arithmetic in the same order.
+// p - 2 on T, writing that plane's z.  Each cell gets k_up's arithmetic in the
+// same order.
 constexpr int kUX = 32, kUY = 16, kUZ = 16;            // fine cells per tile
 constexpr int kUEX = kUX + 4, kUEY = kUY + 4, kUEP = kUEX * kUEY;
 constexpr int kUQX = (kUX + 4) / 2 + 3, kUQY = (kUY + 4) / 2 + 3, kUQP = kUQX * kUQY;   // coarse plane box
@@ -623,18 +623,15 @@ __host__ __device__ inline int march_up_tiles(int nx, int ny, int nz) {
 }
 
 template <class TZF, class TR, class TD, class TZC>
-__global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, const Tile* tiles, int level,
-                                                        int with_dot) {
+__global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, const Tile* tiles, int level) {
   __shared__ float rhs_r[3][kUEP];
   __shared__ float dg_r[3][kUEP];
   __shared__ uint8_t lab_r[3][kUEP];
   __shared__ float z_r[4][kUEP];
   __shared__ float zc_r[3][kUQP];
-  __shared__ double sh[32];
-  __shared__ int flag;
   const Tile tl = tiles[blockIdx.x];
   const InstDev& I = insts[tl.inst];
-  Ctrl* c = I.ctrl;
+  const Ctrl* c = I.ctrl;
   if (c->done) return;
   const LevelDev& F = I.lv[level];
   const LevelDev& C = I.lv[level + 1];
@@ -747,7 +744,6 @@ __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, con
   }
   fetch(pz0);
   __syncthreads();
-  double rz = 0.0, zsum = 0.0, rsum = 0.0;
   for (int p = pz0; p <= pz1; ++p) {
     const int k = p - pz0;
     // stage plane p with the prolongated correction on liquid cells
@@ -804,7 +800,7 @@ __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, con
       }
     }
     __syncthreads();
-    // red cells of plane r = p - 2 on T, then the plane's output and gamma partials
+    // red cells of plane r = p - 2 on T, then the plane's output
     if (k >= 4) {
       const int r = p - 2, sr = slot3(r), zr = slot4(r), zm = slot4(r - 1), zp = slot4(r + 1);
       const float* zr_ = z_r[zr];
@@ -819,33 +815,10 @@ __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, con
           zv = rnd<TZF>((rhs_r[sr][s] + d4sum6(wx * zr_[s - 1], wx * zr_[s + 1], wy * zr_[s - kUEX],
                                                wy * zr_[s + kUEX], wz * z_r[zm][s], wz * z_r[zp][s])) *
                         __frcp_rn(dg_r[sr][s]));
-        if (rin && tofs[kk] >= 0) {
-          zo[tofs[kk] + nxy * r] = fromf<TZF>(zv);
-          if (liq) {
-            const double rv = rhs_r[sr][s];
-            rz += rv * double(zv);
-            zsum += zv;
-            rsum += rv;
-          }
-        }
+        if (rin && tofs[kk] >= 0) zo[tofs[kk] + nxy * r] = fromf<TZF>(zv);
       }
     }
     __syncthreads();
-  }
-  if (!with_dot) return;   // uniform over the launch
-  const int nt = march_up_tiles(nx, ny, nz);
-  double* partial = I.partial;
-  const double a0 = block_sum(rz, sh), a1 = block_sum(zsum, sh), a2 = block_sum(rsum, sh);
-  if (t == 0) {
-    partial[0 * nt + tl.tile] = a0;
-    partial[1 * nt + tl.tile] = a1;
-    partial[2 * nt + tl.tile] = a2;
-  }
-  if (arrive_last(&c->arrive[kStGamma], nt, &flag)) {
-    const double g = gather_slot(partial, 0, nt, 0, sh);
-    const double zs = gather_slot(partial, 1, nt, 0, sh);
-    const double rs = gather_slot(partial, 2, nt, 0, sh);
-    if (t == 0) finish_gamma(c, g, zs, rs);
   }
 }
 

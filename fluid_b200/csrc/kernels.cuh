@@ -806,7 +806,7 @@ __device__ __forceinline__ void for_column(const TileIt& it, int nx, int ny, int
 
 // gamma = r . (z - zmean) with float64 accumulation; beta from the previous gamma.
 __global__ void __launch_bounds__(kThreads) k_dot_rz(const InstDev* insts, const Tile* tiles, int ntiles) {
-  __shared__ double sh[32];
+  __shared__ double sh[96];
   __shared__ int flag;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
@@ -842,6 +842,66 @@ __global__ void __launch_bounds__(kThreads) k_dot_rz(const InstDev* insts, const
       if (threadIdx.x == 0) finish_gamma(c, g, zsum, rsum);
     }
   }
+}
+
+// The same gamma partials as k_dot_rz (per level-0 tile, block_sum's fold)
+// without the per-tile arrival: every thread issues its column's label loads,
+// then the z / r loads of its liquid cells, then folds in cell order.
+// k_dot_rz_finish folds each instance's partials in tile order afterwards.
+__global__ void __launch_bounds__(kThreads) k_dot_rz_part(const InstDev* insts, const Tile* tiles, int ntiles) {
+  __shared__ double sh[96];
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    const InstDev& I = insts[tl.inst];
+    if (I.ctrl->done) continue;   // uniform per CTA
+    const LevelDev& L = I.lv[0];
+    const float* __restrict__ r = static_cast<const float*>(L.rhs);
+    const float* __restrict__ z = static_cast<const float*>(L.z);
+    const uint8_t* __restrict__ lab = L.label;
+    double rz = 0, zs = 0, rs = 0;
+    const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
+    if (it.ok) {
+      const int sz = L.nx * L.ny, i0 = it.x + L.nx * (it.y + L.ny * it.z0);
+      uint8_t lb[kMaxDepth];
+      float zv[kMaxDepth], rv[kMaxDepth];
+#pragma unroll
+      for (int k = 0; k < kMaxDepth; ++k)
+        lb[k] = (k < it.depth && it.z0 + k < L.nz) ? lab[i0 + k * sz] : 0;
+#pragma unroll
+      for (int k = 0; k < kMaxDepth; ++k) {
+        zv[k] = lb[k] ? z[i0 + k * sz] : 0.0f;
+        rv[k] = lb[k] ? r[i0 + k * sz] : 0.0f;
+      }
+#pragma unroll
+      for (int k = 0; k < kMaxDepth; ++k) {
+        if (!lb[k]) continue;
+        const double zd = zv[k], rd = rv[k];
+        rz += rd * zd;
+        zs += zd;
+        rs += rd;
+      }
+    }
+    block_sum3(rz, zs, rs, sh);
+    if (threadIdx.x == 0) {
+      const int nt0 = I.ntiles0;
+      I.partial[0 * nt0 + tl.tile] = rz;
+      I.partial[1 * nt0 + tl.tile] = zs;
+      I.partial[2 * nt0 + tl.tile] = rs;
+    }
+  }
+}
+
+// gamma of each listed instance from its k_dot_rz_part partials (one CTA each).
+__global__ void __launch_bounds__(kThreads) k_dot_rz_finish(const InstDev* insts, const int* ilist) {
+  __shared__ double sh[32];
+  const InstDev& I = insts[ilist[blockIdx.x]];
+  Ctrl* c = I.ctrl;
+  if (c->done) return;
+  const int nt0 = I.ntiles0;
+  const double g = gather_slot(I.partial, 0, nt0, 0, sh);
+  const double zsum = gather_slot(I.partial, 1, nt0, 0, sh);
+  const double rsum = gather_slot(I.partial, 2, nt0, 0, sh);
+  if (threadIdx.x == 0) finish_gamma(c, g, zsum, rsum);
 }
 
 // d = (z - zmean) + beta d on liquid cells.

@@ -322,21 +322,27 @@ void vcycle_fused(fluid_pp_batch* B, int with_dot) {
     if (B->upm[l].n) {
       if (l == 0)
         FPP_LAUNCH(B, kPrUp0, k_up_m<float, float, T, T><<<B->upm[l].n, kMThreads, 0, s>>>(
-                                  B->d_insts, tl(B, B->upm[l]), 0, with_dot));
+                                  B->d_insts, tl(B, B->upm[l]), 0));
       else
-        FPP_LAUNCH(B, kPrUpC, k_up_m<T, T, T, T><<<B->upm[l].n, kMThreads, 0, s>>>(B->d_insts, tl(B, B->upm[l]), l, 0));
+        FPP_LAUNCH(B, kPrUpC, k_up_m<T, T, T, T><<<B->upm[l].n, kMThreads, 0, s>>>(B->d_insts, tl(B, B->upm[l]), l));
     }
     const List& Lu = B->up[l];
     if (!Lu.n) continue;
     if (l == 0)
-      FPP_LAUNCH(B, kPrUp0, k_up<float, float, T, T><<<Lu.n, kFThreads, B->smem_up, s>>>(B->d_insts, tl(B, Lu), 0,
-                                                                                          with_dot));
+      FPP_LAUNCH(B, kPrUp0, k_up<float, float, T, T><<<Lu.n, kFThreads, B->smem_up, s>>>(B->d_insts, tl(B, Lu), 0, 0));
     else
       FPP_LAUNCH(B, kPrUpC, k_up<T, T, T, T><<<Lu.n, kFThreads, B->smem_up, s>>>(B->d_insts, tl(B, Lu), l, 0));
   }
-  if (with_dot && B->l0single.n)
-    FPP_LAUNCH(B, kPrDot, k_dot_rz<<<launch_grid(B->l0single.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->l0single),
-                                                                                 B->l0single.n));
+  // gamma = r . (z - zmean) over the fixed level-0 tiles of every instance: its
+  // fold order does not depend on which up kernel (marching or box, chosen by
+  // how the batch fills the GPU) produced z, so a solve gives the same bits
+  // alone and in any batch
+  if (with_dot) {
+    FPP_LAUNCH(B, kPrDot, k_dot_rz_part<<<launch_grid(B->l0.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n));
+    // every instance: the multi-level list followed by the single-level one
+    FPP_LAUNCH(B, kPrDot, k_dot_rz_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(B->d_insts,
+                                                                                      il(B, B->multi)));
+  }
 }
 
 template <class T>
@@ -610,11 +616,21 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
       add_level(B->rst[l], [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; }, l + 1, true);
     if (l >= 1) add_level(B->crs[l], [l](const InstDev& I) { return l < I.nlev; }, l);
     auto grid_level = [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; };
-    // levels 0 and 1 coarsened by two on every axis take the marching steps
-    auto marching = [l](const InstDev& I) {
+    // levels 0 and 1 coarsened by two on every axis take the marching steps when
+    // the batch has enough of their tiles to fill the GPU (a lone small lattice
+    // keeps the box kernels, whose tile shape follows the lattice)
+    auto eligible = [l](const InstDev& I) {
       const LevelDev& C = I.lv[l + 1];
       return l <= kMarchLevels - 1 && C.sx == 2 && C.sy == 2 && C.sz == 2;
     };
+    long long march_total = 0;
+    for (int k = 0; k < count; ++k)
+      if (grid_level(insts[k]) && eligible(insts[k])) {
+        const LevelDev& C = insts[k].lv[l + 1];
+        march_total += march_down_tiles(C.nx, C.ny, C.nz);
+      }
+    const bool march_level = march_total >= kFillTiles;
+    auto marching = [&](const InstDev& I) { return march_level && eligible(I); };
     B->dn[l].off = int(tiles.size());
     for (int k = 0; k < count; ++k)
       if (grid_level(insts[k]) && !marching(insts[k]))
