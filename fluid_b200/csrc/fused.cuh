@@ -622,13 +622,20 @@ __host__ __device__ inline int march_up_tiles(int nx, int ny, int nz) {
   return ((nx + kUX - 1) / kUX) * ((ny + kUY - 1) / kUY) * ((nz + kUZ - 1) / kUZ);
 }
 
+// Rings of the marching up step (one barrier per step, as in k_down_m).
+constexpr int kURing = 5, kUZRing = 6;
+__host__ __device__ inline int march_up_smem_bytes() {
+  return (2 * kURing * kUEP + kUZRing * kUEP + 3 * kUQP) * 4 + kURing * kUEP;
+}
+
 template <class TZF, class TR, class TD, class TZC>
 __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, const Tile* tiles, int level) {
-  __shared__ float rhs_r[3][kUEP];
-  __shared__ float dg_r[3][kUEP];
-  __shared__ uint8_t lab_r[3][kUEP];
-  __shared__ float z_r[4][kUEP];
-  __shared__ float zc_r[3][kUQP];
+  extern __shared__ float smu[];
+  float* rhs_r = smu;                              // [kURing][kUEP]
+  float* dg_r = rhs_r + kURing * kUEP;             // [kURing][kUEP]
+  float* z_r = dg_r + kURing * kUEP;               // [kUZRing][kUEP]
+  float* zc_r = z_r + kUZRing * kUEP;              // [3][kUQP]
+  uint8_t* lab_r = reinterpret_cast<uint8_t*>(zc_r + 3 * kUQP);   // [kURing][kUEP]
   const Tile tl = tiles[blockIdx.x];
   const InstDev& I = insts[tl.inst];
   const Ctrl* c = I.ctrl;
@@ -701,7 +708,7 @@ __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, con
   }
   // coarse planes: Z goes to slot Z % 3
   auto load_coarse = [&](int Z) {
-    float* d = zc_r[Z % 3];
+    float* d = zc_r + (Z % 3) * kUQP;
     for (int e = t; e < qex * qey; e += kMThreads) {
       const int cxl = e % qex, cyl = e / qex;
       d[cxl + qex * cyl] = tof(zc[(qx0 + cxl) + C.nx * ((qy0 + cyl) + C.ny * Z)]);
@@ -732,8 +739,7 @@ __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, con
       }
     }
   };
-  auto slot3 = [&](int p) { return (p - pz0) % 3; };
-  auto slot4 = [&](int p) { return (p - pz0) & 3; };
+  auto sl = [&](int p, int n) { return (p - pz0) % n; };
   int zhi_loaded;
   {
     int cz[2];
@@ -744,11 +750,13 @@ __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, con
   }
   fetch(pz0);
   __syncthreads();
-  for (int p = pz0; p <= pz1; ++p) {
-    const int k = p - pz0;
+  for (int p = pz0; p <= pz1 + 2; ++p) {
     // stage plane p with the prolongated correction on liquid cells
-    {
-      const int sa = slot3(p), za = slot4(p);
+    if (p <= pz1) {
+      float* rh = rhs_r + sl(p, kURing) * kUEP;
+      float* dd = dg_r + sl(p, kURing) * kUEP;
+      uint8_t* lb = lab_r + sl(p, kURing) * kUEP;
+      float* zz = z_r + sl(p, kUZRing) * kUEP;
       int czs[2];
       float wzz[2];
       taps2(p, 2, C.nz, czs, wzz);
@@ -756,16 +764,16 @@ __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, con
       for (int kk = 0; kk < kUPer; ++kk) {
         const int e = t + kk * kMThreads;
         if (e >= kUEP) continue;
-        rhs_r[sa][e] = pr[kk];
-        dg_r[sa][e] = pd[kk];
-        lab_r[sa][e] = pl[kk];
+        rh[e] = pr[kk];
+        dd[e] = pd[kk];
+        lb[e] = pl[kk];
         float zv = pz_[kk];
         if (pl[kk]) {
           const int sx = int((qstep >> (2 * kk)) & 1u), sy = int((qstep >> (2 * kk + 1)) & 1u) * qex;
           float acc = 0.0f;
 #pragma unroll
           for (int c2 = 0; c2 < 2; ++c2) {
-            const float* q = zc_r[czs[c2] % 3] + qb[kk];
+            const float* q = zc_r + (czs[c2] % 3) * kUQP + qb[kk];
 #pragma unroll
             for (int c1 = 0; c1 < 2; ++c1)
 #pragma unroll
@@ -774,47 +782,55 @@ __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, con
           }
           zv = rnd<TZF>(zv + acc * unscale);
         }
-        z_r[za][e] = zv;
+        zz[e] = zv;
+      }
+      if (p < pz1) {
+        fetch(p + 1);
+        // the next plane's coarse planes: a new plane evicts one that neither
+        // this plane nor the next reads
+        const int need = coarse_hi(p + 1);
+        for (int Z = zhi_loaded + 1; Z <= need; ++Z) load_coarse(Z);
+        zhi_loaded = max(zhi_loaded, need);
       }
     }
-    if (p < pz1) fetch(p + 1);
-    __syncthreads();
-    // the next plane's coarse planes (their slots are free: plane p no longer reads them)
-    if (p < pz1) {
-      const int need = coarse_hi(p + 1);
-      for (int Z = zhi_loaded + 1; Z <= need; ++Z) load_coarse(Z);
-      zhi_loaded = max(zhi_loaded, need);
-    }
-    // black cells of plane q = p - 1 on T +- 1
-    if (k >= 2) {
-      const int q = p - 1, sq = slot3(q), zq = slot4(q), zm = slot4(q - 1), zp = slot4(p);
-      const float* zq_ = z_r[zq];
+    // black cells of plane q = p - 2 on T +- 1
+    const int q = p - 2;
+    if (q >= pz0 + 1 && q <= pz1 - 1) {
+      const float* rh = rhs_r + sl(q, kURing) * kUEP;
+      const float* dd = dg_r + sl(q, kURing) * kUEP;
+      const uint8_t* lb = lab_r + sl(q, kURing) * kUEP;
+      float* zq_ = z_r + sl(q, kUZRing) * kUEP;
+      const float* zm = z_r + sl(q - 1, kUZRing) * kUEP;
+      const float* zp = z_r + sl(q + 1, kUZRing) * kUEP;
 #pragma unroll
       for (int kk = 0; kk < kBPer; ++kk) {
         if (bs[kk] < 0) continue;
         const int s = bs[kk] + int((((bpar >> kk) ^ unsigned(q)) & 1u) ^ 1u);
-        if (!lab_r[sq][s]) continue;
+        if (!lb[s]) continue;
         const float nb = d4sum6(wx * zq_[s - 1], wx * zq_[s + 1], wy * zq_[s - kUEX], wy * zq_[s + kUEX],
-                                wz * z_r[zm][s], wz * z_r[zp][s]);
-        z_r[zq][s] = rnd<TZF>((rhs_r[sq][s] + nb) * __frcp_rn(dg_r[sq][s]));
+                                wz * zm[s], wz * zp[s]);
+        zq_[s] = rnd<TZF>((rh[s] + nb) * __frcp_rn(dd[s]));
       }
     }
-    __syncthreads();
-    // red cells of plane r = p - 2 on T, then the plane's output
-    if (k >= 4) {
-      const int r = p - 2, sr = slot3(r), zr = slot4(r), zm = slot4(r - 1), zp = slot4(r + 1);
-      const float* zr_ = z_r[zr];
+    // red cells of plane r = p - 4 on T, then the plane's output
+    const int r = p - 4;
+    if (r >= pz0 + 2 && r <= pz1 - 2) {
+      const float* rh = rhs_r + sl(r, kURing) * kUEP;
+      const float* dd = dg_r + sl(r, kURing) * kUEP;
+      const uint8_t* lb = lab_r + sl(r, kURing) * kUEP;
+      const float* zr_ = z_r + sl(r, kUZRing) * kUEP;
+      const float* zm = z_r + sl(r - 1, kUZRing) * kUEP;
+      const float* zp = z_r + sl(r + 1, kUZRing) * kUEP;
       const unsigned red = (r & 1) ? tpar : ~tpar;
       const bool rin = r < nz;
 #pragma unroll
       for (int kk = 0; kk < kTPer; ++kk) {
         const int s = ts_[kk];
         float zv = zr_[s];
-        const bool liq = lab_r[sr][s] != 0;
-        if (liq && ((red >> kk) & 1u))
-          zv = rnd<TZF>((rhs_r[sr][s] + d4sum6(wx * zr_[s - 1], wx * zr_[s + 1], wy * zr_[s - kUEX],
-                                               wy * zr_[s + kUEX], wz * z_r[zm][s], wz * z_r[zp][s])) *
-                        __frcp_rn(dg_r[sr][s]));
+        if (lb[s] && ((red >> kk) & 1u))
+          zv = rnd<TZF>((rh[s] + d4sum6(wx * zr_[s - 1], wx * zr_[s + 1], wy * zr_[s - kUEX], wy * zr_[s + kUEX],
+                                        wz * zm[s], wz * zp[s])) *
+                        __frcp_rn(dd[s]));
         if (rin && tofs[kk] >= 0) zo[tofs[kk] + nxy * r] = fromf<TZF>(zv);
       }
     }
@@ -887,6 +903,129 @@ __global__ void __launch_bounds__(kFThreads) k_dirspmv(const InstDev* insts, con
   if (arrive_last(&c->arrive[kStSpmv], nt0, &flag)) {
     const double delta = gather_slot(I.partial, 0, nt0, 0, sh);
     if (threadIdx.x == 0) {
+      finish_delta(c, delta);
+      c->dsel = sel ^ 1;
+    }
+  }
+}
+
+// ================================================ marching direction + SpMV
+// k_dirspmv as a 2.5-D march over tiles of kQX x kQY x kQZ level-0 cells: step
+// p stages d' = (z - zmean) + beta d of fine plane p on T +- 1 into a ring of
+// 4 planes (pointwise, from loads prefetched one step earlier), and applies
+// the operator to plane p - 2, whose neighbour planes earlier steps staged:
+// q = diag d' - (sum of the six neighbours' d'); it writes d' and q of T and
+// folds delta = d' . q.  One barrier per step.
+constexpr int kQX = 32, kQY = 16, kQZ = 16;
+constexpr int kQEX = kQX + 2, kQEY = kQY + 2, kQEP = kQEX * kQEY;
+constexpr int kQPer = (kQEP + kMThreads - 1) / kMThreads;
+constexpr int kQTPer = (kQX * kQY + kMThreads - 1) / kMThreads;
+
+__host__ __device__ inline int march_spmv_tiles(int nx, int ny, int nz) {
+  return ((nx + kQX - 1) / kQX) * ((ny + kQY - 1) / kQY) * ((nz + kQZ - 1) / kQZ);
+}
+
+__global__ void __launch_bounds__(kMThreads, 4) k_dirspmv_m(const InstDev* insts, const Tile* tiles) {
+  __shared__ float dn_r[4][kQEP];
+  __shared__ uint8_t lab_r[4][kQEP];
+  __shared__ double sh[32];
+  __shared__ int flag;
+  const Tile tl = tiles[blockIdx.x];
+  const InstDev& I = insts[tl.inst];
+  Ctrl* c = I.ctrl;
+  if (c->done) return;
+  const LevelDev& L = I.lv[0];
+  const int nx = L.nx, ny = L.ny, nz = L.nz, nxy = nx * ny;
+  const int ntx = (nx + kQX - 1) / kQX, nty = (ny + kQY - 1) / kQY;
+  const int tx = tl.tile % ntx, tr = tl.tile / ntx, ty = tr % nty, tz = tr / nty;
+  const int x0 = tx * kQX, y0 = ty * kQY, z0 = tz * kQZ;
+  const int ex0 = x0 - 1, ey0 = y0 - 1, pz0 = z0 - 1, pz1 = z0 + kQZ;
+  const int sel = c->dsel;
+  const float beta = float(c->beta), zm = float(c->zmean);
+  const float* __restrict__ z = static_cast<const float*>(L.z);
+  const float* __restrict__ dold = sel ? I.d2 : I.d;
+  float* __restrict__ dnew = sel ? I.d : I.d2;
+  const uint8_t* __restrict__ lab = L.label;
+  const float* __restrict__ dgl = L.diag;
+  float* __restrict__ Qo = I.q;
+  const int t = threadIdx.x;
+  int aoff[kQPer];
+#pragma unroll
+  for (int k = 0; k < kQPer; ++k) {
+    const int e = t + k * kMThreads;
+    const int gx = ex0 + e % kQEX, gy = ey0 + e / kQEX;
+    aoff[k] = (e < kQEP && gx >= 0 && gy >= 0 && gx < nx && gy < ny) ? gx + nx * gy : -1;
+  }
+  int ts_[kQTPer], tofs[kQTPer];
+#pragma unroll
+  for (int k = 0; k < kQTPer; ++k) {
+    const int e = t + k * kMThreads;
+    const int lx = e % kQX, ly = e / kQX, gx = x0 + lx, gy = y0 + ly;
+    ts_[k] = (ly + 1) * kQEX + lx + 1;
+    tofs[k] = (e < kQX * kQY && gx < nx && gy < ny) ? gx + nx * gy : -1;
+  }
+  float pz_[kQPer], pd_[kQPer];
+  uint8_t pl[kQPer];
+  auto fetch = [&](int p) {
+    const bool pin = p >= 0 && p < nz;
+#pragma unroll
+    for (int k = 0; k < kQPer; ++k) {
+      pz_[k] = 0.0f;
+      pd_[k] = 0.0f;
+      pl[k] = 0;
+      if (pin && aoff[k] >= 0) {
+        const int i = aoff[k] + nxy * p;
+        pl[k] = lab[i];
+        pz_[k] = z[i];
+        pd_[k] = dold[i];
+      }
+    }
+  };
+  auto sl = [&](int p) { return (p - pz0) & 3; };
+  double dq = 0.0;
+  fetch(pz0);
+  for (int p = pz0; p <= pz1 + 1; ++p) {
+    if (p <= pz1) {
+      float* dn = dn_r[sl(p)];
+      uint8_t* lb = lab_r[sl(p)];
+#pragma unroll
+      for (int k = 0; k < kQPer; ++k) {
+        const int e = t + k * kMThreads;
+        if (e >= kQEP) continue;
+        dn[e] = pl[k] ? (beta == 0.0f ? pz_[k] - zm : (pz_[k] - zm) + beta * pd_[k]) : 0.0f;
+        lb[e] = pl[k];
+      }
+      if (p < pz1) fetch(p + 1);
+    }
+    // operator on plane r = p - 2 (planes r - 1 .. r + 1 were staged by earlier steps)
+    const int r = p - 2;
+    if (r >= z0 && r < z0 + kQZ && r < nz) {
+      const float* dn = dn_r[sl(r)];
+      const float* dm = dn_r[sl(r - 1)];
+      const float* dp = dn_r[sl(r + 1)];
+      const uint8_t* lb = lab_r[sl(r)];
+#pragma unroll
+      for (int k = 0; k < kQTPer; ++k) {
+        if (tofs[k] < 0) continue;
+        const int s = ts_[k], i = tofs[k] + nxy * r;
+        const float dv = dn[s];
+        float q = 0.0f;
+        if (lb[s]) {
+          q = dgl[i] * dv - d4sum6(dn[s - 1], dn[s + 1], dn[s - kQEX], dn[s + kQEX], dm[s], dp[s]);
+          dq += double(dv) * q;
+        }
+        dnew[i] = dv;
+        Qo[i] = q;
+      }
+    }
+    __syncthreads();
+  }
+  const int nt = march_spmv_tiles(nx, ny, nz);
+  const double a0 = block_sum(dq, sh);
+  if (t == 0) I.partial[tl.tile] = a0;
+  if (arrive_last(&c->arrive[kStSpmv], nt, &flag)) {
+    const double delta = gather_slot(I.partial, 0, nt, 0, sh);
+    if (t == 0) {
       finish_delta(c, delta);
       c->dsel = sel ^ 1;
     }

@@ -98,6 +98,7 @@ struct fluid_pp_batch {
   List dn[kMaxLevels];       // fused down-step tiles (coarse tiles of level l+1) of grid level l
   List dnm[kMaxLevels];      // marching down-step tiles of grid level l (levels < kMarchLevels coarsened by two on every axis)
   List upm[kMaxLevels];      // marching up-step tiles (same condition)
+  List spm;                  // marching direction + SpMV tiles of level 0 (every instance)
   List up[kMaxLevels];       // fused up-step tiles (fine tiles of level l) of grid level l
   List l0single;             // level-0 tiles of single-level instances
   List bake;
@@ -321,10 +322,11 @@ void vcycle_fused(fluid_pp_batch* B, int with_dot) {
   for (int l = B->maxL - 2; l >= 0; --l) {
     if (B->upm[l].n) {
       if (l == 0)
-        FPP_LAUNCH(B, kPrUp0, k_up_m<float, float, T, T><<<B->upm[l].n, kMThreads, 0, s>>>(
+        FPP_LAUNCH(B, kPrUp0, k_up_m<float, float, T, T><<<B->upm[l].n, kMThreads, march_up_smem_bytes(), s>>>(
                                   B->d_insts, tl(B, B->upm[l]), 0));
       else
-        FPP_LAUNCH(B, kPrUpC, k_up_m<T, T, T, T><<<B->upm[l].n, kMThreads, 0, s>>>(B->d_insts, tl(B, B->upm[l]), l));
+        FPP_LAUNCH(B, kPrUpC, k_up_m<T, T, T, T><<<B->upm[l].n, kMThreads, march_up_smem_bytes(), s>>>(
+                                  B->d_insts, tl(B, B->upm[l]), l));
     }
     const List& Lu = B->up[l];
     if (!Lu.n) continue;
@@ -352,7 +354,7 @@ void iter_launch(fluid_pp_batch* B, int pre, int post) {
   const int n0 = B->l0.n, g = launch_grid(n0);
   if (pre == 1 && post == 1) {
     vcycle_fused<T>(B, 1);
-    FPP_LAUNCH(B, kPrDirSpmv, k_dirspmv<<<n0, kFThreads, 0, s>>>(B->d_insts, t0));
+    FPP_LAUNCH(B, kPrDirSpmv, k_dirspmv_m<<<B->spm.n, kMThreads, 0, s>>>(B->d_insts, tl(B, B->spm)));
     FPP_LAUNCH(B, kPrUpdate, k_update<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
     FPP_LAUNCH(B, kPrTrue, k_true_residual<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
     return;
@@ -500,6 +502,8 @@ static cudaError_t configure_kernels_t(size_t factor, size_t block, size_t down,
   if (e == cudaSuccess) e = set((const void*)k_down<T, T, T, T>, down);
   if (e == cudaSuccess) e = set((const void*)k_up<float, float, T, T>, up);
   if (e == cudaSuccess) e = set((const void*)k_up<T, T, T, T>, up);
+  if (e == cudaSuccess) e = set((const void*)k_up_m<float, float, T, T>, size_t(march_up_smem_bytes()));
+  if (e == cudaSuccess) e = set((const void*)k_up_m<T, T, T, T>, size_t(march_up_smem_bytes()));
   return e;
 }
 
@@ -659,6 +663,13 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
     B->upm[l].n = int(tiles.size()) - B->upm[l].off;
   }
   add_level(B->l0single, [](const InstDev& I) { return I.nlev == 1; }, 0);
+  B->spm.off = int(tiles.size());
+  for (int k = 0; k < count; ++k) {
+    const InstDev& I = B->h[k]->inst;
+    const int nt = march_spmv_tiles(I.lv[0].nx, I.lv[0].ny, I.lv[0].nz);
+    for (int t = 0; t < nt; ++t) tiles.push_back(Tile{k, 0, t, 0});
+  }
+  B->spm.n = int(tiles.size()) - B->spm.off;
   B->bake.off = int(tiles.size());
   for (int k = 0; k < count; ++k) {
     const InstDev& I = B->h[k]->inst;
