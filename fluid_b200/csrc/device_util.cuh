@@ -137,6 +137,31 @@ __device__ __forceinline__ void block_sum3(double& a, double& b, double& c, doub
   __syncthreads();
 }
 
+// block_sum of a and block_max of m in one pass (each keeps its own tree, so
+// the bits are those of the separate folds); sh holds 2 x 32 doubles.
+__device__ __forceinline__ void block_sum_max(double& a, double& m, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    sh[w] = a;
+    sh[32 + w] = m;
+  }
+  __syncthreads();
+  if (w == 0) {
+    const bool in = l < int(blockDim.x >> 5);
+    a = in ? sh[l] : 0.0;
+    m = in ? sh[32 + l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+  }
+  __syncthreads();
+}
+
 __device__ __forceinline__ double block_sum(double v, double* sh) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
