@@ -303,7 +303,8 @@ __global__ void __launch_bounds__(kMThreads, 4) k_down_m(const InstDev* insts, c
   const int cx0 = tx * kMX, cy0 = ty * kMY, cz0 = tz * kMZ;
   const int hx0 = 2 * cx0 - 3, hy0 = 2 * cy0 - 3;   // staged plane origin
   const int fx0 = 2 * cx0 - 1, fy0 = 2 * cy0 - 1;   // residual plane origin
-  const int pz0 = 2 * cz0 - 3, pz1 = 2 * (cz0 + kMZ) + 2;
+  // the march ends at the last coarse plane of the lattice: planes above it are air
+  const int pz0 = 2 * cz0 - 3, pz1 = 2 * min(cz0 + kMZ, C.nz) + 2;
   const TR* __restrict__ rhs = static_cast<const TR*>(F.rhs);
   const TD* __restrict__ dg = static_cast<const TD*>(F.diagT);
   const uint8_t* __restrict__ lab = F.label;
@@ -648,7 +649,7 @@ __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, con
   const int tx = tl.tile % ntx, tr = tl.tile / ntx, ty = tr % nty, tz = tr / nty;
   const int x0 = tx * kUX, y0 = ty * kUY, z0 = tz * kUZ;
   const int ex0 = x0 - 2, ey0 = y0 - 2;            // staged plane origin
-  const int pz0 = z0 - 2, pz1 = z0 + kUZ + 1;      // fine planes streamed
+  const int pz0 = z0 - 2, pz1 = min(z0 + kUZ, nz) + 1;   // fine planes streamed (none above the lattice)
   // coarse columns under the in-lattice part of the staged plane (k_up's cspan)
   auto cspan = [](int e0, int en, int nf, int nc, int& c0, int& cn) {
     const int lo = max(e0, 0), hi = min(e0 + en - 1, nf - 1);
@@ -939,7 +940,7 @@ __global__ void __launch_bounds__(kMThreads, 4) k_dirspmv_m(const InstDev* insts
   const int ntx = (nx + kQX - 1) / kQX, nty = (ny + kQY - 1) / kQY;
   const int tx = tl.tile % ntx, tr = tl.tile / ntx, ty = tr % nty, tz = tr / nty;
   const int x0 = tx * kQX, y0 = ty * kQY, z0 = tz * kQZ;
-  const int ex0 = x0 - 1, ey0 = y0 - 1, pz0 = z0 - 1, pz1 = z0 + kQZ;
+  const int ex0 = x0 - 1, ey0 = y0 - 1, pz0 = z0 - 1, pz1 = min(z0 + kQZ, nz);   // none above the lattice
   const int sel = c->dsel;
   const float beta = float(c->beta), zm = float(c->zmean);
   const float* __restrict__ z = static_cast<const float*>(L.z);
