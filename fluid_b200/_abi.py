@@ -35,6 +35,8 @@ EXPORTS = (
     "fluid_pp_tall_required_bytes", "fluid_pp_batch_set_graphs",
     "fluid_pp_set_allocation_cache", "fluid_pp_allocation_cache_bytes", "fluid_pp_reserve_allocation",
     "fluid_pp_tall_project_begin", "fluid_pp_tall_project_continue", "fluid_pp_tall_project_end",
+    "fluid_pp_batch_project_async", "fluid_pp_batch_receipts_read", "fluid_pp_download_async",
+    "fluid_pp_synchronize",
 )
 STAGES = ("reset", "label", "coarsen", "bake", "factor", "init", "smooth0", "smoothc", "residual0", "residualc",
           "restrict0", "restrictc", "coarse", "prolong0", "prolongc", "dot", "dir", "spmv", "update", "true",
@@ -111,6 +113,10 @@ def load():
     L.fluid_pp_batch_destroy.argtypes = [vp]
     L.fluid_pp_batch_destroy.restype = None
     L.fluid_pp_batch_project.argtypes = [vp, vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(Receipt)]
+    L.fluid_pp_batch_project_async.argtypes = [vp, vp, ctypes.POINTER(SolveOpts)]
+    L.fluid_pp_batch_receipts_read.argtypes = [vp, ctypes.POINTER(Receipt)]
+    L.fluid_pp_download_async.argtypes = [vp, vp, vp, vp, vp]
+    L.fluid_pp_synchronize.argtypes = [vp]
     L.fluid_pp_kernel_launches.argtypes = []
     L.fluid_pp_kernel_launches.restype = ctypes.c_ulonglong
     L.fluid_pp_set_profiling.argtypes = [vp, ci]

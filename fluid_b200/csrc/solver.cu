@@ -83,6 +83,7 @@ struct List {
 
 struct fluid_pp_batch {
   std::vector<fluid_pp*> h;
+  std::vector<float> dev_dt, dev_pscale;   // values last written into d_insts (NaN = not yet)
   int device = 0;
   int precision = 0;
   cudaStream_t stream = nullptr;
@@ -555,6 +556,8 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
     B->h.push_back(h);
     B->maxL = std::max(B->maxL, h->plan.levels);
   }
+  B->dev_dt.assign(count, std::nanf(""));
+  B->dev_pscale.assign(count, std::nanf(""));
   cudaSetDevice(B->device);
   // The batch's own copies of the instance descriptors.  Fused-kernel tile
   // shapes are chosen over the whole batch: the largest shape whose tiles,
@@ -764,10 +767,18 @@ static int batch_project_t(fluid_pp_batch* B, const float* dts, const fluid_pp_s
     h->last_dt = dt;
     h->inst.dt = dt;
     h->inst.pscale = h->cfg.rho * h->cfg.h / dt;
-    cudaMemcpyAsync(reinterpret_cast<char*>(B->d_insts + k) + offsetof(InstDev, dt), &h->inst.dt, sizeof(float),
-                    cudaMemcpyHostToDevice, B->stream);
-    cudaMemcpyAsync(reinterpret_cast<char*>(B->d_insts + k) + offsetof(InstDev, pscale), &h->inst.pscale,
-                    sizeof(float), cudaMemcpyHostToDevice, B->stream);
+    // only changed values cross: a copy from pageable memory may wait for the
+    // stream, which would stall a caller that keeps two batches in flight
+    if (!(B->dev_dt[k] == h->inst.dt)) {
+      cudaMemcpyAsync(reinterpret_cast<char*>(B->d_insts + k) + offsetof(InstDev, dt), &h->inst.dt, sizeof(float),
+                      cudaMemcpyHostToDevice, B->stream);
+      B->dev_dt[k] = h->inst.dt;
+    }
+    if (!(B->dev_pscale[k] == h->inst.pscale)) {
+      cudaMemcpyAsync(reinterpret_cast<char*>(B->d_insts + k) + offsetof(InstDev, pscale), &h->inst.pscale,
+                      sizeof(float), cudaMemcpyHostToDevice, B->stream);
+      B->dev_pscale[k] = h->inst.pscale;
+    }
   }
   bool graphed = false;
   if (!B->profiling && B->use_graphs) {
@@ -1148,6 +1159,11 @@ int fluid_pp_receipt_read(fluid_pp* pp, fluid_pp_receipt* receipt) {
 }
 
 int fluid_pp_download(fluid_pp* pp, float* p, float* u, float* v, float* w) {
+  const int rc = fluid_pp_download_async(pp, p, u, v, w);
+  return rc == FLUID_PP_OK ? fluid_pp_synchronize(pp) : rc;
+}
+
+int fluid_pp_download_async(fluid_pp* pp, float* p, float* u, float* v, float* w) {
   if (!pp) return FLUID_PP_INVALID_ARG;
   cudaSetDevice(pp->cfg.device);
   const long long nx = pp->cfg.nx, ny = pp->cfg.ny, nz = pp->cfg.nz;
@@ -1157,8 +1173,15 @@ int fluid_pp_download(fluid_pp* pp, float* p, float* u, float* v, float* w) {
   if (u && e == cudaSuccess) e = cudaMemcpyAsync(u, I.u, 4 * (nx + 1) * ny * nz, cudaMemcpyDeviceToHost, pp->stream);
   if (v && e == cudaSuccess) e = cudaMemcpyAsync(v, I.v, 4 * nx * (ny + 1) * nz, cudaMemcpyDeviceToHost, pp->stream);
   if (w && e == cudaSuccess) e = cudaMemcpyAsync(w, I.w, 4 * nx * ny * (nz + 1), cudaMemcpyDeviceToHost, pp->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(pp->stream);
   if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("download: ") + cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_synchronize(fluid_pp* pp) {
+  if (!pp) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(pp->cfg.device);
+  const cudaError_t e = cudaStreamSynchronize(pp->stream);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("synchronize: ") + cudaGetErrorString(e));
   return FLUID_PP_OK;
 }
 
@@ -1184,6 +1207,7 @@ int fluid_pp_prepare(fluid_pp* pp, float dt) {
   pp->last_dt = dt;
   cudaMemcpyAsync(reinterpret_cast<char*>(B->d_insts) + offsetof(InstDev, dt), &pp->inst.dt, sizeof(float),
                   cudaMemcpyHostToDevice, B->stream);
+  B->dev_dt[0] = pp->inst.dt;
   const fluid_pp_solve_opts o = default_opts();
   switch (B->precision) {
     case FLUID_PP_FP16: setup_launch<__half>(B, o); break;
@@ -1345,6 +1369,43 @@ int fluid_pp_batch_project(fluid_pp_batch* B, const float* dts, const fluid_pp_s
   const int rc = batch_project(B, dts, opts, true, receipts);
   if (rc != FLUID_PP_OK && rc != FLUID_PP_NONCONVERGENCE && rc != FLUID_PP_NONFINITE) g_err = B->err;
   return rc;
+}
+
+int fluid_pp_batch_project_async(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts* opts) {
+  if (!B) return FLUID_PP_INVALID_ARG;
+  if (dts)
+    for (size_t k = 0; k < B->h.size(); ++k)
+      if (!(dts[k] > 0) || !std::isfinite(dts[k])) {
+        B->err = "dt must be positive and finite";
+        g_err = B->err;
+        return FLUID_PP_INVALID_ARG;
+      }
+  const int rc = batch_project(B, dts, opts, false, nullptr);
+  if (rc != FLUID_PP_OK) g_err = B->err;
+  return rc;
+}
+
+int fluid_pp_batch_receipts_read(fluid_pp_batch* B, fluid_pp_receipt* receipts) {
+  if (!B) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(B->device);
+  const cudaError_t e = cudaStreamSynchronize(B->stream);
+  if (e != cudaSuccess) {
+    B->err = std::string("project: ") + cudaGetErrorString(e);
+    g_err = B->err;
+    return FLUID_PP_CUDA;
+  }
+  if (B->pending_graph_count) {
+    g_launches.fetch_add((unsigned long long)(*B->h_loop) * B->n_body, std::memory_order_relaxed);
+    B->pending_graph_count = false;
+  }
+  int worst = FLUID_PP_OK;
+  for (size_t k = 0; k < B->h.size(); ++k) {
+    if (receipts) fill_receipt(B->h[k], B->h_ctrl[k], receipts + k);
+    B->h[k]->has_pressure = true;
+    if (B->h_ctrl[k].status != FLUID_PP_OK && worst == FLUID_PP_OK) worst = B->h_ctrl[k].status;
+  }
+  prof_collect(B);
+  return worst;
 }
 
 }  // extern "C"

@@ -155,6 +155,26 @@ class PressureProjector:
         _check(load().fluid_pp_download(self._h, ptr(p), ptr(u), ptr(v), ptr(w)), self._h, "download")
         return p, u, v, w
 
+    def download_async(self, p, u, v, w):
+        """Enqueues the result copies into the caller's arrays (pinned memory, for
+        overlap) on the handle's stream; they hold the results after
+        ``synchronize()``.  Any array may be None."""
+        nx, ny, nz = self.dims
+        shapes = ((nz, ny, nx), (nz, ny, nx + 1), (nz, ny + 1, nx), (nz + 1, ny, nx))
+        ptrs = []
+        for a, shp, name in zip((p, u, v, w), shapes, ("p", "u", "v", "w")):
+            if a is None:
+                ptrs.append(None)
+                continue
+            if a.dtype != np.float32 or a.size != int(np.prod(shp)) or not a.flags.c_contiguous:
+                raise ValueError(f"{name} must be a C-contiguous float32 array of {int(np.prod(shp))} entries")
+            ptrs.append(ptr(a))
+        _check(load().fluid_pp_download_async(self._h, *ptrs), self._h, "download_async")
+
+    def synchronize(self):
+        """Waits for everything enqueued on the handle's stream."""
+        _check(load().fluid_pp_synchronize(self._h), self._h, "synchronize")
+
     def device_arrays(self) -> dict:
         ps = [ctypes.c_void_p() for _ in range(5)]
         _check(load().fluid_pp_device_arrays(self._h, *(ctypes.byref(p) for p in ps)), self._h)
@@ -249,3 +269,86 @@ class BatchProjector:
         if rc not in (_abi.OK, _abi.NONCONVERGENCE, _abi.NONFINITE):
             _check(rc, None, "batch_project")
         return [r.as_dict() for r in rec]
+
+    def project_async(self, dts, **opts):
+        """Enqueues the batched projection on the batch's stream (the first
+        projector's) and returns; ``receipts()`` waits and reads them."""
+        o = solve_opts(**opts)
+        n = len(self.projectors)
+        dt = np.ascontiguousarray(np.broadcast_to(np.asarray(dts, np.float32), (n,)))
+        _check(load().fluid_pp_batch_project_async(self._b, ptr(dt), ctypes.byref(o)), None, "batch_project_async")
+
+    def receipts(self):
+        n = len(self.projectors)
+        rec = (Receipt * n)()
+        rc = load().fluid_pp_batch_receipts_read(self._b, rec)
+        if rc not in (_abi.OK, _abi.NONCONVERGENCE, _abi.NONFINITE):
+            _check(rc, None, "batch_receipts")
+        return [r.as_dict() for r in rec]
+
+
+class PipelinedBatchProjector:
+    """Batches of the same lattices used in turn, each on its own CUDA stream.
+
+    A serving host that projects many independent simulations per tick submits
+    a full set of host inputs per tick; while one batch solves, the next
+    batch's inputs and the previous batch's results cross PCIe on the other
+    stream's copy queue.  ``submit`` enqueues upload -> batched projection ->
+    read-back on the next slot (first waiting for that slot's previous tick)
+    and returns a ticket; ``result(ticket)`` waits for it and returns the
+    receipts.  Inputs must stay untouched and outputs unread until the
+    ticket's result is taken; both should be pinned host memory, or the copies
+    run synchronously.  Results are those of ``BatchProjector.project``.
+    """
+
+    def __init__(self, projector_sets):
+        self.sets = [list(s) for s in projector_sets]
+        if len(self.sets) < 2 or any(len(s) != len(self.sets[0]) for s in self.sets):
+            raise ValueError("need at least two projector sets of equal size")
+        for s in self.sets[1:]:
+            if [p.dims for p in s] != [p.dims for p in self.sets[0]]:
+                raise ValueError("projector sets must hold the same lattices in the same order")
+        self.batches = [BatchProjector(s) for s in self.sets]
+        self._pending = [None] * len(self.sets)   # ticket in flight per slot
+        self._done = {}
+        self._next = 0
+
+    def destroy(self):
+        for t in list(self._pending):
+            if t is not None:
+                self.result(t)
+        for b in self.batches:
+            b.destroy()
+        self.batches = []
+
+    def _drain(self, slot):
+        t = self._pending[slot]
+        if t is not None:
+            self._done[t] = self.batches[slot].receipts()
+            self._pending[slot] = None
+
+    def submit(self, inputs, outputs, dts, **opts) -> int:
+        """inputs: per lattice (vof, u, v, w); outputs: per lattice (p, u, v, w)
+        arrays (any may be None) that receive the results."""
+        t = self._next
+        slot = t % len(self.sets)
+        self._drain(slot)
+        projs = self.sets[slot]
+        if len(inputs) != len(projs) or len(outputs) != len(projs):
+            raise ValueError(f"need {len(projs)} inputs and outputs")
+        for p, arrs in zip(projs, inputs):
+            p.upload_state(*arrs)
+        self.batches[slot].project_async(dts, **opts)
+        for p, arrs in zip(projs, outputs):
+            p.download_async(*arrs)
+        self._pending[slot] = t
+        self._next = t + 1
+        return t
+
+    def result(self, ticket: int):
+        for slot, t in enumerate(self._pending):
+            if t == ticket:
+                self._drain(slot)
+        if ticket not in self._done:
+            raise KeyError(f"ticket {ticket} was never submitted or its result was already taken")
+        return self._done.pop(ticket)

@@ -143,6 +143,14 @@ int fluid_pp_receipt_read(fluid_pp* pp, fluid_pp_receipt* receipt);
  * Replaces the pressureTexture / velocity readback (webgpu-uniform-pressure-multigrid.ts:303). */
 int fluid_pp_download(fluid_pp* pp, float* p, float* u, float* v, float* w);
 
+/* fluid_pp_download without the wait: enqueues the copies on the handle's
+ * stream and returns.  The host buffers must stay valid, and hold the results
+ * only after fluid_pp_synchronize (or any later wait on that stream); pinned
+ * buffers let the copies overlap work on other streams. */
+int fluid_pp_download_async(fluid_pp* pp, float* p, float* u, float* v, float* w);
+/* Waits for everything enqueued on the handle's stream. */
+int fluid_pp_synchronize(fluid_pp* pp);
+
 /* Device pointers of the resident arrays (for zero-copy consumers); any may be NULL. */
 int fluid_pp_device_arrays(fluid_pp* pp, float** p, float** u, float** v, float** w, float** vof);
 
@@ -166,6 +174,17 @@ int fluid_pp_batch_create(fluid_pp* const* handles, int count, fluid_pp_batch** 
 void fluid_pp_batch_destroy(fluid_pp_batch* batch);
 int fluid_pp_batch_project(fluid_pp_batch* batch, const float* dts, const fluid_pp_solve_opts* opts,
                            fluid_pp_receipt* receipts);
+
+/* Asynchronous batch form: enqueues the projection on the batch's stream (its
+ * first handle's stream) and returns.  fluid_pp_batch_receipts_read waits for
+ * that stream, fills `receipts` (one per handle; may be NULL) and returns what
+ * fluid_pp_batch_project would have.  The batch only orders work on its own
+ * stream: uploads and downloads of its handles belong on that stream too.  With
+ * graphs on (the default) nothing waits on the host between the two calls, so a
+ * caller can keep two batches on two streams in flight, the copies of one
+ * overlapping the solve of the other. */
+int fluid_pp_batch_project_async(fluid_pp_batch* batch, const float* dts, const fluid_pp_solve_opts* opts);
+int fluid_pp_batch_receipts_read(fluid_pp_batch* batch, fluid_pp_receipt* receipts);
 
 /* Solve a batch through CUDA graphs (on = 1, the default: the solve is captured
  * once per option set and replayed) or with direct launches (on = 0: for a batch

@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from fluid_b200 import BatchProjector, PressureProjector, configs
+from fluid_b200 import BatchProjector, PipelinedBatchProjector, PressureProjector, configs
 from oracle.oracle import Oracle
 
 pytestmark = pytest.mark.gpu
@@ -216,6 +216,63 @@ def test_marching_batch_is_identical_to_box_singles():
     batch.destroy()
     for pp in pps:
         pp.destroy()
+
+
+def test_pipelined_ticks_match_synchronous_batches():
+    """Four ticks of three lattices through PipelinedBatchProjector (two streams,
+    two ticks in flight, pinned host buffers) give the receipts and the p, u, v, w
+    of BatchProjector.project on each tick's inputs, bit for bit."""
+    import torch
+    dims = [(40, 32, 36), (24, 20, 26), (33, 17, 29)]
+    ticks = [[configs.random_small(nx, ny, nz, seed=300 + 10 * t + k) for k, (nx, ny, nz) in enumerate(dims)]
+             for t in range(4)]
+    s0 = ticks[0]
+
+    def make_set():
+        return [PressureProjector((s.nx, s.ny, s.nz), s.h, precision="fp16") for s in s0]
+
+    ref = []
+    pps = make_set()
+    batch = BatchProjector(pps)
+    for states in ticks:
+        for pp, s in zip(pps, states):
+            pp.upload_state(s.vof, s.u, s.v, s.w)
+        recs = batch.project([s.dt for s in states])
+        ref.append((recs, [pp.download() for pp in pps]))
+    batch.destroy()
+    for pp in pps:
+        pp.destroy()
+
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    sets = [make_set(), make_set()]
+    for st, ps in zip(streams, sets):
+        for pp in ps:
+            pp.set_stream(st.cuda_stream)
+    pipe = PipelinedBatchProjector(sets)
+
+    def pinned(a):
+        return torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory().numpy()
+
+    ins = [[tuple(pinned(a) for a in (s.vof, s.u, s.v, s.w)) for s in states] for states in ticks]
+    outs = [[tuple(pinned(np.zeros(shp, np.float32)) for shp in
+                   ((nz, ny, nx), (nz, ny, nx + 1), (nz, ny + 1, nx), (nz + 1, ny, nx)))
+             for (nx, ny, nz) in dims] for _ in ticks]
+    tickets = [pipe.submit(ins[t], outs[t], [s.dt for s in ticks[t]]) for t in range(len(ticks))]
+    for t, ticket in enumerate(tickets):
+        recs = pipe.result(ticket)
+        ref_recs, ref_fields = ref[t]
+        for r1, r2 in zip(ref_recs, recs):
+            assert r2["status_name"] == "OK"
+            assert r1["iterations"] == r2["iterations"]
+        for f1, f2 in zip(ref_fields, outs[t]):
+            for a, b in zip(f1, f2):
+                np.testing.assert_array_equal(a, b)
+    with pytest.raises(KeyError):
+        pipe.result(tickets[0])
+    pipe.destroy()
+    for ps in sets:
+        for pp in ps:
+            pp.destroy()
 
 
 def test_handles_created_large_first_solve_alone():
