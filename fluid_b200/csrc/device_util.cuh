@@ -162,6 +162,43 @@ __device__ __forceinline__ void block_sum_max(double& a, double& m, double* sh) 
   __syncthreads();
 }
 
+// NS block_sum folds and NM block_max folds in one pass (every value keeps its
+// separate fold's tree, so the bits are those folds'); sh holds (NS + NM) x 32
+// doubles.  Results valid in warp 0.
+template <int NS, int NM>
+__device__ __forceinline__ void block_folds(double* s, double* m, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int k = 0; k < NS; ++k) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
+#pragma unroll
+    for (int k = 0; k < NM; ++k) m[k] = fmax(m[k], __shfl_xor_sync(0xffffffffu, m[k], o));
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+#pragma unroll
+    for (int k = 0; k < NS; ++k) sh[32 * k + w] = s[k];
+#pragma unroll
+    for (int k = 0; k < NM; ++k) sh[32 * (NS + k) + w] = m[k];
+  }
+  __syncthreads();
+  if (w == 0) {
+    const bool in = l < int(blockDim.x >> 5);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) s[k] = in ? sh[32 * k + l] : 0.0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) m[k] = in ? sh[32 * (NS + k) + l] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int k = 0; k < NS; ++k) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
+#pragma unroll
+      for (int k = 0; k < NM; ++k) m[k] = fmax(m[k], __shfl_xor_sync(0xffffffffu, m[k], o));
+    }
+  }
+  __syncthreads();
+}
+
 __device__ __forceinline__ double block_sum(double v, double* sh) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -358,7 +395,9 @@ __device__ __forceinline__ void finish_true(Ctrl* c, double s, double m) {
 
 // In-place Gauss-Jordan inverse of an SPD m x m matrix in shared memory (no
 // pivoting needed), all threads of the CTA; prow/pcol hold m doubles each.
+// Rows go to warps and columns to lanes, so no thread divides an index.
 __device__ __forceinline__ void gauss_jordan_inplace(double* A, int m, double* prow, double* pcol) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (int k = 0; k < m; ++k) {
     const double piv = A[k * m + k];
     for (int j = threadIdx.x; j < m; j += blockDim.x) {
@@ -366,10 +405,14 @@ __device__ __forceinline__ void gauss_jordan_inplace(double* A, int m, double* p
       pcol[j] = A[j * m + k];
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-      const int i = e / m, j = e - i * m;
-      if (i == k) A[e] = prow[j];
-      else A[e] = ((j == k) ? 0.0 : A[e]) - pcol[i] * prow[j];
+    for (int i = warp; i < m; i += nwarps) {
+      double* row = A + i * m;
+      if (i == k) {
+        for (int j = lane; j < m; j += 32) row[j] = prow[j];
+      } else {
+        const double pc = pcol[i];
+        for (int j = lane; j < m; j += 32) row[j] = ((j == k) ? 0.0 : row[j]) - pc * prow[j];
+      }
     }
     __syncthreads();
   }

@@ -12,51 +12,84 @@
 
 namespace fpp {
 
+// Column helper: calls f(k, z, i) for the thread's valid cells of its tile
+// column (TileIt's cells, in the same order), fully unrolled so the loads of
+// all the column's cells are in flight together.
+template <class F>
+__device__ __forceinline__ void for_column(const TileIt& it, int nx, int ny, int nz, F f) {
+  if (!it.ok) return;
+  const int sz = nx * ny;
+  const int i0 = it.x + nx * (it.y + ny * it.z0);
+#pragma unroll
+  for (int k = 0; k < kMaxDepth; ++k)
+    if (k < it.depth && it.z0 + k < nz) f(k, it.z0 + k, i0 + k * sz);
+}
+
 // ================================================================= setup
 // Level 0: labels, level set and right-hand side from the VOF and MAC velocities
 // (ref.wgsl.ts:208-242 labelling; divergenceAt :1010-1024 with closed walls
 // carrying no flux; mgBuildFinestRhs mg.wgsl.ts:152-167 in finest-cell units).
-__global__ void k_label_rhs(const InstDev* insts, const Tile* tiles, int ntiles, int warm) {
+__global__ void __launch_bounds__(kThreads, 2) k_label_rhs(const InstDev* insts, const Tile* tiles, int ntiles,
+                                                         int warm) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
     const LevelDev& L = I.lv[0];
     int liquid = 0, air = 0, top = 0, bad = 0;
-    const long long uS = I.nx + 1, vS = I.ny + 1;
-    int x, y, z, i;
-    for (TileIt it(tl.tile, I.nx, I.ny, I.nz, L.depth); it.next(x, y, z, i);) {
-      const float rho = I.vof[i];
-      const bool liq = rho > 0.5f;
-      L.label[i] = liq ? 1 : 0;
-      L.phi[i] = 0.5f - rho;
-      const float up = I.u[x + 1 + uS * (y + (long long)I.ny * z)];
-      const float um = I.u[x + uS * (y + (long long)I.ny * z)];
-      const float vp = I.v[x + (long long)I.nx * (y + 1 + vS * z)];
-      const float vm = I.v[x + (long long)I.nx * (y + vS * z)];
-      const float wp = I.w[i + (long long)I.nx * I.ny];
-      const float wm = I.w[i];
-      bad |= !(isfinite(rho) && isfinite(up) && isfinite(um) && isfinite(vp) && isfinite(vm) && isfinite(wp) &&
-               isfinite(wm));
+    const int nx = I.nx, ny = I.ny, nz = I.nz;
+    const long long uS = nx + 1, vS = ny + 1, sz = (long long)nx * ny;
+    const float* __restrict__ vof = I.vof;
+    const float* __restrict__ U = I.u;
+    const float* __restrict__ V = I.v;
+    const float* __restrict__ W = I.w;
+    uint8_t* __restrict__ lab = L.label;
+    float* __restrict__ phi = L.phi;
+    float* __restrict__ B = I.b;
+    float* __restrict__ X = I.x;
+    float* __restrict__ Xlo = I.xlo;
+    const bool open_top = I.open_top;
+    const float hdt = I.h / I.dt;
+    const TileIt it(tl.tile, nx, ny, nz, L.depth);
+    const int x = it.x, y = it.y;
+    // every load of the column first, then the arithmetic and the stores
+    float rho[kMaxDepth], up[kMaxDepth], um[kMaxDepth], vp[kMaxDepth], vm[kMaxDepth], wp[kMaxDepth], wm[kMaxDepth];
+    for_column(it, nx, ny, nz, [&](int k, int z, int i) {
+      const long long ur = uS * (y + (long long)ny * z);
+      rho[k] = vof[i];
+      up[k] = U[x + 1 + ur];
+      um[k] = U[x + ur];
+      vp[k] = V[x + (long long)nx * (y + 1 + vS * z)];
+      vm[k] = V[x + (long long)nx * (y + vS * z)];
+      wp[k] = W[i + sz];
+      wm[k] = W[i];
+    });
+    for_column(it, nx, ny, nz, [&](int k, int z, int i) {
+      const float r = rho[k];
+      const bool liq = r > 0.5f;
+      lab[i] = liq ? 1 : 0;
+      phi[i] = 0.5f - r;
+      bad |= !(isfinite(r) && isfinite(up[k]) && isfinite(um[k]) && isfinite(vp[k]) && isfinite(vm[k]) &&
+               isfinite(wp[k]) && isfinite(wm[k]));
       float b = 0.0f;
       if (liq) {
-        const float fxp = x + 1 < I.nx ? up : 0.0f, fxm = x > 0 ? um : 0.0f;
-        const float fyp = (y + 1 < I.ny || I.open_top) ? vp : 0.0f, fym = y > 0 ? vm : 0.0f;
-        const float fzp = z + 1 < I.nz ? wp : 0.0f, fzm = z > 0 ? wm : 0.0f;
+        const float fxp = x + 1 < nx ? up[k] : 0.0f, fxm = x > 0 ? um[k] : 0.0f;
+        const float fyp = (y + 1 < ny || open_top) ? vp[k] : 0.0f, fym = y > 0 ? vm[k] : 0.0f;
+        const float fzp = z + 1 < nz ? wp[k] : 0.0f, fzm = z > 0 ? wm[k] : 0.0f;
         const float div = ((fxp - fxm) + (fzp - fzm)) + (fyp - fym);
         float q = 0.0f;   // cm12VolumeCorrectionDivergence * h (cm12-numerics.ts:127-138)
-        if (rho > 1.0f) q = fminf(fminf(0.5f * (rho - 1.0f), 1.0f), I.h / I.dt);
+        if (r > 1.0f) q = fminf(fminf(0.5f * (r - 1.0f), 1.0f), hdt);
         b = -(div - q);
         ++liquid;
-        top += (y == I.ny - 1);
+        top += (y == ny - 1);
       } else {
         ++air;
       }
-      I.b[i] = b;
+      B[i] = b;
       if (!(warm && liq)) {
-        I.x[i] = 0.0f;
-        I.xlo[i] = 0.0f;
+        X[i] = 0.0f;
+        Xlo[i] = 0.0f;
       }
-    }
+    });
     // integer counts are order independent
     for (int o = 16; o > 0; o >>= 1) {
       liquid += __shfl_xor_sync(0xffffffffu, liquid, o);
@@ -149,7 +182,7 @@ __global__ void k_bake_diag(const InstDev* insts, const Tile* tiles, int ntiles)
 // Air cells are identity rows; a level without Dirichlet contact gets the
 // rank-one term mean(diag)/m * 1 1^T so the inverse is SPD.
 template <class TD>
-__global__ void k_coarse_factor(const InstDev* insts, const int* list) {
+__global__ void __launch_bounds__(kBlockThreads) k_coarse_factor(const InstDev* insts, const int* list) {
   extern __shared__ double A[];
   const InstDev& I = insts[list[blockIdx.x]];
   const LevelDev& L = I.lv[I.nlev - 1];
@@ -203,83 +236,101 @@ __global__ void k_coarse_factor(const InstDev* insts, const int* list) {
 enum Stage { kStInit = 0, kStGamma = 1, kStSpmv = 2, kStUpdate = 3, kStTrue = 4, kStReceipt = 5 };
 
 
-// r = b - A x (x already masked to liquid), bb, sums for the nullspace.
-__global__ void k_cg_init(const InstDev* insts, const Tile* tiles, int ntiles, double rel_tol, double abs_tol,
-                          int max_iter, int true_every, int warm, double rel_tol_inf) {
-  __shared__ double sh[32];
-  __shared__ int flag;
+// r = b - A x (x already masked to liquid) and the tile's partials of b.b,
+// sum b, r.r, max|b|, max|r|; k_cg_init_finish folds them per instance in tile
+// order afterwards.
+__global__ void __launch_bounds__(kThreads) k_cg_init_part(const InstDev* insts, const Tile* tiles, int ntiles,
+                                                            int warm) {
+  __shared__ double sh[5 * 32];
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
-    Ctrl* c = I.ctrl;
     const LevelDev& L = I.lv[0];
-    float* r = static_cast<float*>(L.rhs);
-    double sbb = 0, sb = 0, srr = 0, mb = 0, mr = 0;
-    const int sy = L.nx, sz = L.nx * L.ny;
-    int x, y, z, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth); it.next(x, y, z, i);) {
-      const float b = I.b[i];
+    float* __restrict__ r = static_cast<float*>(L.rhs);
+    const float* __restrict__ B = I.b;
+    const uint8_t* __restrict__ lab = L.label;
+    const int nx = L.nx, ny = L.ny, nz = L.nz, sy = nx, sz = nx * ny;
+    double sums[3] = {0, 0, 0}, maxes[2] = {0, 0};   // bb, b, rr; max|b|, max|r|
+    const TileIt it(tl.tile, nx, ny, nz, L.depth);
+    const int x = it.x, y = it.y;
+    float bv[kMaxDepth];
+    uint8_t lb[kMaxDepth];
+    for_column(it, nx, ny, nz, [&](int k, int, int i) {
+      bv[k] = B[i];
+      lb[k] = warm ? lab[i] : 0;
+    });
+    for_column(it, nx, ny, nz, [&](int k, int z, int i) {
+      const float b = bv[k];
       float rv = b;
-      if (warm && L.label[i]) {
+      if (lb[k]) {
         auto X = [&](int j) { return double(I.x[j]) + double(I.xlo[j]); };
-        auto nb = [&](bool in, int j) { return (in && L.label[j]) ? X(j) : 0.0; };
-        const double s = ((nb(x > 0, i - 1) + nb(x + 1 < L.nx, i + 1)) + (nb(z > 0, i - sz) + nb(z + 1 < L.nz, i + sz))) +
-                         (nb(y > 0, i - sy) + nb(y + 1 < L.ny, i + sy));
+        auto nb = [&](bool in, int j) { return (in && lab[j]) ? X(j) : 0.0; };
+        const double s = ((nb(x > 0, i - 1) + nb(x + 1 < nx, i + 1)) + (nb(z > 0, i - sz) + nb(z + 1 < nz, i + sz))) +
+                         (nb(y > 0, i - sy) + nb(y + 1 < ny, i + sy));
         rv = float(double(b) - (double(L.diag[i]) * X(i) - s));
       }
       r[i] = rv;
-      sbb += double(b) * b;
-      sb += b;
-      srr += double(rv) * rv;
-      mb = fmax(mb, fabs(double(b)));
-      mr = fmax(mr, fabs(double(rv)));
-    }
-    const double a0 = block_sum(sbb, sh), a1 = block_sum(sb, sh), a2 = block_sum(srr, sh);
-    const double a3 = block_max(mb, sh), a4 = block_max(mr, sh);
+      sums[0] += double(b) * b;
+      sums[1] += b;
+      sums[2] += double(rv) * rv;
+      maxes[0] = fmax(maxes[0], fabs(double(b)));
+      maxes[1] = fmax(maxes[1], fabs(double(rv)));
+    });
+    block_folds<3, 2>(sums, maxes, sh);
     if (threadIdx.x == 0) {
-      I.partial[0 * I.ntiles0 + tl.tile] = a0;
-      I.partial[1 * I.ntiles0 + tl.tile] = a1;
-      I.partial[2 * I.ntiles0 + tl.tile] = a2;
-      I.partial[3 * I.ntiles0 + tl.tile] = a3;
-      I.partial[4 * I.ntiles0 + tl.tile] = a4;
+      I.partial[0 * I.ntiles0 + tl.tile] = sums[0];
+      I.partial[1 * I.ntiles0 + tl.tile] = sums[1];
+      I.partial[2 * I.ntiles0 + tl.tile] = sums[2];
+      I.partial[3 * I.ntiles0 + tl.tile] = maxes[0];
+      I.partial[4 * I.ntiles0 + tl.tile] = maxes[1];
     }
-    if (arrive_last(&c->arrive[kStInit], I.ntiles0, &flag)) {
-      const double bb = gather_slot(I.partial, 0, I.ntiles0, 0, sh);
-      const double bs = gather_slot(I.partial, 1, I.ntiles0, 0, sh);
-      const double rr = gather_slot(I.partial, 2, I.ntiles0, 0, sh);
-      const double bmax = gather_slot(I.partial, 3, I.ntiles0, 1, sh);
-      const double rmax = gather_slot(I.partial, 4, I.ntiles0, 1, sh);
-      if (threadIdx.x == 0) {
-        c->anchored = (c->air > 0) || (I.open_top && c->top_liquid > 0);
-        const double nliq = double(c->liquid > 0 ? c->liquid : 1);
-        c->bmean = c->anchored ? 0.0 : bs / nliq;
-        c->bb = bb - (c->anchored ? 0.0 : nliq * c->bmean * c->bmean);
-        c->rr = rr - (c->anchored ? 0.0 : nliq * c->bmean * c->bmean);
-        if (c->bb < 0) c->bb = 0;
-        if (c->rr < 0) c->rr = 0;
-        const double thr = fmax(abs_tol, rel_tol * sqrt(c->bb));
-        c->thr2 = thr * thr;
-        c->bmax = bmax;
-        c->rmax = rmax;
-        c->thr_inf = rel_tol_inf > 0 ? rel_tol_inf * bmax : 0.0;
-        c->iter = 0;
-        c->max_iter = max_iter;
-        c->true_every = true_every;
-        c->first = 1;
-        c->candidate = 0;
-        c->converged = 0;
-        c->done = 0;
-        c->status = FLUID_PP_OK;
-        c->rr_true = c->rr;
-        set_sigma(c, c->rr);
-        if (c->nonfinite) {
-          c->done = 1;
-          c->status = FLUID_PP_NONFINITE;
-        } else if (c->liquid == 0 || (c->rr <= c->thr2 && (c->thr_inf <= 0 || c->rmax <= c->thr_inf))) {
-          c->done = 1;   // nothing to solve, or the initial guess already satisfies the tolerance
-          c->converged = 1;
-        }
-      }
+  }
+}
+
+// CG scalars of each listed instance from its k_cg_init_part partials (one CTA
+// each): nullspace shift, thresholds, and the done flag for an instance with
+// nothing to solve.
+__global__ void __launch_bounds__(kThreads) k_cg_init_finish(const InstDev* insts, const int* ilist, double rel_tol,
+                                                              double abs_tol, int max_iter, int true_every,
+                                                              double rel_tol_inf) {
+  __shared__ double sh[32];
+  const InstDev& I = insts[ilist[blockIdx.x]];
+  Ctrl* c = I.ctrl;
+  const int nt0 = I.ntiles0;
+  const double bb = gather_slot(I.partial, 0, nt0, 0, sh);
+  const double bs = gather_slot(I.partial, 1, nt0, 0, sh);
+  const double rr = gather_slot(I.partial, 2, nt0, 0, sh);
+  const double bmax = gather_slot(I.partial, 3, nt0, 1, sh);
+  const double rmax = gather_slot(I.partial, 4, nt0, 1, sh);
+  if (threadIdx.x == 0) {
+    c->anchored = (c->air > 0) || (I.open_top && c->top_liquid > 0);
+    const double nliq = double(c->liquid > 0 ? c->liquid : 1);
+    c->bmean = c->anchored ? 0.0 : bs / nliq;
+    c->bb = bb - (c->anchored ? 0.0 : nliq * c->bmean * c->bmean);
+    c->rr = rr - (c->anchored ? 0.0 : nliq * c->bmean * c->bmean);
+    if (c->bb < 0) c->bb = 0;
+    if (c->rr < 0) c->rr = 0;
+    const double thr = fmax(abs_tol, rel_tol * sqrt(c->bb));
+    c->thr2 = thr * thr;
+    c->bmax = bmax;
+    c->rmax = rmax;
+    c->thr_inf = rel_tol_inf > 0 ? rel_tol_inf * bmax : 0.0;
+    c->iter = 0;
+    c->max_iter = max_iter;
+    c->true_every = true_every;
+    c->first = 1;
+    c->candidate = 0;
+    c->converged = 0;
+    c->done = 0;
+    c->status = FLUID_PP_OK;
+    c->rr_true = c->rr;
+    set_sigma(c, c->rr);
+    if (c->nonfinite) {
+      c->done = 1;
+      c->status = FLUID_PP_NONFINITE;
+    } else if (c->liquid == 0 || (c->rr <= c->thr2 && (c->thr_inf <= 0 || c->rmax <= c->thr_inf))) {
+      c->done = 1;   // nothing to solve, or the initial guess already satisfies the tolerance
+      c->converged = 1;
     }
   }
 }
@@ -792,18 +843,6 @@ __global__ void k_coarse_apply(const InstDev* insts, const int* list) {
 // ================================================================= CG kernels
 // The current search direction (the fused path alternates two buffers).
 __device__ __forceinline__ float* dir_cur(const InstDev& I) { return I.ctrl->dsel ? I.d2 : I.d; }
-// Level-0 column helper: calls f(k, z, i) for the thread's valid cells, fully
-// unrolled so the loads of all kTZ cells are in flight together.
-template <class F>
-__device__ __forceinline__ void for_column(const TileIt& it, int nx, int ny, int nz, F f) {
-  if (!it.ok) return;
-  const int sz = nx * ny;
-  const int i0 = it.x + nx * (it.y + ny * it.z0);
-#pragma unroll
-  for (int k = 0; k < kMaxDepth; ++k)
-    if (k < it.depth && it.z0 + k < nz) f(k, it.z0 + k, i0 + k * sz);
-}
-
 // gamma = r . (z - zmean) with float64 accumulation; beta from the previous gamma.
 __global__ void __launch_bounds__(kThreads) k_dot_rz(const InstDev* insts, const Tile* tiles, int ntiles) {
   __shared__ double sh[96];
@@ -1153,109 +1192,155 @@ __global__ void __launch_bounds__(kThreads) k_true_residual(const InstDev* insts
 
 // ================================================================= projection
 // One face of the projected velocity, evaluated in float64 from the double-single
-// pressure and rounded once to the stored float32.
-__device__ __forceinline__ float face_update(const InstDev& I, const LevelDev& L, int i, int j, float u) {
-  const bool li = L.label[i], lj = L.label[j];
+// pressures of its two cells (zero on air cells) and rounded once to the stored
+// float32.  li, lj: the cells are liquid; phi_*: their level sets.
+__device__ __forceinline__ float face_value(bool li, bool lj, float phi_i, float phi_j, double pi, double pj,
+                                            float u) {
   if (!li && !lj) return 0.0f;
   float th = 1.0f;
-  if (li && !lj) th = ghost_theta(L.phi[i], L.phi[j]);
-  if (!li && lj) th = ghost_theta(L.phi[j], L.phi[i]);
-  const double pi = li ? double(I.x[i]) + double(I.xlo[i]) : 0.0;
-  const double pj = lj ? double(I.x[j]) + double(I.xlo[j]) : 0.0;
+  if (li && !lj) th = ghost_theta(phi_i, phi_j);
+  if (!li && lj) th = ghost_theta(phi_j, phi_i);
   return float(double(u) - (pj - pi) / double(th));
 }
 
 // Gradient subtract (webgpu-uniform-reference.wgsl.ts:1052-1099 / atlas
 // pressureCorrection :1263-1279): each cell owns its three positive faces and,
 // on the low domain walls, its negative faces.  Closed walls and faces with no
-// liquid side are zero.  Also publishes the pressure in Pa.
-__global__ void k_grad(const InstDev* insts, const Tile* tiles, int ntiles) {
+// liquid side are zero.  Also publishes the pressure in Pa.  Every load of a
+// cell (labels, pressures and level sets of the cell and its +x, +y, +z
+// neighbours, the three faces) is issued together; the labels select what is
+// used afterwards, so no load waits for another.
+__global__ void __launch_bounds__(kThreads, 3) k_grad(const InstDev* insts, const Tile* tiles, int ntiles) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
     const Ctrl* c = I.ctrl;
     if (c->status == FLUID_PP_NONFINITE) continue;   // fail closed: keep the previous state
     const LevelDev& L = I.lv[0];
-    const long long uS = I.nx + 1, vS = I.ny + 1;
-    int x, y, z, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth); it.next(x, y, z, i);) {
-      const long long urow = uS * (y + (long long)I.ny * z);
-      const long long vcol = x + (long long)I.nx * vS * z;
-      const int sz = I.nx * I.ny;
-      const double pi = L.label[i] ? double(I.x[i]) + double(I.xlo[i]) : 0.0;
-      {
-        const long long f = urow + x + 1;
-        I.u[f] = x + 1 < I.nx ? face_update(I, L, i, i + 1, I.u[f]) : 0.0f;
-        if (x == 0) I.u[urow] = 0.0f;
-      }
-      {
-        const long long f = vcol + (long long)I.nx * (y + 1);
-        float nv = 0.0f;
-        if (y + 1 < I.ny) nv = face_update(I, L, i, i + I.nx, I.v[f]);
-        else if (I.open_top && L.label[i]) nv = float(double(I.v[f]) + pi / double(ghost_theta(L.phi[i], 0.5f)));
-        I.v[f] = nv;
-        if (y == 0) I.v[vcol] = 0.0f;
-      }
-      {
-        const long long f = (long long)i + sz;
-        I.w[f] = z + 1 < I.nz ? face_update(I, L, i, i + sz, I.w[f]) : 0.0f;
-        if (z == 0) I.w[i] = 0.0f;
-      }
-      I.p_si[i] = float(pi * double(I.pscale));
-    }
+    const int nx = I.nx, ny = I.ny, nz = I.nz, sz = nx * ny;
+    const long long uS = nx + 1, vS = ny + 1;
+    const uint8_t* __restrict__ lab = L.label;
+    const float* __restrict__ phi = L.phi;
+    const float* __restrict__ Xh = I.x;
+    const float* __restrict__ Xl = I.xlo;
+    float* __restrict__ U = I.u;
+    float* __restrict__ V = I.v;
+    float* __restrict__ W = I.w;
+    float* __restrict__ P = I.p_si;
+    const bool open_top = I.open_top;
+    const double pscale = double(I.pscale);
+    const TileIt it(tl.tile, nx, ny, nz, L.depth);
+    const int x = it.x, y = it.y;
+    const bool hx = x + 1 < nx, hy = y + 1 < ny;
+    for_column(it, nx, ny, nz, [&](int, int z, int i) {
+      const bool hz = z + 1 < nz;
+      const long long urow = uS * (y + (long long)ny * z);
+      const long long vcol = x + (long long)nx * vS * z;
+      const long long fu_i = urow + x + 1, fv_i = vcol + (long long)nx * (y + 1), fw_i = (long long)i + sz;
+      const int jx = hx ? i + 1 : i, jy = hy ? i + nx : i, jz = hz ? i + sz : i;
+      const bool l0 = lab[i], lx = hx && lab[jx], ly = hy && lab[jy], lz = hz && lab[jz];
+      const float xh0 = Xh[i], xl0 = Xl[i], xhx = Xh[jx], xlx = Xl[jx], xhy = Xh[jy], xly = Xl[jy], xhz = Xh[jz],
+                  xlz = Xl[jz];
+      const float f0 = phi[i], fx = phi[jx], fy = phi[jy], fz = phi[jz];
+      const float u = hx ? U[fu_i] : 0.0f, v = V[fv_i], w = hz ? W[fw_i] : 0.0f;
+      const double p0 = l0 ? double(xh0) + double(xl0) : 0.0;
+      const double px = lx ? double(xhx) + double(xlx) : 0.0;
+      const double py = ly ? double(xhy) + double(xly) : 0.0;
+      const double pz = lz ? double(xhz) + double(xlz) : 0.0;
+      U[fu_i] = hx ? face_value(l0, lx, f0, fx, p0, px, u) : 0.0f;
+      if (x == 0) U[urow] = 0.0f;
+      float nv = 0.0f;
+      if (hy) nv = face_value(l0, ly, f0, fy, p0, py, v);
+      else if (open_top && l0) nv = float(double(v) + p0 / double(ghost_theta(f0, 0.5f)));
+      V[fv_i] = nv;
+      if (y == 0) V[vcol] = 0.0f;
+      W[fw_i] = hz ? face_value(l0, lz, f0, fz, p0, pz, w) : 0.0f;
+      if (z == 0) W[i] = 0.0f;
+      P[i] = float(p0 * pscale);
+    });
   }
 }
 
 // Post-projection divergence receipts (atlas divergenceFromEquationResidual,
 // :1283-1296): max and sum of squares of (div u - q) before and after.
-__global__ void k_receipt(const InstDev* insts, const Tile* tiles, int ntiles) {
-  __shared__ double sh[32];
-  __shared__ int flag;
+// k_receipt_part writes each tile's partials; k_receipt_finish folds them per
+// instance in tile order.
+__global__ void __launch_bounds__(kThreads, 2) k_receipt_part(const InstDev* insts, const Tile* tiles, int ntiles) {
+  __shared__ double sh[4 * 32];
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
-    Ctrl* c = I.ctrl;
     const LevelDev& L = I.lv[0];
-    double mb = 0, sb = 0, ma = 0, sa = 0;
-    const long long uS = I.nx + 1, vS = I.ny + 1;
-    int x, y, z, i;
-    for (TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth); it.next(x, y, z, i);) {
-      if (!L.label[i]) continue;
-      const long long urow = uS * (y + (long long)I.ny * z);
-      const long long vcol = x + (long long)I.nx * vS * z;
-      const long long sz = (long long)I.nx * I.ny;
-      const double du = double(I.u[urow + x + 1]) - double(I.u[urow + x]);
-      const double dv = double(I.v[vcol + (long long)I.nx * (y + 1)]) - double(I.v[vcol + (long long)I.nx * y]);
-      const double dw = double(I.w[i + sz]) - double(I.w[i]);
-      const float rho = I.vof[i];
+    const int nx = I.nx, ny = I.ny, nz = I.nz;
+    const long long uS = nx + 1, vS = ny + 1, sz = (long long)nx * ny;
+    const float* __restrict__ U = I.u;
+    const float* __restrict__ V = I.v;
+    const float* __restrict__ W = I.w;
+    const float* __restrict__ vof = I.vof;
+    const float* __restrict__ B = I.b;
+    const uint8_t* __restrict__ lab = L.label;
+    const float hdt = I.h / I.dt;
+    double sums[2] = {0, 0}, maxes[2] = {0, 0};   // after, before
+    const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
+    const int x = it.x, y = it.y;
+    // labels first, then the liquid cells' faces, VOF and right-hand side
+    uint8_t lb[kMaxDepth];
+    for_column(it, nx, ny, nz, [&](int k, int, int i) { lb[k] = lab[i]; });
+    float up[kMaxDepth], um[kMaxDepth], vp[kMaxDepth], vm[kMaxDepth], wp[kMaxDepth], wm[kMaxDepth], rv[kMaxDepth],
+        bv[kMaxDepth];
+    for_column(it, nx, ny, nz, [&](int k, int z, int i) {
+      if (!lb[k]) return;
+      const long long urow = uS * (y + (long long)ny * z);
+      const long long vcol = x + (long long)nx * vS * z;
+      up[k] = U[urow + x + 1];
+      um[k] = U[urow + x];
+      vp[k] = V[vcol + (long long)nx * (y + 1)];
+      vm[k] = V[vcol + (long long)nx * y];
+      wp[k] = W[i + sz];
+      wm[k] = W[i];
+      rv[k] = vof[i];
+      bv[k] = B[i];
+    });
+    for_column(it, nx, ny, nz, [&](int k, int, int) {
+      if (!lb[k]) return;
+      const double du = double(up[k]) - double(um[k]);
+      const double dv = double(vp[k]) - double(vm[k]);
+      const double dw = double(wp[k]) - double(wm[k]);
+      const float rho = rv[k];
       double q = 0.0;
-      if (rho > 1.0f) q = fminf(fminf(0.5f * (rho - 1.0f), 1.0f), I.h / I.dt);
+      if (rho > 1.0f) q = fminf(fminf(0.5f * (rho - 1.0f), 1.0f), hdt);
       const double after = (du + dw) + dv - q;
-      const double before = -double(I.b[i]);
-      ma = fmax(ma, fabs(after));
-      sa += after * after;
-      mb = fmax(mb, fabs(before));
-      sb += before * before;
-    }
-    const double a0 = block_max(ma, sh), a1 = block_sum(sa, sh), a2 = block_max(mb, sh), a3 = block_sum(sb, sh);
+      const double before = -double(bv[k]);
+      maxes[0] = fmax(maxes[0], fabs(after));
+      sums[0] += after * after;
+      maxes[1] = fmax(maxes[1], fabs(before));
+      sums[1] += before * before;
+    });
+    block_folds<2, 2>(sums, maxes, sh);
     if (threadIdx.x == 0) {
-      I.partial[0 * I.ntiles0 + tl.tile] = a0;
-      I.partial[1 * I.ntiles0 + tl.tile] = a1;
-      I.partial[2 * I.ntiles0 + tl.tile] = a2;
-      I.partial[3 * I.ntiles0 + tl.tile] = a3;
+      I.partial[0 * I.ntiles0 + tl.tile] = maxes[0];
+      I.partial[1 * I.ntiles0 + tl.tile] = sums[0];
+      I.partial[2 * I.ntiles0 + tl.tile] = maxes[1];
+      I.partial[3 * I.ntiles0 + tl.tile] = sums[1];
     }
-    if (arrive_last(&c->arrive[kStReceipt], I.ntiles0, &flag)) {
-      const double r0 = gather_slot(I.partial, 0, I.ntiles0, 1, sh);
-      const double r1 = gather_slot(I.partial, 1, I.ntiles0, 0, sh);
-      const double r2 = gather_slot(I.partial, 2, I.ntiles0, 1, sh);
-      const double r3 = gather_slot(I.partial, 3, I.ntiles0, 0, sh);
-      if (threadIdx.x == 0) {
-        c->red[0] = r0;
-        c->red[1] = r1;
-        c->red[2] = r2;
-        c->red[3] = r3;
-      }
-    }
+  }
+}
+
+// The four receipt norms of each listed instance (one CTA each).
+__global__ void __launch_bounds__(kThreads) k_receipt_finish(const InstDev* insts, const int* ilist) {
+  __shared__ double sh[32];
+  const InstDev& I = insts[ilist[blockIdx.x]];
+  Ctrl* c = I.ctrl;
+  const int nt0 = I.ntiles0;
+  const double r0 = gather_slot(I.partial, 0, nt0, 1, sh);
+  const double r1 = gather_slot(I.partial, 1, nt0, 0, sh);
+  const double r2 = gather_slot(I.partial, 2, nt0, 1, sh);
+  const double r3 = gather_slot(I.partial, 3, nt0, 0, sh);
+  if (threadIdx.x == 0) {
+    c->red[0] = r0;
+    c->red[1] = r1;
+    c->red[2] = r2;
+    c->red[3] = r3;
   }
 }
 

@@ -231,12 +231,14 @@ void setup_launch(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
                                                                                              B->crs[l].n));
   FPP_LAUNCH(B, kPrBake, k_bake_diag<T><<<launch_grid(B->bake.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->bake), B->bake.n));
   if (B->multi.n)
-    FPP_LAUNCH(B, kPrFactor, k_coarse_factor<T><<<B->multi.n, kThreads, B->smem_factor, s>>>(B->d_insts, il(B, B->multi)));
+    FPP_LAUNCH(B, kPrFactor, k_coarse_factor<T><<<B->multi.n, kBlockThreads, B->smem_factor, s>>>(B->d_insts, il(B, B->multi)));
   if (B->single.n)
     FPP_LAUNCH(B, kPrFactor,
-               k_coarse_factor<T><<<B->single.n, kThreads, B->smem_factor, s>>>(B->d_insts, il(B, B->single)));
-  FPP_LAUNCH(B, kPrInit, k_cg_init<<<g0, kThreads, 0, s>>>(B->d_insts, t0, n0, o.rel_tol, o.abs_tol, o.max_iters,
-                                                            o.true_residual_every, warm, o.rel_tol_inf));
+               k_coarse_factor<T><<<B->single.n, kBlockThreads, B->smem_factor, s>>>(B->d_insts, il(B, B->single)));
+  FPP_LAUNCH(B, kPrInit, k_cg_init_part<<<g0, kThreads, 0, s>>>(B->d_insts, t0, n0, warm));
+  FPP_LAUNCH(B, kPrInit, k_cg_init_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(
+                             B->d_insts, il(B, B->multi), o.rel_tol, o.abs_tol, o.max_iters, o.true_residual_every,
+                             o.rel_tol_inf));
   FPP_LAUNCH(B, kPrInit, k_project_init<<<g0, kThreads, 0, s>>>(B->d_insts, t0, n0));
 }
 
@@ -375,7 +377,9 @@ void finish_launch_any(fluid_pp_batch* B) {
   const Tile* t0 = tl(B, B->l0);
   const int n0 = B->l0.n, g = launch_grid(n0);
   FPP_LAUNCH(B, kPrGrad, k_grad<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
-  FPP_LAUNCH(B, kPrReceipt, k_receipt<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+  FPP_LAUNCH(B, kPrReceipt, k_receipt_part<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+  FPP_LAUNCH(B, kPrReceipt, k_receipt_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(B->d_insts,
+                                                                                           il(B, B->multi)));
 }
 
 void destroy_graphs(fluid_pp_batch* B) {
