@@ -629,9 +629,17 @@ __host__ __device__ inline int march_up_smem_bytes() {
   return (2 * kURing * kUEP + kUZRing * kUEP + 3 * kUQP) * 4 + kURing * kUEP;
 }
 
-template <class TZF, class TR, class TD, class TZC>
+// With DOT (level 0) the step also writes the gamma partials of the fixed
+// 32 x 8 x 8 level-0 tiles it covers.  Thread t outputs rows t / 32 and
+// 8 + t / 32 of column t % 32 of the tile, in z order: lane and warp of
+// k_dot_rz_part's layout, so its per-thread sums and block folds, and hence
+// gamma's bits, are that kernel's.
+static_assert(kUX == kTX && kUY == 2 * kTY && kUZ % kMaxDepth == 0 && kUX * kUY == 2 * kMThreads,
+              "marching up tiles must cover whole dot tiles, two rows per thread");
+template <class TZF, class TR, class TD, class TZC, bool DOT = false>
 __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, const Tile* tiles, int level) {
   extern __shared__ float smu[];
+  __shared__ double gsh[DOT ? 6 * 32 : 1];
   float* rhs_r = smu;                              // [kURing][kUEP]
   float* dg_r = rhs_r + kURing * kUEP;             // [kURing][kUEP]
   float* z_r = dg_r + kURing * kUEP;               // [kUZRing][kUEP]
@@ -749,6 +757,7 @@ __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, con
     zhi_loaded = coarse_hi(pz0);
     for (int Z = min(cz[0], cz[1]); Z <= zhi_loaded; ++Z) load_coarse(Z);
   }
+  double gacc[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};   // per output row: r.z, sum z, sum r
   fetch(pz0);
   __syncthreads();
   for (int p = pz0; p <= pz1 + 2; ++p) {
@@ -833,6 +842,31 @@ __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, con
                                         wz * zm[s], wz * zp[s])) *
                         __frcp_rn(dd[s]));
         if (rin && tofs[kk] >= 0) zo[tofs[kk] + nxy * r] = fromf<TZF>(zv);
+        if (DOT && lb[s]) {   // liquid cells of the lattice (staged labels are 0 outside it)
+          const double zd = zv, rd = rh[s];
+          gacc[kk][0] += rd * zd;
+          gacc[kk][1] += zd;
+          gacc[kk][2] += rd;
+        }
+      }
+      // a dot tile ends every 8 planes and at the lattice top
+      if (DOT && (((r - z0) & (kMaxDepth - 1)) == kMaxDepth - 1 || r == pz1 - 2)) {
+        double v[6] = {gacc[0][0], gacc[0][1], gacc[0][2], gacc[1][0], gacc[1][1], gacc[1][2]};
+        block_folds<6, 0>(v, nullptr, gsh);
+        if (t == 0) {
+          const int nt0 = I.ntiles0, ntx0 = (nx + kTX - 1) / kTX, nty0 = (ny + kTY - 1) / kTY;
+          const int ta = tx + ntx0 * (2 * ty + nty0 * (r / kMaxDepth));
+          I.partial[ta] = v[0];
+          I.partial[nt0 + ta] = v[1];
+          I.partial[2 * nt0 + ta] = v[2];
+          if (2 * ty + 1 < nty0) {   // the upper dot tile exists
+            I.partial[ta + ntx0] = v[3];
+            I.partial[nt0 + ta + ntx0] = v[4];
+            I.partial[2 * nt0 + ta + ntx0] = v[5];
+          }
+        }
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) gacc[kk][0] = gacc[kk][1] = gacc[kk][2] = 0.0;
       }
     }
     __syncthreads();

@@ -25,6 +25,35 @@ __device__ __forceinline__ void for_column(const TileIt& it, int nx, int ny, int
     if (k < it.depth && it.z0 + k < nz) f(k, it.z0 + k, i0 + k * sz);
 }
 
+// Grid-stride walk over a tile list that visits only the tiles whose instance
+// passes `active`: the CTA reads the flags of up to blockDim.x of its tiles at
+// once (one dependent read chain per round instead of one per tile) and runs
+// body(t) for the active ones in increasing t, uniformly across the CTA.  A
+// skipped tile costs no pass of its own; results are those of the plain walk.
+template <class P, class F>
+__device__ __forceinline__ void for_active_tiles(const InstDev* insts, const Tile* tiles, int ntiles, P active,
+                                                 F body) {
+  __shared__ int act[kThreads];
+  __shared__ int wcnt[kThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int base = blockIdx.x; base < ntiles; base += gridDim.x * blockDim.x) {
+    const int mt = base + threadIdx.x * gridDim.x;
+    const bool a = mt < ntiles && active(insts[tiles[mt].inst]);
+    const unsigned m = __ballot_sync(0xffffffffu, a);
+    if (lane == 0) wcnt[warp] = __popc(m);
+    __syncthreads();
+    int off = 0, n = 0;
+    for (int w = 0; w < nwarps; ++w) {
+      off += w < warp ? wcnt[w] : 0;
+      n += wcnt[w];
+    }
+    if (a) act[off + __popc(m & ((1u << lane) - 1u))] = mt;
+    __syncthreads();
+    for (int j = 0; j < n; ++j) body(act[j]);
+    __syncthreads();
+  }
+}
+
 // ================================================================= setup
 // Level 0: labels, level set and right-hand side from the VOF and MAC velocities
 // (ref.wgsl.ts:208-242 labelling; divergenceAt :1010-1024 with closed walls
@@ -889,10 +918,10 @@ __global__ void __launch_bounds__(kThreads) k_dot_rz(const InstDev* insts, const
 // k_dot_rz_finish folds each instance's partials in tile order afterwards.
 __global__ void __launch_bounds__(kThreads) k_dot_rz_part(const InstDev* insts, const Tile* tiles, int ntiles) {
   __shared__ double sh[96];
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  for_active_tiles(insts, tiles, ntiles, [](const InstDev& I) { return !I.ctrl->done; }, [&](int t) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
-    if (I.ctrl->done) continue;   // uniform per CTA
+    if (I.ctrl->done) return;   // uniform per CTA
     const LevelDev& L = I.lv[0];
     const float* __restrict__ r = static_cast<const float*>(L.rhs);
     const float* __restrict__ z = static_cast<const float*>(L.z);
@@ -927,7 +956,7 @@ __global__ void __launch_bounds__(kThreads) k_dot_rz_part(const InstDev* insts, 
       I.partial[1 * nt0 + tl.tile] = zs;
       I.partial[2 * nt0 + tl.tile] = rs;
     }
-  }
+  });
 }
 
 // gamma of each listed instance from its k_dot_rz_part partials (one CTA each).
@@ -1066,7 +1095,7 @@ __global__ void __launch_bounds__(kThreads) k_update(const InstDev* insts, const
 // instance's partials in tile order afterwards, so the bits are k_update's.
 __global__ void __launch_bounds__(kThreads) k_update_part(const InstDev* insts, const Tile* tiles, int ntiles) {
   __shared__ double sh[64];
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  for_active_tiles(insts, tiles, ntiles, [](const InstDev& I) { return !I.ctrl->done; }, [&](int t) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
     Ctrl* c = I.ctrl;
@@ -1079,7 +1108,7 @@ __global__ void __launch_bounds__(kThreads) k_update_part(const InstDev* insts, 
     float* __restrict__ Xlo = I.xlo;
     const float* __restrict__ D = dir_cur(I);
     const float* __restrict__ Q = I.q;
-    if (done) continue;
+    if (done) return;
     float* __restrict__ r = static_cast<float*>(L.rhs);
     const uint8_t* __restrict__ lab = L.label;
     const float alpha_f = float(alpha);
@@ -1113,7 +1142,7 @@ __global__ void __launch_bounds__(kThreads) k_update_part(const InstDev* insts, 
       partial[tl.tile] = rr;
       partial[nt0 + tl.tile] = mr;
     }
-  }
+  });
 }
 
 // ||r||^2 and max|r| of each listed instance from its k_update_part partials (one CTA each).
@@ -1133,12 +1162,15 @@ __global__ void __launch_bounds__(kThreads) k_update_finish(const InstDev* insts
 __global__ void __launch_bounds__(kThreads) k_true_residual(const InstDev* insts, const Tile* tiles, int ntiles) {
   __shared__ double sh[32];
   __shared__ int flag;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  for_active_tiles(insts, tiles, ntiles, [](const InstDev& I) {
+    const Ctrl* c = I.ctrl;
+    return !c->done && (c->candidate || (c->true_every > 0 && c->iter % c->true_every == 0));
+  }, [&](int t) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
     Ctrl* c = I.ctrl;
     const int done = c->done, cand = c->candidate, every = c->true_every, iter = c->iter;
-    if (done || (!cand && !(every > 0 && iter % every == 0))) continue;
+    if (done || (!cand && !(every > 0 && iter % every == 0))) return;
     const LevelDev L = I.lv[0];
     const int nt0 = I.ntiles0;
     double* partial = I.partial;
@@ -1187,7 +1219,7 @@ __global__ void __launch_bounds__(kThreads) k_true_residual(const InstDev* insts
       const double m = gather_slot(partial, 1, nt0, 1, sh);
       if (threadIdx.x == 0) finish_true(c, s, m);
     }
-  }
+  });
 }
 
 // ================================================================= projection

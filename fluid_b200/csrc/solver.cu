@@ -100,6 +100,7 @@ struct fluid_pp_batch {
   List dnm[kMaxLevels];      // marching down-step tiles of grid level l (levels < kMarchLevels coarsened by two on every axis)
   List upm[kMaxLevels];      // marching up-step tiles (same condition)
   List spm;                  // marching direction + SpMV tiles of level 0 (every instance)
+  List dot0;                 // level-0 tiles of instances whose level-0 up step does not march (gamma by k_dot_rz_part)
   List up[kMaxLevels];       // fused up-step tiles (fine tiles of level l) of grid level l
   List l0single;             // level-0 tiles of single-level instances
   List bake;
@@ -324,7 +325,10 @@ void vcycle_fused(fluid_pp_batch* B, int with_dot) {
                k_coarse_apply<float, float><<<B->single.n, kThreads, 0, s>>>(B->d_insts, il(B, B->single)));
   for (int l = B->maxL - 2; l >= 0; --l) {
     if (B->upm[l].n) {
-      if (l == 0)
+      if (l == 0 && with_dot)
+        FPP_LAUNCH(B, kPrUp0, k_up_m<float, float, T, T, true><<<B->upm[l].n, kMThreads, march_up_smem_bytes(), s>>>(
+                                  B->d_insts, tl(B, B->upm[l]), 0));
+      else if (l == 0)
         FPP_LAUNCH(B, kPrUp0, k_up_m<float, float, T, T><<<B->upm[l].n, kMThreads, march_up_smem_bytes(), s>>>(
                                   B->d_insts, tl(B, B->upm[l]), 0));
       else
@@ -338,12 +342,16 @@ void vcycle_fused(fluid_pp_batch* B, int with_dot) {
     else
       FPP_LAUNCH(B, kPrUpC, k_up<T, T, T, T><<<Lu.n, kFThreads, B->smem_up, s>>>(B->d_insts, tl(B, Lu), l, 0));
   }
-  // gamma = r . (z - zmean) over the fixed level-0 tiles of every instance: its
-  // fold order does not depend on which up kernel (marching or box, chosen by
-  // how the batch fills the GPU) produced z, so a solve gives the same bits
-  // alone and in any batch
+  // gamma = r . (z - zmean) over the fixed level-0 tiles of every instance: the
+  // marching level-0 up step writes the partials of its instances with
+  // k_dot_rz_part's per-thread sums and folds, k_dot_rz_part those of the
+  // rest, so the fold order does not depend on which up kernel (chosen by how
+  // the batch fills the GPU) produced z and a solve gives the same bits alone
+  // and in any batch
   if (with_dot) {
-    FPP_LAUNCH(B, kPrDot, k_dot_rz_part<<<launch_grid(B->l0.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->l0), B->l0.n));
+    if (B->dot0.n)
+      FPP_LAUNCH(B, kPrDot, k_dot_rz_part<<<launch_grid(B->dot0.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->dot0),
+                                                                                      B->dot0.n));
     // every instance: the multi-level list followed by the single-level one
     FPP_LAUNCH(B, kPrDot, k_dot_rz_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(B->d_insts,
                                                                                       il(B, B->multi)));
@@ -511,6 +519,7 @@ static cudaError_t configure_kernels_t(size_t factor, size_t block, size_t down,
   if (e == cudaSuccess) e = set((const void*)k_up<T, T, T, T>, up);
   if (e == cudaSuccess) e = set((const void*)k_up_m<float, float, T, T>, size_t(march_up_smem_bytes()));
   if (e == cudaSuccess) e = set((const void*)k_up_m<T, T, T, T>, size_t(march_up_smem_bytes()));
+  if (e == cudaSuccess) e = set((const void*)k_up_m<float, float, T, T, true>, size_t(march_up_smem_bytes()));
   return e;
 }
 
@@ -609,6 +618,7 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
   // tile lists
   std::vector<Tile> tiles;
   std::vector<int> ilist;
+  std::vector<char> march0(count, 0);   // level-0 up step marches (and forms the gamma partials)
   // restriction tiles (coarse tiles of kRX x kRY x kRZ) when `restrict_tiles`
   auto add_level = [&](List& L, auto pred, int level_of_tiles, bool restrict_tiles = false) {
     L.off = int(tiles.size());
@@ -668,9 +678,15 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
         const LevelDev& Lv = insts[k].lv[l];
         const int nt = march_up_tiles(Lv.nx, Lv.ny, Lv.nz);
         for (int t = 0; t < nt; ++t) tiles.push_back(Tile{k, l, t, 0});
+        if (l == 0) march0[k] = 1;
       }
     B->upm[l].n = int(tiles.size()) - B->upm[l].off;
   }
+  B->dot0.off = int(tiles.size());
+  for (int k = 0; k < count; ++k)
+    if (!march0[k])
+      for (int t = 0; t < insts[k].lv[0].ntiles; ++t) tiles.push_back(Tile{k, 0, t, 0});
+  B->dot0.n = int(tiles.size()) - B->dot0.off;
   add_level(B->l0single, [](const InstDev& I) { return I.nlev == 1; }, 0);
   B->spm.off = int(tiles.size());
   for (int k = 0; k < count; ++k) {
