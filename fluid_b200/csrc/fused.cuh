@@ -964,7 +964,6 @@ __global__ void __launch_bounds__(kMThreads, 4) k_dirspmv_m(const InstDev* insts
   __shared__ float dn_r[4][kQEP];
   __shared__ uint8_t lab_r[4][kQEP];
   __shared__ double sh[32];
-  __shared__ int flag;
   const Tile tl = tiles[blockIdx.x];
   const InstDev& I = insts[tl.inst];
   Ctrl* c = I.ctrl;
@@ -999,8 +998,17 @@ __global__ void __launch_bounds__(kMThreads, 4) k_dirspmv_m(const InstDev* insts
     ts_[k] = (ly + 1) * kQEX + lx + 1;
     tofs[k] = (e < kQX * kQY && gx < nx && gy < ny) ? gx + nx * gy : -1;
   }
-  float pz_[kQPer], pd_[kQPer];
+  float pz_[kQPer], pd_[kQPer], pg_[kQTPer];
   uint8_t pl[kQPer];
+  auto sl = [&](int p) { return (p - pz0) & 3; };
+  // diagonal of plane g's interior liquid cells (g was staged in an earlier
+  // step), one step ahead of its operator
+  auto fetch_diag = [&](int g) {
+    const bool gin = g >= z0 && g < nz;
+#pragma unroll
+    for (int k = 0; k < kQTPer; ++k)
+      pg_[k] = (gin && tofs[k] >= 0 && lab_r[sl(g)][ts_[k]]) ? dgl[tofs[k] + nxy * g] : 0.0f;
+  };
   auto fetch = [&](int p) {
     const bool pin = p >= 0 && p < nz;
 #pragma unroll
@@ -1016,10 +1024,15 @@ __global__ void __launch_bounds__(kMThreads, 4) k_dirspmv_m(const InstDev* insts
       }
     }
   };
-  auto sl = [&](int p) { return (p - pz0) & 3; };
   double dq = 0.0;
   fetch(pz0);
+  fetch_diag(pz0 - 2);
   for (int p = pz0; p <= pz1 + 1; ++p) {
+    // operator on plane r = p - 2 (planes r - 1 .. r + 1 were staged by earlier
+    // steps); its diagonal was fetched in the previous step
+    float dgr[kQTPer];
+#pragma unroll
+    for (int k = 0; k < kQTPer; ++k) dgr[k] = pg_[k];
     if (p <= pz1) {
       float* dn = dn_r[sl(p)];
       uint8_t* lb = lab_r[sl(p)];
@@ -1032,7 +1045,7 @@ __global__ void __launch_bounds__(kMThreads, 4) k_dirspmv_m(const InstDev* insts
       }
       if (p < pz1) fetch(p + 1);
     }
-    // operator on plane r = p - 2 (planes r - 1 .. r + 1 were staged by earlier steps)
+    fetch_diag(p - 1);
     const int r = p - 2;
     if (r >= z0 && r < z0 + kQZ && r < nz) {
       const float* dn = dn_r[sl(r)];
@@ -1046,7 +1059,7 @@ __global__ void __launch_bounds__(kMThreads, 4) k_dirspmv_m(const InstDev* insts
         const float dv = dn[s];
         float q = 0.0f;
         if (lb[s]) {
-          q = dgl[i] * dv - d4sum6(dn[s - 1], dn[s + 1], dn[s - kQEX], dn[s + kQEX], dm[s], dp[s]);
+          q = dgr[k] * dv - d4sum6(dn[s - 1], dn[s + 1], dn[s - kQEX], dn[s + kQEX], dm[s], dp[s]);
           dq += double(dv) * q;
         }
         dnew[i] = dv;
@@ -1055,15 +1068,24 @@ __global__ void __launch_bounds__(kMThreads, 4) k_dirspmv_m(const InstDev* insts
     }
     __syncthreads();
   }
-  const int nt = march_spmv_tiles(nx, ny, nz);
   const double a0 = block_sum(dq, sh);
   if (t == 0) I.partial[tl.tile] = a0;
-  if (arrive_last(&c->arrive[kStSpmv], nt, &flag)) {
-    const double delta = gather_slot(I.partial, 0, nt, 0, sh);
-    if (t == 0) {
-      finish_delta(c, delta);
-      c->dsel = sel ^ 1;
-    }
+}
+
+// delta of each listed instance from its k_dirspmv_m partials in tile order,
+// alpha = gamma / delta, and the direction buffers swap (one CTA each).
+__global__ void __launch_bounds__(kThreads) k_dirspmv_finish(const InstDev* insts, const int* ilist) {
+  __shared__ double sh[32];
+  const InstDev& I = insts[ilist[blockIdx.x]];
+  Ctrl* c = I.ctrl;
+  if (c->done) return;
+  const LevelDev& L = I.lv[0];
+  const int nt = march_spmv_tiles(L.nx, L.ny, L.nz);
+  const int sel = c->dsel;
+  const double delta = gather_slot(I.partial, 0, nt, 0, sh);
+  if (threadIdx.x == 0) {
+    finish_delta(c, delta);
+    c->dsel = sel ^ 1;
   }
 }
 

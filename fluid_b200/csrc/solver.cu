@@ -366,6 +366,8 @@ void iter_launch(fluid_pp_batch* B, int pre, int post) {
   if (pre == 1 && post == 1) {
     vcycle_fused<T>(B, 1);
     FPP_LAUNCH(B, kPrDirSpmv, k_dirspmv_m<<<B->spm.n, kMThreads, 0, s>>>(B->d_insts, tl(B, B->spm)));
+    FPP_LAUNCH(B, kPrDirSpmv, k_dirspmv_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(B->d_insts,
+                                                                                           il(B, B->multi)));
     FPP_LAUNCH(B, kPrUpdate, k_update_part<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
     FPP_LAUNCH(B, kPrUpdate, k_update_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(B->d_insts,
                                                                                          il(B, B->multi)));
