@@ -72,7 +72,7 @@ def stage_bytes_per_cell(stage: str, s: int) -> float:
 # workload (64 instances, fp16 levels, a first-iteration launch with every
 # instance iterating), from the committed ncu capture
 # profiles/marching_vcycle_batch64_fp16.md (cold-cache launches).
-NCU_TRAFFIC_BYTES = {"up0": 197.87e6, "down0": 134.09e6}
+NCU_TRAFFIC_BYTES = {"up0": 197.27e6, "down0": 134.00e6}
 
 
 def peaks():
