@@ -222,6 +222,7 @@ def main():
     import torch
 
     from fluid_b200 import BatchProjector, PipelinedBatchProjector, PressureProjector, _abi, configs
+    from fluid_b200.autotune import autotune_batch
     from fluid_b200.projector import kernel_launches
 
     world, rank, local = dist_setup()
@@ -269,15 +270,16 @@ def main():
         for p, d in zip(pps, dev):
             p.upload_state_device(*(t.data_ptr() for t in d))
 
-    def run_batched(precision, steps, profile=False):
+    def run_batched(precision, steps, profile=False, tuning=None, o=None):
+        o = opts if o is None else o
         pps = make(precision)
-        B = BatchProjector(pps)
+        B = BatchProjector(pps, tuning=tuning)
         B.set_profiling(profile)
         times, recs = [], None
 
         def step():
             upload_dev(pps)
-            return B.project(dts, **opts)
+            return B.project(dts, **o)
         for k in range(args.warmup + steps):
             ms, recs = timed(step)
             if k >= args.warmup:
@@ -308,13 +310,22 @@ def main():
             p.destroy()
         return times, recs
 
+    # the batch's layout and sweep schedule, measured on this batch before timing
+    # (layouts never change results; fluid_b200.autotune)
+    note("autotune")
+    pps_t = make(args.precision)
+    tune = autotune_batch(pps_t, dts, lambda: upload_dev(pps_t), rel_tol=1e-6, repeats=2)
+    for p in pps_t:
+        p.destroy()
+    tuned = dict(opts, pre_sweeps=tune.sweeps[0], post_sweeps=tune.sweeps[1])
+
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     l0 = kernel_launches()
     note("headline: batched mixed")
     with ClockSampler(local) as clk:
-        times, recs, _ = run_batched(args.precision, args.steps)
+        times, recs, _ = run_batched(args.precision, args.steps, tuning=tune.tuning, o=tuned)
     torch.cuda.synchronize()
     launches = kernel_launches() - l0
     tot_ms = max_over_ranks(sum(times))
@@ -369,7 +380,7 @@ def main():
     # algorithmic bytes over the solve are bytes/cell x sum(cells_i x iterations_i).
     note("headline per-stage events")
     prof_steps = 2
-    _, brecs, bprof = run_batched(args.precision, prof_steps, profile=True)
+    _, brecs, bprof = run_batched(args.precision, prof_steps, profile=True, tuning=tune.tuning, o=tuned)
     sbytes = 4 if args.precision == "fp32" else 2
     cell_iters = prof_steps * sum(s_.cells * r["iterations"] for s_, r in zip(insts, brecs))
     stages = {k: v for k, v in bprof.items() if stage_bytes_per_cell(k, sbytes) > 0 and v["launches"] > 0}
@@ -427,7 +438,7 @@ def main():
     # ------------------------------------------- e2e: public API from host buffers
     note("e2e from host buffers")
     pps = make(args.precision)
-    B = BatchProjector(pps)
+    B = BatchProjector(pps, tuning=tune.tuning)
     host_in = [tuple(torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (s.vof, s.u, s.v, s.w))
                for s in insts]
     host_out = [tuple(torch.empty(sh, dtype=torch.float32).pin_memory()
@@ -440,7 +451,7 @@ def main():
     def e2e_step():
         for p, hi in zip(pps, host_in):
             p.upload_state(*(t.numpy() for t in hi))
-        out = B.project(dts, **opts)
+        out = B.project(dts, **tuned)
         for p, ho in zip(pps, host_out):
             L.fluid_pp_download(p.handle, *(_abi.ptr(t.numpy()) for t in ho))
         return out
@@ -464,7 +475,7 @@ def main():
         for p in ps_:
             p.set_stream(st.cuda_stream)
         sets.append(ps_)
-    pipe = PipelinedBatchProjector(sets)
+    pipe = PipelinedBatchProjector(sets, tuning=tune.tuning)
     outs = [host_out, [tuple(torch.empty_like(t).pin_memory() for t in tup) for tup in host_out]]
     ins_np = [tuple(t.numpy() for t in tup) for tup in host_in]
     outs_np = [[tuple(t.numpy() for t in tup) for tup in o] for o in outs]
@@ -479,7 +490,7 @@ def main():
                 pipe_bad += sum(r["status"] != 0 for r in pipe.result(tickets[k - 2]))
             with torch.cuda.stream(side[slot]):
                 flush.zero_()   # L2 flushed before every tick, on the tick's own stream
-            tickets.append(pipe.submit(ins_np, outs_np[slot], dts, **opts))
+            tickets.append(pipe.submit(ins_np, outs_np[slot], dts, **tuned))
         for t in tickets[-2:]:
             pipe_bad += sum(r["status"] != 0 for r in pipe.result(t))
 
@@ -515,7 +526,8 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "instances": BATCH, "cells": cells, "seed": 4,
                    "precision": f"{args.precision} V-cycle levels, f32 CG vectors, f64 dots/scalars/coarsest",
-                   "sweeps": args.sweeps, "l2": "flushed before every timed step (256 MB write)",
+                   "sweeps": list(tune.sweeps), "tuning": tune.tuning,
+                   "l2": "flushed before every timed step (256 MB write)",
                    "parallelism": f"{world} replicas" if world > 1 else "single GPU"},
         "p50_ms": statistics.median(times), "p99_ms": float(np.percentile(times, 99)),
         "iterations_min_max": [min(its), max(its)],
@@ -525,6 +537,11 @@ def main():
         "batched_fp32_solves_per_s": batched32,
         "mixed_batched_vs_plain_single": value / (world * plain),
         "failed_solves": len(bad),
+        "autotune": {"candidates": len(tune.table), "chosen_ms": tune.ms, "default_layout_ms": tune.default_ms,
+                     "table": [[r["tuning"]["fill_tiles"], r["tuning"]["march_levels"], r["tuning"]["box_shape"],
+                                list(r["sweeps"]), round(r["ms"], 3)] for r in tune.table],
+                     "table_columns": ["fill_tiles", "march_levels", "box_shape", "sweeps", "median_ms"],
+                     "note": "median solve of each candidate layout / sweep schedule on this batch before timing"},
         "dam_spheres_128x96x128": {
             "workload": WORKLOAD2, "steps": steps2,
             "mixed_solves_per_s": len(t2_mixed) / (sum(t2_mixed) / 1000.0),

@@ -36,7 +36,7 @@ EXPORTS = (
     "fluid_pp_set_allocation_cache", "fluid_pp_allocation_cache_bytes", "fluid_pp_reserve_allocation",
     "fluid_pp_tall_project_begin", "fluid_pp_tall_project_continue", "fluid_pp_tall_project_end",
     "fluid_pp_batch_project_async", "fluid_pp_batch_receipts_read", "fluid_pp_download_async",
-    "fluid_pp_synchronize",
+    "fluid_pp_synchronize", "fluid_pp_batch_tuning_default", "fluid_pp_batch_create_tuned",
 )
 STAGES = ("reset", "label", "coarsen", "bake", "factor", "init", "smooth0", "smoothc", "residual0", "residualc",
           "restrict0", "restrictc", "coarse", "prolong0", "prolongc", "dot", "dir", "spmv", "update", "true",
@@ -60,6 +60,13 @@ class SolveOpts(ctypes.Structure):
                 ("pre_sweeps", ctypes.c_int), ("post_sweeps", ctypes.c_int),
                 ("true_residual_every", ctypes.c_int), ("warm_start", ctypes.c_int),
                 ("rel_tol_inf", ctypes.c_double)]
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("fill_tiles", ctypes.c_int), ("march_levels", ctypes.c_int), ("box_shape", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class Receipt(ctypes.Structure):
@@ -114,6 +121,9 @@ def load():
     L.fluid_pp_batch_destroy.restype = None
     L.fluid_pp_batch_project.argtypes = [vp, vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(Receipt)]
     L.fluid_pp_batch_project_async.argtypes = [vp, vp, ctypes.POINTER(SolveOpts)]
+    L.fluid_pp_batch_tuning_default.argtypes = [ctypes.POINTER(BatchTuning)]
+    L.fluid_pp_batch_tuning_default.restype = None
+    L.fluid_pp_batch_create_tuned.argtypes = [ctypes.POINTER(vp), ci, ctypes.POINTER(BatchTuning), ctypes.POINTER(vp)]
     L.fluid_pp_batch_receipts_read.argtypes = [vp, ctypes.POINTER(Receipt)]
     L.fluid_pp_download_async.argtypes = [vp, vp, vp, vp, vp]
     L.fluid_pp_synchronize.argtypes = [vp]

@@ -549,7 +549,8 @@ static cudaError_t configure_kernels() {
   return e;
 }
 
-static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out, std::string& err) {
+static int batch_build(fluid_pp* const* handles, int count, const fluid_pp_batch_tuning& tu, fluid_pp_batch** out,
+                       std::string& err) {
   if (!handles || count <= 0 || !out) {
     err = "batch needs at least one handle";
     return FLUID_PP_INVALID_ARG;
@@ -587,7 +588,7 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
       long long total = 0;
       for (const InstDev& I : insts)
         if (grid(I)) total += shape_tiles(I.lv[l + 1].nx, I.lv[l + 1].ny, I.lv[l + 1].nz, kDownShapes[pick]);
-      if (total >= kFillTiles || pick == 4) {
+      if (tu.box_shape >= 0 ? pick == std::min(tu.box_shape, 4) : (total >= tu.fill_tiles || pick == 4)) {
         for (InstDev& I : insts)
           if (grid(I)) {
             LevelDev& L = I.lv[l];
@@ -604,7 +605,7 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
       long long total = 0;
       for (const InstDev& I : insts)
         if (grid(I)) total += shape_tiles(I.lv[l].nx, I.lv[l].ny, I.lv[l].nz, kUpShapes[pick]);
-      if (total >= kFillTiles || pick == 4) {
+      if (tu.box_shape >= 0 ? pick == std::min(tu.box_shape, 4) : (total >= tu.fill_tiles || pick == 4)) {
         for (InstDev& I : insts)
           if (grid(I)) {
             LevelDev& L = I.lv[l];
@@ -644,9 +645,10 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
     // levels 0 and 1 coarsened by two on every axis take the marching steps when
     // the batch has enough of their tiles to fill the GPU (a lone small lattice
     // keeps the box kernels, whose tile shape follows the lattice)
-    auto eligible = [l](const InstDev& I) {
+    const int march_levels = std::min(tu.march_levels, kMarchLevels);
+    auto eligible = [l, march_levels](const InstDev& I) {
       const LevelDev& C = I.lv[l + 1];
-      return l <= kMarchLevels - 1 && C.sx == 2 && C.sy == 2 && C.sz == 2;
+      return l <= march_levels - 1 && C.sx == 2 && C.sy == 2 && C.sz == 2;
     };
     long long march_total = 0;
     for (int k = 0; k < count; ++k)
@@ -654,7 +656,7 @@ static int batch_build(fluid_pp* const* handles, int count, fluid_pp_batch** out
         const LevelDev& C = insts[k].lv[l + 1];
         march_total += march_down_tiles(C.nx, C.ny, C.nz);
       }
-    const bool march_level = march_total >= kFillTiles;
+    const bool march_level = march_total >= tu.fill_tiles;
     auto marching = [&](const InstDev& I) { return march_level && eligible(I); };
     B->dn[l].off = int(tiles.size());
     for (int k = 0; k < count; ++k)
@@ -1089,7 +1091,9 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
   I.ctrl = static_cast<Ctrl*>(a.take(sizeof(Ctrl)));
   fluid_pp* raw = h.get();
   std::string err;
-  int rc = batch_build(&raw, 1, &h->self, err);
+  fluid_pp_batch_tuning tu;
+  fluid_pp_batch_tuning_default(&tu);
+  int rc = batch_build(&raw, 1, tu, &h->self, err);
   if (rc != FLUID_PP_OK) {
     g_err = err;
     dev_release(h->arena, h->stream);
@@ -1321,9 +1325,30 @@ int fluid_pp_apply_vcycle(fluid_pp* pp, const float* r, float* z, int pre, int p
 }
 
 // ------------------------------------------------------------------ batch API
+void fluid_pp_batch_tuning_default(fluid_pp_batch_tuning* tuning) {
+  if (!tuning) return;
+  tuning->fill_tiles = kFillTiles;
+  tuning->march_levels = kMarchLevels;
+  tuning->box_shape = -1;
+}
+
 int fluid_pp_batch_create(fluid_pp* const* handles, int count, fluid_pp_batch** out) {
+  return fluid_pp_batch_create_tuned(handles, count, nullptr, out);
+}
+
+int fluid_pp_batch_create_tuned(fluid_pp* const* handles, int count, const fluid_pp_batch_tuning* tuning,
+                                fluid_pp_batch** out) {
+  fluid_pp_batch_tuning tu;
+  fluid_pp_batch_tuning_default(&tu);
+  if (tuning) {
+    if (tuning->fill_tiles < 1 || tuning->march_levels < 0 || tuning->box_shape < -1 || tuning->box_shape > 4) {
+      g_err = "batch tuning: fill_tiles >= 1, march_levels >= 0, box_shape in -1..4";
+      return FLUID_PP_INVALID_ARG;
+    }
+    tu = *tuning;
+  }
   std::string err;
-  const int rc = batch_build(handles, count, out, err);
+  const int rc = batch_build(handles, count, tu, out, err);
   g_err = err;
   return rc;
 }

@@ -16,7 +16,7 @@ import ctypes
 import numpy as np
 
 from . import _abi
-from ._abi import Config, Receipt, SolveOpts, load, ptr
+from ._abi import BatchTuning, Config, Receipt, SolveOpts, load, ptr
 
 
 class FluidError(RuntimeError):
@@ -229,14 +229,38 @@ class PressureProjector:
         return z
 
 
-class BatchProjector:
-    """Projects several handles with one launch per stage (uneven grid sizes allowed)."""
+def batch_tuning(fill_tiles=None, march_levels=None, box_shape=None) -> BatchTuning:
+    """The library's default batch layout with the given fields replaced
+    (``fluid_pp_batch_tuning``; results never depend on it, only speed)."""
+    t = BatchTuning()
+    load().fluid_pp_batch_tuning_default(ctypes.byref(t))
+    if fill_tiles is not None:
+        t.fill_tiles = int(fill_tiles)
+    if march_levels is not None:
+        t.march_levels = int(march_levels)
+    if box_shape is not None:
+        t.box_shape = int(box_shape)
+    return t
 
-    def __init__(self, projectors):
+
+class BatchProjector:
+    """Projects several handles with one launch per stage (uneven grid sizes allowed).
+
+    ``tuning`` (a dict of ``batch_tuning`` fields, a ``BatchTuning`` or None for
+    the default) sets how the batch lays out its work; ``fluid_b200.autotune``
+    picks it by measurement.
+    """
+
+    def __init__(self, projectors, tuning=None):
         self.projectors = list(projectors)
         arr = (ctypes.c_void_p * len(self.projectors))(*(p.handle for p in self.projectors))
         b = ctypes.c_void_p()
-        _check(load().fluid_pp_batch_create(arr, len(self.projectors), ctypes.byref(b)), None, "batch_create")
+        if tuning is None:
+            rc = load().fluid_pp_batch_create(arr, len(self.projectors), ctypes.byref(b))
+        else:
+            t = tuning if isinstance(tuning, BatchTuning) else batch_tuning(**tuning)
+            rc = load().fluid_pp_batch_create_tuned(arr, len(self.projectors), ctypes.byref(t), ctypes.byref(b))
+        _check(rc, None, "batch_create")
         self._b = b
 
     def destroy(self):
@@ -301,14 +325,14 @@ class PipelinedBatchProjector:
     run synchronously.  Results are those of ``BatchProjector.project``.
     """
 
-    def __init__(self, projector_sets):
+    def __init__(self, projector_sets, tuning=None):
         self.sets = [list(s) for s in projector_sets]
         if len(self.sets) < 2 or any(len(s) != len(self.sets[0]) for s in self.sets):
             raise ValueError("need at least two projector sets of equal size")
         for s in self.sets[1:]:
             if [p.dims for p in s] != [p.dims for p in self.sets[0]]:
                 raise ValueError("projector sets must hold the same lattices in the same order")
-        self.batches = [BatchProjector(s) for s in self.sets]
+        self.batches = [BatchProjector(s, tuning=tuning) for s in self.sets]
         self._pending = [None] * len(self.sets)   # ticket in flight per slot
         self._done = {}
         self._next = 0

@@ -186,6 +186,25 @@ int fluid_pp_batch_project(fluid_pp_batch* batch, const float* dts, const fluid_
 int fluid_pp_batch_project_async(fluid_pp_batch* batch, const float* dts, const fluid_pp_solve_opts* opts);
 int fluid_pp_batch_receipts_read(fluid_pp_batch* batch, fluid_pp_receipt* receipts);
 
+/* How a batch lays out its work (no reference counterpart: the reference
+ * solves one grid per device).  A launch of a V-cycle step needs enough tiles
+ * to fill the GPU; fill_tiles is that count (default 296, two per SM): the box
+ * kernels take the largest tile shape whose tiles over the batch reach it, and
+ * a level of the finest march_levels (0, 1 or 2; default 2) takes the 2.5-D
+ * marching form when its marching tiles reach it.  box_shape 0..4 forces a box
+ * tile shape (largest first), -1 (default) leaves it to fill_tiles.  Every
+ * layout applies the same arithmetic per cell and folds every scalar over the
+ * same fixed tiles, so a batch's results do not depend on its tuning, bit for
+ * bit; only its speed does (fluid_b200.autotune measures the candidates). */
+typedef struct fluid_pp_batch_tuning {
+  int fill_tiles;
+  int march_levels;
+  int box_shape;
+} fluid_pp_batch_tuning;
+void fluid_pp_batch_tuning_default(fluid_pp_batch_tuning* tuning);
+int fluid_pp_batch_create_tuned(fluid_pp* const* handles, int count, const fluid_pp_batch_tuning* tuning,
+                                fluid_pp_batch** out);
+
 /* Solve a batch through CUDA graphs (on = 1, the default: the solve is captured
  * once per option set and replayed) or with direct launches (on = 0: for a batch
  * that lives for a few solves, e.g. a serving tick, capture would cost more

@@ -307,3 +307,41 @@ def test_full_size_dam_spheres_properties():
         rec = pp.project(s.dt, rel_tol=REL_RES, rel_tol_inf=0.5 * DIV_RATIO)
         assert rec["status_name"] == "OK", rec
         assert rec["max_div_after"] <= DIV_RATIO * rec["max_div_before"], rec
+
+
+def test_batch_layouts_give_the_same_bits_and_autotune_keeps_the_fastest():
+    """Every batch layout (box shapes, marching on or off, fill counts) gives the
+    default layout's pressures and iteration counts bit for bit; the autotuner's
+    choice is never slower than the default it measured."""
+    from fluid_b200 import autotune
+    from fluid_b200.projector import batch_tuning
+    states = [configs.random_small(64, 48, 64, seed=90 + k) for k in range(13)]
+    pps = [PressureProjector((s.nx, s.ny, s.nz), s.h, precision="fp16") for s in states]
+
+    def restore():
+        for pp, s in zip(pps, states):
+            pp.upload_state(s.vof, s.u, s.v, s.w)
+
+    dts = [s.dt for s in states]
+    layouts = [None, dict(march_levels=0), dict(march_levels=1, fill_tiles=148), dict(box_shape=4, march_levels=0),
+               dict(fill_tiles=4096)]
+    ref = None
+    for lay in layouts:
+        b = BatchProjector(pps, tuning=lay)
+        restore()
+        recs = b.project(dts)
+        got = ([r["iterations"] for r in recs], [pp.pressure_cells() for pp in pps])
+        b.destroy()
+        assert all(r["status_name"] == "OK" for r in recs), lay
+        if ref is None:
+            ref = got
+            continue
+        assert got[0] == ref[0], lay
+        for a, c in zip(got[1], ref[1]):
+            np.testing.assert_array_equal(a, c, err_msg=str(lay))
+    cands = tuple(dict(batch_tuning(**lay).as_dict()) for lay in [dict(), dict(march_levels=0), dict(fill_tiles=148)])
+    res = autotune.autotune_batch(pps, dts, restore, layouts=cands, sweeps=((1, 1), (2, 2)), repeats=1)
+    assert res.ms <= res.default_ms
+    assert len(res.table) == 4 and res.sweeps in ((1, 1), (2, 2))
+    for pp in pps:
+        pp.destroy()
