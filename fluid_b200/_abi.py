@@ -37,6 +37,7 @@ EXPORTS = (
     "fluid_pp_tall_project_begin", "fluid_pp_tall_project_continue", "fluid_pp_tall_project_end",
     "fluid_pp_batch_project_async", "fluid_pp_batch_receipts_read", "fluid_pp_download_async",
     "fluid_pp_synchronize", "fluid_pp_batch_tuning_default", "fluid_pp_batch_create_tuned",
+    "fluid_pp_batch_upload_state", "fluid_pp_batch_download_async",
 )
 STAGES = ("reset", "label", "coarsen", "bake", "factor", "init", "smooth0", "smoothc", "residual0", "residualc",
           "restrict0", "restrictc", "coarse", "prolong0", "prolongc", "dot", "dir", "spmv", "update", "true",
@@ -121,6 +122,8 @@ def load():
     L.fluid_pp_batch_destroy.restype = None
     L.fluid_pp_batch_project.argtypes = [vp, vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(Receipt)]
     L.fluid_pp_batch_project_async.argtypes = [vp, vp, ctypes.POINTER(SolveOpts)]
+    L.fluid_pp_batch_upload_state.argtypes = [vp, vp, vp, vp, vp]
+    L.fluid_pp_batch_download_async.argtypes = [vp, vp, vp, vp, vp]
     L.fluid_pp_batch_tuning_default.argtypes = [ctypes.POINTER(BatchTuning)]
     L.fluid_pp_batch_tuning_default.restype = None
     L.fluid_pp_batch_create_tuned.argtypes = [ctypes.POINTER(vp), ci, ctypes.POINTER(BatchTuning), ctypes.POINTER(vp)]

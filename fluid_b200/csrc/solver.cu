@@ -1432,6 +1432,35 @@ int fluid_pp_batch_project_async(fluid_pp_batch* B, const float* dts, const flui
   return rc;
 }
 
+int fluid_pp_batch_upload_state(fluid_pp_batch* B, const float* const* vof, const float* const* u,
+                                const float* const* v, const float* const* w) {
+  if (!B || !vof || !u || !v || !w) return FLUID_PP_INVALID_ARG;
+  for (size_t k = 0; k < B->h.size(); ++k) {
+    const int rc = upload(B->h[k], vof[k], u[k], v[k], w[k], cudaMemcpyHostToDevice);
+    if (rc != FLUID_PP_OK) {
+      B->err = B->h[k]->err;
+      g_err = B->err;
+      return rc;
+    }
+  }
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_batch_download_async(fluid_pp_batch* B, float* const* p, float* const* u, float* const* v,
+                                  float* const* w) {
+  if (!B) return FLUID_PP_INVALID_ARG;
+  for (size_t k = 0; k < B->h.size(); ++k) {
+    const int rc = fluid_pp_download_async(B->h[k], p ? p[k] : nullptr, u ? u[k] : nullptr, v ? v[k] : nullptr,
+                                           w ? w[k] : nullptr);
+    if (rc != FLUID_PP_OK) {
+      B->err = B->h[k]->err;
+      g_err = B->err;
+      return rc;
+    }
+  }
+  return FLUID_PP_OK;
+}
+
 int fluid_pp_batch_receipts_read(fluid_pp_batch* B, fluid_pp_receipt* receipts) {
   if (!B) return FLUID_PP_INVALID_ARG;
   cudaSetDevice(B->device);

@@ -360,11 +360,22 @@ class PipelinedBatchProjector:
         projs = self.sets[slot]
         if len(inputs) != len(projs) or len(outputs) != len(projs):
             raise ValueError(f"need {len(projs)} inputs and outputs")
-        for p, arrs in zip(projs, inputs):
-            p.upload_state(*arrs)
-        self.batches[slot].project_async(dts, **opts)
-        for p, arrs in zip(projs, outputs):
-            p.download_async(*arrs)
+        n = len(projs)
+        tabs = [(ctypes.c_void_p * n)() for _ in range(8)]   # vof u v w in, p u v w out
+        for k, (p, ins, outs) in enumerate(zip(projs, inputs, outputs)):
+            nx, ny, nz = p.dims
+            sizes = (nx * ny * nz, (nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1))
+            for j, (a, size) in enumerate(zip(list(ins) + list(outs), sizes + sizes)):
+                if a is None and j >= 4:
+                    continue
+                if a is None or a.dtype != np.float32 or a.size != size or not a.flags.c_contiguous:
+                    raise ValueError(f"lattice {k}: array {j} must be a C-contiguous float32 array of {size} entries")
+                tabs[j][k] = a.ctypes.data
+        b = self.batches[slot]
+        L = load()
+        _check(L.fluid_pp_batch_upload_state(b._b, *tabs[:4]), None, "batch_upload_state")
+        b.project_async(dts, **opts)
+        _check(L.fluid_pp_batch_download_async(b._b, *tabs[4:]), None, "batch_download_async")
         self._pending[slot] = t
         self._next = t + 1
         return t

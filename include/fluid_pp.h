@@ -185,6 +185,13 @@ int fluid_pp_batch_project(fluid_pp_batch* batch, const float* dts, const fluid_
  * overlapping the solve of the other. */
 int fluid_pp_batch_project_async(fluid_pp_batch* batch, const float* dts, const fluid_pp_solve_opts* opts);
 int fluid_pp_batch_receipts_read(fluid_pp_batch* batch, fluid_pp_receipt* receipts);
+/* fluid_pp_upload_state and fluid_pp_download_async for every handle of the
+ * batch in one call: element k of each pointer array belongs to handle k (any
+ * of the download arrays may be NULL, and so may an element). */
+int fluid_pp_batch_upload_state(fluid_pp_batch* batch, const float* const* vof, const float* const* u,
+                                const float* const* v, const float* const* w);
+int fluid_pp_batch_download_async(fluid_pp_batch* batch, float* const* p, float* const* u, float* const* v,
+                                  float* const* w);
 
 /* How a batch lays out its work (no reference counterpart: the reference
  * solves one grid per device).  A launch of a V-cycle step needs enough tiles
