@@ -539,8 +539,8 @@ def main():
         "failed_solves": len(bad),
         "autotune": {"candidates": len(tune.table), "chosen_ms": tune.ms, "default_layout_ms": tune.default_ms,
                      "table": [[r["tuning"]["fill_tiles"], r["tuning"]["march_levels"], r["tuning"]["box_shape"],
-                                list(r["sweeps"]), round(r["ms"], 3)] for r in tune.table],
-                     "table_columns": ["fill_tiles", "march_levels", "box_shape", "sweeps", "median_ms"],
+                                r["tuning"]["parts"], list(r["sweeps"]), round(r["ms"], 3)] for r in tune.table],
+                     "table_columns": ["fill_tiles", "march_levels", "box_shape", "parts", "sweeps", "median_ms"],
                      "note": "median solve of each candidate layout / sweep schedule on this batch before timing"},
         "dam_spheres_128x96x128": {
             "workload": WORKLOAD2, "steps": steps2,

@@ -64,7 +64,8 @@ class SolveOpts(ctypes.Structure):
 
 
 class BatchTuning(ctypes.Structure):
-    _fields_ = [("fill_tiles", ctypes.c_int), ("march_levels", ctypes.c_int), ("box_shape", ctypes.c_int)]
+    _fields_ = [("fill_tiles", ctypes.c_int), ("march_levels", ctypes.c_int), ("box_shape", ctypes.c_int),
+                ("parts", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -1,12 +1,14 @@
 """Measured choice of a batch's work layout and smoothing schedule.
 
 A batch of uneven lattices can lay its V-cycle work out several ways: the box
-kernels' tile shape, the 2.5-D marching form on the finest levels, and the tile
-count a launch must reach before a larger shape or the marching form is used
-(``fluid_pp_batch_tuning``).  The library's default rule picks one from tile
-counts alone.  ``autotune_batch`` instead times the candidates on the caller's
-own batch and keeps the fastest, then tries the other smoothing schedules
-(sweeps down and up per V-cycle) with that layout.
+kernels' tile shape, the 2.5-D marching form on the finest levels, the tile
+count a launch must reach before a larger shape or the marching form is used,
+and how many concurrent parts (sub-batches on their own streams) the handles
+are split into (``fluid_pp_batch_tuning``).  The library's default rule picks
+from tile counts alone, with one part.  ``autotune_batch`` instead times the
+candidates on the caller's own batch: the layouts with one part, then the best
+of those split into more parts, then the other smoothing schedules (sweeps
+down and up per V-cycle) with the fastest layout.
 
 Layouts never change results: every layout applies the same arithmetic per
 cell and folds the CG scalars over the same fixed tiles, so they give the same
@@ -27,7 +29,8 @@ from dataclasses import asdict, dataclass, field
 from .projector import BatchProjector, batch_tuning
 
 # fill_tiles: one or four resident tiles per SM, or the default two
-LAYOUTS = tuple(dict(fill_tiles=f, march_levels=m, box_shape=-1) for f in (148, 296, 592) for m in (0, 1, 2))
+LAYOUTS = tuple(dict(fill_tiles=f, march_levels=m, box_shape=-1, parts=1) for f in (148, 296, 592) for m in (0, 1, 2))
+PARTS = (2, 3, 4)
 SWEEPS = ((1, 1), (2, 2))
 
 
@@ -64,8 +67,8 @@ def _load(cache_path):
         return json.load(f)
 
 
-def autotune_batch(projectors, dts, restore, *, rel_tol=1e-6, layouts=LAYOUTS, sweeps=SWEEPS, repeats=3,
-                   cache_path=None) -> TuneResult:
+def autotune_batch(projectors, dts, restore, *, rel_tol=1e-6, layouts=LAYOUTS, parts=PARTS, sweeps=SWEEPS,
+                   repeats=3, cache_path=None) -> TuneResult:
     """Time ``repeats`` solves (after one untimed) of each candidate on this batch.
 
     ``restore()`` must put every projector's step input back on the device (a
@@ -109,6 +112,16 @@ def autotune_batch(projectors, dts, restore, *, rel_tol=1e-6, layouts=LAYOUTS, s
         b = BatchProjector(projectors)
         try:
             table.append(dict(tuning=default, sweeps=(1, 1), ms=solve_ms(b, 1, 1)))
+        finally:
+            b.destroy()
+    best_layout = pick(table)["tuning"]
+    for np_ in parts:
+        if np_ < 2 or np_ > len(projectors):
+            continue
+        lay = dict(best_layout, parts=np_)
+        b = BatchProjector(projectors, tuning=lay)
+        try:
+            table.append(dict(tuning=lay, sweeps=(1, 1), ms=solve_ms(b, 1, 1)))
         finally:
             b.destroy()
     best_layout = pick(table)["tuning"]

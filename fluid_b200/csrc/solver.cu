@@ -71,6 +71,7 @@ struct fluid_pp {
   bool has_pressure = false;
   float last_dt = 0.f;
   fluid_pp_batch* self = nullptr;   // batch of one
+  long long plan_cells() const { return (long long)cfg.nx * cfg.ny * cfg.nz; }
   int set_error(int code, const std::string& m) {
     err = m;
     return code;
@@ -125,6 +126,17 @@ struct fluid_pp_batch {
   // CUDA graphs for the solve (on by default); a batch whose composition changes
   // every few solves runs direct launches instead of paying for a new capture
   bool use_graphs = true;
+  // Concurrent parts (batch tuning `parts` > 1): sub-batches of the handles on
+  // streams of their own, each with its own graphs, launched together after an
+  // event on this batch's stream and joined back to it, so that one part's
+  // small launches and last iterations overlap another part's work.  Only
+  // graph-mode solves use them; direct launches run the whole batch.
+  std::vector<fluid_pp_batch*> parts;
+  std::vector<std::vector<int>> part_idx;   // handle indices (into h) of each part
+  std::vector<cudaStream_t> part_streams;
+  std::vector<cudaEvent_t> part_done;
+  cudaEvent_t part_start = nullptr;
+  bool parts_pending = false;               // the last solve ran in parts: receipts come from them
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
   std::vector<int> ev_stage;
@@ -748,6 +760,54 @@ static int batch_build(fluid_pp* const* handles, int count, const fluid_pp_batch
     fluid_pp_batch_destroy(B.release());
     return e == cudaErrorMemoryAllocation ? FLUID_PP_OOM : FLUID_PP_CUDA;
   }
+  const int np = std::min(tu.parts, count);
+  if (np > 1) {
+    // handles to parts by cells, largest first onto the lightest part; each
+    // part keeps the batch's order and needs 1/np of the tiles to fill the GPU
+    std::vector<int> order(count);
+    for (int k = 0; k < count; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+      return B->h[a]->plan_cells() > B->h[b]->plan_cells();
+    });
+    std::vector<long long> load(np, 0);
+    std::vector<int> part_of(count, 0);
+    for (int k : order) {
+      const int j = int(std::min_element(load.begin(), load.end()) - load.begin());
+      part_of[k] = j;
+      load[j] += B->h[k]->plan_cells();
+    }
+    fluid_pp_batch_tuning sub = tu;
+    sub.parts = 1;
+    sub.fill_tiles = std::max(1, tu.fill_tiles / np);
+    B->part_idx.assign(np, {});
+    for (int k = 0; k < count; ++k) B->part_idx[part_of[k]].push_back(k);
+    e = cudaEventCreateWithFlags(&B->part_start, cudaEventDisableTiming);
+    for (int j = 0; j < np && e == cudaSuccess; ++j) {
+      std::vector<fluid_pp*> hs;
+      for (int k : B->part_idx[j]) hs.push_back(B->h[k]);
+      fluid_pp_batch* P = nullptr;
+      std::string perr;
+      const int rc = batch_build(hs.data(), int(hs.size()), sub, &P, perr);
+      if (rc != FLUID_PP_OK) {
+        err = "batch part: " + perr;
+        fluid_pp_batch_destroy(B.release());
+        return rc;
+      }
+      B->parts.push_back(P);
+      cudaStream_t st = nullptr;
+      cudaEvent_t done = nullptr;
+      e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+      B->part_streams.push_back(st);
+      B->part_done.push_back(done);
+      P->stream = st;
+    }
+    if (e != cudaSuccess) {
+      err = std::string("batch parts: ") + cudaGetErrorString(e);
+      fluid_pp_batch_destroy(B.release());
+      return FLUID_PP_CUDA;
+    }
+  }
   *out = B.release();
   return FLUID_PP_OK;
 }
@@ -870,6 +930,62 @@ static int batch_project_t(fluid_pp_batch* B, const float* dts, const fluid_pp_s
 }
 
 static int batch_project(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts* opts, bool sync,
+                         fluid_pp_receipt* receipts);
+
+// Receipts of a solve that ran in the batch's parts (waits for the batch's stream).
+static int parts_receipts(fluid_pp_batch* B, fluid_pp_receipt* receipts) {
+  const cudaError_t e = cudaStreamSynchronize(B->stream);
+  if (e != cudaSuccess) {
+    B->err = std::string("project: ") + cudaGetErrorString(e);
+    return FLUID_PP_CUDA;
+  }
+  int worst = FLUID_PP_OK;
+  for (size_t j = 0; j < B->parts.size(); ++j) {
+    fluid_pp_batch* P = B->parts[j];
+    if (P->pending_graph_count) {
+      g_launches.fetch_add((unsigned long long)(*P->h_loop) * P->n_body, std::memory_order_relaxed);
+      P->pending_graph_count = false;
+    }
+    for (size_t i = 0; i < B->part_idx[j].size(); ++i) {
+      const int k = B->part_idx[j][i];
+      if (receipts) fill_receipt(B->h[k], P->h_ctrl[i], receipts + k);
+      B->h[k]->has_pressure = true;
+      if (P->h_ctrl[i].status != FLUID_PP_OK && worst == FLUID_PP_OK) worst = P->h_ctrl[i].status;
+    }
+  }
+  B->parts_pending = false;
+  return worst;
+}
+
+// Every part's graph-mode solve, started together after this batch's stream
+// reaches the launch point and joined back to it.
+static int parts_project(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts* opts) {
+  cudaError_t e = cudaEventRecord(B->part_start, B->stream);
+  std::vector<float> dp;
+  for (size_t j = 0; j < B->parts.size() && e == cudaSuccess; ++j) {
+    fluid_pp_batch* P = B->parts[j];
+    e = cudaStreamWaitEvent(P->stream, B->part_start, 0);
+    if (e != cudaSuccess) break;
+    dp.clear();
+    if (dts)
+      for (int k : B->part_idx[j]) dp.push_back(dts[k]);
+    const int rc = batch_project(P, dts ? dp.data() : nullptr, opts, false, nullptr);
+    if (rc != FLUID_PP_OK) {
+      B->err = P->err;
+      return rc;
+    }
+    e = cudaEventRecord(B->part_done[j], P->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(B->stream, B->part_done[j], 0);
+  }
+  if (e != cudaSuccess) {
+    B->err = std::string("parts: ") + cudaGetErrorString(e);
+    return FLUID_PP_CUDA;
+  }
+  B->parts_pending = true;
+  return FLUID_PP_OK;
+}
+
+static int batch_project(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts* opts, bool sync,
                          fluid_pp_receipt* receipts) {
   const fluid_pp_solve_opts o = opts ? *opts : default_opts();
   if (!(o.rel_tol >= 0) || !(o.abs_tol >= 0) || o.max_iters < 1 || o.pre_sweeps < 0 || o.post_sweeps < 0) {
@@ -882,6 +998,12 @@ static int batch_project(fluid_pp_batch* B, const float* dts, const fluid_pp_sol
       return FLUID_PP_INVALID_ARG;
     }
   cudaSetDevice(B->device);
+  B->parts_pending = false;
+  if (!B->parts.empty() && B->use_graphs && !B->profiling) {
+    const int rc = parts_project(B, dts, &o);
+    if (rc != FLUID_PP_OK || !sync) return rc;
+    return parts_receipts(B, receipts);
+  }
   switch (B->precision) {
     case FLUID_PP_FP16: return batch_project_t<__half>(B, dts, o, sync, receipts);
     case FLUID_PP_BF16: return batch_project_t<__nv_bfloat16>(B, dts, o, sync, receipts);
@@ -1330,6 +1452,7 @@ void fluid_pp_batch_tuning_default(fluid_pp_batch_tuning* tuning) {
   tuning->fill_tiles = kFillTiles;
   tuning->march_levels = kMarchLevels;
   tuning->box_shape = -1;
+  tuning->parts = 1;
 }
 
 int fluid_pp_batch_create(fluid_pp* const* handles, int count, fluid_pp_batch** out) {
@@ -1341,8 +1464,9 @@ int fluid_pp_batch_create_tuned(fluid_pp* const* handles, int count, const fluid
   fluid_pp_batch_tuning tu;
   fluid_pp_batch_tuning_default(&tu);
   if (tuning) {
-    if (tuning->fill_tiles < 1 || tuning->march_levels < 0 || tuning->box_shape < -1 || tuning->box_shape > 4) {
-      g_err = "batch tuning: fill_tiles >= 1, march_levels >= 0, box_shape in -1..4";
+    if (tuning->fill_tiles < 1 || tuning->march_levels < 0 || tuning->box_shape < -1 || tuning->box_shape > 4 ||
+        tuning->parts < 1 || tuning->parts > 16) {
+      g_err = "batch tuning: fill_tiles >= 1, march_levels >= 0, box_shape in -1..4, parts in 1..16";
       return FLUID_PP_INVALID_ARG;
     }
     tu = *tuning;
@@ -1356,6 +1480,12 @@ int fluid_pp_batch_create_tuned(fluid_pp* const* handles, int count, const fluid
 void fluid_pp_batch_destroy(fluid_pp_batch* B) {
   if (!B) return;
   cudaSetDevice(B->device);
+  for (fluid_pp_batch* P : B->parts) fluid_pp_batch_destroy(P);
+  for (cudaStream_t st : B->part_streams)
+    if (st) cudaStreamDestroy(st);
+  for (cudaEvent_t ev : B->part_done)
+    if (ev) cudaEventDestroy(ev);
+  if (B->part_start) cudaEventDestroy(B->part_start);
   destroy_graphs(B);
   dev_release(B->d_insts, B->stream);
   dev_release(B->d_ctrl, B->stream);
@@ -1464,6 +1594,11 @@ int fluid_pp_batch_download_async(fluid_pp_batch* B, float* const* p, float* con
 int fluid_pp_batch_receipts_read(fluid_pp_batch* B, fluid_pp_receipt* receipts) {
   if (!B) return FLUID_PP_INVALID_ARG;
   cudaSetDevice(B->device);
+  if (B->parts_pending) {
+    const int rc = parts_receipts(B, receipts);
+    if (rc == FLUID_PP_CUDA) g_err = B->err;
+    return rc;
+  }
   const cudaError_t e = cudaStreamSynchronize(B->stream);
   if (e != cudaSuccess) {
     B->err = std::string("project: ") + cudaGetErrorString(e);

@@ -229,7 +229,7 @@ class PressureProjector:
         return z
 
 
-def batch_tuning(fill_tiles=None, march_levels=None, box_shape=None) -> BatchTuning:
+def batch_tuning(fill_tiles=None, march_levels=None, box_shape=None, parts=None) -> BatchTuning:
     """The library's default batch layout with the given fields replaced
     (``fluid_pp_batch_tuning``; results never depend on it, only speed)."""
     t = BatchTuning()
@@ -240,6 +240,8 @@ def batch_tuning(fill_tiles=None, march_levels=None, box_shape=None) -> BatchTun
         t.march_levels = int(march_levels)
     if box_shape is not None:
         t.box_shape = int(box_shape)
+    if parts is not None:
+        t.parts = int(parts)
     return t
 
 

@@ -199,14 +199,20 @@ int fluid_pp_batch_download_async(fluid_pp_batch* batch, float* const* p, float*
  * kernels take the largest tile shape whose tiles over the batch reach it, and
  * a level of the finest march_levels (0, 1 or 2; default 2) takes the 2.5-D
  * marching form when its marching tiles reach it.  box_shape 0..4 forces a box
- * tile shape (largest first), -1 (default) leaves it to fill_tiles.  Every
- * layout applies the same arithmetic per cell and folds every scalar over the
- * same fixed tiles, so a batch's results do not depend on its tuning, bit for
- * bit; only its speed does (fluid_b200.autotune measures the candidates). */
+ * tile shape (largest first), -1 (default) leaves it to fill_tiles.  parts
+ * (1..16, default 1) splits the handles into that many sub-batches of about
+ * equal cells, each solved on a stream of its own, all started together and
+ * joined back to the batch's stream (graph-mode solves; direct launches run
+ * the whole batch), so that one part's small launches and last iterations
+ * overlap another's work.  Every layout applies the same arithmetic per cell
+ * and folds every scalar over the same fixed tiles of one instance, so a
+ * batch's results do not depend on its tuning, bit for bit; only its speed
+ * does (fluid_b200.autotune measures the candidates). */
 typedef struct fluid_pp_batch_tuning {
   int fill_tiles;
   int march_levels;
   int box_shape;
+  int parts;
 } fluid_pp_batch_tuning;
 void fluid_pp_batch_tuning_default(fluid_pp_batch_tuning* tuning);
 int fluid_pp_batch_create_tuned(fluid_pp* const* handles, int count, const fluid_pp_batch_tuning* tuning,

@@ -218,7 +218,8 @@ def test_marching_batch_is_identical_to_box_singles():
         pp.destroy()
 
 
-def test_pipelined_ticks_match_synchronous_batches():
+@pytest.mark.parametrize("tuning", [None, {"parts": 2}])
+def test_pipelined_ticks_match_synchronous_batches(tuning):
     """Four ticks of three lattices through PipelinedBatchProjector (two streams,
     two ticks in flight, pinned host buffers) give the receipts and the p, u, v, w
     of BatchProjector.project on each tick's inputs, bit for bit."""
@@ -248,7 +249,7 @@ def test_pipelined_ticks_match_synchronous_batches():
     for st, ps in zip(streams, sets):
         for pp in ps:
             pp.set_stream(st.cuda_stream)
-    pipe = PipelinedBatchProjector(sets)
+    pipe = PipelinedBatchProjector(sets, tuning=tuning)
 
     def pinned(a):
         return torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory().numpy()
@@ -310,7 +311,7 @@ def test_full_size_dam_spheres_properties():
 
 
 def test_batch_layouts_give_the_same_bits_and_autotune_keeps_the_fastest():
-    """Every batch layout (box shapes, marching on or off, fill counts) gives the
+    """Every batch layout (box shapes, marching on or off, fill counts, concurrent parts) gives the
     default layout's pressures and iteration counts bit for bit; the autotuner's
     choice is never slower than the default it measured."""
     from fluid_b200 import autotune
@@ -324,7 +325,7 @@ def test_batch_layouts_give_the_same_bits_and_autotune_keeps_the_fastest():
 
     dts = [s.dt for s in states]
     layouts = [None, dict(march_levels=0), dict(march_levels=1, fill_tiles=148), dict(box_shape=4, march_levels=0),
-               dict(fill_tiles=4096)]
+               dict(fill_tiles=4096), dict(parts=2), dict(parts=3, march_levels=0)]
     ref = None
     for lay in layouts:
         b = BatchProjector(pps, tuning=lay)
@@ -340,8 +341,8 @@ def test_batch_layouts_give_the_same_bits_and_autotune_keeps_the_fastest():
         for a, c in zip(got[1], ref[1]):
             np.testing.assert_array_equal(a, c, err_msg=str(lay))
     cands = tuple(dict(batch_tuning(**lay).as_dict()) for lay in [dict(), dict(march_levels=0), dict(fill_tiles=148)])
-    res = autotune.autotune_batch(pps, dts, restore, layouts=cands, sweeps=((1, 1), (2, 2)), repeats=1)
+    res = autotune.autotune_batch(pps, dts, restore, layouts=cands, parts=(2,), sweeps=((1, 1), (2, 2)), repeats=1)
     assert res.ms <= res.default_ms
-    assert len(res.table) == 4 and res.sweeps in ((1, 1), (2, 2))
+    assert len(res.table) == 5 and res.sweeps in ((1, 1), (2, 2))
     for pp in pps:
         pp.destroy()
