@@ -15,8 +15,8 @@ instance's state device-to-device, as a simulation step hands over its
 advected state); L2 is flushed (256 MB write) before every timed step; every
 step is timed with CUDA events on the launching stream.  `e2e` repeats the
 headline through the public API from pinned host buffers with the results read
-back to the host: PipelinedBatchProjector keeps two ticks in flight on two
-streams, so one tick's copies overlap the other's solve; `serial_solves_per_s`
+back to the host: PipelinedBatchProjector keeps three ticks in flight on three
+streams, so one tick's copies overlap the others' solves; `serial_solves_per_s`
 is the same ticks one after another.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
@@ -465,10 +465,11 @@ def main():
         p.destroy()
     e2e_serial = world * BATCH * len(e2e_ms) / (max_over_ranks(sum(e2e_ms)) / 1000.0)
 
-    # the same ticks with two batches in flight on two streams: one batch's
-    # uploads and read-back overlap the other's solve (PipelinedBatchProjector)
+    # the same ticks with three batches in flight on three streams: one batch's
+    # uploads and read-back overlap the others' solves (PipelinedBatchProjector)
     note("e2e pipelined")
-    side = [torch.cuda.Stream(), torch.cuda.Stream()]
+    depth = 3   # ticks in flight
+    side = [torch.cuda.Stream() for _ in range(depth)]
     sets = []
     for st in side:
         ps_ = make(args.precision)
@@ -476,7 +477,8 @@ def main():
             p.set_stream(st.cuda_stream)
         sets.append(ps_)
     pipe = PipelinedBatchProjector(sets, tuning=tune.tuning)
-    outs = [host_out, [tuple(torch.empty_like(t).pin_memory() for t in tup) for tup in host_out]]
+    outs = [host_out] + [[tuple(torch.empty_like(t).pin_memory() for t in tup) for tup in host_out]
+                         for _ in range(depth - 1)]
     ins_np = [tuple(t.numpy() for t in tup) for tup in host_in]
     outs_np = [[tuple(t.numpy() for t in tup) for tup in o] for o in outs]
     pipe_bad = 0
@@ -485,13 +487,13 @@ def main():
         nonlocal pipe_bad
         tickets = []
         for k in range(n):
-            slot = k % 2
-            if k >= 2:
-                pipe_bad += sum(r["status"] != 0 for r in pipe.result(tickets[k - 2]))
+            slot = k % depth
+            if k >= depth:
+                pipe_bad += sum(r["status"] != 0 for r in pipe.result(tickets[k - depth]))
             with torch.cuda.stream(side[slot]):
                 flush.zero_()   # L2 flushed before every tick, on the tick's own stream
             tickets.append(pipe.submit(ins_np, outs_np[slot], dts, **tuned))
-        for t in tickets[-2:]:
+        for t in tickets[-depth:]:
             pipe_bad += sum(r["status"] != 0 for r in pipe.result(t))
 
     pipe_ticks(args.warmup)
@@ -559,7 +561,7 @@ def main():
                      "stage_gbs": stage_gbs},
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "PipelinedBatchProjector: each tick uploads the 64 inputs from pinned host memory, projects "
-                        "and reads back p,u,v,w; two ticks in flight on two streams; timed over all ticks",
+                        "and reads back p,u,v,w; three ticks in flight on three streams; timed over all ticks",
                 "failed_solves": int(pipe_bad), "serial_solves_per_s": e2e_serial},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),

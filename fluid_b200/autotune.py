@@ -7,7 +7,7 @@ and how many concurrent parts (sub-batches on their own streams) the handles
 are split into (``fluid_pp_batch_tuning``).  The library's default rule picks
 from tile counts alone, with one part.  ``autotune_batch`` instead times the
 candidates on the caller's own batch: the layouts with one part, then the best
-of those split into more parts, then the other smoothing schedules (sweeps
+of those split into 2-8 parts, then the other smoothing schedules (sweeps
 down and up per V-cycle) with the fastest layout.
 
 Layouts never change results: every layout applies the same arithmetic per
@@ -30,7 +30,7 @@ from .projector import BatchProjector, batch_tuning
 
 # fill_tiles: one or four resident tiles per SM, or the default two
 LAYOUTS = tuple(dict(fill_tiles=f, march_levels=m, box_shape=-1, parts=1) for f in (148, 296, 592) for m in (0, 1, 2))
-PARTS = (2, 3, 4)
+PARTS = (2, 3, 4, 6, 8)
 SWEEPS = ((1, 1), (2, 2))
 
 
