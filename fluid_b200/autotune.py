@@ -28,7 +28,7 @@ from dataclasses import asdict, dataclass, field
 
 from .projector import BatchProjector, batch_tuning
 
-# fill_tiles: one or four resident tiles per SM, or the default two
+# fill_tiles: one (the default), two or four tiles per SM
 LAYOUTS = tuple(dict(fill_tiles=f, march_levels=m, box_shape=-1, parts=1) for f in (148, 296, 592) for m in (0, 1, 2))
 PARTS = (2, 3, 4, 6, 8)
 SWEEPS = ((1, 1), (2, 2))

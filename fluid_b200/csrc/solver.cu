@@ -28,7 +28,7 @@ using namespace fpp;
 namespace {
 
 constexpr int kMaxGrid = 148 * 8;   // 148 SMs x 8 resident 256-thread CTAs
-constexpr int kFillTiles = 2 * 148;  // fused-kernel tiles that give every SM two
+constexpr int kFillTiles = 148;  // fused-kernel tiles that give every SM one (the default fill count)
 
 // Fused-kernel tile shapes, largest first: coarse cells per down-step tile and
 // fine cells per up-step tile (level 0's up step always uses the CG kernels'
@@ -589,7 +589,7 @@ static int batch_build(fluid_pp* const* handles, int count, const fluid_pp_batch
   cudaSetDevice(B->device);
   // The batch's own copies of the instance descriptors.  Fused-kernel tile
   // shapes are chosen over the whole batch: the largest shape whose tiles,
-  // summed over every instance with that grid level, still give every SM two.
+  // summed over every instance with that grid level, still reach the fill count.
   // (Results do not depend on the shape: halo cells repeat their owner's
   // arithmetic.)
   std::vector<InstDev> insts(count);
@@ -1162,7 +1162,7 @@ int fluid_pp_create(const fluid_pp_config* cfg, fluid_pp** out) {
   }
   I.lv[plan.levels - 1].to_coarse = 1.0f;
   // Fused-kernel tile shapes per grid level for a solve on its own: the largest
-  // shape that still gives every SM two tiles (a batch re-chooses them over all
+  // shape that still gives every SM a tile (a batch re-chooses them over all
   // its instances, batch_build).
   for (int l = 0; l + 1 < plan.levels; ++l) {
     LevelDev& L = I.lv[l];

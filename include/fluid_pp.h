@@ -195,7 +195,7 @@ int fluid_pp_batch_download_async(fluid_pp_batch* batch, float* const* p, float*
 
 /* How a batch lays out its work (no reference counterpart: the reference
  * solves one grid per device).  A launch of a V-cycle step needs enough tiles
- * to fill the GPU; fill_tiles is that count (default 296, two per SM): the box
+ * to fill the GPU; fill_tiles is that count (default 148, one per SM): the box
  * kernels take the largest tile shape whose tiles over the batch reach it, and
  * a level of the finest march_levels (0, 1 or 2; default 2) takes the 2.5-D
  * marching form when its marching tiles reach it.  box_shape 0..4 forces a box

@@ -41,3 +41,19 @@ def test_cached_choice_is_returned_without_measuring(tmp_path):
     res = autotune.autotune_batch(ps, [1 / 60], never, cache_path=str(path))
     assert res.tuning == stored["tuning"] and res.sweeps == (1, 1) and res.ms == 1.5
     autotune._cache.pop(key, None)
+
+
+def test_tuning_defaults_and_rejected_fields():
+    """The library's default layout, and tunings it refuses before touching a GPU."""
+    import ctypes
+
+    from fluid_b200 import _abi
+    from fluid_b200.projector import batch_tuning
+    assert batch_tuning().as_dict() == {"fill_tiles": 148, "march_levels": 2, "box_shape": -1, "parts": 1}
+    L = _abi.load()
+    out = ctypes.c_void_p()
+    for bad in (dict(fill_tiles=0), dict(march_levels=-1), dict(box_shape=5), dict(parts=0), dict(parts=17)):
+        t = batch_tuning(**bad)
+        assert L.fluid_pp_batch_create_tuned(None, 0, ctypes.byref(t), ctypes.byref(out)) == _abi.INVALID_ARG, bad
+    good = batch_tuning(parts=4)
+    assert L.fluid_pp_batch_create_tuned(None, 0, ctypes.byref(good), ctypes.byref(out)) == _abi.INVALID_ARG
