@@ -472,14 +472,11 @@ __global__ void __launch_bounds__(kMThreads, 4) k_down_m(const InstDev* insts, c
 // ================================================================ up step
 // z_l += P z_{l+1} (mgProlongateAdd, mg.wgsl.ts:243-246; from level 1 into
 // level 0 the sigma scaling is undone), then one sweep black then red, one fine
-// tile per CTA.  On level 0 with `with_dot` the CTA also forms its partials of
-// gamma = r . (z - zmean) and the last tile of the instance finishes gamma and
-// beta (the k_dot_rz contract).
+// tile per CTA.  (gamma is folded by k_dot_rz_part over the fixed level-0
+// tiles, or by the level-0 marching up step.)
 template <class TZF, class TR, class TD, class TZC>
-__global__ void __launch_bounds__(kFThreads, 2) k_up(const InstDev* insts, const Tile* tiles, int level, int with_dot) {
+__global__ void __launch_bounds__(kFThreads, 2) k_up(const InstDev* insts, const Tile* tiles, int level) {
   extern __shared__ float sm[];
-  __shared__ double sh[32];
-  __shared__ int flag;
   const Tile tl = tiles[blockIdx.x];
   const InstDev& I = insts[tl.inst];
   Ctrl* c = I.ctrl;
@@ -576,33 +573,10 @@ __global__ void __launch_bounds__(kFThreads, 2) k_up(const InstDev* insts, const
   });
   __syncthreads();
   TZF* __restrict__ zo = static_cast<TZF*>(F.z);
-  double rz = 0.0, zsum = 0.0, rsum = 0.0;
   for_box(E, x0, y0, z0, TX, TY, TZ, 2, [&](int x, int y, int z, int s) {
     if (!inside(x, y, z, nx, ny, nz)) return;
-    const float zv = z_s[s];
-    zo[x + nx * (y + ny * z)] = fromf<TZF>(zv);
-    if (lab_s[s]) {
-      const double rv = rhs_s[s];
-      rz += rv * double(zv);
-      zsum += zv;
-      rsum += rv;
-    }
+    zo[x + nx * (y + ny * z)] = fromf<TZF>(z_s[s]);
   });
-  if (!with_dot) return;   // uniform over the launch
-  const int nt0 = I.ntiles0;
-  double* partial = I.partial;
-  const double a0 = block_sum(rz, sh), a1 = block_sum(zsum, sh), a2 = block_sum(rsum, sh);
-  if (threadIdx.x == 0) {
-    partial[0 * nt0 + tl.tile] = a0;
-    partial[1 * nt0 + tl.tile] = a1;
-    partial[2 * nt0 + tl.tile] = a2;
-  }
-  if (arrive_last(&c->arrive[kStGamma], nt0, &flag)) {
-    const double g = gather_slot(partial, 0, nt0, 0, sh);
-    const double zs = gather_slot(partial, 1, nt0, 0, sh);
-    const double rs = gather_slot(partial, 2, nt0, 0, sh);
-    if (threadIdx.x == 0) finish_gamma(c, g, zs, rs);
-  }
 }
 
 // ======================================================== marching up step
@@ -611,9 +585,10 @@ __global__ void __launch_bounds__(kFThreads, 2) k_up(const InstDev* insts, const
 // planes under them once.  Step p stages fine plane p of the halo box E = T +- 2
 // with the prolongated coarse correction added (each thread keeps its cells'
 // x / y taps for the whole march; coarse planes arrive in a ring of 3),
-// sweeps the black cells of plane p - 1 on T +- 1, then the red cells of plane
-// p - 2 on T, writing that plane's z.  Each cell gets k_up's arithmetic in the
-// same order.
+// sweeps the black cells of plane p - 2 on T +- 1, then the red cells of plane
+// p - 4 on T, writing that plane's z (the two-plane lags let one barrier per
+// step separate the phases).  Each cell gets k_up's arithmetic in the same
+// order.
 constexpr int kUX = 32, kUY = 16, kUZ = 16;            // fine cells per tile
 constexpr int kUEX = kUX + 4, kUEY = kUY + 4, kUEP = kUEX * kUEY;
 constexpr int kUQX = (kUX + 4) / 2 + 3, kUQY = (kUY + 4) / 2 + 3, kUQP = kUQX * kUQY;   // coarse plane box
@@ -873,79 +848,12 @@ __global__ void __launch_bounds__(kMThreads, 3) k_up_m(const InstDev* insts, con
   }
 }
 
-// ========================================================== direction + SpMV
-// d' = (z - zmean) + beta d on liquid cells, q = A d' and delta = d' . q
-// (applyLiquidOperator, atlas :1171-1192), alpha = gamma / delta.  The new
-// direction is written to the other buffer (Ctrl::dsel flips when the last
-// tile has arrived), so neighbours read the old direction race-free.
-__global__ void __launch_bounds__(kFThreads) k_dirspmv(const InstDev* insts, const Tile* tiles) {
-  __shared__ float dn_s[(kTX + 2) * (kTY + 2) * (8 + 2)];
-  __shared__ uint8_t lab_s[(kTX + 2) * (kTY + 2) * (8 + 2)];
-  __shared__ double sh[32];
-  __shared__ int flag;
-  const Tile tl = tiles[blockIdx.x];
-  const InstDev& I = insts[tl.inst];
-  Ctrl* c = I.ctrl;
-  if (c->done) return;
-  const LevelDev& L = I.lv[0];
-  const int nx = L.nx, ny = L.ny, nz = L.nz;
-  const int ntx = (nx + kTX - 1) / kTX, nty = (ny + kTY - 1) / kTY;
-  const int tx = tl.tile % ntx, tr = tl.tile / ntx, ty = tr % nty, tz = tr / nty;
-  const int x0 = tx * kTX, y0 = ty * kTY, z0 = tz * 8;
-  const SBox B{x0 - 1, y0 - 1, z0 - 1, kTX + 2, kTY + 2, 8 + 2};
-  const int sel = c->dsel;
-  const float beta = float(c->beta), zm = float(c->zmean);
-  const float* __restrict__ z = static_cast<const float*>(L.z);
-  const float* __restrict__ dold = sel ? I.d2 : I.d;
-  float* __restrict__ dnew = sel ? I.d : I.d2;
-  const uint8_t* __restrict__ lab = L.label;
-  stage_box<4, Cell3>(
-      B,
-      [&](int x, int y, int zz, bool ok) {
-        Cell3 v{0.0f, 0.0f, 0};
-        if (ok && inside(x, y, zz, nx, ny, nz)) {
-          const int i = x + nx * (y + ny * zz);
-          v.lb = lab[i];
-          v.a = z[i];
-          v.b = dold[i];
-        }
-        return v;
-      },
-      [&](int s, int, int, int, const Cell3& v) {
-        dn_s[s] = v.lb ? (beta == 0.0f ? v.a - zm : (v.a - zm) + beta * v.b) : 0.0f;
-        lab_s[s] = v.lb;
-      });
-  __syncthreads();
-  const float* __restrict__ dgl = L.diag;
-  float* __restrict__ Qo = I.q;
-  const int sy = B.ex, sz = B.ex * B.ey;
-  double dq = 0.0;
-  for_box(B, x0, y0, z0, kTX, kTY, 8, 2, [&](int x, int y, int zz, int s) {
-    if (!inside(x, y, zz, nx, ny, nz)) return;
-    const int i = x + nx * (y + ny * zz);
-    float q = 0.0f;
-    const float dv = dn_s[s];
-    if (lab_s[s]) {
-      q = dgl[i] * dv - d4sum6(dn_s[s - 1], dn_s[s + 1], dn_s[s - sy], dn_s[s + sy], dn_s[s - sz], dn_s[s + sz]);
-      dq += double(dv) * q;
-    }
-    dnew[i] = dv;
-    Qo[i] = q;
-  });
-  const int nt0 = I.ntiles0;
-  const double a0 = block_sum(dq, sh);
-  if (threadIdx.x == 0) I.partial[tl.tile] = a0;
-  if (arrive_last(&c->arrive[kStSpmv], nt0, &flag)) {
-    const double delta = gather_slot(I.partial, 0, nt0, 0, sh);
-    if (threadIdx.x == 0) {
-      finish_delta(c, delta);
-      c->dsel = sel ^ 1;
-    }
-  }
-}
-
 // ================================================ marching direction + SpMV
-// k_dirspmv as a 2.5-D march over tiles of kQX x kQY x kQZ level-0 cells: step
+// d' = (z - zmean) + beta d on liquid cells, q = A d' and delta = d' . q
+// (applyLiquidOperator, atlas :1171-1192), alpha = gamma / delta, as a 2.5-D
+// march over tiles of kQX x kQY x kQZ level-0 cells.  The new direction goes to
+// the other buffer (Ctrl::dsel flips in k_dirspmv_finish), so neighbours read
+// the old direction race-free.  Step
 // p stages d' = (z - zmean) + beta d of fine plane p on T +- 1 into a ring of
 // 4 planes (pointwise, from loads prefetched one step earlier), and applies
 // the operator to plane p - 2, whose neighbour planes earlier steps staged:

@@ -350,9 +350,9 @@ void vcycle_fused(fluid_pp_batch* B, int with_dot) {
     const List& Lu = B->up[l];
     if (!Lu.n) continue;
     if (l == 0)
-      FPP_LAUNCH(B, kPrUp0, k_up<float, float, T, T><<<Lu.n, kFThreads, B->smem_up, s>>>(B->d_insts, tl(B, Lu), 0, 0));
+      FPP_LAUNCH(B, kPrUp0, k_up<float, float, T, T><<<Lu.n, kFThreads, B->smem_up, s>>>(B->d_insts, tl(B, Lu), 0));
     else
-      FPP_LAUNCH(B, kPrUpC, k_up<T, T, T, T><<<Lu.n, kFThreads, B->smem_up, s>>>(B->d_insts, tl(B, Lu), l, 0));
+      FPP_LAUNCH(B, kPrUpC, k_up<T, T, T, T><<<Lu.n, kFThreads, B->smem_up, s>>>(B->d_insts, tl(B, Lu), l));
   }
   // gamma = r . (z - zmean) over the fixed level-0 tiles of every instance: the
   // marching level-0 up step writes the partials of its instances with

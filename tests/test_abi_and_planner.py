@@ -90,7 +90,7 @@ def test_planner_agrees_with_reference_rules_where_reference_accepts(dims):
         assert product["levelDimensions"] == ref
 
 
-def test_planner_survey_examples():
+def test_planner_known_level_maps():
     assert plan_uniform_cm11a_hierarchy((32, 32, 32))["levelDimensions"] == [
         (32, 32, 32), (16, 16, 16), (8, 8, 8), (4, 4, 4), (2, 2, 2)]
     p = plan_uniform_cm11a_hierarchy((128, 96, 128))

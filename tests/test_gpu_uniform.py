@@ -7,7 +7,7 @@ from oracle.oracle import Oracle
 
 pytestmark = pytest.mark.gpu
 
-REL_L2_PRESSURE = 1e-5      # pressure vs the float64 oracle
+REL_L2_PRESSURE = 1e-5      # pressure vs the float64 oracle (required tolerance)
 DIV_RATIO = 1e-6            # max post-projection divergence / max pre-projection divergence
 REL_RES = 1e-6
 
