@@ -170,9 +170,13 @@ def test_iteration_cap_reports_nonconvergence():
     assert rec["iterations"] == 2
 
 
-def test_batch_is_identical_to_single():
+@pytest.mark.parametrize("tuning", [None, {"parts": 3}])
+def test_batch_is_identical_to_single(tuning):
+    """Uneven lattices (a semi-coarsened one and a tiny one among them) give each
+    single solve's bits in a batch, also split into concurrent parts."""
     states = [configs.random_small(n[0], n[1], n[2], seed=20 + k)
-              for k, n in enumerate([(24, 30, 28), (37, 25, 41), (16, 16, 16), (48, 20, 33)])]
+              for k, n in enumerate([(24, 30, 28), (37, 25, 41), (16, 16, 16), (48, 20, 33), (2, 64, 48),
+                                     (4, 4, 4)])]
     singles = []
     for s in states:
         pp = PressureProjector((s.nx, s.ny, s.nz), s.h)
@@ -183,7 +187,7 @@ def test_batch_is_identical_to_single():
         pp = PressureProjector((s.nx, s.ny, s.nz), s.h)
         pp.upload_state(s.vof, s.u, s.v, s.w)
         pps.append(pp)
-    batch = BatchProjector(pps)
+    batch = BatchProjector(pps, tuning=tuning)
     recs = batch.project([s.dt for s in states])
     for (r1, x1), r2, pp in zip(singles, recs, pps):
         assert r2["status_name"] == "OK"
