@@ -468,7 +468,7 @@ def main():
     # the same ticks with three batches in flight on three streams: one batch's
     # uploads and read-back overlap the others' solves (PipelinedBatchProjector)
     note("e2e pipelined")
-    depth = 3   # ticks in flight
+    depth = 3   # ticks in flight (4 measured slower: 4436 vs 5433 solves/s with 4-part batches)
     side = [torch.cuda.Stream() for _ in range(depth)]
     sets = []
     for st in side:
