@@ -476,7 +476,6 @@ def main():
         for p in ps_:
             p.set_stream(st.cuda_stream)
         sets.append(ps_)
-    pipe = PipelinedBatchProjector(sets, tuning=tune.tuning)
     outs = [host_out] + [[tuple(torch.empty_like(t).pin_memory() for t in tup) for tup in host_out]
                          for _ in range(depth - 1)]
     ins_np = [tuple(t.numpy() for t in tup) for tup in host_in]
@@ -496,13 +495,30 @@ def main():
         for t in tickets[-depth:]:
             pipe_bad += sum(r["status"] != 0 for r in pipe.result(t))
 
+    # parts per batch for the pipeline, measured here before timing: ticks in
+    # flight already overlap one another's solves, so fewer parts than a lone
+    # batch wants can be faster
+    pipe_rates = {}
+    for np_ in sorted({1, 2, int(tune.tuning["parts"])}):
+        pipe = PipelinedBatchProjector(sets, tuning=dict(tune.tuning, parts=np_))
+        pipe_ticks(depth)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pipe_ticks(3 * depth)
+        torch.cuda.synchronize()
+        pipe_rates[np_] = round(3 * depth * BATCH / (time.perf_counter() - t0), 1)
+        pipe.destroy()
+    pipe_parts = max(pipe_rates, key=lambda k: (pipe_rates[k], -k))
+    pipe = PipelinedBatchProjector(sets, tuning=dict(tune.tuning, parts=pipe_parts))
+    pipe_bad = 0
     pipe_ticks(args.warmup)
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev0.record(side[0])
-    side[1].wait_event(ev0)
+    for st in side[1:]:
+        st.wait_event(ev0)
     pipe_ticks(args.steps)
     ends = [torch.cuda.Event(enable_timing=True) for _ in side]
     for e, st in zip(ends, side):
@@ -562,7 +578,8 @@ def main():
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "PipelinedBatchProjector: each tick uploads the 64 inputs from pinned host memory, projects "
                         "and reads back p,u,v,w; three ticks in flight on three streams; timed over all ticks",
-                "failed_solves": int(pipe_bad), "serial_solves_per_s": e2e_serial},
+                "failed_solves": int(pipe_bad), "serial_solves_per_s": e2e_serial, "ticks_in_flight": depth,
+                "parts_per_batch": pipe_parts, "parts_measured_solves_per_s": pipe_rates},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
