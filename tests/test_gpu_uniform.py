@@ -174,14 +174,16 @@ def test_iteration_cap_reports_nonconvergence():
 def test_batch_is_identical_to_single(tuning):
     """Uneven lattices (a semi-coarsened one and a tiny one among them) give each
     single solve's bits in a batch, also split into concurrent parts."""
-    states = [configs.random_small(n[0], n[1], n[2], seed=20 + k)
-              for k, n in enumerate([(24, 30, 28), (37, 25, 41), (16, 16, 16), (48, 20, 33), (2, 64, 48),
-                                     (4, 4, 4)])]
+    import dataclasses
+    # a different dt per instance, so each part must receive its own instances' dts
+    states = [dataclasses.replace(s, dt=s.dt * (1.0 + 0.25 * k)) for k, s in enumerate(
+        configs.random_small(n[0], n[1], n[2], seed=20 + k)
+        for k, n in enumerate([(24, 30, 28), (37, 25, 41), (16, 16, 16), (48, 20, 33), (2, 64, 48), (4, 4, 4)]))]
     singles = []
     for s in states:
         pp = PressureProjector((s.nx, s.ny, s.nz), s.h)
         pp.upload_state(s.vof, s.u, s.v, s.w)
-        singles.append((pp.project(s.dt), pp.pressure_cells()))
+        singles.append((pp.project(s.dt), pp.pressure_cells(), pp.download()[0]))
     pps = []
     for s in states:
         pp = PressureProjector((s.nx, s.ny, s.nz), s.h)
@@ -189,10 +191,11 @@ def test_batch_is_identical_to_single(tuning):
         pps.append(pp)
     batch = BatchProjector(pps, tuning=tuning)
     recs = batch.project([s.dt for s in states])
-    for (r1, x1), r2, pp in zip(singles, recs, pps):
+    for (r1, x1, p1), r2, pp in zip(singles, recs, pps):
         assert r2["status_name"] == "OK"
         assert r1["iterations"] == r2["iterations"]
         np.testing.assert_array_equal(x1, pp.pressure_cells())
+        np.testing.assert_array_equal(p1, pp.download()[0])   # pressure in Pa carries each instance's dt
 
 
 def test_marching_batch_is_identical_to_box_singles():
