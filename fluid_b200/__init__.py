@@ -6,8 +6,8 @@ mirror of the reference's projection interface plus the seeded workload
 generators.  Importing the package does not load the library; the first
 projector does, and fails loudly if it was not built.
 """
-from .projector import (BatchProjector, FluidError, PipelinedBatchProjector, PressureProjector,
+from .projector import (BatchProjector, FluidError, PipelinedBatchProjector, PressureProjector, batch_tuning,
                         plan_uniform_cm11a_hierarchy, solve_opts)
 
 __all__ = ["PressureProjector", "BatchProjector", "PipelinedBatchProjector", "FluidError", "plan_uniform_cm11a_hierarchy",
-           "solve_opts"]
+           "solve_opts", "batch_tuning"]
