@@ -314,7 +314,13 @@ def main():
     # (layouts never change results; fluid_b200.autotune)
     note("autotune")
     pps_t = make(args.precision)
-    tune = autotune_batch(pps_t, dts, lambda: upload_dev(pps_t), rel_tol=1e-6, repeats=2)
+    try:
+        tune = autotune_batch(pps_t, dts, lambda: upload_dev(pps_t), rel_tol=1e-6, repeats=2)
+    except Exception as exc:   # the library's default layout if tuning itself fails
+        note(f"autotune failed ({exc}); default layout")
+        from fluid_b200.autotune import TuneResult
+        from fluid_b200.projector import batch_tuning
+        tune = TuneResult(batch_tuning().as_dict(), (args.sweeps, args.sweeps), None, None, [])
     for p in pps_t:
         p.destroy()
     tuned = dict(opts, pre_sweeps=tune.sweeps[0], post_sweeps=tune.sweeps[1])
