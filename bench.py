@@ -44,7 +44,7 @@ METRIC = "MGPCG solves/s @rel-res 1e-6: mixed/batched vs plain FP32 on 1 B200; p
 WORKLOAD = ("64 independent uniform MAC grids in one batched projection per step: edges log-uniform 24-128 "
             "per axis, liquid = 1-6 seeded boxes/spheres filling 20-70%, Gaussian velocities sigma 0.2 m/s, "
             "rel-res 1e-6 per instance")
-WORKLOAD2 = "dam break + 16 falling spheres, 128x96x128 uniform MAC grid, dt=1/60, rel-res 1e-6"
+WORKLOAD2 = "dam break + 16 falling spheres, 128x96x128 uniform MAC grid, 50 consecutive steps, dt=1/60, rel-res 1e-6"
 L2_FLUSH_BYTES = 256 << 20
 BATCH = 64
 
@@ -169,7 +169,7 @@ def reference_arm(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "instances": BATCH, "cells": int(sum(s.cells for s in insts)),
                    "solver": "Jacobi-PCG float64 (atlas oracle), one instance after another"},
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port", "cpu_model": cpu_model(),
                          "sample": f"{per_step} of the 64 instances per step (rotating), full solves to rel-res "
                                    f"1e-6, mean {statistics.mean(iters):.0f} PCG iterations, OpenMP"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -180,22 +180,63 @@ def reference_arm(args):
     return 0
 
 
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline_sample(insts):
-    """The oracle's float64 Jacobi-PCG on 4 of the 64 headline instances, all host threads."""
+    """The oracle's float64 Jacobi-PCG (the reference's CPU algorithm) on 4 of the 64
+    headline instances: on all host threads (OpenMP, the reported value) and on one
+    thread (the reference's own CPU path is single-threaded JavaScript)."""
     from oracle.oracle import Oracle
     threads = os.cpu_count() or 1
-    t0 = time.perf_counter()
-    its = []
-    for s in insts[:4]:
-        o = Oracle(s.nx, s.ny, s.nz, s.h, s.rho)
-        o.set_threads(threads)
-        o.set_state(s.vof, s.u, s.v, s.w, s.dt)
-        _, info = o.solve_jacobi(1e-6, 0.0)
-        its.append(int(info["iterations"]))
-    dt = time.perf_counter() - t0
-    return {"value": 4 / dt, "unit": "solves/s", "cores": threads, "kind": "port",
+
+    def run(nthreads):
+        t0 = time.perf_counter()
+        its = []
+        for s in insts[:4]:
+            o = Oracle(s.nx, s.ny, s.nz, s.h, s.rho)
+            o.set_threads(nthreads)
+            o.set_state(s.vof, s.u, s.v, s.w, s.dt)
+            _, info = o.solve_jacobi(1e-6, 0.0)
+            its.append(int(info["iterations"]))
+        return time.perf_counter() - t0, its
+    dt, its = run(threads)
+    dt1, _ = run(1)
+    return {"value": 4 / dt, "unit": "solves/s", "cores": threads, "kind": "port", "cpu_model": cpu_model(),
             "sample": f"instances 0-3 of the 64 ({sum(s.cells for s in insts[:4])} cells), float64 Jacobi-PCG "
-                      f"to rel-res 1e-6 ({its} iterations), OpenMP on the host"}
+                      f"to rel-res 1e-6 ({its} iterations), OpenMP on the host",
+            "single_thread": {"value": 4 / dt1, "unit": "solves/s", "cores": 1,
+                              "sample": "the same 4 solves on one thread"}}
+
+
+SEQ_STEPS = 50
+
+
+def fp64_errors(states, steps, results: dict) -> dict:
+    """Relative L2 error of each run's pressure (finest-cell units) against the
+    float64 oracle's MGPCG solved to rel-res 1e-12 on the same input, per step."""
+    from oracle.oracle import Oracle
+    errs = {k: [] for k in results}
+    for j in steps:
+        st = states[j]
+        o = Oracle(st.nx, st.ny, st.nz, st.h, st.rho, st.open_top)
+        o.set_threads(os.cpu_count() or 1)
+        o.set_state(st.vof, st.u, st.v, st.w, st.dt)
+        p_ref, _ = o.solve_mgpcg(1e-12, 0.0, 300, 2, 2)
+        nrm = float(np.linalg.norm(p_ref))
+        for k, ps in results.items():
+            errs[k].append(float(np.linalg.norm(ps[j] - p_ref)) / nrm)
+    out = {"steps": list(steps), "oracle": "float64 MGPCG of the CPU oracle to rel-res 1e-12, same inputs"}
+    for k, e in errs.items():
+        out[k] = {"rel_l2_max": max(e), "rel_l2_median": statistics.median(e), "rel_l2": e}
+    return out
 
 
 def note(msg: str):
@@ -314,10 +355,15 @@ def main():
     # (layouts never change results; fluid_b200.autotune)
     note("autotune")
     pps_t = make(args.precision)
+    tune_failed = None
     try:
         tune = autotune_batch(pps_t, dts, lambda: upload_dev(pps_t), rel_tol=1e-6, repeats=2)
-    except Exception as exc:   # the library's default layout if tuning itself fails
-        note(f"autotune failed ({exc}); default layout")
+    except (RuntimeError, ValueError, MemoryError) as exc:
+        # the library's default layout if tuning itself fails; a CUDA error that
+        # left the context unusable surfaces here, not later in the timed region
+        torch.cuda.synchronize()
+        tune_failed = f"{type(exc).__name__}: {exc}"
+        note(f"autotune failed ({tune_failed}); default layout")
         from fluid_b200.autotune import TuneResult
         from fluid_b200.projector import batch_tuning
         tune = TuneResult(batch_tuning().as_dict(), (args.sweeps, args.sweeps), None, None, [])
@@ -347,20 +393,34 @@ def main():
     batched32 = BATCH * len(times_b32) / (sum(times_b32) / 1000.0)
 
     # ------------------------------------------------ secondary: 128x96x128 single
-    steps2 = min(args.steps, 50)
-    note("128x96x128 single solves")
-    states = [configs.dam_spheres(step=k) for k in range(min(args.warmup + steps2, 50))]
-    nst = len(states)
-    s0 = states[0]
-    dev2 = [tuple(torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (s.vof, s.u, s.v, s.w)) for s in states]
+    # 50 consecutive steps, whatever --steps is: each step's input is the
+    # previous step's plain-FP32 projected velocity plus this step's gravity
+    # (configs.dam_spheres_sequence); mixed and plain time the same 50 inputs,
+    # and both are scored against the float64 oracle on every fifth step.
+    steps2 = SEQ_STEPS
+    note("128x96x128 consecutive inputs")
+    s0 = configs.dam_spheres()
+    seq_pp = PressureProjector((s0.nx, s0.ny, s0.nz), s0.h, s0.rho, precision="fp32", device=local)
 
-    def run_single(precision, profile=False):
+    def carry(st):
+        seq_pp.upload_state(st.vof, st.u, st.v, st.w)
+        seq_pp.project(st.dt, **opts)
+        _, u_, v_, w_ = seq_pp.download()
+        return u_, v_, w_
+    states = configs.dam_spheres_sequence(steps2, carry)
+    seq_pp.destroy()
+    nst = len(states)
+    dev2 = [tuple(torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (s.vof, s.u, s.v, s.w)) for s in states]
+    fp64_steps = list(range(0, nst, 5))
+
+    def run_single(precision, profile=False, keep=()):
         pp = PressureProjector((s0.nx, s0.ny, s0.nz), s0.h, s0.rho, precision=precision, device=local)
         pp.set_stream(stream.cuda_stream)
         pp.set_profiling(profile)
-        tt, rr = [], []
+        tt, rr, kept = [], [], {}
         for k in range(args.warmup + steps2):
-            st, d2 = states[k % nst], dev2[k % nst]
+            j = (k - args.warmup) % nst   # warm-up steps replay the last inputs
+            st, d2 = states[j], dev2[j]
 
             def step():
                 pp.upload_state_device(*(t.data_ptr() for t in d2))
@@ -369,16 +429,20 @@ def main():
             if k >= args.warmup:
                 tt.append(ms)
                 rr.append(rec)
+                if j in keep:
+                    kept[j] = pp.pressure_cells().astype(np.float64)
             if profile and k == args.warmup - 1:
                 pp.profile(reset=True)
         prof = pp.profile(reset=True) if profile else None
         pp.destroy()
-        return tt, rr, prof
+        return tt, rr, prof, kept
 
-    t2_mixed, r2_mixed, _ = run_single(args.precision)
-    t2_plain, _, _ = run_single("fp32")
+    t2_mixed, r2_mixed, _, p2_mixed = run_single(args.precision, keep=fp64_steps)
+    t2_plain, r2_plain, _, p2_plain = run_single("fp32", keep=fp64_steps)
     # per-stage kernel events of the 128x96x128 solves (direct launches), reported per solve
-    _, _, prof = run_single(args.precision, profile=True)
+    _, _, prof, _ = run_single(args.precision, profile=True)
+    note("128x96x128 float64 oracle on every fifth step")
+    fp64 = fp64_errors(states, fp64_steps, {"mixed": p2_mixed, "plain_fp32": p2_plain})
 
     # roofline of the headline: per-stage kernel events of the batched solve
     # (direct launches of the same 64 solves).  A launch of a level-0 stage
@@ -561,17 +625,25 @@ def main():
         "batched_fp32_solves_per_s": batched32,
         "mixed_batched_vs_plain_single": value / (world * plain),
         "failed_solves": len(bad),
-        "autotune": {"candidates": len(tune.table), "chosen_ms": tune.ms, "default_layout_ms": tune.default_ms,
+        "autotune": {"failed": tune_failed, "candidates": len(tune.table), "chosen_ms": tune.ms,
+                     "default_layout_ms": tune.default_ms,
                      "table": [[r["tuning"]["fill_tiles"], r["tuning"]["march_levels"], r["tuning"]["box_shape"],
                                 r["tuning"]["parts"], list(r["sweeps"]), round(r["ms"], 3)] for r in tune.table],
                      "table_columns": ["fill_tiles", "march_levels", "box_shape", "parts", "sweeps", "median_ms"],
                      "note": "median solve of each candidate layout / sweep schedule on this batch before timing"},
         "dam_spheres_128x96x128": {
             "workload": WORKLOAD2, "steps": steps2,
+            "sequence": "consecutive: each input is the previous step's projected velocity (plain FP32) plus "
+                        "this step's gravity, spheres moved a quarter cell per step; mixed and plain time the "
+                        "same inputs",
             "mixed_solves_per_s": len(t2_mixed) / (sum(t2_mixed) / 1000.0),
             "plain_fp32_solves_per_s": len(t2_plain) / (sum(t2_plain) / 1000.0),
             "mixed_p50_ms": statistics.median(t2_mixed), "mixed_p99_ms": float(np.percentile(t2_mixed, 99)),
+            "plain_p50_ms": statistics.median(t2_plain), "plain_p99_ms": float(np.percentile(t2_plain, 99)),
             "iterations_mean": statistics.mean(r["iterations"] for r in r2_mixed),
+            "plain_iterations_mean": statistics.mean(r["iterations"] for r in r2_plain),
+            "failed_solves": sum(r["status_name"] != "OK" for r in r2_mixed + r2_plain),
+            "fp64_error": fp64,
             "stage_ms_per_solve": {k: round(v["ms"] / steps2, 4) for k, v in sorted(prof.items())},
         },
         "tall_cell_256x256x1024": tall_line,

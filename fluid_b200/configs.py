@@ -142,6 +142,33 @@ def dam_spheres(nx=128, ny=96, nz=128, seed: int = 2, step: int = 0, spheres: in
                      meta={"workload": f"dam+{len(placed)} spheres {nx}x{ny}x{nz}", "seed": seed, "step": step})
 
 
+def dam_spheres_sequence(steps: int, project, nx=128, ny=96, nz=128, seed: int = 2) -> list[GridState]:
+    """``steps`` consecutive inputs of the dam-break-with-spheres scene.
+
+    Step 0 is ``dam_spheres(step=0)``.  The input of step k >= 1 is the previous
+    step's projected velocity with the body-force update of this step: the
+    spheres' VOF of ``dam_spheres(step=k)``, faces that have no liquid side under
+    it set to zero, and ``v += dt * g`` on its fluid y-faces (the order of the
+    reference step, ``webgpu-uniform-reference.ts:1180-1282``, without
+    advection).  ``project(state) -> (u, v, w)`` is the projection that carries
+    one step to the next; the caller passes it, so the sequence is defined by
+    that solver's outputs.
+    """
+    out = [dam_spheres(nx, ny, nz, seed=seed, step=0)]
+    for k in range(1, steps):
+        prev = out[-1]
+        u, v, w = project(prev)
+        nxt = dam_spheres(nx, ny, nz, seed=seed, step=k)
+        fu, fv, fw = fluid_face_masks(nxt.vof)
+        v = np.where(fv, v + nxt.dt * GRAVITY, 0.0)
+        out.append(GridState(nx, ny, nz, nxt.h, nxt.dt, nxt.vof,
+                             np.ascontiguousarray(np.where(fu, u, 0.0), np.float32),
+                             np.ascontiguousarray(v, np.float32),
+                             np.ascontiguousarray(np.where(fw, w, 0.0), np.float32),
+                             meta=dict(nxt.meta, sequence=True)))
+    return out
+
+
 def log_uniform_edge(rng, lo=24, hi=128) -> int:
     return int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
 

@@ -9,14 +9,16 @@
 //
 // The scratch array below is file-scope device memory: every GPU that loads
 // the library holds it (about 128 KB) until the process exits.  Its name is a
-// host-side stand-in, not a device address, so the host looks the address up
-// with cudaGetSymbolAddress once per device (with that device current) and
-// passes it to the kernel.  Every call on a device shares the one array and it
-// keeps the last call's contents, so calls whose GPU work overlaps (different
-// streams, or the same stream from several threads without ordering) race on it.
+// host-side stand-in, not a device address, so every call looks the address up
+// with cudaGetSymbolAddress (with the caller's device current; the lookup
+// allocates nothing) and passes it to the kernel.  Looking it up on every call
+// keeps the address right after a device reset recreates the context.  Every
+// call on a device shares the one array and it keeps the last call's contents,
+// so calls whose GPU work overlaps (different streams, or the same stream from
+// several threads without ordering) race on it.
 #include <cuda_runtime.h>
 
-#include <mutex>
+#include <cstdint>
 #include <string>
 
 #include "../../include/fluid_pp.h"
@@ -29,9 +31,11 @@ namespace {
 constexpr int kNoAllocMaxTiles = 16384;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxTiles + 32];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-double* g_scratch_ptr[kMaxDevices] = {};
+// [a, a + na) and [b, b + nb) share a byte.
+bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
+  const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return x < y + nb && y < x + na;
+}
 
 }  // namespace
 
@@ -89,27 +93,28 @@ extern "C" int fluid_pp_apply_operator_noalloc(int nx, int ny, int nz, const uns
                     " work tiles of 32x8x4 cells; the fixed scratch holds " + std::to_string(kNoAllocMaxTiles));
     return FLUID_PP_INVALID_ARG;
   }
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
-    fpp::set_global_error("fluid_pp_apply_operator_noalloc: no usable current device");
+  // The kernel reads label, diag and p through restrict pointers while it
+  // writes out and *p_dot_ap: an output that shares memory with an input would
+  // give wrong neighbour values, so aliasing is rejected.
+  const size_t cells = size_t(nx) * size_t(ny) * size_t(nz);
+  const size_t vbytes = cells * sizeof(float);
+  if (overlaps(out, vbytes, p, vbytes) || overlaps(out, vbytes, diag, vbytes) || overlaps(out, vbytes, label, cells) ||
+      overlaps(p_dot_ap, sizeof(double), p, vbytes) || overlaps(p_dot_ap, sizeof(double), diag, vbytes) ||
+      overlaps(p_dot_ap, sizeof(double), label, cells) || overlaps(p_dot_ap, sizeof(double), out, vbytes)) {
+    fpp::set_global_error("fluid_pp_apply_operator_noalloc: out and p_dot_ap must not overlap label, diag, p or "
+                          "each other");
+    return FLUID_PP_INVALID_ARG;
+  }
+  // The scratch address of the current device, looked up on every call (the
+  // array's host-side name is not a device address).
+  void* ptr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+  if (e != cudaSuccess) {
+    fpp::set_global_error(std::string("fluid_pp_apply_operator_noalloc: cudaGetSymbolAddress: ") +
+                          cudaGetErrorString(e));
     return FLUID_PP_CUDA;
   }
-  double* scratch = nullptr;
-  {
-    // First call on this device: look up the scratch address with the device current.
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-      void* ptr = nullptr;
-      e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-      if (e != cudaSuccess) {
-        fpp::set_global_error(std::string("fluid_pp_apply_operator_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        return FLUID_PP_CUDA;
-      }
-      g_scratch_ptr[dev] = static_cast<double*>(ptr);
-    }
-    scratch = g_scratch_ptr[dev];
-  }
+  double* scratch = static_cast<double*>(ptr);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // The arrival counter must start at zero; the partials are all overwritten.
   e = cudaMemsetAsync(scratch + kNoAllocMaxTiles, 0, sizeof(double), s);

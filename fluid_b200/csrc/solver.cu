@@ -581,6 +581,12 @@ static int batch_build(fluid_pp* const* handles, int count, const fluid_pp_batch
       err = "batched handles must share device and precision";
       return FLUID_PP_INVALID_ARG;
     }
+    // A batch orders its work on one stream; a handle's own uploads, downloads
+    // and release use the handle's stream, so every handle must be on that one.
+    if (h->stream != B->stream) {
+      err = "batched handles must share one stream (fluid_pp_set_stream)";
+      return FLUID_PP_INVALID_ARG;
+    }
     B->h.push_back(h);
     B->maxL = std::max(B->maxL, h->plan.levels);
   }
@@ -1534,9 +1540,24 @@ int fluid_pp_profile_read(fluid_pp* pp, double* ms, long long* launches, int res
   return pp ? fluid_pp_batch_profile_read(pp->self, ms, launches, reset) : FLUID_PP_INVALID_ARG;
 }
 
+// Every handle of a batch must still be on the batch's stream: fluid_pp_set_stream
+// on a member after fluid_pp_batch_create would let that handle's uploads,
+// downloads and release race the batched solve.
+static int batch_streams_ok(fluid_pp_batch* B) {
+  for (fluid_pp* h : B->h)
+    if (h->stream != B->stream) {
+      B->err = "a batched handle's stream no longer matches the batch's stream (fluid_pp_set_stream after "
+               "fluid_pp_batch_create)";
+      g_err = B->err;
+      return FLUID_PP_INVALID_ARG;
+    }
+  return FLUID_PP_OK;
+}
+
 int fluid_pp_batch_project(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts* opts,
                            fluid_pp_receipt* receipts) {
   if (!B) return FLUID_PP_INVALID_ARG;
+  if (batch_streams_ok(B) != FLUID_PP_OK) return FLUID_PP_INVALID_ARG;
   if (dts)
     for (size_t k = 0; k < B->h.size(); ++k)
       if (!(dts[k] > 0) || !std::isfinite(dts[k])) {
@@ -1550,6 +1571,7 @@ int fluid_pp_batch_project(fluid_pp_batch* B, const float* dts, const fluid_pp_s
 
 int fluid_pp_batch_project_async(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts* opts) {
   if (!B) return FLUID_PP_INVALID_ARG;
+  if (batch_streams_ok(B) != FLUID_PP_OK) return FLUID_PP_INVALID_ARG;
   if (dts)
     for (size_t k = 0; k < B->h.size(); ++k)
       if (!(dts[k] > 0) || !std::isfinite(dts[k])) {
@@ -1565,6 +1587,7 @@ int fluid_pp_batch_project_async(fluid_pp_batch* B, const float* dts, const flui
 int fluid_pp_batch_upload_state(fluid_pp_batch* B, const float* const* vof, const float* const* u,
                                 const float* const* v, const float* const* w) {
   if (!B || !vof || !u || !v || !w) return FLUID_PP_INVALID_ARG;
+  if (batch_streams_ok(B) != FLUID_PP_OK) return FLUID_PP_INVALID_ARG;
   for (size_t k = 0; k < B->h.size(); ++k) {
     const int rc = upload(B->h[k], vof[k], u[k], v[k], w[k], cudaMemcpyHostToDevice);
     if (rc != FLUID_PP_OK) {
@@ -1579,6 +1602,7 @@ int fluid_pp_batch_upload_state(fluid_pp_batch* B, const float* const* vof, cons
 int fluid_pp_batch_download_async(fluid_pp_batch* B, float* const* p, float* const* u, float* const* v,
                                   float* const* w) {
   if (!B) return FLUID_PP_INVALID_ARG;
+  if (batch_streams_ok(B) != FLUID_PP_OK) return FLUID_PP_INVALID_ARG;
   for (size_t k = 0; k < B->h.size(); ++k) {
     const int rc = fluid_pp_download_async(B->h[k], p ? p[k] : nullptr, u ? u[k] : nullptr, v ? v[k] : nullptr,
                                            w ? w[k] : nullptr);

@@ -169,7 +169,11 @@ int fluid_pp_get_pressure_cells(fluid_pp* pp, float* x);             /* solution
 
 /* Batched projection of several handles in one set of launches per stage.
  * Replaces nothing in the reference (which runs one solver per device); the
- * per-solve semantics are those of fluid_pp_project. */
+ * per-solve semantics are those of fluid_pp_project.  Every handle must be on
+ * one stream (fluid_pp_set_stream before fluid_pp_batch_create): the batch
+ * orders its work on that stream, and a handle's own uploads, downloads and
+ * release use the handle's stream.  Handles on different streams, or a member
+ * moved to another stream later, give FLUID_PP_INVALID_ARG. */
 int fluid_pp_batch_create(fluid_pp* const* handles, int count, fluid_pp_batch** out);
 void fluid_pp_batch_destroy(fluid_pp_batch* batch);
 int fluid_pp_batch_project(fluid_pp_batch* batch, const float* dts, const fluid_pp_solve_opts* opts,
@@ -251,9 +255,11 @@ int fluid_pp_batch_profile_read(fluid_pp_batch* batch, double* ms, long long* la
  * per GPU, held until the process exits), enough for lattices of up to 16384
  * work tiles of 32x8x4 cells (e.g. 256^3); larger lattices return
  * FLUID_PP_INVALID_ARG with the reason in fluid_pp_last_error(NULL).
- * The first call on each device looks the scratch address up with that device
- * current; make that first call before any stream capture.  Calls on one device
- * share the scratch, so calls whose GPU work overlaps race. */
+ * out and p_dot_ap must not overlap label, diag, p or each other
+ * (FLUID_PP_INVALID_ARG otherwise).  Every call looks the scratch address up
+ * for the current device (no allocation); the first call on a device may load
+ * the library's device code, so make it before any stream capture.  Calls on
+ * one device share the scratch, so calls whose GPU work overlaps race. */
 int fluid_pp_apply_operator_noalloc(int nx, int ny, int nz, const unsigned char* label, const float* diag,
                                     const float* p, float* out, double* p_dot_ap, void* stream);
 

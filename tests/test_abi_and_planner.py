@@ -104,3 +104,28 @@ def test_create_rejects_bad_arguments_without_gpu():
         PressureProjector((1, 8, 8), 0.1)
     with pytest.raises(ValueError):
         PressureProjector((8, 8, 8), -1.0)
+
+
+def test_noalloc_rejects_lattices_beyond_its_scratch():
+    """The size check comes before any CUDA call (no GPU needed)."""
+    L = _abi.load()
+    one = ctypes.c_void_p(16)   # never dereferenced: the size check comes first
+    rc = L.fluid_pp_apply_operator_noalloc(4096, 4096, 64, one, one, one, one, one, None)
+    assert rc == _abi.INVALID_ARG
+    assert b"fixed scratch" in L.fluid_pp_last_error(None)
+
+
+def test_noalloc_rejects_outputs_that_alias_inputs():
+    """The allocation-free operator apply rejects out = p (an in-place call), a dot
+    slot inside an input and partly overlapping buffers before any CUDA call; the
+    pointers are never dereferenced, so this runs without a GPU."""
+    L = _abi.load()
+    n = 16 * 16 * 16
+    base = 1 << 20
+    lab, dg, p, out, dot = (ctypes.c_void_p(base + k * 4 * n + 256) for k in range(5))
+    assert L.fluid_pp_apply_operator_noalloc(16, 16, 16, lab, dg, p, p, dot, None) == _abi.INVALID_ARG
+    assert b"must not overlap" in L.fluid_pp_last_error(None)
+    inside_p = ctypes.c_void_p(p.value + 64)
+    assert L.fluid_pp_apply_operator_noalloc(16, 16, 16, lab, dg, p, out, inside_p, None) == _abi.INVALID_ARG
+    half_over = ctypes.c_void_p(dg.value + 2 * n)
+    assert L.fluid_pp_apply_operator_noalloc(16, 16, 16, lab, dg, p, half_over, dot, None) == _abi.INVALID_ARG
