@@ -69,7 +69,7 @@ def _read_profile(fn, handle, reset: bool) -> dict:
     return {name: {"ms": float(ms[k]), "launches": int(cnt[k])} for k, name in enumerate(_abi.STAGES) if cnt[k]}
 
 
-def solve_opts(rel_tol=1e-6, abs_tol=0.0, max_iters=200, pre_sweeps=1, post_sweeps=1, true_residual_every=0,
+def solve_opts(rel_tol=1e-6, abs_tol=0.0, max_iters=200, pre_sweeps=1, post_sweeps=1, true_residual_every=4,
                warm_start=False, rel_tol_inf=0.0) -> SolveOpts:
     return SolveOpts(rel_tol, abs_tol, max_iters, pre_sweeps, post_sweeps, true_residual_every, int(warm_start),
                      rel_tol_inf)

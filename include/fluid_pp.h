@@ -74,7 +74,10 @@ typedef struct fluid_pp_solve_opts {
   int max_iters;           /* CG iteration cap */
   int pre_sweeps;          /* red-black Gauss-Seidel sweeps before restriction */
   int post_sweeps;         /* ... after prolongation (equal to pre_sweeps keeps M symmetric) */
-  int true_residual_every; /* recompute r = b - A p in float64 every k iterations (0: only at the end) */
+  int true_residual_every; /* replace r by b - A p, recomputed in float64, every k iterations (0: only when the
+                              recursive residual meets the tolerance).  Opts NULL: 4.  Without it the float32
+                              recursive residual drifts on smooth right-hand sides (e.g. a step whose input is
+                              the previous step's projected velocity plus gravity) and CG stalls above 1e-6. */
   int warm_start;          /* 1: start from the previous pressure of this handle */
   double rel_tol_inf;      /* >0: also require max|b - A p| <= rel_tol_inf * max|b| (divergence in max norm) */
 } fluid_pp_solve_opts;
@@ -130,7 +133,7 @@ int fluid_pp_upload_state_device(fluid_pp* pp, const float* vof, const float* u,
  * followed by the `project` dispatch (webgpu-uniform-reference.ts:1280-1282);
  * the receipt replaces the diagnostics words read by readStats
  * (webgpu-uniform-reference.ts:1358-1420).  dt in seconds; opts may be NULL
- * (rel 1e-6, 200 iterations, 1+1 sweeps).  The receipt is written after the
+ * (rel 1e-6, 200 iterations, 1+1 sweeps, true residual every 4).  The receipt is written after the
  * stream synchronises. */
 int fluid_pp_project(fluid_pp* pp, float dt, const fluid_pp_solve_opts* opts, fluid_pp_receipt* receipt);
 
