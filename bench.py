@@ -627,9 +627,9 @@ def main():
         "failed_solves": len(bad),
         "autotune": {"failed": tune_failed, "candidates": len(tune.table), "chosen_ms": tune.ms,
                      "default_layout_ms": tune.default_ms,
-                     "table": [[r["tuning"]["fill_tiles"], r["tuning"]["march_levels"], r["tuning"]["box_shape"],
+                     "table": [[r["tuning"]["fill_tiles"], r["tuning"]["chunk_planes"], r["tuning"]["box_shape"],
                                 r["tuning"]["parts"], list(r["sweeps"]), round(r["ms"], 3)] for r in tune.table],
-                     "table_columns": ["fill_tiles", "march_levels", "box_shape", "parts", "sweeps", "median_ms"],
+                     "table_columns": ["fill_tiles", "chunk_planes", "box_shape", "parts", "sweeps", "median_ms"],
                      "note": "median solve of each candidate layout / sweep schedule on this batch before timing"},
         "dam_spheres_128x96x128": {
             "workload": WORKLOAD2, "steps": steps2,
@@ -652,7 +652,9 @@ def main():
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": peak_kind, "traffic": traffic, "alg_bytes_per_launch": alg,
                      "launch_ms": per_launch_ms, "share_of_step": bprof[dom]["ms"] / tot_prof,
-                     "stage_gbs": stage_gbs},
+                     "stage_gbs": stage_gbs,
+                     "stage_ms_per_step": {k: round(v["ms"] / prof_steps, 4) for k, v in sorted(bprof.items())
+                                           if v["launches"] > 0}},
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "PipelinedBatchProjector: each tick uploads the 64 inputs from pinned host memory, projects "
                         "and reads back p,u,v,w; three ticks in flight on three streams; timed over all ticks",

@@ -64,7 +64,7 @@ class SolveOpts(ctypes.Structure):
 
 
 class BatchTuning(ctypes.Structure):
-    _fields_ = [("fill_tiles", ctypes.c_int), ("march_levels", ctypes.c_int), ("box_shape", ctypes.c_int),
+    _fields_ = [("fill_tiles", ctypes.c_int), ("chunk_planes", ctypes.c_int), ("box_shape", ctypes.c_int),
                 ("parts", ctypes.c_int)]
 
     def as_dict(self) -> dict:

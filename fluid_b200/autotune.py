@@ -1,10 +1,10 @@
 """Measured choice of a batch's work layout and smoothing schedule.
 
 A batch of uneven lattices can lay its V-cycle work out several ways: the box
-kernels' tile shape, the 2.5-D marching form on the finest levels, the tile
-count a launch must reach before a larger shape or the marching form is used,
-and how many concurrent parts (sub-batches on their own streams) the handles
-are split into (``fluid_pp_batch_tuning``).  The library's default rule picks
+kernels' tile shape, the z chunk of the column kernels' tiles, the tile count
+a launch must reach before a larger shape or a longer chunk is used, and how
+many concurrent parts (sub-batches on their own streams) the handles are split
+into (``fluid_pp_batch_tuning``).  The library's default rule picks
 from tile counts alone, with one part.  ``autotune_batch`` instead times the
 candidates on the caller's own batch: the layouts with one part, then the best
 of those split into 2-8 parts, then the other smoothing schedules (sweeps
@@ -28,8 +28,10 @@ from dataclasses import asdict, dataclass, field
 
 from .projector import BatchProjector, batch_tuning
 
-# fill_tiles: one (the default), two or four tiles per SM
-LAYOUTS = tuple(dict(fill_tiles=f, march_levels=m, box_shape=-1, parts=1) for f in (148, 296, 592) for m in (0, 1, 2))
+# fill_tiles: one (the default), two or four tiles per SM; chunk_planes: the
+# default rule (0) or forced z chunks of the column kernels
+LAYOUTS = tuple(dict(fill_tiles=f, chunk_planes=0, box_shape=-1, parts=1) for f in (148, 296, 592)) + tuple(
+    dict(fill_tiles=148, chunk_planes=c, box_shape=-1, parts=1) for c in (16, 32, 64))
 PARTS = (2, 3, 4, 6, 8)
 SWEEPS = ((1, 1), (2, 2))
 

@@ -19,6 +19,7 @@
 
 #include "alloc.h"
 #include "../../include/fluid_pp.h"
+#include "colmg.cuh"
 #include "fused.cuh"
 #include "plan.h"
 #include "types.h"
@@ -98,10 +99,10 @@ struct fluid_pp_batch {
   List rst[kMaxLevels];      // level-(l+1) tiles of instances for which l is not the coarsest
   List crs[kMaxLevels];      // level-l tiles (l >= 1) of every instance having level l
   List dn[kMaxLevels];       // fused down-step tiles (coarse tiles of level l+1) of grid level l
-  List dnm[kMaxLevels];      // marching down-step tiles of grid level l (levels < kMarchLevels coarsened by two on every axis)
-  List upm[kMaxLevels];      // marching up-step tiles (same condition)
-  List spm;                  // marching direction + SpMV tiles of level 0 (every instance)
-  List dot0;                 // level-0 tiles of instances whose level-0 up step does not march (gamma by k_dot_rz_part)
+  List cdn[kMaxLevels];      // column down-step tiles of grid level l (next level halves every axis)
+  List cup[kMaxLevels];      // column up-step tiles of grid level l (same condition)
+  List cq;                   // column direction + SpMV tiles of level 0 (every instance)
+  List dot0;                 // level-0 tiles of instances whose level-0 up step is a box kernel (gamma by k_dot_rz_part)
   List up[kMaxLevels];       // fused up-step tiles (fine tiles of level l) of grid level l
   List l0single;             // level-0 tiles of single-level instances
   List bake;
@@ -315,12 +316,13 @@ template <class T>
 void vcycle_fused(fluid_pp_batch* B, int with_dot) {
   cudaStream_t s = B->stream;
   for (int l = 0; l + 1 < B->maxL; ++l) {
-    const List& Lm = B->dnm[l];
+    const List& Lm = B->cdn[l];
     if (Lm.n) {
       if (l == 0)
-        FPP_LAUNCH(B, kPrDown0, k_down_m<float, float, T, T><<<Lm.n, kMThreads, 0, s>>>(B->d_insts, tl(B, Lm), 0));
+        FPP_LAUNCH(B, kPrDown0, k_cdown<float, float, float, T><<<Lm.n, kCDThreads, cdown_smem(), s>>>(
+                                    B->d_insts, tl(B, Lm), 0));
       else
-        FPP_LAUNCH(B, kPrDownC, k_down_m<T, T, T, T><<<Lm.n, kMThreads, 0, s>>>(B->d_insts, tl(B, Lm), l));
+        FPP_LAUNCH(B, kPrDownC, k_cdown<T, T, T, T><<<Lm.n, kCDThreads, cdown_smem(), s>>>(B->d_insts, tl(B, Lm), l));
     }
     const List& Ld = B->dn[l];
     if (!Ld.n) continue;
@@ -336,16 +338,16 @@ void vcycle_fused(fluid_pp_batch* B, int with_dot) {
     FPP_LAUNCH(B, kPrCoarse,
                k_coarse_apply<float, float><<<B->single.n, kThreads, 0, s>>>(B->d_insts, il(B, B->single)));
   for (int l = B->maxL - 2; l >= 0; --l) {
-    if (B->upm[l].n) {
+    const List& Lc = B->cup[l];
+    if (Lc.n) {
       if (l == 0 && with_dot)
-        FPP_LAUNCH(B, kPrUp0, k_up_m<float, float, T, T, true><<<B->upm[l].n, kMThreads, march_up_smem_bytes(), s>>>(
-                                  B->d_insts, tl(B, B->upm[l]), 0));
+        FPP_LAUNCH(B, kPrUp0, k_cup<float, float, float, T, true><<<Lc.n, kCUThreads, cup_smem(), s>>>(
+                                  B->d_insts, tl(B, Lc), 0));
       else if (l == 0)
-        FPP_LAUNCH(B, kPrUp0, k_up_m<float, float, T, T><<<B->upm[l].n, kMThreads, march_up_smem_bytes(), s>>>(
-                                  B->d_insts, tl(B, B->upm[l]), 0));
+        FPP_LAUNCH(B, kPrUp0, k_cup<float, float, float, T><<<Lc.n, kCUThreads, cup_smem(), s>>>(B->d_insts,
+                                                                                                 tl(B, Lc), 0));
       else
-        FPP_LAUNCH(B, kPrUpC, k_up_m<T, T, T, T><<<B->upm[l].n, kMThreads, march_up_smem_bytes(), s>>>(
-                                  B->d_insts, tl(B, B->upm[l]), l));
+        FPP_LAUNCH(B, kPrUpC, k_cup<T, T, T, T><<<Lc.n, kCUThreads, cup_smem(), s>>>(B->d_insts, tl(B, Lc), l));
     }
     const List& Lu = B->up[l];
     if (!Lu.n) continue;
@@ -354,12 +356,11 @@ void vcycle_fused(fluid_pp_batch* B, int with_dot) {
     else
       FPP_LAUNCH(B, kPrUpC, k_up<T, T, T, T><<<Lu.n, kFThreads, B->smem_up, s>>>(B->d_insts, tl(B, Lu), l));
   }
-  // gamma = r . (z - zmean) over the fixed level-0 tiles of every instance: the
-  // marching level-0 up step writes the partials of its instances with
-  // k_dot_rz_part's per-thread sums and folds, k_dot_rz_part those of the
-  // rest, so the fold order does not depend on which up kernel (chosen by how
-  // the batch fills the GPU) produced z and a solve gives the same bits alone
-  // and in any batch
+  // gamma = r . (z - zmean) over the fixed level-0 dot tiles of every
+  // instance: the column level-0 up step writes the partials of its instances,
+  // k_dot_rz_part those of the instances whose level 0 runs the box kernels.
+  // Which of the two an instance takes depends only on its lattice, so a solve
+  // gives the same bits alone and in any batch
   if (with_dot) {
     if (B->dot0.n)
       FPP_LAUNCH(B, kPrDot, k_dot_rz_part<<<launch_grid(B->dot0.n), kThreads, 0, s>>>(B->d_insts, tl(B, B->dot0),
@@ -377,7 +378,7 @@ void iter_launch(fluid_pp_batch* B, int pre, int post) {
   const int n0 = B->l0.n, g = launch_grid(n0);
   if (pre == 1 && post == 1) {
     vcycle_fused<T>(B, 1);
-    FPP_LAUNCH(B, kPrDirSpmv, k_dirspmv_m<<<B->spm.n, kMThreads, 0, s>>>(B->d_insts, tl(B, B->spm)));
+    FPP_LAUNCH(B, kPrDirSpmv, k_cdirspmv<<<B->cq.n, kSThreads, 0, s>>>(B->d_insts, tl(B, B->cq)));
     FPP_LAUNCH(B, kPrDirSpmv, k_dirspmv_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(B->d_insts,
                                                                                            il(B, B->multi)));
     FPP_LAUNCH(B, kPrUpdate, k_update_part<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
@@ -531,9 +532,15 @@ static cudaError_t configure_kernels_t(size_t factor, size_t block, size_t down,
   if (e == cudaSuccess) e = set((const void*)k_down<T, T, T, T>, down);
   if (e == cudaSuccess) e = set((const void*)k_up<float, float, T, T>, up);
   if (e == cudaSuccess) e = set((const void*)k_up<T, T, T, T>, up);
-  if (e == cudaSuccess) e = set((const void*)k_up_m<float, float, T, T>, size_t(march_up_smem_bytes()));
-  if (e == cudaSuccess) e = set((const void*)k_up_m<T, T, T, T>, size_t(march_up_smem_bytes()));
-  if (e == cudaSuccess) e = set((const void*)k_up_m<float, float, T, T, true>, size_t(march_up_smem_bytes()));
+  // column kernels (level 0: float32 inputs and diagonal; coarser levels: the storage type)
+  auto force = [](const void* f, int bytes) {
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  };
+  if (e == cudaSuccess) e = force((const void*)k_cdown<float, float, float, T>, cdown_smem());
+  if (e == cudaSuccess) e = force((const void*)k_cdown<T, T, T, T>, cdown_smem());
+  if (e == cudaSuccess) e = force((const void*)k_cup<float, float, float, T, true>, cup_smem());
+  if (e == cudaSuccess) e = force((const void*)k_cup<float, float, float, T>, cup_smem());
+  if (e == cudaSuccess) e = force((const void*)k_cup<T, T, T, T>, cup_smem());
   return e;
 }
 
@@ -639,7 +646,7 @@ static int batch_build(fluid_pp* const* handles, int count, const fluid_pp_batch
   // tile lists
   std::vector<Tile> tiles;
   std::vector<int> ilist;
-  std::vector<char> march0(count, 0);   // level-0 up step marches (and forms the gamma partials)
+  std::vector<char> col0(count, 0);   // level-0 up step is the column kernel (it forms the gamma partials)
   // restriction tiles (coarse tiles of kRX x kRY x kRZ) when `restrict_tiles`
   auto add_level = [&](List& L, auto pred, int level_of_tiles, bool restrict_tiles = false) {
     L.off = int(tiles.size());
@@ -652,6 +659,14 @@ static int batch_build(fluid_pp* const* handles, int count, const fluid_pp_batch
     }
     L.n = int(tiles.size()) - L.off;
   };
+  // z-chunk of a column tile: the longest candidate whose tiles over the batch
+  // reach the fill count (or the forced chunk); results do not depend on it
+  auto pick_chunk = [&](const int* cands, int ncand, int forced, auto tiles_at) {
+    if (forced > 0) return forced;
+    for (int i = 0; i < ncand; ++i)
+      if (tiles_at(cands[i]) >= tu.fill_tiles) return cands[i];
+    return cands[ncand - 1];
+  };
   add_level(B->l0, [](const InstDev&) { return true; }, 0);
   // grid-kernel levels of an instance are 0 .. first_block-1; the rest run in the coarse block
   for (int l = 0; l < B->maxL; ++l) {
@@ -660,63 +675,91 @@ static int batch_build(fluid_pp* const* handles, int count, const fluid_pp_batch
       add_level(B->rst[l], [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; }, l + 1, true);
     if (l >= 1) add_level(B->crs[l], [l](const InstDev& I) { return l < I.nlev; }, l);
     auto grid_level = [l](const InstDev& I) { return l < I.first_block && l < I.nlev - 1; };
-    // levels 0 and 1 coarsened by two on every axis take the marching steps when
-    // the batch has enough of their tiles to fill the GPU (a lone small lattice
-    // keeps the box kernels, whose tile shape follows the lattice)
-    const int march_levels = std::min(tu.march_levels, kMarchLevels);
-    auto eligible = [l, march_levels](const InstDev& I) {
+    // a level whose next coarser level halves every axis runs the column
+    // kernels, every other grid level the box kernels: a property of the
+    // lattice alone, never of the batch
+    auto column = [l, &grid_level](const InstDev& I) {
       const LevelDev& C = I.lv[l + 1];
-      return l <= march_levels - 1 && C.sx == 2 && C.sy == 2 && C.sz == 2;
+      return grid_level(I) && C.sx == 2 && C.sy == 2 && C.sz == 2;
     };
-    long long march_total = 0;
+    static const int kDownChunks[] = {16, 8, 4, 2, 1};
+    static const int kUpChunks0[] = {32, 16, 8};
+    static const int kUpChunks[] = {32, 16, 8, 4, 2};
+    const int forced_up = tu.chunk_planes > 0 ? std::max(l == 0 ? 8 : 2, tu.chunk_planes >> l) : 0;
+    const int forced_dn = tu.chunk_planes > 0 ? std::max(1, tu.chunk_planes >> (l + 1)) : 0;
+    const int cdz = pick_chunk(kDownChunks, 5, forced_dn, [&](int cz) {
+      long long n = 0;
+      for (int k = 0; k < count; ++k)
+        if (column(insts[k])) n += cdown_tiles(insts[k].lv[l + 1].nx, insts[k].lv[l + 1].ny, insts[k].lv[l + 1].nz, cz);
+      return n;
+    });
+    const int cuz = l == 0 ? pick_chunk(kUpChunks0, 3, forced_up, [&](int cz) {
+      long long n = 0;
+      for (int k = 0; k < count; ++k)
+        if (column(insts[k])) n += cup_tiles(insts[k].lv[0].nx, insts[k].lv[0].ny, insts[k].lv[0].nz, cz);
+      return n;
+    }) : pick_chunk(kUpChunks, 5, forced_up, [&](int cz) {
+      long long n = 0;
+      for (int k = 0; k < count; ++k)
+        if (column(insts[k])) n += cup_tiles(insts[k].lv[l].nx, insts[k].lv[l].ny, insts[k].lv[l].nz, cz);
+      return n;
+    });
     for (int k = 0; k < count; ++k)
-      if (grid_level(insts[k]) && eligible(insts[k])) {
-        const LevelDev& C = insts[k].lv[l + 1];
-        march_total += march_down_tiles(C.nx, C.ny, C.nz);
+      if (column(insts[k])) {
+        insts[k].lv[l].cdz = cdz;
+        insts[k].lv[l].cuz = cuz;
       }
-    const bool march_level = march_total >= tu.fill_tiles;
-    auto marching = [&](const InstDev& I) { return march_level && eligible(I); };
     B->dn[l].off = int(tiles.size());
     for (int k = 0; k < count; ++k)
-      if (grid_level(insts[k]) && !marching(insts[k]))
+      if (grid_level(insts[k]) && !column(insts[k]))
         for (int t = 0; t < insts[k].lv[l].dtiles; ++t) tiles.push_back(Tile{k, l, t, 0});
     B->dn[l].n = int(tiles.size()) - B->dn[l].off;
-    B->dnm[l].off = int(tiles.size());
+    B->cdn[l].off = int(tiles.size());
     for (int k = 0; k < count; ++k)
-      if (grid_level(insts[k]) && marching(insts[k])) {
+      if (column(insts[k])) {
         const LevelDev& C = insts[k].lv[l + 1];
-        const int nt = march_down_tiles(C.nx, C.ny, C.nz);
+        const int nt = cdown_tiles(C.nx, C.ny, C.nz, cdz);
         for (int t = 0; t < nt; ++t) tiles.push_back(Tile{k, l, t, 0});
       }
-    B->dnm[l].n = int(tiles.size()) - B->dnm[l].off;
+    B->cdn[l].n = int(tiles.size()) - B->cdn[l].off;
     B->up[l].off = int(tiles.size());
     for (int k = 0; k < count; ++k)
-      if (grid_level(insts[k]) && !marching(insts[k]))
+      if (grid_level(insts[k]) && !column(insts[k]))
         for (int t = 0; t < insts[k].lv[l].utiles; ++t) tiles.push_back(Tile{k, l, t, 0});
     B->up[l].n = int(tiles.size()) - B->up[l].off;
-    B->upm[l].off = int(tiles.size());
+    B->cup[l].off = int(tiles.size());
     for (int k = 0; k < count; ++k)
-      if (grid_level(insts[k]) && marching(insts[k])) {
+      if (column(insts[k])) {
         const LevelDev& Lv = insts[k].lv[l];
-        const int nt = march_up_tiles(Lv.nx, Lv.ny, Lv.nz);
+        const int nt = cup_tiles(Lv.nx, Lv.ny, Lv.nz, cuz);
         for (int t = 0; t < nt; ++t) tiles.push_back(Tile{k, l, t, 0});
-        if (l == 0) march0[k] = 1;
+        if (l == 0) col0[k] = 1;
       }
-    B->upm[l].n = int(tiles.size()) - B->upm[l].off;
+    B->cup[l].n = int(tiles.size()) - B->cup[l].off;
   }
   B->dot0.off = int(tiles.size());
   for (int k = 0; k < count; ++k)
-    if (!march0[k])
+    if (!col0[k])
       for (int t = 0; t < insts[k].lv[0].ntiles; ++t) tiles.push_back(Tile{k, 0, t, 0});
   B->dot0.n = int(tiles.size()) - B->dot0.off;
   add_level(B->l0single, [](const InstDev& I) { return I.nlev == 1; }, 0);
-  B->spm.off = int(tiles.size());
-  for (int k = 0; k < count; ++k) {
-    const InstDev& I = B->h[k]->inst;
-    const int nt = march_spmv_tiles(I.lv[0].nx, I.lv[0].ny, I.lv[0].nz);
-    for (int t = 0; t < nt; ++t) tiles.push_back(Tile{k, 0, t, 0});
+  {
+    static const int kSpmvChunks[] = {32, 16, 8};
+    const int forced = tu.chunk_planes > 0 ? std::max(8, tu.chunk_planes) : 0;
+    const int cqz = pick_chunk(kSpmvChunks, 3, forced, [&](int cz) {
+      long long n = 0;
+      for (int k = 0; k < count; ++k) n += cspmv_tiles(insts[k].lv[0].nx, insts[k].lv[0].ny, insts[k].lv[0].nz, cz);
+      return n;
+    });
+    B->cq.off = int(tiles.size());
+    for (int k = 0; k < count; ++k) {
+      insts[k].lv[0].cqz = cqz;
+      const LevelDev& L0 = insts[k].lv[0];
+      const int nt = cspmv_tiles(L0.nx, L0.ny, L0.nz, cqz);
+      for (int t = 0; t < nt; ++t) tiles.push_back(Tile{k, 0, t, 0});
+    }
+    B->cq.n = int(tiles.size()) - B->cq.off;
   }
-  B->spm.n = int(tiles.size()) - B->spm.off;
   B->bake.off = int(tiles.size());
   for (int k = 0; k < count; ++k) {
     const InstDev& I = B->h[k]->inst;
@@ -1067,6 +1110,9 @@ static size_t arena_size(const fluid_pp_config& cfg, const HierarchyPlan& plan) 
   acc(sizeof(double) * kSlots * tiles_of(nx, ny, nz, kMaxDepth));
   acc(sizeof(double) * ncoarse * ncoarse);
   acc(sizeof(Ctrl));
+  // slack: the column kernels copy 2-byte level arrays in aligned 4-byte words,
+  // which may reach up to 6 bytes past an array's last element
+  acc(256);
   return bytes;
 }
 
@@ -1456,7 +1502,7 @@ int fluid_pp_apply_vcycle(fluid_pp* pp, const float* r, float* z, int pre, int p
 void fluid_pp_batch_tuning_default(fluid_pp_batch_tuning* tuning) {
   if (!tuning) return;
   tuning->fill_tiles = kFillTiles;
-  tuning->march_levels = kMarchLevels;
+  tuning->chunk_planes = 0;
   tuning->box_shape = -1;
   tuning->parts = 1;
 }
@@ -1470,9 +1516,11 @@ int fluid_pp_batch_create_tuned(fluid_pp* const* handles, int count, const fluid
   fluid_pp_batch_tuning tu;
   fluid_pp_batch_tuning_default(&tu);
   if (tuning) {
-    if (tuning->fill_tiles < 1 || tuning->march_levels < 0 || tuning->box_shape < -1 || tuning->box_shape > 4 ||
-        tuning->parts < 1 || tuning->parts > 16) {
-      g_err = "batch tuning: fill_tiles >= 1, march_levels >= 0, box_shape in -1..4, parts in 1..16";
+    if (tuning->fill_tiles < 1 || tuning->chunk_planes < 0 || tuning->chunk_planes > 256 ||
+        tuning->chunk_planes % 8 != 0 || tuning->box_shape < -1 || tuning->box_shape > 4 || tuning->parts < 1 ||
+        tuning->parts > 16) {
+      g_err = "batch tuning: fill_tiles >= 1, chunk_planes a multiple of 8 in 0..256, box_shape in -1..4, "
+              "parts in 1..16";
       return FLUID_PP_INVALID_ARG;
     }
     tu = *tuning;

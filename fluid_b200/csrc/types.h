@@ -59,6 +59,9 @@ struct LevelDev {
   int dtiles;         // tiles of that step
   int utx, uty, utz;  // fused up step l+1 -> l: fine cells per tile
   int utiles;
+  int cdz;            // column down step l -> l+1: coarse planes per tile (levels coarsened by two on every axis)
+  int cuz;            // column up step l+1 -> l: fine planes per tile (a multiple of 8 on level 0)
+  int cqz;            // level 0: direction + SpMV, fine planes per tile (a multiple of 8)
   float wx, wy, wz;   // normalised off-diagonal weights w_a / wmax
   float wmax;         // (h0 / h_a)^2 maximum over axes; level operators are stored divided by it
   float ext_phi;      // open-top exterior phi (finest-cell units)

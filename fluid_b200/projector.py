@@ -229,15 +229,15 @@ class PressureProjector:
         return z
 
 
-def batch_tuning(fill_tiles=None, march_levels=None, box_shape=None, parts=None) -> BatchTuning:
+def batch_tuning(fill_tiles=None, chunk_planes=None, box_shape=None, parts=None) -> BatchTuning:
     """The library's default batch layout with the given fields replaced
     (``fluid_pp_batch_tuning``; results never depend on it, only speed)."""
     t = BatchTuning()
     load().fluid_pp_batch_tuning_default(ctypes.byref(t))
     if fill_tiles is not None:
         t.fill_tiles = int(fill_tiles)
-    if march_levels is not None:
-        t.march_levels = int(march_levels)
+    if chunk_planes is not None:
+        t.chunk_planes = int(chunk_planes)
     if box_shape is not None:
         t.box_shape = int(box_shape)
     if parts is not None:

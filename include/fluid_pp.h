@@ -202,22 +202,25 @@ int fluid_pp_batch_download_async(fluid_pp_batch* batch, float* const* p, float*
 
 /* How a batch lays out its work (no reference counterpart: the reference
  * solves one grid per device).  A launch of a V-cycle step needs enough tiles
- * to fill the GPU; fill_tiles is that count (default 148, one per SM): the box
- * kernels take the largest tile shape whose tiles over the batch reach it, and
- * a level of the finest march_levels (0, 1 or 2; default 2) takes the 2.5-D
- * marching form when its marching tiles reach it.  box_shape 0..4 forces a box
- * tile shape (largest first), -1 (default) leaves it to fill_tiles.  parts
- * (1..16, default 1) splits the handles into that many sub-batches of about
- * equal cells, each solved on a stream of its own, all started together and
- * joined back to the batch's stream (graph-mode solves; direct launches run
- * the whole batch), so that one part's small launches and last iterations
- * overlap another's work.  Every layout applies the same arithmetic per cell
- * and folds every scalar over the same fixed tiles of one instance, so a
- * batch's results do not depend on its tuning, bit for bit; only its speed
- * does (fluid_b200.autotune measures the candidates). */
+ * to fill the GPU; fill_tiles is that count (default 148, one per SM).  Levels
+ * whose next coarser level halves every axis run the column-block kernels,
+ * whose tiles are fixed in x / y and split along z into chunks: chunk_planes
+ * is the chunk length in level-0 fine planes (a multiple of 8 up to 256,
+ * halved on each coarser level), 0 (default) takes the longest chunk whose
+ * tiles over the batch reach fill_tiles.  The other levels run box kernels,
+ * which take the largest tile shape whose tiles over the batch reach
+ * fill_tiles; box_shape 0..4 forces one (largest first), -1 (default) leaves
+ * it to fill_tiles.  parts (1..16, default 1) splits the handles into that many
+ * sub-batches of about equal cells, each solved on a stream of its own, all
+ * started together and joined back to the batch's stream (graph-mode solves;
+ * direct launches run the whole batch), so that one part's small launches and
+ * last iterations overlap another's work.  Every layout applies the same
+ * arithmetic per cell and folds every scalar over the same fixed tiles of one
+ * instance, so a batch's results do not depend on its tuning, bit for bit;
+ * only its speed does (fluid_b200.autotune measures the candidates). */
 typedef struct fluid_pp_batch_tuning {
   int fill_tiles;
-  int march_levels;
+  int chunk_planes;
   int box_shape;
   int parts;
 } fluid_pp_batch_tuning;

@@ -30,7 +30,7 @@ def test_cached_choice_is_returned_without_measuring(tmp_path):
     ps = [FakeProjector((16, 16, 16))]
     key = autotune.signature(ps)
     path = tmp_path / "tune.json"
-    stored = {"tuning": {"fill_tiles": 148, "march_levels": 0, "box_shape": -1}, "sweeps": [1, 1], "ms": 1.5,
+    stored = {"tuning": {"fill_tiles": 148, "chunk_planes": 0, "box_shape": -1}, "sweeps": [1, 1], "ms": 1.5,
               "default_ms": 2.0, "table": []}
     path.write_text(json.dumps({key: stored}))
     autotune._cache.pop(key, None)
@@ -49,10 +49,11 @@ def test_tuning_defaults_and_rejected_fields():
 
     from fluid_b200 import _abi
     from fluid_b200.projector import batch_tuning
-    assert batch_tuning().as_dict() == {"fill_tiles": 148, "march_levels": 2, "box_shape": -1, "parts": 1}
+    assert batch_tuning().as_dict() == {"fill_tiles": 148, "chunk_planes": 0, "box_shape": -1, "parts": 1}
     L = _abi.load()
     out = ctypes.c_void_p()
-    for bad in (dict(fill_tiles=0), dict(march_levels=-1), dict(box_shape=5), dict(parts=0), dict(parts=17)):
+    for bad in (dict(fill_tiles=0), dict(chunk_planes=-8), dict(chunk_planes=12), dict(chunk_planes=264), dict(box_shape=5),
+                dict(parts=0), dict(parts=17)):
         t = batch_tuning(**bad)
         assert L.fluid_pp_batch_create_tuned(None, 0, ctypes.byref(t), ctypes.byref(out)) == _abi.INVALID_ARG, bad
     good = batch_tuning(parts=4)

@@ -199,10 +199,11 @@ def test_batch_is_identical_to_single(tuning):
         np.testing.assert_array_equal(p1, pp.download()[0])   # pressure in Pa carries each instance's dt
 
 
-def test_marching_batch_is_identical_to_box_singles():
-    """Thirteen 64x48x64 grids fill the GPU as a batch, which takes the 2.5-D
-    marching level-0 steps; each grid alone keeps the box-tiled steps.  Both apply
-    the same arithmetic per cell, so pressures and iteration counts agree bit for bit."""
+def test_batch_of_thirteen_is_identical_to_singles():
+    """Thirteen 64x48x64 grids fill the GPU as a batch, so the column kernels take
+    long z chunks; each grid alone takes short chunks to fill the GPU by itself.
+    Halo cells repeat their owner's arithmetic and the dot products fold over
+    fixed tiles, so pressures and iteration counts agree bit for bit."""
     states = [configs.random_small(64, 48, 64, seed=60 + k) for k in range(13)]
     singles = []
     for s in states:
@@ -361,7 +362,7 @@ def test_full_size_dam_spheres_matches_fp64_oracle(full_size_dam_spheres, precis
 
 
 def test_batch_layouts_give_the_same_bits_and_autotune_keeps_the_fastest():
-    """Every batch layout (box shapes, marching on or off, fill counts, concurrent parts) gives the
+    """Every batch layout (box shapes, column z chunks, fill counts, concurrent parts) gives the
     default layout's pressures and iteration counts bit for bit; the autotuner's
     choice is never slower than the default it measured."""
     from fluid_b200 import autotune
@@ -374,8 +375,8 @@ def test_batch_layouts_give_the_same_bits_and_autotune_keeps_the_fastest():
             pp.upload_state(s.vof, s.u, s.v, s.w)
 
     dts = [s.dt for s in states]
-    layouts = [None, dict(march_levels=0), dict(march_levels=1, fill_tiles=148), dict(box_shape=4, march_levels=0),
-               dict(fill_tiles=4096), dict(parts=2), dict(parts=3, march_levels=0)]
+    layouts = [None, dict(chunk_planes=8), dict(chunk_planes=64, fill_tiles=148), dict(box_shape=4, chunk_planes=16),
+               dict(fill_tiles=4096), dict(parts=2), dict(parts=3, chunk_planes=32)]
     ref = None
     for lay in layouts:
         b = BatchProjector(pps, tuning=lay)
@@ -390,7 +391,7 @@ def test_batch_layouts_give_the_same_bits_and_autotune_keeps_the_fastest():
         assert got[0] == ref[0], lay
         for a, c in zip(got[1], ref[1]):
             np.testing.assert_array_equal(a, c, err_msg=str(lay))
-    cands = tuple(dict(batch_tuning(**lay).as_dict()) for lay in [dict(), dict(march_levels=0), dict(fill_tiles=148)])
+    cands = tuple(dict(batch_tuning(**lay).as_dict()) for lay in [dict(), dict(chunk_planes=8), dict(fill_tiles=148)])
     res = autotune.autotune_batch(pps, dts, restore, layouts=cands, parts=(2,), sweeps=((1, 1), (2, 2)), repeats=1)
     assert res.ms <= res.default_ms
     assert len(res.table) == 5 and res.sweeps in ((1, 1), (2, 2))
