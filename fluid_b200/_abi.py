@@ -37,7 +37,7 @@ EXPORTS = (
     "fluid_pp_tall_project_begin", "fluid_pp_tall_project_continue", "fluid_pp_tall_project_end",
     "fluid_pp_batch_project_async", "fluid_pp_batch_receipts_read", "fluid_pp_download_async",
     "fluid_pp_synchronize", "fluid_pp_batch_tuning_default", "fluid_pp_batch_create_tuned",
-    "fluid_pp_batch_upload_state", "fluid_pp_batch_download_async",
+    "fluid_pp_batch_upload_state", "fluid_pp_batch_download_async", "fluid_pp_tall_solve_rhs",
 )
 STAGES = ("reset", "label", "coarsen", "bake", "factor", "init", "smooth0", "smoothc", "residual0", "residualc",
           "restrict0", "restrictc", "coarse", "prolong0", "prolongc", "dot", "dir", "spmv", "update", "true",
@@ -161,6 +161,7 @@ def load():
     L.fluid_pp_tall_get_labels.argtypes = [vp, ci, vp]
     L.fluid_pp_tall_apply_operator.argtypes = [vp, vp, vp]
     L.fluid_pp_tall_get_pressure.argtypes = [vp, vp]
+    L.fluid_pp_tall_solve_rhs.argtypes = [vp, cf, vp, ctypes.POINTER(SolveOpts), vp, ctypes.POINTER(Receipt)]
     L.fluid_pp_tall_last_error.argtypes = [vp]
     L.fluid_pp_tall_last_error.restype = ctypes.c_char_p
     L.fluid_pp_required_bytes.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_ulonglong)]

@@ -73,6 +73,13 @@ struct TLevel {
   float* rhs;
   float* res;
   unsigned long long* acc;   // restriction accumulators (levels >= 1)
+  // Level 0 only: the operator's entries in float64 (the assembly's values
+  // before the float rounding).  The true residual applies them, so CG with
+  // residual replacement converges to the float64 system's solution; the
+  // V-cycle and the CG SpMV use the float entries above.
+  double* diag64;
+  double* a0164;
+  double* tval64;
 };
 
 struct TInst {
@@ -285,8 +292,10 @@ __global__ void k_tall_assemble_band(TInst* I, int l) {
         dg += rn.liq ? 1.0 : 1.0 / ghost_theta_d(ph, rn.phi);
       }
       L.diag[k] = float(dg);
+      if (L.diag64) L.diag64[k] = dg;
     } else {
       L.diag[k] = 1.0f;
+      if (L.diag64) L.diag64[k] = 1.0;
     }
   }
 }
@@ -323,6 +332,7 @@ __global__ void k_tall_assemble_tall(TInst* I, int l) {
       }
       L.tidx[cnt * nrow + row] = s;
       L.tval[cnt * nrow + row] = float(v);
+      if (L.tval64) L.tval64[cnt * nrow + row] = v;
       ++cnt;
     };
     if (L.label[s0]) {
@@ -395,18 +405,30 @@ __global__ void k_tall_assemble_tall(TInst* I, int l) {
       L.diag[s0] = float(a00);
       L.diag[s1] = float(a11);
       L.a01[c] = float(a01);
+      if (L.diag64) {
+        L.diag64[s0] = a00;
+        L.diag64[s1] = a11;
+        L.a0164[c] = a01;
+      }
     } else {
       L.diag[s0] = 1.0f;
       L.diag[s1] = 1.0f;
       L.a01[c] = 0.0f;
+      if (L.diag64) {
+        L.diag64[s0] = 1.0;
+        L.diag64[s1] = 1.0;
+        L.a0164[c] = 0.0;
+      }
     }
     for (int s = n0; s < kTallW; ++s) {
       L.tidx[s * nrow + 2 * c] = s0;
       L.tval[s * nrow + 2 * c] = 0.0f;
+      if (L.tval64) L.tval64[s * nrow + 2 * c] = 0.0;
     }
     for (int s = n1; s < kTallW; ++s) {
       L.tidx[s * nrow + 2 * c + 1] = s1;
       L.tval[s * nrow + 2 * c + 1] = 0.0f;
+      if (L.tval64) L.tval64[s * nrow + 2 * c + 1] = 0.0;
     }
   }
 }
@@ -872,13 +894,14 @@ __global__ void k_tall_true(TInst* I) {
     sample_active(L, k, x, j, z, b);
     const int col = x + L.nx * z;
     auto X = [&](int s) { return double(I->x[s]) + double(I->xlo[s]); };
-    double s = double(L.diag[k]) * X(k);
+    // the float64 operator (the assembly's values, band weights unrounded)
+    double s = L.diag64[k] * X(k);
     if (j >= 2) {
-      band_entries(L, x, j, z, b, [&](int sn, double w) { s += double(float(w)) * X(sn); });
+      band_entries(L, x, j, z, b, [&](int sn, double w) { s += w * X(sn); });
     } else {
       const int nrow = 2 * L.ncol, row = 2 * col + j;
-      s += double(L.a01[col]) * X(sidx(L, x, 1 - j, z));
-      for (int e = 0; e < kTallW; ++e) s += double(L.tval[e * nrow + row]) * X(L.tidx[e * nrow + row]);
+      s += L.a0164[col] * X(sidx(L, x, 1 - j, z));
+      for (int e = 0; e < kTallW; ++e) s += L.tval64[e * nrow + row] * X(L.tidx[e * nrow + row]);
     }
     const double rv = double(I->b[k]) - s;
     L.rhs[k] = float(rv);
@@ -1470,6 +1493,11 @@ size_t tall_arena_size(const TallPlan& plan) {
     acc(4 * kTallW * 2 * nc); acc(4 * kTallW * 2 * nc);
     acc(4 * n); acc(4 * n); acc(4 * n);            // z rhs res
     if (l > 0) acc(8 * n);                         // acc
+    if (l == 0) {                                  // float64 operator for the true residual
+      acc(8 * n);
+      acc(8 * nc);
+      acc(8 * kTallW * 2 * nc);
+    }
   }
   const size_t n0 = size_t(plan.levels[0].samples());
   for (int k = 0; k < 10; ++k) acc(4 * n0);        // vof u v w b x xlo d q p_si
@@ -1545,6 +1573,9 @@ int tall_create(const fluid_pp_tall_config* cfg, const int* bases, fluid_pp_tall
     V.rhs = static_cast<float*>(take(4 * n));
     V.res = static_cast<float*>(take(4 * n));
     V.acc = l > 0 ? static_cast<unsigned long long*>(take(8 * n)) : nullptr;
+    V.diag64 = l == 0 ? static_cast<double*>(take(8 * n)) : nullptr;
+    V.a0164 = l == 0 ? static_cast<double*>(take(8 * nc)) : nullptr;
+    V.tval64 = l == 0 ? static_cast<double*>(take(8 * kTallW * 2 * nc)) : nullptr;
   }
   I.vof = static_cast<float*>(take(4 * n0));
   I.u = static_cast<float*>(take(4 * n0));
@@ -1835,6 +1866,53 @@ int fluid_pp_tall_apply_operator(fluid_pp_tall* T, const float* p, float* out) {
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(T->stream);
   return e == cudaSuccess ? FLUID_PP_OK : T->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+}
+
+// Solves the assembled level-0 system A x = b for a caller-given b (finest-cell
+// units; entries on air samples are ignored) with the projection's MGPCG, for
+// parity tests that refine a float64 solution with the device solver; x is the
+// solution in finest-cell units.  Labels, hierarchy and operator come from the
+// uploaded state and dt, as in fluid_pp_tall_prepare.
+int fluid_pp_tall_solve_rhs(fluid_pp_tall* T, float dt, const float* b, const fluid_pp_solve_opts* opts, float* x,
+                            fluid_pp_receipt* receipt) {
+  if (!T || !b || !x) return FLUID_PP_INVALID_ARG;
+  if (!(dt > 0) || !std::isfinite(dt)) return T->set_error(FLUID_PP_INVALID_ARG, "dt must be positive and finite");
+  if (!T->has_state) return T->set_error(FLUID_PP_INVALID_ARG, "state not uploaded");
+  fluid_pp_solve_opts o{1e-6, 0.0, 200, 1, 1, 4, 0, 0.0};
+  if (opts) o = *opts;
+  if (!(o.rel_tol >= 0) || !(o.abs_tol >= 0) || o.max_iters < 1)
+    return T->set_error(FLUID_PP_INVALID_ARG, "invalid solve options");
+  cudaSetDevice(T->cfg.device);
+  cudaStream_t s = T->stream;
+  TInst& I = T->inst;
+  tall_set_dt(T, dt);
+  launch_setup(T);
+  cudaMemcpyAsync(I.b, b, size_t(I.lv[0].n) * 4, cudaMemcpyHostToDevice, s);
+  k_tall_cg_init<<<grid_for(I.lv[0].n), kTB, 0, s>>>(T->d_inst, o.rel_tol, o.abs_tol, o.max_iters,
+                                                      o.true_residual_every, o.rel_tol_inf);
+  T->solving = true;
+  T->solved = false;
+  T->it = 0;
+  T->cap = o.max_iters + 2;
+  int finished = 0;
+  int rc = fluid_pp_tall_project_continue(T, 0, &finished);
+  T->solving = false;
+  if (rc != FLUID_PP_OK) return rc;
+  const Ctrl& c = *T->h_ctrl;
+  int status = c.status;
+  if (!c.done && status == FLUID_PP_OK) status = FLUID_PP_NONCONVERGENCE;
+  if (receipt) {
+    std::memset(receipt, 0, sizeof(*receipt));
+    receipt->status = status;
+    receipt->iterations = c.iter;
+    receipt->liquid_cells = c.liquid;
+    receipt->levels = I.nlev;
+    receipt->b_norm = std::sqrt(std::max(0.0, c.bb));
+    receipt->rel_residual = c.bb > 0 ? std::sqrt(std::max(0.0, c.rr) / c.bb) : 0.0;
+    receipt->true_rel_residual = c.bb > 0 ? std::sqrt(std::max(0.0, c.rr_true) / c.bb) : 0.0;
+  }
+  rc = fluid_pp_tall_get_pressure(T, x);
+  return rc != FLUID_PP_OK ? rc : status;
 }
 
 const char* fluid_pp_tall_last_error(fluid_pp_tall* T) { return T ? T->err.c_str() : ""; }

@@ -175,3 +175,15 @@ class TallProjector:
         p = np.empty(self.shape, np.float32)
         _check(load().fluid_pp_tall_get_pressure(self._h, ptr(p)), self._h, "pressure")
         return p
+
+    def solve_rhs(self, dt: float, b, **opts):
+        """Parity hook: solve A x = b (finest-cell units, packed) with the device
+        MGPCG on the system built from the uploaded state; returns (x, receipt)."""
+        b = np.ascontiguousarray(np.asarray(b, np.float32).reshape(self.shape))
+        x = np.empty(self.shape, np.float32)
+        o = solve_opts(**opts)
+        r = Receipt()
+        rc = load().fluid_pp_tall_solve_rhs(self._h, float(dt), ptr(b), ctypes.byref(o), ptr(x), ctypes.byref(r))
+        if rc not in (_abi.OK, _abi.NONCONVERGENCE, _abi.NONFINITE, _abi.UNSUPPORTED):
+            _check(rc, self._h, "solve_rhs")
+        return x, r.as_dict()

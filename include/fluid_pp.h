@@ -358,6 +358,14 @@ int fluid_pp_tall_get_rhs(fluid_pp_tall* tall, float* b);
 int fluid_pp_tall_get_labels(fluid_pp_tall* tall, int level, unsigned char* label);
 int fluid_pp_tall_apply_operator(fluid_pp_tall* tall, const float* p, float* out);
 int fluid_pp_tall_get_pressure(fluid_pp_tall* tall, float* p);
+/* Parity hook: solve the assembled finest system A x = b for a caller-given b
+ * (host, finest-cell units, packed; air entries ignored) with the projection's
+ * MGPCG, after labels, hierarchy and operator are built from the uploaded state
+ * and dt.  x (host, packed) receives the solution in finest-cell units.  Lets a
+ * test refine a float64 solution of an independently assembled system with the
+ * device solver.  Returns the solve status. */
+int fluid_pp_tall_solve_rhs(fluid_pp_tall* tall, float dt, const float* b, const fluid_pp_solve_opts* opts,
+                            float* x, fluid_pp_receipt* receipt);
 const char* fluid_pp_tall_last_error(fluid_pp_tall* tall);
 /* Device bytes a tall handle for this layout allocates; host only. */
 int fluid_pp_tall_required_bytes(const fluid_pp_tall_config* config, const int* bases, unsigned long long* bytes);

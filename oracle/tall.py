@@ -264,3 +264,38 @@ class TallGrid:
                         th = 1.0 if (li and lj) else (ghost_theta(pi_, pj_) if li else ghost_theta(pj_, pi_))
                         arr[z, j, x] -= (self.pressure_at(p, xn, yn, zn) - self.pressure_at(p, x, y, z)) / th
         return u2, v2, w2
+
+
+# ---------------------------------------------------------------------------
+# The same system at any size: oracle/tall_oracle.cpp assembles the operator and
+# right-hand side from the dense faces in float64 (per column, in parallel).
+def assemble_fp64(nx: int, fine_ny: int, nz: int, band: int, bases, vof, u, v, w):
+    """(A as scipy CSR over the packed samples, b = T^T (-div u)) in float64;
+    the arrays are packed (nz, band + 2, nx) as in TallGrid.set_state."""
+    import ctypes
+
+    from .oracle import lib
+    L = lib()
+    f = L.orc_tall_assemble
+    vp, ci, cl = ctypes.c_void_p, ctypes.c_int, ctypes.c_long
+    f.argtypes = [ci, ci, ci, ci, vp, vp, vp, vp, vp, vp, vp, vp, cl, ctypes.POINTER(cl), vp]
+    f.restype = ci
+    P = band + 2
+    n = nx * P * nz
+    arrs = [np.ascontiguousarray(np.asarray(a, np.float32).reshape(nz, P, nx)) for a in (vof, u, v, w)]
+    bs = np.ascontiguousarray(np.asarray(bases, np.int32).reshape(nz, nx))
+    ptr = lambda a: a.ctypes.data_as(vp) if a is not None else None
+    indptr = np.zeros(n + 1, np.int64)
+    nnz = cl(0)
+    rc = f(nx, fine_ny, nz, band, ptr(bs), *(ptr(a) for a in arrs), ptr(indptr), None, None, 0, ctypes.byref(nnz),
+           None)
+    if rc:
+        raise ValueError("tall oracle: band too wide")
+    indices = np.zeros(nnz.value, np.int32)
+    data = np.zeros(nnz.value, np.float64)
+    b = np.zeros(n, np.float64)
+    rc = f(nx, fine_ny, nz, band, ptr(bs), *(ptr(a) for a in arrs), ptr(indptr), ptr(indices), ptr(data), nnz.value,
+           ctypes.byref(nnz), ptr(b))
+    if rc:
+        raise ValueError("tall oracle: assembly failed")
+    return sp.csr_matrix((data, indices, indptr), shape=(n, n)), b

@@ -10,6 +10,13 @@ pytestmark = pytest.mark.gpu
 
 REL_L2_PRESSURE = 1e-5
 REL_RES = 1e-6
+# The tall layout's weakest mode (a near-constant pressure offset, coupled to the
+# free surface through tall cells hundreds of rows high) lets a relative
+# residual of 1e-6 leave a pressure error of about 2e-5 against the float64
+# solution (measured at 256^2 x 1024: 2.0e-5 at 1e-6, 2.5e-6 at 1e-8, with the
+# true residual evaluated in float64).  The parity tests therefore solve to
+# 1e-7; the bench states the float64 error at its 1e-6 operating point.
+REL_RES_PARITY = 1e-7
 
 CASES = {
     "waves12x10": lambda: configs.tall_waves(12, 10, 64, 16, seed=21, mean=30, amp_max=4, lam=(4, 16),
@@ -49,9 +56,9 @@ def test_tall_labels_rhs_operator(name):
 def test_tall_project_matches_oracle(name):
     s = CASES[name]()
     tp, g = _pair(s)
-    rec = tp.project(s.dt, rel_tol=REL_RES)
+    rec = tp.project(s.dt, rel_tol=REL_RES_PARITY)
     assert rec["status_name"] == "OK", rec
-    assert rec["true_rel_residual"] <= REL_RES
+    assert rec["true_rel_residual"] <= REL_RES_PARITY
     assert rec["levels"] >= 2
     p_o, _, _ = g.solve()
     p_d = tp.pressure().ravel().astype(np.float64)
@@ -64,8 +71,58 @@ def test_tall_project_matches_oracle(name):
     assert rec["max_div_after"] <= 1e-5 * rec["max_div_before"], rec
 
 
-def test_tall_full_size_waves_converge():
+@pytest.fixture(scope="module")
+def full_size_tall():
+    """The 256^2 x 1024 wave tank (2.23M samples) with its float64 operator and
+    right-hand side assembled by the oracle from the dense faces."""
     s = configs.tall_waves()
+    A, b = oracle.assemble_fp64(s.nx, s.fine_ny, s.nz, s.band, s.bases, s.vof, s.u, s.v, s.w)
+    return s, A, b
+
+
+def fp64_solution(tp, s, A, b, max_steps=12):
+    """The float64 solution of the oracle's system A x = b by iterative
+    refinement: float64 residuals with the oracle's operator, corrections from
+    the device MGPCG.  Returns x and ||b - A x|| / ||b|| (certified in float64)."""
+    x = np.zeros_like(b)
+    nb = np.linalg.norm(b)
+    rel = 1.0
+    for _ in range(max_steps):
+        r = b - A @ x
+        rel = np.linalg.norm(r) / nb
+        if rel <= 1e-12:
+            break
+        e, rec = tp.solve_rhs(s.dt, r.astype(np.float32), rel_tol=REL_RES)
+        assert rec["status_name"] in ("OK", "NONCONVERGENCE"), rec
+        x += e.ravel().astype(np.float64)
+    return x, rel
+
+
+def test_tall_full_size_labels_rhs_operator(full_size_tall):
+    s, A, b = full_size_tall
+    tp = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho)
+    tp.upload_state(s.vof, s.u, s.v, s.w)
+    tp.prepare(s.dt)
+    # liquid samples: vof > 0.5 on active band rows; a tall segment follows its bottom sample
+    rows = configs.tall_sample_rows(s.bases, s.band)
+    lab = (s.vof > 0.5) & (rows < s.fine_ny)
+    lab[:, 1, :] = lab[:, 0, :]
+    np.testing.assert_array_equal(tp.labels(0).reshape(lab.shape), lab.astype(np.uint8))
+    b_d = tp.rhs().ravel()
+    assert np.abs(b_d - b).max() <= 1e-5 * np.abs(b).max()
+    p = (np.random.default_rng(3).normal(size=tp.shape) * lab).astype(np.float32)
+    ap_o = A @ p.ravel().astype(np.float64)
+    ap_d = tp.apply_operator(p).ravel()
+    assert np.linalg.norm(ap_d - ap_o) <= 1e-6 * np.linalg.norm(ap_o)
+    tp.destroy()
+
+
+def test_tall_full_size_matches_fp64(full_size_tall):
+    """The 2.23M-sample projection against the float64 solution of the oracle's
+    independently assembled system: receipts at the 1e-6 operating point,
+    divergence over represented band cells reduced by 1e-4, and at the parity
+    tolerance pressure rel-L2 <= 1e-5."""
+    s, A, b = full_size_tall
     tp = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho)
     tp.upload_state(s.vof, s.u, s.v, s.w)
     rec = tp.project(s.dt, rel_tol=REL_RES)
@@ -73,6 +130,16 @@ def test_tall_full_size_waves_converge():
     assert rec["true_rel_residual"] <= REL_RES
     assert rec["levels"] == 7
     assert rec["max_div_after"] <= 1e-4 * rec["max_div_before"], rec
+    tp.upload_state(s.vof, s.u, s.v, s.w)
+    rec = tp.project(s.dt, rel_tol=REL_RES_PARITY)
+    assert rec["status_name"] == "OK", rec
+    p_d = tp.pressure().ravel().astype(np.float64)
+    tp.upload_state(s.vof, s.u, s.v, s.w)
+    x, rel = fp64_solution(tp, s, A, b)
+    assert rel <= 1e-12, rel
+    err = np.linalg.norm(p_d - x) / np.linalg.norm(x)
+    assert err <= REL_L2_PRESSURE, err
+    tp.destroy()
 
 
 def test_tall_sliced_projection_matches_one_call():
