@@ -62,17 +62,18 @@ def stage_bytes_per_cell(stage: str, s: int) -> float:
         "dot": 4 + 4 + 1,
         "dir": 4 + 4 + 1 + 4,
         "true": 4 * 4 + 1 + 4,
-        "down0": 4 + s + 1 + 4 + (1 + s) / 8.0,     # r, diag, label in; z out; coarse label in, coarse rhs out
-        "up0": 4 + 4 + s + 1 + 4 + s / 8.0,         # z, r, diag, label, coarse z in; z out
-        "dirspmv": 4 + 4 + 1 + 4 + 4 + 4,           # z, d, label, diag in; d', q out
+        "down0": 4 + 4 + 4 + (1 + s) / 8.0,         # r, diag (f32) in; z out; coarse label in, coarse rhs out
+        "up0": 4 + 4 + 4 + 4 + s / 8.0,             # pre-smoothed z, r, diag (f32), coarse z in; z out
+        "dirspmv": 4 + 4 + 4 + 4 + 4,               # z, d, diag in; d', q out (liquid = diag > 0)
     }.get(stage, 0.0)
 
 
-# DRAM bytes (read + write) per launch of a stage's kernel on the batched
-# workload (64 instances, fp16 levels, a first-iteration launch with every
-# instance iterating), from the committed ncu capture
-# profiles/marching_vcycle_batch64_fp16.md (cold-cache launches).
-NCU_TRAFFIC_BYTES = {"up0": 197.27e6, "down0": 134.00e6}
+# DRAM bytes (read + write) of one launch of a stage's kernel on the headline
+# batch when every one of the 64 instances iterates (the first CG iteration),
+# from the committed ncu capture of that launch (profiles/column_kernels_batch64_fp16.md,
+# cold cache).  The roofline scales it to the average launch of a solve by the
+# cells that launch processes (later launches skip finished instances).
+NCU_FIRST_LAUNCH_BYTES = {"down0": 150.08e6, "up0": 215.03e6, "dirspmv": 251.89e6}
 
 
 def peaks():
@@ -484,7 +485,11 @@ def main():
     hbm, peak_kind = peaks()
     achieved = alg / (per_launch_ms / 1000.0) / 1e9
     tot_prof = sum(v["ms"] for v in bprof.values())
-    traffic = NCU_TRAFFIC_BYTES.get(dom)
+    # traffic of the average launch: the first-iteration capture times the share
+    # of the batch's cells an average launch of the stage processes
+    first = NCU_FIRST_LAUNCH_BYTES.get(dom)
+    avg_cells = cell_iters / bprof[dom]["launches"]
+    traffic = first * avg_cells / (cells * 1.0) if first else None
     stage_gbs = {k: round(stage_bytes_per_cell(k, sbytes) * cell_iters / (v["ms"] / 1000.0) / 1e9, 1)
                  for k, v in stages.items()}
 
@@ -678,6 +683,9 @@ def main():
         "roofline": {"bound": "hbm", "kernel": dom, "workload": "the headline batch (64 instances per launch)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": peak_kind, "traffic": traffic, "alg_bytes_per_launch": alg,
+                     "traffic_note": "ncu DRAM bytes of the first-iteration launch (all 64 instances) scaled by "
+                                     "the cells of the average launch; alg_bytes_per_launch is that average launch",
+                     "first_launch_traffic": first, "first_launch_alg_bytes": stage_bytes_per_cell(dom, sbytes) * cells,
                      "launch_ms": per_launch_ms, "share_of_step": bprof[dom]["ms"] / tot_prof,
                      "stage_gbs": stage_gbs,
                      "stage_ms_per_step": {k: round(v["ms"] / prof_steps, 4) for k, v in sorted(bprof.items())

@@ -360,7 +360,7 @@ struct CDown {
 // per CTA.  On level 0 the residual is scaled by sigma and the smoother reads
 // the float32 diagonal (TD = float), on coarser levels the stored one.
 template <class TZ, class TR, class TD, class TS>
-__global__ void __launch_bounds__(kCDThreads, 2) k_cdown(const InstDev* insts, const Tile* tiles, int level) {
+__global__ void __launch_bounds__(kCDThreads, 3) k_cdown(const InstDev* insts, const Tile* tiles, int level) {
   using K = CDown<TZ, TR, TD, TS>;
   extern __shared__ __align__(16) unsigned char csm[];
   const Tile tl = tiles[blockIdx.x];
@@ -874,6 +874,125 @@ __global__ void __launch_bounds__(kSThreads, 2) k_cdirspmv(const InstDev* insts,
   for (int p = pa; p <= z1; p += 2) {
     step(p, std::integral_constant<int, 0>());
     if (p + 1 <= z1) step(p + 1, std::integral_constant<int, 1>());
+  }
+}
+
+// ================================================ float64 true residual (level 0)
+// r = b - A x in float64 from the double-single pressure x + xlo, written over
+// the CG residual, with ||r||^2 and max |r| (the acceptance check of
+// octree-pipelined-pcg.ts:501-541), on the tiles of k_cdirspmv: one cell per
+// thread marching its z chunk, the pressure of the in-plane neighbours staged
+// as doubles in a ring of three planes.  Each dot tile's partials fold in a
+// fixed order, and the instance's last tile to finish folds the dot tiles in
+// order and applies the acceptance rule.  Runs when the instance is a
+// candidate or on every true_every-th iteration.
+__global__ void __launch_bounds__(kSThreads, 2) k_ctrue(const InstDev* insts, const Tile* tiles) {
+  __shared__ double xs[3][kSThreads];
+  __shared__ double gsh[2 * 2 * 256];
+  __shared__ int flag;
+  const Tile tl = tiles[blockIdx.x];
+  const InstDev& I = insts[tl.inst];
+  Ctrl* c = I.ctrl;
+  if (c->done || !(c->candidate || (c->true_every > 0 && c->iter % c->true_every == 0))) return;
+  const LevelDev& L = I.lv[0];
+  const float* __restrict__ Xh = I.x;
+  const float* __restrict__ Xl = I.xlo;
+  const float* __restrict__ B = I.b;
+  const float* __restrict__ dgl = L.diag;
+  float* __restrict__ R = static_cast<float*>(L.rhs);
+  const int nx = L.nx, ny = L.ny, nz = L.nz, nxy = nx * ny;
+  const int ntx = (nx + kSX - 1) / kSX, nty = (ny + kSY - 1) / kSY;
+  const int tx = tl.tile % ntx, tr = tl.tile / ntx, ty = tr % nty, tz = tr / nty;
+  const int z0 = tz * L.cqz, z1 = min(z0 + L.cqz, nz);
+  const int t = threadIdx.x, lx = t % kSEX, ly = t / kSEX;
+  const int x = tx * kSX - 1 + lx, y = ty * kSY - 1 + ly;
+  const bool in = x >= 0 && y >= 0 && x < nx && y < ny;
+  const bool interior = lx >= 1 && lx <= kSX && ly >= 1 && ly <= kSY;
+  const bool out = in && interior;
+  const int col = in ? x + nx * y : 0;
+  const int lo = max(z0 - 1, 0), hi = min(z1, nz - 1);
+  // prefetch of planes p + 1 and p + 2: pressure (hi, lo), and for the
+  // operator's own cells b and the diagonal
+  float ph[2], pl[2], pb[2], pg[2];
+  auto fetch = [&](int p, int k) {
+    const bool v = in && p >= lo && p <= hi;
+    const int i = col + nxy * min(max(p, lo), hi);
+    ph[k] = v ? Xh[i] : 0.0f;
+    pl[k] = v ? Xl[i] : 0.0f;
+    const bool own = v && interior && p >= z0 && p < z1;
+    pb[k] = own ? B[i] : 0.0f;
+    pg[k] = own ? dgl[i] : 0.0f;
+  };
+  const int pa = z0 - 1;
+  fetch(pa, 0);
+  fetch(pa + 1, 1);
+  double xm2 = 0.0, xm1 = 0.0;   // pressure of planes p - 2, p - 1 in this column
+  float bm1 = 0.0f, gm1 = 0.0f;  // b and diagonal of plane p - 1
+  double rr = 0.0, mr = 0.0;
+  const int ntx0 = (nx + kTX - 1) / kTX, nty0 = (ny + kTY - 1) / kTY, nt0 = I.ntiles0;
+  double* partial = I.partial;
+  int s0 = 0;
+  auto step = [&](int p, auto K) {
+    constexpr int k = decltype(K)::value;
+    const double xp = double(ph[k]) + double(pl[k]);
+    const float bp = pb[k], gp = pg[k];
+    fetch(p + 2, k);
+    xs[s0][t] = xp;
+    __syncthreads();
+    const int r = p - 1;
+    if (r >= z0 && r < z1) {
+      const double* sp = xs[s0 == 0 ? 2 : s0 - 1];   // plane r
+      if (out && gm1 > 0.0f) {
+        const double nbs = ((sp[t - 1] + sp[t + 1]) + (xm2 + xp)) + (sp[t - kSEX] + sp[t + kSEX]);
+        const double rv = double(bm1) - (double(gm1) * xm1 - nbs);
+        R[col + nxy * r] = float(rv);
+        rr += rv * rv;
+        mr = fmax(mr, fabs(rv));
+      }
+      if ((r & 7) == 7 || r == nz - 1) {
+        if (interior) {
+          const int q = ((ly - 1) >> 3) * 256 + (lx - 1) + kSX * ((ly - 1) & 7);
+          gsh[q] = rr;
+          gsh[512 + q] = mr;
+        }
+        rr = 0.0;
+        mr = 0.0;
+        __syncthreads();
+        const int w = t >> 5, l = t & 31;
+        if (w < 4) {
+          const int dy = w & 1, m = w >> 1;   // warps 0, 1: sums; 2, 3: maxima
+          double v = 0.0;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const double e = gsh[m * 512 + dy * 256 + l + 32 * j];
+            v = m ? fmax(v, e) : v + e;
+          }
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            const double e = __shfl_xor_sync(0xffffffffu, v, o);
+            v = m ? fmax(v, e) : v + e;
+          }
+          const int tyd = 2 * ty + dy;
+          if (l == 0 && tyd < nty0) partial[m * nt0 + tx + ntx0 * (tyd + nty0 * (r >> 3))] = v;
+        }
+      }
+    }
+    xm2 = xm1;
+    xm1 = xp;
+    bm1 = bp;
+    gm1 = gp;
+    s0 = s0 == 2 ? 0 : s0 + 1;
+  };
+  for (int p = pa; p <= z1; p += 2) {
+    step(p, std::integral_constant<int, 0>());
+    if (p + 1 <= z1) step(p + 1, std::integral_constant<int, 1>());
+  }
+  // the instance's last tile folds the dot tiles in order
+  __shared__ double sh[32];
+  if (arrive_last(&c->arrive[kStTrue], cspmv_tiles(nx, ny, nz, L.cqz), &flag)) {
+    const double sum = gather_slot(partial, 0, nt0, 0, sh);
+    const double mx = gather_slot(partial, 1, nt0, 1, sh);
+    if (threadIdx.x == 0) finish_true(c, sum, mx);
   }
 }
 

@@ -384,7 +384,7 @@ void iter_launch(fluid_pp_batch* B, int pre, int post) {
     FPP_LAUNCH(B, kPrUpdate, k_update_part<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
     FPP_LAUNCH(B, kPrUpdate, k_update_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(B->d_insts,
                                                                                          il(B, B->multi)));
-    FPP_LAUNCH(B, kPrTrue, k_true_residual<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+    FPP_LAUNCH(B, kPrTrue, k_ctrue<<<B->cq.n, kSThreads, 0, s>>>(B->d_insts, tl(B, B->cq)));
     return;
   }
   vcycle_launch<T>(B, pre, post);
