@@ -996,6 +996,108 @@ __global__ void __launch_bounds__(kSThreads, 2) k_ctrue(const InstDev* insts, co
   }
 }
 
+// ==================================================== CG update (level 0)
+// x += alpha d (double-single), r -= alpha q, with the ||r||^2 and max |r|
+// partials of each dot tile (k_update_finish folds them in dot-tile order), on
+// the tiles of k_cdirspmv without their ring: one cell per thread, loads issued
+// two planes ahead.  Each warp holds one x row of a dot tile, so a dot tile's
+// partial folds its eight warps' shuffle trees in order.
+constexpr int kUThreads = kSX * kSY;   // 512
+__global__ void __launch_bounds__(kUThreads, 3) k_cupdate(const InstDev* insts, const Tile* tiles) {
+  __shared__ double wsh[2][kUThreads / 32];
+  const Tile tl = tiles[blockIdx.x];
+  const InstDev& I = insts[tl.inst];
+  Ctrl* c = I.ctrl;
+  if (c->done) return;
+  const LevelDev& L = I.lv[0];
+  const double alpha = c->alpha;
+  const float alpha_f = float(alpha);
+  float* __restrict__ X = I.x;
+  float* __restrict__ Xlo = I.xlo;
+  const float* __restrict__ D = dir_cur(I);
+  const float* __restrict__ Q = I.q;
+  float* __restrict__ R = static_cast<float*>(L.rhs);
+  const uint8_t* __restrict__ lab = L.label;
+  const int nx = L.nx, ny = L.ny, nz = L.nz, nxy = nx * ny;
+  const int ntx = (nx + kSX - 1) / kSX, nty = (ny + kSY - 1) / kSY;
+  const int tx = tl.tile % ntx, tr = tl.tile / ntx, ty = tr % nty, tz = tr / nty;
+  const int z0 = tz * L.cqz, z1 = min(z0 + L.cqz, nz);
+  const int t = threadIdx.x, lx = t % kSX, ly = t / kSX;
+  const int x = tx * kSX + lx, y = ty * kSY + ly;
+  const bool in = x < nx && y < ny;
+  const int col = in ? x + nx * y : 0;
+  float ph[2], pl[2], pd[2], pq[2], pr[2];
+  uint8_t pb[2];
+  auto fetch = [&](int p, int k) {
+    const bool v = in && p < z1;
+    const int i = col + nxy * min(p, z1 - 1);
+    pb[k] = v ? lab[i] : 0;
+    ph[k] = v ? X[i] : 0.0f;
+    pl[k] = v ? Xlo[i] : 0.0f;
+    pd[k] = v ? D[i] : 0.0f;
+    pq[k] = v ? Q[i] : 0.0f;
+    pr[k] = v ? R[i] : 0.0f;
+  };
+  fetch(z0, 0);
+  fetch(z0 + 1, 1);
+  double rr = 0.0, mr = 0.0;
+  const int ntx0 = (nx + kTX - 1) / kTX, nty0 = (ny + kTY - 1) / kTY, nt0 = I.ntiles0;
+  auto step = [&](int p, auto K) {
+    constexpr int k = decltype(K)::value;
+    const bool lq = pb[k] != 0;
+    const float h = ph[k], lo = pl[k], dv = pd[k], qv = pq[k], r0 = pr[k];
+    fetch(p + 2, k);
+    if (lq) {
+      const int i = col + nxy * p;
+      // double-single accumulation: x_hi + x_lo carries the pressure to ~1e-14
+      const double xv = double(h) + double(lo) + alpha * double(dv);
+      const float hi = float(xv);
+      X[i] = hi;
+      Xlo[i] = float(xv - double(hi));
+      const float rv = r0 - alpha_f * qv;
+      R[i] = rv;
+      rr += double(rv) * rv;
+      mr = fmax(mr, fabs(double(rv)));
+    }
+    // a dot tile ends every 8 planes and at the lattice top
+    if ((p & 7) == 7 || p == nz - 1) {
+      double a = rr, m = mr;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      }
+      const int w = t >> 5;
+      if ((t & 31) == 0) {
+        wsh[0][w] = a;
+        wsh[1][w] = m;
+      }
+      rr = 0.0;
+      mr = 0.0;
+      __syncthreads();
+      if (t < 2) {   // thread dy folds the eight rows of dot tile dy in order
+        double sa = 0.0, sm = 0.0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          sa += wsh[0][8 * t + j];
+          sm = fmax(sm, wsh[1][8 * t + j]);
+        }
+        const int tyd = 2 * ty + t;
+        if (tyd < nty0) {
+          const int ta = tx + ntx0 * (tyd + nty0 * (p >> 3));
+          I.partial[ta] = sa;
+          I.partial[nt0 + ta] = sm;
+        }
+      }
+      __syncthreads();
+    }
+  };
+  for (int p = z0; p < z1; p += 2) {
+    step(p, std::integral_constant<int, 0>());
+    if (p + 1 < z1) step(p + 1, std::integral_constant<int, 1>());
+  }
+}
+
 // delta of each listed instance from its k_cdirspmv partials in dot-tile
 // order, alpha = gamma / delta, and the direction buffers swap (one CTA each).
 __global__ void __launch_bounds__(kThreads) k_dirspmv_finish(const InstDev* insts, const int* ilist) {

@@ -381,7 +381,7 @@ void iter_launch(fluid_pp_batch* B, int pre, int post) {
     FPP_LAUNCH(B, kPrDirSpmv, k_cdirspmv<<<B->cq.n, kSThreads, 0, s>>>(B->d_insts, tl(B, B->cq)));
     FPP_LAUNCH(B, kPrDirSpmv, k_dirspmv_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(B->d_insts,
                                                                                            il(B, B->multi)));
-    FPP_LAUNCH(B, kPrUpdate, k_update_part<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+    FPP_LAUNCH(B, kPrUpdate, k_cupdate<<<B->cq.n, kUThreads, 0, s>>>(B->d_insts, tl(B, B->cq)));
     FPP_LAUNCH(B, kPrUpdate, k_update_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(B->d_insts,
                                                                                          il(B, B->multi)));
     FPP_LAUNCH(B, kPrTrue, k_ctrue<<<B->cq.n, kSThreads, 0, s>>>(B->d_insts, tl(B, B->cq)));
