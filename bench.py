@@ -73,7 +73,8 @@ def stage_bytes_per_cell(stage: str, s: int) -> float:
 # from the committed ncu capture of that launch (profiles/column_kernels_batch64_fp16.md,
 # cold cache).  The roofline scales it to the average launch of a solve by the
 # cells that launch processes (later launches skip finished instances).
-NCU_FIRST_LAUNCH_BYTES = {"down0": 150.08e6, "up0": 215.03e6, "dirspmv": 251.89e6}
+CYCLE_STEPS = 8
+NCU_FIRST_LAUNCH_BYTES = {"down0": 149.1e6, "up0": 214.4e6, "dirspmv": 250.8e6}
 
 
 def peaks():
@@ -438,18 +439,20 @@ def main():
     dev2 = [tuple(torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (s.vof, s.u, s.v, s.w)) for s in states]
     fp64_steps = list(range(0, nst, 5))
 
-    def run_single(precision, profile=False, keep=()):
+    def run_single(precision, profile=False, keep=(), o=None, nsteps=None):
+        o = opts if o is None else o
+        nsteps = steps2 if nsteps is None else nsteps
         pp = PressureProjector((s0.nx, s0.ny, s0.nz), s0.h, s0.rho, precision=precision, device=local)
         pp.set_stream(stream.cuda_stream)
         pp.set_profiling(profile)
         tt, rr, kept = [], [], {}
-        for k in range(args.warmup + steps2):
+        for k in range(args.warmup + nsteps):
             j = (k - args.warmup) % nst   # warm-up steps replay the last inputs
             st, d2 = states[j], dev2[j]
 
             def step():
                 pp.upload_state_device(*(t.data_ptr() for t in d2))
-                return pp.project(st.dt, **opts)
+                return pp.project(st.dt, **o)
             ms, rec = timed(step)
             if k >= args.warmup:
                 tt.append(ms)
@@ -468,6 +471,22 @@ def main():
     _, _, prof, _ = run_single(args.precision, profile=True)
     note("128x96x128 float64 oracle on every fifth step")
     fp64 = fp64_errors(states, fp64_steps, {"mixed": p2_mixed, "plain_fp32": p2_plain})
+
+    # preconditioner choice: one V-cycle under PCG (the default) against one
+    # full cycle under flexible CG, on the first CYCLE_STEPS inputs of the
+    # 128x96x128 sequence and on the headline batch
+    note("V-cycle vs full cycle")
+    cycles = {}
+    for cyc in ("v", "f"):
+        tt, rr, _, _ = run_single(args.precision, o=dict(opts, cycle=cyc), nsteps=CYCLE_STEPS)
+        tb, rb, _ = run_batched(args.precision, CYCLE_STEPS, tuning=tune.tuning, o=dict(tuned, cycle=cyc))
+        cycles[cyc] = {
+            "dam_spheres_128x96x128": {"solves_per_s": len(tt) / (sum(tt) / 1000.0),
+                                       "iterations_mean": statistics.mean(r["iterations"] for r in rr),
+                                       "failed_solves": sum(r["status_name"] != "OK" for r in rr)},
+            "batch64": {"solves_per_s": BATCH * len(tb) / (sum(tb) / 1000.0),
+                        "iterations_mean": statistics.mean(r["iterations"] for r in rb),
+                        "failed_solves": sum(r["status_name"] != "OK" for r in rb)}}
 
     # roofline of the headline: per-stage kernel events of the batched solve
     # (direct launches of the same 64 solves).  A launch of a level-0 stage
@@ -678,6 +697,10 @@ def main():
             "fp64_error": fp64,
             "stage_ms_per_solve": {k: round(v["ms"] / steps2, 4) for k, v in sorted(prof.items())},
         },
+        "preconditioner_cycles": {"steps": CYCLE_STEPS, "default": "v",
+                                  "v": cycles["v"], "f": cycles["f"],
+                                  "note": "v: one V-cycle under PCG (fused column kernels); f: one full cycle "
+                                          "under flexible CG (per-pass kernels); same inputs, same tolerance"},
         "tall_cell_256x256x1024": tall_line,
         "serving": serving,
         "roofline": {"bound": "hbm", "kernel": dom, "workload": "the headline batch (64 instances per launch)",

@@ -22,7 +22,7 @@ EXPORTS = (
     "fluid_pp_upload_state", "fluid_pp_upload_state_device", "fluid_pp_project", "fluid_pp_project_async",
     "fluid_pp_receipt_read", "fluid_pp_download", "fluid_pp_device_arrays", "fluid_pp_last_error",
     "fluid_pp_prepare", "fluid_pp_level_dims", "fluid_pp_get_level", "fluid_pp_get_rhs",
-    "fluid_pp_apply_operator", "fluid_pp_apply_vcycle", "fluid_pp_get_pressure_cells",
+    "fluid_pp_apply_operator", "fluid_pp_apply_vcycle", "fluid_pp_apply_fcycle", "fluid_pp_get_pressure_cells",
     "fluid_pp_batch_create", "fluid_pp_batch_destroy", "fluid_pp_batch_project",
     "fluid_pp_kernel_launches", "fluid_pp_set_profiling", "fluid_pp_profile_read",
     "fluid_pp_batch_set_profiling", "fluid_pp_batch_profile_read",
@@ -60,7 +60,7 @@ class SolveOpts(ctypes.Structure):
     _fields_ = [("rel_tol", ctypes.c_double), ("abs_tol", ctypes.c_double), ("max_iters", ctypes.c_int),
                 ("pre_sweeps", ctypes.c_int), ("post_sweeps", ctypes.c_int),
                 ("true_residual_every", ctypes.c_int), ("warm_start", ctypes.c_int),
-                ("rel_tol_inf", ctypes.c_double)]
+                ("rel_tol_inf", ctypes.c_double), ("cycle", ctypes.c_int)]
 
 
 class BatchTuning(ctypes.Structure):
@@ -117,6 +117,7 @@ def load():
     L.fluid_pp_get_rhs.argtypes = [vp, vp]
     L.fluid_pp_apply_operator.argtypes = [vp, vp, vp]
     L.fluid_pp_apply_vcycle.argtypes = [vp, vp, vp, ci, ci]
+    L.fluid_pp_apply_fcycle.argtypes = [vp, vp, vp, ci, ci, vp]
     L.fluid_pp_get_pressure_cells.argtypes = [vp, vp]
     L.fluid_pp_batch_create.argtypes = [ctypes.POINTER(vp), ci, ctypes.POINTER(vp)]
     L.fluid_pp_batch_destroy.argtypes = [vp]

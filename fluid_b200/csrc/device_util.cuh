@@ -328,9 +328,11 @@ __device__ __forceinline__ void set_sigma(Ctrl* c, double rr) {
 }
 
 // gamma = r . (z - zmean) from its three sums; beta from the previous gamma.
-// A non-positive or non-finite gamma ends the solve (the preconditioned system
-// lost definiteness).
-__device__ __forceinline__ void finish_gamma(Ctrl* c, double rz, double zsum, double rsum) {
+// With the full-cycle preconditioner (not symmetric) beta is flexible CG's
+// Polak-Ribiere form r_k+1 . (z_k+1 - z_k) / (r_k . z_k); rzp = r_k+1 . z_k
+// (raw, before the previous step's mean removal).  A non-positive or
+// non-finite gamma ends the solve (the preconditioned system lost definiteness).
+__device__ __forceinline__ void finish_gamma(Ctrl* c, double rz, double zsum, double rsum, double rzp = 0.0) {
   double gamma = rz;
   c->zmean = 0.0;
   if (!c->anchored) {
@@ -341,8 +343,10 @@ __device__ __forceinline__ void finish_gamma(Ctrl* c, double rz, double zsum, do
     c->done = 1;
     c->status = FLUID_PP_NONCONVERGENCE;
   } else {
-    c->beta = c->first ? 0.0 : gamma / c->gamma;
+    const double num = (c->fcg && !c->first) ? gamma - (rzp - c->zmean_prev * rsum) : gamma;
+    c->beta = c->first ? 0.0 : num / c->gamma;
     c->gamma = gamma;
+    c->zmean_prev = c->zmean;
     c->first = 0;
   }
 }

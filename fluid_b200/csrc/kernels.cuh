@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(kThreads) k_cg_init_part(const InstDev* insts,
 // nothing to solve.
 __global__ void __launch_bounds__(kThreads) k_cg_init_finish(const InstDev* insts, const int* ilist, double rel_tol,
                                                               double abs_tol, int max_iter, int true_every,
-                                                              double rel_tol_inf) {
+                                                              double rel_tol_inf, int fcg) {
   __shared__ double sh[32];
   const InstDev& I = insts[ilist[blockIdx.x]];
   Ctrl* c = I.ctrl;
@@ -348,6 +348,9 @@ __global__ void __launch_bounds__(kThreads) k_cg_init_finish(const InstDev* inst
     c->max_iter = max_iter;
     c->true_every = true_every;
     c->first = 1;
+    c->fcg = fcg;
+    c->zmean_prev = 0.0;
+    c->dsel = 0;
     c->candidate = 0;
     c->converged = 0;
     c->done = 0;
@@ -873,6 +876,7 @@ __global__ void k_coarse_apply(const InstDev* insts, const int* list) {
 // The current search direction (the fused path alternates two buffers).
 __device__ __forceinline__ float* dir_cur(const InstDev& I) { return I.ctrl->dsel ? I.d2 : I.d; }
 // gamma = r . (z - zmean) with float64 accumulation; beta from the previous gamma.
+template <bool FCG = false>
 __global__ void __launch_bounds__(kThreads) k_dot_rz(const InstDev* insts, const Tile* tiles, int ntiles) {
   __shared__ double sh[96];
   __shared__ int flag;
@@ -888,7 +892,8 @@ __global__ void __launch_bounds__(kThreads) k_dot_rz(const InstDev* insts, const
     const float* __restrict__ r = static_cast<const float*>(L.rhs);
     const float* __restrict__ z = static_cast<const float*>(L.z);
     const uint8_t* __restrict__ lab = L.label;
-    double rz = 0, zs = 0, rs = 0;
+    float* __restrict__ zprev = I.d2;   // flexible CG: the previous preconditioned residual (d2 is idle here)
+    double rz = 0, zs = 0, rs = 0, rzp = 0;
     const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
     for_column(it, L.nx, L.ny, L.nz, [&](int, int, int i) {
       if (!lab[i]) return;
@@ -896,18 +901,25 @@ __global__ void __launch_bounds__(kThreads) k_dot_rz(const InstDev* insts, const
       rz += rv * zv;
       zs += zv;
       rs += rv;
+      if (FCG) {
+        rzp += rv * double(zprev[i]);
+        zprev[i] = float(zv);
+      }
     });
     const double a0 = block_sum(rz, sh), a1 = block_sum(zs, sh), a2 = block_sum(rs, sh);
+    const double a3 = FCG ? block_sum(rzp, sh) : 0.0;
     if (threadIdx.x == 0) {
       partial[0 * nt0 + tl.tile] = a0;
       partial[1 * nt0 + tl.tile] = a1;
       partial[2 * nt0 + tl.tile] = a2;
+      if (FCG) partial[3 * nt0 + tl.tile] = a3;
     }
     if (arrive_last(&c->arrive[kStGamma], nt0, &flag)) {
       const double g = gather_slot(partial, 0, nt0, 0, sh);
       const double zsum = gather_slot(partial, 1, nt0, 0, sh);
       const double rsum = gather_slot(partial, 2, nt0, 0, sh);
-      if (threadIdx.x == 0) finish_gamma(c, g, zsum, rsum);
+      const double p = FCG ? gather_slot(partial, 3, nt0, 0, sh) : 0.0;
+      if (threadIdx.x == 0) finish_gamma(c, g, zsum, rsum, p);
     }
   }
 }

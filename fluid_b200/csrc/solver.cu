@@ -107,6 +107,7 @@ struct fluid_pp_batch {
   List l0single;             // level-0 tiles of single-level instances
   List bake;
   List multi, single;        // instance lists (offsets into d_ilist) by coarsest level
+  List fcb[kMaxLevels];      // multi-level instances for which level l is a grid level (full-cycle coarse steps)
   int maxL = 0;
   cudaError_t launch_err = cudaSuccess;   // first failed launch since the last check
   size_t smem_factor = 0;
@@ -252,7 +253,7 @@ void setup_launch(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
   FPP_LAUNCH(B, kPrInit, k_cg_init_part<<<g0, kThreads, 0, s>>>(B->d_insts, t0, n0, warm));
   FPP_LAUNCH(B, kPrInit, k_cg_init_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(
                              B->d_insts, il(B, B->multi), o.rel_tol, o.abs_tol, o.max_iters, o.true_residual_every,
-                             o.rel_tol_inf));
+                             o.rel_tol_inf, o.cycle == 1));
   FPP_LAUNCH(B, kPrInit, k_project_init<<<g0, kThreads, 0, s>>>(B->d_insts, t0, n0));
 }
 
@@ -268,19 +269,72 @@ void smooth_pass(fluid_pp_batch* B, int l, int colour, int zero_init) {
                k_smooth<T, T, T><<<g, kThreads, 0, B->stream>>>(B->d_insts, tl(B, Ls), Ls.n, l, colour, zero_init));
 }
 
+// One V-cycle from grid level `from` down to the coarse block and back
+// (vCycle, webgpu-uniform-pressure-multigrid.ts:524-538).  Level `from` starts
+// from zero, or from the z it holds when `keep` (the full cycle's prolongated
+// guess); every deeper level starts from zero.  `coarse` lists the instances
+// whose coarse block closes the cycle.
 template <class T>
-void vcycle_launch(fluid_pp_batch* B, int pre, int post) {
+void vcycle_from(fluid_pp_batch* B, int from, int pre, int post, bool keep, const List& coarse) {
   cudaStream_t s = B->stream;
-  for (int l = 0; l + 1 < B->maxL; ++l) {
+  for (int l = from; l + 1 < B->maxL; ++l) {
+    const List& Ls = B->lvl[l];
+    if (!Ls.n) continue;
+    const bool zero = !(keep && l == from);
+    for (int sw = 0; sw < pre; ++sw) {
+      smooth_pass<T>(B, l, 0, zero && sw == 0);
+      smooth_pass<T>(B, l, 1, 0);
+    }
+    if (pre == 0 && zero) smooth_pass<T>(B, l, 2, 1);   // z must start at zero
+    const List& Lr = B->rst[l];
+    if (l == 0)
+      FPP_LAUNCH(B, kPrRestrict0, k_residual_restrict<float, float, T, T><<<launch_grid(Lr.n), kThreads, 0, s>>>(
+                                      B->d_insts, tl(B, Lr), Lr.n, l));
+    else
+      FPP_LAUNCH(B, kPrRestrictC, k_residual_restrict<T, T, T, T><<<launch_grid(Lr.n), kThreads, 0, s>>>(
+                                      B->d_insts, tl(B, Lr), Lr.n, l));
+  }
+  if (coarse.n)
+    FPP_LAUNCH(B, kPrCoarse, k_coarse_block<T><<<coarse.n, kBlockThreads, B->smem_block, s>>>(
+                                 B->d_insts, il(B, coarse), pre, post));
+  if (from == 0 && B->single.n)
+    FPP_LAUNCH(B, kPrCoarse,
+               k_coarse_apply<float, float><<<B->single.n, kThreads, 0, s>>>(B->d_insts, il(B, B->single)));
+  for (int l = B->maxL - 2; l >= from; --l) {
     const List& Ls = B->lvl[l];
     if (!Ls.n) continue;
     const int g = launch_grid(Ls.n);
-    for (int sw = 0; sw < pre; ++sw) {
-      smooth_pass<T>(B, l, 0, sw == 0);
+    if (l == 0)
+      FPP_LAUNCH(B, kPrProlong0, k_prolong<float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l));
+    else
+      FPP_LAUNCH(B, kPrProlongC, k_prolong<T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l));
+    for (int sw = 0; sw < post; ++sw) {
       smooth_pass<T>(B, l, 1, 0);
+      smooth_pass<T>(B, l, 0, 0);
     }
-    if (pre == 0) smooth_pass<T>(B, l, 2, 1);   // z must start at zero
-    (void)g;
+  }
+}
+
+template <class T>
+void vcycle_launch(fluid_pp_batch* B, int pre, int post) {
+  vcycle_from<T>(B, 0, pre, post, false, B->multi);
+}
+
+// One full cycle z = F(r), zero initial guess (fullCycle,
+// webgpu-uniform-pressure-multigrid.ts:539-563): the residual restricted down
+// every grid level, the coarse block's V-cycle as the coarsest correction,
+// then for each grid level from the coarsest up, z_l = P z_{l+1} as the guess
+// of a V-cycle started at level l.  The levels inside the coarse block (at
+// most 4096 cells each) are not nested: the block's one V-cycle stands for
+// their full cycle.
+template <class T>
+void fcycle_launch(fluid_pp_batch* B, int pre, int post) {
+  cudaStream_t s = B->stream;
+  // descent: z = 0 on every grid level (so prolongation below assigns), the
+  // restricted right-hand side of each level is the residual of that zero guess
+  for (int l = 0; l + 1 < B->maxL; ++l) {
+    if (!B->lvl[l].n) continue;
+    smooth_pass<T>(B, l, 2, 1);
     const List& Lr = B->rst[l];
     if (l == 0)
       FPP_LAUNCH(B, kPrRestrict0, k_residual_restrict<float, float, T, T><<<launch_grid(Lr.n), kThreads, 0, s>>>(
@@ -303,10 +357,7 @@ void vcycle_launch(fluid_pp_batch* B, int pre, int post) {
       FPP_LAUNCH(B, kPrProlong0, k_prolong<float, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l));
     else
       FPP_LAUNCH(B, kPrProlongC, k_prolong<T, T><<<g, kThreads, 0, s>>>(B->d_insts, tl(B, Ls), Ls.n, l));
-    for (int sw = 0; sw < post; ++sw) {
-      smooth_pass<T>(B, l, 1, 0);
-      smooth_pass<T>(B, l, 0, 0);
-    }
+    vcycle_from<T>(B, l, pre, post, true, B->fcb[l]);
   }
 }
 
@@ -372,11 +423,16 @@ void vcycle_fused(fluid_pp_batch* B, int with_dot) {
 }
 
 template <class T>
-void iter_launch(fluid_pp_batch* B, int pre, int post) {
+void iter_launch(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
   cudaStream_t s = B->stream;
   const Tile* t0 = tl(B, B->l0);
   const int n0 = B->l0.n, g = launch_grid(n0);
-  if (pre == 1 && post == 1) {
+  const int pre = o.pre_sweeps, post = o.post_sweeps;
+  if (o.cycle == 1) {
+    // flexible CG: gamma also takes r . z_prev (z_prev kept in d2)
+    fcycle_launch<T>(B, pre, post);
+    FPP_LAUNCH(B, kPrDot, k_dot_rz<true><<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+  } else if (pre == 1 && post == 1) {
     vcycle_fused<T>(B, 1);
     FPP_LAUNCH(B, kPrDirSpmv, k_cdirspmv<<<B->cq.n, kSThreads, 0, s>>>(B->d_insts, tl(B, B->cq)));
     FPP_LAUNCH(B, kPrDirSpmv, k_dirspmv_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(B->d_insts,
@@ -386,9 +442,10 @@ void iter_launch(fluid_pp_batch* B, int pre, int post) {
                                                                                          il(B, B->multi)));
     FPP_LAUNCH(B, kPrTrue, k_ctrue<<<B->cq.n, kSThreads, 0, s>>>(B->d_insts, tl(B, B->cq)));
     return;
+  } else {
+    vcycle_launch<T>(B, pre, post);
+    FPP_LAUNCH(B, kPrDot, k_dot_rz<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
   }
-  vcycle_launch<T>(B, pre, post);
-  FPP_LAUNCH(B, kPrDot, k_dot_rz<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
   FPP_LAUNCH(B, kPrDir, k_dir<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
   FPP_LAUNCH(B, kPrSpmv, k_spmv<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
   FPP_LAUNCH(B, kPrUpdate, k_update<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
@@ -423,7 +480,7 @@ bool same_opts(const fluid_pp_solve_opts& a, const fluid_pp_solve_opts& b) {
   return a.rel_tol == b.rel_tol && a.abs_tol == b.abs_tol && a.max_iters == b.max_iters &&
          a.pre_sweeps == b.pre_sweeps && a.post_sweeps == b.post_sweeps &&
          a.true_residual_every == b.true_residual_every && a.warm_start == b.warm_start &&
-         a.rel_tol_inf == b.rel_tol_inf;
+         a.rel_tol_inf == b.rel_tol_inf && a.cycle == b.cycle;
 }
 
 // Captures the solve into three graphs: setup, a conditional WHILE node whose
@@ -472,7 +529,7 @@ int ensure_graphs(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
   if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     const unsigned long long c0 = g_launches.load();
-    iter_launch<T>(B, o.pre_sweeps, o.post_sweeps);
+    iter_launch<T>(B, o);
     const unsigned cap = unsigned(o.max_iters + 2);
     k_loop_cond<<<1, 256, 0, cs>>>(B->d_insts, n, B->d_loop, cap, handle);
     const cudaError_t le = cudaGetLastError();
@@ -775,6 +832,14 @@ static int batch_build(fluid_pp* const* handles, int count, const fluid_pp_batch
   for (int k = 0; k < count; ++k)
     if (B->h[k]->inst.nlev == 1) ilist.push_back(k);
   B->single.n = int(ilist.size()) - B->single.off;
+  for (int l = 0; l < B->maxL; ++l) {
+    B->fcb[l].off = int(ilist.size());
+    for (int k = 0; k < count; ++k) {
+      const InstDev& I = B->h[k]->inst;
+      if (I.nlev > 1 && l < I.first_block) ilist.push_back(k);
+    }
+    B->fcb[l].n = int(ilist.size()) - B->fcb[l].off;
+  }
   int mmax = 0;
   for (int k = 0; k < count; ++k) {
     mmax = std::max(mmax, B->h[k]->inst.coarse_m);
@@ -935,7 +1000,7 @@ static int batch_project_t(fluid_pp_batch* B, const float* dts, const fluid_pp_s
     const int cap = o.max_iters + 2;
     while (it < cap) {
       const int burst = std::min(check, cap - it);
-      for (int b = 0; b < burst; ++b) iter_launch<T>(B, o.pre_sweeps, o.post_sweeps);
+      for (int b = 0; b < burst; ++b) iter_launch<T>(B, o);
       it += burst;
       cudaMemcpyAsync(B->h_ctrl, B->d_ctrl, sizeof(Ctrl) * n, cudaMemcpyDeviceToHost, B->stream);
       cudaError_t e = take_launch_error(B);
@@ -1037,7 +1102,8 @@ static int parts_project(fluid_pp_batch* B, const float* dts, const fluid_pp_sol
 static int batch_project(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts* opts, bool sync,
                          fluid_pp_receipt* receipts) {
   const fluid_pp_solve_opts o = opts ? *opts : default_opts();
-  if (!(o.rel_tol >= 0) || !(o.abs_tol >= 0) || o.max_iters < 1 || o.pre_sweeps < 0 || o.post_sweeps < 0) {
+  if (!(o.rel_tol >= 0) || !(o.abs_tol >= 0) || o.max_iters < 1 || o.pre_sweeps < 0 || o.post_sweeps < 0 ||
+      o.cycle < 0 || o.cycle > 1) {
     B->err = "invalid solve options";
     return FLUID_PP_INVALID_ARG;
   }
@@ -1471,11 +1537,9 @@ int fluid_pp_apply_operator(fluid_pp* pp, const float* p, float* out) {
   return FLUID_PP_OK;
 }
 
-int fluid_pp_apply_vcycle(fluid_pp* pp, const float* r, float* z, int pre, int post) {
-  if (!pp || !r || !z || pre < 0 || post < 0) return FLUID_PP_INVALID_ARG;
-  cudaSetDevice(pp->cfg.device);
-  fluid_pp_batch* B = pp->self;
-  const long long N = pp->inst.lv[0].n;
+// The preconditioner input scale the solve would use for residual r: one over
+// the rms of its nonzero entries (keeps half-precision levels in range).
+static double hook_sigma(const float* r, long long N) {
   double ss = 0;
   long long cnt = 0;
   for (long long i = 0; i < N; ++i) {
@@ -1483,14 +1547,40 @@ int fluid_pp_apply_vcycle(fluid_pp* pp, const float* r, float* z, int pre, int p
     cnt += r[i] != 0.0f;
   }
   const double per = cnt ? ss / double(cnt) : 0.0;
-  const double sigma = per > 1e-300 ? 1.0 / std::sqrt(per) : 1.0;
+  return per > 1e-300 ? 1.0 / std::sqrt(per) : 1.0;
+}
+
+int fluid_pp_apply_vcycle(fluid_pp* pp, const float* r, float* z, int pre, int post) {
+  if (!pp || !r || !z || pre < 0 || post < 0) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(pp->cfg.device);
+  fluid_pp_batch* B = pp->self;
+  const long long N = pp->inst.lv[0].n;
   cudaMemcpyAsync(pp->inst.lv[0].rhs, r, 4 * N, cudaMemcpyHostToDevice, B->stream);
-  k_hook_ctrl<<<1, 1, 0, B->stream>>>(B->d_insts, sigma);
+  k_hook_ctrl<<<1, 1, 0, B->stream>>>(B->d_insts, hook_sigma(r, N));
   const bool fused = pre == 1 && post == 1;
   switch (B->precision) {
     case FLUID_PP_FP16: fused ? vcycle_fused<__half>(B, 0) : vcycle_launch<__half>(B, pre, post); break;
     case FLUID_PP_BF16: fused ? vcycle_fused<__nv_bfloat16>(B, 0) : vcycle_launch<__nv_bfloat16>(B, pre, post); break;
     default: fused ? vcycle_fused<float>(B, 0) : vcycle_launch<float>(B, pre, post);
+  }
+  cudaMemcpyAsync(z, pp->inst.lv[0].z, 4 * N, cudaMemcpyDeviceToHost, B->stream);
+  cudaError_t e = cudaStreamSynchronize(B->stream);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_apply_fcycle(fluid_pp* pp, const float* r, float* z, int pre, int post, int* first_block) {
+  if (!pp || !r || !z || pre < 0 || post < 0) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(pp->cfg.device);
+  fluid_pp_batch* B = pp->self;
+  const long long N = pp->inst.lv[0].n;
+  if (first_block) *first_block = pp->inst.nlev > 1 ? pp->inst.first_block : 0;
+  cudaMemcpyAsync(pp->inst.lv[0].rhs, r, 4 * N, cudaMemcpyHostToDevice, B->stream);
+  k_hook_ctrl<<<1, 1, 0, B->stream>>>(B->d_insts, hook_sigma(r, N));
+  switch (B->precision) {
+    case FLUID_PP_FP16: fcycle_launch<__half>(B, pre, post); break;
+    case FLUID_PP_BF16: fcycle_launch<__nv_bfloat16>(B, pre, post); break;
+    default: fcycle_launch<float>(B, pre, post);
   }
   cudaMemcpyAsync(z, pp->inst.lv[0].z, 4 * N, cudaMemcpyDeviceToHost, B->stream);
   cudaError_t e = cudaStreamSynchronize(B->stream);

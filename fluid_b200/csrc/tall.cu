@@ -1695,10 +1695,11 @@ int fluid_pp_tall_project_begin(fluid_pp_tall* T, float dt, const fluid_pp_solve
   if (!T) return FLUID_PP_INVALID_ARG;
   if (!(dt > 0) || !std::isfinite(dt)) return T->set_error(FLUID_PP_INVALID_ARG, "dt must be positive and finite");
   if (!T->has_state) return T->set_error(FLUID_PP_INVALID_ARG, "state not uploaded");
-  fluid_pp_solve_opts o{1e-6, 0.0, 200, 1, 1, 4, 0, 0.0};
+  fluid_pp_solve_opts o{1e-6, 0.0, 200, 1, 1, 4, 0, 0.0, 0};
   if (opts) o = *opts;
   if (!(o.rel_tol >= 0) || !(o.abs_tol >= 0) || o.max_iters < 1)
     return T->set_error(FLUID_PP_INVALID_ARG, "invalid solve options");
+  if (o.cycle != 0) return T->set_error(FLUID_PP_INVALID_ARG, "the tall grid solves with the V-cycle only (cycle 0)");
   cudaSetDevice(T->cfg.device);
   cudaStream_t s = T->stream;
   TInst& I = T->inst;
@@ -1878,10 +1879,11 @@ int fluid_pp_tall_solve_rhs(fluid_pp_tall* T, float dt, const float* b, const fl
   if (!T || !b || !x) return FLUID_PP_INVALID_ARG;
   if (!(dt > 0) || !std::isfinite(dt)) return T->set_error(FLUID_PP_INVALID_ARG, "dt must be positive and finite");
   if (!T->has_state) return T->set_error(FLUID_PP_INVALID_ARG, "state not uploaded");
-  fluid_pp_solve_opts o{1e-6, 0.0, 200, 1, 1, 4, 0, 0.0};
+  fluid_pp_solve_opts o{1e-6, 0.0, 200, 1, 1, 4, 0, 0.0, 0};
   if (opts) o = *opts;
   if (!(o.rel_tol >= 0) || !(o.abs_tol >= 0) || o.max_iters < 1)
     return T->set_error(FLUID_PP_INVALID_ARG, "invalid solve options");
+  if (o.cycle != 0) return T->set_error(FLUID_PP_INVALID_ARG, "the tall grid solves with the V-cycle only (cycle 0)");
   cudaSetDevice(T->cfg.device);
   cudaStream_t s = T->stream;
   TInst& I = T->inst;

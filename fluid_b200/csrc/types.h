@@ -31,6 +31,7 @@ struct Ctrl {
   double rmax;        // max |r| of the last residual (recursive or true)
   double thr_inf;     // max-norm threshold (0: criterion off)
   double red[kSlots]; // last finalised reduction values
+  double zmean_prev;  // zmean of the previous preconditioned residual (flexible CG)
   int iter;
   int max_iter;
   int true_every;
@@ -46,7 +47,7 @@ struct Ctrl {
   int converged;
   unsigned arrive[8]; // per-stage completion counters (self-resetting)
   int dsel;           // which of d / d2 holds the current search direction
-  int pad;
+  int fcg;            // 1: full-cycle preconditioner under flexible CG (Polak-Ribiere beta)
 };
 
 struct LevelDev {

@@ -69,10 +69,16 @@ def _read_profile(fn, handle, reset: bool) -> dict:
     return {name: {"ms": float(ms[k]), "launches": int(cnt[k])} for k, name in enumerate(_abi.STAGES) if cnt[k]}
 
 
+CYCLES = {"v": 0, "f": 1}
+
+
 def solve_opts(rel_tol=1e-6, abs_tol=0.0, max_iters=200, pre_sweeps=1, post_sweeps=1, true_residual_every=4,
-               warm_start=False, rel_tol_inf=0.0) -> SolveOpts:
+               warm_start=False, rel_tol_inf=0.0, cycle="v") -> SolveOpts:
+    """``cycle``: "v" one V-cycle under PCG, "f" one full cycle under flexible CG."""
+    if cycle not in CYCLES:
+        raise ValueError(f"cycle must be one of {sorted(CYCLES)}")
     return SolveOpts(rel_tol, abs_tol, max_iters, pre_sweeps, post_sweeps, true_residual_every, int(warm_start),
-                     rel_tol_inf)
+                     rel_tol_inf, CYCLES[cycle])
 
 
 class PressureProjector:
@@ -227,6 +233,14 @@ class PressureProjector:
         z = np.empty_like(r)
         _check(load().fluid_pp_apply_vcycle(self._h, ptr(r), ptr(z), int(pre), int(post)), self._h)
         return z
+
+    def apply_fcycle(self, r, pre: int = 1, post: int = 1):
+        """One full cycle z = F(r); returns (z, first block level)."""
+        r = np.ascontiguousarray(r, np.float32)
+        z = np.empty_like(r)
+        fb = ctypes.c_int(0)
+        _check(load().fluid_pp_apply_fcycle(self._h, ptr(r), ptr(z), int(pre), int(post), ctypes.byref(fb)), self._h)
+        return z, int(fb.value)
 
 
 def batch_tuning(fill_tiles=None, chunk_planes=None, box_shape=None, parts=None) -> BatchTuning:

@@ -80,6 +80,10 @@ typedef struct fluid_pp_solve_opts {
                               the previous step's projected velocity plus gravity) and CG stalls above 1e-6. */
   int warm_start;          /* 1: start from the previous pressure of this handle */
   double rel_tol_inf;      /* >0: also require max|b - A p| <= rel_tol_inf * max|b| (divergence in max norm) */
+  int cycle;               /* preconditioner: 0 (opts NULL) one V-cycle under PCG; 1 one full (F) cycle under
+                              flexible CG, beta = r_k+1 . (z_k+1 - z_k) / r_k . z_k (Polak-Ribiere), the
+                              schedule of the reference's fullCycle (webgpu-uniform-pressure-multigrid.ts:539-563).
+                              Uniform grid only; the tall grid rejects 1. */
 } fluid_pp_solve_opts;
 
 typedef struct fluid_pp_receipt {
@@ -168,6 +172,13 @@ int fluid_pp_get_level(fluid_pp* pp, int level, unsigned char* label, float* phi
 int fluid_pp_get_rhs(fluid_pp* pp, float* b);
 int fluid_pp_apply_operator(fluid_pp* pp, const float* p, float* out);  /* finest A, host in/out */
 int fluid_pp_apply_vcycle(fluid_pp* pp, const float* r, float* z, int pre, int post);
+/* One full (F) cycle z = F(r) with zero initial guess, the preconditioner of
+ * solve option cycle = 1: r restricted down every grid level, the levels from
+ * *first_block on (at most 4096 cells each, one CTA) solved by one V-cycle,
+ * then for each grid level from the coarsest up the prolongated correction is
+ * the initial guess of a V-cycle started at that level.  *first_block (may be
+ * NULL) receives that first block level (0 for a single-level hierarchy). */
+int fluid_pp_apply_fcycle(fluid_pp* pp, const float* r, float* z, int pre, int post, int* first_block);
 int fluid_pp_get_pressure_cells(fluid_pp* pp, float* x);             /* solution, finest-cell units */
 
 /* Batched projection of several handles in one set of launches per stage.

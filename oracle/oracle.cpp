@@ -472,12 +472,14 @@ struct VWork {
   std::vector<std::vector<double>> rhs, z, res;
 };
 
-void vcycle(const Ctx& c, VWork& wk, int l, int pre, int post) {
+// keep: level l starts from the z it holds (the full cycle's prolongated
+// guess, webgpu-uniform-pressure-multigrid.ts:560-561) instead of zero.
+void vcycle(const Ctx& c, VWork& wk, int l, int pre, int post, bool keep = false) {
   const Level& L = c.lv[l];
   double* z = wk.z[l].data();
   const double* rhs = wk.rhs[l].data();
   if (l == (int)c.lv.size() - 1) { solveCoarsest(c, rhs, z); return; }
-  std::fill(z, z + L.cells, 0.0);
+  if (!keep) std::fill(z, z + L.cells, 0.0);
   for (int s = 0; s < pre; ++s) { smooth(L, rhs, z, 0); smooth(L, rhs, z, 1); }
   double* res = wk.res[l].data();
   applyLevel(L, z, res, 1);
@@ -504,6 +506,27 @@ void precondition(const Ctx& c, VWork& wk, const double* r, double* z, int pre, 
   const Level& L0 = c.lv[0];
   std::copy(r, r + L0.cells, wk.rhs[0].begin());
   vcycle(c, wk, 0, pre, post);
+  std::copy(wk.z[0].begin(), wk.z[0].end(), z);
+  if (!L0.anchored) meanZero(L0, z);
+}
+
+// One full cycle with zero initial guess (fullCycle,
+// webgpu-uniform-pressure-multigrid.ts:539-563): r restricted down to level
+// fb, one V-cycle from fb (levels fb.. are not nested: they stand for the small
+// levels a device solves in one CTA), then for each level l = fb-1 .. 0 the
+// prolongated correction is the guess of a V-cycle from l.
+void fcycle(const Ctx& c, VWork& wk, const double* r, double* z, int pre, int post, int fb) {
+  const Level& L0 = c.lv[0];
+  const int last = (int)c.lv.size() - 1;
+  fb = std::max(0, std::min(fb, last));
+  std::copy(r, r + L0.cells, wk.rhs[0].begin());
+  for (int l = 0; l < fb; ++l) restrictRes(c.lv[l], c.lv[l + 1], wk.rhs[l].data(), wk.rhs[l + 1].data());
+  vcycle(c, wk, fb, pre, post);
+  for (int l = fb - 1; l >= 0; --l) {
+    std::fill(wk.z[l].begin(), wk.z[l].end(), 0.0);
+    prolongAdd(c.lv[l], c.lv[l + 1], wk.z[l + 1].data(), wk.z[l].data());
+    vcycle(c, wk, l, pre, post, true);
+  }
   std::copy(wk.z[0].begin(), wk.z[0].end(), z);
   if (!L0.anchored) meanZero(L0, z);
 }
@@ -624,6 +647,17 @@ void orc_vcycle(void* h, const double* r, double* z, int pre, int post) {
   precondition(c, wk, r, z, pre, post);
 }
 
+void orc_fcycle(void* h, const double* r, double* z, int pre, int post, int firstBlock) {
+  Ctx& c = *static_cast<Ctx*>(h);
+  VWork wk;
+  for (auto& L : c.lv) {
+    wk.rhs.emplace_back(L.cells, 0.0);
+    wk.z.emplace_back(L.cells, 0.0);
+    wk.res.emplace_back(L.cells, 0.0);
+  }
+  fcycle(c, wk, r, z, pre, post, firstBlock);
+}
+
 // info layout (doubles): 0 iterations, 1 converged, 2 recursive rel residual,
 // 3 true rel residual, 4 |b|_2, 5 reductions, 6 failure code (0 none,
 // 1 curvature, 2 max-iterations, 3 true-residual-validation), 7 liquid cells.
@@ -705,9 +739,12 @@ namespace {
 // accept only after an independent b - Ax check.  Failure codes: 1 lost
 // positivity/curvature, 2 maximum iterations, 3 true-residual validation.
 template <class ApplyA, class ApplyM>
+//
+// flexible: beta = r_k+1 . (z_k+1 - z_k) / r_k . z_k (Polak-Ribiere), for a
+// preconditioner that is not a fixed symmetric operator (the full cycle).
 int directCurvaturePCG(long N, ApplyA applyA, ApplyM applyM, const double* b, double* x, bool hasGuess,
-                       double relTol, double absTol, int maxIter, double* info, long liquid) {
-  std::vector<double> r(b, b + N), z(N), Az(N), d(N), Ad(N), tr(N);
+                       double relTol, double absTol, int maxIter, double* info, long liquid, bool flexible = false) {
+  std::vector<double> r(b, b + N), z(N), Az(N), d(N), Ad(N), tr(N), zOld;
   if (hasGuess) {
     applyA(x, tr.data());
     for (long i = 0; i < N; ++i) r[i] = b[i] - tr[i];
@@ -743,8 +780,10 @@ int directCurvaturePCG(long N, ApplyA applyA, ApplyM applyM, const double* b, do
   for (;;) {
     for (long i = 0; i < N; ++i) { x[i] += alpha * d[i]; r[i] -= alpha * Ad[i]; }
     ++it;
+    if (flexible) zOld = z;
     applyM(r.data(), z.data());
     const double gammaN = neumaierDot(r.data(), z.data(), N);
+    const double gammaOld = flexible ? neumaierDot(r.data(), zOld.data(), N) : 0.0;
     rr = neumaierDot(r.data(), r.data(), N);
     ++reductions;
     rec = std::sqrt(std::max(0.0, rr));
@@ -756,7 +795,7 @@ int directCurvaturePCG(long N, ApplyA applyA, ApplyM applyM, const double* b, do
     }
     if (!(gammaN > 0)) { fail = 1; break; }
     if (it >= maxIter) { fail = 2; break; }
-    const double beta = gammaN / gamma;
+    const double beta = (gammaN - gammaOld) / gamma;
     for (long i = 0; i < N; ++i) d[i] = z[i] + beta * d[i];
     applyA(d.data(), Ad.data());
     delta = neumaierDot(d.data(), Ad.data(), N);
@@ -792,6 +831,27 @@ int orc_solve_mgpcg(void* h, double relTol, double absTol, int maxIter, int pre,
   auto A = [&](const double* in, double* out) { applyLevel(L, in, out, 1); };
   auto M = [&](const double* in, double* out) { precondition(c, wk, in, out, pre, post); };
   return directCurvaturePCG(N, A, M, b.data(), x, false, relTol, absTol, maxIter, info, liquid);
+}
+
+// The full cycle (first block level firstBlock) under flexible PCG.
+int orc_solve_fcg(void* h, double relTol, double absTol, int maxIter, int pre, int post, int firstBlock, double* x,
+                  double* info) {
+  Ctx& c = *static_cast<Ctx*>(h);
+  const Level& L = c.lv[0];
+  const long N = L.cells;
+  VWork wk;
+  for (auto& Lv : c.lv) {
+    wk.rhs.emplace_back(Lv.cells, 0.0);
+    wk.z.emplace_back(Lv.cells, 0.0);
+    wk.res.emplace_back(Lv.cells, 0.0);
+  }
+  std::vector<double> b(c.b);
+  if (!L.anchored) meanZero(L, b.data());
+  long liquid = 0;
+  for (long i = 0; i < N; ++i) liquid += L.label[i];
+  auto A = [&](const double* in, double* out) { applyLevel(L, in, out, 1); };
+  auto M = [&](const double* in, double* out) { fcycle(c, wk, in, out, pre, post, firstBlock); };
+  return directCurvaturePCG(N, A, M, b.data(), x, false, relTol, absTol, maxIter, info, liquid, true);
 }
 
 // Dense-matrix form of the same recurrence for the reference's known-answer

@@ -47,6 +47,9 @@ def lib():
         L.orc_get_rhs.argtypes = [vp, vp, vp]
         L.orc_apply_level.argtypes = [vp, c_int, vp, vp]
         L.orc_vcycle.argtypes = [vp, vp, vp, c_int, c_int]
+        L.orc_fcycle.argtypes = [vp, vp, vp, c_int, c_int, c_int]
+        L.orc_solve_fcg.argtypes = [vp, c_double, c_double, c_int, c_int, c_int, c_int, vp, vp]
+        L.orc_solve_fcg.restype = c_int
         L.orc_solve_jacobi.argtypes = [vp, c_double, c_double, c_int, vp, vp]
         L.orc_solve_jacobi.restype = c_int
         L.orc_solve_mgpcg.argtypes = [vp, c_double, c_double, c_int, c_int, c_int, vp, vp]
@@ -168,6 +171,14 @@ class Oracle:
         lib().orc_vcycle(self._h, _p(r), _p(z), pre, post)
         return z
 
+    def fcycle(self, r, pre: int = 1, post: int = 1, first_block: int = 1):
+        """One full cycle from a zero guess; levels from `first_block` on take one V-cycle."""
+        nx, ny, nz = self.n
+        r = np.ascontiguousarray(r, np.float64).reshape(nz, ny, nx)
+        z = np.zeros_like(r)
+        lib().orc_fcycle(self._h, _p(r), _p(z), pre, post, int(first_block))
+        return z
+
     def solve_jacobi(self, rel_tol=1e-10, abs_tol=1e-12, max_iter=None):
         nx, ny, nz = self.n
         p = np.zeros((nz, ny, nx), np.float64)
@@ -182,6 +193,14 @@ class Oracle:
         p = np.zeros((nz, ny, nx), np.float64)
         info = np.zeros(8, np.float64)
         lib().orc_solve_mgpcg(self._h, rel_tol, abs_tol, int(max_iter), pre, post, _p(p), _p(info))
+        return p, dict(zip(INFO_KEYS, info.tolist()))
+
+    def solve_fcg(self, rel_tol=1e-10, abs_tol=0.0, max_iter=200, pre=1, post=1, first_block=1):
+        """Flexible PCG (Polak-Ribiere beta) with the full cycle as preconditioner."""
+        nx, ny, nz = self.n
+        p = np.zeros((nz, ny, nx), np.float64)
+        info = np.zeros(8, np.float64)
+        lib().orc_solve_fcg(self._h, rel_tol, abs_tol, int(max_iter), pre, post, int(first_block), _p(p), _p(info))
         return p, dict(zip(INFO_KEYS, info.tolist()))
 
     def grad_subtract(self, p):

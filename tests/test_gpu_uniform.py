@@ -80,6 +80,40 @@ def test_vcycle_matches_oracle_and_is_symmetric(name):
         assert abs(a - b) <= 1e-5 * np.sqrt(abs(np.dot(x.ravel(), zx.ravel()) * np.dot(y.ravel(), zy.ravel())))
 
 
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+@pytest.mark.parametrize("name", ["dam32", "odd37x50x29", "semi2x64x48", "open_top24"])
+def test_fcycle_matches_oracle(name, precision):
+    """One full cycle (cycle = 1's preconditioner) against the float64 full
+    cycle of the oracle with the same first block level."""
+    s = CASES[name]()
+    pp, o = _pair(s, precision)
+    pp.prepare(s.dt)
+    lab, _, _ = o.level(0)
+    x = (np.random.default_rng(8).normal(size=lab.shape) * lab).astype(np.float32)
+    tol = 2e-5 if precision == "fp32" else 3e-3
+    for pre in (1, 2):
+        z, fb = pp.apply_fcycle(x, pre, pre)
+        assert 1 <= fb < o.num_levels or (o.num_levels == 1 and fb == 0)
+        zo = o.fcycle(x.astype(np.float64), pre, pre, fb)
+        assert np.linalg.norm(z - zo) <= tol * np.linalg.norm(zo), (pre, fb)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16"])
+@pytest.mark.parametrize("name", ["dam32", "odd37x50x29", "open_top24", "semi2x64x48"])
+def test_project_full_cycle_matches_oracle(name, precision):
+    """The full cycle under flexible CG meets the same parity bars as the
+    V-cycle solve, in the iterations of the float64 flexible PCG (within one)."""
+    s = CASES[name]()
+    pp, o = _pair(s, precision)
+    rec = pp.project(s.dt, rel_tol=REL_RES, rel_tol_inf=0.5 * DIV_RATIO, cycle="f")
+    _check_projection(s, precision, rec, pp, o)
+    _, fb = pp.apply_fcycle(np.zeros(o.level(0)[0].shape, np.float32))
+    _, info = o.solve_fcg(REL_RES, 0.0, 300, 1, 1, fb)
+    assert info["converged"] == 1.0
+    if precision == "fp32":
+        assert abs(rec["iterations"] - info["iterations"]) <= 1, (rec["iterations"], info)
+
+
 def _check_projection(s, precision, rec, pp, o, p_ref=None):
     assert rec["status_name"] == "OK", rec
     assert rec["true_rel_residual"] <= REL_RES
@@ -358,6 +392,21 @@ def test_full_size_dam_spheres_matches_fp64_oracle(full_size_dam_spheres, precis
     assert rec["l2_div_after"] <= DIV_RATIO * rec["l2_div_before"], rec
     err = np.linalg.norm(pp.pressure_cells().astype(np.float64) - p_ref) / np.linalg.norm(p_ref)
     assert err <= REL_L2_PRESSURE, (precision, err)
+    pp.destroy()
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+def test_full_size_dam_spheres_full_cycle_matches_fp64_oracle(full_size_dam_spheres, precision):
+    """The full-cycle solve at 128x96x128 against the float64 solution, with
+    fewer iterations than the V-cycle solve of the same system."""
+    s, o, p_ref = full_size_dam_spheres
+    pp = PressureProjector((s.nx, s.ny, s.nz), s.h, s.rho, precision=precision)
+    pp.upload_state(s.vof, s.u, s.v, s.w)
+    rec_v = pp.project(s.dt, rel_tol=REL_RES, rel_tol_inf=0.5 * DIV_RATIO)
+    pp.upload_state(s.vof, s.u, s.v, s.w)
+    rec = pp.project(s.dt, rel_tol=REL_RES, rel_tol_inf=0.5 * DIV_RATIO, cycle="f")
+    _check_projection(s, precision, rec, pp, o, p_ref=p_ref)
+    assert rec["iterations"] < rec_v["iterations"], (rec["iterations"], rec_v["iterations"])
     pp.destroy()
 
 
