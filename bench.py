@@ -74,6 +74,8 @@ def stage_bytes_per_cell(stage: str, s: int) -> float:
 # cold cache).  The roofline scales it to the average launch of a solve by the
 # cells that launch processes (later launches skip finished instances).
 CYCLE_STEPS = 8
+SERVE_CELLS = 8e6     # resident uniform cells: the batched step stays near 8 ms
+SERVE_TALL = 2        # resident tall-cell simulations (they share the tall slices)
 NCU_FIRST_LAUNCH_BYTES = {"down0": 149.1e6, "up0": 214.4e6, "dirspmv": 250.8e6}
 
 
@@ -241,13 +243,12 @@ def fp64_errors(states, steps, results: dict) -> dict:
     return out
 
 
-def tall_fp64_error(tp, ts) -> dict:
-    """Relative L2 error of the last timed tall-cell pressure against the float64
+def tall_fp64_error(tp, ts, pressures: dict) -> dict:
+    """Relative L2 error of each timed tall-cell pressure against the float64
     solution of the oracle's independently assembled system (iterative
     refinement: float64 residuals with the oracle's operator, corrections from
-    the device solver); outside the timed region."""
+    the device solver `tp`); outside the timed region."""
     from oracle import tall as toracle
-    p_d = tp.pressure().ravel().astype(np.float64)
     A, b = toracle.assemble_fp64(ts.nx, ts.fine_ny, ts.nz, ts.band, ts.bases, ts.vof, ts.u, ts.v, ts.w)
     tp.upload_state(ts.vof, ts.u, ts.v, ts.w)
     x = np.zeros_like(b)
@@ -259,7 +260,9 @@ def tall_fp64_error(tp, ts) -> dict:
             break
         e, _ = tp.solve_rhs(ts.dt, r.astype(np.float32), rel_tol=1e-6)
         x += e.ravel().astype(np.float64)
-    return {"rel_l2": float(np.linalg.norm(p_d - x) / np.linalg.norm(x)), "oracle_rel_residual": rel,
+    out = {k: float(np.linalg.norm(p.ravel().astype(np.float64) - x) / np.linalg.norm(x))
+           for k, p in pressures.items()}
+    return {"rel_l2": out["plain_fp32"], "rel_l2_by_precision": out, "oracle_rel_residual": rel,
             "refinement_steps": steps,
             "oracle": "float64 tall-cell operator and rhs assembled by the CPU oracle from the dense faces; "
                       "solution by iterative refinement with device corrections"}
@@ -280,6 +283,8 @@ def main():
     ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16", "bf16"])
     ap.add_argument("--sweeps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=120.0,
+                    help="length of the serving stream (single GPU only; 0 skips it)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -516,21 +521,29 @@ def main():
     note("tall-cell waves")
     from fluid_b200.tall import TallProjector
     ts = configs.tall_waves()
-    tp = TallProjector(ts.nx, ts.nz, ts.fine_ny, ts.band, ts.bases, ts.h, ts.rho, device=local)
-    tp.set_stream(stream.cuda_stream)
     dev3 = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (ts.vof, ts.u, ts.v, ts.w)]
-    t3, r3 = [], None
     steps3 = max(3, min(args.steps, 20))
 
-    def tall_step():
-        tp.upload_state_device(*(t.data_ptr() for t in dev3))
-        return tp.project(ts.dt, rel_tol=1e-6)
-    for k in range(args.warmup + steps3):
-        ms, r3 = timed(tall_step)
-        if k >= args.warmup:
-            t3.append(ms)
+    def run_tall(precision):
+        tp_ = TallProjector(ts.nx, ts.nz, ts.fine_ny, ts.band, ts.bases, ts.h, ts.rho, precision=precision,
+                            device=local)
+        tp_.set_stream(stream.cuda_stream)
+        tt, rec_ = [], None
+
+        def tall_step():
+            tp_.upload_state_device(*(t.data_ptr() for t in dev3))
+            return tp_.project(ts.dt, rel_tol=1e-6)
+        for k in range(args.warmup + steps3):
+            ms, rec_ = timed(tall_step)
+            if k >= args.warmup:
+                tt.append(ms)
+        return tp_, tt, rec_
+    tp, t3, r3 = run_tall("fp32")
+    tpm, t3m, r3m = run_tall(args.precision)
+    p3m = tpm.pressure()
+    tpm.destroy()
     note("tall-cell float64 oracle")
-    tall_fp64 = tall_fp64_error(tp, ts)
+    tall_fp64 = tall_fp64_error(tp, ts, {"plain_fp32": tp.pressure(), "mixed": p3m})
     tp.destroy()
     tall_line = {
         "workload": ts.meta["workload"] + ", surface 600 + 8 seeded sinusoids (amplitude <= 12, wavelength 16-256)",
@@ -540,21 +553,32 @@ def main():
         "status": r3["status_name"], "true_rel_residual": r3["true_rel_residual"],
         "sample_iterations_per_s": ts.samples * r3["iterations"] * len(t3) / (sum(t3) / 1000.0),
         "precision": "f32 levels, f32 CG vectors, f64 dots/scalars/coarsest",
+        "mixed": {"precision": f"{args.precision} grid levels 1-2, f32 level 0 and block levels",
+                  "solves_per_s": len(t3m) / (sum(t3m) / 1000.0), "p50_ms": statistics.median(t3m),
+                  "iterations": r3m["iterations"], "status": r3m["status_name"],
+                  "true_rel_residual": r3m["true_rel_residual"]},
         "fp64_error": tall_fp64,
     }
 
     # ------------------------- serving: Poisson stream with continuous batching
-    note("serving stream")
-    from fluid_b200.serving import Server, serving_requests
-    serve_s = 10.0
-    reqs = serving_requests(rate=40.0, duration_s=serve_s, seed=5, templates=6)
-    srv = Server(budget_bytes=150e9, max_slots=16, precision=args.precision, device=local)
-    serving = srv.run(reqs, duration_s=serve_s)
-    srv.shutdown()
-    serving.update({"workload": f"Poisson arrivals at 40/s for {serve_s:.0f} s (first {serve_s:.0f} s of the "
-                                "120 s stream): 50/50 uniform grids (edges log-uniform 32-160, one 1.2M-cell shape) "
-                                "and tall-cell grids (64^2-256^2 columns, 24-40 band), 30-300 steps each",
-                    "budget_bytes": 150e9, "slots": 16})
+    serving = None
+    if world == 1 and args.serve_seconds > 0:
+        note(f"serving stream ({args.serve_seconds:.0f} s)")
+        from fluid_b200.serving import Server, serving_requests
+        serve_s = float(args.serve_seconds)
+        reqs = serving_requests(rate=40.0, duration_s=serve_s, seed=5)
+        srv = Server(budget_bytes=150e9, precision=args.precision, device=local, max_resident_cells=SERVE_CELLS,
+                     max_tall=SERVE_TALL)
+        serving = srv.run(reqs, duration_s=serve_s)
+        srv.shutdown()
+        serving.update({
+            "workload": f"Poisson arrivals at 40/s for {serve_s:.0f} s: 50/50 uniform grids (edges log-uniform "
+                        "32-160 per axis, drawn per request) and tall-cell grids (64^2-256^2 columns, 24-40 band, "
+                        "256 rows, drawn per request), 30-300 steps each, each from its own seeded initial state",
+            "budget_bytes": 150e9, "max_resident_uniform_cells": SERVE_CELLS, "max_resident_tall": SERVE_TALL,
+            "note": "admission: HBM budget (hard) and the step-latency budget (resident uniform cells, resident "
+                    "tall simulations); the offered load (about 6600 step-solves/s, half of them tall) exceeds one "
+                    "GPU, so requests queue: queue delay is reported beside step latency"})
 
     # ------------------------------------------- e2e: public API from host buffers
     note("e2e from host buffers")

@@ -57,6 +57,24 @@ constexpr int kTB = 256;          // threads per CTA
 constexpr int kTGrid = 148 * 8;   // grid cap (grid-stride beyond)
 constexpr double kFix = 4294967296.0;   // 2^32: restriction fixed point
 
+// Level vectors (z, rhs, res) are float on level 0 (the CG vectors) and on the
+// block levels, and the handle's storage type S (float, half or bfloat16) on
+// the grid levels 1 .. first block - 1.  Arithmetic is float: a read view
+// converts on load, stores round once.
+template <class S>
+struct VecView {
+  const S* p;
+  __device__ __forceinline__ float operator[](long long k) const { return tof(p[k]); }
+};
+template <class S>
+__device__ __forceinline__ VecView<S> view(const float* p) {
+  return VecView<S>{reinterpret_cast<const S*>(p)};
+}
+template <class S>
+__device__ __forceinline__ S* stor(float* p) {
+  return reinterpret_cast<S*>(p);
+}
+
 struct TLevel {
   int nx, nz, fine_ny, band, P;
   int n;        // samples
@@ -467,7 +485,8 @@ __device__ __forceinline__ double tall_off(const TLevel& L, int col, int j, cons
 
 // tall_off for both tall rows of column col (rows 2 col and 2 col + 1 are
 // adjacent in every slot: one 8-byte load per slot for the pair).
-__device__ __forceinline__ void tall_off_pair(const TLevel& L, int col, const float* v, double& o0, double& o1) {
+template <class VP>
+__device__ __forceinline__ void tall_off_pair(const TLevel& L, int col, VP v, double& o0, double& o1) {
   const float2* tv = reinterpret_cast<const float2*>(L.tval);
   const int2* ti = reinterpret_cast<const int2*>(L.tidx);
   double s0 = 0.0, s1 = 0.0;
@@ -538,7 +557,8 @@ __device__ __forceinline__ void band_col(const TLevel& L, int col, BandCol& c) {
 // The off-diagonal operands of band row jb (own sample k): per lateral
 // neighbour its band sample, or its tall pair, or nothing (0); then the
 // sample below (the tall cell's top sample for jb = 0: also k - nx) and above.
-__device__ __forceinline__ void band_row_loads(const TLevel& L, const BandCol& c, int jb, int k, const float* v,
+template <class VP>
+__device__ __forceinline__ void band_row_loads(const TLevel& L, const BandCol& c, int jb, int k, VP v,
                                                float (&vv)[10]) {
 #pragma unroll
   for (int d = 0; d < 4; ++d) {
@@ -582,8 +602,8 @@ __host__ __device__ inline long long apply_items(int ncol, int band, int G) {
 }
 
 // (A v)_k of both tall rows of column col: out(k, liquid, Av, v_k).
-template <class Out>
-__device__ __forceinline__ void tall_pair_apply(const TLevel& L, int col, const float* v, Out out) {
+template <class VP, class Out>
+__device__ __forceinline__ void tall_pair_apply(const TLevel& L, int col, VP v, Out out) {
   const int z = int(divq(unsigned(col), L.mnx)), x = col - z * L.nx;
   const int s0 = sidx(L, x, 0, z), s1 = s0 + L.nx;
   const bool l0 = L.label[s0] != 0, l1 = L.label[s1] != 0;
@@ -608,8 +628,8 @@ __device__ __forceinline__ void tall_pair_apply(const TLevel& L, int col, const 
 // liquid, Av, v_k, e) for each row inside the band (inactive rows above the
 // fine grid as not liquid), e = extra(k) loaded with the row's operands.  v
 // must be 0 on every sample that is not liquid.
-template <int G, class Extra, class Out>
-__device__ __forceinline__ void band_rows_apply(const TLevel& L, int it, const float* v, Extra extra, Out out) {
+template <int G, class VP, class Extra, class Out>
+__device__ __forceinline__ void band_rows_apply(const TLevel& L, int it, VP v, Extra extra, Out out) {
   const int g = int(divq(unsigned(it), L.mnc));
   BandCol c;
   band_col(L, it - g * L.ncol, c);
@@ -914,13 +934,28 @@ __global__ void k_tall_true(TInst* I) {
   if (reduce_grid<2>(I, 4, v, mx, o) && threadIdx.x == 0) finish_true(I->ctrl, o[0], o[1]);
 }
 
+// Loop condition of the iteration graph: one more iteration while the solve
+// is not done and fewer than loop[1] iterations have run.
+__global__ void k_tall_loop_cond(const TInst* I, unsigned* loop, cudaGraphConditionalHandle handle) {
+  const unsigned c = loop[0] + 1;
+  loop[0] = c;
+  cudaGraphSetConditional(handle, (!I->ctrl->done && c < loop[1]) ? 1u : 0u);
+}
+
+__global__ void k_tall_loop_reset(unsigned* loop, unsigned cap) {
+  loop[0] = 0u;
+  loop[1] = cap;
+}
+
 // ------------------------------------------------------------------ V-cycle
 // Each V-cycle stage is a device function over the samples t0, t0 + ts, ...;
 // the grid kernels call it with the grid's threads, the single-CTA block for
 // the small levels (k_tall_vblock) with the CTA's.
+template <class S>
 __device__ __forceinline__ void tv_zero(TInst* I, int l, int t0, int ts) {
   const TLevel& L = I->lv[l];
-  for (int k = t0; k < L.n; k += ts) L.z[k] = 0.0f;
+  S* z = stor<S>(L.z);
+  for (int k = t0; k < L.n; k += ts) z[k] = fromf<S>(0.0f);
 }
 
 // Band colour sweeps run over work items of G consecutive band rows of one
@@ -933,10 +968,12 @@ __device__ __forceinline__ void tv_zero(TInst* I, int l, int t0, int ts) {
 constexpr int kBandGroup = 4;
 constexpr int kBlockBandGroup = 2;
 
-template <int G>
+template <int G, class S>
 __device__ __forceinline__ void tv_smooth_band(TInst* I, int l, int colour, int t0, int ts) {
   static_assert(G % 2 == 0, "a band row group holds both colours");
   const TLevel& L = I->lv[l];
+  const VecView<S> Z = view<S>(L.z), Rh = view<S>(L.rhs);
+  S* zw = stor<S>(L.z);
   constexpr int R = G / 2;
   const int items = ((L.band + G - 1) / G) * L.ncol;
   for (int it = t0; it < items; it += ts) {
@@ -955,9 +992,9 @@ __device__ __forceinline__ void tv_smooth_band(TInst* I, int l, int colour, int 
       rh[r] = dg[r] = 0.0f;
       if (act[r]) {
         liq[r] = L.label[k] != 0;
-        rh[r] = L.rhs[k];
+        rh[r] = Rh[k];
         dg[r] = L.diag[k];
-        band_row_loads(L, c, jb, k, L.z, vv[r]);
+        band_row_loads(L, c, jb, k, Z, vv[r]);
       }
     }
 #pragma unroll
@@ -965,7 +1002,7 @@ __device__ __forceinline__ void tv_smooth_band(TInst* I, int l, int colour, int 
       if (!act[r]) continue;
       const int jb = jb0 + 2 * r;
       const int k = sidx(L, c.x, jb + 2, c.z);
-      L.z[k] = liq[r] ? (rh[r] - band_row_off(L, c, jb, vv[r])) / dg[r] : 0.0f;
+      zw[k] = fromf<S>(liq[r] ? (rh[r] - band_row_off(L, c, jb, vv[r])) / dg[r] : 0.0f);
     }
   }
 }
@@ -973,49 +1010,53 @@ __device__ __forceinline__ void tv_smooth_band(TInst* I, int l, int colour, int 
 // One colour of the block Gauss-Seidel sweep: 0/1 band cells with (x + y + z)
 // even/odd (items of G band rows), 2/3 tall blocks of columns with (x + z)
 // even/odd.
-template <int G>
+template <int G, class S>
 __device__ __forceinline__ void tv_smooth(TInst* I, int l, int colour, int t0, int ts) {
   const TLevel& L = I->lv[l];
   if (colour < 2) {
-    tv_smooth_band<G>(I, l, colour, t0, ts);
+    tv_smooth_band<G, S>(I, l, colour, t0, ts);
   } else {
+    const VecView<S> Z = view<S>(L.z), Rh = view<S>(L.rhs);
+    S* zw = stor<S>(L.z);
     for (int c = t0; c < L.ncol; c += ts) {
       const int z = int(divq(unsigned(c), L.mnx)), x = c - z * L.nx;
       if (((x + z) & 1) != colour - 2) continue;
       const int s0 = sidx(L, x, 0, z), s1 = sidx(L, x, 1, z);
       if (!L.label[s0]) {
-        L.z[s0] = L.z[s1] = 0.0f;
+        zw[s0] = zw[s1] = fromf<S>(0.0f);
         continue;
       }
       double o0, o1;
-      tall_off_pair(L, c, L.z, o0, o1);
-      const double r0 = double(L.rhs[s0]) - o0;
-      const double r1 = double(L.rhs[s1]) - o1;
+      tall_off_pair(L, c, Z, o0, o1);
+      const double r0 = double(Rh[s0]) - o0;
+      const double r1 = double(Rh[s1]) - o1;
       const double a00 = L.diag[s0], a11 = L.diag[s1], a01 = L.a01[c];
       const double det = a00 * a11 - a01 * a01;
-      L.z[s0] = float((a11 * r0 - a01 * r1) / det);
-      L.z[s1] = float((a00 * r1 - a01 * r0) / det);
+      zw[s0] = fromf<S>(float((a11 * r0 - a01 * r1) / det));
+      zw[s1] = fromf<S>(float((a00 * r1 - a01 * r0) / det));
     }
   }
 }
 
 // res = scale (rhs - A z); level 0 scales by sigma.  Work items as in the
 // operator apply, G band rows each.
-template <int G>
+template <int G, class S>
 __device__ __forceinline__ void tv_residual(TInst* I, int l, int t0, int ts) {
   const TLevel& L = I->lv[l];
   const double scale = l == 0 ? I->ctrl->sigma : 1.0;
+  const VecView<S> Z = view<S>(L.z), Rh = view<S>(L.rhs);
+  S* res = stor<S>(L.res);
   const long long items = apply_items(L.ncol, L.band, G);
   for (long long it = t0; it < items; it += ts) {
     if (it < L.ncol) {
-      tall_pair_apply(L, int(it), L.z, [&](int k, bool liq, double av, float) {
-        L.res[k] = liq ? float(scale * (double(L.rhs[k]) - av)) : 0.0f;
+      tall_pair_apply(L, int(it), Z, [&](int k, bool liq, double av, float) {
+        res[k] = fromf<S>(liq ? float(scale * (double(Rh[k]) - av)) : 0.0f);
       });
     } else {
-      band_rows_apply<G>(L, int(it - L.ncol), L.z, [&](int k) { return L.rhs[k]; },
-                                [&](int k, bool liq, float av, float, float rhs) {
-                                  L.res[k] = liq ? float(scale * double(rhs - av)) : 0.0f;
-                                });
+      band_rows_apply<G>(L, int(it - L.ncol), Z, [&](int k) { return Rh[k]; },
+                         [&](int k, bool liq, float av, float, float rhs) {
+                           res[k] = fromf<S>(liq ? float(scale * double(rhs - av)) : 0.0f);
+                         });
     }
   }
 }
@@ -1028,15 +1069,17 @@ __device__ __forceinline__ void tv_residual(TInst* I, int l, int t0, int ts) {
 // coarse dense cells around it (taps2: a dropped tap has weight 0); a coarse
 // tall cell passes its share to the column's two samples (1 - t, t), a coarse
 // band cell to its sample, air cells take nothing.
+template <class SF>
 __device__ __forceinline__ void tv_restrict(TInst* I, int l, int t0, int ts) {
   const TLevel& F = I->lv[l];
   const TLevel& C = I->lv[l + 1];
+  const VecView<SF> Res = view<SF>(F.res);
   constexpr float kFixF = 4294967296.0f;
   for (int k = t0; k < F.n; k += ts) {
     int x, j, z;
     decode(F, k, x, j, z);
     const bool liq = F.label[k] != 0;   // the three loads issue together
-    const float r = F.res[k];
+    const float r = Res[k];
     const int b = F.bases[x + F.nx * z];
     if (!liq || r == 0.0f) continue;
     int cx[2], cy[2], cz[2];
@@ -1079,11 +1122,13 @@ __device__ __forceinline__ void tv_restrict(TInst* I, int l, int t0, int ts) {
   }
 }
 
+template <class SC>
 __device__ __forceinline__ void tv_restrict_finish(TInst* I, int l, int t0, int ts) {
   const TLevel& C = I->lv[l];
+  SC* rhs = stor<SC>(C.rhs);
   for (int k = t0; k < C.n; k += ts) {
     const long long a = (long long)C.acc[k];
-    C.rhs[k] = C.label[k] ? float(double(a) / kFix) : 0.0f;
+    rhs[k] = fromf<SC>(C.label[k] ? float(double(a) / kFix) : 0.0f);
     C.acc[k] = 0ull;
   }
 }
@@ -1091,15 +1136,19 @@ __device__ __forceinline__ void tv_restrict_finish(TInst* I, int l, int t0, int 
 // z_f += P z_c on liquid fine samples (the taps of tv_restrict, a coarse tall
 // cell interpolating its column's two samples); into level 0 the sigma scale
 // is undone.
+template <class SF, class SC>
 __device__ __forceinline__ void tv_prolong(TInst* I, int l, int t0, int ts) {
   const TLevel& F = I->lv[l];
   const TLevel& C = I->lv[l + 1];
+  const VecView<SF> Zf = view<SF>(F.z);
+  const VecView<SC> Zc = view<SC>(C.z);
+  SF* zw = stor<SF>(F.z);
   const float unscale = l == 0 ? float(1.0 / I->ctrl->sigma) : 1.0f;
   for (int k = t0; k < F.n; k += ts) {
     int x, j, z;
     decode(F, k, x, j, z);
     const bool liq = F.label[k] != 0;   // the three loads issue together
-    const float zf = F.z[k];
+    const float zf = Zf[k];
     const int b = F.bases[x + F.nx * z];
     if (!liq) continue;
     int cx[2], cy[2], cz[2];
@@ -1126,13 +1175,13 @@ __device__ __forceinline__ void tv_prolong(TInst* I, int l, int t0, int ts) {
           float val = 0.0f;
           if (Y < B) {
             const float t = float(Y) * __frcp_rn(float(B - 1));
-            val = (1.0f - t) * C.z[s0] + t * C.z[s0 + C.nx];
+            val = (1.0f - t) * Zc[s0] + t * Zc[s0 + C.nx];
           } else if (Y < B + C.band) {
-            val = C.z[s0 + C.nx * (Y - B + 2)];
+            val = Zc[s0 + C.nx * (Y - B + 2)];
           }
           s = fmaf(w, val, s);
         }
-    F.z[k] = fmaf(s, unscale, zf);
+    zw[k] = fromf<SF>(fmaf(s, unscale, zf));
   }
 }
 
@@ -1149,19 +1198,22 @@ __device__ __forceinline__ void tv_coarse_apply(TInst* I) {
   }
 }
 
-#define TALL_GRID_KERNEL(name, call)                                                        \
+#define TALL_GRID_KERNEL(name, tparams, call)                                               \
+  template <tparams>                                                                         \
   __global__ void name(TInst* I, int l, int arg) {                                           \
     if (I->ctrl->done) return;                                                               \
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x, ts = gridDim.x * blockDim.x;      \
     (void)arg;                                                                               \
     call;                                                                                    \
   }
-TALL_GRID_KERNEL(k_tall_zero, tv_zero(I, l, t0, ts))
-TALL_GRID_KERNEL(k_tall_smooth, tv_smooth<kBandGroup>(I, l, arg, t0, ts))
-TALL_GRID_KERNEL(k_tall_residual, tv_residual<kApplyGroup>(I, l, t0, ts))
-TALL_GRID_KERNEL(k_tall_restrict, tv_restrict(I, l, t0, ts))
-TALL_GRID_KERNEL(k_tall_restrict_finish, tv_restrict_finish(I, l, t0, ts))
-TALL_GRID_KERNEL(k_tall_prolong, tv_prolong(I, l, t0, ts))
+#define TALL_COMMA ,
+TALL_GRID_KERNEL(k_tall_zero, class S, tv_zero<S>(I, l, t0, ts))
+TALL_GRID_KERNEL(k_tall_smooth, class S, (tv_smooth<kBandGroup, S>(I, l, arg, t0, ts)))
+TALL_GRID_KERNEL(k_tall_residual, class S, (tv_residual<kApplyGroup, S>(I, l, t0, ts)))
+TALL_GRID_KERNEL(k_tall_restrict, class S, tv_restrict<S>(I, l, t0, ts))
+TALL_GRID_KERNEL(k_tall_restrict_finish, class S, tv_restrict_finish<S>(I, l, t0, ts))
+TALL_GRID_KERNEL(k_tall_prolong, class SF TALL_COMMA class SC, (tv_prolong<SF, SC>(I, l, t0, ts)))
+#undef TALL_COMMA
 #undef TALL_GRID_KERNEL
 
 __global__ void k_tall_coarse_apply(TInst* I) {
@@ -1254,26 +1306,26 @@ __global__ void __launch_bounds__(1024) k_tall_vblock(TInst* I, int first, int o
     W = &SI;
   }
   for (int l = first; l < last; ++l) {
-    tv_zero(W, l, t0, ts);
+    tv_zero<float>(W, l, t0, ts);
     __syncthreads();
     for (int c = 0; c < 4; ++c) {
-      tv_smooth<kBlockBandGroup>(W, l, c, t0, ts);
+      tv_smooth<kBlockBandGroup, float>(W, l, c, t0, ts);
       __syncthreads();
     }
-    tv_residual<1>(W, l, t0, ts);
+    tv_residual<1, float>(W, l, t0, ts);
     __syncthreads();
-    tv_restrict(W, l, t0, ts);
+    tv_restrict<float>(W, l, t0, ts);
     __syncthreads();
-    tv_restrict_finish(W, l + 1, t0, ts);
+    tv_restrict_finish<float>(W, l + 1, t0, ts);
     __syncthreads();
   }
   tv_coarse_apply(W);
   __syncthreads();
   for (int l = last - 1; l >= first; --l) {
-    tv_prolong(W, l, t0, ts);
+    tv_prolong<float, float>(W, l, t0, ts);
     __syncthreads();
     for (int c = 3; c >= 0; --c) {
-      tv_smooth<kBlockBandGroup>(W, l, c, t0, ts);
+      tv_smooth<kBlockBandGroup, float>(W, l, c, t0, ts);
       __syncthreads();
     }
   }
@@ -1376,6 +1428,14 @@ struct fluid_pp_tall {
   bool solving = false;   // between fluid_pp_tall_project_begin and _end
   bool solved = false;    // the CG loop reported done
   int it = 0, cap = 0;    // CG iterations launched, iteration cap (+2 slack)
+  // CUDA graphs of the CG iteration, captured once per handle (the launches
+  // depend only on the hierarchy): x_body is one iteration (the sliced solve
+  // replays it), x_loop a conditional WHILE node around it that ends on the
+  // device when the solve is done or after d_loop[1] iterations.
+  cudaGraph_t g_body = nullptr, g_loop = nullptr;
+  cudaGraphExec_t x_body = nullptr, x_loop = nullptr;
+  unsigned* d_loop = nullptr;   // [0] iterations run, [1] iteration cap
+  bool graphs_tried = false;
   int set_error(int code, const std::string& m) {
     err = m;
     return code;
@@ -1435,29 +1495,141 @@ int tall_first_block(const TallPlan& plan) {
   return L - 1;
 }
 
-void launch_vcycle(fluid_pp_tall* T, int first) {
+// The V-cycle's launches: grid levels 0 .. first - 1 (level 0 in float,
+// levels 1 .. first - 1 in the storage type S), then the block levels in one
+// CTA, then back up.
+template <class S>
+void launch_vcycle_t(fluid_pp_tall* T, int first) {
   TInst& I = T->inst;
   cudaStream_t s = T->stream;
+  TInst* D = T->d_inst;
+  // grid level l's vectors are float on level 0, S above it; the block levels are float
+  auto zero = [&](int l, int g) {
+    if (l == 0) k_tall_zero<float><<<g, kTB, 0, s>>>(D, l, 0);
+    else k_tall_zero<S><<<g, kTB, 0, s>>>(D, l, 0);
+  };
+  auto smooth = [&](int l, int g, int colour) {
+    if (l == 0) k_tall_smooth<float><<<g, kTB, 0, s>>>(D, l, colour);
+    else k_tall_smooth<S><<<g, kTB, 0, s>>>(D, l, colour);
+  };
   for (int l = 0; l < first; ++l) {
     const int g = grid_for(I.lv[l].n), gc = grid_for(I.lv[l].ncol), gb = grid_band(I.lv[l]);
-    k_tall_zero<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
-    k_tall_smooth<<<gb, kTB, 0, s>>>(T->d_inst, l, 0);
-    k_tall_smooth<<<gb, kTB, 0, s>>>(T->d_inst, l, 1);
-    k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 2);
-    k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 3);
-    k_tall_residual<<<grid_for(apply_items(I.lv[l].ncol, I.lv[l].band, kApplyGroup)), kTB, 0, s>>>(T->d_inst, l, 0);
-    k_tall_restrict<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
-    k_tall_restrict_finish<<<grid_for(I.lv[l + 1].n), kTB, 0, s>>>(T->d_inst, l + 1, 0);
+    const int gr = grid_for(apply_items(I.lv[l].ncol, I.lv[l].band, kApplyGroup));
+    const int gf = grid_for(I.lv[l + 1].n);
+    zero(l, g);
+    smooth(l, gb, 0);
+    smooth(l, gb, 1);
+    smooth(l, gc, 2);
+    smooth(l, gc, 3);
+    if (l == 0) {
+      k_tall_residual<float><<<gr, kTB, 0, s>>>(D, l, 0);
+      k_tall_restrict<float><<<g, kTB, 0, s>>>(D, l, 0);
+    } else {
+      k_tall_residual<S><<<gr, kTB, 0, s>>>(D, l, 0);
+      k_tall_restrict<S><<<g, kTB, 0, s>>>(D, l, 0);
+    }
+    if (l + 1 < first) k_tall_restrict_finish<S><<<gf, kTB, 0, s>>>(D, l + 1, 0);
+    else k_tall_restrict_finish<float><<<gf, kTB, 0, s>>>(D, l + 1, 0);
   }
   const size_t sm = vblock_smem_bytes(I, first);
-  k_tall_vblock<<<1, 1024, sm, s>>>(T->d_inst, first, sm > 0 ? 1 : 0);
+  k_tall_vblock<<<1, 1024, sm, s>>>(D, first, sm > 0 ? 1 : 0);
   for (int l = first - 1; l >= 0; --l) {
     const int g = grid_for(I.lv[l].n), gc = grid_for(I.lv[l].ncol), gb = grid_band(I.lv[l]);
-    k_tall_prolong<<<g, kTB, 0, s>>>(T->d_inst, l, 0);
-    k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 3);
-    k_tall_smooth<<<gc, kTB, 0, s>>>(T->d_inst, l, 2);
-    k_tall_smooth<<<gb, kTB, 0, s>>>(T->d_inst, l, 1);
-    k_tall_smooth<<<gb, kTB, 0, s>>>(T->d_inst, l, 0);
+    const bool fine_s = l > 0, coarse_s = l + 1 < first;
+    if (!fine_s && !coarse_s) k_tall_prolong<float, float><<<g, kTB, 0, s>>>(D, l, 0);
+    else if (!fine_s) k_tall_prolong<float, S><<<g, kTB, 0, s>>>(D, l, 0);
+    else if (!coarse_s) k_tall_prolong<S, float><<<g, kTB, 0, s>>>(D, l, 0);
+    else k_tall_prolong<S, S><<<g, kTB, 0, s>>>(D, l, 0);
+    smooth(l, gc, 3);
+    smooth(l, gc, 2);
+    smooth(l, gb, 1);
+    smooth(l, gb, 0);
+  }
+}
+
+void launch_vcycle(fluid_pp_tall* T, int first) {
+  switch (T->cfg.precision) {
+    case FLUID_PP_FP16: launch_vcycle_t<__half>(T, first); break;
+    case FLUID_PP_BF16: launch_vcycle_t<__nv_bfloat16>(T, first); break;
+    default: launch_vcycle_t<float>(T, first);
+  }
+}
+
+// One CG iteration on the handle's stream: the V-cycle (or the dense coarsest
+// apply of a single-level hierarchy), gamma, direction, A d, update, float64
+// true residual.
+void launch_iteration(fluid_pp_tall* T) {
+  TInst& I = T->inst;
+  cudaStream_t s = T->stream;
+  const int g0 = grid_for(I.lv[0].n);
+  if (I.nlev > 1) {
+    launch_vcycle(T, tall_first_block(T->plan));
+  } else {
+    k_tall_coarse_apply<<<1, 1024, 0, s>>>(T->d_inst);
+  }
+  k_tall_dot<<<g0, kTB, 0, s>>>(T->d_inst);
+  k_tall_dir<<<g0, kTB, 0, s>>>(T->d_inst);
+  k_tall_spmv<<<g0, kTB, 0, s>>>(T->d_inst);
+  k_tall_update<<<g0, kTB, 0, s>>>(T->d_inst);
+  k_tall_true<<<g0, kTB, 0, s>>>(T->d_inst);
+}
+
+void destroy_tall_graphs(fluid_pp_tall* T) {
+  for (cudaGraphExec_t* x : {&T->x_body, &T->x_loop})
+    if (*x) {
+      cudaGraphExecDestroy(*x);
+      *x = nullptr;
+    }
+  for (cudaGraph_t* g : {&T->g_body, &T->g_loop})
+    if (*g) {
+      cudaGraphDestroy(*g);
+      *g = nullptr;
+    }
+}
+
+// Captures the iteration graphs once; on any failure the handle keeps direct
+// launches (same kernels, same order, same bits).
+void ensure_tall_graphs(fluid_pp_tall* T) {
+  if (T->graphs_tried) return;
+  T->graphs_tried = true;
+  cudaStream_t cs = nullptr;
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  cudaStream_t saved = T->stream;
+  T->stream = cs;
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    launch_iteration(T);
+    e = cudaStreamEndCapture(cs, &T->g_body);
+  }
+  cudaGraphConditionalHandle handle{};
+  cudaGraph_t body = nullptr;
+  if (e == cudaSuccess) e = cudaGraphCreate(&T->g_loop, 0);
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, T->g_loop, 1, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess) {
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+    p.conditional.handle = handle;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, T->g_loop, nullptr, 0, &p);
+    if (e == cudaSuccess) body = p.conditional.phGraph_out[0];
+  }
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    launch_iteration(T);
+    k_tall_loop_cond<<<1, 1, 0, cs>>>(T->d_inst, T->d_loop, handle);
+    e = cudaStreamEndCapture(cs, &body);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&T->x_body, T->g_body, 0);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&T->x_loop, T->g_loop, 0);
+  T->stream = saved;
+  cudaStreamDestroy(cs);
+  if (e != cudaSuccess) {
+    destroy_tall_graphs(T);
+    cudaGetLastError();
   }
 }
 
@@ -1511,9 +1683,9 @@ size_t tall_arena_size(const TallPlan& plan) {
 
 int tall_create(const fluid_pp_tall_config* cfg, const int* bases, fluid_pp_tall** out) {
   if (!cfg || !bases || !out) return FLUID_PP_INVALID_ARG;
-  if (cfg->precision != FLUID_PP_FP32) {
-    fpp::set_global_error("the tall-cell solver stores its levels in float32 only");
-    return FLUID_PP_UNSUPPORTED;
+  if (cfg->precision != FLUID_PP_FP32 && cfg->precision != FLUID_PP_FP16 && cfg->precision != FLUID_PP_BF16) {
+    fpp::set_global_error("unknown precision");
+    return FLUID_PP_INVALID_ARG;
   }
   TallPlan plan = plan_tall(cfg->nx, cfg->nz, cfg->fine_ny, cfg->band, bases);
   if (!plan.ok) {
@@ -1594,11 +1766,13 @@ int tall_create(const fluid_pp_tall_config* cfg, const int* bases, fluid_pp_tall
   I.err = static_cast<int*>(take(sizeof(int)));
   cudaError_t e = dev_alloc(reinterpret_cast<void**>(&T->d_inst), sizeof(TInst));
   if (e == cudaSuccess) e = host_alloc(reinterpret_cast<void**>(&T->h_ctrl), sizeof(Ctrl));
+  if (e == cudaSuccess) e = dev_alloc(reinterpret_cast<void**>(&T->d_loop), 2 * sizeof(unsigned));
   if (e == cudaSuccess) e = configure_tall_kernels();
   if (e != cudaSuccess) {
     fpp::set_global_error(std::string("tall setup: ") + cudaGetErrorString(e));
     dev_release(T->d_inst, T->stream);
     host_release(T->h_ctrl, T->stream);
+    dev_release(T->d_loop, T->stream);
     dev_release(T->arena, T->stream);
     return FLUID_PP_OOM;
   }
@@ -1647,8 +1821,10 @@ int fluid_pp_tall_create(const fluid_pp_tall_config* config, const int* bases, f
 void fluid_pp_tall_destroy(fluid_pp_tall* T) {
   if (!T) return;
   cudaSetDevice(T->cfg.device);
+  destroy_tall_graphs(T);
   dev_release(T->d_inst, T->stream);
   host_release(T->h_ctrl, T->stream);
+  dev_release(T->d_loop, T->stream);
   dev_release(T->arena, T->stream);
   delete T;
 }
@@ -1722,21 +1898,15 @@ int fluid_pp_tall_project_continue(fluid_pp_tall* T, int max_iterations, int* fi
   cudaSetDevice(T->cfg.device);
   cudaStream_t s = T->stream;
   TInst& I = T->inst;
-  const int g0 = grid_for(I.lv[0].n);
   int budget = max_iterations > 0 ? max_iterations : T->cap;
+  ensure_tall_graphs(T);
   while (!T->solved && T->it < T->cap && budget > 0) {
     const int burst = std::min({4, T->cap - T->it, budget});
     for (int k = 0; k < burst; ++k) {
-      if (I.nlev > 1) {
-        launch_vcycle(T, tall_first_block(T->plan));
-      } else {
-        k_tall_coarse_apply<<<1, 1024, 0, s>>>(T->d_inst);
-      }
-      k_tall_dot<<<g0, kTB, 0, s>>>(T->d_inst);
-      k_tall_dir<<<g0, kTB, 0, s>>>(T->d_inst);
-      k_tall_spmv<<<g0, kTB, 0, s>>>(T->d_inst);
-      k_tall_update<<<g0, kTB, 0, s>>>(T->d_inst);
-      k_tall_true<<<g0, kTB, 0, s>>>(T->d_inst);
+      if (T->x_body)
+        cudaGraphLaunch(T->x_body, s);
+      else
+        launch_iteration(T);
     }
     T->it += burst;
     budget -= burst;
@@ -1793,6 +1963,14 @@ int fluid_pp_tall_project_end(fluid_pp_tall* T, fluid_pp_receipt* receipt) {
 int fluid_pp_tall_project(fluid_pp_tall* T, float dt, const fluid_pp_solve_opts* opts, fluid_pp_receipt* receipt) {
   int rc = fluid_pp_tall_project_begin(T, dt, opts);
   if (rc != FLUID_PP_OK) return rc;
+  ensure_tall_graphs(T);
+  if (T->x_loop) {
+    // the whole CG loop as one graph launch; it ends on the device
+    k_tall_loop_reset<<<1, 1, 0, T->stream>>>(T->d_loop, unsigned(T->cap));
+    cudaGraphLaunch(T->x_loop, T->stream);
+    T->it = T->cap;
+    return fluid_pp_tall_project_end(T, receipt);
+  }
   int finished = 0;
   rc = fluid_pp_tall_project_continue(T, 0, &finished);
   if (rc != FLUID_PP_OK) return rc;

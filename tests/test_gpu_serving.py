@@ -68,6 +68,26 @@ def test_poisson_stream_short():
     assert stats["p99_step_ms"] is not None and stats["solves_per_s"] > 0
 
 
+def test_per_request_shapes_and_latency_budgets():
+    """Requests with their own seeded shapes, built by the background thread;
+    admission keeps the resident uniform cells and tall simulations inside the
+    latency budgets (one request alone may exceed the cell budget), and every
+    admitted request reports its queue delay."""
+    reqs = serving_requests(rate=30.0, duration_s=1.0, seed=9, steps=(3, 6), uniform_edge=(24, 56),
+                            tall_side=(16, 40), tall_band=(24, 32), tall_rows=96)
+    assert all(r.states is None for r in reqs)
+    cap = 150_000
+    srv = Server(max_resident_cells=cap, max_tall=1)
+    stats = srv.run(reqs)
+    srv.shutdown()
+    assert stats["requests_finished"] == len(reqs) == stats["requests_admitted"]
+    assert stats["failed_steps"] == 0
+    biggest = max(r.meta["cells"] for r in reqs if r.kind == "uniform")
+    assert stats["peak_resident_uniform_cells"] <= max(cap, biggest)
+    assert stats["peak_resident_tall"] <= 1
+    assert stats["p99_queue_delay_ms"] is not None and stats["p50_queue_delay_ms"] <= stats["p99_queue_delay_ms"]
+
+
 def test_allocation_cache_carves_and_returns_reserved_memory():
     """Handles are carved from a reserved slab, give their ranges back on destroy,
     and a solve on reused memory is bit-identical to the first."""

@@ -117,13 +117,29 @@ def test_tall_full_size_labels_rhs_operator(full_size_tall):
     tp.destroy()
 
 
-def test_tall_full_size_matches_fp64(full_size_tall):
-    """The 2.23M-sample projection against the float64 solution of the oracle's
-    independently assembled system: receipts at the 1e-6 operating point,
-    divergence over represented band cells reduced by 1e-4, and at the parity
-    tolerance pressure rel-L2 <= 1e-5."""
+@pytest.fixture(scope="module")
+def full_size_tall_solution(full_size_tall):
+    """The float64 solution of the full-size system (iterative refinement with
+    float32-level device corrections), certified by its float64 residual."""
     s, A, b = full_size_tall
     tp = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho)
+    tp.upload_state(s.vof, s.u, s.v, s.w)
+    x, rel = fp64_solution(tp, s, A, b)
+    tp.destroy()
+    assert rel <= 1e-12, rel
+    return x
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16"])
+def test_tall_full_size_matches_fp64(full_size_tall, full_size_tall_solution, precision):
+    """The 2.23M-sample projection with every level storage type against the
+    float64 solution of the oracle's independently assembled system: receipts
+    at the 1e-6 operating point, divergence over represented band cells
+    reduced by 1e-4, and at the parity tolerance pressure rel-L2 <= 1e-5.
+    Levels 1-2 are grid levels here, so fp16 / bf16 change their storage."""
+    s, A, b = full_size_tall
+    x = full_size_tall_solution
+    tp = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho, precision=precision)
     tp.upload_state(s.vof, s.u, s.v, s.w)
     rec = tp.project(s.dt, rel_tol=REL_RES)
     assert rec["status_name"] == "OK", rec
@@ -134,21 +150,22 @@ def test_tall_full_size_matches_fp64(full_size_tall):
     rec = tp.project(s.dt, rel_tol=REL_RES_PARITY)
     assert rec["status_name"] == "OK", rec
     p_d = tp.pressure().ravel().astype(np.float64)
-    tp.upload_state(s.vof, s.u, s.v, s.w)
-    x, rel = fp64_solution(tp, s, A, b)
-    assert rel <= 1e-12, rel
     err = np.linalg.norm(p_d - x) / np.linalg.norm(x)
-    assert err <= REL_L2_PRESSURE, err
+    assert err <= REL_L2_PRESSURE, (precision, err)
     tp.destroy()
 
 
-def test_tall_sliced_projection_matches_one_call():
-    """begin + continue in slices of 3 iterations + end gives the one-call result bit for bit."""
-    s = configs.tall_waves(20, 20, 96, 24, seed=2, mean=50, amp_max=4, lam=(8, 32))
-    a = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho)
+@pytest.mark.parametrize("shape,precision", [((20, 20, 96, 24), "fp32"), ((64, 64, 128, 16), "fp16")])
+def test_tall_sliced_projection_matches_one_call(shape, precision):
+    """begin + continue in slices of 3 iterations + end (the one-iteration graph
+    replayed) gives the one-call result (the whole loop as one graph) bit for
+    bit; the 64^2 case has grid level 1 in fp16."""
+    nx, nz, fny, band = shape
+    s = configs.tall_waves(nx, nz, fny, band, seed=2, mean=fny // 2, amp_max=4, lam=(8, 32))
+    a = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho, precision=precision)
     a.upload_state(s.vof, s.u, s.v, s.w)
     ra = a.project(s.dt, rel_tol=1e-6)
-    b = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho)
+    b = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho, precision=precision)
     b.upload_state(s.vof, s.u, s.v, s.w)
     b.project_begin(s.dt, rel_tol=1e-6)
     slices = 1
