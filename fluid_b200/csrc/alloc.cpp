@@ -200,6 +200,21 @@ int current_device() {
 
 namespace fpp {
 
+cudaError_t order_streams(cudaStream_t prev, cudaStream_t next) {
+  if (prev == next) return cudaSuccess;
+  cudaEvent_t ev;
+  cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  if (e != cudaSuccess) return e;
+  e = cudaEventRecord(ev, prev);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(next, ev, 0);
+  cudaEventDestroy(ev);   // released once the wait has been satisfied
+  return e;
+}
+
+}  // namespace fpp
+
+namespace fpp {
+
 cudaError_t dev_alloc(void** p, size_t bytes) { return alloc_key(current_device(), p, bytes); }
 void dev_release(void* p, cudaStream_t last_use) { release_key(p, last_use); }
 cudaError_t host_alloc(void** p, size_t bytes) { return alloc_key(kHostKey, p, bytes); }

@@ -26,4 +26,9 @@ void dev_release(void* p, cudaStream_t last_use);
 cudaError_t host_alloc(void** p, size_t bytes);
 void host_release(void* p, cudaStream_t last_use);
 
+// Orders `next` after the work already issued to `prev` (an event recorded on
+// prev that next waits for), so a handle moved to another stream never runs
+// beside its own earlier work.  No-op when the two are the same stream.
+cudaError_t order_streams(cudaStream_t prev, cudaStream_t next);
+
 }  // namespace fpp

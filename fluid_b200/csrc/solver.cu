@@ -1366,7 +1366,11 @@ void fluid_pp_destroy(fluid_pp* pp) {
 
 int fluid_pp_set_stream(fluid_pp* pp, void* stream) {
   if (!pp) return FLUID_PP_INVALID_ARG;
-  pp->stream = static_cast<cudaStream_t>(stream);
+  cudaSetDevice(pp->cfg.device);
+  const cudaStream_t next = static_cast<cudaStream_t>(stream);
+  const cudaError_t e = order_streams(pp->stream, next);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  pp->stream = next;
   if (pp->self) pp->self->stream = pp->stream;
   return FLUID_PP_OK;
 }

@@ -1831,7 +1831,11 @@ void fluid_pp_tall_destroy(fluid_pp_tall* T) {
 
 int fluid_pp_tall_set_stream(fluid_pp_tall* T, void* stream) {
   if (!T) return FLUID_PP_INVALID_ARG;
-  T->stream = static_cast<cudaStream_t>(stream);
+  cudaSetDevice(T->cfg.device);
+  const cudaStream_t next = static_cast<cudaStream_t>(stream);
+  const cudaError_t e = fpp::order_streams(T->stream, next);
+  if (e != cudaSuccess) return T->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  T->stream = next;
   return FLUID_PP_OK;
 }
 
