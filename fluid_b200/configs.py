@@ -329,3 +329,71 @@ def tall_waves(nx: int = 256, nz: int = 256, fine_ny: int = 1024, band: int = 32
         arr[fluid] = rng.normal(0.0, sigma, size=int(fluid.sum())).astype(np.float32)
     return TallState(nx, nz, fine_ny, band, bases, 1.0 / nx, 1.0 / 60.0, vof, u, v, w,
                      meta={"workload": f"tall waves {nx}x{nz} columns, {fine_ny} rows, band {band}", "seed": seed})
+
+
+@dataclass
+class SolidScene:
+    """A uniform-grid state with embedded solids: cell open fractions and the
+    MAC faces' dual-cell open fractions and solid normal velocities."""
+    state: GridState
+    open: np.ndarray
+    fx: np.ndarray
+    fy: np.ndarray
+    fz: np.ndarray
+    usx: np.ndarray
+    usy: np.ndarray
+    usz: np.ndarray
+
+    def solids(self):
+        return self.open, self.fx, self.fy, self.fz, self.usx, self.usy, self.usz
+
+
+def _solid_samples(points, ramp, sphere):
+    """(solid, sphere) flags of sample points [..., 3] (x, y, z in cell units):
+    terrain below y = ramp[0] + ramp[1] * x, and a ball (centre, radius)."""
+    x, y, z = points[..., 0], points[..., 1], points[..., 2]
+    terrain = y < ramp[0] + ramp[1] * x
+    c, r = sphere
+    ball = (x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2 < r * r
+    return terrain | ball, ball & ~terrain
+
+
+def solid_scene(nx: int = 48, ny: int = 40, nz: int = 44, seed: int = 3, sphere_velocity=(0.0, -0.5, 0.0),
+                open_top: bool = False) -> SolidScene:
+    """A dam break over a sloped terrain around a (moving) ball obstacle.
+
+    Open fractions are measured the reference's way (pressureFaceData,
+    webgpu-uniform-reference.wgsl.ts:530-556): a face's dual cell by 8 samples
+    at +-0.4 cell around the face centre, a cell by 8 samples at +-0.25 cell.
+    The liquid fills the open part of the dam block (vof = block fraction x open
+    fraction).  The solids' face velocity is the ball's velocity on faces whose
+    solid samples are the ball's (weighted by their share), 0 for the terrain."""
+    rng = np.random.default_rng(seed)
+    ramp = (0.12 * ny, 0.25 * ny / nx)
+    sphere = ((0.62 * nx, 0.42 * ny, 0.5 * nz), 0.16 * min(nx, ny, nz))
+    off8 = np.array([[(c & 1) * 2 - 1, ((c >> 1) & 1) * 2 - 1, ((c >> 2) & 1) * 2 - 1] for c in range(8)],
+                    np.float64)
+
+    def fraction(centres, half):
+        pts = centres[..., None, :] + half * off8
+        solid, ball = _solid_samples(pts, ramp, sphere)
+        ns, nb = solid.sum(-1), ball.sum(-1)
+        return 1.0 - ns / 8.0, np.where(ns > 0, nb / np.maximum(ns, 1), 0.0)
+
+    zc, yc, xc = np.meshgrid(np.arange(nz) + 0.5, np.arange(ny) + 0.5, np.arange(nx) + 0.5, indexing="ij")
+    open_frac, _ = fraction(np.stack([xc, yc, zc], -1), 0.25)
+    faces, vel = [], []
+    for a, shape in enumerate(((nz, ny, nx + 1), (nz, ny + 1, nx), (nz + 1, ny, nx))):
+        idx = np.meshgrid(*(np.arange(s, dtype=np.float64) for s in shape), indexing="ij")   # z, y, x
+        cen = [idx[2] + 0.5, idx[1] + 0.5, idx[0] + 0.5]
+        cen[a] = idx[2 - a]   # the face sits on the cell boundary along its axis
+        f, share = fraction(np.stack(cen, -1), 0.4)
+        faces.append(np.ascontiguousarray(f, np.float32))
+        vel.append(np.ascontiguousarray(share * sphere_velocity[a], np.float32))
+    block = box_vof(nx, ny, nz, (0, 0, 0), (0.45 * nx, 0.7 * ny, nz))
+    vof = np.ascontiguousarray(block * open_frac, np.float32)
+    dt = 1.0 / 60.0
+    u, v, w = velocities(vof, rng, dt, "gauss", 0.2)
+    st = GridState(nx, ny, nz, 1.0 / max(nx, ny, nz), dt, vof, u, v, w, open_top=open_top,
+                   meta={"workload": f"dam break over a ramp around a moving ball, {nx}x{ny}x{nz}", "seed": seed})
+    return SolidScene(st, np.ascontiguousarray(open_frac, np.float32), *faces, *vel)

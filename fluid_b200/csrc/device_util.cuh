@@ -102,6 +102,22 @@ __device__ __forceinline__ float ghost_theta(float liquid_phi, float air_phi) {
   return fminf(1.0f, fmaxf(0.05f, a / fmaxf(a + fabsf(air_phi), 1e-12f)));
 }
 
+// Embedded solids: a face's open fraction at or below this is closed
+// (mgCoefficientRaw, mg.wgsl.ts:108: vf <= 1e-6 has no coefficient).
+constexpr float kClosedFace = 1e-6f;
+// Cells with an open fraction at or below this are solid (pressureDensity,
+// webgpu-uniform-reference.wgsl.ts:213-233).
+constexpr float kSolidCell = 1e-5f;
+
+// Coupling weight of the face between cell i and its +axis neighbour on a level
+// with the per-axis weight w: w itself without embedded solids, otherwise w
+// times the face's open fraction, zero for a closed face.
+__device__ __forceinline__ float face_w(const float* ff, long long n, int axis, long long i, float w) {
+  if (!ff) return w;
+  const float f = ff[axis * n + i];
+  return f > kClosedFace ? w * f : 0.0f;
+}
+
 // Canonical fold of the six face terms (mgD4Sum6, mg.wgsl.ts:49).
 __device__ __forceinline__ float d4sum6(float xm, float xp, float ym, float yp, float zm, float zp) {
   return ((xm + xp) + (zm + zp)) + (ym + yp);

@@ -174,8 +174,9 @@ __global__ void k_coarsen_phi(const InstDev* insts, const Tile* tiles, int ntile
 }
 
 // Diagonal of every level (mgCoefficientRaw / mgBakeCoefficients, mg.wgsl.ts:93-115,
-// 299-307, Neumann walls, no embedded solids): face to liquid w_a, face to air
-// w_a / theta, open top w_y / theta(phi, h_y / 2).
+// 299-307, Neumann walls): face to liquid w_a, face to air w_a / theta, open top
+// w_y / theta(phi, h_y / 2); with embedded solids each face's w_a is scaled by its
+// open fraction (a closed face adds nothing).
 template <class T>
 __global__ void k_bake_diag(const InstDev* insts, const Tile* tiles, int ntiles) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -190,16 +191,23 @@ __global__ void k_bake_diag(const InstDev* insts, const Tile* tiles, int ntiles)
       float d = 0.0f;
       if (L.label[i]) {
         const float ph = L.phi[i];
-        auto term = [&](bool inside, int j, float w) -> float {
+        const float* ff = L.ff;
+        const long long n = L.n;
+        // the face between cells f and f + stride of `axis` (j is the neighbour)
+        auto term = [&](bool inside, int j, int axis, int f, float w) -> float {
           if (!inside) return 0.0f;
-          return L.label[j] ? w : w / ghost_theta(ph, L.phi[j]);
+          const float wf = face_w(ff, n, axis, f, w);
+          return L.label[j] ? wf : wf / ghost_theta(ph, L.phi[j]);
         };
-        const float xm = term(x > 0, i - 1, wx), xp = term(x + 1 < L.nx, i + 1, wx);
-        const float ym = term(y > 0, i - sy, wy);
-        float yp = term(y + 1 < L.ny, i + sy, wy);
-        if (y + 1 == L.ny && I.open_top) yp = wy / ghost_theta(ph, L.ext_phi);
-        const float zm = term(z > 0, i - sz, wz), zp = term(z + 1 < L.nz, i + sz, wz);
+        const float xm = term(x > 0, i - 1, 0, i - 1, wx), xp = term(x + 1 < L.nx, i + 1, 0, i, wx);
+        const float ym = term(y > 0, i - sy, 1, i - sy, wy);
+        float yp = term(y + 1 < L.ny, i + sy, 1, i, wy);
+        if (y + 1 == L.ny && I.open_top) yp = face_w(ff, n, 1, i, wy) / ghost_theta(ph, L.ext_phi);
+        const float zm = term(z > 0, i - sz, 2, i - sz, wz), zp = term(z + 1 < L.nz, i + sz, 2, i, wz);
         d = d4sum6(xm, xp, ym, yp, zm, zp);
+        // embedded solids: a liquid cell whose faces are all closed has an empty
+        // row and leaves the system (its neighbours see it through closed faces only)
+        if (ff && d == 0.0f) L.label[i] = 0;
       }
       L.diag[i] = d;
       St<T>::st(L.diagT, i, d * norm);
@@ -238,12 +246,14 @@ __global__ void __launch_bounds__(kBlockThreads) k_coarse_factor(const InstDev* 
     if (I.open_top && y == L.ny - 1) atomicOr(&anchored, 1);
     A[i * m + i] = St<TD>::ld(L.diagT, i);
     const int sy = L.nx, sz = L.nx * L.ny;
-    if (x > 0 && L.label[i - 1]) A[i * m + i - 1] = -L.wx;
-    if (x + 1 < L.nx && L.label[i + 1]) A[i * m + i + 1] = -L.wx;
-    if (y > 0 && L.label[i - sy]) A[i * m + i - sy] = -L.wy;
-    if (y + 1 < L.ny && L.label[i + sy]) A[i * m + i + sy] = -L.wy;
-    if (z > 0 && L.label[i - sz]) A[i * m + i - sz] = -L.wz;
-    if (z + 1 < L.nz && L.label[i + sz]) A[i * m + i + sz] = -L.wz;
+    const float* ff = L.ff;
+    const long long n = L.n;
+    if (x > 0 && L.label[i - 1]) A[i * m + i - 1] = -face_w(ff, n, 0, i - 1, L.wx);
+    if (x + 1 < L.nx && L.label[i + 1]) A[i * m + i + 1] = -face_w(ff, n, 0, i, L.wx);
+    if (y > 0 && L.label[i - sy]) A[i * m + i - sy] = -face_w(ff, n, 1, i - sy, L.wy);
+    if (y + 1 < L.ny && L.label[i + sy]) A[i * m + i + sy] = -face_w(ff, n, 1, i, L.wy);
+    if (z > 0 && L.label[i - sz]) A[i * m + i - sz] = -face_w(ff, n, 2, i - sz, L.wz);
+    if (z + 1 < L.nz && L.label[i + sz]) A[i * m + i + sz] = -face_w(ff, n, 2, i, L.wz);
   }
   __syncthreads();
   if (!anchored) {
@@ -293,9 +303,15 @@ __global__ void __launch_bounds__(kThreads) k_cg_init_part(const InstDev* insts,
       float rv = b;
       if (lb[k]) {
         auto X = [&](int j) { return double(I.x[j]) + double(I.xlo[j]); };
-        auto nb = [&](bool in, int j) { return (in && lab[j]) ? X(j) : 0.0; };
-        const double s = ((nb(x > 0, i - 1) + nb(x + 1 < nx, i + 1)) + (nb(z > 0, i - sz) + nb(z + 1 < nz, i + sz))) +
-                         (nb(y > 0, i - sy) + nb(y + 1 < ny, i + sy));
+        const float* ff = L.ff;
+        const long long n = L.n;
+        // neighbour j across the face between cells f and f + stride of `axis`
+        auto nb = [&](bool in, int j, int axis, int f) {
+          return (in && lab[j]) ? double(face_w(ff, n, axis, f, 1.0f)) * X(j) : 0.0;
+        };
+        const double s = ((nb(x > 0, i - 1, 0, i - 1) + nb(x + 1 < nx, i + 1, 0, i)) +
+                          (nb(z > 0, i - sz, 2, i - sz) + nb(z + 1 < nz, i + sz, 2, i))) +
+                         (nb(y > 0, i - sy, 1, i - sy) + nb(y + 1 < ny, i + sy, 1, i));
         rv = float(double(b) - (double(L.diag[i]) * X(i) - s));
       }
       r[i] = rv;
@@ -426,9 +442,14 @@ __global__ void __launch_bounds__(kThreads) k_smooth(const InstDev* insts, const
         if (((x + y + zz) & 1) == colour) {
           float s = 0.0f;
           if (!zero_init) {
-            const float xm = x > 0 ? L.wx * tof(z[i - 1]) : 0.0f, xp = x + 1 < L.nx ? L.wx * tof(z[i + 1]) : 0.0f;
-            const float ym = y > 0 ? L.wy * tof(z[i - sy]) : 0.0f, yp = y + 1 < L.ny ? L.wy * tof(z[i + sy]) : 0.0f;
-            const float zm = zz > 0 ? L.wz * tof(z[i - sz]) : 0.0f, zp = zz + 1 < L.nz ? L.wz * tof(z[i + sz]) : 0.0f;
+            const float* ff = L.ff;
+            const long long n = L.n;
+            const float xm = x > 0 ? face_w(ff, n, 0, i - 1, L.wx) * tof(z[i - 1]) : 0.0f;
+            const float xp = x + 1 < L.nx ? face_w(ff, n, 0, i, L.wx) * tof(z[i + 1]) : 0.0f;
+            const float ym = y > 0 ? face_w(ff, n, 1, i - sy, L.wy) * tof(z[i - sy]) : 0.0f;
+            const float yp = y + 1 < L.ny ? face_w(ff, n, 1, i, L.wy) * tof(z[i + sy]) : 0.0f;
+            const float zm = zz > 0 ? face_w(ff, n, 2, i - sz, L.wz) * tof(z[i - sz]) : 0.0f;
+            const float zp = zz + 1 < L.nz ? face_w(ff, n, 2, i, L.wz) * tof(z[i + sz]) : 0.0f;
             s = d4sum6(xm, xp, ym, yp, zm, zp);
           }
           val[k] = lab[i] ? (tof(rhs[i]) + s) / tof(dg[i]) : 0.0f;
@@ -517,9 +538,14 @@ __global__ void __launch_bounds__(kThreads) k_residual_restrict(const InstDev* i
       const int i = x + F.nx * (y + F.ny * zz);
       float r = 0.0f;
       if (lab[i]) {
-        const float xm = x > 0 ? F.wx * tof(z[i - 1]) : 0.0f, xp = x + 1 < F.nx ? F.wx * tof(z[i + 1]) : 0.0f;
-        const float ym = y > 0 ? F.wy * tof(z[i - sy]) : 0.0f, yp = y + 1 < F.ny ? F.wy * tof(z[i + sy]) : 0.0f;
-        const float zm = zz > 0 ? F.wz * tof(z[i - sz]) : 0.0f, zp = zz + 1 < F.nz ? F.wz * tof(z[i + sz]) : 0.0f;
+        const float* ff = F.ff;
+        const long long n = F.n;
+        const float xm = x > 0 ? face_w(ff, n, 0, i - 1, F.wx) * tof(z[i - 1]) : 0.0f;
+        const float xp = x + 1 < F.nx ? face_w(ff, n, 0, i, F.wx) * tof(z[i + 1]) : 0.0f;
+        const float ym = y > 0 ? face_w(ff, n, 1, i - sy, F.wy) * tof(z[i - sy]) : 0.0f;
+        const float yp = y + 1 < F.ny ? face_w(ff, n, 1, i, F.wy) * tof(z[i + sy]) : 0.0f;
+        const float zm = zz > 0 ? face_w(ff, n, 2, i - sz, F.wz) * tof(z[i - sz]) : 0.0f;
+        const float zp = zz + 1 < F.nz ? face_w(ff, n, 2, i, F.wz) * tof(z[i + sz]) : 0.0f;
         r = scale * (tof(rhs[i]) - (tof(dg[i]) * tof(z[i]) - d4sum6(xm, xp, ym, yp, zm, zp)));
       }
       res_s[(lz * kRFY + ly) * kRFX + lx] = r;
@@ -1026,9 +1052,14 @@ __global__ void __launch_bounds__(kThreads) k_spmv(const InstDev* insts, const T
     for_column(it, L.nx, L.ny, L.nz, [&](int, int zz, int i) {
       float q = 0.0f;
       if (lab[i]) {
-        const float s = d4sum6(x > 0 ? D[i - 1] : 0.0f, x + 1 < L.nx ? D[i + 1] : 0.0f, y > 0 ? D[i - sy] : 0.0f,
-                               y + 1 < L.ny ? D[i + sy] : 0.0f, zz > 0 ? D[i - sz] : 0.0f,
-                               zz + 1 < L.nz ? D[i + sz] : 0.0f);
+        const float* ff = L.ff;
+        const long long n = L.n;
+        const float s = d4sum6(x > 0 ? face_w(ff, n, 0, i - 1, 1.0f) * D[i - 1] : 0.0f,
+                               x + 1 < L.nx ? face_w(ff, n, 0, i, 1.0f) * D[i + 1] : 0.0f,
+                               y > 0 ? face_w(ff, n, 1, i - sy, 1.0f) * D[i - sy] : 0.0f,
+                               y + 1 < L.ny ? face_w(ff, n, 1, i, 1.0f) * D[i + sy] : 0.0f,
+                               zz > 0 ? face_w(ff, n, 2, i - sz, 1.0f) * D[i - sz] : 0.0f,
+                               zz + 1 < L.nz ? face_w(ff, n, 2, i, 1.0f) * D[i + sz] : 0.0f);
         q = dg[i] * D[i] - s;
         dq += double(D[i]) * q;
       }
@@ -1201,14 +1232,16 @@ __global__ void __launch_bounds__(kThreads) k_true_residual(const InstDev* insts
     double sv[kMaxDepth], av[kMaxDepth];
     float bv[kMaxDepth];
     uint8_t lb[kMaxDepth];
+    const float* ff = L.ff;
+    const long long n = L.n;
     for_column(it, L.nx, L.ny, L.nz, [&](int k, int zz, int i) {
       double s = 0;
-      s += x > 0 ? X(i - 1) : 0.0;
-      s += x + 1 < L.nx ? X(i + 1) : 0.0;
-      s += y > 0 ? X(i - sy) : 0.0;
-      s += y + 1 < L.ny ? X(i + sy) : 0.0;
-      s += zz > 0 ? X(i - sz) : 0.0;
-      s += zz + 1 < L.nz ? X(i + sz) : 0.0;
+      s += x > 0 ? double(face_w(ff, n, 0, i - 1, 1.0f)) * X(i - 1) : 0.0;
+      s += x + 1 < L.nx ? double(face_w(ff, n, 0, i, 1.0f)) * X(i + 1) : 0.0;
+      s += y > 0 ? double(face_w(ff, n, 1, i - sy, 1.0f)) * X(i - sy) : 0.0;
+      s += y + 1 < L.ny ? double(face_w(ff, n, 1, i, 1.0f)) * X(i + sy) : 0.0;
+      s += zz > 0 ? double(face_w(ff, n, 2, i - sz, 1.0f)) * X(i - sz) : 0.0;
+      s += zz + 1 < L.nz ? double(face_w(ff, n, 2, i, 1.0f)) * X(i + sz) : 0.0;
       lb[k] = lab[i];
       sv[k] = s;
       av[k] = double(dg[i]) * X(i);

@@ -21,6 +21,7 @@
 #include "../../include/fluid_pp.h"
 #include "colmg.cuh"
 #include "fused.cuh"
+#include "solids.cuh"
 #include "plan.h"
 #include "types.h"
 
@@ -72,6 +73,7 @@ struct fluid_pp {
   bool has_pressure = false;
   float last_dt = 0.f;
   fluid_pp_batch* self = nullptr;   // batch of one
+  char* solid_mem = nullptr;         // embedded solids: open fractions, face fractions and velocities, level fractions
   long long plan_cells() const { return (long long)cfg.nx * cfg.ny * cfg.nz; }
   int set_error(int code, const std::string& m) {
     err = m;
@@ -107,6 +109,7 @@ struct fluid_pp_batch {
   List l0single;             // level-0 tiles of single-level instances
   List bake;
   List multi, single;        // instance lists (offsets into d_ilist) by coarsest level
+  bool solids = false;       // the instances have embedded solids (per-pass kernels, face-weighted operators)
   List fcb[kMaxLevels];      // multi-level instances for which level l is a grid level (full-cycle coarse steps)
   int maxL = 0;
   cudaError_t launch_err = cudaSuccess;   // first failed launch since the last check
@@ -239,7 +242,10 @@ void setup_launch(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
   const Tile* t0 = tl(B, B->l0);
   const int n0 = B->l0.n, g0 = launch_grid(n0);
   FPP_LAUNCH(B, kPrReset, k_reset_ctrl<<<(n + 127) / 128, 128, 0, s>>>(B->d_insts, n, B->d_loop));
-  FPP_LAUNCH(B, kPrLabel, k_label_rhs<<<g0, kThreads, 0, s>>>(B->d_insts, t0, n0, warm));
+  if (B->solids)
+    FPP_LAUNCH(B, kPrLabel, k_label_rhs_solid<<<g0, kThreads, 0, s>>>(B->d_insts, t0, n0, warm));
+  else
+    FPP_LAUNCH(B, kPrLabel, k_label_rhs<<<g0, kThreads, 0, s>>>(B->d_insts, t0, n0, warm));
   for (int l = 1; l < B->maxL; ++l)
     if (B->crs[l].n)
       FPP_LAUNCH(B, kPrCoarsen, k_coarsen_phi<<<launch_grid(B->crs[l].n), kThreads, 0, s>>>(B->d_insts, tl(B, B->crs[l]),
@@ -432,7 +438,7 @@ void iter_launch(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
     // flexible CG: gamma also takes r . z_prev (z_prev kept in d2)
     fcycle_launch<T>(B, pre, post);
     FPP_LAUNCH(B, kPrDot, k_dot_rz<true><<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
-  } else if (pre == 1 && post == 1) {
+  } else if (pre == 1 && post == 1 && !B->solids) {
     vcycle_fused<T>(B, 1);
     FPP_LAUNCH(B, kPrDirSpmv, k_cdirspmv<<<B->cq.n, kSThreads, 0, s>>>(B->d_insts, tl(B, B->cq)));
     FPP_LAUNCH(B, kPrDirSpmv, k_dirspmv_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(B->d_insts,
@@ -456,8 +462,13 @@ void finish_launch_any(fluid_pp_batch* B) {
   cudaStream_t s = B->stream;
   const Tile* t0 = tl(B, B->l0);
   const int n0 = B->l0.n, g = launch_grid(n0);
-  FPP_LAUNCH(B, kPrGrad, k_grad<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
-  FPP_LAUNCH(B, kPrReceipt, k_receipt_part<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+  if (B->solids) {
+    FPP_LAUNCH(B, kPrGrad, k_grad_solid<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+    FPP_LAUNCH(B, kPrReceipt, k_receipt_solid<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+  } else {
+    FPP_LAUNCH(B, kPrGrad, k_grad<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+    FPP_LAUNCH(B, kPrReceipt, k_receipt_part<<<g, kThreads, 0, s>>>(B->d_insts, t0, n0));
+  }
   FPP_LAUNCH(B, kPrReceipt, k_receipt_finish<<<B->multi.n + B->single.n, kThreads, 0, s>>>(B->d_insts,
                                                                                            il(B, B->multi)));
 }
@@ -651,6 +662,13 @@ static int batch_build(fluid_pp* const* handles, int count, const fluid_pp_batch
       err = "batched handles must share one stream (fluid_pp_set_stream)";
       return FLUID_PP_INVALID_ARG;
     }
+    // a batch runs one kind of kernels: the fused ones without embedded solids,
+    // the face-weighted per-pass ones with them
+    if (k > 0 && (h->inst.solids != 0) != B->solids) {
+      err = "batched handles must all have embedded solids or none";
+      return FLUID_PP_INVALID_ARG;
+    }
+    B->solids = h->inst.solids != 0;
     B->h.push_back(h);
     B->maxL = std::max(B->maxL, h->plan.levels);
   }
@@ -1360,6 +1378,7 @@ void fluid_pp_destroy(fluid_pp* pp) {
   if (!pp) return;
   cudaSetDevice(pp->cfg.device);
   if (pp->self) fluid_pp_batch_destroy(pp->self);
+  dev_release(pp->solid_mem, pp->stream);
   dev_release(pp->arena, pp->stream);
   delete pp;
 }
@@ -1527,6 +1546,85 @@ int fluid_pp_get_pressure_cells(fluid_pp* pp, float* x) {
   return FLUID_PP_OK;
 }
 
+int fluid_pp_upload_solids(fluid_pp* pp, const float* open, const float* fx, const float* fy, const float* fz,
+                           const float* usx, const float* usy, const float* usz) {
+  if (!pp || !open || !fx || !fy || !fz) return FLUID_PP_INVALID_ARG;
+  if ((usx != nullptr) != (usy != nullptr) || (usx != nullptr) != (usz != nullptr))
+    return pp->set_error(FLUID_PP_INVALID_ARG, "solid velocities: all three face arrays or none");
+  cudaSetDevice(pp->cfg.device);
+  InstDev& I = pp->inst;
+  const long long N = I.lv[0].n, nx = I.nx, ny = I.ny, nz = I.nz;
+  const long long nf[3] = {(nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1)};
+  long long floats = N + 2 * (nf[0] + nf[1] + nf[2]);
+  for (int l = 0; l < I.nlev; ++l) floats += 3 * I.lv[l].n;
+  cudaStream_t s = pp->stream;
+  if (!pp->solid_mem) {
+    cudaError_t e = dev_alloc(reinterpret_cast<void**>(&pp->solid_mem), size_t(floats) * 4);
+    if (e != cudaSuccess) return pp->set_error(FLUID_PP_OOM, std::string("solids: ") + cudaGetErrorString(e));
+  }
+  float* p = reinterpret_cast<float*>(pp->solid_mem);
+  I.open = p;
+  p += N;
+  for (int a = 0; a < 3; ++a) {
+    I.fv[a] = p;
+    p += nf[a];
+  }
+  for (int a = 0; a < 3; ++a) {
+    I.us[a] = p;
+    p += nf[a];
+  }
+  for (int l = 0; l < I.nlev; ++l) {
+    I.lv[l].ff = p;
+    p += 3 * I.lv[l].n;
+  }
+  const float* src[3] = {fx, fy, fz};
+  const float* vel[3] = {usx, usy, usz};
+  cudaError_t e = cudaMemcpyAsync(const_cast<float*>(I.open), open, 4 * N, cudaMemcpyHostToDevice, s);
+  for (int a = 0; a < 3 && e == cudaSuccess; ++a) {
+    e = cudaMemcpyAsync(const_cast<float*>(I.fv[a]), src[a], 4 * nf[a], cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = vel[a] ? cudaMemcpyAsync(const_cast<float*>(I.us[a]), vel[a], 4 * nf[a], cudaMemcpyHostToDevice, s)
+                 : cudaMemsetAsync(const_cast<float*>(I.us[a]), 0, 4 * nf[a], s);
+  }
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("solids: ") + cudaGetErrorString(e));
+  // every level below the coarsest runs the face-weighted grid kernels; the
+  // coarse block only applies the dense coarsest inverse
+  I.solids = 1;
+  if (I.nlev > 1) {
+    I.first_block = I.nlev - 1;
+    I.block_smem = int(block_level_bytes(I.lv[I.nlev - 1].n));
+  }
+  if (pp->self) {
+    fluid_pp_batch_destroy(pp->self);
+    pp->self = nullptr;
+  }
+  fluid_pp* raw = pp;
+  std::string err;
+  fluid_pp_batch_tuning tu;
+  fluid_pp_batch_tuning_default(&tu);
+  int rc = batch_build(&raw, 1, tu, &pp->self, err);
+  if (rc != FLUID_PP_OK) return pp->set_error(rc, err);
+  fluid_pp_batch* B = pp->self;
+  k_solid_faces<<<launch_grid(int(std::min<long long>((N + kThreads - 1) / kThreads, kMaxGrid))), kThreads, 0, s>>>(
+      B->d_insts);
+  for (int l = 1; l < I.nlev; ++l)
+    k_coarsen_faces<<<launch_grid(int(std::min<long long>((I.lv[l].n + kThreads - 1) / kThreads, kMaxGrid))),
+                      kThreads, 0, s>>>(B->d_insts, l);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("solids: ") + cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_get_level_faces(fluid_pp* pp, int level, float* ff) {
+  if (!pp || !ff || level < 0 || level >= pp->inst.nlev) return FLUID_PP_INVALID_ARG;
+  if (!pp->inst.solids) return pp->set_error(FLUID_PP_INVALID_ARG, "no embedded solids uploaded");
+  cudaSetDevice(pp->cfg.device);
+  const LevelDev& L = pp->inst.lv[level];
+  cudaError_t e = cudaMemcpy(ff, L.ff, 12 * size_t(L.n), cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? FLUID_PP_OK : pp->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+}
+
 int fluid_pp_apply_operator(fluid_pp* pp, const float* p, float* out) {
   if (!pp || !p || !out) return FLUID_PP_INVALID_ARG;
   cudaSetDevice(pp->cfg.device);
@@ -1561,7 +1659,7 @@ int fluid_pp_apply_vcycle(fluid_pp* pp, const float* r, float* z, int pre, int p
   const long long N = pp->inst.lv[0].n;
   cudaMemcpyAsync(pp->inst.lv[0].rhs, r, 4 * N, cudaMemcpyHostToDevice, B->stream);
   k_hook_ctrl<<<1, 1, 0, B->stream>>>(B->d_insts, hook_sigma(r, N));
-  const bool fused = pre == 1 && post == 1;
+  const bool fused = pre == 1 && post == 1 && !B->solids;
   switch (B->precision) {
     case FLUID_PP_FP16: fused ? vcycle_fused<__half>(B, 0) : vcycle_launch<__half>(B, pre, post); break;
     case FLUID_PP_BF16: fused ? vcycle_fused<__nv_bfloat16>(B, 0) : vcycle_launch<__nv_bfloat16>(B, pre, post); break;

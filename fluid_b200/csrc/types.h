@@ -74,6 +74,7 @@ struct LevelDev {
   void* z;            // level solution (level 0: float CG vector)
   void* rhs;          // level right-hand side (level 0: the CG residual r, float)
   void* res;          // scratch in the z type: the pre-smoothed z between the fused down and up steps
+  const float* ff;    // embedded solids: open fraction of each cell's +x, +y, +z face (planar, 3 x n), or null
 };
 
 struct InstDev {
@@ -98,6 +99,12 @@ struct InstDev {
   float* d2;
   float* q;           // A d
   float* p_si;        // pressure output in Pa
+  // embedded solids (null / 0 without): cell open fraction, face open fractions
+  // and solid normal velocities on the MAC faces (layouts of u, v, w)
+  int solids;
+  const float* open;
+  const float* fv[3];
+  const float* us[3];
   double* partial;    // kSlots * ntiles0 per-tile reduction partials
   double* coarse_inv; // coarse_m^2 dense inverse of the coarsest operator
   Ctrl* ctrl;

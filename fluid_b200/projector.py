@@ -120,6 +120,32 @@ class PressureProjector:
         _check(load().fluid_pp_set_stream(self._h, ctypes.c_void_p(int(stream))), self._h)
 
     # -- state -----------------------------------------------------------------
+    def upload_solids(self, open_frac, fx, fy, fz, usx=None, usy=None, usz=None):
+        """Embedded solids: cell open fractions [nz][ny][nx], face open fractions
+        and (optionally) solid normal face velocities in the layouts of u, v, w."""
+        nx, ny, nz = self.dims
+        sizes = (nx * ny * nz, (nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1))
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (open_frac, fx, fy, fz)]
+        for a, s, name in zip(arrs, sizes, ("open", "fx", "fy", "fz")):
+            if a.size != s:
+                raise ValueError(f"{name} has {a.size} entries; expected {s}")
+        vel = [None, None, None]
+        if usx is not None:
+            vel = [np.ascontiguousarray(a, np.float32) for a in (usx, usy, usz)]
+            for a, s, name in zip(vel, sizes[1:], ("usx", "usy", "usz")):
+                if a.size != s:
+                    raise ValueError(f"{name} has {a.size} entries; expected {s}")
+        self._solids = (arrs, vel)   # keep the host arrays alive until the copies are done
+        _check(load().fluid_pp_upload_solids(self._h, *(ptr(a) for a in arrs),
+                                             *(ptr(a) if a is not None else None for a in vel)), self._h, "solids")
+
+    def level_faces(self, level: int) -> np.ndarray:
+        """Face open fractions of a level, [3][nz][ny][nx] (+x, +y, +z face of each cell)."""
+        nx, ny, nz = self.level_dims(level)
+        out = np.empty((3, nz, ny, nx), np.float32)
+        _check(load().fluid_pp_get_level_faces(self._h, int(level), ptr(out)), self._h)
+        return out
+
     def upload_state(self, vof, u, v, w):
         nx, ny, nz = self.dims
         arrs = [np.ascontiguousarray(a, np.float32) for a in (vof, u, v, w)]

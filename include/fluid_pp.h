@@ -132,6 +132,25 @@ int fluid_pp_upload_state(fluid_pp* pp, const float* vof, const float* u, const 
 /* Device-pointer variant of upload: copies from device buffers (same layouts). */
 int fluid_pp_upload_state_device(fluid_pp* pp, const float* vof, const float* u, const float* v, const float* w);
 
+/* Embedded solids (cut cells), host arrays, kept for every later projection of
+ * the handle.  Replaces the solid topology the reference bakes on the finest
+ * level (mgBuildFinestTopology, webgpu-uniform-pressure-multigrid.wgsl.ts:
+ * 136-150: cellOpenFraction and pressureFaceVolumeFraction,
+ * webgpu-uniform-reference.wgsl.ts:208-233, 530-556) and the solid face
+ * velocities of its divergence and projection (:1005-1024, :1052-1099).
+ *   open  [nz][ny][nx]    open (non-solid) volume fraction of each cell, in [0, 1]
+ *   fx, fy, fz            open fraction of each MAC face's dual cell, layouts of u, v, w
+ *   usx, usy, usz         the solids' normal velocity on each face (all NULL: static solids)
+ * Fractions are clamped to [0, 1]; a face at or below 1e-6 is closed.  The
+ * operator's face weights become the face fractions (coarse levels: the mean of
+ * the eight children's), rho' = vof / open with the open neighbours' maximum
+ * continued into solid cells (open <= 1e-5), and every level below the coarsest
+ * runs the face-weighted grid kernels.  Allocates about (4 + 24 + 14) bytes per
+ * cell beside the arena, once.  Upload solids before creating a batch of the
+ * handle; a batch holds handles that all have solids or none. */
+int fluid_pp_upload_solids(fluid_pp* pp, const float* open, const float* fx, const float* fy, const float* fz,
+                           const float* usx, const float* usy, const float* usz);
+
 /* Label -> divergence -> assemble -> MGPCG -> gradient subtract, on the device.
  * Replaces WebGPUUniformPressureMultigrid.encode (webgpu-uniform-pressure-multigrid.ts:327-364)
  * followed by the `project` dispatch (webgpu-uniform-reference.ts:1280-1282);
@@ -180,6 +199,8 @@ int fluid_pp_apply_vcycle(fluid_pp* pp, const float* r, float* z, int pre, int p
  * NULL) receives that first block level (0 for a single-level hierarchy). */
 int fluid_pp_apply_fcycle(fluid_pp* pp, const float* r, float* z, int pre, int post, int* first_block);
 int fluid_pp_get_pressure_cells(fluid_pp* pp, float* x);             /* solution, finest-cell units */
+/* Embedded solids: a level's face open fractions, planar [3][n] (+x, +y, +z face of each cell). */
+int fluid_pp_get_level_faces(fluid_pp* pp, int level, float* ff);
 
 /* Batched projection of several handles in one set of launches per stage.
  * Replaces nothing in the reference (which runs one solver per device); the

@@ -170,8 +170,16 @@ struct Level {
   std::vector<uint8_t> label;  // 1 liquid, 0 air
   std::vector<float> phi;      // level-set sample, finest-cell units
   std::vector<double> diag;
+  std::vector<float> ff;       // embedded solids: open fraction of each cell's +x, +y, +z face (3 x cells)
   bool anchored = true;
   long idx(int x, int y, int z) const { return x + long(n[0]) * (y + long(n[1]) * z); }
+  // weight of the face between cell i and its +axis neighbour: w_a, scaled by
+  // the face's open fraction with embedded solids, 0 for a closed face
+  double fw(int a, long i) const {
+    if (ff.empty()) return w[a];
+    const float f = ff[a * cells + i];
+    return f > 1e-6f ? w[a] * double(f) : 0.0;
+  }
 };
 
 struct Ctx {
@@ -184,6 +192,10 @@ struct Ctx {
   std::vector<double> b;           // rhs in cell units
   std::vector<double> q;           // volume-correction target divergence (cell units)
   std::vector<double> coarseChol;  // dense Cholesky factor of the coarsest level
+  // embedded solids (webgpu-uniform-reference.wgsl.ts:208-233, 530-556, 1005-1024)
+  bool solids = false;
+  std::vector<float> open;         // cell open fraction
+  std::vector<float> fv[3], us[3]; // face open fractions and solid normal velocities (layouts of u, v, w)
   int threads = 1;
   long cells() const { return long(n[0]) * n[1] * n[2]; }
   long uIdx(int x, int y, int z) const { return x + long(n[0] + 1) * (y + long(n[1]) * z); }
@@ -191,15 +203,113 @@ struct Ctx {
   long wIdx(int x, int y, int z) const { return x + long(n[0]) * (y + long(n[1]) * z); }
 };
 
-// ref.wgsl.ts:208-242 with no embedded solids (open fraction 1): rho' = vof,
+float clamp01(float v) { return std::min(v > 0.0f ? v : 0.0f, 1.0f); }   // NaN -> 0
+
+// pressureDensity (ref.wgsl.ts:213-233): rho' = vof / open for an open cell
+// (open > 1e-5), otherwise the largest rho' of its open neighbours; float32.
+float solidDensity(const Ctx& c, int x, int y, int z) {
+  const int nx = c.n[0], ny = c.n[1], nz = c.n[2];
+  const long i = x + long(nx) * (y + long(ny) * z);
+  const float v = clamp01(c.open[i]);
+  if (v > 1e-5f) return c.vof[i] / v;
+  float best = 0.0f;
+  auto take = [&](bool inside, long j) {
+    if (!inside) return;
+    const float vj = clamp01(c.open[j]);
+    if (vj > 1e-5f) best = std::max(best, c.vof[j] / vj);
+  };
+  take(x > 0, i - 1);
+  take(x + 1 < nx, i + 1);
+  take(y > 0, i - nx);
+  take(y + 1 < ny, i + nx);
+  take(z > 0, i - long(nx) * ny);
+  take(z + 1 < nz, i + long(nx) * ny);
+  return best;
+}
+
+// ref.wgsl.ts:208-242: rho' = vof (no embedded solids) or solidDensity,
 // liquid <=> rho' > 0.5, phi = 0.5 - rho' in cell units (the WGSL multiplies by dx).
 void labelFine(Ctx& c) {
   Level& L = c.lv[0];
-  for (long i = 0; i < c.cells(); ++i) {
-    float rho = c.vof[i];
-    L.label[i] = rho > 0.5f ? 1 : 0;
-    L.phi[i] = 0.5f - rho;
-  }
+  for (int z = 0; z < c.n[2]; ++z)
+    for (int y = 0; y < c.n[1]; ++y)
+      for (int x = 0; x < c.n[0]; ++x) {
+        const long i = L.idx(x, y, z);
+        const float rho = c.solids ? solidDensity(c, x, y, z) : c.vof[i];
+        L.label[i] = rho > 0.5f ? 1 : 0;
+        L.phi[i] = 0.5f - rho;
+        if (c.solids && L.label[i]) {   // a liquid cell needs an open face (mg.wgsl.ts:341)
+          auto open = [&](int a, long f) { return clamp01(c.fv[a][f]) > 1e-6f; };
+          const int nx = c.n[0], ny = c.n[1], nz = c.n[2];
+          const bool any = (x > 0 && open(0, c.uIdx(x, y, z))) || (x + 1 < nx && open(0, c.uIdx(x + 1, y, z))) ||
+                           (y > 0 && open(1, c.vIdx(x, y, z))) ||
+                           ((y + 1 < ny || c.openTop) && open(1, c.vIdx(x, y + 1, z))) ||
+                           (z > 0 && open(2, c.wIdx(x, y, z))) || (z + 1 < nz && open(2, c.wIdx(x, y, z + 1)));
+          if (!any) L.label[i] = 0;
+        }
+      }
+}
+
+// divergenceAt (ref.wgsl.ts:1010-1024, CM11a Eqs. 8-10) in cell units with
+// face weights W = open fraction (0 for a closed face or a wall): per axis
+// (W+ u+ - W- u-) + (W+ - V) us+ - (W- - V) us-, for velocities U, V, W.
+template <class TV>
+double solidDivergence(const Ctx& c, int x, int y, int z, const TV* U, const TV* Vv, const TV* Wv) {
+  const int nx = c.n[0], ny = c.n[1], nz = c.n[2];
+  const long i = x + long(nx) * (y + long(ny) * z);
+  const double vi = clamp01(c.open[i]);
+  auto weight = [](float f) { const float g = clamp01(f); return g > 1e-6f ? double(g) : 0.0; };
+  auto axis = [&](int a, bool hm, long fm, bool hp, long fp, const TV* vel) {
+    const double wm = hm ? weight(c.fv[a][fm]) : 0.0, wp = hp ? weight(c.fv[a][fp]) : 0.0;
+    const double um = hm ? vel[fm] : 0.0, up = hp ? vel[fp] : 0.0;
+    const double sm = hm ? c.us[a][fm] : 0.0, sp = hp ? c.us[a][fp] : 0.0;
+    return (wp * up - wm * um) + ((wp - vi) * sp - (wm - vi) * sm);
+  };
+  const double fx = axis(0, x > 0, c.uIdx(x, y, z), x + 1 < nx, c.uIdx(x + 1, y, z), U);
+  const double fy = axis(1, y > 0, c.vIdx(x, y, z), y + 1 < ny || c.openTop, c.vIdx(x, y + 1, z), Vv);
+  const double fz = axis(2, z > 0, c.wIdx(x, y, z), z + 1 < nz, c.wIdx(x, y, z + 1), Wv);
+  return (fx + fz) + fy;
+}
+
+// Level-0 face fractions in the level layout: the +x, +y, +z face of each
+// cell, a domain-wall face 1 (no coupling; it only enters the coarse means),
+// the open top its given fraction.
+void solidFacesFine(Ctx& c) {
+  Level& L = c.lv[0];
+  L.ff.assign(3 * L.cells, 1.0f);
+  for (int z = 0; z < c.n[2]; ++z)
+    for (int y = 0; y < c.n[1]; ++y)
+      for (int x = 0; x < c.n[0]; ++x) {
+        const long i = L.idx(x, y, z);
+        if (x + 1 < c.n[0]) L.ff[i] = clamp01(c.fv[0][c.uIdx(x + 1, y, z)]);
+        if (y + 1 < c.n[1] || c.openTop) L.ff[L.cells + i] = clamp01(c.fv[1][c.vIdx(x, y + 1, z)]);
+        if (z + 1 < c.n[2]) L.ff[2 * L.cells + i] = clamp01(c.fv[2][c.wIdx(x, y, z + 1)]);
+      }
+}
+
+// Coarse face fractions: the mean of the eight children's, per axis
+// (mgDownsampleTopology, mg.wgsl.ts:170-183), in float32 in mgD4Sum8 order.
+void coarsenFaces(const Level& F, Level& C) {
+  C.ff.assign(3 * C.cells, 0.0f);
+  for (int z = 0; z < C.n[2]; ++z)
+    for (int y = 0; y < C.n[1]; ++y)
+      for (int x = 0; x < C.n[0]; ++x) {
+        long child[8];
+        int cc[3] = {x, y, z};
+        for (int corner = 0; corner < 8; ++corner) {
+          int o[3] = {corner & 1, (corner >> 1) & 1, (corner >> 2) & 1};
+          int f[3];
+          for (int a = 0; a < 3; ++a) f[a] = std::min(C.stride[a] * cc[a] + o[a] * (C.stride[a] - 1), F.n[a] - 1);
+          child[corner] = F.idx(f[0], f[1], f[2]);
+        }
+        for (int a = 0; a < 3; ++a) {
+          float v[8];
+          for (int k = 0; k < 8; ++k) v[k] = F.ff[a * F.cells + child[k]];
+          const float y0 = (v[0] + v[5]) + (v[1] + v[4]);
+          const float y1 = (v[2] + v[7]) + (v[3] + v[6]);
+          C.ff[a * C.cells + C.idx(x, y, z)] = (y0 + y1) / 8.0f;
+        }
+      }
 }
 
 // cm12-numerics.ts:127-138 scaled by h (cell units).
@@ -228,7 +338,12 @@ void buildRhs(Ctx& c) {
         double wp = z + 1 < nz ? c.w[c.wIdx(x, y, z + 1)] : 0.0;
         double wm = z > 0 ? c.w[c.wIdx(x, y, z)] : 0.0;
         double div = (up - um) + (wp - wm) + (vp - vm);
-        c.q[i] = volumeCorrection(c.vof[i], c.h, c.dt);
+        if (c.solids) {   // weighted flux divergence and the volume correction of rho'
+          div = solidDivergence(c, x, y, z, c.u.data(), c.v.data(), c.w.data());
+          c.q[i] = volumeCorrection(solidDensity(c, x, y, z), c.h, c.dt);
+        } else {
+          c.q[i] = volumeCorrection(c.vof[i], c.h, c.dt);
+        }
         c.b[i] = -(div - c.q[i]);
       }
 }
@@ -289,16 +404,19 @@ void bakeDiag(Level& L, int openTop) {
           int q[3] = {x, y, z};
           q[a] += dir;
           double t = 0;
+          const long stride = a == 0 ? 1 : (a == 1 ? L.n[0] : long(L.n[0]) * L.n[1]);
+          const long face = dir > 0 ? i : i - stride;   // the face's lower cell
           if (q[a] < 0 || q[a] >= L.n[a]) {
-            if (openTop && a == 1 && dir > 0) t = L.w[1] / theta(pi, L.extPhi);
+            if (openTop && a == 1 && dir > 0) t = L.fw(1, i) / theta(pi, L.extPhi);
           } else {
             long j = L.idx(q[0], q[1], q[2]);
-            t = L.label[j] ? L.w[a] : L.w[a] / theta(pi, L.phi[j]);
+            t = L.label[j] ? L.fw(a, face) : L.fw(a, face) / theta(pi, L.phi[j]);
           }
           terms[nb] = t;
           (void)c;
         }
         L.diag[i] = ((terms[0] + terms[1]) + (terms[4] + terms[5])) + (terms[2] + terms[3]);
+        if (!L.ff.empty() && L.diag[i] == 0.0) L.label[i] = 0;   // every face closed: no unknown
       }
   L.anchored = anyAir || (openTop && anyTopLiquid);
 }
@@ -314,13 +432,14 @@ void applyLevel(const Level& L, const double* p, double* out, int threads) {
       for (int x = 0; x < nx; ++x) {
         long i = L.idx(x, y, z);
         if (!L.label[i]) { out[i] = 0; continue; }
+        const long sz = long(nx) * ny;
         double s = 0;
-        if (x > 0) s += L.w[0] * p[i - 1];
-        if (x + 1 < nx) s += L.w[0] * p[i + 1];
-        if (y > 0) s += L.w[1] * p[i - nx];
-        if (y + 1 < ny) s += L.w[1] * p[i + nx];
-        if (z > 0) s += L.w[2] * p[i - long(nx) * ny];
-        if (z + 1 < nz) s += L.w[2] * p[i + long(nx) * ny];
+        if (x > 0) s += L.fw(0, i - 1) * p[i - 1];
+        if (x + 1 < nx) s += L.fw(0, i) * p[i + 1];
+        if (y > 0) s += L.fw(1, i - nx) * p[i - nx];
+        if (y + 1 < ny) s += L.fw(1, i) * p[i + nx];
+        if (z > 0) s += L.fw(2, i - sz) * p[i - sz];
+        if (z + 1 < nz) s += L.fw(2, i) * p[i + sz];
         out[i] = L.diag[i] * p[i] - s;   // air neighbours hold zero
       }
 }
@@ -350,13 +469,14 @@ void smooth(const Level& L, const double* rhs, double* z, int colour) {
         if (((x + y + zz) & 1) != colour) continue;
         long i = L.idx(x, y, zz);
         if (!L.label[i]) { z[i] = 0; continue; }
+        const long sz = long(nx) * ny;
         double s = 0;
-        if (x > 0) s += L.w[0] * z[i - 1];
-        if (x + 1 < nx) s += L.w[0] * z[i + 1];
-        if (y > 0) s += L.w[1] * z[i - nx];
-        if (y + 1 < ny) s += L.w[1] * z[i + nx];
-        if (zz > 0) s += L.w[2] * z[i - long(nx) * ny];
-        if (zz + 1 < nz) s += L.w[2] * z[i + long(nx) * ny];
+        if (x > 0) s += L.fw(0, i - 1) * z[i - 1];
+        if (x + 1 < nx) s += L.fw(0, i) * z[i + 1];
+        if (y > 0) s += L.fw(1, i - nx) * z[i - nx];
+        if (y + 1 < ny) s += L.fw(1, i) * z[i + nx];
+        if (zz > 0) s += L.fw(2, i - sz) * z[i - sz];
+        if (zz + 1 < nz) s += L.fw(2, i) * z[i + sz];
         z[i] = (rhs[i] + s) / L.diag[i];
       }
 }
@@ -425,7 +545,7 @@ void factorCoarsest(Ctx& c) {
           q[a] += dir;
           if (q[a] < 0 || q[a] >= L.n[a]) continue;
           long j = L.idx(q[0], q[1], q[2]);
-          if (L.label[j]) A[i * m + j] = -L.w[a];
+          if (L.label[j]) A[i * m + j] = -L.fw(a, std::min(i, j));
         }
       }
   if (!L.anchored) {
@@ -535,7 +655,19 @@ void buildAll(Ctx& c) {
   labelFine(c);
   buildRhs(c);
   for (int l = 1; l < (int)c.lv.size(); ++l) coarsenPhi(c.lv[l - 1], c.lv[l], l);
+  if (c.solids) {
+    solidFacesFine(c);
+    for (int l = 1; l < (int)c.lv.size(); ++l) coarsenFaces(c.lv[l - 1], c.lv[l]);
+  }
   for (auto& L : c.lv) bakeDiag(L, c.openTop);
+  if (c.solids) {   // a liquid cell dropped for its closed faces is no Dirichlet contact
+    Level& L = c.lv[0];
+    bool air = false, top = false;
+    for (long i = 0; i < L.cells; ++i) air |= !(L.phi[i] < 0.0f);
+    for (int z = 0; z < L.n[2]; ++z)
+      for (int x = 0; x < L.n[0]; ++x) top |= L.label[L.idx(x, L.n[1] - 1, z)] != 0;
+    L.anchored = air || (c.openTop && top);
+  }
   factorCoarsest(c);
 }
 
@@ -645,6 +777,32 @@ void orc_vcycle(void* h, const double* r, double* z, int pre, int post) {
     wk.res.emplace_back(L.cells, 0.0);
   }
   precondition(c, wk, r, z, pre, post);
+}
+
+// Embedded solids (cell open fractions, face open fractions and optional solid
+// normal velocities in the layouts of u, v, w); rebuilds the system of the
+// current state.
+int orc_set_solids(void* h, const float* open, const float* fx, const float* fy, const float* fz, const float* usx,
+                   const float* usy, const float* usz) {
+  Ctx& c = *static_cast<Ctx*>(h);
+  const long N = c.cells();
+  c.solids = true;
+  c.open.assign(open, open + N);
+  const float* f[3] = {fx, fy, fz};
+  const float* s[3] = {usx, usy, usz};
+  const long nf[3] = {long(c.u.size()), long(c.v.size()), long(c.w.size())};
+  for (int a = 0; a < 3; ++a) {
+    c.fv[a].assign(f[a], f[a] + nf[a]);
+    if (s[a]) c.us[a].assign(s[a], s[a] + nf[a]);
+    else c.us[a].assign(nf[a], 0.0f);
+  }
+  buildAll(c);
+  return 0;
+}
+
+void orc_level_faces(void* h, int l, float* ff) {
+  const Level& L = static_cast<Ctx*>(h)->lv[l];
+  std::copy(L.ff.begin(), L.ff.end(), ff);
 }
 
 void orc_fcycle(void* h, const double* r, double* z, int pre, int post, int firstBlock) {
@@ -891,12 +1049,15 @@ void orc_grad_subtract(void* h, const double* p, float* uo, float* vo, float* wo
     if (!li && lj) th = theta(L.phi[j], L.phi[i]);
     return (pv(j) - pv(i)) / th;
   };
+  // embedded solids: a closed face carries the solids' velocity (ref.wgsl.ts:1085)
+  auto closed = [&](int a, long f) { return c.solids && !(clamp01(c.fv[a][f]) > 1e-6f); };
   for (int z = 0; z < nz; ++z)
     for (int y = 0; y < ny; ++y)
       for (int x = 0; x <= nx; ++x) {
         long f = c.uIdx(x, y, z);
         if (x == 0 || x == nx) { U[f] = 0; continue; }
         long i = L.idx(x - 1, y, z), j = L.idx(x, y, z);
+        if (closed(0, f)) { U[f] = c.us[0][f]; continue; }
         U[f] = (L.label[i] || L.label[j]) ? c.u[f] - faceCorr(i, j) : 0.0;
       }
   for (int z = 0; z < nz; ++z)
@@ -906,11 +1067,13 @@ void orc_grad_subtract(void* h, const double* p, float* uo, float* vo, float* wo
         if (y == 0) { V[f] = 0; continue; }
         if (y == ny) {
           long i = L.idx(x, y - 1, z);
-          if (c.openTop && L.label[i]) V[f] = c.v[f] - (0.0 - p[i]) / theta(L.phi[i], 0.5);
+          if (c.openTop && closed(1, f)) V[f] = c.us[1][f];
+          else if (c.openTop && L.label[i]) V[f] = c.v[f] - (0.0 - p[i]) / theta(L.phi[i], 0.5);
           else V[f] = 0;
           continue;
         }
         long i = L.idx(x, y - 1, z), j = L.idx(x, y, z);
+        if (closed(1, f)) { V[f] = c.us[1][f]; continue; }
         V[f] = (L.label[i] || L.label[j]) ? c.v[f] - faceCorr(i, j) : 0.0;
       }
   for (int z = 0; z <= nz; ++z)
@@ -919,6 +1082,7 @@ void orc_grad_subtract(void* h, const double* p, float* uo, float* vo, float* wo
         long f = c.wIdx(x, y, z);
         if (z == 0 || z == nz) { W[f] = 0; continue; }
         long i = L.idx(x, y, z - 1), j = L.idx(x, y, z);
+        if (closed(2, f)) { W[f] = c.us[2][f]; continue; }
         W[f] = (L.label[i] || L.label[j]) ? c.w[f] - faceCorr(i, j) : 0.0;
       }
   double m0 = 0, m1 = 0, s0 = 0, s1 = 0;
@@ -930,6 +1094,8 @@ void orc_grad_subtract(void* h, const double* p, float* uo, float* vo, float* wo
         double before = -c.b[i];
         double after = (U[c.uIdx(x + 1, y, z)] - U[c.uIdx(x, y, z)]) + (W[c.wIdx(x, y, z + 1)] - W[c.wIdx(x, y, z)]) +
                        (V[c.vIdx(x, y + 1, z)] - V[c.vIdx(x, y, z)]) - c.q[i];
+        if (c.solids)   // the weighted divergence of the projected faces
+          after = solidDivergence(c, x, y, z, U.data(), V.data(), W.data()) - c.q[i];
         m0 = std::max(m0, std::fabs(before));
         m1 = std::max(m1, std::fabs(after));
         s0 += before * before;

@@ -47,6 +47,9 @@ def lib():
         L.orc_get_rhs.argtypes = [vp, vp, vp]
         L.orc_apply_level.argtypes = [vp, c_int, vp, vp]
         L.orc_vcycle.argtypes = [vp, vp, vp, c_int, c_int]
+        L.orc_set_solids.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
+        L.orc_set_solids.restype = c_int
+        L.orc_level_faces.argtypes = [vp, c_int, vp]
         L.orc_fcycle.argtypes = [vp, vp, vp, c_int, c_int, c_int]
         L.orc_solve_fcg.argtypes = [vp, c_double, c_double, c_int, c_int, c_int, c_int, vp, vp]
         L.orc_solve_fcg.restype = c_int
@@ -170,6 +173,19 @@ class Oracle:
         z = np.zeros_like(r)
         lib().orc_vcycle(self._h, _p(r), _p(z), pre, post)
         return z
+
+    def set_solids(self, open_frac, fx, fy, fz, usx=None, usy=None, usz=None):
+        """Embedded solids (cell and face open fractions, optional solid face
+        velocities); rebuilds the current state's system."""
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (open_frac, fx, fy, fz)]
+        vel = [np.ascontiguousarray(a, np.float32) if a is not None else None for a in (usx, usy, usz)]
+        lib().orc_set_solids(self._h, *(_p(a) for a in arrs), *(_p(a) if a is not None else None for a in vel))
+
+    def level_faces(self, level: int) -> np.ndarray:
+        (nx, ny, nz), _, _ = self.level_dims(level)
+        out = np.empty((3, nz, ny, nx), np.float32)
+        lib().orc_level_faces(self._h, int(level), _p(out))
+        return out
 
     def fcycle(self, r, pre: int = 1, post: int = 1, first_block: int = 1):
         """One full cycle from a zero guess; levels from `first_block` on take one V-cycle."""
