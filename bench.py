@@ -74,6 +74,8 @@ def stage_bytes_per_cell(stage: str, s: int) -> float:
 # cold cache).  The roofline scales it to the average launch of a solve by the
 # cells that launch processes (later launches skip finished instances).
 CYCLE_STEPS = 8
+SOLID_DIMS = (128, 96, 128)   # the 128x96x128 lattice with a ramp and a moving ball as embedded solids
+SOLID_STEPS = 8
 SERVE_CELLS = 8e6     # resident uniform cells: the batched step stays near 8 ms
 SERVE_TALL = 2        # resident tall-cell simulations (they share the tall slices)
 NCU_FIRST_LAUNCH_BYTES = {"down0": 149.1e6, "up0": 214.4e6, "dirspmv": 250.8e6}
@@ -517,6 +519,52 @@ def main():
     stage_gbs = {k: round(stage_bytes_per_cell(k, sbytes) * cell_iters / (v["ms"] / 1000.0) / 1e9, 1)
                  for k, v in stages.items()}
 
+    # ------------------------------------ secondary: embedded solids (cut cells)
+    note("embedded solids")
+    sc = configs.solid_scene(*SOLID_DIMS)
+    ss = sc.state
+    dev4 = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (ss.vof, ss.u, ss.v, ss.w)]
+
+    def run_solid(precision):
+        pp_ = PressureProjector((ss.nx, ss.ny, ss.nz), ss.h, ss.rho, ss.open_top, precision, device=local)
+        pp_.set_stream(stream.cuda_stream)
+        pp_.upload_solids(*sc.solids())
+        tt, rec_ = [], None
+
+        def step():
+            pp_.upload_state_device(*(t.data_ptr() for t in dev4))
+            return pp_.project(ss.dt, **opts)
+        for k in range(args.warmup + SOLID_STEPS):
+            ms, rec_ = timed(step)
+            if k >= args.warmup:
+                tt.append(ms)
+        p_ = pp_.pressure_cells().astype(np.float64)
+        pp_.destroy()
+        return tt, rec_, p_
+    t5, r5, p5 = run_solid("fp32")
+    t5m, r5m, p5m = run_solid(args.precision)
+    from oracle.oracle import Oracle
+    o5 = Oracle(ss.nx, ss.ny, ss.nz, ss.h, ss.rho, ss.open_top)
+    o5.set_threads(os.cpu_count() or 1)
+    o5.set_state(ss.vof, ss.u, ss.v, ss.w, ss.dt)
+    o5.set_solids(*sc.solids())
+    p5_ref, _ = o5.solve_mgpcg(1e-12, 0.0, 400, 2, 2)
+    nref = float(np.linalg.norm(p5_ref))
+    solids_line = {
+        "workload": sc.state.meta["workload"] + " (cell and dual-face open fractions by 8 samples, "
+                    "the ball's velocity on its faces)",
+        "cells": ss.cells, "steps": SOLID_STEPS,
+        "plain_fp32_solves_per_s": len(t5) / (sum(t5) / 1000.0), "plain_p50_ms": statistics.median(t5),
+        "mixed_solves_per_s": len(t5m) / (sum(t5m) / 1000.0), "mixed_p50_ms": statistics.median(t5m),
+        "iterations": r5["iterations"], "mixed_iterations": r5m["iterations"],
+        "status": [r5["status_name"], r5m["status_name"]],
+        "max_div_ratio": r5["max_div_after"] / max(r5["max_div_before"], 1e-30),
+        "fp64_error": {"plain_fp32": float(np.linalg.norm(p5 - p5_ref)) / nref,
+                       "mixed": float(np.linalg.norm(p5m - p5_ref)) / nref,
+                       "oracle": "float64 MGPCG of the CPU oracle with the same solids, rel-res 1e-12"},
+        "kernels": "face-weighted per-pass V-cycle and CG kernels (the fused column kernels assume uniform weights)",
+    }
+
     # ------------------------------------ secondary: tall-cell 256^2 columns x 1024 rows
     note("tall-cell waves")
     from fluid_b200.tall import TallProjector
@@ -725,6 +773,7 @@ def main():
                                   "v": cycles["v"], "f": cycles["f"],
                                   "note": "v: one V-cycle under PCG (fused column kernels); f: one full cycle "
                                           "under flexible CG (per-pass kernels); same inputs, same tolerance"},
+        "embedded_solids_128x96x128": solids_line,
         "tall_cell_256x256x1024": tall_line,
         "serving": serving,
         "roofline": {"bound": "hbm", "kernel": dom, "workload": "the headline batch (64 instances per launch)",
