@@ -359,18 +359,19 @@ def _solid_samples(points, ramp, sphere):
 
 
 def solid_scene(nx: int = 48, ny: int = 40, nz: int = 44, seed: int = 3, sphere_velocity=(0.0, -0.5, 0.0),
-                open_top: bool = False) -> SolidScene:
+                open_top: bool = False, ball=(0.62, 0.42, 0.5)) -> SolidScene:
     """A dam break over a sloped terrain around a (moving) ball obstacle.
 
     Open fractions are measured the reference's way (pressureFaceData,
     webgpu-uniform-reference.wgsl.ts:530-556): a face's dual cell by 8 samples
     at +-0.4 cell around the face centre, a cell by 8 samples at +-0.25 cell.
     The liquid fills the open part of the dam block (vof = block fraction x open
-    fraction).  The solids' face velocity is the ball's velocity on faces whose
+    fraction); `ball` is the ball's centre as fractions of the lattice (the
+    default sits beside the block, (0.25, 0.35, 0.5) inside it).  The solids' face velocity is the ball's velocity on faces whose
     solid samples are the ball's (weighted by their share), 0 for the terrain."""
     rng = np.random.default_rng(seed)
     ramp = (0.12 * ny, 0.25 * ny / nx)
-    sphere = ((0.62 * nx, 0.42 * ny, 0.5 * nz), 0.16 * min(nx, ny, nz))
+    sphere = ((ball[0] * nx, ball[1] * ny, ball[2] * nz), 0.16 * min(nx, ny, nz))
     off8 = np.array([[(c & 1) * 2 - 1, ((c >> 1) & 1) * 2 - 1, ((c >> 2) & 1) * 2 - 1] for c in range(8)],
                     np.float64)
 

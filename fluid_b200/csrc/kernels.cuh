@@ -412,9 +412,13 @@ __global__ void k_project_init(const InstDev* insts, const Tile* tiles, int ntil
 // One colour pass of red-black Gauss-Seidel on the normalised level operator
 // (mgSmoothColour, mg.wgsl.ts:325-344, without the p_min projection).  With
 // zero_init the pass starts from z = 0 and also clears the other colour.
+//
+// project = 1 (the LCP solve, CM11a Eq. 18 as mgSmoothColour applies it): every
+// updated value is raised to the level's lower bound pmin, and the liquid cells
+// of the other colour are projected too (z = max(z, pmin)).
 template <class TZ, class TR, class TD>
 __global__ void __launch_bounds__(kThreads) k_smooth(const InstDev* insts, const Tile* tiles, int ntiles, int level,
-                                                     int colour, int zero_init) {
+                                                     int colour, int zero_init, int project = 0) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const InstDev& I = insts[tl.inst];
@@ -453,8 +457,12 @@ __global__ void __launch_bounds__(kThreads) k_smooth(const InstDev* insts, const
             s = d4sum6(xm, xp, ym, yp, zm, zp);
           }
           val[k] = lab[i] ? (tof(rhs[i]) + s) / tof(dg[i]) : 0.0f;
+          if (project && lab[i]) val[k] = fmaxf(val[k], L.pmin[i]);
           wr[k] = true;
         } else if (zero_init) {
+          wr[k] = true;
+        } else if (project && lab[i]) {
+          val[k] = fmaxf(tof(z[i]), L.pmin[i]);
           wr[k] = true;
         }
       }

@@ -21,6 +21,7 @@
 #include "../../include/fluid_pp.h"
 #include "colmg.cuh"
 #include "fused.cuh"
+#include "lcp.cuh"
 #include "solids.cuh"
 #include "plan.h"
 #include "types.h"
@@ -264,15 +265,15 @@ void setup_launch(fluid_pp_batch* B, const fluid_pp_solve_opts& o) {
 }
 
 template <class T>
-void smooth_pass(fluid_pp_batch* B, int l, int colour, int zero_init) {
+void smooth_pass(fluid_pp_batch* B, int l, int colour, int zero_init, int project = 0) {
   const List& Ls = B->lvl[l];
   const int g = launch_grid(Ls.n);
   if (l == 0)
     FPP_LAUNCH(B, kPrSmooth0, k_smooth<float, float, T><<<g, kThreads, 0, B->stream>>>(B->d_insts, tl(B, Ls), Ls.n, l,
-                                                                                       colour, zero_init));
+                                                                                       colour, zero_init, project));
   else
-    FPP_LAUNCH(B, kPrSmoothC,
-               k_smooth<T, T, T><<<g, kThreads, 0, B->stream>>>(B->d_insts, tl(B, Ls), Ls.n, l, colour, zero_init));
+    FPP_LAUNCH(B, kPrSmoothC, k_smooth<T, T, T><<<g, kThreads, 0, B->stream>>>(B->d_insts, tl(B, Ls), Ls.n, l, colour,
+                                                                               zero_init, project));
 }
 
 // One V-cycle from grid level `from` down to the coarse block and back
@@ -972,11 +973,9 @@ static fluid_pp_solve_opts default_opts() {
   return o;
 }
 
-template <class T>
-static int batch_project_t(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts& o, bool sync_receipts,
-                           fluid_pp_receipt* receipts) {
+// Per-instance dt and pressure scale into the batch's descriptor table.
+static void push_dts(fluid_pp_batch* B, const float* dts) {
   const int n = int(B->h.size());
-  // per-instance dt into the descriptor table
   for (int k = 0; k < n; ++k) {
     fluid_pp* h = B->h[k];
     const float dt = dts ? dts[k] : h->last_dt;
@@ -996,6 +995,13 @@ static int batch_project_t(fluid_pp_batch* B, const float* dts, const fluid_pp_s
       B->dev_pscale[k] = h->inst.pscale;
     }
   }
+}
+
+template <class T>
+static int batch_project_t(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts& o, bool sync_receipts,
+                           fluid_pp_receipt* receipts) {
+  const int n = int(B->h.size());
+  push_dts(B, dts);
   bool graphed = false;
   if (!B->profiling && B->use_graphs) {
     const int rc = ensure_graphs<T>(B, o);
@@ -1063,6 +1069,124 @@ static int batch_project_t(fluid_pp_batch* B, const float* dts, const fluid_pp_s
 
 static int batch_project(fluid_pp_batch* B, const float* dts, const fluid_pp_solve_opts* opts, bool sync,
                          fluid_pp_receipt* receipts);
+
+// ------------------------------------------------------------ CM11a LCP solve
+// Grid passes of the projected multigrid (one instance: the handle's own batch,
+// every level below the coarsest a grid level).
+template <class T>
+void restrict_pass(fluid_pp_batch* B, int l) {
+  const List& Lr = B->rst[l];
+  if (l == 0)
+    FPP_LAUNCH(B, kPrRestrict0, k_residual_restrict<float, float, T, T><<<launch_grid(Lr.n), kThreads, 0, B->stream>>>(
+                                    B->d_insts, tl(B, Lr), Lr.n, l));
+  else
+    FPP_LAUNCH(B, kPrRestrictC, k_residual_restrict<T, T, T, T><<<launch_grid(Lr.n), kThreads, 0, B->stream>>>(
+                                    B->d_insts, tl(B, Lr), Lr.n, l));
+}
+
+template <class T>
+void prolong_pass(fluid_pp_batch* B, int l) {
+  const List& Ls = B->lvl[l];
+  const int g = launch_grid(Ls.n);
+  if (l == 0)
+    FPP_LAUNCH(B, kPrProlong0, k_prolong<float, T><<<g, kThreads, 0, B->stream>>>(B->d_insts, tl(B, Ls), Ls.n, l));
+  else
+    FPP_LAUNCH(B, kPrProlongC, k_prolong<T, T><<<g, kThreads, 0, B->stream>>>(B->d_insts, tl(B, Ls), Ls.n, l));
+}
+
+// The bound of level l + 1 from level l (mode: k_lcp_bound_down).
+template <class T>
+void bound_pass(fluid_pp_batch* B, int l, int mode) {
+  const List& Lc = B->crs[l + 1];
+  if (l == 0)
+    FPP_LAUNCH(B, kPrRestrict0, k_lcp_bound_down<float><<<launch_grid(Lc.n), kThreads, 0, B->stream>>>(
+                                    B->d_insts, tl(B, Lc), Lc.n, l, mode));
+  else
+    FPP_LAUNCH(B, kPrRestrictC, k_lcp_bound_down<T><<<launch_grid(Lc.n), kThreads, 0, B->stream>>>(
+                                    B->d_insts, tl(B, Lc), Lc.n, l, mode));
+}
+
+template <class T>
+void lcp_coarse_pass(fluid_pp_batch* B, const fluid_pp_lcp_opts& o) {
+  if (B->multi.n)
+    FPP_LAUNCH(B, kPrCoarse, k_lcp_coarse<T><<<B->multi.n, kMaxCoarse, 0, B->stream>>>(
+                                 B->d_insts, il(B, B->multi), o.coarse_sweeps, o.coarse_tol));
+  if (B->single.n)   // a one-level hierarchy: the coarsest is level 0 (float vectors)
+    FPP_LAUNCH(B, kPrCoarse, k_lcp_coarse<float><<<B->single.n, kMaxCoarse, 0, B->stream>>>(
+                                 B->d_insts, il(B, B->single), o.coarse_sweeps, o.coarse_tol));
+}
+
+// vCycle (mg.ts:524-538) from level l with the projected smoother; level l
+// keeps its z, each coarser level starts its correction at zero with the bound
+// of mgDownsampleSubtract on the first constraint_levels levels.
+template <class T>
+void lcp_vcycle_from(fluid_pp_batch* B, int l, const fluid_pp_lcp_opts& o) {
+  const int last = B->maxL - 1;
+  if (l == last) {
+    lcp_coarse_pass<T>(B, o);
+    return;
+  }
+  for (int sw = 0; sw < o.pre_sweeps; ++sw) {
+    smooth_pass<T>(B, l, 0, 0, 1);
+    smooth_pass<T>(B, l, 1, 0, 1);
+  }
+  restrict_pass<T>(B, l);
+  if (l + 1 < last) smooth_pass<T>(B, l + 1, 2, 1);   // the coarse correction starts at zero
+  bound_pass<T>(B, l, l < o.constraint_levels ? 0 : 2);
+  lcp_vcycle_from<T>(B, l + 1, o);
+  prolong_pass<T>(B, l);
+  for (int sw = 0; sw < o.post_sweeps; ++sw) {
+    smooth_pass<T>(B, l, 1, 0, 1);
+    smooth_pass<T>(B, l, 0, 0, 1);
+  }
+}
+
+// fullCycle (mg.ts:539-563): the correction e of p with bound p_min - p; the
+// residual and the bound restricted down every level, the coarsest solved,
+// then per level from the coarsest up the prolongated e starts a V-cycle there.
+template <class T>
+void lcp_fcycle(fluid_pp_batch* B, const fluid_pp_lcp_opts& o) {
+  const Tile* t0 = tl(B, B->l0);
+  const int n0 = B->l0.n, g0 = launch_grid(n0);
+  FPP_LAUNCH(B, kPrInit, k_lcp_fc_begin<<<g0, kThreads, 0, B->stream>>>(B->d_insts, t0, n0));
+  const int last = B->maxL - 1;
+  for (int l = 0; l < last; ++l) {
+    smooth_pass<T>(B, l, 2, 1);   // e = 0 on level l
+    restrict_pass<T>(B, l);
+    bound_pass<T>(B, l, l < o.constraint_levels ? 1 : 2);
+  }
+  lcp_coarse_pass<T>(B, o);
+  for (int l = last - 1; l >= 0; --l) {
+    prolong_pass<T>(B, l);
+    lcp_vcycle_from<T>(B, l, o);
+  }
+  FPP_LAUNCH(B, kPrInit, k_lcp_fc_end<<<g0, kThreads, 0, B->stream>>>(B->d_insts, t0, n0));
+}
+
+template <class T>
+static int lcp_project_t(fluid_pp* pp, float dt, const fluid_pp_lcp_opts& o, fluid_pp_receipt* receipt) {
+  fluid_pp_batch* B = pp->self;
+  push_dts(B, &dt);
+  fluid_pp_solve_opts so = default_opts();
+  so.warm_start = o.warm_start;
+  setup_launch<T>(B, so);
+  const Tile* t0 = tl(B, B->l0);
+  const int n0 = B->l0.n, g0 = launch_grid(n0);
+  FPP_LAUNCH(B, kPrInit, k_lcp_init<<<g0, kThreads, 0, B->stream>>>(B->d_insts, t0, n0, o.warm_start));
+  for (int c = 0; c < o.full_cycles; ++c) lcp_fcycle<T>(B, o);
+  for (int c = 0; c < o.v_cycles; ++c) lcp_vcycle_from<T>(B, 0, o);
+  FPP_LAUNCH(B, kPrTrue, k_lcp_measure<<<g0, kThreads, 0, B->stream>>>(B->d_insts, t0, n0,
+                                                                      o.full_cycles + o.v_cycles));
+  finish_launch_any(B);
+  cudaMemcpyAsync(B->h_ctrl, B->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, B->stream);
+  cudaError_t e = take_launch_error(B);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("lcp: ") + cudaGetErrorString(e));
+  if (receipt) fill_receipt(pp, B->h_ctrl[0], receipt);
+  pp->has_pressure = true;
+  prof_collect(B);
+  return B->h_ctrl[0].status;
+}
 
 // Receipts of a solve that ran in the batch's parts (waits for the batch's stream).
 static int parts_receipts(fluid_pp_batch* B, fluid_pp_receipt* receipts) {
@@ -1556,7 +1680,7 @@ int fluid_pp_upload_solids(fluid_pp* pp, const float* open, const float* fx, con
   const long long N = I.lv[0].n, nx = I.nx, ny = I.ny, nz = I.nz;
   const long long nf[3] = {(nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1)};
   long long floats = N + 2 * (nf[0] + nf[1] + nf[2]);
-  for (int l = 0; l < I.nlev; ++l) floats += 3 * I.lv[l].n;
+  for (int l = 0; l < I.nlev; ++l) floats += 4 * I.lv[l].n;   // face fractions and the LCP bound
   cudaStream_t s = pp->stream;
   if (!pp->solid_mem) {
     cudaError_t e = dev_alloc(reinterpret_cast<void**>(&pp->solid_mem), size_t(floats) * 4);
@@ -1576,6 +1700,8 @@ int fluid_pp_upload_solids(fluid_pp* pp, const float* open, const float* fx, con
   for (int l = 0; l < I.nlev; ++l) {
     I.lv[l].ff = p;
     p += 3 * I.lv[l].n;
+    I.lv[l].pmin = p;
+    p += I.lv[l].n;
   }
   const float* src[3] = {fx, fy, fz};
   const float* vel[3] = {usx, usy, usz};
@@ -1614,6 +1740,39 @@ int fluid_pp_upload_solids(fluid_pp* pp, const float* open, const float* fx, con
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("solids: ") + cudaGetErrorString(e));
   return FLUID_PP_OK;
+}
+
+void fluid_pp_lcp_opts_default(fluid_pp_lcp_opts* o) {
+  if (!o) return;
+  o->full_cycles = 3;
+  o->v_cycles = 4;
+  o->pre_sweeps = 1;
+  o->post_sweeps = 1;
+  o->constraint_levels = 3;
+  o->coarse_sweeps = 4096;
+  o->coarse_tol = 1e-6;
+  o->warm_start = 0;
+}
+
+int fluid_pp_project_lcp(fluid_pp* pp, float dt, const fluid_pp_lcp_opts* opts, fluid_pp_receipt* receipt) {
+  if (!pp) return FLUID_PP_INVALID_ARG;
+  if (!(dt > 0) || !std::isfinite(dt)) return pp->set_error(FLUID_PP_INVALID_ARG, "dt must be positive and finite");
+  if (!pp->has_state) return pp->set_error(FLUID_PP_INVALID_ARG, "state not uploaded");
+  if (!pp->inst.solids)
+    return pp->set_error(FLUID_PP_INVALID_ARG,
+                         "the LCP solve bounds solid cells: upload embedded solids first (fluid_pp_upload_solids)");
+  fluid_pp_lcp_opts o;
+  fluid_pp_lcp_opts_default(&o);
+  if (opts) o = *opts;
+  if (o.full_cycles < 0 || o.v_cycles < 0 || o.full_cycles + o.v_cycles < 1 || o.pre_sweeps < 0 ||
+      o.post_sweeps < 0 || o.constraint_levels < 0 || o.coarse_sweeps < 1 || !(o.coarse_tol >= 0))
+    return pp->set_error(FLUID_PP_INVALID_ARG, "invalid LCP options");
+  cudaSetDevice(pp->cfg.device);
+  switch (pp->cfg.precision) {
+    case FLUID_PP_FP16: return lcp_project_t<__half>(pp, dt, o, receipt);
+    case FLUID_PP_BF16: return lcp_project_t<__nv_bfloat16>(pp, dt, o, receipt);
+    default: return lcp_project_t<float>(pp, dt, o, receipt);
+  }
 }
 
 int fluid_pp_get_level_faces(fluid_pp* pp, int level, float* ff) {

@@ -75,6 +75,7 @@ struct LevelDev {
   void* rhs;          // level right-hand side (level 0: the CG residual r, float)
   void* res;          // scratch in the z type: the pre-smoothed z between the fused down and up steps
   const float* ff;    // embedded solids: open fraction of each cell's +x, +y, +z face (planar, 3 x n), or null
+  float* pmin;        // embedded solids: the LCP solve's lower bound of z (CM11a p_min), or null
 };
 
 struct InstDev {

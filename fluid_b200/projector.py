@@ -167,6 +167,22 @@ class PressureProjector:
             _check(rc, self._h, "project")
         return r.as_dict()
 
+    def project_lcp(self, dt: float, **opts) -> dict:
+        """The CM11a LCP solve (p >= 0 on solid unknowns; needs embedded solids).
+        opts: full_cycles, v_cycles, pre_sweeps, post_sweeps, constraint_levels,
+        coarse_sweeps, coarse_tol, warm_start."""
+        o = _abi.LcpOpts()
+        load().fluid_pp_lcp_opts_default(ctypes.byref(o))
+        for k, v in opts.items():
+            if k not in dict(_abi.LcpOpts._fields_):
+                raise TypeError(f"unknown LCP option {k}")
+            setattr(o, k, type(getattr(o, k))(v))
+        r = Receipt()
+        rc = load().fluid_pp_project_lcp(self._h, float(dt), ctypes.byref(o), ctypes.byref(r))
+        if rc not in (_abi.OK, _abi.NONCONVERGENCE, _abi.NONFINITE):
+            _check(rc, self._h, "project_lcp")
+        return r.as_dict()
+
     def project_async(self, dt: float, **opts):
         o = solve_opts(**opts)
         _check(load().fluid_pp_project_async(self._h, float(dt), ctypes.byref(o)), self._h, "project_async")

@@ -151,6 +151,34 @@ int fluid_pp_upload_state_device(fluid_pp* pp, const float* vof, const float* u,
 int fluid_pp_upload_solids(fluid_pp* pp, const float* open, const float* fx, const float* fy, const float* fz,
                            const float* usx, const float* usy, const float* usz);
 
+/* The CM11a LCP variant (the reference's uniform GPU method,
+ * webgpu-uniform-pressure-multigrid.ts:419-576, .wgsl.ts:155-166, 267-344,
+ * 404-471): a standalone projected multigrid solve of A p = b with p >= 0 on
+ * solid cells that are pressure unknowns (a separating boundary; a domain wall
+ * that should separate is a layer of solid cells, the reference's halo) and
+ * p unbounded elsewhere.  full_cycles full cycles, then v_cycles V-cycles, each
+ * level smoothed by projected red-black Gauss-Seidel; a coarse correction is
+ * bounded by max over the children of (p_min - p) on the first
+ * constraint_levels coarse levels (mgDownsampleSubtract) and unbounded below
+ * them; the coarsest runs projected sweeps until its projected residual is at
+ * most coarse_tol x max|rhs| or coarse_sweeps sweeps.  Needs embedded solids
+ * (fluid_pp_upload_solids).  The receipt's true_rel_residual is the fine
+ * level's projected fixed-point residual over ||b|| (mgMeasureFineResidual),
+ * iterations the number of cycles; the velocities are projected like
+ * fluid_pp_project's. */
+typedef struct fluid_pp_lcp_opts {
+  int full_cycles;        /* 3 (UNIFORM_CM11A_FULL_CYCLES) */
+  int v_cycles;           /* 4 (UNIFORM_CM11A_V_CYCLES) */
+  int pre_sweeps;         /* 1 */
+  int post_sweeps;        /* 1 */
+  int constraint_levels;  /* 3 (UNIFORM_CM11A_CONSTRAINT_LEVELS) */
+  int coarse_sweeps;      /* 4096 (UNIFORM_CM11A_COARSE_SWEEP_CAP) */
+  double coarse_tol;      /* 1e-6 */
+  int warm_start;         /* 1: start from the handle's previous pressure */
+} fluid_pp_lcp_opts;
+void fluid_pp_lcp_opts_default(fluid_pp_lcp_opts* opts);
+int fluid_pp_project_lcp(fluid_pp* pp, float dt, const fluid_pp_lcp_opts* opts, fluid_pp_receipt* receipt);
+
 /* Label -> divergence -> assemble -> MGPCG -> gradient subtract, on the device.
  * Replaces WebGPUUniformPressureMultigrid.encode (webgpu-uniform-pressure-multigrid.ts:327-364)
  * followed by the `project` dispatch (webgpu-uniform-reference.ts:1280-1282);

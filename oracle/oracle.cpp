@@ -651,6 +651,166 @@ void fcycle(const Ctx& c, VWork& wk, const double* r, double* z, int pre, int po
   if (!L0.anchored) meanZero(L0, z);
 }
 
+// ------------------------------------------------------------ CM11a LCP
+// The projected multigrid of the reference's uniform GPU method
+// (webgpu-uniform-pressure-multigrid.ts:419-576, .wgsl.ts:155-166, 267-344,
+// 404-471) on this oracle's face-weighted levels: p >= p_min with p_min = 0 on
+// solid cells that are unknowns (open fraction <= 1e-5), unbounded elsewhere.
+constexpr double kNoBound = -3.402823e38;
+
+struct LcpWork {
+  std::vector<std::vector<double>> z, rhs, res, pmin;
+};
+
+// mgSmoothColour with the projection to the bound (Eq. 18): the colour's liquid
+// cells take max(GS update, p_min), the other colour's liquid cells max(z, p_min).
+void lcpSmooth(const Level& L, const double* rhs, double* z, const double* pmin, int colour) {
+  const int nx = L.n[0], ny = L.n[1], nz = L.n[2];
+  const long sz = long(nx) * ny;
+  for (int zz = 0; zz < nz; ++zz)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        long i = L.idx(x, y, zz);
+        if (((x + y + zz) & 1) != colour) {
+          if (L.label[i]) z[i] = std::max(z[i], pmin[i]);
+          continue;
+        }
+        if (!L.label[i]) { z[i] = 0; continue; }
+        double s = 0;
+        if (x > 0) s += L.fw(0, i - 1) * z[i - 1];
+        if (x + 1 < nx) s += L.fw(0, i) * z[i + 1];
+        if (y > 0) s += L.fw(1, i - nx) * z[i - nx];
+        if (y + 1 < ny) s += L.fw(1, i) * z[i + nx];
+        if (zz > 0) s += L.fw(2, i - sz) * z[i - sz];
+        if (zz + 1 < nz) s += L.fw(2, i) * z[i + sz];
+        z[i] = std::max((rhs[i] + s) / L.diag[i], pmin[i]);
+      }
+}
+
+// Bound of level C from level F: mode 0 max over the children of (p_min - z),
+// 1 max of the children's p_min, 2 unbounded.
+void lcpBoundDown(const Level& F, const Level& C, const double* zf, const double* pf, double* pc, int mode) {
+  for (int z = 0; z < C.n[2]; ++z)
+    for (int y = 0; y < C.n[1]; ++y)
+      for (int x = 0; x < C.n[0]; ++x) {
+        double b = kNoBound;
+        if (mode != 2) {
+          int cc[3] = {x, y, z};
+          for (int corner = 0; corner < 8; ++corner) {
+            int o[3] = {corner & 1, (corner >> 1) & 1, (corner >> 2) & 1};
+            int f[3];
+            for (int a = 0; a < 3; ++a) f[a] = std::min(C.stride[a] * cc[a] + o[a] * (C.stride[a] - 1), F.n[a] - 1);
+            const long k = F.idx(f[0], f[1], f[2]);
+            b = std::max(b, mode == 0 && pf[k] != kNoBound ? pf[k] - zf[k] : pf[k]);
+          }
+        }
+        pc[C.idx(x, y, z)] = b;
+      }
+}
+
+// Projected fixed-point residual of one row (mgMeasureFineResidual / mgSolveCoarsest).
+double lcpRowResidual(double r, double z, double pmin, double diag) {
+  const double gap = std::max(0.0, z - pmin);
+  return (r < 0.0 && -r >= gap * diag) ? gap * diag : std::fabs(r);
+}
+
+// mgSolveCoarsest: projected red-black sweeps from z = 0 until the largest
+// projected residual is at most tol * max|rhs| or after cap sweeps.
+void lcpCoarse(const Level& L, const double* rhs, double* z, const double* pmin, int cap, double tol) {
+  std::fill(z, z + L.cells, 0.0);
+  double bmax = 0;
+  for (long i = 0; i < L.cells; ++i)
+    if (L.label[i]) bmax = std::max(bmax, std::fabs(rhs[i]));
+  std::vector<double> az(L.cells);
+  for (int sweep = 0; sweep < cap; ++sweep) {
+    for (int colour = 0; colour < 2; ++colour)
+      for (int zz = 0; zz < L.n[2]; ++zz)
+        for (int y = 0; y < L.n[1]; ++y)
+          for (int x = 0; x < L.n[0]; ++x) {
+            const long i = L.idx(x, y, zz);
+            if (((x + y + zz) & 1) != colour || !L.label[i] || !(L.diag[i] > 0)) continue;
+            const long sy = L.n[0], sz = long(L.n[0]) * L.n[1];
+            double s = 0;
+            if (x > 0 && L.label[i - 1]) s += L.fw(0, i - 1) * z[i - 1];
+            if (x + 1 < L.n[0] && L.label[i + 1]) s += L.fw(0, i) * z[i + 1];
+            if (y > 0 && L.label[i - sy]) s += L.fw(1, i - sy) * z[i - sy];
+            if (y + 1 < L.n[1] && L.label[i + sy]) s += L.fw(1, i) * z[i + sy];
+            if (zz > 0 && L.label[i - sz]) s += L.fw(2, i - sz) * z[i - sz];
+            if (zz + 1 < L.n[2] && L.label[i + sz]) s += L.fw(2, i) * z[i + sz];
+            z[i] = std::max((rhs[i] + s) / L.diag[i], pmin[i]);
+          }
+    applyLevel(L, z, az.data(), 1);
+    double worst = 0;
+    for (long i = 0; i < L.cells; ++i)
+      if (L.label[i] && L.diag[i] > 0) worst = std::max(worst, lcpRowResidual(rhs[i] - az[i], z[i], pmin[i], L.diag[i]));
+    if (worst <= tol * bmax) break;
+  }
+}
+
+void lcpResidualRestrict(const Ctx& c, LcpWork& wk, int l) {
+  const Level& L = c.lv[l];
+  applyLevel(L, wk.z[l].data(), wk.res[l].data(), 1);
+  for (long i = 0; i < L.cells; ++i) wk.res[l][i] = L.label[i] ? wk.rhs[l][i] - wk.res[l][i] : 0.0;
+  restrictRes(L, c.lv[l + 1], wk.res[l].data(), wk.rhs[l + 1].data());
+}
+
+struct LcpOpts {
+  int pre, post, constraintLevels, coarseSweeps;
+  double coarseTol;
+};
+
+void lcpVcycle(const Ctx& c, LcpWork& wk, int l, const LcpOpts& o) {
+  const int last = (int)c.lv.size() - 1;
+  const Level& L = c.lv[l];
+  if (l == last) { lcpCoarse(L, wk.rhs[l].data(), wk.z[l].data(), wk.pmin[l].data(), o.coarseSweeps, o.coarseTol); return; }
+  for (int s = 0; s < o.pre; ++s) {
+    lcpSmooth(L, wk.rhs[l].data(), wk.z[l].data(), wk.pmin[l].data(), 0);
+    lcpSmooth(L, wk.rhs[l].data(), wk.z[l].data(), wk.pmin[l].data(), 1);
+  }
+  lcpResidualRestrict(c, wk, l);
+  std::fill(wk.z[l + 1].begin(), wk.z[l + 1].end(), 0.0);
+  lcpBoundDown(L, c.lv[l + 1], wk.z[l].data(), wk.pmin[l].data(), wk.pmin[l + 1].data(), l < o.constraintLevels ? 0 : 2);
+  lcpVcycle(c, wk, l + 1, o);
+  prolongAdd(L, c.lv[l + 1], wk.z[l + 1].data(), wk.z[l].data());
+  for (int s = 0; s < o.post; ++s) {
+    lcpSmooth(L, wk.rhs[l].data(), wk.z[l].data(), wk.pmin[l].data(), 1);
+    lcpSmooth(L, wk.rhs[l].data(), wk.z[l].data(), wk.pmin[l].data(), 0);
+  }
+}
+
+double lcpBaseBound(const Ctx& c, long i) {
+  return (c.lv[0].label[i] && !(clamp01(c.open[i]) > 1e-5f)) ? 0.0 : kNoBound;
+}
+
+void lcpFcycle(const Ctx& c, LcpWork& wk, const LcpOpts& o) {
+  const Level& L0 = c.lv[0];
+  const int last = (int)c.lv.size() - 1;
+  std::vector<double> keep(wk.z[0]), az(L0.cells);
+  applyLevel(L0, keep.data(), az.data(), 1);
+  for (long i = 0; i < L0.cells; ++i) {
+    wk.rhs[0][i] = L0.label[i] ? c.b[i] - az[i] : 0.0;
+    const double base = lcpBaseBound(c, i);
+    wk.pmin[0][i] = base == kNoBound ? kNoBound : base - keep[i];
+  }
+  for (int l = 0; l < last; ++l) {
+    std::fill(wk.z[l].begin(), wk.z[l].end(), 0.0);
+    restrictRes(c.lv[l], c.lv[l + 1], wk.rhs[l].data(), wk.rhs[l + 1].data());
+    lcpBoundDown(c.lv[l], c.lv[l + 1], wk.z[l].data(), wk.pmin[l].data(), wk.pmin[l + 1].data(),
+                 l < o.constraintLevels ? 1 : 2);
+  }
+  lcpCoarse(c.lv[last], wk.rhs[last].data(), wk.z[last].data(), wk.pmin[last].data(), o.coarseSweeps, o.coarseTol);
+  for (int l = last - 1; l >= 0; --l) {
+    std::fill(wk.z[l].begin(), wk.z[l].end(), 0.0);
+    prolongAdd(c.lv[l], c.lv[l + 1], wk.z[l + 1].data(), wk.z[l].data());
+    lcpVcycle(c, wk, l, o);
+  }
+  for (long i = 0; i < L0.cells; ++i) {
+    wk.z[0][i] = L0.label[i] ? keep[i] + wk.z[0][i] : 0.0;
+    wk.rhs[0][i] = L0.label[i] ? c.b[i] : 0.0;
+    wk.pmin[0][i] = lcpBaseBound(c, i);
+  }
+}
+
 void buildAll(Ctx& c) {
   labelFine(c);
   buildRhs(c);
@@ -797,6 +957,45 @@ int orc_set_solids(void* h, const float* open, const float* fx, const float* fy,
     else c.us[a].assign(nf[a], 0.0f);
   }
   buildAll(c);
+  return 0;
+}
+
+// The CM11a LCP solve (embedded solids required); info: 0 cycles, 1 max and
+// 2 L2 of the fine projected residual, 3 ||b||_2, 4 bounded rows at their bound.
+int orc_solve_lcp(void* h, int fullCycles, int vCycles, int pre, int post, int constraintLevels, int coarseSweeps,
+                  double coarseTol, double* p, double* info) {
+  Ctx& c = *static_cast<Ctx*>(h);
+  if (!c.solids) return 1;
+  LcpWork wk;
+  for (auto& L : c.lv) {
+    wk.z.emplace_back(L.cells, 0.0);
+    wk.rhs.emplace_back(L.cells, 0.0);
+    wk.res.emplace_back(L.cells, 0.0);
+    wk.pmin.emplace_back(L.cells, kNoBound);
+  }
+  const Level& L0 = c.lv[0];
+  for (long i = 0; i < L0.cells; ++i) {
+    wk.rhs[0][i] = L0.label[i] ? c.b[i] : 0.0;
+    wk.pmin[0][i] = lcpBaseBound(c, i);
+  }
+  const LcpOpts o{pre, post, constraintLevels, coarseSweeps, coarseTol};
+  for (int k = 0; k < fullCycles; ++k) lcpFcycle(c, wk, o);
+  for (int k = 0; k < vCycles; ++k) lcpVcycle(c, wk, 0, o);
+  std::vector<double> az(L0.cells);
+  applyLevel(L0, wk.z[0].data(), az.data(), 1);
+  double mx = 0, ss = 0, bb = 0;
+  long atBound = 0;
+  for (long i = 0; i < L0.cells; ++i) {
+    p[i] = L0.label[i] ? wk.z[0][i] : 0.0;
+    if (!L0.label[i] || !(L0.diag[i] > 0)) continue;
+    const double r = lcpRowResidual(c.b[i] - az[i], wk.z[0][i], wk.pmin[0][i], L0.diag[i]);
+    mx = std::max(mx, r);
+    ss += r * r;
+    bb += c.b[i] * c.b[i];
+    atBound += wk.pmin[0][i] != kNoBound && wk.z[0][i] <= wk.pmin[0][i];
+  }
+  info[0] = fullCycles + vCycles; info[1] = mx; info[2] = std::sqrt(ss); info[3] = std::sqrt(bb);
+  info[4] = double(atBound);
   return 0;
 }
 

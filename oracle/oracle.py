@@ -50,6 +50,8 @@ def lib():
         L.orc_set_solids.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
         L.orc_set_solids.restype = c_int
         L.orc_level_faces.argtypes = [vp, c_int, vp]
+        L.orc_solve_lcp.argtypes = [vp, c_int, c_int, c_int, c_int, c_int, c_int, c_double, vp, vp]
+        L.orc_solve_lcp.restype = c_int
         L.orc_fcycle.argtypes = [vp, vp, vp, c_int, c_int, c_int]
         L.orc_solve_fcg.argtypes = [vp, c_double, c_double, c_int, c_int, c_int, c_int, vp, vp]
         L.orc_solve_fcg.restype = c_int
@@ -180,6 +182,19 @@ class Oracle:
         arrs = [np.ascontiguousarray(a, np.float32) for a in (open_frac, fx, fy, fz)]
         vel = [np.ascontiguousarray(a, np.float32) if a is not None else None for a in (usx, usy, usz)]
         lib().orc_set_solids(self._h, *(_p(a) for a in arrs), *(_p(a) if a is not None else None for a in vel))
+
+    def solve_lcp(self, full_cycles=3, v_cycles=4, pre=1, post=1, constraint_levels=3, coarse_sweeps=4096,
+                  coarse_tol=1e-6):
+        """The CM11a LCP solve (p >= 0 on solid unknowns); returns p and
+        {cycles, max/l2 projected residual, ||b||, rows at their bound}."""
+        nx, ny, nz = self.n
+        p = np.zeros((nz, ny, nx), np.float64)
+        info = np.zeros(5, np.float64)
+        rc = lib().orc_solve_lcp(self._h, full_cycles, v_cycles, pre, post, constraint_levels, coarse_sweeps,
+                                 coarse_tol, _p(p), _p(info))
+        if rc != 0:
+            raise ValueError("the LCP solve needs embedded solids")
+        return p, dict(zip(("cycles", "max_residual", "l2_residual", "b_norm", "at_bound"), info.tolist()))
 
     def level_faces(self, level: int) -> np.ndarray:
         (nx, ny, nz), _, _ = self.level_dims(level)

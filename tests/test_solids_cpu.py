@@ -175,3 +175,25 @@ def test_coarse_face_fractions_are_child_means():
         # every coarse cell halves each axis here: the mean of its 2 x 2 x 2 children
         ch = f0[a].reshape(cz, 2, cy, 2, cx, 2).astype(np.float64).mean(axis=(1, 3, 5))
         np.testing.assert_allclose(f1[a], ch, rtol=0, atol=1e-7)
+
+
+def test_oracle_lcp_holds_the_bound_and_reduces_to_the_linear_solve_without_one():
+    """The CM11a LCP restatement: p >= 0 on solid unknowns, rows at the bound
+    where the linear solve would pull (negative pressure), and with no active
+    bound the projected multigrid converges to the linear solution."""
+    sc = configs.solid_scene(32, 28, 30, seed=3, sphere_velocity=(0.0, -2.0, 0.0), ball=(0.25, 0.35, 0.5))
+    o = _oracle(sc)
+    lab = o.level(0)[0].astype(bool)
+    solid = lab & (np.clip(sc.open, 0, 1) <= 1e-5)
+    p_lin, _ = o.solve_mgpcg(1e-10, 0.0, 400, 1, 1)
+    assert (p_lin[solid] < 0).any()
+    p, info = o.solve_lcp(3, 4)
+    assert p[solid].min() >= 0.0 and info["at_bound"] > 0
+    p2, info2 = o.solve_lcp(3, 20)
+    assert info2["l2_residual"] < info["l2_residual"]
+    quiet = configs.solid_scene(24, 20, 22, seed=4)   # the ball beside the liquid: no bound active
+    oq = _oracle(quiet)
+    pq, iq = oq.solve_lcp(3, 60)
+    ref, _ = oq.solve_mgpcg(1e-12, 0.0, 400, 1, 1)
+    assert np.linalg.norm(pq - ref) <= 1e-3 * np.linalg.norm(ref)
+    assert iq["at_bound"] == 0
