@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -21,6 +22,7 @@
 #include "../../include/fluid_pp.h"
 #include "colmg.cuh"
 #include "fused.cuh"
+#include "extrap.cuh"
 #include "lcp.cuh"
 #include "solids.cuh"
 #include "plan.h"
@@ -75,6 +77,7 @@ struct fluid_pp {
   float last_dt = 0.f;
   fluid_pp_batch* self = nullptr;   // batch of one
   char* solid_mem = nullptr;         // embedded solids: open fractions, face fractions and velocities, level fractions
+  char* ext_mem = nullptr;           // velocity extrapolation: FIM sides and the known-value hierarchy
   long long plan_cells() const { return (long long)cfg.nx * cfg.ny * cfg.nz; }
   int set_error(int code, const std::string& m) {
     err = m;
@@ -1503,6 +1506,7 @@ void fluid_pp_destroy(fluid_pp* pp) {
   cudaSetDevice(pp->cfg.device);
   if (pp->self) fluid_pp_batch_destroy(pp->self);
   dev_release(pp->solid_mem, pp->stream);
+  dev_release(pp->ext_mem, pp->stream);
   dev_release(pp->arena, pp->stream);
   delete pp;
 }
@@ -1739,6 +1743,101 @@ int fluid_pp_upload_solids(fluid_pp* pp, const float* open, const float* fx, con
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("solids: ") + cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_extrapolate_velocity(fluid_pp* pp, long long* filled_faces) {
+  if (!pp) return FLUID_PP_INVALID_ARG;
+  if (!pp->has_state) return pp->set_error(FLUID_PP_INVALID_ARG, "state not uploaded");
+  cudaSetDevice(pp->cfg.device);
+  const InstDev& I = pp->inst;
+  const int nx = I.nx, ny = I.ny, nz = I.nz;
+  const long long n = (long long)nx * ny * nz;
+  // the hierarchy: ceil-halved lattices until the shortest axis is one cell
+  std::vector<std::array<int, 3>> dims;
+  std::array<int, 3> d{nx, ny, nz};
+  while (std::min({d[0], d[1], d[2]}) > 1) {
+    d = {(d[0] + 1) / 2, (d[1] + 1) / 2, (d[2] + 1) / 2};
+    dims.push_back(d);
+  }
+  long long cells = 4 * n;
+  for (const auto& l : dims) cells += 2LL * l[0] * l[1] * l[2];
+  const size_t bytes = size_t(cells) * sizeof(float4) + 16;
+  cudaStream_t s = pp->stream;
+  if (!pp->ext_mem) {
+    const cudaError_t e = dev_alloc(reinterpret_cast<void**>(&pp->ext_mem), bytes);
+    if (e != cudaSuccess) return pp->set_error(FLUID_PP_OOM, std::string("extrapolation: ") + cudaGetErrorString(e));
+  }
+  float4* p = reinterpret_cast<float4*>(pp->ext_mem);
+  ExtDev E{};
+  E.nx = nx;
+  E.ny = ny;
+  E.nz = nz;
+  E.h = I.h;   // cubic cells of edge h (the band is 2 h)
+  E.open_top = I.open_top;
+  E.solids = I.solids;
+  E.vof = I.vof;
+  E.open = I.open;
+  for (int c = 0; c < 3; ++c) E.fv[c] = I.fv[c];
+  E.vel[0] = I.u;
+  E.vel[1] = I.v;
+  E.vel[2] = I.w;
+  for (int k = 0; k < 2; ++k) {
+    E.val[k] = p;
+    p += n;
+    E.dist[k] = p;
+    p += n;
+  }
+  std::vector<float4*> down, up;
+  for (const auto& l : dims) {
+    const long long m = 1LL * l[0] * l[1] * l[2];
+    down.push_back(p);
+    p += m;
+    up.push_back(p);
+    p += m;
+  }
+  E.count = reinterpret_cast<unsigned*>(p);
+  auto grid = [](long long cnt) { return int(std::max(1LL, std::min<long long>((cnt + kThreads - 1) / kThreads, kMaxGrid))); };
+  cudaMemsetAsync(E.count, 0, 16, s);
+  k_ext_seed<<<grid(n), kThreads, 0, s>>>(E);
+  const int passes = std::min(std::max({nx, ny, nz}), 16);
+  for (int k = 0; k < passes; ++k) {
+    const int src = k & 1;
+    k_ext_reset<<<1, 1, 0, s>>>(E.count, 1 - src);
+    k_ext_update<<<grid(n), kThreads, 0, s>>>(E, src);
+  }
+  const int last = passes & 1;
+  const float4* result = E.val[last];
+  if (!dims.empty()) {
+    const float4* finer = E.val[last];
+    std::array<int, 3> fd{nx, ny, nz};
+    for (size_t l = 0; l < dims.size(); ++l) {
+      ExtLevel L{dims[l][0], dims[l][1], dims[l][2], finer, fd[0], fd[1], fd[2], nullptr, down[l]};
+      k_ext_restrict<<<grid(1LL * dims[l][0] * dims[l][1] * dims[l][2]), kThreads, 0, s>>>(L);
+      finer = down[l];
+      fd = dims[l];
+    }
+    const float4* coarser = down.back();
+    std::array<int, 3> cd = dims.back();
+    float4* finest = E.val[1 - last];   // free after the band solve
+    for (int l = int(dims.size()) - 2; l >= -1; --l) {
+      const std::array<int, 3> td = l >= 0 ? dims[l] : std::array<int, 3>{nx, ny, nz};
+      const float4* keep = l >= 0 ? down[l] : E.val[last];
+      float4* out = l >= 0 ? up[l] : finest;
+      ExtLevel L{td[0], td[1], td[2], coarser, cd[0], cd[1], cd[2], keep, out};
+      k_ext_prolong<<<grid(1LL * td[0] * td[1] * td[2]), kThreads, 0, s>>>(L);
+      coarser = out;
+      cd = td;
+    }
+    result = finest;
+  }
+  k_ext_pack<<<grid(n), kThreads, 0, s>>>(E, result, E.count + 2);
+  unsigned got = 0;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&got, E.count + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("extrapolation: ") + cudaGetErrorString(e));
+  if (filled_faces) *filled_faces = got;
   return FLUID_PP_OK;
 }
 

@@ -183,6 +183,13 @@ class PressureProjector:
             _check(rc, self._h, "project_lcp")
         return r.as_dict()
 
+    def extrapolate_velocity(self) -> int:
+        """Extrapolates the handle's face velocities into the air (in place);
+        returns the number of open faces holding a value."""
+        filled = ctypes.c_longlong(0)
+        _check(load().fluid_pp_extrapolate_velocity(self._h, ctypes.byref(filled)), self._h, "extrapolate")
+        return int(filled.value)
+
     def project_async(self, dt: float, **opts):
         o = solve_opts(**opts)
         _check(load().fluid_pp_project_async(self._h, float(dt), ctypes.byref(o)), self._h, "project_async")

@@ -166,6 +166,18 @@ int fluid_pp_upload_solids(fluid_pp* pp, const float* open, const float* fx, con
  * level's projected fixed-point residual over ||b|| (mgMeasureFineResidual),
  * iterations the number of cycles; the velocities are projected like
  * fluid_pp_project's. */
+/* Velocity extrapolation into the air (CM12 Sec. 3.3 / CM11b Secs. 3.3-3.3.1),
+ * replacing WebGPUUniformVelocityExtrapolator.encode
+ * (lib/methods/uniform/webgpu-uniform-velocity-extrapolation.ts:328-395), in
+ * place on the handle's u, v, w (e.g. after fluid_pp_project, before the host's
+ * advection reads them back with fluid_pp_download).  Source faces (open faces
+ * with a liquid side, rho' > 0.5) keep their values; the other open faces take
+ * the Fast Iterative Method's upwind extension within two cells of the liquid
+ * and, farther out, the known-value hierarchy's fill (0 where none reaches);
+ * closed faces (walls, closed solid faces) are left as they are.
+ * *filled_faces (may be NULL) receives the open faces holding a value. */
+int fluid_pp_extrapolate_velocity(fluid_pp* pp, long long* filled_faces);
+
 typedef struct fluid_pp_lcp_opts {
   int full_cycles;        /* 3 (UNIFORM_CM11A_FULL_CYCLES) */
   int v_cycles;           /* 4 (UNIFORM_CM11A_V_CYCLES) */

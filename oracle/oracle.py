@@ -52,6 +52,8 @@ def lib():
         L.orc_level_faces.argtypes = [vp, c_int, vp]
         L.orc_solve_lcp.argtypes = [vp, c_int, c_int, c_int, c_int, c_int, c_int, c_double, vp, vp]
         L.orc_solve_lcp.restype = c_int
+        L.orc_extrapolate.argtypes = [c_int, c_int, c_int, c_double, c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.orc_extrapolate.restype = ctypes.c_long
         L.orc_fcycle.argtypes = [vp, vp, vp, c_int, c_int, c_int]
         L.orc_solve_fcg.argtypes = [vp, c_double, c_double, c_int, c_int, c_int, c_int, vp, vp]
         L.orc_solve_fcg.restype = c_int
@@ -248,3 +250,17 @@ class Oracle:
     def pressure_si(self, p_cells):
         """Dimensional pressure (Pa) from finest-cell-unit pressure."""
         return p_cells * self.rho * self.h / self.dt
+
+
+def extrapolate_velocity(nx, ny, nz, h, open_top, vof, u, v, w, open_frac=None, fx=None, fy=None, fz=None):
+    """The velocity extrapolation restatement (float32, in the device's
+    operation order): returns (u, v, w) extrapolated copies, the open faces
+    holding a value, and the band passes that changed the state."""
+    f32 = lambda a: np.ascontiguousarray(a, np.float32) if a is not None else None
+    vof, u, v, w = (f32(a) for a in (vof, u, v, w))
+    u, v, w = u.copy(), v.copy(), w.copy()
+    open_frac, fx, fy, fz = (f32(a) for a in (open_frac, fx, fy, fz))
+    ran = ctypes.c_int(0)
+    filled = lib().orc_extrapolate(nx, ny, nz, float(h), int(open_top), _p(vof), _p(open_frac), _p(fx), _p(fy),
+                                   _p(fz), _p(u), _p(v), _p(w), ctypes.byref(ran))
+    return (u, v, w), int(filled), int(ran.value)
