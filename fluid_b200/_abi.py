@@ -21,7 +21,7 @@ EXPORTS = (
     "fluid_pp_plan_hierarchy", "fluid_pp_create", "fluid_pp_destroy", "fluid_pp_set_stream",
     "fluid_pp_upload_state", "fluid_pp_upload_state_device", "fluid_pp_project", "fluid_pp_project_async",
     "fluid_pp_upload_solids", "fluid_pp_get_level_faces", "fluid_pp_lcp_opts_default", "fluid_pp_project_lcp",
-    "fluid_pp_extrapolate_velocity",
+    "fluid_pp_extrapolate_velocity", "fluid_pp_tall_set_graphs",
     "fluid_pp_receipt_read", "fluid_pp_download", "fluid_pp_device_arrays", "fluid_pp_last_error",
     "fluid_pp_prepare", "fluid_pp_level_dims", "fluid_pp_get_level", "fluid_pp_get_rhs",
     "fluid_pp_apply_operator", "fluid_pp_apply_vcycle", "fluid_pp_apply_fcycle", "fluid_pp_get_pressure_cells",
@@ -117,6 +117,7 @@ def load():
     L.fluid_pp_lcp_opts_default.restype = None
     L.fluid_pp_project_lcp.argtypes = [vp, ctypes.c_float, vp, vp]
     L.fluid_pp_extrapolate_velocity.argtypes = [vp, vp]
+    L.fluid_pp_tall_set_graphs.argtypes = [vp, ci]
     L.fluid_pp_upload_state_device.argtypes = [vp, vp, vp, vp, vp]
     L.fluid_pp_project.argtypes = [vp, cf, ctypes.POINTER(SolveOpts), ctypes.POINTER(Receipt)]
     L.fluid_pp_project_async.argtypes = [vp, cf, ctypes.POINTER(SolveOpts)]

@@ -1829,6 +1829,14 @@ void fluid_pp_tall_destroy(fluid_pp_tall* T) {
   delete T;
 }
 
+int fluid_pp_tall_set_graphs(fluid_pp_tall* T, int on) {
+  if (!T) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(T->cfg.device);
+  destroy_tall_graphs(T);
+  T->graphs_tried = !on;   // off: no capture is attempted, every launch is direct
+  return FLUID_PP_OK;
+}
+
 int fluid_pp_tall_set_stream(fluid_pp_tall* T, void* stream) {
   if (!T) return FLUID_PP_INVALID_ARG;
   cudaSetDevice(T->cfg.device);

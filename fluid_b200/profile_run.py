@@ -37,6 +37,7 @@ def main() -> int:
     elif args.workload == "tall":
         s = configs.tall_waves()
         tp = TallProjector(s.nx, s.nz, s.fine_ny, s.band, s.bases, s.h, s.rho)
+        tp.set_graphs(False)
         for _ in range(args.solves):
             tp.upload_state(s.vof, s.u, s.v, s.w)
             r = tp.project(s.dt, rel_tol=1e-6)

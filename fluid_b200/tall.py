@@ -103,6 +103,10 @@ class TallProjector:
         except Exception:
             pass
 
+    def set_graphs(self, on: bool):
+        """CUDA graphs of the CG iteration (default on); off for profilers."""
+        _check(load().fluid_pp_tall_set_graphs(self._h, int(bool(on))), self._h, "set_graphs")
+
     def set_stream(self, stream: int):
         _check(load().fluid_pp_tall_set_stream(self._h, ctypes.c_void_p(int(stream))), self._h, "set_stream")
 

@@ -403,6 +403,9 @@ int fluid_pp_tall_plan(int nx, int nz, int fine_ny, int band, const int* bases, 
 int fluid_pp_tall_create(const fluid_pp_tall_config* config, const int* bases, fluid_pp_tall** out);
 void fluid_pp_tall_destroy(fluid_pp_tall* tall);
 int fluid_pp_tall_set_stream(fluid_pp_tall* tall, void* stream);
+/* CUDA graphs of the tall CG iteration (on by default; off: one launch per
+ * kernel, e.g. for profilers, which do not see kernels inside conditional graphs). */
+int fluid_pp_tall_set_graphs(fluid_pp_tall* T, int on);
 /* Packed VOF and owned face velocities from host (or device) memory. */
 int fluid_pp_tall_upload_state(fluid_pp_tall* tall, const float* vof, const float* u, const float* v, const float* w);
 int fluid_pp_tall_upload_state_device(fluid_pp_tall* tall, const float* vof, const float* u, const float* v,
