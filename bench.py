@@ -81,6 +81,22 @@ SERVE_TALL = 2        # resident tall-cell simulations (they share the tall slic
 NCU_FIRST_LAUNCH_BYTES = {"down0": 149.1e6, "up0": 214.4e6, "dirspmv": 250.8e6}
 
 
+def tall_bytes_per_iteration(level_samples, level_storage, sweeps=1) -> float:
+    """Algorithmic bytes of one tall-cell CG iteration: the CG vector kernels on
+    the finest samples (SpMV s + 16 + s, update 6x4, direction 3x4 at float32
+    vectors) plus, on every level l at its storage width s_l (coefficients 3
+    floats and a flag: 16 B, or 8 B at 2-byte storage), (pre + post) RBGS sweeps
+    of 2(s + s + coeff) + s, residual + restriction s + s + coeff + s/8 and
+    prolongation s/8 + 2s per sample."""
+    n0 = level_samples[0]
+    total = n0 * ((4 + 16 + 4) + 6 * 4 + 3 * 4)
+    for n, s in zip(level_samples, level_storage):
+        coeff = 16 if s == 4 else 8
+        per = 2 * sweeps * (2 * (s + s + coeff) + s) + (s + s + coeff + s / 8.0) + (s / 8.0 + 2 * s)
+        total += n * per
+    return total
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -625,6 +641,22 @@ def main():
         return tp_, tt, rec_
     tp, t3, r3 = run_tall("fp32")
     tpm, t3m, r3m = run_tall(args.precision)
+    # solve-level roofline of the tall path: the formula's bytes of every CG
+    # iteration over the whole solve time (setup and receipt included)
+    from fluid_b200.tall import plan_tall_hierarchy
+    tshapes = plan_tall_hierarchy(ts.nx, ts.nz, ts.fine_ny, ts.band, ts.bases)
+    tsamples = [lx * lz * (lb + 2) for lx, _, lz, lb in tshapes]
+    hbm3, kind3 = peaks()
+
+    def tall_roofline(times, rec, storage):
+        alg = tall_bytes_per_iteration(tsamples, storage) * rec["iterations"]
+        gbs = alg / (statistics.mean(times) / 1000.0) / 1e9
+        return {"bound": "hbm", "scope": "whole solve (all kernels, setup and receipt included)",
+                "algorithmic_bytes_per_solve": alg, "achieved": round(gbs, 1), "peak": hbm3,
+                "unit": "GB/s", "frac": round(gbs / hbm3, 4), "peak_kind": kind3}
+    half = 4 if args.precision == "fp32" else 2
+    roof3 = tall_roofline(t3, r3, [4] * len(tsamples))
+    roof3m = tall_roofline(t3m, r3m, [4] + [half, half] + [4] * max(0, len(tsamples) - 3))
     p3m = tpm.pressure()
     tpm.destroy()
     note("tall-cell float64 oracle")
@@ -641,7 +673,9 @@ def main():
         "mixed": {"precision": f"{args.precision} grid levels 1-2, f32 level 0 and block levels",
                   "solves_per_s": len(t3m) / (sum(t3m) / 1000.0), "p50_ms": statistics.median(t3m),
                   "iterations": r3m["iterations"], "status": r3m["status_name"],
-                  "true_rel_residual": r3m["true_rel_residual"]},
+                  "true_rel_residual": r3m["true_rel_residual"], "roofline": roof3m},
+        "roofline": roof3,
+        "level_samples": tsamples,
         "fp64_error": tall_fp64,
     }
 
