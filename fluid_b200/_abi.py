@@ -21,7 +21,8 @@ EXPORTS = (
     "fluid_pp_plan_hierarchy", "fluid_pp_create", "fluid_pp_destroy", "fluid_pp_set_stream",
     "fluid_pp_upload_state", "fluid_pp_upload_state_device", "fluid_pp_project", "fluid_pp_project_async",
     "fluid_pp_upload_solids", "fluid_pp_get_level_faces", "fluid_pp_lcp_opts_default", "fluid_pp_project_lcp",
-    "fluid_pp_extrapolate_velocity", "fluid_pp_tall_set_graphs",
+    "fluid_pp_extrapolate_velocity", "fluid_pp_tall_set_graphs", "fluid_pp_transport_opts_default",
+    "fluid_pp_transport_density", "fluid_pp_set_gamma", "fluid_pp_get_gamma", "fluid_pp_get_vof",
     "fluid_pp_receipt_read", "fluid_pp_download", "fluid_pp_device_arrays", "fluid_pp_last_error",
     "fluid_pp_prepare", "fluid_pp_level_dims", "fluid_pp_get_level", "fluid_pp_get_rhs",
     "fluid_pp_apply_operator", "fluid_pp_apply_vcycle", "fluid_pp_apply_fcycle", "fluid_pp_get_pressure_cells",
@@ -71,6 +72,20 @@ class LcpOpts(ctypes.Structure):
                 ("coarse_tol", ctypes.c_double), ("warm_start", ctypes.c_int)]
 
 
+class TransportOpts(ctypes.Structure):
+    _fields_ = [("gamma_diffusion_iterations", ctypes.c_int), ("sharpening", ctypes.c_int),
+                ("sharpening_mass_return", ctypes.c_int), ("sharpening_strength", ctypes.c_float),
+                ("sharpening_distance", ctypes.c_float)]
+
+
+class TransportReceipt(ctypes.Structure):
+    _fields_ = [("mass_before", ctypes.c_double), ("mass_after", ctypes.c_double), ("rho_min", ctypes.c_float),
+                ("rho_max", ctypes.c_float)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class BatchTuning(ctypes.Structure):
     _fields_ = [("fill_tiles", ctypes.c_int), ("chunk_planes", ctypes.c_int), ("box_shape", ctypes.c_int),
                 ("parts", ctypes.c_int)]
@@ -118,6 +133,12 @@ def load():
     L.fluid_pp_project_lcp.argtypes = [vp, ctypes.c_float, vp, vp]
     L.fluid_pp_extrapolate_velocity.argtypes = [vp, vp]
     L.fluid_pp_tall_set_graphs.argtypes = [vp, ci]
+    L.fluid_pp_transport_opts_default.argtypes = [vp]
+    L.fluid_pp_transport_opts_default.restype = None
+    L.fluid_pp_transport_density.argtypes = [vp, cf, vp, vp]
+    L.fluid_pp_set_gamma.argtypes = [vp, vp]
+    L.fluid_pp_get_gamma.argtypes = [vp, vp]
+    L.fluid_pp_get_vof.argtypes = [vp, vp]
     L.fluid_pp_upload_state_device.argtypes = [vp, vp, vp, vp, vp]
     L.fluid_pp_project.argtypes = [vp, cf, ctypes.POINTER(SolveOpts), ctypes.POINTER(Receipt)]
     L.fluid_pp_project_async.argtypes = [vp, cf, ctypes.POINTER(SolveOpts)]

@@ -107,6 +107,51 @@ def dam_break_32(seed: int = 1) -> GridState:
     return GridState(n, n, n, 1.0 / n, dt, vof, u, v, w, meta={"workload": "dam-break 32^3", "seed": seed})
 
 
+def transport_scene(nx: int = 48, ny: int = 40, nz: int = 44, seed: int = 5, cells_per_step: float = 2.5,
+                    open_top: bool = False, noise: float = 0.15) -> GridState:
+    """Density-transport input: a dam block (x < 0.45, y < 0.5) and a ball of
+    radius 0.18 min(n) in the air (VOF ramps over one cell), and face
+    velocities on every open face as an extrapolated field would have them: a
+    smooth swirl in x-y plus a sinking drift in y, with seeded relative noise,
+    scaled so the fastest face moves cells_per_step cells per step; wall faces
+    are 0.  dt = 1/60 s, h = 1/max(n) m."""
+    rng = np.random.default_rng(seed)
+    n = max(nx, ny, nz)
+    h = 1.0 / n
+    dt = 1.0 / 60.0
+    vof = box_vof(nx, ny, nz, (0, 0, 0), (0.45 * nx, 0.5 * ny, nz))
+    r = 0.18 * min(nx, ny, nz)
+    vof = np.maximum(vof, sphere_vof(nx, ny, nz, (0.7 * nx, 0.72 * ny, 0.5 * nz), r))
+
+    def field(shape, c):
+        z, y, x = np.meshgrid(*(np.arange(k, dtype=np.float64) for k in shape), indexing="ij")
+        X = (x + (0.0 if c == 0 else 0.5)) / nx
+        Y = (y + (0.0 if c == 1 else 0.5)) / ny
+        Z = (z + (0.0 if c == 2 else 0.5)) / nz
+        if c == 0:
+            f = np.sin(np.pi * X) * np.cos(np.pi * Y) * (0.8 + 0.2 * np.cos(2 * np.pi * Z))
+        elif c == 1:
+            f = -np.cos(np.pi * X) * np.sin(np.pi * Y) - 0.4
+        else:
+            f = 0.3 * np.sin(2 * np.pi * X) * np.sin(np.pi * Z)
+        return f * (1.0 + noise * rng.uniform(-1.0, 1.0, size=f.shape))
+
+    u = field((nz, ny, nx + 1), 0)
+    v = field((nz, ny + 1, nx), 1)
+    w = field((nz + 1, ny, nx), 2)
+    u[:, :, 0] = u[:, :, nx] = 0.0
+    v[:, 0, :] = 0.0
+    if not open_top:
+        v[:, ny, :] = 0.0
+    w[0] = w[nz] = 0.0
+    top = max(np.abs(u).max(), np.abs(v).max(), np.abs(w).max())
+    scale = cells_per_step * h / dt / top
+    u, v, w = (np.ascontiguousarray(a * scale, np.float32) for a in (u, v, w))
+    return GridState(nx, ny, nz, h, dt, vof.astype(np.float32), u, v, w, open_top=open_top,
+                     meta={"workload": f"density transport {nx}x{ny}x{nz}", "seed": seed,
+                           "cells_per_step": cells_per_step})
+
+
 def dam_spheres(nx=128, ny=96, nz=128, seed: int = 2, step: int = 0, spheres: int = 16) -> GridState:
     """Dam block holding 40% of the volume plus falling spheres (r in [4,10] cells) in the air.
 

@@ -25,6 +25,7 @@
 #include "extrap.cuh"
 #include "lcp.cuh"
 #include "solids.cuh"
+#include "transport.cuh"
 #include "plan.h"
 #include "types.h"
 
@@ -78,6 +79,7 @@ struct fluid_pp {
   fluid_pp_batch* self = nullptr;   // batch of one
   char* solid_mem = nullptr;         // embedded solids: open fractions, face fractions and velocities, level fractions
   char* ext_mem = nullptr;           // velocity extrapolation: FIM sides and the known-value hierarchy
+  char* tr_mem = nullptr;            // density transport: persistent gamma, scratch fields, fixed-point deposits
   long long plan_cells() const { return (long long)cfg.nx * cfg.ny * cfg.nz; }
   int set_error(int code, const std::string& m) {
     err = m;
@@ -1507,6 +1509,7 @@ void fluid_pp_destroy(fluid_pp* pp) {
   if (pp->self) fluid_pp_batch_destroy(pp->self);
   dev_release(pp->solid_mem, pp->stream);
   dev_release(pp->ext_mem, pp->stream);
+  dev_release(pp->tr_mem, pp->stream);
   dev_release(pp->arena, pp->stream);
   delete pp;
 }
@@ -1838,6 +1841,163 @@ int fluid_pp_extrapolate_velocity(fluid_pp* pp, long long* filled_faces) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("extrapolation: ") + cudaGetErrorString(e));
   if (filled_faces) *filled_faces = got;
+  return FLUID_PP_OK;
+}
+
+// Density transport scratch, allocated on first use: five fields of n floats
+// (gamma, the second gamma, two density fields, the sharpening delta), 3 n
+// fixed-point deposits and the mass partials.  Gamma starts at 1 everywhere.
+struct TrMem {
+  float *gam, *gam2, *r1, *r2, *delta;
+  int* dep;
+  double* part;   // 3 kTrMassGrid partials, then 6 receipt values
+};
+
+TrMem tr_layout(fluid_pp* pp) {
+  const long long n = pp->plan_cells();
+  TrMem M;
+  float* f = reinterpret_cast<float*>(pp->tr_mem);
+  M.gam = f;
+  M.gam2 = f + n;
+  M.r1 = f + 2 * n;
+  M.r2 = f + 3 * n;
+  M.delta = f + 4 * n;
+  M.dep = reinterpret_cast<int*>(f + 5 * n);
+  const size_t off = (size_t(8 * n) * 4 + 15) & ~size_t(15);
+  M.part = reinterpret_cast<double*>(pp->tr_mem + off);
+  return M;
+}
+
+int ensure_transport(fluid_pp* pp) {
+  if (pp->tr_mem) return FLUID_PP_OK;
+  const long long n = pp->plan_cells();
+  const size_t bytes = ((size_t(8 * n) * 4 + 15) & ~size_t(15)) + sizeof(double) * (3 * kTrMassGrid + 6);
+  const cudaError_t e = dev_alloc(reinterpret_cast<void**>(&pp->tr_mem), bytes);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_OOM, std::string("density transport: ") + cudaGetErrorString(e));
+  const TrMem M = tr_layout(pp);
+  k_tr_fill<<<int(std::min<long long>((n + kThreads - 1) / kThreads, kMaxGrid)), kThreads, 0, pp->stream>>>(M.gam, n, 1.0f);
+  return FLUID_PP_OK;
+}
+
+void fluid_pp_transport_opts_default(fluid_pp_transport_opts* o) {
+  if (!o) return;
+  o->gamma_diffusion_iterations = 1;
+  o->sharpening = 1;
+  o->sharpening_mass_return = 1;
+  o->sharpening_strength = 1.0f;
+  o->sharpening_distance = 2.1f;
+}
+
+int fluid_pp_transport_density(fluid_pp* pp, float dt, const fluid_pp_transport_opts* opts,
+                               fluid_pp_transport_receipt* receipt) {
+  if (!pp) return FLUID_PP_INVALID_ARG;
+  if (!(dt > 0.0f) || !std::isfinite(dt)) return pp->set_error(FLUID_PP_INVALID_ARG, "dt must be positive and finite");
+  if (!pp->has_state) return pp->set_error(FLUID_PP_INVALID_ARG, "state not uploaded");
+  if (pp->inst.solids)
+    return pp->set_error(FLUID_PP_UNSUPPORTED, "density transport: handles with embedded solids are not supported");
+  fluid_pp_transport_opts o;
+  fluid_pp_transport_opts_default(&o);
+  if (opts) o = *opts;
+  if (!std::isfinite(o.sharpening_strength) || !std::isfinite(o.sharpening_distance))
+    return pp->set_error(FLUID_PP_INVALID_ARG, "sharpening strength and distance must be finite");
+  // the reference's clamps (webgpu-uniform-reference.ts:374-377)
+  const int iters = std::min(7, std::max(0, o.gamma_diffusion_iterations));
+  const float strength = std::min(2.0f, std::max(0.25f, o.sharpening_strength));
+  const float dist = std::min(3.1f, std::max(0.1f, o.sharpening_distance));
+  cudaSetDevice(pp->cfg.device);
+  int rc = ensure_transport(pp);
+  if (rc != FLUID_PP_OK) return rc;
+  const InstDev& I = pp->inst;
+  const long long n = pp->plan_cells();
+  const TrMem M = tr_layout(pp);
+  TrDev T{I.nx, I.ny, I.nz, I.open_top, I.h, dt, I.u, I.v, I.w};
+  cudaStream_t s = pp->stream;
+  const int g = int(std::min<long long>((n + kThreads - 1) / kThreads, kMaxGrid));
+  float* vof = const_cast<float*>(I.vof);
+  k_tr_mass_part<<<kTrMassGrid, 256, 0, s>>>(vof, n, M.part);
+  k_tr_mass_fold<<<1, 32, 0, s>>>(M.part, kTrMassGrid, M.part + 3 * kTrMassGrid);
+  cudaMemsetAsync(M.dep, 0, sizeof(int) * 3 * size_t(n), s);
+  int* beta = M.dep;
+  k_tr_trace_beta<<<g, kThreads, 0, s>>>(T, M.gam, M.gam2, beta);
+  k_tr_deficit<<<g, kThreads, 0, s>>>(T, vof, M.gam, beta, M.dep + n, M.dep + 2 * n);
+  k_tr_gather<<<g, kThreads, 0, s>>>(T, vof, M.gam2, beta, M.dep + n, M.dep + 2 * n, M.r1, M.gam);
+  float *cr = M.r1, *cg = M.gam, *nr = M.r2, *ng = M.gam2;
+  for (int it = 0; it < iters; ++it)
+    for (int a = 0; a < 3; ++a) {
+      k_tr_diffuse<<<g, kThreads, 0, s>>>(T, a, cr, cg, nr, ng);
+      std::swap(cr, nr);
+      std::swap(cg, ng);
+    }
+  if (cg != M.gam) cudaMemcpyAsync(M.gam, cg, sizeof(float) * size_t(n), cudaMemcpyDeviceToDevice, s);
+  if (o.sharpening) {
+    if (o.sharpening_mass_return) {
+      cudaMemsetAsync(M.dep, 0, sizeof(int) * size_t(n), s);
+      k_tr_sharpen<<<g, kThreads, 0, s>>>(T, cr, strength, nr, M.delta);
+      k_tr_sharpen_scatter<<<g, kThreads, 0, s>>>(T, M.delta, nr, dist, M.dep);
+      k_tr_sharpen_resolve<<<g, kThreads, 0, s>>>(T, nr, M.dep, vof);
+    } else {
+      k_tr_sharpen<<<g, kThreads, 0, s>>>(T, cr, strength, vof, M.delta);
+    }
+  } else {
+    cudaMemcpyAsync(vof, cr, sizeof(float) * size_t(n), cudaMemcpyDeviceToDevice, s);
+  }
+  k_tr_mass_part<<<kTrMassGrid, 256, 0, s>>>(vof, n, M.part);
+  k_tr_mass_fold<<<1, 32, 0, s>>>(M.part, kTrMassGrid, M.part + 3 * kTrMassGrid + 3);
+  double out[6] = {};
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, M.part + 3 * kTrMassGrid, sizeof(out), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("density transport: ") + cudaGetErrorString(e));
+  pp->has_pressure = false;
+  if (receipt) {
+    receipt->mass_before = out[0];
+    receipt->mass_after = out[3];
+    receipt->rho_min = float(out[4]);
+    receipt->rho_max = float(out[5]);
+  }
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_get_vof(fluid_pp* pp, float* vof) {
+  if (!pp || !vof) return FLUID_PP_INVALID_ARG;
+  if (!pp->has_state) return pp->set_error(FLUID_PP_INVALID_ARG, "state not uploaded");
+  cudaSetDevice(pp->cfg.device);
+  cudaError_t e = cudaMemcpyAsync(vof, pp->inst.vof, sizeof(float) * size_t(pp->plan_cells()), cudaMemcpyDeviceToHost,
+                                  pp->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(pp->stream);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("get vof: ") + cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_set_gamma(fluid_pp* pp, const float* gamma) {
+  if (!pp) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(pp->cfg.device);
+  int rc = ensure_transport(pp);
+  if (rc != FLUID_PP_OK) return rc;
+  const long long n = pp->plan_cells();
+  const TrMem M = tr_layout(pp);
+  cudaError_t e = cudaSuccess;
+  if (gamma) {
+    e = cudaMemcpyAsync(M.gam, gamma, sizeof(float) * size_t(n), cudaMemcpyHostToDevice, pp->stream);
+  } else {
+    k_tr_fill<<<int(std::min<long long>((n + kThreads - 1) / kThreads, kMaxGrid)), kThreads, 0, pp->stream>>>(M.gam, n, 1.0f);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(pp->stream);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("set gamma: ") + cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_get_gamma(fluid_pp* pp, float* gamma) {
+  if (!pp || !gamma) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(pp->cfg.device);
+  int rc = ensure_transport(pp);
+  if (rc != FLUID_PP_OK) return rc;
+  const TrMem M = tr_layout(pp);
+  cudaError_t e = cudaMemcpyAsync(gamma, M.gam, sizeof(float) * size_t(pp->plan_cells()), cudaMemcpyDeviceToHost, pp->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(pp->stream);
+  if (e != cudaSuccess) return pp->set_error(FLUID_PP_CUDA, std::string("get gamma: ") + cudaGetErrorString(e));
   return FLUID_PP_OK;
 }
 

@@ -190,6 +190,46 @@ class PressureProjector:
         _check(load().fluid_pp_extrapolate_velocity(self._h, ctypes.byref(filled)), self._h, "extrapolate")
         return int(filled.value)
 
+    def transport_density(self, dt: float, gamma_diffusion_iterations: int = 1, sharpening: bool = True,
+                          mass_return: bool = True, strength: float = 1.0, distance: float = 2.1) -> dict:
+        """CM12 conservative density transport of the handle's VOF and gamma
+        along its face velocities; returns the mass receipt."""
+        o = _abi.TransportOpts()
+        load().fluid_pp_transport_opts_default(ctypes.byref(o))
+        o.gamma_diffusion_iterations = int(gamma_diffusion_iterations)
+        o.sharpening = int(bool(sharpening))
+        o.sharpening_mass_return = int(bool(mass_return))
+        o.sharpening_strength = float(strength)
+        o.sharpening_distance = float(distance)
+        r = _abi.TransportReceipt()
+        _check(load().fluid_pp_transport_density(self._h, float(dt), ctypes.byref(o), ctypes.byref(r)), self._h,
+               "transport_density")
+        return r.as_dict()
+
+    def set_gamma(self, gamma=None):
+        """Sets the persistent gamma ([nz][ny][nx]); None resets it to 1."""
+        if gamma is None:
+            _check(load().fluid_pp_set_gamma(self._h, None), self._h, "set_gamma")
+            return
+        nx, ny, nz = self.dims
+        g = np.ascontiguousarray(gamma, np.float32)
+        if g.size != nx * ny * nz:
+            raise ValueError(f"gamma has {g.size} values; expected {nx * ny * nz}")
+        _check(load().fluid_pp_set_gamma(self._h, ptr(g)), self._h, "set_gamma")
+
+    def vof(self) -> np.ndarray:
+        """The handle's VOF (surface density), [nz][ny][nx]."""
+        nx, ny, nz = self.dims
+        r = np.empty((nz, ny, nx), np.float32)
+        _check(load().fluid_pp_get_vof(self._h, ptr(r)), self._h, "vof")
+        return r
+
+    def gamma(self) -> np.ndarray:
+        nx, ny, nz = self.dims
+        g = np.empty((nz, ny, nx), np.float32)
+        _check(load().fluid_pp_get_gamma(self._h, ptr(g)), self._h, "gamma")
+        return g
+
     def project_async(self, dt: float, **opts):
         o = solve_opts(**opts)
         _check(load().fluid_pp_project_async(self._h, float(dt), ctypes.byref(o)), self._h, "project_async")

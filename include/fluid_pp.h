@@ -178,6 +178,38 @@ int fluid_pp_upload_solids(fluid_pp* pp, const float* open, const float* fx, con
  * *filled_faces (may be NULL) receives the open faces holding a value. */
 int fluid_pp_extrapolate_velocity(fluid_pp* pp, long long* filled_faces);
 
+/* CM12 conservative surface-density transport (Secs. 3.4-3.5), replacing the
+ * dense uniform method's density passes (lib/methods/uniform/
+ * webgpu-uniform-reference.ts:1150-1215; .wgsl.ts:640-858, 1187-1255): the
+ * handle's VOF (surface density rho) and its persistent gamma advance by dt
+ * along the handle's face velocities (extrapolate them first), then gamma
+ * diffuses and the density is sharpened with its local mass return.  The new
+ * rho replaces the handle's VOF, ready for fluid_pp_project.  Options outside
+ * the reference's ranges are clamped as it clamps them.  Handles with
+ * embedded solids: FLUID_PP_UNSUPPORTED. */
+typedef struct fluid_pp_transport_opts {
+  int gamma_diffusion_iterations;   /* 1 (0 .. 7), x -> y -> z Jacobi repetitions */
+  int sharpening;                   /* 1 */
+  int sharpening_mass_return;       /* 1: removed mass carried to the 0.5 contour */
+  float sharpening_strength;        /* 1 (0.25 .. 2) */
+  float sharpening_distance;        /* 2.1 cells (0.1 .. 3.1) */
+} fluid_pp_transport_opts;
+void fluid_pp_transport_opts_default(fluid_pp_transport_opts* opts);
+
+typedef struct fluid_pp_transport_receipt {
+  double mass_before;   /* sum of rho over the cells before the step (float64) */
+  double mass_after;
+  float rho_min, rho_max;   /* after the step */
+} fluid_pp_transport_receipt;
+int fluid_pp_transport_density(fluid_pp* pp, float dt, const fluid_pp_transport_opts* opts,
+                               fluid_pp_transport_receipt* receipt);
+/* The persistent gamma, [nz][ny][nx] host floats (1 everywhere until set;
+ * NULL resets it to 1). */
+int fluid_pp_set_gamma(fluid_pp* pp, const float* gamma);
+/* The handle's VOF (rho), [nz][ny][nx] host floats. */
+int fluid_pp_get_vof(fluid_pp* pp, float* vof);
+int fluid_pp_get_gamma(fluid_pp* pp, float* gamma);
+
 typedef struct fluid_pp_lcp_opts {
   int full_cycles;        /* 3 (UNIFORM_CM11A_FULL_CYCLES) */
   int v_cycles;           /* 4 (UNIFORM_CM11A_V_CYCLES) */

@@ -54,6 +54,9 @@ def lib():
         L.orc_solve_lcp.restype = c_int
         L.orc_extrapolate.argtypes = [c_int, c_int, c_int, c_double, c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp]
         L.orc_extrapolate.restype = ctypes.c_long
+        L.orc_transport.argtypes = [c_int, c_int, c_int, c_double, c_double, c_int, vp, vp, vp, vp, vp, c_int, c_int,
+                                    c_int, c_double, c_double, vp]
+        L.orc_transport.restype = None
         L.orc_fcycle.argtypes = [vp, vp, vp, c_int, c_int, c_int]
         L.orc_solve_fcg.argtypes = [vp, c_double, c_double, c_int, c_int, c_int, c_int, vp, vp]
         L.orc_solve_fcg.restype = c_int
@@ -264,3 +267,27 @@ def extrapolate_velocity(nx, ny, nz, h, open_top, vof, u, v, w, open_frac=None, 
     filled = lib().orc_extrapolate(nx, ny, nz, float(h), int(open_top), _p(vof), _p(open_frac), _p(fx), _p(fy),
                                    _p(fz), _p(u), _p(v), _p(w), ctypes.byref(ran))
     return (u, v, w), int(filled), int(ran.value)
+
+
+def transport_density(nx, ny, nz, h, dt, open_top, vof, u, v, w, gamma=None, diffusion=1, sharpening=True,
+                      mass_return=True, strength=1.0, distance=2.1, stages=False):
+    """The CM12 density transport restatement (float32, in the device's
+    operation order).  Returns (rho, gamma) after the step, and with stages a
+    dict of the intermediate fields (rho and gamma after the gather, rho after
+    the diffusion, the sharpening delta)."""
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    rho = f32(vof).copy().reshape(nz, ny, nx)
+    g = np.ones((nz, ny, nx), np.float32) if gamma is None else f32(gamma).copy().reshape(nz, ny, nx)
+    u, v, w = f32(u), f32(v), f32(w)
+    st = np.empty((4, nz, ny, nx), np.float32) if stages else None
+    # the reference's option clamps (webgpu-uniform-reference.ts:374-377)
+    diffusion = int(min(7, max(0, diffusion)))
+    strength = float(np.float32(min(2.0, max(0.25, strength))))
+    distance = float(np.float32(min(3.1, max(0.1, distance))))
+    lib().orc_transport(nx, ny, nz, float(np.float32(h)), float(np.float32(dt)), int(open_top), _p(u), _p(v), _p(w),
+                        _p(rho), _p(g), diffusion, int(bool(sharpening)), int(bool(mass_return)), strength, distance,
+                        _p(st))
+    if stages:
+        return rho, g, {"rho_gather": st[0], "gamma_gather": st[1], "rho_diffused": st[2], "delta": st[3]}
+    return rho, g
+
