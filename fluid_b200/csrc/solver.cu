@@ -1846,12 +1846,22 @@ int fluid_pp_extrapolate_velocity(fluid_pp* pp, long long* filled_faces) {
 
 // Density transport scratch, allocated on first use: five fields of n floats
 // (gamma, the second gamma, two density fields, the sharpening delta), 3 n
-// fixed-point deposits and the mass partials.  Gamma starts at 1 everywhere.
+// fixed-point deposits, 3 n floats of backward trace offsets, the three
+// velocity transport shells and the mass partials.  Gamma starts at 1
+// everywhere.
 struct TrMem {
-  float *gam, *gam2, *r1, *r2, *delta;
+  float *gam, *gam2, *r1, *r2, *delta, *trace;
+  float* sh[3];
   int* dep;
   double* part;   // 3 kTrMassGrid partials, then 6 receipt values
 };
+
+long long tr_floats(const fluid_pp* pp) {
+  const int nx = pp->cfg.nx, ny = pp->cfg.ny, nz = pp->cfg.nz;
+  long long f = 11LL * nx * ny * nz;
+  for (int c = 0; c < 3; ++c) f += tr_shell_size(nx, ny, nz, c);
+  return f;
+}
 
 TrMem tr_layout(fluid_pp* pp) {
   const long long n = pp->plan_cells();
@@ -1863,7 +1873,13 @@ TrMem tr_layout(fluid_pp* pp) {
   M.r2 = f + 3 * n;
   M.delta = f + 4 * n;
   M.dep = reinterpret_cast<int*>(f + 5 * n);
-  const size_t off = (size_t(8 * n) * 4 + 15) & ~size_t(15);
+  M.trace = f + 8 * n;
+  float* q = f + 11 * n;
+  for (int c = 0; c < 3; ++c) {
+    M.sh[c] = q;
+    q += tr_shell_size(pp->cfg.nx, pp->cfg.ny, pp->cfg.nz, c);
+  }
+  const size_t off = (size_t(tr_floats(pp)) * 4 + 15) & ~size_t(15);
   M.part = reinterpret_cast<double*>(pp->tr_mem + off);
   return M;
 }
@@ -1871,7 +1887,7 @@ TrMem tr_layout(fluid_pp* pp) {
 int ensure_transport(fluid_pp* pp) {
   if (pp->tr_mem) return FLUID_PP_OK;
   const long long n = pp->plan_cells();
-  const size_t bytes = ((size_t(8 * n) * 4 + 15) & ~size_t(15)) + sizeof(double) * (3 * kTrMassGrid + 6);
+  const size_t bytes = ((size_t(tr_floats(pp)) * 4 + 15) & ~size_t(15)) + sizeof(double) * (3 * kTrMassGrid + 6);
   const cudaError_t e = dev_alloc(reinterpret_cast<void**>(&pp->tr_mem), bytes);
   if (e != cudaSuccess) return pp->set_error(FLUID_PP_OOM, std::string("density transport: ") + cudaGetErrorString(e));
   const TrMem M = tr_layout(pp);
@@ -1910,17 +1926,18 @@ int fluid_pp_transport_density(fluid_pp* pp, float dt, const fluid_pp_transport_
   const InstDev& I = pp->inst;
   const long long n = pp->plan_cells();
   const TrMem M = tr_layout(pp);
-  TrDev T{I.nx, I.ny, I.nz, I.open_top, I.h, dt, I.u, I.v, I.w};
+  TrDev T{I.nx, I.ny, I.nz, I.open_top, I.h, dt, I.u, I.v, I.w, {M.sh[0], M.sh[1], M.sh[2]}};
   cudaStream_t s = pp->stream;
   const int g = int(std::min<long long>((n + kThreads - 1) / kThreads, kMaxGrid));
+  for (int c = 0; c < 3; ++c) k_tr_shell<<<g, kThreads, 0, s>>>(T, c, M.sh[c]);
   float* vof = const_cast<float*>(I.vof);
   k_tr_mass_part<<<kTrMassGrid, 256, 0, s>>>(vof, n, M.part);
-  k_tr_mass_fold<<<1, 32, 0, s>>>(M.part, kTrMassGrid, M.part + 3 * kTrMassGrid);
+  k_tr_mass_fold<<<1, 256, 0, s>>>(M.part, kTrMassGrid, M.part + 3 * kTrMassGrid);
   cudaMemsetAsync(M.dep, 0, sizeof(int) * 3 * size_t(n), s);
   int* beta = M.dep;
-  k_tr_trace_beta<<<g, kThreads, 0, s>>>(T, M.gam, M.gam2, beta);
+  k_tr_trace_beta<<<g, kThreads, 0, s>>>(T, M.gam, M.gam2, beta, M.trace);
   k_tr_deficit<<<g, kThreads, 0, s>>>(T, vof, M.gam, beta, M.dep + n, M.dep + 2 * n);
-  k_tr_gather<<<g, kThreads, 0, s>>>(T, vof, M.gam2, beta, M.dep + n, M.dep + 2 * n, M.r1, M.gam);
+  k_tr_gather<<<g, kThreads, 0, s>>>(T, vof, M.gam2, beta, M.dep + n, M.dep + 2 * n, M.trace, M.r1, M.gam);
   float *cr = M.r1, *cg = M.gam, *nr = M.r2, *ng = M.gam2;
   for (int it = 0; it < iters; ++it)
     for (int a = 0; a < 3; ++a) {
@@ -1942,7 +1959,7 @@ int fluid_pp_transport_density(fluid_pp* pp, float dt, const fluid_pp_transport_
     cudaMemcpyAsync(vof, cr, sizeof(float) * size_t(n), cudaMemcpyDeviceToDevice, s);
   }
   k_tr_mass_part<<<kTrMassGrid, 256, 0, s>>>(vof, n, M.part);
-  k_tr_mass_fold<<<1, 32, 0, s>>>(M.part, kTrMassGrid, M.part + 3 * kTrMassGrid + 3);
+  k_tr_mass_fold<<<1, 256, 0, s>>>(M.part, kTrMassGrid, M.part + 3 * kTrMassGrid + 3);
   double out[6] = {};
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess)

@@ -48,7 +48,21 @@ struct TrDev {
   const float* u;   // [nz][ny][nx + 1]
   const float* v;   // [nz][ny + 1][nx]
   const float* w;   // [nz + 1][ny][nx]
+  // The transport shell of each component (k_tr_shell): the face lattice with
+  // face indices 0 .. d + 1 along the component's axis and cell indices
+  // 0 .. d across it, walls and the outer layer 0, so the sampler's eight
+  // corners need no bounds or wall tests (corners outside the lattice carry
+  // weight 0 and read 0, as the reference's sampler sees them).
+  float* sh[3];
 };
+
+__host__ __device__ inline long long tr_shell_sy(int nx, int c) { return c == 0 ? nx + 2 : nx + 1; }
+__host__ __device__ inline long long tr_shell_sz(int nx, int ny, int c) {
+  return tr_shell_sy(nx, c) * (c == 1 ? ny + 2 : ny + 1);
+}
+__host__ __device__ inline long long tr_shell_size(int nx, int ny, int nz, int c) {
+  return tr_shell_sz(nx, ny, c) * (c == 2 ? nz + 2 : nz + 1);
+}
 
 struct TrV3 {
   float x, y, z;
@@ -84,41 +98,47 @@ __device__ __forceinline__ float tr_corner_w(const TrV3& f, int k) {
   return __fmul_rn(__fmul_rn(wx, wy), wz);
 }
 
-// sampleVelocityComponent: trilinear over the component's face lattice, the
-// query clamped to [-1, d - 1] along the axis and [0, d - 1] across it.
-__device__ float tr_sample_c(const TrDev& T, TrV3 p, int c) {
+// sampleVelocityComponent for the three components at once: trilinear over
+// each component's face lattice, the query clamped to [-1, d - 1] along the
+// component's axis (face coordinate, offset 1) and to [0, d - 1] across it
+// (cell coordinate, offset 0.5).  The two coordinates of each axis are shared
+// by the components, the arithmetic per component is the reference's; the
+// corners are read from the transport shell.
+__device__ TrV3 tr_sample(const TrDev& T, TrV3 p) {
   const int d[3] = {T.nx, T.ny, T.nz};
   const float pp[3] = {p.x, p.y, p.z};
-  int base[3];
-  float fr[3];
+  int bc[3], bf[3];
+  float rc[3], rf[3], sc[3], sf[3];   // fractions and 1 - fractions
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const float off = a == c ? 1.0f : 0.5f, lo = a == c ? -1.0f : 0.0f;
-    const float q = tr_clamp(__fsub_rn(pp[a], off), lo, float(d[a] - 1));
-    const float fl = floorf(q);
-    base[a] = int(fl);
-    fr[a] = __fsub_rn(q, fl);
+    const float qc = tr_clamp(__fsub_rn(pp[a], 0.5f), 0.0f, float(d[a] - 1));
+    const float qf = tr_clamp(__fsub_rn(pp[a], 1.0f), -1.0f, float(d[a] - 1));
+    const float fc = floorf(qc), ff = floorf(qf);
+    bc[a] = int(fc);
+    bf[a] = int(ff);
+    rc[a] = __fsub_rn(qc, fc);
+    rf[a] = __fsub_rn(qf, ff);
+    sc[a] = __fsub_rn(1.0f, rc[a]);
+    sf[a] = __fsub_rn(1.0f, rf[a]);
   }
-  float t[8];
+  float out[3];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int o0 = k & 1, o1 = (k >> 1) & 1, o2 = (k >> 2) & 1;
-    const float wx = o0 ? fr[0] : __fsub_rn(1.0f, fr[0]);
-    const float wy = o1 ? fr[1] : __fsub_rn(1.0f, fr[1]);
-    const float wz = o2 ? fr[2] : __fsub_rn(1.0f, fr[2]);
-    const int ix = base[0] + o0 + (c == 0), iy = base[1] + o1 + (c == 1), iz = base[2] + o2 + (c == 2);
-    const int ic = c == 0 ? ix : (c == 1 ? iy : iz);
-    const bool in = ix >= 0 && iy >= 0 && iz >= 0 && ix <= (c == 0 ? T.nx : T.nx - 1) &&
-                    iy <= (c == 1 ? T.ny : T.ny - 1) && iz <= (c == 2 ? T.nz : T.nz - 1);
-    const bool wall = ic == 0 || (ic == d[c] && !(c == 1 && T.open_top));
-    const float val = in && !wall ? tr_face(T, c, ix, iy, iz) : 0.0f;
-    t[k] = __fmul_rn(__fmul_rn(__fmul_rn(wx, wy), wz), val);
+  for (int c = 0; c < 3; ++c) {
+    const long long sy = tr_shell_sy(T.nx, c), sz = tr_shell_sz(T.nx, T.ny, c);
+    const int b0 = c == 0 ? bf[0] + 1 : bc[0], b1 = c == 1 ? bf[1] + 1 : bc[1], b2 = c == 2 ? bf[2] + 1 : bc[2];
+    const float r0 = c == 0 ? rf[0] : rc[0], r1 = c == 1 ? rf[1] : rc[1], r2 = c == 2 ? rf[2] : rc[2];
+    const float s0 = c == 0 ? sf[0] : sc[0], s1 = c == 1 ? sf[1] : sc[1], s2 = c == 2 ? sf[2] : sc[2];
+    const float* q = T.sh[c] + (b0 + sy * b1 + sz * b2);
+    float t[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int o0 = k & 1, o1 = (k >> 1) & 1, o2 = (k >> 2) & 1;
+      const float w = __fmul_rn(__fmul_rn(o0 ? r0 : s0, o1 ? r1 : s1), o2 ? r2 : s2);
+      t[k] = __fmul_rn(w, q[o0 + sy * o1 + sz * o2]);
+    }
+    out[c] = tr_d4sum8(t);
   }
-  return tr_d4sum8(t);
-}
-
-__device__ __forceinline__ TrV3 tr_sample(const TrDev& T, TrV3 p) {
-  return TrV3{tr_sample_c(T, p, 0), tr_sample_c(T, p, 1), tr_sample_c(T, p, 2)};
+  return TrV3{out[0], out[1], out[2]};
 }
 
 __device__ __forceinline__ TrV3 tr_clamp_trace(const TrDev& T, TrV3 p) {
@@ -210,12 +230,35 @@ __device__ __forceinline__ long long tr_corner(const TrDev& T, const TrStencil& 
                  n_ = (long long)(T).nx * (T).ny * (T).nz;                                       \
        i < n_; i += (long long)gridDim.x * blockDim.x)
 
+// The transport shell of component c from the MAC array: face F along the
+// axis (0 .. d + 1), cells across (0 .. d); F = 0, F = d (a wall unless it is
+// the open top) and every index past the lattice hold 0.
+__global__ void k_tr_shell(TrDev T, int c, float* __restrict__ out) {
+  const long long sy = tr_shell_sy(T.nx, c), sz = tr_shell_sz(T.nx, T.ny, c);
+  const long long total = tr_shell_size(T.nx, T.ny, T.nz, c);
+  const int wall_hi = (c == 1 && T.open_top) ? -1 : (c == 0 ? T.nx : (c == 1 ? T.ny : T.nz));
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int iz = int(i / sz), iy = int((i / sy) % (sz / sy)), ix = int(i % sy);
+    const int ic = c == 0 ? ix : (c == 1 ? iy : iz), dc = c == 0 ? T.nx : (c == 1 ? T.ny : T.nz);
+    const bool across = (c != 0 && ix >= T.nx) || (c != 1 && iy >= T.ny) || (c != 2 && iz >= T.nz);
+    const bool zero = across || ic == 0 || ic == wall_hi || ic > dc;
+    out[i] = zero ? 0.0f : tr_face(T, c, ix, iy, iz);
+  }
+}
+
 // Steps 1-3 of CM12 Sec. 3.4: gamma~ at the departure point (conditioned),
 // beta_j += gamma~_i w_ij / sum w.
-__global__ void k_tr_trace_beta(TrDev T, const float* __restrict__ gam, float* __restrict__ gam_adv, int* beta) {
+// The backward offset is kept (trace[3 i ..]) for the gather, which would
+// compute the same bits again.
+__global__ void k_tr_trace_beta(TrDev T, const float* __restrict__ gam, float* __restrict__ gam_adv, int* beta,
+                                float* __restrict__ trace) {
   TR_CELLS(T) {
     const int x = int(i % T.nx), y = int((i / T.nx) % T.ny), z = int(i / ((long long)T.nx * T.ny));
-    const TrStencil S = tr_stencil(T, x, y, z, tr_trace(T, x, y, z, -1.0f));
+    const TrV3 tr = tr_trace(T, x, y, z, -1.0f);
+    trace[3 * i] = tr.x;
+    trace[3 * i + 1] = tr.y;
+    trace[3 * i + 2] = tr.z;
+    const TrStencil S = tr_stencil(T, x, y, z, tr);
     float t[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) t[k] = S.w[k] > 0.0f ? __fmul_rn(S.w[k], gam[tr_corner(T, S, k)]) : 0.0f;
@@ -260,10 +303,11 @@ __global__ void k_tr_deficit(TrDev T, const float* __restrict__ rho, const float
 // Steps 4-5 and the resolve of 6-7.
 __global__ void k_tr_gather(TrDev T, const float* __restrict__ rho, const float* __restrict__ gam_adv,
                             const int* __restrict__ beta, const int* __restrict__ dep_rho,
-                            const int* __restrict__ dep_gam, float* __restrict__ rho_out, float* __restrict__ gam_out) {
+                            const int* __restrict__ dep_gam, const float* __restrict__ trace,
+                            float* __restrict__ rho_out, float* __restrict__ gam_out) {
   TR_CELLS(T) {
     const int x = int(i % T.nx), y = int((i / T.nx) % T.ny), z = int(i / ((long long)T.nx * T.ny));
-    const TrStencil S = tr_stencil(T, x, y, z, tr_trace(T, x, y, z, -1.0f));
+    const TrStencil S = tr_stencil(T, x, y, z, TrV3{trace[3 * i], trace[3 * i + 1], trace[3 * i + 2]});
     const float g = gam_adv[i];
     float rn = 0.0f, gn = 0.0f;
     if (S.total > 1e-9f) {
@@ -475,17 +519,33 @@ __global__ void __launch_bounds__(256) k_tr_mass_part(const float* __restrict__ 
   }
 }
 
-__global__ void k_tr_mass_fold(const double* part, int parts, double* out) {
-  if (threadIdx.x != 0) return;
+// One CTA of 256 threads: thread t folds partials t, t + 256, ... in order,
+// then a fixed shared-memory tree.
+__global__ void __launch_bounds__(256) k_tr_mass_fold(const double* part, int parts, double* out) {
+  __shared__ double ss[256], smin[256], smax[256];
   double s = 0.0, mn = 3.402823e38, mx = -3.402823e38;
-  for (int b = 0; b < parts; ++b) {
+  for (int b = threadIdx.x; b < parts; b += 256) {
     s += part[3 * b];
     mn = fmin(mn, part[3 * b + 1]);
     mx = fmax(mx, part[3 * b + 2]);
   }
-  out[0] = s;
-  out[1] = mn;
-  out[2] = mx;
+  ss[threadIdx.x] = s;
+  smin[threadIdx.x] = mn;
+  smax[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (int(threadIdx.x) < o) {
+      ss[threadIdx.x] += ss[threadIdx.x + o];
+      smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + o]);
+      smax[threadIdx.x] = fmax(smax[threadIdx.x], smax[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = ss[0];
+    out[1] = smin[0];
+    out[2] = smax[0];
+  }
 }
 
 __global__ void k_tr_fill(float* p, long long n, float v) {

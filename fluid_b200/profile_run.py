@@ -11,6 +11,7 @@ mode of the library) and prints one line per solve:
 dam   : 128x96x128 dam break + 16 spheres, fp16 levels (the bench's secondary uniform workload)
 tall  : 256^2 columns x 1024 rows, band 32 (the bench's tall-cell workload)
 batch : the bench's 64 uneven uniform grids in one batched solve
+transport : CM12 density transport steps on the 128x96x128 transport lattice (one launch per kernel always)
 """
 from __future__ import annotations
 
@@ -22,7 +23,7 @@ from .tall import TallProjector
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["dam", "tall", "batch"], default="dam")
+    ap.add_argument("--workload", choices=["dam", "tall", "batch", "transport"], default="dam")
     ap.add_argument("--solves", type=int, default=2)
     ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16", "bf16"])
     args = ap.parse_args()
@@ -42,6 +43,13 @@ def main() -> int:
             tp.upload_state(s.vof, s.u, s.v, s.w)
             r = tp.project(s.dt, rel_tol=1e-6)
             print(r["status_name"], r["iterations"], flush=True)
+    elif args.workload == "transport":
+        s = configs.transport_scene(128, 96, 128, seed=21, cells_per_step=2.5)
+        pp = PressureProjector((s.nx, s.ny, s.nz), s.h, s.rho, s.open_top)
+        pp.upload_state(s.vof, s.u, s.v, s.w)
+        for _ in range(args.solves):
+            r = pp.transport_density(s.dt)
+            print("mass", r["mass_before"], r["mass_after"], flush=True)
     else:
         insts = configs.batch_instances()
         pps = [PressureProjector((s.nx, s.ny, s.nz), s.h, s.rho, precision=args.precision) for s in insts]
