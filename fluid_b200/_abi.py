@@ -23,6 +23,8 @@ EXPORTS = (
     "fluid_pp_upload_solids", "fluid_pp_get_level_faces", "fluid_pp_lcp_opts_default", "fluid_pp_project_lcp",
     "fluid_pp_extrapolate_velocity", "fluid_pp_tall_set_graphs", "fluid_pp_transport_opts_default",
     "fluid_pp_transport_density", "fluid_pp_set_gamma", "fluid_pp_get_gamma", "fluid_pp_get_vof",
+    "fluid_pp_atlas_plan", "fluid_pp_atlas_create", "fluid_pp_atlas_destroy", "fluid_pp_atlas_set_stream",
+    "fluid_pp_atlas_upload", "fluid_pp_atlas_project", "fluid_pp_atlas_download", "fluid_pp_atlas_last_error",
     "fluid_pp_receipt_read", "fluid_pp_download", "fluid_pp_device_arrays", "fluid_pp_last_error",
     "fluid_pp_prepare", "fluid_pp_level_dims", "fluid_pp_get_level", "fluid_pp_get_rhs",
     "fluid_pp_apply_operator", "fluid_pp_apply_vcycle", "fluid_pp_apply_fcycle", "fluid_pp_get_pressure_cells",
@@ -70,6 +72,11 @@ class LcpOpts(ctypes.Structure):
     _fields_ = [("full_cycles", ctypes.c_int), ("v_cycles", ctypes.c_int), ("pre_sweeps", ctypes.c_int),
                 ("post_sweeps", ctypes.c_int), ("constraint_levels", ctypes.c_int), ("coarse_sweeps", ctypes.c_int),
                 ("coarse_tol", ctypes.c_double), ("warm_start", ctypes.c_int)]
+
+
+class AtlasConfig(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("h", ctypes.c_float),
+                ("rho", ctypes.c_float), ("device", ctypes.c_int)]
 
 
 class TransportOpts(ctypes.Structure):
@@ -139,6 +146,16 @@ def load():
     L.fluid_pp_set_gamma.argtypes = [vp, vp]
     L.fluid_pp_get_gamma.argtypes = [vp, vp]
     L.fluid_pp_get_vof.argtypes = [vp, vp]
+    L.fluid_pp_atlas_plan.argtypes = [ci, ci, ci, ci, vp, vp, vp, vp, vp, vp]
+    L.fluid_pp_atlas_create.argtypes = [vp, vp]
+    L.fluid_pp_atlas_destroy.argtypes = [vp]
+    L.fluid_pp_atlas_destroy.restype = None
+    L.fluid_pp_atlas_set_stream.argtypes = [vp, vp]
+    L.fluid_pp_atlas_upload.argtypes = [vp, ci, vp, vp, vp]
+    L.fluid_pp_atlas_project.argtypes = [vp, cf, vp, vp]
+    L.fluid_pp_atlas_download.argtypes = [vp, vp, vp]
+    L.fluid_pp_atlas_last_error.argtypes = [vp]
+    L.fluid_pp_atlas_last_error.restype = ctypes.c_char_p
     L.fluid_pp_upload_state_device.argtypes = [vp, vp, vp, vp, vp]
     L.fluid_pp_project.argtypes = [vp, cf, ctypes.POINTER(SolveOpts), ctypes.POINTER(Receipt)]
     L.fluid_pp_project_async.argtypes = [vp, cf, ctypes.POINTER(SolveOpts)]

@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libfluid_pp.so")
-SOURCES = ["solver.cu", "noalloc.cu", "tall.cu", "plan.cpp", "tall_plan.cpp", "alloc.cpp"]
+SOURCES = ["solver.cu", "noalloc.cu", "tall.cu", "atlas.cu", "plan.cpp", "tall_plan.cpp", "alloc.cpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -152,6 +152,49 @@ def transport_scene(nx: int = 48, ny: int = 40, nz: int = 44, seed: int = 5, cel
                            "cells_per_step": cells_per_step})
 
 
+def atlas_bricks(vof: np.ndarray, dilate: int = 1) -> np.ndarray:
+    """Brick coordinates (8-cell bricks) of an atlas over a dense VOF: every
+    brick holding density, grown by ``dilate`` bricks in the 26-neighbourhood
+    (the bricks a sparse method keeps around the liquid), in key order."""
+    nz, ny, nx = vof.shape
+    gz, gy, gx = nz // 8, ny // 8, nx // 8
+    occ = vof.reshape(gz, 8, gy, 8, gx, 8).max(axis=(1, 3, 5)) > 1e-6
+    grown = occ.copy()
+    for _ in range(dilate):
+        g = grown.copy()
+        for dz in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    sh = np.zeros_like(grown)
+                    zs, ys, xs = (slice(max(0, d), n + min(0, d)) for d, n in ((dz, gz), (dy, gy), (dx, gx)))
+                    zd, yd, xd = (slice(max(0, -d), n + min(0, -d)) for d, n in ((dz, gz), (dy, gy), (dx, gx)))
+                    sh[zd, yd, xd] = grown[zs, ys, xs]
+                    g |= sh
+        grown = g
+    z, y, x = np.nonzero(grown)
+    return np.stack([x, y, z], axis=1).astype(np.int32)
+
+
+def atlas_scene(nx: int = 64, ny: int = 48, nz: int = 56, seed: int = 7, drops: int = 5) -> GridState:
+    """A sparse-atlas workload: a shallow pool (18 % of the height) and
+    ``drops`` falling balls (radius 3-6 cells) in the air, Gaussian velocities
+    (sigma 0.2 m/s) on the faces with a liquid side, dt 1/60.  Most of the
+    domain is air, so the atlas holds a fraction of its bricks."""
+    rng = np.random.default_rng(seed)
+    vof = box_vof(nx, ny, nz, (0, 0, 0), (nx, 0.18 * ny, nz))
+    for _ in range(drops):
+        r = rng.uniform(3.0, 6.0)
+        c = (rng.uniform(r + 2, nx - r - 2), rng.uniform(0.35 * ny + r, ny - r - 2), rng.uniform(r + 2, nz - r - 2))
+        vof = np.maximum(vof, sphere_vof(nx, ny, nz, c, r))
+    vof = vof.astype(np.float32)
+    # no cell exactly at the 0.5 contour (the atlas and the dense labellers differ only there)
+    vof[vof == np.float32(0.5)] = np.float32(0.5001)
+    dt = 1.0 / 60.0
+    u, v, w = velocities(vof, rng, dt, "gauss", 0.2)
+    return GridState(nx, ny, nz, 1.0 / max(nx, ny, nz), dt, vof, u, v, w,
+                     meta={"workload": f"sparse atlas {nx}x{ny}x{nz}: pool + {drops} drops", "seed": seed})
+
+
 def dam_spheres(nx=128, ny=96, nz=128, seed: int = 2, step: int = 0, spheres: int = 16) -> GridState:
     """Dam block holding 40% of the volume plus falling spheres (r in [4,10] cells) in the air.
 

@@ -1,0 +1,1278 @@
+// Sparse brick-atlas pressure projection: the default adaptive method's
+// projection (lib/methods/adaptive-mass/webgpu-sparse-cm12-resident.ts, whose
+// CPU statement is projectSparseAtlasVelocity,
+// lib/methods/adaptive-mass/sparse-atlas-composite-projection.ts:978-1566)
+// for atlases whose bricks all carry the finest resolution.
+//
+// Storage is brick-compact: only the present bricks of 8^3 cells exist; a
+// brick table over the brick grid maps coordinates to slots (-1 absent).
+// Cell i of the level-0 arrays is slot i / 512, local (x, y, z) = i % 512 in
+// x-fastest order.  Faces are stored per brick as the dense MAC layout of the
+// brick (u [8][8][9], v [8][9][8], w [9][8][8]: face f of an axis sits between
+// local cells f - 1 and f), so the face between two present bricks has two
+// copies: the lower brick's f = 8 copy is the one read, both are written.
+//
+// The system is the atlas's (buildLiquidSystem, :978-1168): a cell is liquid
+// iff phi = 0.5 - rho <= 0; every face that is not a domain wall is a row:
+// inside a brick, between present bricks (ports), or to an absent brick inside
+// the domain (sparse-air rows, air phi 0.5); a row with a liquid and an air
+// side weighs 1 / theta, theta = clamp(|phi_l| / max(|phi_l| + |phi_a|, 1e-12),
+// 0.05, 1); b = G^T u over liquid cells; liquid components with no cut row are
+// pure Neumann problems whose mean is projected out (projectNullspace,
+// :1194-1213).  Units: finest cells, so the solve gives p' = p dt / (rho h)
+// and a face takes u - jump / theta (pressureCorrection, :1263-1279); faces of
+// rows without a liquid side become 0 (:1474-1493).
+//
+// The solve is PCG (float64 x, r, d, q and scalars) preconditioned by one
+// V-cycle on a block hierarchy: levels with 4, 2 and 1 cells per brick edge
+// (children 2 x 2 x 2 inside the brick), then levels of one cell per block
+// whose block grid halves (a block exists if any child exists), until at most
+// kAtCoarseMax cells remain, solved by a dense inverse.  Coarse phi is the mean
+// of the children's phi (absent children inside the domain count as air,
+// 0.5); coarse rows are rediscretised by the same rule.  Red-black
+// Gauss-Seidel by global coordinate parity, one sweep before and one after
+// (reversed), restriction R = P^T / 2 with P piecewise constant, so the
+// preconditioner is symmetric.  Jacobi (precond = 0) is the reference's own
+// preconditioner.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "alloc.h"
+#include "../../include/fluid_pp.h"
+#include "device_util.cuh"
+
+namespace fpp {
+namespace atlas {
+
+constexpr int kRes = 8;            // finest cells per brick edge
+constexpr int kCells = kRes * kRes * kRes;
+constexpr int kFaces = (kRes + 1) * kRes * kRes;   // faces per axis per brick
+constexpr int kAT = 256;           // threads per CTA
+constexpr int kAGrid = 148 * 8;    // grid cap
+constexpr int kAtMaxLevels = 16;
+constexpr int kAtCoarseMax = 64;   // the dense coarsest level
+constexpr int kRedGrid = 296;      // fixed reduction grid (partials folded in block order)
+
+struct ALevel {
+  int B;                    // cells per block edge
+  int dx, dy, dz;           // domain in this level's cells
+  int gx, gy, gz;           // block grid
+  int nblocks;
+  long long n;              // nblocks * B^3
+  const int* table;         // gx gy gz -> slot or -1
+  const int* coords;        // nblocks x 3 block coordinates
+  const int* children;      // levels made by halving a block grid: 8 finer slots per block (-1 absent)
+  const int* parent;        // levels whose next coarser level halves the block grid: coarser slot per block
+  uint8_t* label;
+  float* phi;
+  float* diag;
+  float* z;
+  float* rhs;
+  float* res;
+};
+
+struct ACtrl {
+  double bb, thr2, gamma, rr, rr_true;
+  double div[4];     // max |b| and sum b^2 of the faces before and after the projection
+  double red[4];     // last folded reductions
+  double liquid;     // liquid cells
+  int iter, max_iter, done, status, converged;
+};
+
+struct AInst {
+  ALevel lv[kAtMaxLevels];
+  int nlev;
+  int precond;              // 1: V-cycle, 0: Jacobi
+  int nb;                   // bricks
+  float* faces;             // nb x 3 x kFaces, per brick u, v, w
+  double* b;
+  double* x;
+  double* r;
+  double* d;
+  double* q;
+  double* part;             // kRedGrid x 4
+  double* coarse_inv;       // dense inverse of the coarsest level
+  int coarse_m;
+  int ncomp;                // liquid components without a cut row
+  const int* comp_off;      // ncomp + 1
+  const int* comp_cells;    // their level-0 cells
+  double* comp_mean;
+  ACtrl* ctrl;
+};
+
+// ----------------------------------------------------------------- geometry
+struct Cell {
+  int slot, lx, ly, lz;     // block slot and local coordinates
+  int gx, gy, gz;           // level coordinates
+};
+
+__device__ __forceinline__ Cell cell_of(const ALevel& L, long long i) {
+  const int B3 = L.B * L.B * L.B;
+  Cell c;
+  c.slot = int(i / B3);
+  const int loc = int(i - (long long)c.slot * B3);
+  c.lx = loc % L.B;
+  c.ly = (loc / L.B) % L.B;
+  c.lz = loc / (L.B * L.B);
+  c.gx = L.coords[3 * c.slot] * L.B + c.lx;
+  c.gy = L.coords[3 * c.slot + 1] * L.B + c.ly;
+  c.gz = L.coords[3 * c.slot + 2] * L.B + c.lz;
+  return c;
+}
+
+// Neighbour of cell c across its face on axis a, side s (+1 / -1):
+// kWall outside the domain, kAbsent in an absent block inside it, else the
+// neighbour's index.
+constexpr long long kWall = -1, kAbsent = -2;
+
+__device__ __forceinline__ long long neighbour(const ALevel& L, const Cell& c, int a, int s) {
+  int g[3] = {c.gx, c.gy, c.gz};
+  int l[3] = {c.lx, c.ly, c.lz};
+  const int dom[3] = {L.dx, L.dy, L.dz};
+  g[a] += s;
+  if (g[a] < 0 || g[a] >= dom[a]) return kWall;
+  l[a] += s;
+  const int B = L.B;
+  if (l[a] >= 0 && l[a] < B) return (long long)c.slot * B * B * B + l[0] + B * (l[1] + B * l[2]);
+  const int bx = g[0] / B, by = g[1] / B, bz = g[2] / B;
+  if (bx >= L.gx || by >= L.gy || bz >= L.gz) return kAbsent;
+  const int t = L.table[bx + L.gx * (by + L.gy * bz)];
+  if (t < 0) return kAbsent;
+  l[a] = s > 0 ? 0 : B - 1;
+  return (long long)t * B * B * B + l[0] + B * (l[1] + B * l[2]);
+}
+
+__device__ __forceinline__ double theta_d(double lphi, double aphi) {
+  const double a = fabs(lphi);
+  return fmin(1.0, fmax(0.05, a / fmax(a + fabs(aphi), 1e-12)));
+}
+
+// Row weight of cell i's face (a, s) for a liquid i: 0 on walls, 1 to a liquid
+// neighbour, 1 / theta to an air cell or an absent block (phi 0.5).
+__device__ __forceinline__ double face_weight(const ALevel& L, long long i, const Cell& c, int a, int s, long long& j) {
+  j = neighbour(L, c, a, s);
+  if (j == kWall) return 0.0;
+  if (j == kAbsent) return 1.0 / theta_d(L.phi[i], 0.5);
+  if (L.label[j]) return 1.0;
+  return 1.0 / theta_d(L.phi[i], L.phi[j]);
+}
+
+// ------------------------------------------------------------------ kernels
+#define A_CELLS(L)                                                                                   \
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (L).n;                  \
+       i += (long long)gridDim.x * blockDim.x)
+
+// Level 0 labels and phi from the bricks' density.
+__global__ void k_at_label(AInst* I, const float* __restrict__ rho) {
+  const ALevel& L = I->lv[0];
+  A_CELLS(L) {
+    const float ph = 0.5f - rho[i];
+    L.phi[i] = ph;
+    L.label[i] = ph <= 0.0f ? 1 : 0;
+  }
+}
+
+// Coarse phi: mean of the children's phi; children in absent blocks inside the
+// fine domain count as air (0.5), children outside it are left out.
+__global__ void k_at_coarsen(AInst* I, int l) {
+  const ALevel& F = I->lv[l];
+  const ALevel& C = I->lv[l + 1];
+  A_CELLS(C) {
+    const Cell c = cell_of(C, i);
+    double s = 0.0;
+    int cnt = 0;
+    for (int k = 0; k < 8; ++k) {
+      const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
+      const int fx = 2 * c.gx + ox, fy = 2 * c.gy + oy, fz = 2 * c.gz + oz;
+      if (fx >= F.dx || fy >= F.dy || fz >= F.dz) continue;
+      ++cnt;
+      long long fi = -1;
+      if (C.children) {   // one cell per block: the child block
+        const int t = C.children[8 * (long long)c.slot + k];
+        fi = t;           // B == 1 on the finer level too
+      } else {            // children inside the same block
+        const int B = F.B;
+        fi = (long long)c.slot * B * B * B + (2 * c.lx + ox) + B * ((2 * c.ly + oy) + B * (2 * c.lz + oz));
+      }
+      s += fi >= 0 ? double(F.phi[fi]) : 0.5;
+    }
+    const float ph = float(s / double(max(cnt, 1)));
+    C.phi[i] = ph;
+    C.label[i] = ph <= 0.0f ? 1 : 0;
+  }
+}
+
+// Diagonal of every level: the sum of the row weights (1 for air cells, which
+// are identity rows of the smoother).
+__global__ void k_at_diag(AInst* I, int l) {
+  const ALevel& L = I->lv[l];
+  A_CELLS(L) {
+    if (!L.label[i]) {
+      L.diag[i] = 1.0f;
+      continue;
+    }
+    const Cell c = cell_of(L, i);
+    double d = 0.0;
+    long long j;
+    for (int a = 0; a < 3; ++a) {
+      d += face_weight(L, i, c, a, -1, j);
+      d += face_weight(L, i, c, a, +1, j);
+    }
+    L.diag[i] = float(d);
+  }
+}
+
+// Face f (0 .. 8) of a brick's axis-a array at the local tangential
+// coordinates of cell c.
+__device__ __forceinline__ long long face_index(int slot, int a, int lx, int ly, int lz) {
+  long long off;
+  if (a == 0) off = lx + (kRes + 1) * (ly + kRes * lz);
+  else if (a == 1) off = lx + kRes * (ly + (kRes + 1) * lz);
+  else off = lx + kRes * (ly + kRes * lz);
+  return (long long)slot * 3 * kFaces + (long long)a * kFaces + off;
+}
+
+// The stored value of the face on the low side (s = -1) or high side (+1) of
+// level-0 cell c along axis a: a port's value is the lower brick's copy.
+__device__ __forceinline__ float face_value(const AInst* I, const Cell& c, int a, int s) {
+  int l[3] = {c.lx, c.ly, c.lz};
+  if (s > 0) {
+    l[a] += 1;
+    return I->faces[face_index(c.slot, a, l[0], l[1], l[2])];
+  }
+  if (l[a] > 0) return I->faces[face_index(c.slot, a, l[0], l[1], l[2])];
+  // low face of the brick: the lower neighbour's f = 8 copy when it exists
+  const ALevel& L = I->lv[0];
+  int bc[3] = {L.coords[3 * c.slot], L.coords[3 * c.slot + 1], L.coords[3 * c.slot + 2]};
+  if (bc[a] > 0) {
+    bc[a] -= 1;
+    const int t = L.table[bc[0] + L.gx * (bc[1] + L.gy * bc[2])];
+    if (t >= 0) {
+      l[a] = kRes;
+      return I->faces[face_index(t, a, l[0], l[1], l[2])];
+    }
+  }
+  return I->faces[face_index(c.slot, a, l[0], l[1], l[2])];
+}
+
+// b = G^T u on liquid cells: the low face's value minus the high face's over
+// every face that is a row (not a domain wall).
+__global__ void k_at_rhs(AInst* I) {
+  const ALevel& L = I->lv[0];
+  A_CELLS(L) {
+    double b = 0.0;
+    if (L.label[i]) {
+      const Cell c = cell_of(L, i);
+      for (int a = 0; a < 3; ++a) {
+        if (neighbour(L, c, a, -1) != kWall) b += double(face_value(I, c, a, -1));
+        if (neighbour(L, c, a, +1) != kWall) b -= double(face_value(I, c, a, +1));
+      }
+    }
+    I->b[i] = b;
+  }
+}
+
+// (A v)_i for a liquid level-0 cell, float64.
+__device__ __forceinline__ double apply0(const AInst* I, const double* v, long long i) {
+  const ALevel& L = I->lv[0];
+  const Cell c = cell_of(L, i);
+  double s = double(L.diag[i]) * v[i];
+  for (int a = 0; a < 3; ++a)
+    for (int sd = -1; sd <= 1; sd += 2) {
+      const long long j = neighbour(L, c, a, sd);
+      if (j >= 0 && L.label[j]) s -= v[j];
+    }
+  return s;
+}
+
+// Fixed-grid float64 reductions: per-CTA tree sums into part[4 blockIdx + k],
+// folded by one CTA in CTA order.
+template <int K>
+__device__ __forceinline__ void block_reduce(double (&v)[K], double* part) {
+  __shared__ double sh[K][kAT];
+#pragma unroll
+  for (int k = 0; k < K; ++k) sh[k][threadIdx.x] = v[k];
+  __syncthreads();
+  for (int o = kAT / 2; o > 0; o >>= 1) {
+    if (int(threadIdx.x) < o)
+#pragma unroll
+      for (int k = 0; k < K; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) part[4 * blockIdx.x + k] = sh[k][0];
+}
+
+__global__ void __launch_bounds__(kAT) k_at_fold(AInst* I, int K, int slot0) {
+  __shared__ double sh[4][kAT];
+  double v[4] = {0, 0, 0, 0};
+  for (int b = threadIdx.x; b < kRedGrid; b += kAT)
+    for (int k = 0; k < K; ++k) v[k] += I->part[4 * b + k];
+  for (int k = 0; k < 4; ++k) sh[k][threadIdx.x] = v[k];
+  __syncthreads();
+  for (int o = kAT / 2; o > 0; o >>= 1) {
+    if (int(threadIdx.x) < o)
+      for (int k = 0; k < 4; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < K; ++k) I->ctrl->red[slot0 + k] = sh[k][0];
+}
+
+// Nullspace: mean of each unanchored component (one CTA each, fixed order),
+// then the subtraction.
+__global__ void __launch_bounds__(kAT) k_at_comp_mean(AInst* I, const double* v) {
+  __shared__ double sh[kAT];
+  const int c = blockIdx.x;
+  const int b0 = I->comp_off[c], b1 = I->comp_off[c + 1];
+  double s = 0.0;
+  for (int k = b0 + threadIdx.x; k < b1; k += kAT) s += v[I->comp_cells[k]];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = kAT / 2; o > 0; o >>= 1) {
+    if (int(threadIdx.x) < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) I->comp_mean[c] = sh[0] / double(b1 - b0);
+}
+
+__global__ void k_at_comp_sub(AInst* I, double* v) {
+  const int c = blockIdx.y;
+  const int b0 = I->comp_off[c], b1 = I->comp_off[c + 1];
+  const double m = I->comp_mean[c];
+  for (int k = b0 + blockIdx.x * kAT + threadIdx.x; k < b1; k += gridDim.x * kAT) v[I->comp_cells[k]] -= m;
+}
+
+// ------------------------------------------------------------ the V-cycle
+// One colour of red-black Gauss-Seidel on level l (from a zero guess when
+// zero_init: the first colour then reads no neighbours).
+__global__ void k_at_smooth(AInst* I, int l, int colour, int zero_init) {
+  const ALevel& L = I->lv[l];
+  A_CELLS(L) {
+    if (!L.label[i]) {
+      if (zero_init) L.z[i] = 0.0f;
+      continue;
+    }
+    const Cell c = cell_of(L, i);
+    if (((c.gx + c.gy + c.gz) & 1) != colour) {
+      if (zero_init && colour == 0) L.z[i] = 0.0f;
+      continue;
+    }
+    float s = L.rhs[i];
+    if (!(zero_init && colour == 0)) {
+      for (int a = 0; a < 3; ++a)
+        for (int sd = -1; sd <= 1; sd += 2) {
+          const long long j = neighbour(L, c, a, sd);
+          if (j >= 0 && L.label[j]) s += L.z[j];
+        }
+    }
+    L.z[i] = s / L.diag[i];
+  }
+}
+
+// res = rhs - A z on level l.
+__global__ void k_at_residual(AInst* I, int l) {
+  const ALevel& L = I->lv[l];
+  A_CELLS(L) {
+    if (!L.label[i]) {
+      L.res[i] = 0.0f;
+      continue;
+    }
+    const Cell c = cell_of(L, i);
+    float s = L.rhs[i] - L.diag[i] * L.z[i];
+    for (int a = 0; a < 3; ++a)
+      for (int sd = -1; sd <= 1; sd += 2) {
+        const long long j = neighbour(L, c, a, sd);
+        if (j >= 0 && L.label[j]) s += L.z[j];
+      }
+    L.res[i] = s;
+  }
+}
+
+// Finer level index of child k (0 .. 7) of coarse cell c, -1 if none.
+__device__ __forceinline__ long long child_of(const ALevel& F, const ALevel& C, const Cell& c, int k) {
+  const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
+  if (2 * c.gx + ox >= F.dx || 2 * c.gy + oy >= F.dy || 2 * c.gz + oz >= F.dz) return -1;
+  if (C.children) return C.children[8 * (long long)c.slot + k];
+  const int B = F.B;
+  return (long long)c.slot * B * B * B + (2 * c.lx + ox) + B * ((2 * c.ly + oy) + B * (2 * c.lz + oz));
+}
+
+// rhs_c = 1/2 sum of the liquid children's residuals (R = P^T / 2).
+__global__ void k_at_restrict(AInst* I, int l) {
+  const ALevel& F = I->lv[l];
+  const ALevel& C = I->lv[l + 1];
+  A_CELLS(C) {
+    if (!C.label[i]) {
+      C.rhs[i] = 0.0f;
+      continue;
+    }
+    const Cell c = cell_of(C, i);
+    float s = 0.0f;
+    for (int k = 0; k < 8; ++k) {
+      const long long f = child_of(F, C, c, k);
+      if (f >= 0) s += F.res[f];   // res is 0 on air children
+    }
+    C.rhs[i] = 0.5f * s;
+  }
+}
+
+// z_f += z_c on liquid fine cells (P piecewise constant).
+__global__ void k_at_prolong(AInst* I, int l) {
+  const ALevel& F = I->lv[l];
+  const ALevel& C = I->lv[l + 1];
+  A_CELLS(F) {
+    if (!F.label[i]) continue;
+    long long ci;
+    if (F.parent) {
+      const Cell f = cell_of(F, i);   // B == 1: the block is the cell
+      ci = F.parent[f.slot];
+    } else {
+      const Cell f = cell_of(F, i);
+      const int B = C.B;
+      ci = (long long)f.slot * B * B * B + (f.lx / 2) + B * ((f.ly / 2) + B * (f.lz / 2));
+    }
+    if (ci >= 0 && C.label[ci]) F.z[i] += C.z[ci];
+  }
+}
+
+// Dense inverse of the coarsest level's operator (one CTA, shared memory):
+// air cells are identity rows; a level with no cut row gets the rank-one
+// term mean(diag) / m 1 1^T so the inverse is SPD.
+__global__ void __launch_bounds__(1024) k_at_coarse_factor(AInst* I) {
+  const ALevel& L = I->lv[I->nlev - 1];
+  const int m = int(L.n);
+  __shared__ double A[kAtCoarseMax * kAtCoarseMax];
+  __shared__ double prow[kAtCoarseMax], pcol[kAtCoarseMax];
+  __shared__ int anchored;
+  if (threadIdx.x == 0) anchored = 0;
+  for (int e = threadIdx.x; e < m * m; e += blockDim.x) A[e] = 0.0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    if (!L.label[i]) {
+      A[i * m + i] = 1.0;
+      atomicOr(&anchored, 1);
+      continue;
+    }
+    const Cell c = cell_of(L, i);
+    A[i * m + i] = L.diag[i];
+    for (int a = 0; a < 3; ++a)
+      for (int sd = -1; sd <= 1; sd += 2) {
+        const long long j = neighbour(L, c, a, sd);
+        if (j == kAbsent) atomicOr(&anchored, 1);
+        if (j >= 0 && L.label[j]) A[i * m + j] = -1.0;
+      }
+  }
+  __syncthreads();
+  if (!anchored) {
+    __shared__ double add;
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int i = 0; i < m; ++i) s += A[i * m + i];
+      add = s / double(m) / double(m);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) A[e] += add;
+    __syncthreads();
+  }
+  gauss_jordan_inplace(A, m, prow, pcol);
+  for (int e = threadIdx.x; e < m * m; e += blockDim.x) I->coarse_inv[e] = A[e];
+}
+
+__global__ void k_at_coarse_apply(AInst* I) {
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[I->nlev - 1];
+  const int m = int(L.n);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int i = warp; i < m; i += nw) {
+    double s = 0.0;
+    for (int j = lane; j < m; j += 32) s += I->coarse_inv[i * m + j] * (L.label[j] ? double(L.rhs[j]) : 0.0);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) L.z[i] = L.label[i] ? float(s) : 0.0f;
+  }
+}
+
+// Level-0 rhs of the V-cycle from the CG residual (float).
+__global__ void k_at_vin(AInst* I) {
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[0];
+  A_CELLS(L) L.rhs[i] = L.label[i] ? float(I->r[i]) : 0.0f;
+}
+
+// ------------------------------------------------------------ CG kernels
+// z as a float64 vector (for the nullspace projection of z before the dot):
+// the preconditioned residual is written to q temporarily.
+__global__ void k_at_zvec(AInst* I) {
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[0];
+  A_CELLS(L) {
+    I->q[i] = L.label[i] ? (I->precond ? double(L.z[i]) : I->r[i] / double(L.diag[i])) : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(kAT) k_at_dot_rq(AInst* I) {
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[0];
+  double v[1] = {0.0};
+  A_CELLS(L) if (L.label[i]) v[0] += I->r[i] * I->q[i];
+  block_reduce<1>(v, I->part);
+}
+
+__global__ void __launch_bounds__(kAT) k_at_rr(AInst* I) {
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[0];
+  double v[1] = {0.0};
+  A_CELLS(L) if (L.label[i]) v[0] += I->r[i] * I->r[i];
+  block_reduce<1>(v, I->part);
+}
+
+// beta and d = z + beta d (first iteration: d = z); z is in q.
+__global__ void k_at_dir(AInst* I) {
+  ACtrl* C = I->ctrl;
+  if (C->done) return;
+  const double gnew = C->red[0];
+  const double beta = C->iter == 0 ? 0.0 : gnew / C->gamma;
+  const ALevel& L = I->lv[0];
+  A_CELLS(L) I->d[i] = L.label[i] ? I->q[i] + beta * I->d[i] : 0.0;
+}
+
+__global__ void k_at_set_gamma(AInst* I) {
+  ACtrl* C = I->ctrl;
+  if (C->done) return;
+  C->gamma = C->red[0];
+}
+
+// q = A d, delta = d . q
+__global__ void __launch_bounds__(kAT) k_at_spmv(AInst* I) {
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[0];
+  double v[1] = {0.0};
+  A_CELLS(L) {
+    double q = 0.0;
+    if (L.label[i]) {
+      q = apply0(I, I->d, i);
+      v[0] += I->d[i] * q;
+    }
+    I->q[i] = q;
+  }
+  block_reduce<1>(v, I->part);
+}
+
+// x += alpha d, r -= alpha q, rr = r . r
+__global__ void __launch_bounds__(kAT) k_at_update(AInst* I) {
+  ACtrl* C = I->ctrl;
+  if (C->done) return;
+  const double alpha = C->gamma / C->red[0];
+  const ALevel& L = I->lv[0];
+  double v[1] = {0.0};
+  A_CELLS(L) {
+    if (!L.label[i]) continue;
+    I->x[i] += alpha * I->d[i];
+    const double r = I->r[i] - alpha * I->q[i];
+    I->r[i] = r;
+    v[0] += r * r;
+  }
+  block_reduce<1>(v, I->part);
+}
+
+// r = b - A x (float64), rr = r . r
+__global__ void __launch_bounds__(kAT) k_at_true(AInst* I) {
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[0];
+  double v[1] = {0.0};
+  A_CELLS(L) {
+    if (!L.label[i]) continue;
+    const double r = I->b[i] - apply0(I, I->x, i);
+    I->r[i] = r;
+    v[0] += r * r;
+  }
+  block_reduce<1>(v, I->part);
+}
+
+// After an update: count the iteration, stop on the tolerance (the
+// recursive float64 residual, as projectSparseAtlasVelocity does), the cap,
+// or a non-finite residual.
+__global__ void k_at_check(AInst* I) {
+  ACtrl* C = I->ctrl;
+  if (C->done) return;
+  const double rr = C->red[0];
+  C->iter += 1;
+  C->rr = rr;
+  if (!(rr == rr) || fabs(rr) > 1e300) {
+    C->done = 1;
+    C->status = FLUID_PP_NONFINITE;
+    return;
+  }
+  if (rr <= C->thr2) {
+    C->done = 1;
+    C->converged = 1;
+    C->status = FLUID_PP_OK;
+    return;
+  }
+  if (C->iter >= C->max_iter) {
+    C->done = 1;
+    C->status = FLUID_PP_NONCONVERGENCE;
+  }
+}
+
+__global__ void k_at_init(AInst* I, double thr_rel, double thr_abs, int max_iter) {
+  ACtrl* C = I->ctrl;
+  const double bb = C->red[0];
+  C->bb = bb;
+  C->liquid = C->red[1];
+  const double t = fmax(thr_abs, thr_rel * sqrt(bb));
+  C->thr2 = t * t;
+  C->iter = 0;
+  C->max_iter = max_iter;
+  C->done = bb <= C->thr2 ? 1 : 0;
+  C->converged = C->done;
+  C->status = FLUID_PP_OK;
+  C->rr = bb;
+  C->rr_true = bb;
+}
+
+__global__ void __launch_bounds__(kAT) k_at_bb(AInst* I) {
+  const ALevel& L = I->lv[0];
+  double v[2] = {0.0, 0.0};
+  A_CELLS(L) {
+    if (!L.label[i]) continue;
+    v[0] += I->b[i] * I->b[i];
+    v[1] += 1.0;
+  }
+  block_reduce<2>(v, I->part);
+}
+
+__global__ void k_at_start(AInst* I) {
+  const ALevel& L = I->lv[0];
+  A_CELLS(L) {
+    I->x[i] = 0.0;
+    I->r[i] = L.label[i] ? I->b[i] : 0.0;
+    I->d[i] = 0.0;
+  }
+}
+
+// Faces: u -= jump / theta on rows with a liquid side, 0 on rows without;
+// domain walls keep their values.  Both copies of a port are written.
+__global__ void k_at_project(AInst* I) {
+  const ALevel& L = I->lv[0];
+  A_CELLS(L) {
+    const Cell c = cell_of(L, i);
+    for (int a = 0; a < 3; ++a) {
+      // the cell's high face on axis a; low faces of bricks whose lower
+      // neighbour is absent are handled by the cell itself below
+      for (int sd = -1; sd <= 1; sd += 2) {
+        const int lcoord = a == 0 ? c.lx : (a == 1 ? c.ly : c.lz);
+        if (sd < 0 && lcoord > 0) continue;   // interior low faces are the lower cell's high faces
+        const long long j = neighbour(L, c, a, sd);
+        if (j == kWall) continue;
+        if (sd < 0 && j >= 0) continue;       // a port: the lower brick's cell writes it
+        const bool li = L.label[i] != 0;
+        const bool lj = j >= 0 && L.label[j] != 0;
+        float val;
+        int lc[3] = {c.lx, c.ly, c.lz};
+        if (sd > 0) lc[a] += 1;
+        const long long fi = face_index(c.slot, a, lc[0], lc[1], lc[2]);
+        const float u0 = face_value(I, c, a, sd);
+        if (!li && !lj) {
+          val = 0.0f;
+        } else {
+          // jump = p(pos) - p(neg) over liquid terms; the cell is the neg side for sd > 0
+          const double pi = li ? I->x[i] : 0.0;
+          const double pj = lj ? I->x[j] : 0.0;
+          const double jump = sd > 0 ? pj - pi : pi - pj;
+          double th = 1.0;
+          if (li != lj) {
+            const double lphi = li ? L.phi[i] : L.phi[j];
+            const double aphi = j < 0 ? 0.5 : (li ? L.phi[j] : L.phi[i]);
+            th = theta_d(lphi, aphi);
+          }
+          val = float(double(u0) - jump / th);
+        }
+        I->faces[fi] = val;
+        if (sd > 0 && j >= 0 && lc[a] == kRes) {   // the port's copy in the upper brick
+          const Cell cj = cell_of(L, j);
+          int lu[3] = {cj.lx, cj.ly, cj.lz};
+          I->faces[face_index(cj.slot, a, lu[0], lu[1], lu[2])] = val;
+        }
+      }
+    }
+  }
+}
+
+// Divergence receipt over liquid cells: max |b| and sum b^2 of the current faces.
+__global__ void __launch_bounds__(kAT) k_at_div(AInst* I) {
+  const ALevel& L = I->lv[0];
+  double v[2] = {0.0, 0.0};
+  A_CELLS(L) {
+    if (!L.label[i]) continue;
+    const Cell c = cell_of(L, i);
+    double b = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      if (neighbour(L, c, a, -1) != kWall) b += double(face_value(I, c, a, -1));
+      if (neighbour(L, c, a, +1) != kWall) b -= double(face_value(I, c, a, +1));
+    }
+    v[0] = fmax(v[0], fabs(b));
+    v[1] += b * b;
+  }
+  // max and sum in one tree: the max slot folds with max
+  __shared__ double sm[kAT], ss[kAT];
+  sm[threadIdx.x] = v[0];
+  ss[threadIdx.x] = v[1];
+  __syncthreads();
+  for (int o = kAT / 2; o > 0; o >>= 1) {
+    if (int(threadIdx.x) < o) {
+      sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
+      ss[threadIdx.x] += ss[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    I->part[4 * blockIdx.x] = sm[0];
+    I->part[4 * blockIdx.x + 1] = ss[0];
+  }
+}
+
+__global__ void k_at_div_fold(AInst* I, int slot0) {
+  if (threadIdx.x != 0) return;
+  double m = 0.0, s = 0.0;
+  for (int b = 0; b < kRedGrid; ++b) {
+    m = fmax(m, I->part[4 * b]);
+    s += I->part[4 * b + 1];
+  }
+  I->ctrl->div[slot0] = m;
+  I->ctrl->div[slot0 + 1] = s;
+}
+
+__global__ void k_at_pressure(AInst* I, float* out, double pscale) {
+  const ALevel& L = I->lv[0];
+  A_CELLS(L) out[i] = L.label[i] ? float(I->x[i] * pscale) : 0.0f;
+}
+
+#undef A_CELLS
+
+}  // namespace atlas
+}  // namespace fpp
+
+// ==================================================================== host
+using namespace fpp;
+using namespace fpp::atlas;
+
+namespace {
+
+struct HostLevel {
+  int B, dx, dy, dz, gx, gy, gz;
+  std::vector<int> table, coords, children, parent;
+  long long n() const { return (long long)coords.size() / 3 * B * B * B; }
+};
+
+// The block hierarchy: levels with 4, 2, 1 cells per brick edge, then block
+// grids halved until at most kAtCoarseMax cells remain.
+std::vector<HostLevel> plan_levels(int nx, int ny, int nz, const std::vector<int>& coords) {
+  std::vector<HostLevel> lv;
+  HostLevel L0;
+  L0.B = kRes;
+  L0.dx = nx;
+  L0.dy = ny;
+  L0.dz = nz;
+  L0.gx = nx / kRes;
+  L0.gy = ny / kRes;
+  L0.gz = nz / kRes;
+  L0.coords = coords;
+  L0.table.assign(size_t(L0.gx) * L0.gy * L0.gz, -1);
+  for (size_t s = 0; s < coords.size() / 3; ++s)
+    L0.table[coords[3 * s] + size_t(L0.gx) * (coords[3 * s + 1] + size_t(L0.gy) * coords[3 * s + 2])] = int(s);
+  lv.push_back(std::move(L0));
+  while (lv.back().n() > kAtCoarseMax && int(lv.size()) < kAtMaxLevels) {
+    const HostLevel& F = lv.back();
+    HostLevel C;
+    if (F.B > 1) {
+      C = F;
+      C.B = F.B / 2;
+      C.dx = F.dx / 2;
+      C.dy = F.dy / 2;
+      C.dz = F.dz / 2;
+      C.children.clear();
+      C.parent.clear();
+    } else {
+      C.B = 1;
+      C.dx = (F.dx + 1) / 2;
+      C.dy = (F.dy + 1) / 2;
+      C.dz = (F.dz + 1) / 2;
+      C.gx = C.dx;
+      C.gy = C.dy;
+      C.gz = C.dz;
+      C.table.assign(size_t(C.gx) * C.gy * C.gz, -1);
+      const int nf = int(F.coords.size() / 3);
+      std::vector<int> parent(nf);
+      for (int s = 0; s < nf; ++s) {
+        const int cx = F.coords[3 * s] / 2, cy = F.coords[3 * s + 1] / 2, cz = F.coords[3 * s + 2] / 2;
+        int& t = C.table[cx + size_t(C.gx) * (cy + size_t(C.gy) * cz)];
+        if (t < 0) {
+          t = int(C.coords.size() / 3);
+          C.coords.insert(C.coords.end(), {cx, cy, cz});
+        }
+        parent[s] = t;
+      }
+      const int nc = int(C.coords.size() / 3);
+      C.children.assign(size_t(8) * nc, -1);
+      for (int s = 0; s < nf; ++s) {
+        const int k = (F.coords[3 * s] & 1) | ((F.coords[3 * s + 1] & 1) << 1) | ((F.coords[3 * s + 2] & 1) << 2);
+        C.children[8 * size_t(parent[s]) + k] = s;
+      }
+      lv.back().parent = std::move(parent);
+    }
+    lv.push_back(std::move(C));
+  }
+  return lv;
+}
+
+// Liquid components without a cut row (no face to an air cell or an absent
+// brick): union-find over the level-0 cells, CSR of their cells.
+void plan_components(const HostLevel& L, const std::vector<float>& rho, std::vector<int>& off, std::vector<int>& cells) {
+  const long long n = L.n();
+  std::vector<int> par(n);
+  std::iota(par.begin(), par.end(), 0);
+  std::function<int(int)> find = [&](int a) {
+    while (par[a] != a) {
+      par[a] = par[par[a]];
+      a = par[a];
+    }
+    return a;
+  };
+  auto liquid = [&](long long i) { return 0.5f - rho[i] <= 0.0f; };
+  std::vector<uint8_t> anchored(n, 0);
+  for (long long i = 0; i < n; ++i) {
+    if (!liquid(i)) continue;
+    const int slot = int(i / kCells), loc = int(i % kCells);
+    const int l[3] = {loc % kRes, (loc / kRes) % kRes, loc / (kRes * kRes)};
+    const int g[3] = {L.coords[3 * slot] * kRes + l[0], L.coords[3 * slot + 1] * kRes + l[1],
+                      L.coords[3 * slot + 2] * kRes + l[2]};
+    const int dom[3] = {L.dx, L.dy, L.dz};
+    for (int a = 0; a < 3; ++a)
+      for (int s = -1; s <= 1; s += 2) {
+        int gg[3] = {g[0], g[1], g[2]};
+        gg[a] += s;
+        if (gg[a] < 0 || gg[a] >= dom[a]) continue;   // wall
+        const int t = L.table[gg[0] / kRes + size_t(L.gx) * (gg[1] / kRes + size_t(L.gy) * (gg[2] / kRes))];
+        if (t < 0) {
+          anchored[i] = 1;   // sparse-air row
+          continue;
+        }
+        const long long j = (long long)t * kCells + (gg[0] % kRes) + kRes * ((gg[1] % kRes) + kRes * (gg[2] % kRes));
+        if (!liquid(j)) {
+          anchored[i] = 1;
+          continue;
+        }
+        const int ra = find(int(i)), rb = find(int(j));
+        if (ra != rb) par[std::max(ra, rb)] = std::min(ra, rb);
+      }
+  }
+  std::vector<uint8_t> root_anchor(n, 0);
+  for (long long i = 0; i < n; ++i)
+    if (liquid(i) && anchored[i]) root_anchor[find(int(i))] = 1;
+  std::vector<int> comp_of(n, -1);
+  std::vector<int> roots;
+  for (long long i = 0; i < n; ++i) {
+    if (!liquid(i)) continue;
+    const int r = find(int(i));
+    if (root_anchor[r]) continue;
+    if (comp_of[r] < 0) {
+      comp_of[r] = int(roots.size());
+      roots.push_back(r);
+    }
+  }
+  off.assign(roots.size() + 1, 0);
+  for (long long i = 0; i < n; ++i)
+    if (liquid(i) && !root_anchor[find(int(i))]) ++off[comp_of[find(int(i))] + 1];
+  for (size_t c = 0; c < roots.size(); ++c) off[c + 1] += off[c];
+  cells.assign(off.back(), 0);
+  std::vector<int> fill(off.begin(), off.end() - 1);
+  for (long long i = 0; i < n; ++i)
+    if (liquid(i) && !root_anchor[find(int(i))]) cells[fill[comp_of[find(int(i))]]++] = int(i);
+}
+
+int grid_n(long long n) { return int(std::max(1LL, std::min<long long>((n + kAT - 1) / kAT, kAGrid))); }
+
+}  // namespace
+
+struct fluid_pp_atlas {
+  fluid_pp_atlas_config cfg{};
+  cudaStream_t stream = nullptr;
+  std::string err;
+  char* arena = nullptr;   // level arrays, CG vectors, tables, faces
+  size_t arena_bytes = 0;
+  AInst inst{};
+  AInst* d_inst = nullptr;
+  ACtrl* h_ctrl = nullptr;  // pinned
+  int nb = 0;
+  float dt = 0.0f;
+  bool has_state = false;
+  int set_error(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+};
+
+namespace {
+
+std::mutex g_atlas_err_mutex;
+std::string g_atlas_err;
+
+int global_error(int code, const std::string& m) {
+  std::lock_guard<std::mutex> lock(g_atlas_err_mutex);
+  g_atlas_err = m;
+  return code;
+}
+
+void proj(fluid_pp_atlas* A, double* v) {
+  if (A->inst.ncomp == 0) return;
+  k_at_comp_mean<<<A->inst.ncomp, kAT, 0, A->stream>>>(A->d_inst, v);
+  k_at_comp_sub<<<dim3(8, A->inst.ncomp), kAT, 0, A->stream>>>(A->d_inst, v);
+}
+
+void vcycle(fluid_pp_atlas* A) {
+  const AInst& I = A->inst;
+  cudaStream_t s = A->stream;
+  k_at_vin<<<grid_n(I.lv[0].n), kAT, 0, s>>>(A->d_inst);
+  const int last = I.nlev - 1;
+  for (int l = 0; l < last; ++l) {
+    const int g = grid_n(I.lv[l].n);
+    k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 1);
+    k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 1, 0);
+    k_at_residual<<<g, kAT, 0, s>>>(A->d_inst, l);
+    k_at_restrict<<<grid_n(I.lv[l + 1].n), kAT, 0, s>>>(A->d_inst, l);
+  }
+  k_at_coarse_apply<<<1, 1024, 0, s>>>(A->d_inst);
+  for (int l = last - 1; l >= 0; --l) {
+    const int g = grid_n(I.lv[l].n);
+    k_at_prolong<<<g, kAT, 0, s>>>(A->d_inst, l);
+    k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 1, 0);
+    k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 0);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fluid_pp_atlas_last_error(fluid_pp_atlas* A) {
+  if (A) return A->err.c_str();
+  std::lock_guard<std::mutex> lock(g_atlas_err_mutex);
+  return g_atlas_err.c_str();
+}
+
+int fluid_pp_atlas_plan(int nx, int ny, int nz, int nbricks, const int* coords, const float* density,
+                        int* level_count, long long* level_cells, int* components, int* component_cells) {
+  if (nx <= 0 || ny <= 0 || nz <= 0 || nx % kRes || ny % kRes || nz % kRes || nbricks <= 0 || !coords || !level_count)
+    return global_error(FLUID_PP_INVALID_ARG, "atlas plan: bad arguments");
+  const int gx = nx / kRes, gy = ny / kRes, gz = nz / kRes;
+  std::vector<int> c(coords, coords + 3 * size_t(nbricks));
+  std::vector<uint8_t> seen(size_t(gx) * gy * gz, 0);
+  for (int b = 0; b < nbricks; ++b) {
+    const int x = c[3 * b], y = c[3 * b + 1], z = c[3 * b + 2];
+    if (x < 0 || y < 0 || z < 0 || x >= gx || y >= gy || z >= gz)
+      return global_error(FLUID_PP_INVALID_ARG, "a brick lies outside the domain");
+    uint8_t& m = seen[x + size_t(gx) * (y + size_t(gy) * z)];
+    if (m) return global_error(FLUID_PP_INVALID_ARG, "a brick is given twice");
+    m = 1;
+  }
+  const std::vector<HostLevel> lv = plan_levels(nx, ny, nz, c);
+  *level_count = int(lv.size());
+  if (level_cells)
+    for (size_t l = 0; l < lv.size(); ++l) level_cells[l] = lv[l].n();
+  if (density && (components || component_cells)) {
+    std::vector<float> rho(density, density + size_t(nbricks) * kCells);
+    std::vector<int> off, cells;
+    plan_components(lv[0], rho, off, cells);
+    if (components) *components = int(off.size()) - 1;
+    if (component_cells) *component_cells = int(cells.size());
+  }
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_atlas_create(const fluid_pp_atlas_config* cfg, fluid_pp_atlas** out) {
+  if (!cfg || !out) return FLUID_PP_INVALID_ARG;
+  *out = nullptr;
+  if (cfg->nx <= 0 || cfg->ny <= 0 || cfg->nz <= 0 || cfg->nx % kRes || cfg->ny % kRes || cfg->nz % kRes)
+    return global_error(FLUID_PP_INVALID_ARG, "atlas domain must be positive multiples of 8 cells per axis");
+  if (!(cfg->h > 0.0f) || !(cfg->rho > 0.0f) || !std::isfinite(cfg->h) || !std::isfinite(cfg->rho))
+    return global_error(FLUID_PP_INVALID_ARG, "h and rho must be positive and finite");
+  const long long bricks = (long long)(cfg->nx / kRes) * (cfg->ny / kRes) * (cfg->nz / kRes);
+  if (bricks > (1LL << 22)) return global_error(FLUID_PP_INVALID_ARG, "brick grid too large");
+  if (cudaSetDevice(cfg->device) != cudaSuccess) return global_error(FLUID_PP_CUDA, "cannot select the device");
+  auto A = std::make_unique<fluid_pp_atlas>();
+  A->cfg = *cfg;
+  cudaError_t e = dev_alloc(reinterpret_cast<void**>(&A->d_inst), sizeof(AInst));
+  if (e == cudaSuccess) e = host_alloc(reinterpret_cast<void**>(&A->h_ctrl), sizeof(ACtrl));
+  if (e != cudaSuccess) {
+    dev_release(A->d_inst, A->stream);
+    return global_error(FLUID_PP_OOM, std::string("atlas: ") + cudaGetErrorString(e));
+  }
+  *out = A.release();
+  return FLUID_PP_OK;
+}
+
+void fluid_pp_atlas_destroy(fluid_pp_atlas* A) {
+  if (!A) return;
+  cudaSetDevice(A->cfg.device);
+  dev_release(A->arena, A->stream);
+  dev_release(A->d_inst, A->stream);
+  host_release(A->h_ctrl, A->stream);
+  delete A;
+}
+
+int fluid_pp_atlas_set_stream(fluid_pp_atlas* A, void* stream) {
+  if (!A) return FLUID_PP_INVALID_ARG;
+  cudaSetDevice(A->cfg.device);
+  const cudaStream_t next = static_cast<cudaStream_t>(stream);
+  const cudaError_t e = order_streams(A->stream, next);
+  if (e != cudaSuccess) return A->set_error(FLUID_PP_CUDA, cudaGetErrorString(e));
+  A->stream = next;
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_atlas_upload(fluid_pp_atlas* A, int nbricks, const int* coords, const float* density, const float* faces) {
+  if (!A || nbricks <= 0 || !coords || !density || !faces) return FLUID_PP_INVALID_ARG;
+  const int gx = A->cfg.nx / kRes, gy = A->cfg.ny / kRes, gz = A->cfg.nz / kRes;
+  std::vector<int> c(coords, coords + 3 * size_t(nbricks));
+  std::vector<uint8_t> seen(size_t(gx) * gy * gz, 0);
+  for (int s = 0; s < nbricks; ++s) {
+    const int x = c[3 * s], y = c[3 * s + 1], z = c[3 * s + 2];
+    if (x < 0 || y < 0 || z < 0 || x >= gx || y >= gy || z >= gz)
+      return A->set_error(FLUID_PP_INVALID_ARG, "a brick lies outside the domain");
+    uint8_t& m = seen[x + size_t(gx) * (y + size_t(gy) * z)];
+    if (m) return A->set_error(FLUID_PP_INVALID_ARG, "a brick is given twice");
+    m = 1;
+  }
+  const long long n0 = (long long)nbricks * kCells;
+  std::vector<float> rho(density, density + n0);
+  for (long long i = 0; i < n0; ++i)
+    if (!std::isfinite(rho[i])) return A->set_error(FLUID_PP_NONFINITE, "non-finite density");
+  std::vector<HostLevel> lv = plan_levels(A->cfg.nx, A->cfg.ny, A->cfg.nz, c);
+  if (lv.back().n() > kAtCoarseMax)
+    return A->set_error(FLUID_PP_UNSUPPORTED, "the brick hierarchy does not reach a small coarsest level");
+  std::vector<int> comp_off, comp_cells;
+  plan_components(lv[0], rho, comp_off, comp_cells);
+  const int ncomp = int(comp_off.size()) - 1;
+  if (ncomp > 65535) return A->set_error(FLUID_PP_UNSUPPORTED, "more than 65535 liquid components without air");
+  // arena: per level 1 + 5 x 4 bytes per cell and its int tables; level-0
+  // CG vectors (b x r d q float64), density, faces, partials, components
+  size_t bytes = 0;
+  auto up = [](size_t v) { return (v + 255) / 256 * 256; };
+  for (const HostLevel& L : lv) {
+    const size_t n = size_t(L.n());
+    bytes += up(n) + 5 * up(4 * n) + up(4 * L.table.size()) + up(4 * L.coords.size()) + up(4 * L.children.size()) +
+             up(4 * L.parent.size());
+  }
+  bytes += 5 * up(8 * size_t(n0)) + up(4 * size_t(n0)) + up(4 * size_t(nbricks) * 3 * kFaces);
+  bytes += up(8 * 4 * kRedGrid) + up(8 * kAtCoarseMax * kAtCoarseMax) + up(4 * comp_off.size()) +
+           up(4 * comp_cells.size()) + up(8 * std::max(ncomp, 1)) + up(sizeof(ACtrl));
+  cudaSetDevice(A->cfg.device);
+  cudaStream_t s = A->stream;
+  if (bytes > A->arena_bytes) {
+    dev_release(A->arena, s);
+    A->arena_bytes = 0;
+    const cudaError_t e = dev_alloc(reinterpret_cast<void**>(&A->arena), bytes);
+    if (e != cudaSuccess) return A->set_error(FLUID_PP_OOM, std::string("atlas arena: ") + cudaGetErrorString(e));
+    A->arena_bytes = bytes;
+  }
+  char* p = A->arena;
+  auto take = [&](size_t b) {
+    void* r = p;
+    p += up(b);
+    return r;
+  };
+  AInst& I = A->inst;
+  I = AInst{};
+  I.nlev = int(lv.size());
+  I.nb = nbricks;
+  cudaError_t e = cudaSuccess;
+  auto put = [&](const void* src, size_t b) -> void* {
+    void* d = take(b);
+    if (b && e == cudaSuccess) e = cudaMemcpyAsync(d, src, b, cudaMemcpyHostToDevice, s);
+    return d;
+  };
+  for (int l = 0; l < I.nlev; ++l) {
+    const HostLevel& H = lv[l];
+    ALevel& L = I.lv[l];
+    const size_t n = size_t(H.n());
+    L.B = H.B;
+    L.dx = H.dx;
+    L.dy = H.dy;
+    L.dz = H.dz;
+    L.gx = H.gx;
+    L.gy = H.gy;
+    L.gz = H.gz;
+    L.nblocks = int(H.coords.size() / 3);
+    L.n = (long long)n;
+    L.label = static_cast<uint8_t*>(take(n));
+    L.phi = static_cast<float*>(take(4 * n));
+    L.diag = static_cast<float*>(take(4 * n));
+    L.z = static_cast<float*>(take(4 * n));
+    L.rhs = static_cast<float*>(take(4 * n));
+    L.res = static_cast<float*>(take(4 * n));
+    L.table = static_cast<const int*>(put(H.table.data(), 4 * H.table.size()));
+    L.coords = static_cast<const int*>(put(H.coords.data(), 4 * H.coords.size()));
+    L.children = H.children.empty() ? nullptr : static_cast<const int*>(put(H.children.data(), 4 * H.children.size()));
+    L.parent = H.parent.empty() ? nullptr : static_cast<const int*>(put(H.parent.data(), 4 * H.parent.size()));
+  }
+  I.b = static_cast<double*>(take(8 * size_t(n0)));
+  I.x = static_cast<double*>(take(8 * size_t(n0)));
+  I.r = static_cast<double*>(take(8 * size_t(n0)));
+  I.d = static_cast<double*>(take(8 * size_t(n0)));
+  I.q = static_cast<double*>(take(8 * size_t(n0)));
+  float* d_rho = static_cast<float*>(put(rho.data(), 4 * size_t(n0)));
+  I.faces = static_cast<float*>(put(faces, 4 * size_t(nbricks) * 3 * kFaces));
+  I.part = static_cast<double*>(take(8 * 4 * kRedGrid));
+  I.coarse_inv = static_cast<double*>(take(8 * kAtCoarseMax * kAtCoarseMax));
+  I.coarse_m = int(lv.back().n());
+  I.ncomp = ncomp;
+  I.comp_off = static_cast<const int*>(put(comp_off.data(), 4 * comp_off.size()));
+  I.comp_cells = static_cast<const int*>(put(comp_cells.data(), 4 * comp_cells.size()));
+  I.comp_mean = static_cast<double*>(take(8 * std::max(ncomp, 1)));
+  I.ctrl = static_cast<ACtrl*>(take(sizeof(ACtrl)));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(A->d_inst, &I, sizeof(AInst), cudaMemcpyHostToDevice, s);
+  // labels, phi and diagonals of every level, the coarsest inverse
+  if (e == cudaSuccess) {
+    k_at_label<<<grid_n(n0), kAT, 0, s>>>(A->d_inst, d_rho);
+    for (int l = 0; l + 1 < I.nlev; ++l) k_at_coarsen<<<grid_n(I.lv[l + 1].n), kAT, 0, s>>>(A->d_inst, l);
+    for (int l = 0; l < I.nlev; ++l) k_at_diag<<<grid_n(I.lv[l].n), kAT, 0, s>>>(A->d_inst, l);
+    k_at_coarse_factor<<<1, 1024, 0, s>>>(A->d_inst);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return A->set_error(FLUID_PP_CUDA, std::string("atlas upload: ") + cudaGetErrorString(e));
+  A->nb = nbricks;
+  A->has_state = true;
+  return FLUID_PP_OK;
+}
+
+int fluid_pp_atlas_project(fluid_pp_atlas* A, float dt, const fluid_pp_solve_opts* opts, fluid_pp_receipt* receipt) {
+  if (!A) return FLUID_PP_INVALID_ARG;
+  if (!A->has_state) return A->set_error(FLUID_PP_INVALID_ARG, "state not uploaded");
+  if (!(dt > 0.0f) || !std::isfinite(dt)) return A->set_error(FLUID_PP_INVALID_ARG, "dt must be positive and finite");
+  double rel = 1e-6, abs_tol = 0.0;
+  int max_iters = 200, cycle = 0;
+  if (opts) {
+    rel = opts->rel_tol;
+    abs_tol = opts->abs_tol;
+    max_iters = opts->max_iters;
+    cycle = opts->cycle;
+  }
+  if (cycle != 0 && cycle != 2)
+    return A->set_error(FLUID_PP_UNSUPPORTED, "atlas preconditioners: cycle 0 (V-cycle) or 2 (Jacobi)");
+  if (!(rel >= 0.0) || !(abs_tol >= 0.0) || max_iters <= 0) return A->set_error(FLUID_PP_INVALID_ARG, "bad solve options");
+  cudaSetDevice(A->cfg.device);
+  AInst& I = A->inst;
+  I.precond = cycle == 0 ? 1 : 0;
+  cudaStream_t s = A->stream;
+  cudaError_t e = cudaMemcpyAsync(&A->d_inst->precond, &I.precond, sizeof(int), cudaMemcpyHostToDevice, s);
+  const long long n0 = I.lv[0].n;
+  const int g0 = grid_n(n0);
+  // divergence before, the right-hand side, the start
+  k_at_div<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+  k_at_div_fold<<<1, 32, 0, s>>>(A->d_inst, 0);
+  k_at_rhs<<<g0, kAT, 0, s>>>(A->d_inst);
+  proj(A, I.b);
+  k_at_bb<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+  k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 2, 0);
+  k_at_init<<<1, 1, 0, s>>>(A->d_inst, rel, abs_tol, max_iters);
+  k_at_start<<<g0, kAT, 0, s>>>(A->d_inst);
+  const int poll = 8;
+  for (int it = 0; it < max_iters; ++it) {
+    if (I.precond) vcycle(A);
+    k_at_zvec<<<g0, kAT, 0, s>>>(A->d_inst);
+    proj(A, I.q);
+    k_at_dot_rq<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+    k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 0);
+    k_at_dir<<<g0, kAT, 0, s>>>(A->d_inst);
+    k_at_set_gamma<<<1, 1, 0, s>>>(A->d_inst);
+    proj(A, I.d);
+    k_at_spmv<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+    k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 0);
+    k_at_update<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+    if (I.ncomp) {
+      proj(A, I.x);
+      proj(A, I.r);
+      k_at_rr<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+    }
+    k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 0);
+    k_at_check<<<1, 1, 0, s>>>(A->d_inst);
+    if ((it + 1) % poll == 0) {
+      e = cudaMemcpyAsync(A->h_ctrl, I.ctrl, sizeof(ACtrl), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) break;
+      if (A->h_ctrl->done) break;
+    }
+  }
+  // float64 true residual, projected faces, receipts
+  k_at_true<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+  k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 1);
+  k_at_project<<<g0, kAT, 0, s>>>(A->d_inst);
+  k_at_div<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+  k_at_div_fold<<<1, 32, 0, s>>>(A->d_inst, 2);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(A->h_ctrl, I.ctrl, sizeof(ACtrl), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return A->set_error(FLUID_PP_CUDA, std::string("atlas project: ") + cudaGetErrorString(e));
+  const ACtrl& C = *A->h_ctrl;
+  int status = C.status;
+  if (!C.done) status = FLUID_PP_NONCONVERGENCE;
+  A->dt = dt;
+  if (receipt) {
+    const double h = A->cfg.h;
+    receipt->status = status;
+    receipt->iterations = C.iter;
+    receipt->liquid_cells = int(C.liquid);
+    receipt->levels = I.precond ? I.nlev : 1;
+    receipt->b_norm = std::sqrt(C.bb);
+    receipt->rel_residual = C.bb > 0 ? std::sqrt(C.rr / C.bb) : 0.0;
+    receipt->true_rel_residual = C.bb > 0 ? std::sqrt(C.red[1] / C.bb) : 0.0;
+    // b = h div u per cell: div in 1/s, the L2 norm over the liquid volume
+    receipt->max_div_before = C.div[0] / h;
+    receipt->l2_div_before = std::sqrt(C.div[1] * h);
+    receipt->max_div_after = C.div[2] / h;
+    receipt->l2_div_after = std::sqrt(C.div[3] * h);
+  }
+  return status;
+}
+
+int fluid_pp_atlas_download(fluid_pp_atlas* A, float* pressure, float* faces) {
+  if (!A) return FLUID_PP_INVALID_ARG;
+  if (!A->has_state) return A->set_error(FLUID_PP_INVALID_ARG, "state not uploaded");
+  cudaSetDevice(A->cfg.device);
+  cudaStream_t s = A->stream;
+  const long long n0 = A->inst.lv[0].n;
+  cudaError_t e = cudaSuccess;
+  float* tmp = nullptr;
+  if (pressure) {
+    if (!(A->dt > 0.0f)) return A->set_error(FLUID_PP_INVALID_ARG, "no projection yet");
+    e = dev_alloc(reinterpret_cast<void**>(&tmp), sizeof(float) * size_t(n0));
+    if (e == cudaSuccess) {
+      const double pscale = double(A->cfg.rho) * double(A->cfg.h) / double(A->dt);
+      k_at_pressure<<<grid_n(n0), kAT, 0, s>>>(A->d_inst, tmp, pscale);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(pressure, tmp, sizeof(float) * size_t(n0), cudaMemcpyDeviceToHost, s);
+  }
+  if (e == cudaSuccess && faces)
+    e = cudaMemcpyAsync(faces, A->inst.faces, sizeof(float) * size_t(A->nb) * 3 * kFaces, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  dev_release(tmp, s);
+  if (e != cudaSuccess) return A->set_error(FLUID_PP_CUDA, std::string("atlas download: ") + cudaGetErrorString(e));
+  return FLUID_PP_OK;
+}
+
+}  // extern "C"
+

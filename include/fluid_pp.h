@@ -477,6 +477,52 @@ const char* fluid_pp_tall_last_error(fluid_pp_tall* tall);
 /* Device bytes a tall handle for this layout allocates; host only. */
 int fluid_pp_tall_required_bytes(const fluid_pp_tall_config* config, const int* bases, unsigned long long* bytes);
 
+/* ------------------------------------------------------------------------
+ * Sparse brick atlas: the default adaptive method's pressure projection
+ * (lib/methods/adaptive-mass/webgpu-sparse-cm12-resident.ts; its CPU
+ * statement projectSparseAtlasVelocity, sparse-atlas-composite-projection.ts:
+ * 978-1566) for atlases whose bricks all carry the finest resolution.  Only
+ * the present bricks of 8^3 cells are stored.  Faces between present bricks,
+ * faces to absent bricks inside the domain (air, phi 0.5) and faces inside a
+ * brick are the system's rows; domain faces are walls.  A cell is liquid iff
+ * rho >= 0.5; liquid with no face to air is a pure Neumann problem whose mean
+ * pressure is removed, as the reference removes it.
+ * ---------------------------------------------------------------------- */
+typedef struct fluid_pp_atlas fluid_pp_atlas;
+
+typedef struct fluid_pp_atlas_config {
+  int nx, ny, nz;   /* domain in finest cells, multiples of 8 */
+  float h;          /* cell size, m */
+  float rho;        /* liquid density, kg/m^3 */
+  int device;
+} fluid_pp_atlas_config;
+
+/* Host only: the block hierarchy's level count and cells per level (at most
+ * 16 levels), and (with density) the liquid components without a face to air
+ * and their cells. */
+int fluid_pp_atlas_plan(int nx, int ny, int nz, int nbricks, const int* coords, const float* density,
+                        int* level_count, long long* level_cells, int* components, int* component_cells);
+int fluid_pp_atlas_create(const fluid_pp_atlas_config* config, fluid_pp_atlas** out);
+void fluid_pp_atlas_destroy(fluid_pp_atlas* atlas);
+int fluid_pp_atlas_set_stream(fluid_pp_atlas* atlas, void* stream);
+/* nbricks bricks: coords (bx, by, bz) per brick (each in [0, n / 8)), density
+ * nbricks x 512 floats [brick][z][y][x], faces nbricks x 3 x 576 floats: per
+ * brick its u [8][8][9], v [8][9][8], w [9][8][8] (face f of an axis between
+ * local cells f - 1 and f).  A face between two present bricks is read from
+ * the lower brick's copy.  Builds the rows' weights and the block hierarchy. */
+int fluid_pp_atlas_upload(fluid_pp_atlas* atlas, int nbricks, const int* coords, const float* density,
+                          const float* faces);
+/* PCG to ||b - A p|| <= max(abs_tol, rel_tol ||b||) (opts NULL: 1e-6, 200
+ * iterations).  opts->cycle 0: one V-cycle on the brick hierarchy per
+ * iteration; 2: Jacobi (the reference's own preconditioner); others
+ * FLUID_PP_UNSUPPORTED.  Faces of rows with a liquid side take
+ * u - (dt / rho) grad p / theta, faces of rows without one become 0, domain
+ * walls keep their values.  Divergence receipts are over liquid cells. */
+int fluid_pp_atlas_project(fluid_pp_atlas* atlas, float dt, const fluid_pp_solve_opts* opts, fluid_pp_receipt* receipt);
+/* pressure: nbricks x 512 floats in Pa (0 off the liquid); faces: as uploaded.  Either may be NULL. */
+int fluid_pp_atlas_download(fluid_pp_atlas* atlas, float* pressure, float* faces);
+const char* fluid_pp_atlas_last_error(fluid_pp_atlas* atlas);
+
 #ifdef __cplusplus
 }
 #endif
