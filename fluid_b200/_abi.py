@@ -23,7 +23,7 @@ EXPORTS = (
     "fluid_pp_upload_solids", "fluid_pp_get_level_faces", "fluid_pp_lcp_opts_default", "fluid_pp_project_lcp",
     "fluid_pp_extrapolate_velocity", "fluid_pp_tall_set_graphs", "fluid_pp_transport_opts_default",
     "fluid_pp_transport_density", "fluid_pp_set_gamma", "fluid_pp_get_gamma", "fluid_pp_get_vof",
-    "fluid_pp_atlas_plan", "fluid_pp_atlas_create", "fluid_pp_atlas_destroy", "fluid_pp_atlas_set_stream",
+    "fluid_pp_atlas_plan", "fluid_pp_atlas_create", "fluid_pp_atlas_destroy", "fluid_pp_atlas_set_stream", "fluid_pp_atlas_set_graphs",
     "fluid_pp_atlas_upload", "fluid_pp_atlas_project", "fluid_pp_atlas_download", "fluid_pp_atlas_last_error",
     "fluid_pp_receipt_read", "fluid_pp_download", "fluid_pp_device_arrays", "fluid_pp_last_error",
     "fluid_pp_prepare", "fluid_pp_level_dims", "fluid_pp_get_level", "fluid_pp_get_rhs",
@@ -151,6 +151,7 @@ def load():
     L.fluid_pp_atlas_destroy.argtypes = [vp]
     L.fluid_pp_atlas_destroy.restype = None
     L.fluid_pp_atlas_set_stream.argtypes = [vp, vp]
+    L.fluid_pp_atlas_set_graphs.argtypes = [vp, ci]
     L.fluid_pp_atlas_upload.argtypes = [vp, ci, vp, vp, vp]
     L.fluid_pp_atlas_project.argtypes = [vp, cf, vp, vp]
     L.fluid_pp_atlas_download.argtypes = [vp, vp, vp]

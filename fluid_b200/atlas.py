@@ -69,6 +69,10 @@ class AtlasProjector:
     def set_stream(self, stream: int):
         _check(load().fluid_pp_atlas_set_stream(self._h, ctypes.c_void_p(stream)), self._h, "set_stream")
 
+    def set_graphs(self, on: bool):
+        """The PCG iteration as a CUDA graph (default on); off for profilers."""
+        _check(load().fluid_pp_atlas_set_graphs(self._h, int(bool(on))), self._h, "set_graphs")
+
     def upload(self, coords, density, faces):
         """coords [nb][3] brick coordinates; density [nb][8][8][8]; faces [nb][3][576]."""
         c = np.ascontiguousarray(np.asarray(coords, np.int32).reshape(-1, 3))

@@ -101,6 +101,7 @@ struct AInst {
   double* d;
   double* q;
   double* part;             // kRedGrid x 4
+  double* bpart;            // one partial per brick (the brick-tiled reductions)
   double* coarse_inv;       // dense inverse of the coarsest level
   int coarse_m;
   int ncomp;                // liquid components without a cut row
@@ -358,6 +359,7 @@ __global__ void k_at_comp_sub(AInst* I, double* v) {
 // One colour of red-black Gauss-Seidel on level l (from a zero guess when
 // zero_init: the first colour then reads no neighbours).
 __global__ void k_at_smooth(AInst* I, int l, int colour, int zero_init) {
+  if (I->ctrl->done) return;
   const ALevel& L = I->lv[l];
   A_CELLS(L) {
     if (!L.label[i]) {
@@ -383,6 +385,7 @@ __global__ void k_at_smooth(AInst* I, int l, int colour, int zero_init) {
 
 // res = rhs - A z on level l.
 __global__ void k_at_residual(AInst* I, int l) {
+  if (I->ctrl->done) return;
   const ALevel& L = I->lv[l];
   A_CELLS(L) {
     if (!L.label[i]) {
@@ -400,6 +403,127 @@ __global__ void k_at_residual(AInst* I, int l) {
   }
 }
 
+// ----------------------------------------------- level 0, one CTA per brick
+// The brick's values and its six face halos staged in shared memory as a
+// 10^3 tile (index (z + 1) 100 + (y + 1) 10 + x + 1; edges and corners
+// unused).  A halo cell in an absent brick or beyond a wall holds 0, which is
+// what the stencils need: air and absent cells carry z = 0 and d = 0, and a
+// liquid cell's diagonal already holds its walls' and air faces' weights.
+constexpr int kTile = (kRes + 2) * (kRes + 2) * (kRes + 2);
+
+__device__ __forceinline__ int tix(int x, int y, int z) { return (z + 1) * 100 + (y + 1) * 10 + (x + 1); }
+
+template <class T>
+__device__ __forceinline__ void load_tile(const ALevel& L, int slot, const T* v, T* t) {
+  __shared__ int nb[6];
+  if (threadIdx.x < 6) {
+    const int a = threadIdx.x >> 1, sd = (threadIdx.x & 1) ? 1 : -1;
+    int b[3] = {L.coords[3 * slot], L.coords[3 * slot + 1], L.coords[3 * slot + 2]};
+    const int g[3] = {L.gx, L.gy, L.gz};
+    b[a] += sd;
+    nb[threadIdx.x] = (b[a] < 0 || b[a] >= g[a]) ? -1 : L.table[b[0] + L.gx * (b[1] + L.gy * b[2])];
+  }
+  const T* src = v + (long long)slot * kCells;
+  for (int k = threadIdx.x; k < kCells; k += blockDim.x) t[tix(k & 7, (k >> 3) & 7, k >> 6)] = src[k];
+  __syncthreads();
+  for (int k = threadIdx.x; k < 6 * 64; k += blockDim.x) {
+    const int f = k >> 6, u = k & 7, w = (k >> 3) & 7;
+    const int a = f >> 1, sd = (f & 1) ? 1 : -1;
+    // the halo cell (one step outside the brick) and the neighbour's cell it mirrors
+    int h[3], m[3];
+    if (a == 0) { h[0] = sd > 0 ? kRes : -1; h[1] = u; h[2] = w; }
+    else if (a == 1) { h[0] = u; h[1] = sd > 0 ? kRes : -1; h[2] = w; }
+    else { h[0] = u; h[1] = w; h[2] = sd > 0 ? kRes : -1; }
+    m[0] = h[0]; m[1] = h[1]; m[2] = h[2];
+    m[a] = sd > 0 ? 0 : kRes - 1;
+    const int ns = nb[f];
+    t[tix(h[0], h[1], h[2])] = ns >= 0 ? v[(long long)ns * kCells + m[0] + kRes * (m[1] + kRes * m[2])] : T(0);
+  }
+  __syncthreads();
+}
+
+template <class T>
+__device__ __forceinline__ T nbr_sum(const T* t, int x, int y, int z) {
+  const int c = tix(x, y, z);
+  return ((t[c - 1] + t[c + 1]) + (t[c - 10] + t[c + 10])) + (t[c - 100] + t[c + 100]);
+}
+
+// One colour of the level-0 smoother (z in place; the other colour's values,
+// inside and across the brick, are not written by this launch): thread t
+// takes the t-th cell of the colour, (x + y + z) & 1 == colour.
+__global__ void __launch_bounds__(256) k_at_smooth0(AInst* I, int colour) {
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[0];
+  __shared__ float t[kTile];
+  const int slot = blockIdx.x;
+  load_tile<float>(L, slot, L.z, t);
+  const int ty = (threadIdx.x >> 2) & 7, tz = threadIdx.x >> 5;
+  const int tx = 2 * (threadIdx.x & 3) + ((ty + tz + colour) & 1);
+  const long long i = (long long)slot * kCells + tx + kRes * (ty + kRes * tz);
+  if (!L.label[i]) return;
+  L.z[i] = (L.rhs[i] + nbr_sum(t, tx, ty, tz)) / L.diag[i];
+}
+
+// res = rhs - A z on level 0, two cells per thread.
+__global__ void __launch_bounds__(256) k_at_residual0(AInst* I) {
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[0];
+  __shared__ float t[kTile];
+  const int slot = blockIdx.x;
+  load_tile<float>(L, slot, L.z, t);
+  for (int k = threadIdx.x; k < kCells; k += 256) {
+    const int x = k & 7, y = (k >> 3) & 7, z = k >> 6;
+    const long long i = (long long)slot * kCells + k;
+    L.res[i] = L.label[i] ? (L.rhs[i] - L.diag[i] * t[tix(x, y, z)]) + nbr_sum(t, x, y, z) : 0.0f;
+  }
+}
+
+// q = A d and the CTA's d . q partial (level 0, float64).  One CTA per
+// brick; the partials go to part[4 brick] (the fold reads kRedGrid of them
+// per pass, so the brick kernels write a per-brick array folded separately).
+__global__ void __launch_bounds__(256) k_at_spmv0(AInst* I, double* bpart) {
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[0];
+  __shared__ double t[kTile];
+  const int slot = blockIdx.x;
+  load_tile<double>(L, slot, I->d, t);
+  double acc = 0.0;
+  for (int k = threadIdx.x; k < kCells; k += 256) {
+    const int x = k & 7, y = (k >> 3) & 7, z = k >> 6;
+    const long long i = (long long)slot * kCells + k;
+    double q = 0.0;
+    if (L.label[i]) {
+      const double dv = t[tix(x, y, z)];
+      q = double(L.diag[i]) * dv - nbr_sum(t, x, y, z);
+      acc += dv * q;
+    }
+    I->q[i] = q;
+  }
+  __shared__ double sh[256];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (int(threadIdx.x) < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) bpart[slot] = sh[0];
+}
+
+// Folds the per-brick partials into ctrl->red[0]: 256 threads each sum a
+// fixed stride of bricks, then a fixed tree.
+__global__ void __launch_bounds__(256) k_at_fold_bricks(AInst* I, const double* bpart) {
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < I->nb; b += 256) s += bpart[b];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (int(threadIdx.x) < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) I->ctrl->red[0] = sh[0];
+}
+
 // Finer level index of child k (0 .. 7) of coarse cell c, -1 if none.
 __device__ __forceinline__ long long child_of(const ALevel& F, const ALevel& C, const Cell& c, int k) {
   const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
@@ -411,6 +535,7 @@ __device__ __forceinline__ long long child_of(const ALevel& F, const ALevel& C, 
 
 // rhs_c = 1/2 sum of the liquid children's residuals (R = P^T / 2).
 __global__ void k_at_restrict(AInst* I, int l) {
+  if (I->ctrl->done) return;
   const ALevel& F = I->lv[l];
   const ALevel& C = I->lv[l + 1];
   A_CELLS(C) {
@@ -430,6 +555,7 @@ __global__ void k_at_restrict(AInst* I, int l) {
 
 // z_f += z_c on liquid fine cells (P piecewise constant).
 __global__ void k_at_prolong(AInst* I, int l) {
+  if (I->ctrl->done) return;
   const ALevel& F = I->lv[l];
   const ALevel& C = I->lv[l + 1];
   A_CELLS(F) {
@@ -918,6 +1044,9 @@ struct fluid_pp_atlas {
   int nb = 0;
   float dt = 0.0f;
   bool has_state = false;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};   // one iteration: Jacobi, V-cycle
+  bool graph_failed[2] = {false, false};
+  bool use_graphs = true;
   int set_error(int code, const std::string& m) {
     err = m;
     return code;
@@ -935,30 +1064,96 @@ int global_error(int code, const std::string& m) {
   return code;
 }
 
-void proj(fluid_pp_atlas* A, double* v) {
+void proj(fluid_pp_atlas* A, double* v, cudaStream_t s) {
   if (A->inst.ncomp == 0) return;
-  k_at_comp_mean<<<A->inst.ncomp, kAT, 0, A->stream>>>(A->d_inst, v);
-  k_at_comp_sub<<<dim3(8, A->inst.ncomp), kAT, 0, A->stream>>>(A->d_inst, v);
+  k_at_comp_mean<<<A->inst.ncomp, kAT, 0, s>>>(A->d_inst, v);
+  k_at_comp_sub<<<dim3(8, A->inst.ncomp), kAT, 0, s>>>(A->d_inst, v);
 }
 
-void vcycle(fluid_pp_atlas* A) {
+void vcycle(fluid_pp_atlas* A, cudaStream_t s) {
   const AInst& I = A->inst;
-  cudaStream_t s = A->stream;
   k_at_vin<<<grid_n(I.lv[0].n), kAT, 0, s>>>(A->d_inst);
   const int last = I.nlev - 1;
   for (int l = 0; l < last; ++l) {
     const int g = grid_n(I.lv[l].n);
-    k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 1);
-    k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 1, 0);
-    k_at_residual<<<g, kAT, 0, s>>>(A->d_inst, l);
+    k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 1);   // first colour from zero: elementwise
+    if (l == 0) {
+      k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 1);
+      k_at_residual0<<<I.nb, 256, 0, s>>>(A->d_inst);
+    } else {
+      k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 1, 0);
+      k_at_residual<<<g, kAT, 0, s>>>(A->d_inst, l);
+    }
     k_at_restrict<<<grid_n(I.lv[l + 1].n), kAT, 0, s>>>(A->d_inst, l);
   }
   k_at_coarse_apply<<<1, 1024, 0, s>>>(A->d_inst);
   for (int l = last - 1; l >= 0; --l) {
     const int g = grid_n(I.lv[l].n);
     k_at_prolong<<<g, kAT, 0, s>>>(A->d_inst, l);
-    k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 1, 0);
-    k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 0);
+    if (l == 0) {
+      k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 1);
+      k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 0);
+    } else {
+      k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 1, 0);
+      k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 0);
+    }
+  }
+}
+
+// One PCG iteration on stream s (kernels skip their work once the solve is done).
+void iteration(fluid_pp_atlas* A, cudaStream_t s) {
+  const AInst& I = A->inst;
+  const int g0 = grid_n(I.lv[0].n);
+  if (I.precond) vcycle(A, s);
+  k_at_zvec<<<g0, kAT, 0, s>>>(A->d_inst);
+  proj(A, I.q, s);
+  k_at_dot_rq<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+  k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 0);
+  k_at_dir<<<g0, kAT, 0, s>>>(A->d_inst);
+  k_at_set_gamma<<<1, 1, 0, s>>>(A->d_inst);
+  proj(A, I.d, s);
+  k_at_spmv0<<<I.nb, 256, 0, s>>>(A->d_inst, I.bpart);
+  k_at_fold_bricks<<<1, 256, 0, s>>>(A->d_inst, I.bpart);
+  k_at_update<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+  if (I.ncomp) {
+    proj(A, I.x, s);
+    proj(A, I.r, s);
+    k_at_rr<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+  }
+  k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 0);
+  k_at_check<<<1, 1, 0, s>>>(A->d_inst);
+}
+
+// The iteration as a CUDA graph, captured once per upload and preconditioner
+// on a private stream (the caller's may be the legacy stream); on any
+// failure the solve launches the same kernels directly.
+cudaGraphExec_t iteration_graph(fluid_pp_atlas* A) {
+  const int k = A->inst.precond ? 1 : 0;
+  if (A->graph[k] || A->graph_failed[k]) return A->graph[k];
+  cudaStream_t cs = nullptr;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    iteration(A, cs);
+    e = cudaStreamEndCapture(cs, &g);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&A->graph[k], g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (cs) cudaStreamDestroy(cs);
+  if (e != cudaSuccess) {
+    A->graph[k] = nullptr;
+    A->graph_failed[k] = true;
+    cudaGetLastError();
+  }
+  return A->graph[k];
+}
+
+void drop_graphs(fluid_pp_atlas* A) {
+  for (int k = 0; k < 2; ++k) {
+    if (A->graph[k]) cudaGraphExecDestroy(A->graph[k]);
+    A->graph[k] = nullptr;
+    A->graph_failed[k] = false;
   }
 }
 
@@ -1026,10 +1221,17 @@ int fluid_pp_atlas_create(const fluid_pp_atlas_config* cfg, fluid_pp_atlas** out
 void fluid_pp_atlas_destroy(fluid_pp_atlas* A) {
   if (!A) return;
   cudaSetDevice(A->cfg.device);
+  drop_graphs(A);
   dev_release(A->arena, A->stream);
   dev_release(A->d_inst, A->stream);
   host_release(A->h_ctrl, A->stream);
   delete A;
+}
+
+int fluid_pp_atlas_set_graphs(fluid_pp_atlas* A, int on) {
+  if (!A) return FLUID_PP_INVALID_ARG;
+  A->use_graphs = on != 0;
+  return FLUID_PP_OK;
 }
 
 int fluid_pp_atlas_set_stream(fluid_pp_atlas* A, void* stream) {
@@ -1076,10 +1278,11 @@ int fluid_pp_atlas_upload(fluid_pp_atlas* A, int nbricks, const int* coords, con
              up(4 * L.parent.size());
   }
   bytes += 5 * up(8 * size_t(n0)) + up(4 * size_t(n0)) + up(4 * size_t(nbricks) * 3 * kFaces);
-  bytes += up(8 * 4 * kRedGrid) + up(8 * kAtCoarseMax * kAtCoarseMax) + up(4 * comp_off.size()) +
+  bytes += up(8 * size_t(nbricks)) + up(8 * 4 * kRedGrid) + up(8 * kAtCoarseMax * kAtCoarseMax) + up(4 * comp_off.size()) +
            up(4 * comp_cells.size()) + up(8 * std::max(ncomp, 1)) + up(sizeof(ACtrl));
   cudaSetDevice(A->cfg.device);
   cudaStream_t s = A->stream;
+  drop_graphs(A);   // the graphs hold the old hierarchy's launch shapes
   if (bytes > A->arena_bytes) {
     dev_release(A->arena, s);
     A->arena_bytes = 0;
@@ -1135,6 +1338,7 @@ int fluid_pp_atlas_upload(fluid_pp_atlas* A, int nbricks, const int* coords, con
   float* d_rho = static_cast<float*>(put(rho.data(), 4 * size_t(n0)));
   I.faces = static_cast<float*>(put(faces, 4 * size_t(nbricks) * 3 * kFaces));
   I.part = static_cast<double*>(take(8 * 4 * kRedGrid));
+  I.bpart = static_cast<double*>(take(8 * size_t(nbricks)));
   I.coarse_inv = static_cast<double*>(take(8 * kAtCoarseMax * kAtCoarseMax));
   I.coarse_m = int(lv.back().n());
   I.ncomp = ncomp;
@@ -1184,31 +1388,17 @@ int fluid_pp_atlas_project(fluid_pp_atlas* A, float dt, const fluid_pp_solve_opt
   k_at_div<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
   k_at_div_fold<<<1, 32, 0, s>>>(A->d_inst, 0);
   k_at_rhs<<<g0, kAT, 0, s>>>(A->d_inst);
-  proj(A, I.b);
+  proj(A, I.b, s);
   k_at_bb<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
   k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 2, 0);
   k_at_init<<<1, 1, 0, s>>>(A->d_inst, rel, abs_tol, max_iters);
   k_at_start<<<g0, kAT, 0, s>>>(A->d_inst);
   const int poll = 8;
+  cudaGraphExec_t gx = A->use_graphs ? iteration_graph(A) : nullptr;
   for (int it = 0; it < max_iters; ++it) {
-    if (I.precond) vcycle(A);
-    k_at_zvec<<<g0, kAT, 0, s>>>(A->d_inst);
-    proj(A, I.q);
-    k_at_dot_rq<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
-    k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 0);
-    k_at_dir<<<g0, kAT, 0, s>>>(A->d_inst);
-    k_at_set_gamma<<<1, 1, 0, s>>>(A->d_inst);
-    proj(A, I.d);
-    k_at_spmv<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
-    k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 0);
-    k_at_update<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
-    if (I.ncomp) {
-      proj(A, I.x);
-      proj(A, I.r);
-      k_at_rr<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
-    }
-    k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 0);
-    k_at_check<<<1, 1, 0, s>>>(A->d_inst);
+    if (gx) e = cudaGraphLaunch(gx, s);
+    else iteration(A, s);
+    if (e != cudaSuccess) break;
     if ((it + 1) % poll == 0) {
       e = cudaMemcpyAsync(A->h_ctrl, I.ctrl, sizeof(ACtrl), cudaMemcpyDeviceToHost, s);
       if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -12,6 +12,7 @@ dam   : 128x96x128 dam break + 16 spheres, fp16 levels (the bench's secondary un
 tall  : 256^2 columns x 1024 rows, band 32 (the bench's tall-cell workload)
 batch : the bench's 64 uneven uniform grids in one batched solve
 transport : CM12 density transport steps on the 128x96x128 transport lattice (one launch per kernel always)
+atlas : the sparse brick atlas of a 256x192x256 pool with 40 drops (8508 bricks), V-cycle PCG
 """
 from __future__ import annotations
 
@@ -23,7 +24,7 @@ from .tall import TallProjector
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["dam", "tall", "batch", "transport"], default="dam")
+    ap.add_argument("--workload", choices=["dam", "tall", "batch", "transport", "atlas"], default="dam")
     ap.add_argument("--solves", type=int, default=2)
     ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16", "bf16"])
     args = ap.parse_args()
@@ -42,6 +43,17 @@ def main() -> int:
         for _ in range(args.solves):
             tp.upload_state(s.vof, s.u, s.v, s.w)
             r = tp.project(s.dt, rel_tol=1e-6)
+            print(r["status_name"], r["iterations"], flush=True)
+    elif args.workload == "atlas":
+        from .atlas import AtlasProjector, bricks_from_dense
+        s = configs.atlas_scene(256, 192, 256, seed=11, drops=40)
+        coords = configs.atlas_bricks(s.vof)
+        dens, faces = bricks_from_dense(s.vof, s.u, s.v, s.w, coords)
+        A = AtlasProjector((s.nx, s.ny, s.nz), s.h, s.rho)
+        A.set_graphs(False)
+        for _ in range(args.solves):
+            A.upload(coords, dens, faces)
+            r = A.project(s.dt, rel_tol=1e-6)
             print(r["status_name"], r["iterations"], flush=True)
     elif args.workload == "transport":
         s = configs.transport_scene(128, 96, 128, seed=21, cells_per_step=2.5)

@@ -505,6 +505,8 @@ int fluid_pp_atlas_plan(int nx, int ny, int nz, int nbricks, const int* coords, 
 int fluid_pp_atlas_create(const fluid_pp_atlas_config* config, fluid_pp_atlas** out);
 void fluid_pp_atlas_destroy(fluid_pp_atlas* atlas);
 int fluid_pp_atlas_set_stream(fluid_pp_atlas* atlas, void* stream);
+/* The PCG iteration as a CUDA graph (default on); off: one launch per kernel (profilers). */
+int fluid_pp_atlas_set_graphs(fluid_pp_atlas* atlas, int on);
 /* nbricks bricks: coords (bx, by, bz) per brick (each in [0, n / 8)), density
  * nbricks x 512 floats [brick][z][y][x], faces nbricks x 3 x 576 floats: per
  * brick its u [8][8][9], v [8][9][8], w [9][8][8] (face f of an axis between

@@ -123,3 +123,20 @@ def test_atlas_rejects_bad_input():
     with pytest.raises(Exception):
         A.project(1.0 / 60, cycle="f")
     A.destroy()
+
+
+def test_atlas_graph_and_direct_launches_give_the_same_bits():
+    s = configs.atlas_scene(48, 40, 32, seed=5, drops=4)
+    coords = configs.atlas_bricks(s.vof)
+    dens, faces = bricks_from_dense(s.vof, s.u, s.v, s.w, coords)
+    out = []
+    for graphs in (True, False):
+        A = AtlasProjector((s.nx, s.ny, s.nz), s.h, s.rho)
+        A.set_graphs(graphs)
+        A.upload(coords, dens, faces)
+        rec = A.project(s.dt, rel_tol=1e-6)
+        out.append((rec["iterations"], *A.download()))
+        A.destroy()
+    assert out[0][0] == out[1][0]
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    np.testing.assert_array_equal(out[0][2], out[1][2])
