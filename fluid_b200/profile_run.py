@@ -12,6 +12,7 @@ dam   : 128x96x128 dam break + 16 spheres, fp16 levels (the bench's secondary un
 tall  : 256^2 columns x 1024 rows, band 32 (the bench's tall-cell workload)
 batch : the bench's 64 uneven uniform grids in one batched solve
 transport : CM12 density transport steps on the 128x96x128 transport lattice (one launch per kernel always)
+extrap : velocity extrapolation of the projected 128x96x128 dam break + 16 spheres
 atlas : the sparse brick atlas of a 256x192x256 pool with 40 drops (8508 bricks), V-cycle PCG
 """
 from __future__ import annotations
@@ -24,7 +25,7 @@ from .tall import TallProjector
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["dam", "tall", "batch", "transport", "atlas"], default="dam")
+    ap.add_argument("--workload", choices=["dam", "tall", "batch", "transport", "atlas", "extrap"], default="dam")
     ap.add_argument("--solves", type=int, default=2)
     ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16", "bf16"])
     args = ap.parse_args()
@@ -44,6 +45,15 @@ def main() -> int:
             tp.upload_state(s.vof, s.u, s.v, s.w)
             r = tp.project(s.dt, rel_tol=1e-6)
             print(r["status_name"], r["iterations"], flush=True)
+    elif args.workload == "extrap":
+        s = configs.dam_spheres()
+        pp = PressureProjector((s.nx, s.ny, s.nz), s.h, s.rho, precision=args.precision)
+        pp.upload_state(s.vof, s.u, s.v, s.w)
+        pp.project(s.dt, rel_tol=1e-6)
+        _, u, v, w = pp.download()
+        for _ in range(args.solves):
+            pp.upload_state(s.vof, u, v, w)
+            print("filled", pp.extrapolate_velocity(), flush=True)
     elif args.workload == "atlas":
         from .atlas import AtlasProjector, bricks_from_dense
         s = configs.atlas_scene(256, 192, 256, seed=11, drops=40)
