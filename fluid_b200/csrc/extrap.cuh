@@ -41,8 +41,19 @@ struct ExtDev {
   float* vel[3];           // u, v, w (the handle's MAC arrays)
   float4* val[2];          // FIM values (xyz) and known mask (w)
   float4* dist[2];         // FIM distances (xyz) and active mask (w)
-  unsigned* count;         // active components written per side
+  unsigned* count;         // active components written per side; [3] the band's node count
+  uint8_t* mark[2];        // band marks (liquid cells, then dilated)
+  unsigned* band;          // the band's node indices
 };
+
+// The narrow band's passes touch only nodes within a few cells of a source
+// face: a node becomes known only at an upwind distance <= 2 h, and one is
+// activated only next to a node with a finite distance; a node of a liquid
+// cell is a source face (skipped).  The passes therefore run over the air
+// cells within kBandReach cells (Chebyshev) of a liquid cell, listed once per
+// call; every other node keeps its seeded state, which the seed writes to
+// both sides.
+constexpr int kBandReach = 6;
 
 __device__ __forceinline__ bool ext_in(const ExtDev& E, int x, int y, int z) {
   return x >= 0 && y >= 0 && z >= 0 && x < E.nx && y < E.ny && z < E.nz;
@@ -243,9 +254,41 @@ __global__ void k_ext_seed(ExtDev E) {
     d.w = float(active);
     E.val[0][i] = v;
     E.dist[0][i] = d;
+    E.val[1][i] = v;
+    E.dist[1][i] = d;
+    E.mark[0][i] = ext_density(E, x, y, z) > 0.5f ? 1 : 0;
     active_total += __popc(active);
   }
   if (active_total) atomicAdd(&E.count[0], active_total);
+}
+
+// One axis of the band dilation: out = max of in over [-kBandReach, kBandReach] along the axis.
+__global__ void k_ext_dilate(ExtDev E, int axis, const uint8_t* in, uint8_t* out) {
+  EXT_FOR_CELLS(E, x, y, z, i) {
+    const int p[3] = {x, y, z}, d[3] = {E.nx, E.ny, E.nz};
+    const long long st = axis == 0 ? 1 : (axis == 1 ? E.nx : (long long)E.nx * E.ny);
+    const int lo = max(0, p[axis] - kBandReach), hi = min(d[axis] - 1, p[axis] + kBandReach);
+    uint8_t m = 0;
+    for (int k = lo; k <= hi && !m; ++k) m = in[i + (k - p[axis]) * st];
+    out[i] = m;
+  }
+}
+
+// The band's node list: air cells near the liquid.  Each warp reserves one
+// run of the list for its marked cells, in cell order, so a pass's loads stay
+// coalesced (the order of the runs does not matter: a pass computes every node
+// from the other side only).
+__global__ void k_ext_band_list(ExtDev E, const uint8_t* mark) {
+  EXT_FOR_CELLS(E, x, y, z, i) {
+    const bool m = mark[i] && !(ext_density(E, x, y, z) > 0.5f);
+    const unsigned act = __activemask();
+    const unsigned bal = __ballot_sync(act, m);
+    const int lane = threadIdx.x & 31, leader = __ffs(act) - 1;
+    unsigned base = 0;
+    if (lane == leader && bal) base = atomicAdd(&E.count[3], unsigned(__popc(bal)));
+    base = __shfl_sync(act, base, leader);
+    if (m) E.band[base + __popc(bal & ((1u << lane) - 1u))] = unsigned(i);
+  }
 }
 
 __global__ void k_ext_reset(unsigned* count, int side) { count[side] = 0u; }
@@ -257,7 +300,10 @@ __global__ void k_ext_update(ExtDev E, int src) {
   const bool run = E.count[src] != 0u;
   const ExtSrc S{E, E.val[src], E.dist[src]};
   unsigned active_total = 0;
-  EXT_FOR_CELLS(E, x, y, z, i) {
+  const unsigned nband = E.count[3];
+  for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < nband; k += gridDim.x * blockDim.x) {
+    const long long i = E.band[k];
+    const int x = int(i % E.nx), y = int((i / E.nx) % E.ny), z = int(i / ((long long)E.nx * E.ny));
     float4 v = S.val[i], d = S.dist[i];
     if (run) {
       unsigned known = unsigned(v.w), active = unsigned(d.w);

@@ -1765,7 +1765,8 @@ int fluid_pp_extrapolate_velocity(fluid_pp* pp, long long* filled_faces) {
   }
   long long cells = 4 * n;
   for (const auto& l : dims) cells += 2LL * l[0] * l[1] * l[2];
-  const size_t bytes = size_t(cells) * sizeof(float4) + 16;
+  // float4 states, the counters, two band mark arrays and the band list
+  const size_t bytes = size_t(cells) * sizeof(float4) + 16 + 2 * size_t(n) + 4 * size_t(n) + 16;
   cudaStream_t s = pp->stream;
   if (!pp->ext_mem) {
     const cudaError_t e = dev_alloc(reinterpret_cast<void**>(&pp->ext_mem), bytes);
@@ -1800,9 +1801,16 @@ int fluid_pp_extrapolate_velocity(fluid_pp* pp, long long* filled_faces) {
     p += m;
   }
   E.count = reinterpret_cast<unsigned*>(p);
+  E.mark[0] = reinterpret_cast<uint8_t*>(p + 1);
+  E.mark[1] = E.mark[0] + n;
+  E.band = reinterpret_cast<unsigned*>((reinterpret_cast<uintptr_t>(E.mark[1] + n) + 15) & ~uintptr_t(15));
   auto grid = [](long long cnt) { return int(std::max(1LL, std::min<long long>((cnt + kThreads - 1) / kThreads, kMaxGrid))); };
   cudaMemsetAsync(E.count, 0, 16, s);
   k_ext_seed<<<grid(n), kThreads, 0, s>>>(E);
+  k_ext_dilate<<<grid(n), kThreads, 0, s>>>(E, 0, E.mark[0], E.mark[1]);
+  k_ext_dilate<<<grid(n), kThreads, 0, s>>>(E, 1, E.mark[1], E.mark[0]);
+  k_ext_dilate<<<grid(n), kThreads, 0, s>>>(E, 2, E.mark[0], E.mark[1]);
+  k_ext_band_list<<<grid(n), kThreads, 0, s>>>(E, E.mark[1]);
   const int passes = std::min(std::max({nx, ny, nz}), 16);
   for (int k = 0; k < passes; ++k) {
     const int src = k & 1;
