@@ -958,6 +958,36 @@ __device__ __forceinline__ void tv_zero(TInst* I, int l, int t0, int ts) {
   for (int k = t0; k < L.n; k += ts) z[k] = fromf<S>(0.0f);
 }
 
+// The start of a grid level's pre-smoothing in one pass: with from_acc the
+// restricted right-hand side out of the fixed-point accumulators (as
+// tv_restrict_finish), then z = 0 everywhere except the liquid red band
+// rows, which take rhs / diag: the red band sweep from zero, whose neighbour
+// terms all vanish.  Same values as tv_restrict_finish + tv_zero +
+// tv_smooth_band(colour 0).
+template <class S>
+__device__ __forceinline__ void tv_start(TInst* I, int l, int from_acc, int t0, int ts) {
+  const TLevel& L = I->lv[l];
+  S* z = stor<S>(L.z);
+  S* rhs = stor<S>(L.rhs);
+  for (int k = t0; k < L.n; k += ts) {
+    const bool liq = L.label[k] != 0;
+    float rh;
+    if (from_acc) {
+      const long long a = (long long)L.acc[k];
+      const S r = fromf<S>(liq ? float(double(a) / kFix) : 0.0f);
+      rhs[k] = r;
+      L.acc[k] = 0ull;
+      rh = tof(r);
+    } else {
+      rh = tof(rhs[k]);
+    }
+    int x, j, zc, b;
+    const bool act = sample_active(L, k, x, j, zc, b);
+    const bool red = j >= 2 && act && j - 2 < L.band && ((x + (b + j - 2) + zc) & 1) == 0;
+    z[k] = fromf<S>(red && liq ? (rh - 0.0f) / L.diag[k] : 0.0f);
+  }
+}
+
 // Band colour sweeps run over work items of G consecutive band rows of one
 // column (item = column + ncol * group, so a warp's lanes are adjacent
 // columns): an item loads its column's base and the four lateral bases once,
@@ -1208,6 +1238,7 @@ __device__ __forceinline__ void tv_coarse_apply(TInst* I) {
   }
 #define TALL_COMMA ,
 TALL_GRID_KERNEL(k_tall_zero, class S, tv_zero<S>(I, l, t0, ts))
+TALL_GRID_KERNEL(k_tall_start, class S, tv_start<S>(I, l, arg, t0, ts))
 TALL_GRID_KERNEL(k_tall_smooth, class S, (tv_smooth<kBandGroup, S>(I, l, arg, t0, ts)))
 TALL_GRID_KERNEL(k_tall_residual, class S, (tv_residual<kApplyGroup, S>(I, l, t0, ts)))
 TALL_GRID_KERNEL(k_tall_restrict, class S, tv_restrict<S>(I, l, t0, ts))
@@ -1504,9 +1535,10 @@ void launch_vcycle_t(fluid_pp_tall* T, int first) {
   cudaStream_t s = T->stream;
   TInst* D = T->d_inst;
   // grid level l's vectors are float on level 0, S above it; the block levels are float
-  auto zero = [&](int l, int g) {
-    if (l == 0) k_tall_zero<float><<<g, kTB, 0, s>>>(D, l, 0);
-    else k_tall_zero<S><<<g, kTB, 0, s>>>(D, l, 0);
+  // zero + (restricted rhs) + red band sweep from zero, in one launch
+  auto start = [&](int l, int g) {
+    if (l == 0) k_tall_start<float><<<g, kTB, 0, s>>>(D, l, 0);
+    else k_tall_start<S><<<g, kTB, 0, s>>>(D, l, 1);
   };
   auto smooth = [&](int l, int g, int colour) {
     if (l == 0) k_tall_smooth<float><<<g, kTB, 0, s>>>(D, l, colour);
@@ -1516,8 +1548,7 @@ void launch_vcycle_t(fluid_pp_tall* T, int first) {
     const int g = grid_for(I.lv[l].n), gc = grid_for(I.lv[l].ncol), gb = grid_band(I.lv[l]);
     const int gr = grid_for(apply_items(I.lv[l].ncol, I.lv[l].band, kApplyGroup));
     const int gf = grid_for(I.lv[l + 1].n);
-    zero(l, g);
-    smooth(l, gb, 0);
+    start(l, g);
     smooth(l, gb, 1);
     smooth(l, gc, 2);
     smooth(l, gc, 3);
@@ -1528,8 +1559,8 @@ void launch_vcycle_t(fluid_pp_tall* T, int first) {
       k_tall_residual<S><<<gr, kTB, 0, s>>>(D, l, 0);
       k_tall_restrict<S><<<g, kTB, 0, s>>>(D, l, 0);
     }
-    if (l + 1 < first) k_tall_restrict_finish<S><<<gf, kTB, 0, s>>>(D, l + 1, 0);
-    else k_tall_restrict_finish<float><<<gf, kTB, 0, s>>>(D, l + 1, 0);
+    // the next grid level finishes its rhs in its start pass; the block levels here
+    if (l + 1 >= first) k_tall_restrict_finish<float><<<gf, kTB, 0, s>>>(D, l + 1, 0);
   }
   const size_t sm = vblock_smem_bytes(I, first);
   k_tall_vblock<<<1, 1024, sm, s>>>(D, first, sm > 0 ? 1 : 0);
