@@ -113,6 +113,16 @@ def transport_bytes_per_cell(diffusion_iterations: int = 1) -> float:
     return 16 + 36 + 20 + 40 + 16 * passes + (8 if passes % 2 else 0) + 12 + 4 + 12 + 8
 
 
+def atlas_bytes_per_cell_iteration() -> float:
+    """Algorithmic bytes of one V-cycle PCG iteration of the sparse atlas per
+    level-0 cell (float32 level arrays, float64 CG vectors, byte labels; each
+    array once per launch): the level-0 V-cycle (first colour from zero 13,
+    each tiled smoother colour 15 (three launches), residual 17, restriction 5,
+    prolongation 9, input 13) and the CG kernels (z 13, r.z 17, direction 25,
+    SpMV 21, update 49), times 8/7 for the coarser levels."""
+    return (13 + 3 * 15 + 17 + 5 + 9 + 13 + 13 + 17 + 25 + 21 + 49) * 8.0 / 7.0
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -732,6 +742,7 @@ def main():
             if k >= args.warmup:
                 ta.append(ms)
         atlas_runs[cyc] = {"solves_per_s": len(ta) / (sum(ta) / 1000.0), "p50_ms": statistics.median(ta),
+                           "mean_ms": statistics.mean(ta),
                            "iterations": ra["iterations"], "status": ra["status_name"],
                            "true_rel_residual": ra["true_rel_residual"],
                            "max_div_ratio": ra["max_div_after"] / max(ra["max_div_before"], 1e-30)}
@@ -757,12 +768,19 @@ def main():
     t_cpu_a = time.perf_counter()
     _, ja = oa.solve_jacobi(1e-6, 0.0)
     t_cpu_a = time.perf_counter() - t_cpu_a
+    hbm_a, kind_a = peaks()
+    a_alg = atlas_bytes_per_cell_iteration() * len(acoords) * 512 * atlas_runs["v"]["iterations"]
+    a_gbs = a_alg / (atlas_runs["v"]["mean_ms"] / 1000.0) / 1e9
     atlas_line = {
         "workload": asc.meta["workload"] + f": {len(acoords)} of {(ATLAS_DIMS[0] // 8) * (ATLAS_DIMS[1] // 8) * (ATLAS_DIMS[2] // 8)} "
                     "bricks (8^3 cells) present, Gaussian velocities sigma 0.2 on faces with a liquid side, rel-res 1e-6",
         "cells": len(acoords) * 512, "dense_equivalent_cells": int(np.prod(ATLAS_DIMS)), "steps": ATLAS_STEPS,
         "v_cycle": atlas_runs["v"], "jacobi": atlas_runs["jacobi"],
         "fp64_error_128x96x128": float(np.linalg.norm(pa - pa_ref) / np.linalg.norm(pa_ref)),
+        "roofline": {"bound": "hbm", "scope": "whole V-cycle PCG solve (setup, receipts and projection included)",
+                     "alg_bytes_per_cell_iteration": round(atlas_bytes_per_cell_iteration(), 1),
+                     "achieved": round(a_gbs, 1), "peak": hbm_a, "unit": "GB/s", "frac": round(a_gbs / hbm_a, 4),
+                     "peak_kind": kind_a},
         "cpu_baseline": {"value": 1.0 / t_cpu_a, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "port",
                          "sample": f"the 128x96x128 atlas ({len(scoords)} bricks) as its dense embedding: the oracle's "
                                    f"float64 Jacobi-PCG (the reference's CPU algorithm) to rel-res 1e-6, "
