@@ -61,7 +61,7 @@ constexpr int kAT = 256;           // threads per CTA
 constexpr int kAGrid = 148 * 8;    // grid cap
 constexpr int kAtMaxLevels = 16;
 constexpr int kAtCoarseMax = 64;   // the dense coarsest level
-constexpr int kRedGrid = 296;      // fixed reduction grid (partials folded in block order)
+constexpr int kRedGrid = 1184;     // fixed reduction grid (partials folded in block order)
 
 struct ALevel {
   int B;                    // cells per block edge
@@ -464,6 +464,19 @@ __global__ void __launch_bounds__(256) k_at_smooth0(AInst* I, int colour) {
   L.z[i] = (L.rhs[i] + nbr_sum(t, tx, ty, tz)) / L.diag[i];
 }
 
+// The first colour of the level-0 pre-smoothing from zero: red liquid cells
+// z = rhs / diag, every other cell 0 (no neighbour terms).
+__global__ void __launch_bounds__(256) k_at_smooth0_zero(AInst* I) {
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[0];
+  const int slot = blockIdx.x;
+  for (int k = threadIdx.x; k < kCells; k += 256) {
+    const int x = k & 7, y = (k >> 3) & 7, z = k >> 6;
+    const long long i = (long long)slot * kCells + k;
+    L.z[i] = (L.label[i] && ((x + y + z) & 1) == 0) ? L.rhs[i] / L.diag[i] : 0.0f;
+  }
+}
+
 // res = rhs - A z on level 0, two cells per thread.
 __global__ void __launch_bounds__(256) k_at_residual0(AInst* I) {
   if (I->ctrl->done) return;
@@ -655,6 +668,19 @@ __global__ void __launch_bounds__(kAT) k_at_dot_rq(AInst* I) {
   block_reduce<1>(v, I->part);
 }
 
+// zvec and dot_rq in one pass (no nullspace projection between them).
+__global__ void __launch_bounds__(kAT) k_at_zdot(AInst* I) {
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[0];
+  double v[1] = {0.0};
+  A_CELLS(L) {
+    const double z = L.label[i] ? (I->precond ? double(L.z[i]) : I->r[i] / double(L.diag[i])) : 0.0;
+    I->q[i] = z;
+    if (L.label[i]) v[0] += I->r[i] * z;
+  }
+  block_reduce<1>(v, I->part);
+}
+
 __global__ void __launch_bounds__(kAT) k_at_rr(AInst* I) {
   if (I->ctrl->done) return;
   const ALevel& L = I->lv[0];
@@ -695,7 +721,8 @@ __global__ void __launch_bounds__(kAT) k_at_spmv(AInst* I) {
   block_reduce<1>(v, I->part);
 }
 
-// x += alpha d, r -= alpha q, rr = r . r
+// x += alpha d, r -= alpha q, rr = r . r; with VIN also the next V-cycle's level-0 input
+template <bool VIN>
 __global__ void __launch_bounds__(kAT) k_at_update(AInst* I) {
   ACtrl* C = I->ctrl;
   if (C->done) return;
@@ -707,6 +734,7 @@ __global__ void __launch_bounds__(kAT) k_at_update(AInst* I) {
     I->x[i] += alpha * I->d[i];
     const double r = I->r[i] - alpha * I->q[i];
     I->r[i] = r;
+    if (VIN) L.rhs[i] = float(r);   // the next V-cycle's input (air cells keep rhs 0)
     v[0] += r * r;
   }
   block_reduce<1>(v, I->part);
@@ -785,6 +813,7 @@ __global__ void k_at_start(AInst* I) {
     I->x[i] = 0.0;
     I->r[i] = L.label[i] ? I->b[i] : 0.0;
     I->d[i] = 0.0;
+    L.rhs[i] = L.label[i] ? float(I->b[i]) : 0.0f;   // the first V-cycle's input
   }
 }
 
@@ -869,15 +898,29 @@ __global__ void __launch_bounds__(kAT) k_at_div(AInst* I) {
   }
 }
 
-__global__ void k_at_div_fold(AInst* I, int slot0) {
-  if (threadIdx.x != 0) return;
+// The divergence receipt's fold: 256 threads over the partials in a fixed
+// stride, then a fixed tree (max and sum).
+__global__ void __launch_bounds__(kAT) k_at_div_fold(AInst* I, int slot0) {
+  __shared__ double sm[kAT], ss[kAT];
   double m = 0.0, s = 0.0;
-  for (int b = 0; b < kRedGrid; ++b) {
+  for (int b = threadIdx.x; b < kRedGrid; b += kAT) {
     m = fmax(m, I->part[4 * b]);
     s += I->part[4 * b + 1];
   }
-  I->ctrl->div[slot0] = m;
-  I->ctrl->div[slot0 + 1] = s;
+  sm[threadIdx.x] = m;
+  ss[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = kAT / 2; o > 0; o >>= 1) {
+    if (int(threadIdx.x) < o) {
+      sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
+      ss[threadIdx.x] += ss[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    I->ctrl->div[slot0] = sm[0];
+    I->ctrl->div[slot0 + 1] = ss[0];
+  }
 }
 
 __global__ void k_at_pressure(AInst* I, float* out, double pscale) {
@@ -1070,13 +1113,14 @@ void proj(fluid_pp_atlas* A, double* v, cudaStream_t s) {
   k_at_comp_sub<<<dim3(8, A->inst.ncomp), kAT, 0, s>>>(A->d_inst, v);
 }
 
-void vcycle(fluid_pp_atlas* A, cudaStream_t s) {
+void vcycle(fluid_pp_atlas* A, cudaStream_t s, bool vin) {
   const AInst& I = A->inst;
-  k_at_vin<<<grid_n(I.lv[0].n), kAT, 0, s>>>(A->d_inst);
+  if (vin) k_at_vin<<<grid_n(I.lv[0].n), kAT, 0, s>>>(A->d_inst);
   const int last = I.nlev - 1;
   for (int l = 0; l < last; ++l) {
     const int g = grid_n(I.lv[l].n);
-    k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 1);   // first colour from zero: elementwise
+    if (l == 0) k_at_smooth0_zero<<<I.nb, 256, 0, s>>>(A->d_inst);   // first colour from zero
+    else k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 1);
     if (l == 0) {
       k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 1);
       k_at_residual0<<<I.nb, 256, 0, s>>>(A->d_inst);
@@ -1101,20 +1145,29 @@ void vcycle(fluid_pp_atlas* A, cudaStream_t s) {
 }
 
 // One PCG iteration on stream s (kernels skip their work once the solve is done).
+// Without liquid components free of air (no projections) the V-cycle's input
+// is written by the previous update (and by the start for the first
+// iteration), and z is formed with its dot product in one pass.
 void iteration(fluid_pp_atlas* A, cudaStream_t s) {
   const AInst& I = A->inst;
   const int g0 = grid_n(I.lv[0].n);
-  if (I.precond) vcycle(A, s);
-  k_at_zvec<<<g0, kAT, 0, s>>>(A->d_inst);
-  proj(A, I.q, s);
-  k_at_dot_rq<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+  const bool fused = I.ncomp == 0;
+  if (I.precond) vcycle(A, s, !fused);
+  if (fused) {
+    k_at_zdot<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+  } else {
+    k_at_zvec<<<g0, kAT, 0, s>>>(A->d_inst);
+    proj(A, I.q, s);
+    k_at_dot_rq<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+  }
   k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 0);
   k_at_dir<<<g0, kAT, 0, s>>>(A->d_inst);
   k_at_set_gamma<<<1, 1, 0, s>>>(A->d_inst);
   proj(A, I.d, s);
   k_at_spmv0<<<I.nb, 256, 0, s>>>(A->d_inst, I.bpart);
   k_at_fold_bricks<<<1, 256, 0, s>>>(A->d_inst, I.bpart);
-  k_at_update<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+  if (fused && I.precond) k_at_update<true><<<kRedGrid, kAT, 0, s>>>(A->d_inst);
+  else k_at_update<false><<<kRedGrid, kAT, 0, s>>>(A->d_inst);
   if (I.ncomp) {
     proj(A, I.x, s);
     proj(A, I.r, s);
@@ -1386,7 +1439,7 @@ int fluid_pp_atlas_project(fluid_pp_atlas* A, float dt, const fluid_pp_solve_opt
   const int g0 = grid_n(n0);
   // divergence before, the right-hand side, the start
   k_at_div<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
-  k_at_div_fold<<<1, 32, 0, s>>>(A->d_inst, 0);
+  k_at_div_fold<<<1, kAT, 0, s>>>(A->d_inst, 0);
   k_at_rhs<<<g0, kAT, 0, s>>>(A->d_inst);
   proj(A, I.b, s);
   k_at_bb<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
@@ -1411,7 +1464,7 @@ int fluid_pp_atlas_project(fluid_pp_atlas* A, float dt, const fluid_pp_solve_opt
   k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 1);
   k_at_project<<<g0, kAT, 0, s>>>(A->d_inst);
   k_at_div<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
-  k_at_div_fold<<<1, 32, 0, s>>>(A->d_inst, 2);
+  k_at_div_fold<<<1, kAT, 0, s>>>(A->d_inst, 2);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(A->h_ctrl, I.ctrl, sizeof(ACtrl), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
