@@ -1861,7 +1861,7 @@ struct TrMem {
   float *gam, *gam2, *r1, *r2, *delta, *trace;
   float* sh[3];
   int* dep;
-  double* part;   // 3 kTrMassGrid partials, then 6 receipt values
+  double* part;   // 3 kTrMassGrid partials, 6 receipt values, the sharpening list counter
 };
 
 long long tr_floats(const fluid_pp* pp) {
@@ -1895,7 +1895,7 @@ TrMem tr_layout(fluid_pp* pp) {
 int ensure_transport(fluid_pp* pp) {
   if (pp->tr_mem) return FLUID_PP_OK;
   const long long n = pp->plan_cells();
-  const size_t bytes = ((size_t(tr_floats(pp)) * 4 + 15) & ~size_t(15)) + sizeof(double) * (3 * kTrMassGrid + 6);
+  const size_t bytes = ((size_t(tr_floats(pp)) * 4 + 15) & ~size_t(15)) + sizeof(double) * (3 * kTrMassGrid + 8);
   const cudaError_t e = dev_alloc(reinterpret_cast<void**>(&pp->tr_mem), bytes);
   if (e != cudaSuccess) return pp->set_error(FLUID_PP_OOM, std::string("density transport: ") + cudaGetErrorString(e));
   const TrMem M = tr_layout(pp);
@@ -1937,7 +1937,7 @@ int fluid_pp_transport_density(fluid_pp* pp, float dt, const fluid_pp_transport_
   TrDev T{I.nx, I.ny, I.nz, I.open_top, I.h, dt, I.u, I.v, I.w, {M.sh[0], M.sh[1], M.sh[2]}};
   cudaStream_t s = pp->stream;
   const int g = int(std::min<long long>((n + kThreads - 1) / kThreads, kMaxGrid));
-  for (int c = 0; c < 3; ++c) k_tr_shell<<<g, kThreads, 0, s>>>(T, c, M.sh[c]);
+  k_tr_shells<<<g, kThreads, 0, s>>>(T, M.sh[0], M.sh[1], M.sh[2]);
   float* vof = const_cast<float*>(I.vof);
   k_tr_mass_part<<<kTrMassGrid, 256, 0, s>>>(vof, n, M.part);
   k_tr_mass_fold<<<1, 256, 0, s>>>(M.part, kTrMassGrid, M.part + 3 * kTrMassGrid);
@@ -1957,11 +1957,15 @@ int fluid_pp_transport_density(fluid_pp* pp, float dt, const fluid_pp_transport_
   if (o.sharpening) {
     if (o.sharpening_mass_return) {
       cudaMemsetAsync(M.dep, 0, sizeof(int) * size_t(n), s);
-      k_tr_sharpen<<<g, kThreads, 0, s>>>(T, cr, strength, nr, M.delta);
-      k_tr_sharpen_scatter<<<g, kThreads, 0, s>>>(T, M.delta, nr, dist, M.dep);
+      // the trace offsets are spent: their buffer holds the list of cells losing density
+      unsigned* lost = reinterpret_cast<unsigned*>(M.trace);
+      unsigned* nlost = reinterpret_cast<unsigned*>(M.part + 3 * kTrMassGrid + 6);
+      cudaMemsetAsync(nlost, 0, sizeof(unsigned), s);
+      k_tr_sharpen<<<g, kThreads, 0, s>>>(T, cr, strength, nr, M.delta, lost, nlost);
+      k_tr_sharpen_scatter<<<g, kThreads, 0, s>>>(T, M.delta, nr, dist, lost, nlost, M.dep);
       k_tr_sharpen_resolve<<<g, kThreads, 0, s>>>(T, nr, M.dep, vof);
     } else {
-      k_tr_sharpen<<<g, kThreads, 0, s>>>(T, cr, strength, vof, M.delta);
+      k_tr_sharpen<<<g, kThreads, 0, s>>>(T, cr, strength, vof, M.delta, nullptr, nullptr);
     }
   } else {
     cudaMemcpyAsync(vof, cr, sizeof(float) * size_t(n), cudaMemcpyDeviceToDevice, s);

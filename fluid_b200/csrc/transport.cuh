@@ -230,14 +230,19 @@ __device__ __forceinline__ long long tr_corner(const TrDev& T, const TrStencil& 
                  n_ = (long long)(T).nx * (T).ny * (T).nz;                                       \
        i < n_; i += (long long)gridDim.x * blockDim.x)
 
-// The transport shell of component c from the MAC array: face F along the
-// axis (0 .. d + 1), cells across (0 .. d); F = 0, F = d (a wall unless it is
-// the open top) and every index past the lattice hold 0.
-__global__ void k_tr_shell(TrDev T, int c, float* __restrict__ out) {
-  const long long sy = tr_shell_sy(T.nx, c), sz = tr_shell_sz(T.nx, T.ny, c);
-  const long long total = tr_shell_size(T.nx, T.ny, T.nz, c);
-  const int wall_hi = (c == 1 && T.open_top) ? -1 : (c == 0 ? T.nx : (c == 1 ? T.ny : T.nz));
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+// The transport shells of the three components from the MAC arrays, in one
+// launch over their concatenation: face F along the component's axis
+// (0 .. d + 1), cells across (0 .. d); F = 0, F = d (a wall unless it is the
+// open top) and every index past the lattice hold 0.
+__global__ void k_tr_shells(TrDev T, float* __restrict__ s0, float* __restrict__ s1, float* __restrict__ s2) {
+  const long long n0 = tr_shell_size(T.nx, T.ny, T.nz, 0), n1 = tr_shell_size(T.nx, T.ny, T.nz, 1);
+  const long long total = n0 + n1 + tr_shell_size(T.nx, T.ny, T.nz, 2);
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
+    const int c = g < n0 ? 0 : (g < n0 + n1 ? 1 : 2);
+    const long long i = c == 0 ? g : (c == 1 ? g - n0 : g - n0 - n1);
+    float* out = c == 0 ? s0 : (c == 1 ? s1 : s2);
+    const long long sy = tr_shell_sy(T.nx, c), sz = tr_shell_sz(T.nx, T.ny, c);
+    const int wall_hi = (c == 1 && T.open_top) ? -1 : (c == 0 ? T.nx : (c == 1 ? T.ny : T.nz));
     const int iz = int(i / sz), iy = int((i / sy) % (sz / sy)), ix = int(i % sy);
     const int ic = c == 0 ? ix : (c == 1 ? iy : iz), dc = c == 0 ? T.nx : (c == 1 ? T.ny : T.nz);
     const bool across = (c != 0 && ix >= T.nx) || (c != 1 && iy >= T.ny) || (c != 2 && iz >= T.nz);
@@ -381,7 +386,7 @@ __device__ __forceinline__ float tr_face_open(const TrDev& T, int x, int y, int 
 
 // sharpenDeltaRho + sharpenCompute: rho_s = rho + delta, delta kept.
 __global__ void k_tr_sharpen(TrDev T, const float* __restrict__ rho, float strength, float* __restrict__ rho_s,
-                             float* __restrict__ delta) {
+                             float* __restrict__ delta, unsigned* __restrict__ lost, unsigned* nlost) {
   const float dT = __fmul_rn(__fmul_rn(3.0f, T.dt), strength);
   TR_CELLS(T) {
     const int x = int(i % T.nx), y = int((i / T.nx) % T.ny), z = int(i / ((long long)T.nx * T.ny));
@@ -415,6 +420,15 @@ __global__ void k_tr_sharpen(TrDev T, const float* __restrict__ rho, float stren
     else if (r > 0.5f) dr = 0.0f;
     rho_s[i] = __fadd_rn(r, dr);
     delta[i] = dr;
+    if (lost) {   // the cells whose mass the scatter carries, one run of the list per warp
+      const unsigned act = __activemask();
+      const unsigned bal = __ballot_sync(act, dr < 0.0f);
+      const int lane = threadIdx.x & 31, leader = __ffs(act) - 1;
+      unsigned base = 0;
+      if (lane == leader && bal) base = atomicAdd(nlost, unsigned(__popc(bal)));
+      base = __shfl_sync(act, base, leader);
+      if (dr < 0.0f) lost[base + __popc(bal & ((1u << lane) - 1u))] = unsigned(i);
+    }
   }
 }
 
@@ -435,11 +449,12 @@ __device__ float tr_sample_volume(const TrDev& T, const float* rho, TrV3 p) {
 // sharpenScatter: a cell that lost density carries it along the (sharpened)
 // density gradient towards the 0.5 contour and deposits it trilinearly.
 __global__ void k_tr_sharpen_scatter(TrDev T, const float* __restrict__ delta, const float* __restrict__ rho_s,
-                                     float max_dist, int* dep) {
+                                     float max_dist, const unsigned* __restrict__ lost, const unsigned* nlost, int* dep) {
   const float h2 = __fmul_rn(2.0f, T.h);
-  TR_CELLS(T) {
+  const unsigned m = *nlost;
+  for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+    const long long i = lost[k];
     const float dr = delta[i];
-    if (dr >= 0.0f) continue;
     const int x = int(i % T.nx), y = int((i / T.nx) % T.ny), z = int(i / ((long long)T.nx * T.ny));
     TrV3 p{__fadd_rn(float(x), 0.5f), __fadd_rn(float(y), 0.5f), __fadd_rn(float(z), 0.5f)};
     float travelled = 0.0f;
@@ -487,7 +502,7 @@ __global__ void k_tr_sharpen_resolve(TrDev T, const float* __restrict__ rho_s, c
 
 // Mass receipt: per-CTA float64 sums and min / max of rho in a fixed tree,
 // folded by one CTA in CTA order (the same bits for every launch).
-constexpr int kTrMassGrid = 296;
+constexpr int kTrMassGrid = 1184;
 
 __global__ void __launch_bounds__(256) k_tr_mass_part(const float* __restrict__ rho, long long n, double* part) {
   __shared__ double ss[256];
