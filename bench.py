@@ -113,14 +113,14 @@ def transport_bytes_per_cell(diffusion_iterations: int = 1) -> float:
     return 16 + 36 + 20 + 40 + 16 * passes + (8 if passes % 2 else 0) + 12 + 4 + 12 + 8
 
 
-def atlas_bytes_per_cell_iteration() -> float:
+def atlas_bytes_per_cell_iteration(sweeps: int = 2) -> float:
     """Algorithmic bytes of one V-cycle PCG iteration of the sparse atlas per
     level-0 cell (float32 level arrays, float64 CG vectors, byte labels; each
     array once per launch): the level-0 V-cycle (first colour from zero 13,
-    each tiled smoother colour 15 (three launches), residual 17, restriction 5,
-    prolongation 9, input 13) and the CG kernels (z 13, r.z 17, direction 25,
-    SpMV 21, update 49), times 8/7 for the coarser levels."""
-    return (13 + 3 * 15 + 17 + 5 + 9 + 13 + 13 + 17 + 25 + 21 + 49) * 8.0 / 7.0
+    each tiled smoother colour 15 (4 sweeps - 1 launches), residual 17,
+    restriction 5, prolongation 9, input 13) and the CG kernels (z 13, r.z 17,
+    direction 25, SpMV 21, update 49), times 8/7 for the coarser levels."""
+    return (13 + (4 * sweeps - 1) * 15 + 17 + 5 + 9 + 13 + 13 + 17 + 25 + 21 + 49) * 8.0 / 7.0
 
 
 def peaks():

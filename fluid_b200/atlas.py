@@ -83,9 +83,11 @@ class AtlasProjector:
         self.nbricks = nb
 
     def project(self, dt: float, cycle: str = "v", **opts) -> dict:
-        """cycle "v": one V-cycle on the brick hierarchy per PCG iteration;
-        "jacobi": the reference's diagonal preconditioner."""
-        o = solve_opts(**opts)
+        """cycle "v": one V-cycle on the brick hierarchy per PCG iteration,
+        two red-black sweeps before and after the coarse correction unless
+        pre_sweeps / post_sweeps say otherwise; "jacobi": the reference's
+        diagonal preconditioner."""
+        o = solve_opts(**{"pre_sweeps": 2, "post_sweeps": 2, **opts})
         o.cycle = {"v": 0, "jacobi": 2}[cycle]
         r = Receipt()
         rc = load().fluid_pp_atlas_project(self._h, float(dt), ctypes.byref(o), ctypes.byref(r))

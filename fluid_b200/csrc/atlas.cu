@@ -1090,6 +1090,7 @@ struct fluid_pp_atlas {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};   // one iteration: Jacobi, V-cycle
   bool graph_failed[2] = {false, false};
   bool use_graphs = true;
+  int pre = 1, post = 1;   // red-black sweeps before and after the coarse correction (every level)
   int set_error(int code, const std::string& m) {
     err = m;
     return code;
@@ -1123,9 +1124,17 @@ void vcycle(fluid_pp_atlas* A, cudaStream_t s, bool vin) {
     else k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 1);
     if (l == 0) {
       k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 1);
+      for (int k = 1; k < A->pre; ++k) {
+        k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 0);
+        k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 1);
+      }
       k_at_residual0<<<I.nb, 256, 0, s>>>(A->d_inst);
     } else {
       k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 1, 0);
+      for (int k = 1; k < A->pre; ++k) {
+        k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 0);
+        k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 1, 0);
+      }
       k_at_residual<<<g, kAT, 0, s>>>(A->d_inst, l);
     }
     k_at_restrict<<<grid_n(I.lv[l + 1].n), kAT, 0, s>>>(A->d_inst, l);
@@ -1134,12 +1143,14 @@ void vcycle(fluid_pp_atlas* A, cudaStream_t s, bool vin) {
   for (int l = last - 1; l >= 0; --l) {
     const int g = grid_n(I.lv[l].n);
     k_at_prolong<<<g, kAT, 0, s>>>(A->d_inst, l);
-    if (l == 0) {
-      k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 1);
-      k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 0);
-    } else {
-      k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 1, 0);
-      k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 0);
+    for (int k = 0; k < A->post; ++k) {
+      if (l == 0) {
+        k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 1);
+        k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 0);
+      } else {
+        k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 1, 0);
+        k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 0);
+      }
     }
   }
 }
@@ -1429,6 +1440,13 @@ int fluid_pp_atlas_project(fluid_pp_atlas* A, float dt, const fluid_pp_solve_opt
   }
   if (cycle != 0 && cycle != 2)
     return A->set_error(FLUID_PP_UNSUPPORTED, "atlas preconditioners: cycle 0 (V-cycle) or 2 (Jacobi)");
+  const int pre = opts ? opts->pre_sweeps : 2, post = opts ? opts->post_sweeps : 2;
+  if (pre < 1 || post < 1 || pre > 4 || post > 4) return A->set_error(FLUID_PP_INVALID_ARG, "sweeps: 1 to 4");
+  if (pre != A->pre || post != A->post) {   // the iteration graphs hold the launch sequence
+    A->pre = pre;
+    A->post = post;
+    drop_graphs(A);
+  }
   if (!(rel >= 0.0) || !(abs_tol >= 0.0) || max_iters <= 0) return A->set_error(FLUID_PP_INVALID_ARG, "bad solve options");
   cudaSetDevice(A->cfg.device);
   AInst& I = A->inst;

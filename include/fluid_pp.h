@@ -518,8 +518,9 @@ int fluid_pp_atlas_upload(fluid_pp_atlas* atlas, int nbricks, const int* coords,
                           const float* faces);
 /* PCG to ||b - A p|| <= max(abs_tol, rel_tol ||b||) (opts NULL: 1e-6, 200
  * iterations).  opts->cycle 0: one V-cycle on the brick hierarchy per
- * iteration; 2: Jacobi (the reference's own preconditioner); others
- * FLUID_PP_UNSUPPORTED.  Faces of rows with a liquid side take
+ * iteration (pre_sweeps / post_sweeps red-black sweeps on every level, 1 to
+ * 4; opts NULL: 2 and 2); 2: Jacobi (the reference's own preconditioner);
+ * others FLUID_PP_UNSUPPORTED.  Faces of rows with a liquid side take
  * u - (dt / rho) grad p / theta, faces of rows without one become 0, domain
  * walls keep their values.  Divergence receipts are over liquid cells. */
 int fluid_pp_atlas_project(fluid_pp_atlas* atlas, float dt, const fluid_pp_solve_opts* opts, fluid_pp_receipt* receipt);
