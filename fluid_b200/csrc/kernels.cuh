@@ -1141,62 +1141,7 @@ __global__ void __launch_bounds__(kThreads) k_update(const InstDev* insts, const
   }
 }
 
-// The k_update step without the per-tile arrival: every tile writes its
-// partials (block_sum / block_max folds), and k_update_finish folds each
-// instance's partials in tile order afterwards, so the bits are k_update's.
-__global__ void __launch_bounds__(kThreads) k_update_part(const InstDev* insts, const Tile* tiles, int ntiles) {
-  __shared__ double sh[64];
-  for_active_tiles(insts, tiles, ntiles, [](const InstDev& I) { return !I.ctrl->done; }, [&](int t) {
-    const Tile tl = tiles[t];
-    const InstDev& I = insts[tl.inst];
-    Ctrl* c = I.ctrl;
-    const int done = c->done;
-    const double alpha = c->alpha;
-    const LevelDev L = I.lv[0];
-    const int nt0 = I.ntiles0;
-    double* partial = I.partial;
-    float* __restrict__ X = I.x;
-    float* __restrict__ Xlo = I.xlo;
-    const float* __restrict__ D = dir_cur(I);
-    const float* __restrict__ Q = I.q;
-    if (done) return;
-    float* __restrict__ r = static_cast<float*>(L.rhs);
-    const uint8_t* __restrict__ lab = L.label;
-    const float alpha_f = float(alpha);
-    double rr = 0, mr = 0;
-    const TileIt it(tl.tile, L.nx, L.ny, L.nz, L.depth);
-    // every load of the column first (the label does not gate them), then the updates
-    float xh[kMaxDepth], xl[kMaxDepth], dv[kMaxDepth], qv[kMaxDepth], rv0[kMaxDepth];
-    uint8_t lb[kMaxDepth];
-    for_column(it, L.nx, L.ny, L.nz, [&](int k, int, int i) {
-      lb[k] = lab[i];
-      xh[k] = X[i];
-      xl[k] = Xlo[i];
-      dv[k] = D[i];
-      qv[k] = Q[i];
-      rv0[k] = r[i];
-    });
-    for_column(it, L.nx, L.ny, L.nz, [&](int k, int, int i) {
-      if (!lb[k]) return;
-      // double-single accumulation: x_hi + x_lo carries the pressure to ~1e-14
-      const double xv = double(xh[k]) + double(xl[k]) + alpha * double(dv[k]);
-      const float hi = float(xv);
-      X[i] = hi;
-      Xlo[i] = float(xv - double(hi));
-      const float rv = rv0[k] - alpha_f * qv[k];
-      r[i] = rv;
-      rr += double(rv) * rv;
-      mr = fmax(mr, fabs(double(rv)));
-    });
-    block_sum_max(rr, mr, sh);
-    if (threadIdx.x == 0) {
-      partial[tl.tile] = rr;
-      partial[nt0 + tl.tile] = mr;
-    }
-  });
-}
-
-// ||r||^2 and max|r| of each listed instance from its k_update_part partials (one CTA each).
+// ||r||^2 and max|r| of each listed instance from its k_cupdate partials (one CTA each).
 __global__ void __launch_bounds__(kThreads) k_update_finish(const InstDev* insts, const int* ilist) {
   __shared__ double sh[32];
   const InstDev& I = insts[ilist[blockIdx.x]];
