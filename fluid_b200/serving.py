@@ -141,7 +141,7 @@ class Server:
 
     def __init__(self, budget_bytes: float = 150e9, max_slots: int = 256, precision: str = "fp16", device: int = 0,
                  rel_tol: float = 1e-6, record: bool = False, admit_per_step: int = 1,
-                 cache_bytes: float = 16e9, reserve_bytes: float = 4e9, tall_slice_iterations: int = 4,
+                 cache_bytes: float = 16e9, reserve_bytes: float = 4e9, tall_slice_iterations: int = 3,
                  max_resident_cells: float = float("inf"), max_tall: int = 1 << 30, prefetch: int = 6):
         import torch
         self.torch = torch
