@@ -561,292 +561,306 @@ def main():
     stage_gbs = {k: round(stage_bytes_per_cell(k, sbytes) * cell_iters / (v["ms"] / 1000.0) / 1e9, 1)
                  for k, v in stages.items()}
 
-    # ------------------------------------ secondary: embedded solids (cut cells)
-    note("embedded solids")
-    sc = configs.solid_scene(*SOLID_DIMS)
-    ss = sc.state
-    dev4 = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (ss.vof, ss.u, ss.v, ss.w)]
+    # The per-feature workloads (embedded solids, LCP, extrapolation, transport,
+    # sparse atlas, tall cells) run at N = 1 only: under torchrun every rank
+    # would repeat the same single-GPU measurement and its CPU oracle.
+    def secondary_lines():
+        # ------------------------------------ secondary: embedded solids (cut cells)
+        note("embedded solids")
+        sc = configs.solid_scene(*SOLID_DIMS)
+        ss = sc.state
+        dev4 = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (ss.vof, ss.u, ss.v, ss.w)]
 
-    def run_solid(precision):
-        pp_ = PressureProjector((ss.nx, ss.ny, ss.nz), ss.h, ss.rho, ss.open_top, precision, device=local)
-        pp_.set_stream(stream.cuda_stream)
-        pp_.upload_solids(*sc.solids())
-        tt, rec_ = [], None
+        def run_solid(precision):
+            pp_ = PressureProjector((ss.nx, ss.ny, ss.nz), ss.h, ss.rho, ss.open_top, precision, device=local)
+            pp_.set_stream(stream.cuda_stream)
+            pp_.upload_solids(*sc.solids())
+            tt, rec_ = [], None
 
-        def step():
-            pp_.upload_state_device(*(t.data_ptr() for t in dev4))
-            return pp_.project(ss.dt, **opts)
+            def step():
+                pp_.upload_state_device(*(t.data_ptr() for t in dev4))
+                return pp_.project(ss.dt, **opts)
+            for k in range(args.warmup + SOLID_STEPS):
+                ms, rec_ = timed(step)
+                if k >= args.warmup:
+                    tt.append(ms)
+            p_ = pp_.pressure_cells().astype(np.float64)
+            pp_.destroy()
+            return tt, rec_, p_
+        t5, r5, p5 = run_solid("fp32")
+        t5m, r5m, p5m = run_solid(args.precision)
+        from oracle.oracle import Oracle
+        o5 = Oracle(ss.nx, ss.ny, ss.nz, ss.h, ss.rho, ss.open_top)
+        o5.set_threads(os.cpu_count() or 1)
+        o5.set_state(ss.vof, ss.u, ss.v, ss.w, ss.dt)
+        o5.set_solids(*sc.solids())
+        p5_ref, _ = o5.solve_mgpcg(1e-12, 0.0, 400, 2, 2)
+        nref = float(np.linalg.norm(p5_ref))
+        solids_line = {
+            "workload": sc.state.meta["workload"] + " (cell and dual-face open fractions by 8 samples, "
+                        "the ball's velocity on its faces)",
+            "cells": ss.cells, "steps": SOLID_STEPS,
+            "plain_fp32_solves_per_s": len(t5) / (sum(t5) / 1000.0), "plain_p50_ms": statistics.median(t5),
+            "mixed_solves_per_s": len(t5m) / (sum(t5m) / 1000.0), "mixed_p50_ms": statistics.median(t5m),
+            "iterations": r5["iterations"], "mixed_iterations": r5m["iterations"],
+            "status": [r5["status_name"], r5m["status_name"]],
+            "max_div_ratio": r5["max_div_after"] / max(r5["max_div_before"], 1e-30),
+            "fp64_error": {"plain_fp32": float(np.linalg.norm(p5 - p5_ref)) / nref,
+                           "mixed": float(np.linalg.norm(p5m - p5_ref)) / nref,
+                           "oracle": "float64 MGPCG of the CPU oracle with the same solids, rel-res 1e-12"},
+            "kernels": "face-weighted per-pass V-cycle and CG kernels (the fused column kernels assume uniform weights)",
+        }
+
+        # ------------------------------------ secondary: the CM11a LCP variant
+        note("LCP variant")
+        lc = configs.solid_scene(*SOLID_DIMS, sphere_velocity=(0.0, -2.0, 0.0), ball=(0.25, 0.35, 0.5))
+        ls = lc.state
+        dev6 = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (ls.vof, ls.u, ls.v, ls.w)]
+        lp = PressureProjector((ls.nx, ls.ny, ls.nz), ls.h, ls.rho, ls.open_top, args.precision, device=local)
+        lp.set_stream(stream.cuda_stream)
+        lp.upload_solids(*lc.solids())
+        t6, r6 = [], None
+
+        def lcp_step():
+            lp.upload_state_device(*(t.data_ptr() for t in dev6))
+            return lp.project_lcp(ls.dt)
         for k in range(args.warmup + SOLID_STEPS):
-            ms, rec_ = timed(step)
+            ms, r6 = timed(lcp_step)
             if k >= args.warmup:
-                tt.append(ms)
-        p_ = pp_.pressure_cells().astype(np.float64)
-        pp_.destroy()
-        return tt, rec_, p_
-    t5, r5, p5 = run_solid("fp32")
-    t5m, r5m, p5m = run_solid(args.precision)
-    from oracle.oracle import Oracle
-    o5 = Oracle(ss.nx, ss.ny, ss.nz, ss.h, ss.rho, ss.open_top)
-    o5.set_threads(os.cpu_count() or 1)
-    o5.set_state(ss.vof, ss.u, ss.v, ss.w, ss.dt)
-    o5.set_solids(*sc.solids())
-    p5_ref, _ = o5.solve_mgpcg(1e-12, 0.0, 400, 2, 2)
-    nref = float(np.linalg.norm(p5_ref))
-    solids_line = {
-        "workload": sc.state.meta["workload"] + " (cell and dual-face open fractions by 8 samples, "
-                    "the ball's velocity on its faces)",
-        "cells": ss.cells, "steps": SOLID_STEPS,
-        "plain_fp32_solves_per_s": len(t5) / (sum(t5) / 1000.0), "plain_p50_ms": statistics.median(t5),
-        "mixed_solves_per_s": len(t5m) / (sum(t5m) / 1000.0), "mixed_p50_ms": statistics.median(t5m),
-        "iterations": r5["iterations"], "mixed_iterations": r5m["iterations"],
-        "status": [r5["status_name"], r5m["status_name"]],
-        "max_div_ratio": r5["max_div_after"] / max(r5["max_div_before"], 1e-30),
-        "fp64_error": {"plain_fp32": float(np.linalg.norm(p5 - p5_ref)) / nref,
-                       "mixed": float(np.linalg.norm(p5m - p5_ref)) / nref,
-                       "oracle": "float64 MGPCG of the CPU oracle with the same solids, rel-res 1e-12"},
-        "kernels": "face-weighted per-pass V-cycle and CG kernels (the fused column kernels assume uniform weights)",
-    }
+                t6.append(ms)
+        x6 = lp.pressure_cells().astype(np.float64)
+        lp.destroy()
+        o6 = Oracle(ls.nx, ls.ny, ls.nz, ls.h, ls.rho, ls.open_top)
+        o6.set_threads(os.cpu_count() or 1)
+        o6.set_state(ls.vof, ls.u, ls.v, ls.w, ls.dt)
+        o6.set_solids(*lc.solids())
+        p6, i6 = o6.solve_lcp(3, 4)
+        lab6 = o6.level(0)[0].astype(bool)
+        solid6 = lab6 & (np.clip(lc.open, 0, 1) <= 1e-5)
+        lcp_line = {
+            "workload": ls.meta["workload"] + " with the ball inside the liquid moving down at 2 m/s (the bound active "
+                        "on the solid cells the linear solve would pull)",
+            "schedule": "3 full cycles + 4 V-cycles (the reference's), projected red-black smoother, 3 constrained levels",
+            "solves_per_s": len(t6) / (sum(t6) / 1000.0), "p50_ms": statistics.median(t6),
+            "projected_rel_residual": r6["true_rel_residual"], "rows_at_bound_oracle": i6["at_bound"],
+            "min_pressure_on_solid_unknowns": float(x6[solid6].min()) if solid6.any() else None,
+            "vs_fp64_oracle_schedule": float(np.linalg.norm(x6 - p6) / np.linalg.norm(p6)),
+            "precision": f"{args.precision} coarse levels, f32 level 0, f64 coarsest sweeps",
+        }
 
-    # ------------------------------------ secondary: the CM11a LCP variant
-    note("LCP variant")
-    lc = configs.solid_scene(*SOLID_DIMS, sphere_velocity=(0.0, -2.0, 0.0), ball=(0.25, 0.35, 0.5))
-    ls = lc.state
-    dev6 = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (ls.vof, ls.u, ls.v, ls.w)]
-    lp = PressureProjector((ls.nx, ls.ny, ls.nz), ls.h, ls.rho, ls.open_top, args.precision, device=local)
-    lp.set_stream(stream.cuda_stream)
-    lp.upload_solids(*lc.solids())
-    t6, r6 = [], None
-
-    def lcp_step():
-        lp.upload_state_device(*(t.data_ptr() for t in dev6))
-        return lp.project_lcp(ls.dt)
-    for k in range(args.warmup + SOLID_STEPS):
-        ms, r6 = timed(lcp_step)
-        if k >= args.warmup:
-            t6.append(ms)
-    x6 = lp.pressure_cells().astype(np.float64)
-    lp.destroy()
-    o6 = Oracle(ls.nx, ls.ny, ls.nz, ls.h, ls.rho, ls.open_top)
-    o6.set_threads(os.cpu_count() or 1)
-    o6.set_state(ls.vof, ls.u, ls.v, ls.w, ls.dt)
-    o6.set_solids(*lc.solids())
-    p6, i6 = o6.solve_lcp(3, 4)
-    lab6 = o6.level(0)[0].astype(bool)
-    solid6 = lab6 & (np.clip(lc.open, 0, 1) <= 1e-5)
-    lcp_line = {
-        "workload": ls.meta["workload"] + " with the ball inside the liquid moving down at 2 m/s (the bound active "
-                    "on the solid cells the linear solve would pull)",
-        "schedule": "3 full cycles + 4 V-cycles (the reference's), projected red-black smoother, 3 constrained levels",
-        "solves_per_s": len(t6) / (sum(t6) / 1000.0), "p50_ms": statistics.median(t6),
-        "projected_rel_residual": r6["true_rel_residual"], "rows_at_bound_oracle": i6["at_bound"],
-        "min_pressure_on_solid_unknowns": float(x6[solid6].min()) if solid6.any() else None,
-        "vs_fp64_oracle_schedule": float(np.linalg.norm(x6 - p6) / np.linalg.norm(p6)),
-        "precision": f"{args.precision} coarse levels, f32 level 0, f64 coarsest sweeps",
-    }
-
-    # ------------------------------------ secondary: velocity extrapolation
-    note("velocity extrapolation")
-    from oracle import oracle as orc
-    xs = configs.dam_spheres()
-    xpp = PressureProjector((xs.nx, xs.ny, xs.nz), xs.h, xs.rho, xs.open_top, args.precision, device=local)
-    xpp.set_stream(stream.cuda_stream)
-    devx = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (xs.vof, xs.u, xs.v, xs.w)]
-    xpp.upload_state_device(*(t.data_ptr() for t in devx))
-    xpp.project(xs.dt, **opts)
-    _, xu, xv, xw = xpp.download()   # the projected faces, the extrapolation's input
-    devxp = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (xs.vof, xu, xv, xw)]
-    t8 = []
-    for k in range(args.warmup + TRANSPORT_STEPS):
-        xpp.upload_state_device(*(t.data_ptr() for t in devxp))
-        ms, filled8 = timed(lambda: xpp.extrapolate_velocity())
-        if k >= args.warmup:
-            t8.append(ms)
-    _, eu, ev, ew = xpp.download()
-    xpp.destroy()
-    t_cpu8 = time.perf_counter()
-    (ou, ov, ow), filled_o, _ = orc.extrapolate_velocity(xs.nx, xs.ny, xs.nz, xs.h, xs.open_top, xs.vof, xu, xv, xw)
-    t_cpu8 = time.perf_counter() - t_cpu8
-    extrap_line = {
-        "workload": "the dam break + 16 spheres 128x96x128 step after its projection: FIM band of 2 cells, then "
-                    "the known-value hierarchy fill",
-        "cells": xs.cells, "steps": TRANSPORT_STEPS,
-        "extrapolations_per_s": len(t8) / (sum(t8) / 1000.0), "p50_ms": statistics.median(t8),
-        "filled_faces": int(filled8),
-        "bit_exact_vs_oracle": bool(int(filled8) == int(filled_o)
-                                    and all(np.array_equal(a.view(np.uint32), b.view(np.uint32))
-                                            for a, b in ((eu, ou), (ev, ov), (ew, ow)))),
-        "cpu_baseline": {"value": 1.0 / t_cpu8, "unit": "extrapolations/s", "cores": 1, "kind": "port",
-                         "sample": "one extrapolation of the same faces by the oracle's float32 restatement"},
-    }
-
-    # ------------------------------------ secondary: CM12 density transport
-    note("density transport")
-    tsc = configs.transport_scene(*TRANSPORT_DIMS, seed=21, cells_per_step=2.5)
-    devt = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (tsc.vof, tsc.u, tsc.v, tsc.w)]
-    tpp = PressureProjector((tsc.nx, tsc.ny, tsc.nz), tsc.h, tsc.rho, tsc.open_top, device=local)
-    tpp.set_stream(stream.cuda_stream)
-    tpp.upload_state_device(*(t.data_ptr() for t in devt))
-    tpp.set_gamma(None)
-    tpp.transport_density(tsc.dt)
-    rho_dev, g_dev = tpp.vof(), tpp.gamma()
-    t_cpu = time.perf_counter()
-    rho_orc, g_orc = orc.transport_density(tsc.nx, tsc.ny, tsc.nz, tsc.h, tsc.dt, tsc.open_top, tsc.vof, tsc.u, tsc.v,
-                                           tsc.w)
-    t_cpu = time.perf_counter() - t_cpu
-    tr_exact = bool(np.array_equal(rho_dev.view(np.uint32), rho_orc.view(np.uint32))
-                    and np.array_equal(g_dev.view(np.uint32), g_orc.view(np.uint32)))
-    tpp.upload_state_device(*(t.data_ptr() for t in devt))
-    tpp.set_gamma(None)
-    t7, r7s = [], []
-    for k in range(args.warmup + TRANSPORT_STEPS):
-        ms, r7 = timed(lambda: tpp.transport_density(tsc.dt))
-        if k >= args.warmup:
-            t7.append(ms)
-            r7s.append(r7)
-    tpp.destroy()
-    hbm7, kind7 = peaks()
-    tr_bytes = transport_bytes_per_cell(1) * tsc.cells
-    tr_gbs = tr_bytes / (statistics.mean(t7) / 1000.0) / 1e9
-    transport_line = {
-        "workload": tsc.meta["workload"] + ": dam block + ball, swirling face velocities on every open face "
-                    "(an extrapolated field), fastest face 2.5 cells per step, dt 1/60, consecutive steps with "
-                    "the persistent gamma carried",
-        "cells": tsc.cells, "steps": TRANSPORT_STEPS,
-        "steps_per_s": len(t7) / (sum(t7) / 1000.0), "p50_ms": statistics.median(t7),
-        "p99_ms": float(np.percentile(t7, 99)),
-        "cells_per_s": tsc.cells * len(t7) / (sum(t7) / 1000.0),
-        "passes": "trace + beta, deficit scatter, gather, 3 gamma-diffusion passes, sharpening + mass return",
-        "bit_exact_vs_oracle": tr_exact,
-        "mass_drift_rel_over_steps": (r7s[-1]["mass_after"] - r7s[0]["mass_before"]) / r7s[0]["mass_before"],
-        "roofline": {"bound": "hbm (formula); the traces are issue-bound", "alg_bytes_per_cell": transport_bytes_per_cell(1),
-                     "achieved": round(tr_gbs, 1), "peak": hbm7, "unit": "GB/s", "frac": round(tr_gbs / hbm7, 4),
-                     "peak_kind": kind7},
-        "cpu_baseline": {"value": 1.0 / t_cpu, "unit": "steps/s", "cores": 1, "kind": "port",
-                         "sample": "one step of the same lattice by the oracle's float32 restatement"},
-    }
-
-    # ------------------------------------ secondary: sparse brick atlas
-    note("sparse brick atlas")
-    from fluid_b200.atlas import AtlasProjector, bricks_from_dense
-    asc = configs.atlas_scene(*ATLAS_DIMS, seed=11, drops=40)
-    acoords = configs.atlas_bricks(asc.vof)
-    adens, afaces = bricks_from_dense(asc.vof, asc.u, asc.v, asc.w, acoords)
-    ap = AtlasProjector(ATLAS_DIMS, asc.h, asc.rho, device=local)
-    ap.set_stream(stream.cuda_stream)
-    atlas_runs = {}
-    for cyc in ("v", "jacobi"):
-        ta, ra = [], None
-        for k in range(args.warmup + ATLAS_STEPS):
-            ap.upload(acoords, adens, afaces)   # host planning and copies, outside the timed region
-            ms, ra = timed(lambda: ap.project(asc.dt, cycle=cyc, rel_tol=1e-6, max_iters=4000))
+        # ------------------------------------ secondary: velocity extrapolation
+        note("velocity extrapolation")
+        from oracle import oracle as orc
+        xs = configs.dam_spheres()
+        xpp = PressureProjector((xs.nx, xs.ny, xs.nz), xs.h, xs.rho, xs.open_top, args.precision, device=local)
+        xpp.set_stream(stream.cuda_stream)
+        devx = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (xs.vof, xs.u, xs.v, xs.w)]
+        xpp.upload_state_device(*(t.data_ptr() for t in devx))
+        xpp.project(xs.dt, **opts)
+        _, xu, xv, xw = xpp.download()   # the projected faces, the extrapolation's input
+        devxp = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (xs.vof, xu, xv, xw)]
+        t8 = []
+        for k in range(args.warmup + TRANSPORT_STEPS):
+            xpp.upload_state_device(*(t.data_ptr() for t in devxp))
+            ms, filled8 = timed(lambda: xpp.extrapolate_velocity())
             if k >= args.warmup:
-                ta.append(ms)
-        atlas_runs[cyc] = {"solves_per_s": len(ta) / (sum(ta) / 1000.0), "p50_ms": statistics.median(ta),
-                           "mean_ms": statistics.mean(ta),
-                           "iterations": ra["iterations"], "status": ra["status_name"],
-                           "true_rel_residual": ra["true_rel_residual"],
-                           "max_div_ratio": ra["max_div_after"] / max(ra["max_div_before"], 1e-30)}
-    ap.destroy()
-    # float64 parity and the CPU baseline on the 128x96x128 atlas (the dense oracle on the embedding)
-    asm = configs.atlas_scene(128, 96, 128, seed=11, drops=12)
-    scoords = configs.atlas_bricks(asm.vof)
-    sdens, sfaces = bricks_from_dense(asm.vof, asm.u, asm.v, asm.w, scoords)
-    ap = AtlasProjector((128, 96, 128), asm.h, asm.rho, device=local)
-    ap.set_stream(stream.cuda_stream)
-    ap.upload(scoords, sdens, sfaces)
-    ap.project(asm.dt, rel_tol=1e-6)
-    ps, _ = ap.download()
-    ap.destroy()
-    from oracle.oracle import Oracle as _Oracle
-    oa = _Oracle(128, 96, 128, asm.h, asm.rho)
-    oa.set_threads(os.cpu_count() or 1)
-    oa.set_state(asm.vof, asm.u, asm.v, asm.w, asm.dt)
-    pa_ref, _ = oa.solve_mgpcg(1e-12, 0.0, 400, 2, 2)
-    pa = np.zeros_like(pa_ref)
-    for k, (bx, by, bz) in enumerate(scoords):
-        pa[bz * 8:bz * 8 + 8, by * 8:by * 8 + 8, bx * 8:bx * 8 + 8] = ps[k] / (asm.rho * asm.h / asm.dt)
-    t_cpu_a = time.perf_counter()
-    _, ja = oa.solve_jacobi(1e-6, 0.0)
-    t_cpu_a = time.perf_counter() - t_cpu_a
-    hbm_a, kind_a = peaks()
-    a_alg = atlas_bytes_per_cell_iteration() * len(acoords) * 512 * atlas_runs["v"]["iterations"]
-    a_gbs = a_alg / (atlas_runs["v"]["mean_ms"] / 1000.0) / 1e9
-    atlas_line = {
-        "workload": asc.meta["workload"] + f": {len(acoords)} of {(ATLAS_DIMS[0] // 8) * (ATLAS_DIMS[1] // 8) * (ATLAS_DIMS[2] // 8)} "
-                    "bricks (8^3 cells) present, Gaussian velocities sigma 0.2 on faces with a liquid side, rel-res 1e-6",
-        "cells": len(acoords) * 512, "dense_equivalent_cells": int(np.prod(ATLAS_DIMS)), "steps": ATLAS_STEPS,
-        "v_cycle": atlas_runs["v"], "jacobi": atlas_runs["jacobi"],
-        "fp64_error_128x96x128": float(np.linalg.norm(pa - pa_ref) / np.linalg.norm(pa_ref)),
-        "roofline": {"bound": "hbm", "scope": "whole V-cycle PCG solve (setup, receipts and projection included)",
-                     "alg_bytes_per_cell_iteration": round(atlas_bytes_per_cell_iteration(), 1),
-                     "achieved": round(a_gbs, 1), "peak": hbm_a, "unit": "GB/s", "frac": round(a_gbs / hbm_a, 4),
-                     "peak_kind": kind_a},
-        "cpu_baseline": {"value": 1.0 / t_cpu_a, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "port",
-                         "sample": f"the 128x96x128 atlas ({len(scoords)} bricks) as its dense embedding: the oracle's "
-                                   f"float64 Jacobi-PCG (the reference's CPU algorithm) to rel-res 1e-6, "
-                                   f"{int(ja['iterations'])} iterations, OpenMP"},
-    }
+                t8.append(ms)
+        _, eu, ev, ew = xpp.download()
+        xpp.destroy()
+        t_cpu8 = time.perf_counter()
+        (ou, ov, ow), filled_o, _ = orc.extrapolate_velocity(xs.nx, xs.ny, xs.nz, xs.h, xs.open_top, xs.vof, xu, xv, xw)
+        t_cpu8 = time.perf_counter() - t_cpu8
+        extrap_line = {
+            "workload": "the dam break + 16 spheres 128x96x128 step after its projection: FIM band of 2 cells, then "
+                        "the known-value hierarchy fill",
+            "cells": xs.cells, "steps": TRANSPORT_STEPS,
+            "extrapolations_per_s": len(t8) / (sum(t8) / 1000.0), "p50_ms": statistics.median(t8),
+            "filled_faces": int(filled8),
+            "bit_exact_vs_oracle": bool(int(filled8) == int(filled_o)
+                                        and all(np.array_equal(a.view(np.uint32), b.view(np.uint32))
+                                                for a, b in ((eu, ou), (ev, ov), (ew, ow)))),
+            "cpu_baseline": {"value": 1.0 / t_cpu8, "unit": "extrapolations/s", "cores": 1, "kind": "port",
+                             "sample": "one extrapolation of the same faces by the oracle's float32 restatement"},
+        }
 
-    # ------------------------------------ secondary: tall-cell 256^2 columns x 1024 rows
-    note("tall-cell waves")
-    from fluid_b200.tall import TallProjector
-    ts = configs.tall_waves()
-    dev3 = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (ts.vof, ts.u, ts.v, ts.w)]
-    steps3 = max(3, min(args.steps, 20))
-
-    def run_tall(precision):
-        tp_ = TallProjector(ts.nx, ts.nz, ts.fine_ny, ts.band, ts.bases, ts.h, ts.rho, precision=precision,
-                            device=local)
-        tp_.set_stream(stream.cuda_stream)
-        tt, rec_ = [], None
-
-        def tall_step():
-            tp_.upload_state_device(*(t.data_ptr() for t in dev3))
-            return tp_.project(ts.dt, rel_tol=1e-6)
-        for k in range(args.warmup + steps3):
-            ms, rec_ = timed(tall_step)
+        # ------------------------------------ secondary: CM12 density transport
+        note("density transport")
+        tsc = configs.transport_scene(*TRANSPORT_DIMS, seed=21, cells_per_step=2.5)
+        devt = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (tsc.vof, tsc.u, tsc.v, tsc.w)]
+        tpp = PressureProjector((tsc.nx, tsc.ny, tsc.nz), tsc.h, tsc.rho, tsc.open_top, device=local)
+        tpp.set_stream(stream.cuda_stream)
+        tpp.upload_state_device(*(t.data_ptr() for t in devt))
+        tpp.set_gamma(None)
+        tpp.transport_density(tsc.dt)
+        rho_dev, g_dev = tpp.vof(), tpp.gamma()
+        t_cpu = time.perf_counter()
+        rho_orc, g_orc = orc.transport_density(tsc.nx, tsc.ny, tsc.nz, tsc.h, tsc.dt, tsc.open_top, tsc.vof, tsc.u, tsc.v,
+                                               tsc.w)
+        t_cpu = time.perf_counter() - t_cpu
+        tr_exact = bool(np.array_equal(rho_dev.view(np.uint32), rho_orc.view(np.uint32))
+                        and np.array_equal(g_dev.view(np.uint32), g_orc.view(np.uint32)))
+        tpp.upload_state_device(*(t.data_ptr() for t in devt))
+        tpp.set_gamma(None)
+        t7, r7s = [], []
+        for k in range(args.warmup + TRANSPORT_STEPS):
+            ms, r7 = timed(lambda: tpp.transport_density(tsc.dt))
             if k >= args.warmup:
-                tt.append(ms)
-        return tp_, tt, rec_
-    tp, t3, r3 = run_tall("fp32")
-    tpm, t3m, r3m = run_tall(args.precision)
-    # solve-level roofline of the tall path: the formula's bytes of every CG
-    # iteration over the whole solve time (setup and receipt included)
-    from fluid_b200.tall import plan_tall_hierarchy
-    tshapes = plan_tall_hierarchy(ts.nx, ts.nz, ts.fine_ny, ts.band, ts.bases)
-    tsamples = [lx * lz * (lb + 2) for lx, _, lz, lb in tshapes]
-    hbm3, kind3 = peaks()
+                t7.append(ms)
+                r7s.append(r7)
+        tpp.destroy()
+        hbm7, kind7 = peaks()
+        tr_bytes = transport_bytes_per_cell(1) * tsc.cells
+        tr_gbs = tr_bytes / (statistics.mean(t7) / 1000.0) / 1e9
+        transport_line = {
+            "workload": tsc.meta["workload"] + ": dam block + ball, swirling face velocities on every open face "
+                        "(an extrapolated field), fastest face 2.5 cells per step, dt 1/60, consecutive steps with "
+                        "the persistent gamma carried",
+            "cells": tsc.cells, "steps": TRANSPORT_STEPS,
+            "steps_per_s": len(t7) / (sum(t7) / 1000.0), "p50_ms": statistics.median(t7),
+            "p99_ms": float(np.percentile(t7, 99)),
+            "cells_per_s": tsc.cells * len(t7) / (sum(t7) / 1000.0),
+            "passes": "trace + beta, deficit scatter, gather, 3 gamma-diffusion passes, sharpening + mass return",
+            "bit_exact_vs_oracle": tr_exact,
+            "mass_drift_rel_over_steps": (r7s[-1]["mass_after"] - r7s[0]["mass_before"]) / r7s[0]["mass_before"],
+            "roofline": {"bound": "hbm (formula); the traces are issue-bound", "alg_bytes_per_cell": transport_bytes_per_cell(1),
+                         "achieved": round(tr_gbs, 1), "peak": hbm7, "unit": "GB/s", "frac": round(tr_gbs / hbm7, 4),
+                         "peak_kind": kind7},
+            "cpu_baseline": {"value": 1.0 / t_cpu, "unit": "steps/s", "cores": 1, "kind": "port",
+                             "sample": "one step of the same lattice by the oracle's float32 restatement"},
+        }
 
-    def tall_roofline(times, rec, storage):
-        alg = tall_bytes_per_iteration(tsamples, storage, sweeps=2) * rec["iterations"]   # the default two sweeps
-        gbs = alg / (statistics.mean(times) / 1000.0) / 1e9
-        return {"bound": "hbm", "scope": "whole solve (all kernels, setup and receipt included)",
-                "algorithmic_bytes_per_solve": alg, "achieved": round(gbs, 1), "peak": hbm3,
-                "unit": "GB/s", "frac": round(gbs / hbm3, 4), "peak_kind": kind3}
-    half = 4 if args.precision == "fp32" else 2
-    roof3 = tall_roofline(t3, r3, [4] * len(tsamples))
-    roof3m = tall_roofline(t3m, r3m, [4] + [half, half] + [4] * max(0, len(tsamples) - 3))
-    p3m = tpm.pressure()
-    tpm.destroy()
-    note("tall-cell float64 oracle")
-    tall_fp64 = tall_fp64_error(tp, ts, {"plain_fp32": tp.pressure(), "mixed": p3m})
-    tp.destroy()
-    tall_line = {
-        "workload": ts.meta["workload"] + ", surface 600 + 8 seeded sinusoids (amplitude <= 12, wavelength 16-256)",
-        "samples": ts.samples, "dense_equivalent_cells": ts.dense_cells, "steps": steps3,
-        "solves_per_s": len(t3) / (sum(t3) / 1000.0), "p50_ms": statistics.median(t3),
-        "p99_ms": float(np.percentile(t3, 99)), "iterations": r3["iterations"], "levels": r3["levels"],
-        "status": r3["status_name"], "true_rel_residual": r3["true_rel_residual"],
-        "sample_iterations_per_s": ts.samples * r3["iterations"] * len(t3) / (sum(t3) / 1000.0),
-        "precision": "f32 levels, f32 CG vectors, f64 dots/scalars/coarsest",
-        "mixed": {"precision": f"{args.precision} grid levels 1-2, f32 level 0 and block levels",
-                  "solves_per_s": len(t3m) / (sum(t3m) / 1000.0), "p50_ms": statistics.median(t3m),
-                  "iterations": r3m["iterations"], "status": r3m["status_name"],
-                  "true_rel_residual": r3m["true_rel_residual"], "roofline": roof3m},
-        "roofline": roof3,
-        "level_samples": tsamples,
-        "fp64_error": tall_fp64,
-    }
+        # ------------------------------------ secondary: sparse brick atlas
+        note("sparse brick atlas")
+        from fluid_b200.atlas import AtlasProjector, bricks_from_dense
+        asc = configs.atlas_scene(*ATLAS_DIMS, seed=11, drops=40)
+        acoords = configs.atlas_bricks(asc.vof)
+        adens, afaces = bricks_from_dense(asc.vof, asc.u, asc.v, asc.w, acoords)
+        ap = AtlasProjector(ATLAS_DIMS, asc.h, asc.rho, device=local)
+        ap.set_stream(stream.cuda_stream)
+        atlas_runs = {}
+        for cyc in ("v", "jacobi"):
+            ta, ra = [], None
+            for k in range(args.warmup + ATLAS_STEPS):
+                ap.upload(acoords, adens, afaces)   # host planning and copies, outside the timed region
+                ms, ra = timed(lambda: ap.project(asc.dt, cycle=cyc, rel_tol=1e-6, max_iters=4000))
+                if k >= args.warmup:
+                    ta.append(ms)
+            atlas_runs[cyc] = {"solves_per_s": len(ta) / (sum(ta) / 1000.0), "p50_ms": statistics.median(ta),
+                               "mean_ms": statistics.mean(ta),
+                               "iterations": ra["iterations"], "status": ra["status_name"],
+                               "true_rel_residual": ra["true_rel_residual"],
+                               "max_div_ratio": ra["max_div_after"] / max(ra["max_div_before"], 1e-30)}
+        ap.destroy()
+        # float64 parity and the CPU baseline on the 128x96x128 atlas (the dense oracle on the embedding)
+        asm = configs.atlas_scene(128, 96, 128, seed=11, drops=12)
+        scoords = configs.atlas_bricks(asm.vof)
+        sdens, sfaces = bricks_from_dense(asm.vof, asm.u, asm.v, asm.w, scoords)
+        ap = AtlasProjector((128, 96, 128), asm.h, asm.rho, device=local)
+        ap.set_stream(stream.cuda_stream)
+        ap.upload(scoords, sdens, sfaces)
+        ap.project(asm.dt, rel_tol=1e-6)
+        ps, _ = ap.download()
+        ap.destroy()
+        from oracle.oracle import Oracle as _Oracle
+        oa = _Oracle(128, 96, 128, asm.h, asm.rho)
+        oa.set_threads(os.cpu_count() or 1)
+        oa.set_state(asm.vof, asm.u, asm.v, asm.w, asm.dt)
+        pa_ref, _ = oa.solve_mgpcg(1e-12, 0.0, 400, 2, 2)
+        pa = np.zeros_like(pa_ref)
+        for k, (bx, by, bz) in enumerate(scoords):
+            pa[bz * 8:bz * 8 + 8, by * 8:by * 8 + 8, bx * 8:bx * 8 + 8] = ps[k] / (asm.rho * asm.h / asm.dt)
+        t_cpu_a = time.perf_counter()
+        _, ja = oa.solve_jacobi(1e-6, 0.0)
+        t_cpu_a = time.perf_counter() - t_cpu_a
+        hbm_a, kind_a = peaks()
+        a_alg = atlas_bytes_per_cell_iteration() * len(acoords) * 512 * atlas_runs["v"]["iterations"]
+        a_gbs = a_alg / (atlas_runs["v"]["mean_ms"] / 1000.0) / 1e9
+        atlas_line = {
+            "workload": asc.meta["workload"] + f": {len(acoords)} of {(ATLAS_DIMS[0] // 8) * (ATLAS_DIMS[1] // 8) * (ATLAS_DIMS[2] // 8)} "
+                        "bricks (8^3 cells) present, Gaussian velocities sigma 0.2 on faces with a liquid side, rel-res 1e-6",
+            "cells": len(acoords) * 512, "dense_equivalent_cells": int(np.prod(ATLAS_DIMS)), "steps": ATLAS_STEPS,
+            "v_cycle": atlas_runs["v"], "jacobi": atlas_runs["jacobi"],
+            "fp64_error_128x96x128": float(np.linalg.norm(pa - pa_ref) / np.linalg.norm(pa_ref)),
+            "roofline": {"bound": "hbm", "scope": "whole V-cycle PCG solve (setup, receipts and projection included)",
+                         "alg_bytes_per_cell_iteration": round(atlas_bytes_per_cell_iteration(), 1),
+                         "achieved": round(a_gbs, 1), "peak": hbm_a, "unit": "GB/s", "frac": round(a_gbs / hbm_a, 4),
+                         "peak_kind": kind_a},
+            "cpu_baseline": {"value": 1.0 / t_cpu_a, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "port",
+                             "sample": f"the 128x96x128 atlas ({len(scoords)} bricks) as its dense embedding: the oracle's "
+                                       f"float64 Jacobi-PCG (the reference's CPU algorithm) to rel-res 1e-6, "
+                                       f"{int(ja['iterations'])} iterations, OpenMP"},
+        }
+
+        # ------------------------------------ secondary: tall-cell 256^2 columns x 1024 rows
+        note("tall-cell waves")
+        from fluid_b200.tall import TallProjector
+        ts = configs.tall_waves()
+        dev3 = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (ts.vof, ts.u, ts.v, ts.w)]
+        steps3 = max(3, min(args.steps, 20))
+
+        def run_tall(precision):
+            tp_ = TallProjector(ts.nx, ts.nz, ts.fine_ny, ts.band, ts.bases, ts.h, ts.rho, precision=precision,
+                                device=local)
+            tp_.set_stream(stream.cuda_stream)
+            tt, rec_ = [], None
+
+            def tall_step():
+                tp_.upload_state_device(*(t.data_ptr() for t in dev3))
+                return tp_.project(ts.dt, rel_tol=1e-6)
+            for k in range(args.warmup + steps3):
+                ms, rec_ = timed(tall_step)
+                if k >= args.warmup:
+                    tt.append(ms)
+            return tp_, tt, rec_
+        tp, t3, r3 = run_tall("fp32")
+        tpm, t3m, r3m = run_tall(args.precision)
+        # solve-level roofline of the tall path: the formula's bytes of every CG
+        # iteration over the whole solve time (setup and receipt included)
+        from fluid_b200.tall import plan_tall_hierarchy
+        tshapes = plan_tall_hierarchy(ts.nx, ts.nz, ts.fine_ny, ts.band, ts.bases)
+        tsamples = [lx * lz * (lb + 2) for lx, _, lz, lb in tshapes]
+        hbm3, kind3 = peaks()
+
+        def tall_roofline(times, rec, storage):
+            alg = tall_bytes_per_iteration(tsamples, storage, sweeps=2) * rec["iterations"]   # the default two sweeps
+            gbs = alg / (statistics.mean(times) / 1000.0) / 1e9
+            return {"bound": "hbm", "scope": "whole solve (all kernels, setup and receipt included)",
+                    "algorithmic_bytes_per_solve": alg, "achieved": round(gbs, 1), "peak": hbm3,
+                    "unit": "GB/s", "frac": round(gbs / hbm3, 4), "peak_kind": kind3}
+        half = 4 if args.precision == "fp32" else 2
+        roof3 = tall_roofline(t3, r3, [4] * len(tsamples))
+        roof3m = tall_roofline(t3m, r3m, [4] + [half, half] + [4] * max(0, len(tsamples) - 3))
+        p3m = tpm.pressure()
+        tpm.destroy()
+        note("tall-cell float64 oracle")
+        tall_fp64 = tall_fp64_error(tp, ts, {"plain_fp32": tp.pressure(), "mixed": p3m})
+        tp.destroy()
+        tall_line = {
+            "workload": ts.meta["workload"] + ", surface 600 + 8 seeded sinusoids (amplitude <= 12, wavelength 16-256)",
+            "samples": ts.samples, "dense_equivalent_cells": ts.dense_cells, "steps": steps3,
+            "solves_per_s": len(t3) / (sum(t3) / 1000.0), "p50_ms": statistics.median(t3),
+            "p99_ms": float(np.percentile(t3, 99)), "iterations": r3["iterations"], "levels": r3["levels"],
+            "status": r3["status_name"], "true_rel_residual": r3["true_rel_residual"],
+            "sample_iterations_per_s": ts.samples * r3["iterations"] * len(t3) / (sum(t3) / 1000.0),
+            "precision": "f32 levels, f32 CG vectors, f64 dots/scalars/coarsest",
+            "mixed": {"precision": f"{args.precision} grid levels 1-2, f32 level 0 and block levels",
+                      "solves_per_s": len(t3m) / (sum(t3m) / 1000.0), "p50_ms": statistics.median(t3m),
+                      "iterations": r3m["iterations"], "status": r3m["status_name"],
+                      "true_rel_residual": r3m["true_rel_residual"], "roofline": roof3m},
+            "roofline": roof3,
+            "level_samples": tsamples,
+            "fp64_error": tall_fp64,
+        }
+        return {"embedded_solids_128x96x128": solids_line, "lcp_cm11a_128x96x128": lcp_line,
+                "velocity_extrapolation_128x96x128": extrap_line, "density_transport_128x96x128": transport_line,
+                "sparse_atlas_256x192x256": atlas_line, "tall_cell_256x256x1024": tall_line}
+
+    if world == 1:
+        sec = secondary_lines()
+    else:
+        sec = {k: {"skipped": "measured at N = 1 only (each rank would repeat the single-GPU workload)"}
+               for k in ("embedded_solids_128x96x128", "lcp_cm11a_128x96x128", "velocity_extrapolation_128x96x128",
+                         "density_transport_128x96x128", "sparse_atlas_256x192x256", "tall_cell_256x256x1024")}
 
     # ------------------------- serving: Poisson stream with continuous batching
     serving = None
@@ -1013,12 +1027,7 @@ def main():
                                   "v": cycles["v"], "f": cycles["f"],
                                   "note": "v: one V-cycle under PCG (fused column kernels); f: one full cycle "
                                           "under flexible CG (per-pass kernels); same inputs, same tolerance"},
-        "embedded_solids_128x96x128": solids_line,
-        "lcp_cm11a_128x96x128": lcp_line,
-        "velocity_extrapolation_128x96x128": extrap_line,
-        "density_transport_128x96x128": transport_line,
-        "sparse_atlas_256x192x256": atlas_line,
-        "tall_cell_256x256x1024": tall_line,
+        **sec,
         "serving": serving,
         "roofline": {"bound": "hbm", "kernel": dom, "workload": "the headline batch (64 instances per launch)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
