@@ -171,14 +171,15 @@ __device__ __forceinline__ float tr_length(TrV3 v) {
 __device__ TrV3 tr_trace(const TrDev& T, int x, int y, int z, float dir) {
   const TrV3 pos{__fadd_rn(float(x), 0.5f), __fadd_rn(float(y), 0.5f), __fadd_rn(float(z), 0.5f)};
   const float h = T.h, dt = T.dt;
-  const float steps_f = ceilf(__fdiv_rn(__fmul_rn(tr_length(tr_sample(T, pos)), dt), h));
+  const TrV3 v0 = tr_sample(T, pos);   // also the first sub-step's start sample (same point)
+  const float steps_f = ceilf(__fdiv_rn(__fmul_rn(tr_length(v0), dt), h));
   int steps = steps_f >= 16.0f ? 16 : int(steps_f);
   if (steps < 1) steps = 1;
   const float sdt = __fdiv_rn(dt, float(steps));
   const float half = __fmul_rn(dir, 0.5f);
   TrV3 p = pos;
   for (int s = 0; s < steps; ++s) {
-    const TrV3 a = tr_sample(T, p);
+    const TrV3 a = s == 0 ? v0 : tr_sample(T, p);
     const TrV3 mid = tr_clamp_trace(T, TrV3{__fadd_rn(p.x, __fdiv_rn(__fmul_rn(__fmul_rn(half, a.x), sdt), h)),
                                             __fadd_rn(p.y, __fdiv_rn(__fmul_rn(__fmul_rn(half, a.y), sdt), h)),
                                             __fadd_rn(p.z, __fdiv_rn(__fmul_rn(__fmul_rn(half, a.z), sdt), h))});
