@@ -243,46 +243,6 @@ __device__ __forceinline__ long long face_index(int slot, int a, int lx, int ly,
   return (long long)slot * 3 * kFaces + (long long)a * kFaces + off;
 }
 
-// The stored value of the face on the low side (s = -1) or high side (+1) of
-// level-0 cell c along axis a: a port's value is the lower brick's copy.
-__device__ __forceinline__ float face_value(const AInst* I, const Cell& c, int a, int s) {
-  int l[3] = {c.lx, c.ly, c.lz};
-  if (s > 0) {
-    l[a] += 1;
-    return I->faces[face_index(c.slot, a, l[0], l[1], l[2])];
-  }
-  if (l[a] > 0) return I->faces[face_index(c.slot, a, l[0], l[1], l[2])];
-  // low face of the brick: the lower neighbour's f = 8 copy when it exists
-  const ALevel& L = I->lv[0];
-  int bc[3] = {L.coords[3 * c.slot], L.coords[3 * c.slot + 1], L.coords[3 * c.slot + 2]};
-  if (bc[a] > 0) {
-    bc[a] -= 1;
-    const int t = L.table[bc[0] + L.gx * (bc[1] + L.gy * bc[2])];
-    if (t >= 0) {
-      l[a] = kRes;
-      return I->faces[face_index(t, a, l[0], l[1], l[2])];
-    }
-  }
-  return I->faces[face_index(c.slot, a, l[0], l[1], l[2])];
-}
-
-// b = G^T u on liquid cells: the low face's value minus the high face's over
-// every face that is a row (not a domain wall).
-__global__ void k_at_rhs(AInst* I) {
-  const ALevel& L = I->lv[0];
-  A_CELLS(L) {
-    double b = 0.0;
-    if (L.label[i]) {
-      const Cell c = cell_of(L, i);
-      for (int a = 0; a < 3; ++a) {
-        if (neighbour(L, c, a, -1) != kWall) b += double(face_value(I, c, a, -1));
-        if (neighbour(L, c, a, +1) != kWall) b -= double(face_value(I, c, a, +1));
-      }
-    }
-    I->b[i] = b;
-  }
-}
-
 // (A v)_i for a liquid level-0 cell, float64.
 __device__ __forceinline__ double apply0(const AInst* I, const double* v, long long i) {
   const ALevel& L = I->lv[0];
@@ -817,110 +777,191 @@ __global__ void k_at_start(AInst* I) {
   }
 }
 
-// Faces: u -= jump / theta on rows with a liquid side, 0 on rows without;
-// domain walls keep their values.  Both copies of a port are written.
-__global__ void k_at_project(AInst* I) {
-  const ALevel& L = I->lv[0];
-  A_CELLS(L) {
-    const Cell c = cell_of(L, i);
-    for (int a = 0; a < 3; ++a) {
-      // the cell's high face on axis a; low faces of bricks whose lower
-      // neighbour is absent are handled by the cell itself below
-      for (int sd = -1; sd <= 1; sd += 2) {
-        const int lcoord = a == 0 ? c.lx : (a == 1 ? c.ly : c.lz);
-        if (sd < 0 && lcoord > 0) continue;   // interior low faces are the lower cell's high faces
-        const long long j = neighbour(L, c, a, sd);
-        if (j == kWall) continue;
-        if (sd < 0 && j >= 0) continue;       // a port: the lower brick's cell writes it
-        const bool li = L.label[i] != 0;
-        const bool lj = j >= 0 && L.label[j] != 0;
-        float val;
-        int lc[3] = {c.lx, c.ly, c.lz};
-        if (sd > 0) lc[a] += 1;
-        const long long fi = face_index(c.slot, a, lc[0], lc[1], lc[2]);
-        const float u0 = face_value(I, c, a, sd);
-        if (!li && !lj) {
-          val = 0.0f;
-        } else {
-          // jump = p(pos) - p(neg) over liquid terms; the cell is the neg side for sd > 0
-          const double pi = li ? I->x[i] : 0.0;
-          const double pj = lj ? I->x[j] : 0.0;
-          const double jump = sd > 0 ? pj - pi : pi - pj;
-          double th = 1.0;
-          if (li != lj) {
-            const double lphi = li ? L.phi[i] : L.phi[j];
-            const double aphi = j < 0 ? 0.5 : (li ? L.phi[j] : L.phi[i]);
-            th = theta_d(lphi, aphi);
-          }
-          val = float(double(u0) - jump / th);
-        }
-        I->faces[fi] = val;
-        if (sd > 0 && j >= 0 && lc[a] == kRes) {   // the port's copy in the upper brick
-          const Cell cj = cell_of(L, j);
-          int lu[3] = {cj.lx, cj.ly, cj.lz};
-          I->faces[face_index(cj.slot, a, lu[0], lu[1], lu[2])] = val;
-        }
-      }
+// ------------------------------------------ the faces, one CTA per brick
+// A brick's six neighbour slots (-1 absent) and which of its faces lie on the
+// domain walls, index 2 a + (side > 0).
+__device__ __forceinline__ void brick_sides(const ALevel& L, int slot, int* nbs, int* nbw) {
+  if (threadIdx.x < 6) {
+    const int a = threadIdx.x >> 1, sd = (threadIdx.x & 1) ? 1 : -1;
+    int b[3] = {L.coords[3 * slot], L.coords[3 * slot + 1], L.coords[3 * slot + 2]};
+    const int g[3] = {L.gx, L.gy, L.gz};
+    b[a] += sd;
+    const bool wall = b[a] < 0 || b[a] >= g[a];
+    nbw[threadIdx.x] = wall;
+    nbs[threadIdx.x] = wall ? -1 : L.table[b[0] + L.gx * (b[1] + L.gy * b[2])];
+  }
+}
+
+// Face entry k (0 .. 575) of a brick's axis-A array as local (x, y, z), the
+// axis coordinate being the face index 0 .. 8; face_off is the inverse.
+template <int A>
+__device__ __forceinline__ void face_local(int k, int* l) {
+  if (A == 0) { l[0] = k % (kRes + 1); l[1] = (k / (kRes + 1)) % kRes; l[2] = k / ((kRes + 1) * kRes); }
+  else if (A == 1) { l[0] = k % kRes; l[1] = (k / kRes) % (kRes + 1); l[2] = k / (kRes * (kRes + 1)); }
+  else { l[0] = k % kRes; l[1] = (k / kRes) % kRes; l[2] = k / (kRes * kRes); }
+}
+
+template <int A>
+__device__ __forceinline__ int face_off(int x, int y, int z) {
+  if (A == 0) return x + (kRes + 1) * (y + kRes * z);
+  if (A == 1) return x + kRes * (y + (kRes + 1) * z);
+  return x + kRes * (y + kRes * z);
+}
+
+// Stage a brick's axis-A faces in shared memory, the canonical copy of each
+// port (a low face shared with a present lower brick is that brick's f = 8
+// copy); with sync the brick's own f = 0 copy of such a port is set to it.
+template <int A>
+__device__ __forceinline__ void stage_faces(const AInst* I, int slot, const int* nbs, int sync, float* fs) {
+  for (int k = threadIdx.x; k < kFaces; k += blockDim.x) {
+    int l[3];
+    face_local<A>(k, l);
+    const long long own = (long long)slot * 3 * kFaces + (long long)A * kFaces + k;
+    if (l[A] == 0 && nbs[2 * A] >= 0) {
+      l[A] = kRes;
+      const float v = I->faces[(long long)nbs[2 * A] * 3 * kFaces + (long long)A * kFaces + face_off<A>(l[0], l[1], l[2])];
+      fs[k] = v;
+      if (sync) I->faces[own] = v;
+    } else {
+      fs[k] = I->faces[own];
     }
   }
 }
 
-// Divergence receipt over liquid cells: max |b| and sum b^2 of the current faces.
-__global__ void __launch_bounds__(kAT) k_at_div(AInst* I) {
+// The axis-A part of b for local cell l: its low face minus its high face,
+// each only where it is a row (not a domain wall).
+template <int A>
+__device__ __forceinline__ double div_axis(const float* fs, const int* nbw, const int* l) {
+  int h[3] = {l[0], l[1], l[2]};
+  h[A] += 1;
+  double b = 0.0;
+  if (!(l[A] == 0 && nbw[2 * A])) b += double(fs[face_off<A>(l[0], l[1], l[2])]);
+  if (!(l[A] == kRes - 1 && nbw[2 * A + 1])) b -= double(fs[face_off<A>(h[0], h[1], h[2])]);
+  return b;
+}
+
+// b = G^T u of every cell of the brick (0 off the liquid), written to I->b
+// when write_b, and the brick's max |b| and sum b^2 over liquid cells into
+// bpart[2 brick ..].  With write_b the brick's own f = 0 copy of each port is
+// also set to the canonical value, so that the projection can read its own
+// copies.  No CTA writes a face another CTA reads here: f = 8 copies are only
+// read.
+__global__ void __launch_bounds__(256) k_at_div0(AInst* I, int write_b, double* bpart) {
   const ALevel& L = I->lv[0];
-  double v[2] = {0.0, 0.0};
-  A_CELLS(L) {
-    if (!L.label[i]) continue;
-    const Cell c = cell_of(L, i);
-    double b = 0.0;
-    for (int a = 0; a < 3; ++a) {
-      if (neighbour(L, c, a, -1) != kWall) b += double(face_value(I, c, a, -1));
-      if (neighbour(L, c, a, +1) != kWall) b -= double(face_value(I, c, a, +1));
-    }
-    v[0] = fmax(v[0], fabs(b));
-    v[1] += b * b;
-  }
-  // max and sum in one tree: the max slot folds with max
-  __shared__ double sm[kAT], ss[kAT];
-  sm[threadIdx.x] = v[0];
-  ss[threadIdx.x] = v[1];
+  const int slot = blockIdx.x;
+  __shared__ float fs[3][kFaces];
+  __shared__ int nbs[6], nbw[6];
+  brick_sides(L, slot, nbs, nbw);
   __syncthreads();
-  for (int o = kAT / 2; o > 0; o >>= 1) {
+  stage_faces<0>(I, slot, nbs, write_b, fs[0]);
+  stage_faces<1>(I, slot, nbs, write_b, fs[1]);
+  stage_faces<2>(I, slot, nbs, write_b, fs[2]);
+  __syncthreads();
+  double mx = 0.0, ss = 0.0;
+  for (int k = threadIdx.x; k < kCells; k += 256) {
+    const int l[3] = {k & 7, (k >> 3) & 7, k >> 6};
+    const long long i = (long long)slot * kCells + k;
+    double b = 0.0;
+    if (L.label[i]) {
+      b += div_axis<0>(fs[0], nbw, l);
+      b += div_axis<1>(fs[1], nbw, l);
+      b += div_axis<2>(fs[2], nbw, l);
+      mx = fmax(mx, fabs(b));
+      ss += b * b;
+    }
+    if (write_b) I->b[i] = b;
+  }
+  __shared__ double sm[256], sq[256];
+  sm[threadIdx.x] = mx;
+  sq[threadIdx.x] = ss;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
     if (int(threadIdx.x) < o) {
       sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
-      ss[threadIdx.x] += ss[threadIdx.x + o];
+      sq[threadIdx.x] += sq[threadIdx.x + o];
     }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    I->part[4 * blockIdx.x] = sm[0];
-    I->part[4 * blockIdx.x + 1] = ss[0];
+    bpart[2 * slot] = sm[0];
+    bpart[2 * slot + 1] = sq[0];
   }
 }
 
-// The divergence receipt's fold: 256 threads over the partials in a fixed
-// stride, then a fixed tree (max and sum).
-__global__ void __launch_bounds__(kAT) k_at_div_fold(AInst* I, int slot0) {
-  __shared__ double sm[kAT], ss[kAT];
-  double m = 0.0, s = 0.0;
-  for (int b = threadIdx.x; b < kRedGrid; b += kAT) {
-    m = fmax(m, I->part[4 * b]);
-    s += I->part[4 * b + 1];
+// The divergence receipt from the per-brick partials (fixed stride and tree).
+__global__ void __launch_bounds__(256) k_at_div_fold_bricks(AInst* I, const double* bpart, int slot0) {
+  __shared__ double sm[256], sq[256];
+  double m = 0.0, q = 0.0;
+  for (int b = threadIdx.x; b < I->nb; b += 256) {
+    m = fmax(m, bpart[2 * b]);
+    q += bpart[2 * b + 1];
   }
   sm[threadIdx.x] = m;
-  ss[threadIdx.x] = s;
+  sq[threadIdx.x] = q;
   __syncthreads();
-  for (int o = kAT / 2; o > 0; o >>= 1) {
+  for (int o = 128; o > 0; o >>= 1) {
     if (int(threadIdx.x) < o) {
       sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
-      ss[threadIdx.x] += ss[threadIdx.x + o];
+      sq[threadIdx.x] += sq[threadIdx.x + o];
     }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
     I->ctrl->div[slot0] = sm[0];
-    I->ctrl->div[slot0 + 1] = ss[0];
+    I->ctrl->div[slot0 + 1] = sq[0];
   }
+}
+
+// The projection of a brick's own faces: u - jump / theta on rows with a
+// liquid side, 0 on rows without, walls kept.  A port (a face shared with a
+// present neighbour brick) is computed by both bricks from the same values:
+// the pressures and levels of its two cells, and the face value, whose two
+// copies k_at_div0 made equal.  Each CTA reads and writes only its own faces.
+template <int A>
+__device__ __forceinline__ void project_axis(AInst* I, int slot, const int* nbs, const int* nbw, const double* xs,
+                                             const float* ph, const uint8_t* lb) {
+  for (int k = threadIdx.x; k < kFaces; k += blockDim.x) {
+    int l[3];
+    face_local<A>(k, l);
+    const int f = l[A];
+    if ((f == 0 && nbw[2 * A]) || (f == kRes && nbw[2 * A + 1])) continue;   // a domain wall keeps its value
+    const bool lo_absent = f == 0 && nbs[2 * A] < 0, hi_absent = f == kRes && nbs[2 * A + 1] < 0;
+    int lo[3] = {l[0], l[1], l[2]};
+    lo[A] = f - 1;
+    const int tlo = tix(lo[0], lo[1], lo[2]), thi = tix(l[0], l[1], l[2]);
+    const bool li = !lo_absent && lb[tlo] != 0, lj = !hi_absent && lb[thi] != 0;
+    const long long own = (long long)slot * 3 * kFaces + (long long)A * kFaces + k;
+    float val = 0.0f;
+    if (li || lj) {
+      const float u0 = I->faces[own];
+      const double jump = (lj ? xs[thi] : 0.0) - (li ? xs[tlo] : 0.0);
+      double th = 1.0;
+      if (li != lj) {
+        const double lphi = li ? ph[tlo] : ph[thi];
+        const bool air_absent = li ? hi_absent : lo_absent;
+        const double aphi = air_absent ? 0.5 : (li ? ph[thi] : ph[tlo]);
+        th = theta_d(lphi, aphi);
+      }
+      val = float(double(u0) - jump / th);
+    }
+    I->faces[own] = val;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_at_project0(AInst* I) {
+  const ALevel& L = I->lv[0];
+  const int slot = blockIdx.x;
+  __shared__ double xs[kTile];
+  __shared__ float ph[kTile];
+  __shared__ uint8_t lb[kTile];
+  __shared__ int nbs[6], nbw[6];
+  brick_sides(L, slot, nbs, nbw);
+  load_tile<double>(L, slot, I->x, xs);
+  load_tile<float>(L, slot, L.phi, ph);
+  load_tile<uint8_t>(L, slot, L.label, lb);
+  project_axis<0>(I, slot, nbs, nbw, xs, ph, lb);
+  project_axis<1>(I, slot, nbs, nbw, xs, ph, lb);
+  project_axis<2>(I, slot, nbs, nbw, xs, ph, lb);
 }
 
 __global__ void k_at_pressure(AInst* I, float* out, double pscale) {
@@ -1402,7 +1443,7 @@ int fluid_pp_atlas_upload(fluid_pp_atlas* A, int nbricks, const int* coords, con
   float* d_rho = static_cast<float*>(put(rho.data(), 4 * size_t(n0)));
   I.faces = static_cast<float*>(put(faces, 4 * size_t(nbricks) * 3 * kFaces));
   I.part = static_cast<double*>(take(8 * 4 * kRedGrid));
-  I.bpart = static_cast<double*>(take(8 * size_t(nbricks)));
+  I.bpart = static_cast<double*>(take(16 * size_t(nbricks)));
   I.coarse_inv = static_cast<double*>(take(8 * kAtCoarseMax * kAtCoarseMax));
   I.coarse_m = int(lv.back().n());
   I.ncomp = ncomp;
@@ -1456,9 +1497,8 @@ int fluid_pp_atlas_project(fluid_pp_atlas* A, float dt, const fluid_pp_solve_opt
   const long long n0 = I.lv[0].n;
   const int g0 = grid_n(n0);
   // divergence before, the right-hand side, the start
-  k_at_div<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
-  k_at_div_fold<<<1, kAT, 0, s>>>(A->d_inst, 0);
-  k_at_rhs<<<g0, kAT, 0, s>>>(A->d_inst);
+  k_at_div0<<<I.nb, 256, 0, s>>>(A->d_inst, 1, I.bpart);
+  k_at_div_fold_bricks<<<1, 256, 0, s>>>(A->d_inst, I.bpart, 0);
   proj(A, I.b, s);
   k_at_bb<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
   k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 2, 0);
@@ -1480,9 +1520,9 @@ int fluid_pp_atlas_project(fluid_pp_atlas* A, float dt, const fluid_pp_solve_opt
   // float64 true residual, projected faces, receipts
   k_at_true<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
   k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 1);
-  k_at_project<<<g0, kAT, 0, s>>>(A->d_inst);
-  k_at_div<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
-  k_at_div_fold<<<1, kAT, 0, s>>>(A->d_inst, 2);
+  k_at_project0<<<I.nb, 256, 0, s>>>(A->d_inst);
+  k_at_div0<<<I.nb, 256, 0, s>>>(A->d_inst, 0, I.bpart);
+  k_at_div_fold_bricks<<<1, 256, 0, s>>>(A->d_inst, I.bpart, 2);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(A->h_ctrl, I.ctrl, sizeof(ACtrl), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
