@@ -1815,7 +1815,8 @@ int fluid_pp_extrapolate_velocity(fluid_pp* pp, long long* filled_faces) {
   for (int k = 0; k < passes; ++k) {
     const int src = k & 1;
     k_ext_reset<<<1, 1, 0, s>>>(E.count, 1 - src);
-    k_ext_update<<<grid(n), kThreads, 0, s>>>(E, src);
+    if (E.solids) k_ext_update<true><<<grid(n), kThreads, 0, s>>>(E, src);
+    else k_ext_update<false><<<grid(n), kThreads, 0, s>>>(E, src);
   }
   const int last = passes & 1;
   const float4* result = E.val[last];
