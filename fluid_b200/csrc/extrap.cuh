@@ -253,8 +253,11 @@ __device__ __forceinline__ bool touches_source(const ExtDev& E, int x, int y, in
     if (const int x = int(i % (E).nx), y = int((i / (E).nx) % (E).ny), z = int(i / ((long long)(E).nx * (E).ny)); \
         true)
 
-// seedActiveFront into side 0.
-__global__ void k_ext_seed(ExtDev E) {
+// seedActiveFront into both sides (SOLIDS as in k_ext_update).
+template <bool SOLIDS>
+__global__ void k_ext_seed(ExtDev Ein) {
+  ExtDev E = Ein;
+  E.solids = SOLIDS ? 1 : 0;
   unsigned active_total = 0;
   EXT_FOR_CELLS(E, x, y, z, i) {
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f), d = make_float4(kDistInf, kDistInf, kDistInf, 0.f);
@@ -262,7 +265,8 @@ __global__ void k_ext_seed(ExtDev E) {
     for (int c = 0; c < 3; ++c) {
       if (!ext_open(E, x, y, z, c)) continue;
       if (ext_source(E, x, y, z, c)) {
-        set3(v, c, E.vel[c][ext_face(E, c, x, y, z)]);
+        const float* vc = c == 0 ? E.vel[0] : (c == 1 ? E.vel[1] : E.vel[2]);
+        set3(v, c, vc[ext_face(E, c, x, y, z)]);
         set3(d, c, 0.0f);
         known |= 1u << c;
       } else if (touches_source(E, x, y, z, c)) {

@@ -1806,7 +1806,8 @@ int fluid_pp_extrapolate_velocity(fluid_pp* pp, long long* filled_faces) {
   E.band = reinterpret_cast<unsigned*>((reinterpret_cast<uintptr_t>(E.mark[1] + n) + 15) & ~uintptr_t(15));
   auto grid = [](long long cnt) { return int(std::max(1LL, std::min<long long>((cnt + kThreads - 1) / kThreads, kMaxGrid))); };
   cudaMemsetAsync(E.count, 0, 16, s);
-  k_ext_seed<<<grid(n), kThreads, 0, s>>>(E);
+  if (E.solids) k_ext_seed<true><<<grid(n), kThreads, 0, s>>>(E);
+  else k_ext_seed<false><<<grid(n), kThreads, 0, s>>>(E);
   k_ext_dilate<<<grid(n), kThreads, 0, s>>>(E, 0, E.mark[0], E.mark[1]);
   k_ext_dilate<<<grid(n), kThreads, 0, s>>>(E, 1, E.mark[1], E.mark[0]);
   k_ext_dilate<<<grid(n), kThreads, 0, s>>>(E, 2, E.mark[0], E.mark[1]);

@@ -140,3 +140,42 @@ def test_atlas_graph_and_direct_launches_give_the_same_bits():
     assert out[0][0] == out[1][0]
     np.testing.assert_array_equal(out[0][1], out[1][1])
     np.testing.assert_array_equal(out[0][2], out[1][2])
+
+
+def test_a_port_takes_the_lower_bricks_copy():
+    """A face shared by two present bricks is stored twice; the lower brick's
+    copy is the canonical one.  An upper copy that disagrees on input changes
+    nothing, and after the projection both copies hold the projected value."""
+    s = configs.atlas_scene(48, 40, 32, seed=7, drops=4)
+    coords = configs.atlas_bricks(s.vof)
+    dens, faces = bricks_from_dense(s.vof, s.u, s.v, s.w, coords)
+    present = {tuple(c): k for k, c in enumerate(coords)}
+    noisy = faces.copy()
+    shapes = [(RES, RES, RES + 1), (RES, RES + 1, RES), (RES + 1, RES, RES)]
+    rng = np.random.default_rng(3)
+    ports = 0
+    for k, c in enumerate(coords):
+        for a in range(3):
+            low = list(c)
+            low[a] -= 1
+            if tuple(low) not in present:
+                continue
+            blk = noisy[k, a].reshape(shapes[a])
+            sl = [slice(None)] * 3
+            sl[2 - a] = 0   # the f = 0 layer of the axis (arrays are z, y, x)
+            blk[tuple(sl)] = rng.normal(0.0, 5.0, blk[tuple(sl)].shape).astype(np.float32)
+            noisy[k, a] = blk.reshape(-1)
+            ports += 1
+    assert ports > 0
+    out = []
+    for f in (faces, noisy):
+        A = AtlasProjector((s.nx, s.ny, s.nz), s.h, s.rho)
+        A.upload(coords, dens, f)
+        rec = A.project(s.dt, rel_tol=1e-6)
+        assert rec["status_name"] == "OK", rec
+        out.append((rec["iterations"], rec["max_div_before"], *A.download()))
+        A.destroy()
+    assert out[0][:2] == out[1][:2]
+    np.testing.assert_array_equal(out[0][2], out[1][2])
+    np.testing.assert_array_equal(out[0][3], out[1][3])
+    dense_faces((s.nx, s.ny, s.nz), coords, out[1][3])   # both copies of every port agree
