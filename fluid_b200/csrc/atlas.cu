@@ -61,6 +61,7 @@ constexpr int kAT = 256;           // threads per CTA
 constexpr int kAGrid = 148 * 8;    // grid cap
 constexpr int kAtMaxLevels = 16;
 constexpr int kAtCoarseMax = 64;   // the dense coarsest level
+constexpr long long kAtSmallCells = 2048;   // levels this small run in one CTA (k_at_vsmall)
 constexpr int kRedGrid = 1184;     // fixed reduction grid (partials folded in block order)
 
 struct ALevel {
@@ -169,6 +170,8 @@ __device__ __forceinline__ double face_weight(const ALevel& L, long long i, cons
 }
 
 // ------------------------------------------------------------------ kernels
+// Cells of level L taken by thread t0 of ts (a grid-stride walk).
+#define A_RANGE(L, t0, ts) for (long long i = (t0); i < (L).n; i += (ts))
 #define A_CELLS(L)                                                                                   \
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (L).n;                  \
        i += (long long)gridDim.x * blockDim.x)
@@ -318,10 +321,9 @@ __global__ void k_at_comp_sub(AInst* I, double* v) {
 // ------------------------------------------------------------ the V-cycle
 // One colour of red-black Gauss-Seidel on level l (from a zero guess when
 // zero_init: the first colour then reads no neighbours).
-__global__ void k_at_smooth(AInst* I, int l, int colour, int zero_init) {
-  if (I->ctrl->done) return;
+__device__ __forceinline__ void at_smooth(AInst* I, int l, int colour, int zero_init, long long t0, long long ts) {
   const ALevel& L = I->lv[l];
-  A_CELLS(L) {
+  A_RANGE(L, t0, ts) {
     if (!L.label[i]) {
       if (zero_init) L.z[i] = 0.0f;
       continue;
@@ -344,10 +346,9 @@ __global__ void k_at_smooth(AInst* I, int l, int colour, int zero_init) {
 }
 
 // res = rhs - A z on level l.
-__global__ void k_at_residual(AInst* I, int l) {
-  if (I->ctrl->done) return;
+__device__ __forceinline__ void at_residual(AInst* I, int l, long long t0, long long ts) {
   const ALevel& L = I->lv[l];
-  A_CELLS(L) {
+  A_RANGE(L, t0, ts) {
     if (!L.label[i]) {
       L.res[i] = 0.0f;
       continue;
@@ -361,6 +362,19 @@ __global__ void k_at_residual(AInst* I, int l) {
       }
     L.res[i] = s;
   }
+}
+
+__device__ __forceinline__ long long grid_t0() { return blockIdx.x * (long long)blockDim.x + threadIdx.x; }
+__device__ __forceinline__ long long grid_ts() { return (long long)gridDim.x * blockDim.x; }
+
+__global__ void k_at_smooth(AInst* I, int l, int colour, int zero_init) {
+  if (I->ctrl->done) return;
+  at_smooth(I, l, colour, zero_init, grid_t0(), grid_ts());
+}
+
+__global__ void k_at_residual(AInst* I, int l) {
+  if (I->ctrl->done) return;
+  at_residual(I, l, grid_t0(), grid_ts());
 }
 
 // ----------------------------------------------- level 0, one CTA per brick
@@ -507,11 +521,10 @@ __device__ __forceinline__ long long child_of(const ALevel& F, const ALevel& C, 
 }
 
 // rhs_c = 1/2 sum of the liquid children's residuals (R = P^T / 2).
-__global__ void k_at_restrict(AInst* I, int l) {
-  if (I->ctrl->done) return;
+__device__ __forceinline__ void at_restrict(AInst* I, int l, long long t0, long long ts) {
   const ALevel& F = I->lv[l];
   const ALevel& C = I->lv[l + 1];
-  A_CELLS(C) {
+  A_RANGE(C, t0, ts) {
     if (!C.label[i]) {
       C.rhs[i] = 0.0f;
       continue;
@@ -527,11 +540,10 @@ __global__ void k_at_restrict(AInst* I, int l) {
 }
 
 // z_f += z_c on liquid fine cells (P piecewise constant).
-__global__ void k_at_prolong(AInst* I, int l) {
-  if (I->ctrl->done) return;
+__device__ __forceinline__ void at_prolong(AInst* I, int l, long long t0, long long ts) {
   const ALevel& F = I->lv[l];
   const ALevel& C = I->lv[l + 1];
-  A_CELLS(F) {
+  A_RANGE(F, t0, ts) {
     if (!F.label[i]) continue;
     long long ci;
     if (F.parent) {
@@ -544,6 +556,16 @@ __global__ void k_at_prolong(AInst* I, int l) {
     }
     if (ci >= 0 && C.label[ci]) F.z[i] += C.z[ci];
   }
+}
+
+__global__ void k_at_restrict(AInst* I, int l) {
+  if (I->ctrl->done) return;
+  at_restrict(I, l, grid_t0(), grid_ts());
+}
+
+__global__ void k_at_prolong(AInst* I, int l) {
+  if (I->ctrl->done) return;
+  at_prolong(I, l, grid_t0(), grid_ts());
 }
 
 // Dense inverse of the coarsest level's operator (one CTA, shared memory):
@@ -589,8 +611,8 @@ __global__ void __launch_bounds__(1024) k_at_coarse_factor(AInst* I) {
   for (int e = threadIdx.x; e < m * m; e += blockDim.x) I->coarse_inv[e] = A[e];
 }
 
-__global__ void k_at_coarse_apply(AInst* I) {
-  if (I->ctrl->done) return;
+// z = A^{-1} rhs on the coarsest level, a warp per row.
+__device__ __forceinline__ void at_coarse_apply(AInst* I) {
   const ALevel& L = I->lv[I->nlev - 1];
   const int m = int(L.n);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -599,6 +621,51 @@ __global__ void k_at_coarse_apply(AInst* I) {
     for (int j = lane; j < m; j += 32) s += I->coarse_inv[i * m + j] * (L.label[j] ? double(L.rhs[j]) : 0.0);
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) L.z[i] = L.label[i] ? float(s) : 0.0f;
+  }
+}
+
+__global__ void k_at_coarse_apply(AInst* I) {
+  if (I->ctrl->done) return;
+  at_coarse_apply(I);
+}
+
+// The small levels first .. nlev - 1 of the V-cycle in one CTA: the same
+// stages in the same order as the per-level launches (pre-smoothing from
+// zero, residual, restriction down to the dense coarsest level, then
+// prolongation and post-smoothing up to level first), separated by barriers
+// instead of launches.  Each stage computes every cell from values the
+// previous stages wrote, as the launches do, so the results are the same.
+__global__ void __launch_bounds__(1024) k_at_vsmall(AInst* I, int first, int pre, int post) {
+  if (I->ctrl->done) return;
+  const long long t0 = threadIdx.x, ts = blockDim.x;
+  const int last = I->nlev - 1;
+  for (int l = first; l < last; ++l) {
+    at_smooth(I, l, 0, 1, t0, ts);
+    __syncthreads();
+    at_smooth(I, l, 1, 0, t0, ts);
+    __syncthreads();
+    for (int k = 1; k < pre; ++k) {
+      at_smooth(I, l, 0, 0, t0, ts);
+      __syncthreads();
+      at_smooth(I, l, 1, 0, t0, ts);
+      __syncthreads();
+    }
+    at_residual(I, l, t0, ts);
+    __syncthreads();
+    at_restrict(I, l, t0, ts);
+    __syncthreads();
+  }
+  at_coarse_apply(I);
+  __syncthreads();
+  for (int l = last - 1; l >= first; --l) {
+    at_prolong(I, l, t0, ts);
+    __syncthreads();
+    for (int k = 0; k < post; ++k) {
+      at_smooth(I, l, 1, 0, t0, ts);
+      __syncthreads();
+      at_smooth(I, l, 0, 0, t0, ts);
+      __syncthreads();
+    }
   }
 }
 
@@ -1132,6 +1199,7 @@ struct fluid_pp_atlas {
   bool graph_failed[2] = {false, false};
   bool use_graphs = true;
   int pre = 1, post = 1;   // red-black sweeps before and after the coarse correction (every level)
+  int small_first = 0;     // first level of the one-CTA V-cycle tail (k_at_vsmall), 0 = none
   int set_error(int code, const std::string& m) {
     err = m;
     return code;
@@ -1159,7 +1227,9 @@ void vcycle(fluid_pp_atlas* A, cudaStream_t s, bool vin) {
   const AInst& I = A->inst;
   if (vin) k_at_vin<<<grid_n(I.lv[0].n), kAT, 0, s>>>(A->d_inst);
   const int last = I.nlev - 1;
-  for (int l = 0; l < last; ++l) {
+  const int fs = A->small_first;   // levels fs .. last in one CTA
+  const int grid_last = fs > 0 ? fs : last;
+  for (int l = 0; l < grid_last; ++l) {
     const int g = grid_n(I.lv[l].n);
     if (l == 0) k_at_smooth0_zero<<<I.nb, 256, 0, s>>>(A->d_inst);   // first colour from zero
     else k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 1);
@@ -1180,8 +1250,9 @@ void vcycle(fluid_pp_atlas* A, cudaStream_t s, bool vin) {
     }
     k_at_restrict<<<grid_n(I.lv[l + 1].n), kAT, 0, s>>>(A->d_inst, l);
   }
-  k_at_coarse_apply<<<1, 1024, 0, s>>>(A->d_inst);
-  for (int l = last - 1; l >= 0; --l) {
+  if (fs > 0) k_at_vsmall<<<1, 1024, 0, s>>>(A->d_inst, fs, A->pre, A->post);
+  else k_at_coarse_apply<<<1, 1024, 0, s>>>(A->d_inst);
+  for (int l = grid_last - 1; l >= 0; --l) {
     const int g = grid_n(I.lv[l].n);
     k_at_prolong<<<g, kAT, 0, s>>>(A->d_inst, l);
     for (int k = 0; k < A->post; ++k) {
@@ -1405,6 +1476,14 @@ int fluid_pp_atlas_upload(fluid_pp_atlas* A, int nbricks, const int* coords, con
   I = AInst{};
   I.nlev = int(lv.size());
   I.nb = nbricks;
+  // the levels from the first one of at most kAtSmallCells cells (not level
+  // 0, whose kernels are brick-tiled) down to the coarsest run in one CTA
+  A->small_first = 0;
+  for (int l = 1; l + 1 < I.nlev; ++l)
+    if (lv[l].n() <= kAtSmallCells) {
+      A->small_first = l;
+      break;
+    }
   cudaError_t e = cudaSuccess;
   auto put = [&](const void* src, size_t b) -> void* {
     void* d = take(b);
