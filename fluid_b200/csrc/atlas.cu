@@ -95,6 +95,7 @@ struct AInst {
   int nlev;
   int precond;              // 1: V-cycle, 0: Jacobi
   int nb;                   // bricks
+  const int* bnb;           // nb x 6 neighbour slots of each brick (kBrickAbsent, kBrickWall)
   float* faces;             // nb x 3 x kFaces, per brick u, v, w
   double* b;
   double* x;
@@ -387,19 +388,22 @@ constexpr int kTile = (kRes + 2) * (kRes + 2) * (kRes + 2);
 
 __device__ __forceinline__ int tix(int x, int y, int z) { return (z + 1) * 100 + (y + 1) * 10 + (x + 1); }
 
+// A brick's six neighbours, index 2 a + (side > 0): a slot, kBrickAbsent for
+// an absent brick inside the domain, kBrickWall beyond a domain face.
+constexpr int kBrickAbsent = -1, kBrickWall = -2;
+
+// Threads 0 .. 5 fetch the brick's neighbours into nb (shared); the caller
+// synchronises before reading them.
+__device__ __forceinline__ void brick_nbrs(const AInst* I, int slot, int* nb) {
+  if (threadIdx.x < 6) nb[threadIdx.x] = I->bnb[6 * slot + threadIdx.x];
+}
+
+// Stage the brick's values and its halos (nb: the brick's neighbours, already
+// visible to every thread); ends with a barrier.
 template <class T>
-__device__ __forceinline__ void load_tile(const ALevel& L, int slot, const T* v, T* t) {
-  __shared__ int nb[6];
-  if (threadIdx.x < 6) {
-    const int a = threadIdx.x >> 1, sd = (threadIdx.x & 1) ? 1 : -1;
-    int b[3] = {L.coords[3 * slot], L.coords[3 * slot + 1], L.coords[3 * slot + 2]};
-    const int g[3] = {L.gx, L.gy, L.gz};
-    b[a] += sd;
-    nb[threadIdx.x] = (b[a] < 0 || b[a] >= g[a]) ? -1 : L.table[b[0] + L.gx * (b[1] + L.gy * b[2])];
-  }
+__device__ __forceinline__ void load_tile(int slot, const int* nb, const T* v, T* t) {
   const T* src = v + (long long)slot * kCells;
   for (int k = threadIdx.x; k < kCells; k += blockDim.x) t[tix(k & 7, (k >> 3) & 7, k >> 6)] = src[k];
-  __syncthreads();
   for (int k = threadIdx.x; k < 6 * 64; k += blockDim.x) {
     const int f = k >> 6, u = k & 7, w = (k >> 3) & 7;
     const int a = f >> 1, sd = (f & 1) ? 1 : -1;
@@ -429,13 +433,18 @@ __global__ void __launch_bounds__(256) k_at_smooth0(AInst* I, int colour) {
   if (I->ctrl->done) return;
   const ALevel& L = I->lv[0];
   __shared__ float t[kTile];
+  __shared__ int nb[6];
   const int slot = blockIdx.x;
-  load_tile<float>(L, slot, L.z, t);
+  brick_nbrs(I, slot, nb);
   const int ty = (threadIdx.x >> 2) & 7, tz = threadIdx.x >> 5;
   const int tx = 2 * (threadIdx.x & 3) + ((ty + tz + colour) & 1);
   const long long i = (long long)slot * kCells + tx + kRes * (ty + kRes * tz);
-  if (!L.label[i]) return;
-  L.z[i] = (L.rhs[i] + nbr_sum(t, tx, ty, tz)) / L.diag[i];
+  const bool liq = L.label[i];   // the cell's own inputs load while the tile comes in
+  const float r = L.rhs[i], d = L.diag[i];
+  __syncthreads();
+  load_tile<float>(slot, nb, L.z, t);
+  if (!liq) return;
+  L.z[i] = (r + nbr_sum(t, tx, ty, tz)) / d;
 }
 
 // The first colour of the level-0 pre-smoothing from zero: red liquid cells
@@ -456,12 +465,26 @@ __global__ void __launch_bounds__(256) k_at_residual0(AInst* I) {
   if (I->ctrl->done) return;
   const ALevel& L = I->lv[0];
   __shared__ float t[kTile];
+  __shared__ int nb[6];
   const int slot = blockIdx.x;
-  load_tile<float>(L, slot, L.z, t);
-  for (int k = threadIdx.x; k < kCells; k += 256) {
+  brick_nbrs(I, slot, nb);
+  bool liq[2];   // the cells' own inputs load while the tile comes in
+  float r[2], d[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const long long i = (long long)slot * kCells + threadIdx.x + 256 * h;
+    liq[h] = L.label[i];
+    r[h] = L.rhs[i];
+    d[h] = L.diag[i];
+  }
+  __syncthreads();
+  load_tile<float>(slot, nb, L.z, t);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int k = threadIdx.x + 256 * h;
     const int x = k & 7, y = (k >> 3) & 7, z = k >> 6;
     const long long i = (long long)slot * kCells + k;
-    L.res[i] = L.label[i] ? (L.rhs[i] - L.diag[i] * t[tix(x, y, z)]) + nbr_sum(t, x, y, z) : 0.0f;
+    L.res[i] = liq[h] ? (r[h] - d[h] * t[tix(x, y, z)]) + nbr_sum(t, x, y, z) : 0.0f;
   }
 }
 
@@ -472,16 +495,29 @@ __global__ void __launch_bounds__(256) k_at_spmv0(AInst* I, double* bpart) {
   if (I->ctrl->done) return;
   const ALevel& L = I->lv[0];
   __shared__ double t[kTile];
+  __shared__ int nb[6];
   const int slot = blockIdx.x;
-  load_tile<double>(L, slot, I->d, t);
+  brick_nbrs(I, slot, nb);
+  bool liq[2];   // the cells' own inputs load while the tile comes in
+  float dg[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const long long i = (long long)slot * kCells + threadIdx.x + 256 * h;
+    liq[h] = L.label[i];
+    dg[h] = L.diag[i];
+  }
+  __syncthreads();
+  load_tile<double>(slot, nb, I->d, t);
   double acc = 0.0;
-  for (int k = threadIdx.x; k < kCells; k += 256) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int k = threadIdx.x + 256 * h;
     const int x = k & 7, y = (k >> 3) & 7, z = k >> 6;
     const long long i = (long long)slot * kCells + k;
     double q = 0.0;
-    if (L.label[i]) {
+    if (liq[h]) {
       const double dv = t[tix(x, y, z)];
-      q = double(L.diag[i]) * dv - nbr_sum(t, x, y, z);
+      q = double(dg[h]) * dv - nbr_sum(t, x, y, z);
       acc += dv * q;
     }
     I->q[i] = q;
@@ -845,17 +881,13 @@ __global__ void k_at_start(AInst* I) {
 }
 
 // ------------------------------------------ the faces, one CTA per brick
-// A brick's six neighbour slots (-1 absent) and which of its faces lie on the
-// domain walls, index 2 a + (side > 0).
-__device__ __forceinline__ void brick_sides(const ALevel& L, int slot, int* nbs, int* nbw) {
+// A brick's six neighbour slots (-1 absent or beyond a wall) and which of its
+// faces lie on the domain walls, index 2 a + (side > 0).
+__device__ __forceinline__ void brick_sides(const AInst* I, int slot, int* nbs, int* nbw) {
   if (threadIdx.x < 6) {
-    const int a = threadIdx.x >> 1, sd = (threadIdx.x & 1) ? 1 : -1;
-    int b[3] = {L.coords[3 * slot], L.coords[3 * slot + 1], L.coords[3 * slot + 2]};
-    const int g[3] = {L.gx, L.gy, L.gz};
-    b[a] += sd;
-    const bool wall = b[a] < 0 || b[a] >= g[a];
-    nbw[threadIdx.x] = wall;
-    nbs[threadIdx.x] = wall ? -1 : L.table[b[0] + L.gx * (b[1] + L.gy * b[2])];
+    const int b = I->bnb[6 * slot + threadIdx.x];
+    nbw[threadIdx.x] = b == kBrickWall;
+    nbs[threadIdx.x] = b >= 0 ? b : -1;
   }
 }
 
@@ -918,7 +950,7 @@ __global__ void __launch_bounds__(256) k_at_div0(AInst* I, int write_b, double* 
   const int slot = blockIdx.x;
   __shared__ float fs[3][kFaces];
   __shared__ int nbs[6], nbw[6];
-  brick_sides(L, slot, nbs, nbw);
+  brick_sides(I, slot, nbs, nbw);
   __syncthreads();
   stage_faces<0>(I, slot, nbs, write_b, fs[0]);
   stage_faces<1>(I, slot, nbs, write_b, fs[1]);
@@ -1022,10 +1054,11 @@ __global__ void __launch_bounds__(256) k_at_project0(AInst* I) {
   __shared__ float ph[kTile];
   __shared__ uint8_t lb[kTile];
   __shared__ int nbs[6], nbw[6];
-  brick_sides(L, slot, nbs, nbw);
-  load_tile<double>(L, slot, I->x, xs);
-  load_tile<float>(L, slot, L.phi, ph);
-  load_tile<uint8_t>(L, slot, L.label, lb);
+  brick_sides(I, slot, nbs, nbw);
+  __syncthreads();
+  load_tile<double>(slot, nbs, I->x, xs);
+  load_tile<float>(slot, nbs, L.phi, ph);
+  load_tile<uint8_t>(slot, nbs, L.label, lb);
   project_axis<0>(I, slot, nbs, nbw, xs, ph, lb);
   project_axis<1>(I, slot, nbs, nbw, xs, ph, lb);
   project_axis<2>(I, slot, nbs, nbw, xs, ph, lb);
@@ -1520,6 +1553,23 @@ int fluid_pp_atlas_upload(fluid_pp_atlas* A, int nbricks, const int* coords, con
   I.d = static_cast<double*>(take(8 * size_t(n0)));
   I.q = static_cast<double*>(take(8 * size_t(n0)));
   float* d_rho = static_cast<float*>(put(rho.data(), 4 * size_t(n0)));
+  {   // each brick's six neighbours: a slot, absent, or beyond a domain face
+    const HostLevel& H = lv[0];
+    std::vector<int> bnb(6 * size_t(nbricks));
+    for (int k = 0; k < nbricks; ++k)
+      for (int f = 0; f < 6; ++f) {
+        int b[3] = {H.coords[3 * k], H.coords[3 * k + 1], H.coords[3 * k + 2]};
+        const int a = f >> 1, g[3] = {H.gx, H.gy, H.gz};
+        b[a] += (f & 1) ? 1 : -1;
+        int t = kBrickWall;
+        if (b[a] >= 0 && b[a] < g[a]) {
+          t = H.table[b[0] + size_t(H.gx) * (b[1] + size_t(H.gy) * b[2])];
+          if (t < 0) t = kBrickAbsent;
+        }
+        bnb[6 * size_t(k) + f] = t;
+      }
+    I.bnb = static_cast<const int*>(put(bnb.data(), 4 * bnb.size()));
+  }
   I.faces = static_cast<float*>(put(faces, 4 * size_t(nbricks) * 3 * kFaces));
   I.part = static_cast<double*>(take(8 * 4 * kRedGrid));
   I.bpart = static_cast<double*>(take(16 * size_t(nbricks)));
