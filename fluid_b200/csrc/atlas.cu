@@ -880,6 +880,145 @@ __global__ void k_at_start(AInst* I) {
   }
 }
 
+// ------------------------------- levels 1 and 2, K blocks of B^3 per CTA
+// Levels with B = 4 and 2 cells per brick edge hold the bricks' own blocks
+// (same slots, same block grid), so the brick neighbour table serves them.
+// Each block and its face halos are staged in a (B + 2)^3 tile; the stencil
+// adds the six neighbours in the order of the per-cell kernels (x-, x+, y-,
+// y+, z-, z+).  Air cells of these levels hold z = 0 from the first colour of
+// the pre-smoothing on (it writes every cell, the prolongation adds only to
+// liquid ones), and absent or beyond-wall halo cells are staged as 0, so the
+// tile needs no labels.
+template <int B>
+struct BTile {
+  static constexpr int C = B * B * B, W = B + 2, N = W * W * W;
+  static __device__ __forceinline__ int ix(int x, int y, int z) { return (z + 1) * W * W + (y + 1) * W + (x + 1); }
+};
+
+template <int B, int K>
+__device__ __forceinline__ void load_btiles(const ALevel& L, const int (*nb)[6], const float* v, float (*t)[BTile<B>::N]) {
+  using T = BTile<B>;
+  for (int e = threadIdx.x; e < K * T::C; e += blockDim.x) {
+    const int j = e / T::C, k = e - j * T::C;
+    const int slot = blockIdx.x * K + j;
+    t[j][T::ix(k % B, (k / B) % B, k / (B * B))] = slot < L.nblocks ? v[(long long)slot * T::C + k] : 0.0f;
+  }
+  for (int e = threadIdx.x; e < K * 6 * B * B; e += blockDim.x) {
+    const int j = e / (6 * B * B), r = e - j * 6 * B * B;
+    const int f = r / (B * B), u = r % B, w = (r / B) % B;
+    const int a = f >> 1, sd = (f & 1) ? 1 : -1;
+    int h[3], m[3];
+    if (a == 0) { h[0] = sd > 0 ? B : -1; h[1] = u; h[2] = w; }
+    else if (a == 1) { h[0] = u; h[1] = sd > 0 ? B : -1; h[2] = w; }
+    else { h[0] = u; h[1] = w; h[2] = sd > 0 ? B : -1; }
+    m[0] = h[0]; m[1] = h[1]; m[2] = h[2];
+    m[a] = sd > 0 ? 0 : B - 1;
+    const int ns = nb[j][f];
+    t[j][T::ix(h[0], h[1], h[2])] = ns >= 0 ? v[(long long)ns * T::C + m[0] + B * (m[1] + B * m[2])] : 0.0f;
+  }
+}
+
+// The CTA's K blocks' neighbours (beyond the level's blocks: walls).
+template <int K>
+__device__ __forceinline__ void block_nbrs(const AInst* I, const ALevel& L, int (*nb)[6]) {
+  if (threadIdx.x < 6 * K) {
+    const int j = threadIdx.x / 6, f = threadIdx.x - 6 * j, slot = blockIdx.x * K + j;
+    nb[j][f] = slot < L.nblocks ? I->bnb[6 * slot + f] : kBrickWall;
+  }
+}
+
+// One colour of the smoother on level l (B cells per block edge, B even, so a
+// cell's colour is its local parity); thread t: block t / B^3, cell t % B^3.
+template <int B, int K>
+__global__ void __launch_bounds__(K * B * B * B) k_at_smooth_t(AInst* I, int l, int colour, int zero_init) {
+  using T = BTile<B>;
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[l];
+  __shared__ float t[K][T::N];
+  __shared__ int nb[K][6];
+  block_nbrs<K>(I, L, nb);
+  const int j = threadIdx.x / T::C, k = threadIdx.x - j * T::C;
+  const int slot = blockIdx.x * K + j;
+  const bool act = slot < L.nblocks;
+  const int x = k % B, y = (k / B) % B, z = k / (B * B);
+  const long long i = (long long)slot * T::C + k;
+  bool liq = false;   // the cell's own inputs load while the tile comes in
+  float r = 0.0f, d = 1.0f;
+  if (act) {
+    liq = L.label[i];
+    r = L.rhs[i];
+    d = L.diag[i];
+  }
+  const bool first = zero_init && colour == 0;   // from zero: no neighbour terms
+  __syncthreads();
+  if (!first) {
+    load_btiles<B, K>(L, nb, L.z, t);
+    __syncthreads();
+  }
+  if (!act) return;
+  if (!liq) {
+    if (zero_init) L.z[i] = 0.0f;
+    return;
+  }
+  if (((x + y + z) & 1) != colour) {
+    if (first) L.z[i] = 0.0f;
+    return;
+  }
+  float s = r;
+  if (!first) {
+    const float* tt = t[j];
+    const int c = T::ix(x, y, z);
+    s += tt[c - 1];
+    s += tt[c + 1];
+    s += tt[c - T::W];
+    s += tt[c + T::W];
+    s += tt[c - T::W * T::W];
+    s += tt[c + T::W * T::W];
+  }
+  L.z[i] = s / d;
+}
+
+// res = rhs - A z on level l (B as k_at_smooth_t).
+template <int B, int K>
+__global__ void __launch_bounds__(K * B * B * B) k_at_residual_t(AInst* I, int l) {
+  using T = BTile<B>;
+  if (I->ctrl->done) return;
+  const ALevel& L = I->lv[l];
+  __shared__ float t[K][T::N];
+  __shared__ int nb[K][6];
+  block_nbrs<K>(I, L, nb);
+  const int j = threadIdx.x / T::C, k = threadIdx.x - j * T::C;
+  const int slot = blockIdx.x * K + j;
+  const bool act = slot < L.nblocks;
+  const int x = k % B, y = (k / B) % B, z = k / (B * B);
+  const long long i = (long long)slot * T::C + k;
+  bool liq = false;
+  float r = 0.0f, d = 0.0f;
+  if (act) {
+    liq = L.label[i];
+    r = L.rhs[i];
+    d = L.diag[i];
+  }
+  __syncthreads();
+  load_btiles<B, K>(L, nb, L.z, t);
+  __syncthreads();
+  if (!act) return;
+  if (!liq) {
+    L.res[i] = 0.0f;
+    return;
+  }
+  const float* tt = t[j];
+  const int c = T::ix(x, y, z);
+  float s = r - d * tt[c];
+  s += tt[c - 1];
+  s += tt[c + 1];
+  s += tt[c - T::W];
+  s += tt[c + T::W];
+  s += tt[c - T::W * T::W];
+  s += tt[c + T::W * T::W];
+  L.res[i] = s;
+}
+
 // ------------------------------------------ the faces, one CTA per brick
 // A brick's six neighbour slots (-1 absent or beyond a wall) and which of its
 // faces lie on the domain walls, index 2 a + (side > 0).
@@ -1262,10 +1401,23 @@ void vcycle(fluid_pp_atlas* A, cudaStream_t s, bool vin) {
   const int last = I.nlev - 1;
   const int fs = A->small_first;   // levels fs .. last in one CTA
   const int grid_last = fs > 0 ? fs : last;
+  // levels 1 and 2 (4 and 2 cells per brick edge) run block-tiled kernels
+  auto smooth = [&](int l, int colour, int zero) {
+    const ALevel& L = I.lv[l];
+    if (L.B == 4) k_at_smooth_t<4, 2><<<(L.nblocks + 1) / 2, 128, 0, s>>>(A->d_inst, l, colour, zero);
+    else if (L.B == 2) k_at_smooth_t<2, 16><<<(L.nblocks + 15) / 16, 128, 0, s>>>(A->d_inst, l, colour, zero);
+    else k_at_smooth<<<grid_n(L.n), kAT, 0, s>>>(A->d_inst, l, colour, zero);
+  };
+  auto residual = [&](int l) {
+    const ALevel& L = I.lv[l];
+    if (L.B == 4) k_at_residual_t<4, 2><<<(L.nblocks + 1) / 2, 128, 0, s>>>(A->d_inst, l);
+    else if (L.B == 2) k_at_residual_t<2, 16><<<(L.nblocks + 15) / 16, 128, 0, s>>>(A->d_inst, l);
+    else k_at_residual<<<grid_n(L.n), kAT, 0, s>>>(A->d_inst, l);
+  };
   for (int l = 0; l < grid_last; ++l) {
     const int g = grid_n(I.lv[l].n);
     if (l == 0) k_at_smooth0_zero<<<I.nb, 256, 0, s>>>(A->d_inst);   // first colour from zero
-    else k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 1);
+    else smooth(l, 0, 1);
     if (l == 0) {
       k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 1);
       for (int k = 1; k < A->pre; ++k) {
@@ -1274,12 +1426,12 @@ void vcycle(fluid_pp_atlas* A, cudaStream_t s, bool vin) {
       }
       k_at_residual0<<<I.nb, 256, 0, s>>>(A->d_inst);
     } else {
-      k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 1, 0);
+      smooth(l, 1, 0);
       for (int k = 1; k < A->pre; ++k) {
-        k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 0);
-        k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 1, 0);
+        smooth(l, 0, 0);
+        smooth(l, 1, 0);
       }
-      k_at_residual<<<g, kAT, 0, s>>>(A->d_inst, l);
+      residual(l);
     }
     k_at_restrict<<<grid_n(I.lv[l + 1].n), kAT, 0, s>>>(A->d_inst, l);
   }
@@ -1293,8 +1445,8 @@ void vcycle(fluid_pp_atlas* A, cudaStream_t s, bool vin) {
         k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 1);
         k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 0);
       } else {
-        k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 1, 0);
-        k_at_smooth<<<g, kAT, 0, s>>>(A->d_inst, l, 0, 0);
+        smooth(l, 1, 0);
+        smooth(l, 0, 0);
       }
     }
   }
