@@ -460,11 +460,17 @@ __global__ void __launch_bounds__(256) k_at_smooth0_zero(AInst* I) {
   }
 }
 
-// res = rhs - A z on level 0, two cells per thread.
+// res = rhs - A z on level 0 (two cells per thread, kept in shared memory)
+// and its restriction into the brick's own block of level 1 (4^3 cells):
+// rhs_c = 1/2 sum of the 8 children's residuals in child order, 0 on air,
+// as k_at_restrict forms it.
 __global__ void __launch_bounds__(256) k_at_residual0(AInst* I) {
   if (I->ctrl->done) return;
   const ALevel& L = I->lv[0];
+  const ALevel& C = I->lv[1];
+  constexpr int CB = kRes / 2, CC = CB * CB * CB;
   __shared__ float t[kTile];
+  __shared__ float rs[kCells];
   __shared__ int nb[6];
   const int slot = blockIdx.x;
   brick_nbrs(I, slot, nb);
@@ -477,14 +483,23 @@ __global__ void __launch_bounds__(256) k_at_residual0(AInst* I) {
     r[h] = L.rhs[i];
     d[h] = L.diag[i];
   }
+  const bool cl = threadIdx.x < CC && C.label[(long long)slot * CC + threadIdx.x];
   __syncthreads();
   load_tile<float>(slot, nb, L.z, t);
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int k = threadIdx.x + 256 * h;
     const int x = k & 7, y = (k >> 3) & 7, z = k >> 6;
-    const long long i = (long long)slot * kCells + k;
-    L.res[i] = liq[h] ? (r[h] - d[h] * t[tix(x, y, z)]) + nbr_sum(t, x, y, z) : 0.0f;
+    rs[k] = liq[h] ? (r[h] - d[h] * t[tix(x, y, z)]) + nbr_sum(t, x, y, z) : 0.0f;
+  }
+  __syncthreads();
+  if (threadIdx.x < CC) {
+    const int cx = threadIdx.x % CB, cy = (threadIdx.x / CB) % CB, cz = threadIdx.x / (CB * CB);
+    float sum = 0.0f;
+    if (cl)
+      for (int k = 0; k < 8; ++k)
+        sum += rs[(2 * cx + (k & 1)) + kRes * ((2 * cy + ((k >> 1) & 1)) + kRes * (2 * cz + ((k >> 2) & 1)))];
+    C.rhs[(long long)slot * CC + threadIdx.x] = cl ? 0.5f * sum : 0.0f;
   }
 }
 
@@ -978,13 +993,20 @@ __global__ void __launch_bounds__(K * B * B * B) k_at_smooth_t(AInst* I, int l, 
   L.z[i] = s / d;
 }
 
-// res = rhs - A z on level l (B as k_at_smooth_t).
+// res = rhs - A z on level l (B as k_at_smooth_t), kept in shared memory, and
+// its restriction into level l + 1, whose blocks are the same bricks' with
+// B / 2 cells per edge: rhs_c = 1/2 sum of the 8 children's residuals in
+// child order, 0 on air, as k_at_restrict forms it.
 template <int B, int K>
 __global__ void __launch_bounds__(K * B * B * B) k_at_residual_t(AInst* I, int l) {
   using T = BTile<B>;
+  constexpr int CB = B / 2, CC = CB * CB * CB;
+  static_assert(K * CC <= K * T::C, "a thread per coarse cell");
   if (I->ctrl->done) return;
   const ALevel& L = I->lv[l];
+  const ALevel& Cl = I->lv[l + 1];
   __shared__ float t[K][T::N];
+  __shared__ float rs[K][T::C];
   __shared__ int nb[K][6];
   block_nbrs<K>(I, L, nb);
   const int j = threadIdx.x / T::C, k = threadIdx.x - j * T::C;
@@ -999,24 +1021,36 @@ __global__ void __launch_bounds__(K * B * B * B) k_at_residual_t(AInst* I, int l
     r = L.rhs[i];
     d = L.diag[i];
   }
+  // the coarse cell of thread e < K CC: block e / CC, cell e % CC
+  const int cj = threadIdx.x / CC, ck = threadIdx.x - cj * CC, cslot = blockIdx.x * K + cj;
+  const bool cown = threadIdx.x < K * CC && cslot < L.nblocks;
+  const bool cl = cown && Cl.label[(long long)cslot * CC + ck];
   __syncthreads();
   load_btiles<B, K>(L, nb, L.z, t);
   __syncthreads();
-  if (!act) return;
-  if (!liq) {
-    L.res[i] = 0.0f;
-    return;
+  float res = 0.0f;
+  if (act && liq) {
+    const float* tt = t[j];
+    const int c = T::ix(x, y, z);
+    float s = r - d * tt[c];
+    s += tt[c - 1];
+    s += tt[c + 1];
+    s += tt[c - T::W];
+    s += tt[c + T::W];
+    s += tt[c - T::W * T::W];
+    s += tt[c + T::W * T::W];
+    res = s;
   }
-  const float* tt = t[j];
-  const int c = T::ix(x, y, z);
-  float s = r - d * tt[c];
-  s += tt[c - 1];
-  s += tt[c + 1];
-  s += tt[c - T::W];
-  s += tt[c + T::W];
-  s += tt[c - T::W * T::W];
-  s += tt[c + T::W * T::W];
-  L.res[i] = s;
+  rs[j][k] = res;
+  __syncthreads();
+  if (cown) {
+    const int cx = ck % CB, cy = (ck / CB) % CB, cz = ck / (CB * CB);
+    float sum = 0.0f;
+    if (cl)
+      for (int q = 0; q < 8; ++q)
+        sum += rs[cj][(2 * cx + (q & 1)) + B * ((2 * cy + ((q >> 1) & 1)) + B * (2 * cz + ((q >> 2) & 1)))];
+    Cl.rhs[(long long)cslot * CC + ck] = cl ? 0.5f * sum : 0.0f;
+  }
 }
 
 // ------------------------------------------ the faces, one CTA per brick
@@ -1408,11 +1442,17 @@ void vcycle(fluid_pp_atlas* A, cudaStream_t s, bool vin) {
     else if (L.B == 2) k_at_smooth_t<2, 16><<<(L.nblocks + 15) / 16, 128, 0, s>>>(A->d_inst, l, colour, zero);
     else k_at_smooth<<<grid_n(L.n), kAT, 0, s>>>(A->d_inst, l, colour, zero);
   };
-  auto residual = [&](int l) {
+  // the residual and its restriction into level l + 1 (one kernel where level
+  // l + 1 holds the same bricks' blocks)
+  auto residual_restrict = [&](int l) {
     const ALevel& L = I.lv[l];
-    if (L.B == 4) k_at_residual_t<4, 2><<<(L.nblocks + 1) / 2, 128, 0, s>>>(A->d_inst, l);
+    if (l == 0) k_at_residual0<<<I.nb, 256, 0, s>>>(A->d_inst);
+    else if (L.B == 4) k_at_residual_t<4, 2><<<(L.nblocks + 1) / 2, 128, 0, s>>>(A->d_inst, l);
     else if (L.B == 2) k_at_residual_t<2, 16><<<(L.nblocks + 15) / 16, 128, 0, s>>>(A->d_inst, l);
-    else k_at_residual<<<grid_n(L.n), kAT, 0, s>>>(A->d_inst, l);
+    else {
+      k_at_residual<<<grid_n(L.n), kAT, 0, s>>>(A->d_inst, l);
+      k_at_restrict<<<grid_n(I.lv[l + 1].n), kAT, 0, s>>>(A->d_inst, l);
+    }
   };
   for (int l = 0; l < grid_last; ++l) {
     const int g = grid_n(I.lv[l].n);
@@ -1424,16 +1464,14 @@ void vcycle(fluid_pp_atlas* A, cudaStream_t s, bool vin) {
         k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 0);
         k_at_smooth0<<<I.nb, 256, 0, s>>>(A->d_inst, 1);
       }
-      k_at_residual0<<<I.nb, 256, 0, s>>>(A->d_inst);
     } else {
       smooth(l, 1, 0);
       for (int k = 1; k < A->pre; ++k) {
         smooth(l, 0, 0);
         smooth(l, 1, 0);
       }
-      residual(l);
     }
-    k_at_restrict<<<grid_n(I.lv[l + 1].n), kAT, 0, s>>>(A->d_inst, l);
+    residual_restrict(l);
   }
   if (fs > 0) k_at_vsmall<<<1, 1024, 0, s>>>(A->d_inst, fs, A->pre, A->post);
   else k_at_coarse_apply<<<1, 1024, 0, s>>>(A->d_inst);
