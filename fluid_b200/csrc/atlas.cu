@@ -279,7 +279,7 @@ __device__ __forceinline__ void block_reduce(double (&v)[K], double* part) {
     for (int k = 0; k < K; ++k) part[4 * blockIdx.x + k] = sh[k][0];
 }
 
-__global__ void __launch_bounds__(kAT) k_at_fold(AInst* I, int K, int slot0) {
+__device__ __forceinline__ void at_fold(AInst* I, int K, int slot0) {
   __shared__ double sh[4][kAT];
   double v[4] = {0, 0, 0, 0};
   for (int b = threadIdx.x; b < kRedGrid; b += kAT)
@@ -294,6 +294,8 @@ __global__ void __launch_bounds__(kAT) k_at_fold(AInst* I, int K, int slot0) {
   if (threadIdx.x == 0)
     for (int k = 0; k < K; ++k) I->ctrl->red[slot0 + k] = sh[k][0];
 }
+
+__global__ void __launch_bounds__(kAT) k_at_fold(AInst* I, int K, int slot0) { at_fold(I, K, slot0); }
 
 // Nullspace: mean of each unanchored component (one CTA each, fixed order),
 // then the subtraction.
@@ -549,7 +551,9 @@ __global__ void __launch_bounds__(256) k_at_spmv0(AInst* I, double* bpart) {
 
 // Folds the per-brick partials into ctrl->red[0]: 256 threads each sum a
 // fixed stride of bricks, then a fixed tree.
-__global__ void __launch_bounds__(256) k_at_fold_bricks(AInst* I, const double* bpart) {
+// keep_gamma: first move the folded gamma (red[0]) to ctrl->gamma, which
+// red[0] is about to be overwritten by delta (the CG's set-gamma step).
+__global__ void __launch_bounds__(256) k_at_fold_bricks(AInst* I, const double* bpart, int keep_gamma) {
   __shared__ double sh[256];
   double s = 0.0;
   for (int b = threadIdx.x; b < I->nb; b += 256) s += bpart[b];
@@ -559,7 +563,10 @@ __global__ void __launch_bounds__(256) k_at_fold_bricks(AInst* I, const double* 
     if (int(threadIdx.x) < o) sh[threadIdx.x] += sh[threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x == 0) I->ctrl->red[0] = sh[0];
+  if (threadIdx.x == 0) {
+    if (keep_gamma && !I->ctrl->done) I->ctrl->gamma = I->ctrl->red[0];
+    I->ctrl->red[0] = sh[0];
+  }
 }
 
 // Finer level index of child k (0 .. 7) of coarse cell c, -1 if none.
@@ -777,11 +784,7 @@ __global__ void k_at_dir(AInst* I) {
   A_CELLS(L) I->d[i] = L.label[i] ? I->q[i] + beta * I->d[i] : 0.0;
 }
 
-__global__ void k_at_set_gamma(AInst* I) {
-  ACtrl* C = I->ctrl;
-  if (C->done) return;
-  C->gamma = C->red[0];
-}
+
 
 // q = A d, delta = d . q
 __global__ void __launch_bounds__(kAT) k_at_spmv(AInst* I) {
@@ -835,7 +838,8 @@ __global__ void __launch_bounds__(kAT) k_at_true(AInst* I) {
 // After an update: count the iteration, stop on the tolerance (the
 // recursive float64 residual, as projectSparseAtlasVelocity does), the cap,
 // or a non-finite residual.
-__global__ void k_at_check(AInst* I) {
+// The stopping test on the folded rr (red[0]).
+__device__ __forceinline__ void at_check(AInst* I) {
   ACtrl* C = I->ctrl;
   if (C->done) return;
   const double rr = C->red[0];
@@ -856,6 +860,12 @@ __global__ void k_at_check(AInst* I) {
     C->done = 1;
     C->status = FLUID_PP_NONCONVERGENCE;
   }
+}
+
+// The fold of rr (red[0]) and the stopping test in one launch.
+__global__ void __launch_bounds__(kAT) k_at_fold_check(AInst* I) {
+  at_fold(I, 1, 0);
+  if (threadIdx.x == 0) at_check(I);   // the thread that wrote red[0]
 }
 
 __global__ void k_at_init(AInst* I, double thr_rel, double thr_abs, int max_iter) {
@@ -1508,10 +1518,9 @@ void iteration(fluid_pp_atlas* A, cudaStream_t s) {
   }
   k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 0);
   k_at_dir<<<g0, kAT, 0, s>>>(A->d_inst);
-  k_at_set_gamma<<<1, 1, 0, s>>>(A->d_inst);
   proj(A, I.d, s);
   k_at_spmv0<<<I.nb, 256, 0, s>>>(A->d_inst, I.bpart);
-  k_at_fold_bricks<<<1, 256, 0, s>>>(A->d_inst, I.bpart);
+  k_at_fold_bricks<<<1, 256, 0, s>>>(A->d_inst, I.bpart, 1);   // also sets gamma from red[0]
   if (fused && I.precond) k_at_update<true><<<kRedGrid, kAT, 0, s>>>(A->d_inst);
   else k_at_update<false><<<kRedGrid, kAT, 0, s>>>(A->d_inst);
   if (I.ncomp) {
@@ -1519,8 +1528,7 @@ void iteration(fluid_pp_atlas* A, cudaStream_t s) {
     proj(A, I.r, s);
     k_at_rr<<<kRedGrid, kAT, 0, s>>>(A->d_inst);
   }
-  k_at_fold<<<1, kAT, 0, s>>>(A->d_inst, 1, 0);
-  k_at_check<<<1, 1, 0, s>>>(A->d_inst);
+  k_at_fold_check<<<1, kAT, 0, s>>>(A->d_inst);
 }
 
 // The iteration as a CUDA graph, captured once per upload and preconditioner
