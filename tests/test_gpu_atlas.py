@@ -179,3 +179,33 @@ def test_a_port_takes_the_lower_bricks_copy():
     np.testing.assert_array_equal(out[0][2], out[1][2])
     np.testing.assert_array_equal(out[0][3], out[1][3])
     dense_faces((s.nx, s.ny, s.nz), coords, out[1][3])   # both copies of every port agree
+
+
+@pytest.mark.parametrize("sweeps", [1, 3])
+def test_atlas_sweep_counts_match_fp64_dense_oracle(sweeps):
+    """One and three red-black sweeps per level (the tiled level 0-2 kernels,
+    the fused residual-restriction and the one-CTA tail all run them) give the
+    float64 dense oracle's pressure; more sweeps never take more iterations."""
+    s = configs.atlas_scene(64, 48, 56, seed=7)
+    coords = configs.atlas_bricks(s.vof)
+    dens, faces = bricks_from_dense(s.vof, s.u, s.v, s.w, coords)
+    A = AtlasProjector((s.nx, s.ny, s.nz), s.h, s.rho)
+    its = {}
+    for k in (sweeps, 2):
+        A.upload(coords, dens, faces)
+        rec = A.project(s.dt, rel_tol=1e-7, pre_sweeps=k, post_sweeps=k)
+        assert rec["status_name"] == "OK" and rec["true_rel_residual"] <= 2e-7, rec
+        its[k] = rec["iterations"]
+        if k == sweeps:
+            p, _ = A.download()
+    A.destroy()
+    assert (its[sweeps] >= its[2]) if sweeps < 2 else (its[sweeps] <= its[2])
+    o = Oracle(s.nx, s.ny, s.nz, s.h, s.rho)
+    o.set_state(s.vof, s.u, s.v, s.w, s.dt)
+    p_ref, info = o.solve_mgpcg(1e-12, 0.0, 400, 2, 2)
+    assert info["converged"] == 1.0
+    pscale = s.rho * s.h / s.dt
+    got = np.zeros_like(p_ref)
+    for k, (bx, by, bz) in enumerate(coords):
+        got[bz * 8:bz * 8 + 8, by * 8:by * 8 + 8, bx * 8:bx * 8 + 8] = p[k] / pscale
+    assert np.linalg.norm(got - p_ref) <= 1e-5 * np.linalg.norm(p_ref)
