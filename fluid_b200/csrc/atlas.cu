@@ -400,24 +400,39 @@ __device__ __forceinline__ void brick_nbrs(const AInst* I, int slot, int* nb) {
   if (threadIdx.x < 6) nb[threadIdx.x] = I->bnb[6 * slot + threadIdx.x];
 }
 
+// Two adjacent values of a brick row as one aligned load (cells 2q, 2q + 1).
+template <class T> struct Pair;
+template <> struct Pair<float> { using V = float2; };
+template <> struct Pair<double> { using V = double2; };
+template <> struct Pair<uint8_t> { using V = uchar2; };
+
 // Stage the brick's values and its halos (nb: the brick's neighbours, already
-// visible to every thread); ends with a barrier.
+// visible to every thread); ends with a barrier.  The body is read as row
+// pairs; halo entry e (face f = e / 64, face cell u = e % 8, w = e / 8 % 8)
+// is the neighbour's cell on the shared face (f = 2 a + (side > 0)).
 template <class T>
 __device__ __forceinline__ void load_tile(int slot, const int* nb, const T* v, T* t) {
-  const T* src = v + (long long)slot * kCells;
-  for (int k = threadIdx.x; k < kCells; k += blockDim.x) t[tix(k & 7, (k >> 3) & 7, k >> 6)] = src[k];
-  for (int k = threadIdx.x; k < 6 * 64; k += blockDim.x) {
-    const int f = k >> 6, u = k & 7, w = (k >> 3) & 7;
-    const int a = f >> 1, sd = (f & 1) ? 1 : -1;
-    // the halo cell (one step outside the brick) and the neighbour's cell it mirrors
-    int h[3], m[3];
-    if (a == 0) { h[0] = sd > 0 ? kRes : -1; h[1] = u; h[2] = w; }
-    else if (a == 1) { h[0] = u; h[1] = sd > 0 ? kRes : -1; h[2] = w; }
-    else { h[0] = u; h[1] = w; h[2] = sd > 0 ? kRes : -1; }
-    m[0] = h[0]; m[1] = h[1]; m[2] = h[2];
-    m[a] = sd > 0 ? 0 : kRes - 1;
+  using V = typename Pair<T>::V;
+  const V* src = reinterpret_cast<const V*>(v + (long long)slot * kCells);
+  for (int q = threadIdx.x; q < kCells / 2; q += blockDim.x) {
+    const V p = src[q];
+    const int k = 2 * q, c = tix(k & 7, (k >> 3) & 7, k >> 6);
+    t[c] = p.x;
+    t[c + 1] = p.y;
+  }
+  for (int e = threadIdx.x; e < 6 * 64; e += blockDim.x) {
+    const int f = e >> 6, u = e & 7, w = (e >> 3) & 7;
+    int c, o;   // tile index, cell of the neighbour brick
+    switch (f) {
+      case 0: c = (w + 1) * 100 + (u + 1) * 10; o = (kRes - 1) + kRes * (u + kRes * w); break;
+      case 1: c = (w + 1) * 100 + (u + 1) * 10 + kRes + 1; o = kRes * (u + kRes * w); break;
+      case 2: c = (w + 1) * 100 + (u + 1); o = u + kRes * ((kRes - 1) + kRes * w); break;
+      case 3: c = (w + 1) * 100 + (kRes + 1) * 10 + (u + 1); o = u + kRes * kRes * w; break;
+      case 4: c = (w + 1) * 10 + (u + 1); o = u + kRes * (w + kRes * (kRes - 1)); break;
+      default: c = (kRes + 1) * 100 + (w + 1) * 10 + (u + 1); o = u + kRes * w; break;
+    }
     const int ns = nb[f];
-    t[tix(h[0], h[1], h[2])] = ns >= 0 ? v[(long long)ns * kCells + m[0] + kRes * (m[1] + kRes * m[2])] : T(0);
+    t[c] = ns >= 0 ? v[(long long)ns * kCells + o] : T(0);
   }
   __syncthreads();
 }
